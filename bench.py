@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""RK3 cell-updates/s of the WFE per-step hot path on B200.
+
+Workload: the WK82-type supercell of cases/wk82_160.ini -- 160 x 160 x 40
+cells at 1 km, stretched 20 km column, moist WK82 sounding with straight-line
+shear, +3 K bubble, Kessler + mixed-phase microphysics, dt = 6 s with 6
+acoustic substeps, FP32 state (the precision the reference runs in).  A "step"
+is one large RK3 step (3 stages, 1 + 3 + 6 acoustic substeps, Kessler).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours       K steps replayed from captured CUDA graphs, timed with CUDA events on
+           the library's stream, max over ranks; N > 1 runs one independent
+           member per GPU (weak scaling, no collective on the data path).
+           Also: a per-kernel CUDA-event profile of one extra step (roofline of
+           the dominant kernel), an end-to-end run through the C ABI with host
+           buffers at the reference driver's I/O cadence, and (rank 0, N = 1)
+           the CPU oracle on a bounded sample as the CPU baseline.
+reference  the reference's own CUDA implementation, compiled from its sources
+           (oracle/_ref/refdump_f32, its Integrator::step through its C++ API)
+           on the same GPU, same case, K steps after W warm-up steps.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CASE = ROOT / "cases" / "wk82_160.ini"
+METRIC = "RK3 cell-updates/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM = 6650.0  # GB/s, used only when MEASURED_PEAKS.json is absent
+
+# Algorithmic FP32 fields per cell of each kernel (unique fields a launch must
+# read or write; moist case, no boundary relaxation).  Bytes = fields x 4.
+KERNEL_FIELDS = {
+    # u', v' new, w, pi', theta', tw, ttheta, theta_b^w, dtheta_b/dz, rtjx, rtjy,
+    # kt3, aw, qv, qc, qr, qv_b (17 reads) + w, pi'_next, theta' (3 writes)
+    "acoustic_column": 20,
+    # u, v, pi', pi'_prev, theta', theta_b, tu, tv, qv (9 reads) + u, v (2 writes)
+    "acoustic_uv": 11,
+    # u v w theta' qv qc qr (est) + qv qc qr (time n) + rho_b rho_b^w mfx mfy mfz
+    # (15 reads) + tu tv tw ttheta + qv qc qr stage values (7 writes)
+    "tendencies": 22,
+    "mass_flux": 8,     # u v w rho_b rho_b^w -> mfx mfy mfz
+    "kessler": 12,      # theta' pi' qv qc qr theta_b pi_b rho_b -> theta' qv qc qr
+    "pd_ratio": 8,
+    "fill_ghosts": 0,   # surface-area only
+}
+# Per cell and step, the reference-set algorithmic bytes (moist + Kessler, ns=6):
+# 3 x 19 slow-tendency fields + 10 x 26 acoustic fields + 12 Kessler fields.
+STEP_FIELDS = 3 * 19 + 10 * 26 + 12
+
+
+def peaks():
+    if PEAKS.exists():
+        d = json.loads(PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sync_device(world):
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+    except Exception:
+        pass
+
+
+def cpu_baseline(steps_cap: float = 20.0):
+    """CPU oracle (FP64, OpenMP over all host cores) on the same workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    o = O.Case(CASE)
+    it = o.integrator()
+    it.set_state(o.initial_state())
+    cells = o.nx * o.ny * o.nz
+    n, t0 = 0, time.perf_counter()
+    while True:
+        it.step(o.dt, n * o.dt)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > steps_cap or n >= 3:
+            break
+    return {"value": cells * n / el, "unit": "cell-updates/s", "cores": O.threads(),
+            "kind": "port",
+            "sample": f"{n} RK3 steps of the full 160x160x40 WK82 case from t=0, FP64 CPU oracle "
+                      f"(oracle/wfe_oracle.cpp, OpenMP), {el:.1f} s"}
+
+
+def run_reference(args) -> dict:
+    exe = ROOT / "oracle" / "_ref" / "refdump_f32"
+    if not exe.exists():
+        return {"impl": "reference", "unavailable": "oracle/_ref/refdump_f32 not built"}
+    cmd = [str(exe), str(CASE), "/tmp/wfe_refbench", "mode=bench", f"warmup={args.warmup}",
+           f"steps={args.steps}"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    m = re.search(r"refbench cells=(\d+) steps=(\d+) ms=([\d.]+)", r.stdout)
+    if r.returncode != 0 or not m:
+        return {"impl": "reference", "unavailable": f"reference run failed: {r.stderr[-200:]}"}
+    cells, steps, ms = int(m.group(1)), int(m.group(2)), float(m.group(3))
+    v = cells * steps / (ms / 1000.0)
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s",
+        "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (analytic WK82 sounding, seeded nothing: deterministic bubble)",
+        "config": {"workload": "WK82 supercell 160x160x40, dx=1 km, 20 km stretched top, "
+                               "moist + Kessler, dt=6 s, ns=6",
+                   "case": "cases/wk82_160.ini", "l2": "per-step working set > L2 (126 MB)"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                         "sample": f"{steps} steps of the same case through the reference's own "
+                                   "Integrator::step, its CUDA build compiled from its sources "
+                                   "for sm_100a (FP32); the reference has no CPU path"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def e2e_run(W, case_ini, steps: int, device: int):
+    """End to end through the public API with host buffers, at the reference
+    driver's cadence (src/main.cpp:425-467): initial state uploaded from host,
+    every step the |w| watchdog read back, diagnostics (w, theta', pi', qc, qr)
+    every diag_interval and the full state every out_interval downloaded."""
+    import numpy as np
+
+    c = W.Case(case_ini, precision="f32", device=device)
+    host = {k: c.field(k, interior=True, dtype=np.float32) for k in W.FIELDS}
+    diag_every = max(1, round(120.0 / c.dt))
+    out_every = max(1, round(600.0 / c.dt))
+    h2d = d2h = 0
+    sync_device(1)
+    t0 = time.perf_counter()
+    for k, a in host.items():
+        c.set_field(k, a, interior=True)
+        h2d += a.nbytes
+    for s in range(1, steps + 1):
+        c.run(1, c.dt, (s - 1) * c.dt)
+        wmax = c.field_absmax("w")
+        d2h += 4
+        if not wmax < 150.0:
+            raise RuntimeError(f"|w| watchdog tripped at step {s}: {wmax}")
+        if s % diag_every == 0:
+            for k in ("w", "thp", "pip", "qc", "qr"):
+                d2h += c.field(k, interior=True, dtype=np.float32).nbytes
+        if s % out_every == 0 or s == steps:
+            for k in W.FIELDS:
+                d2h += c.field(k, interior=True, dtype=np.float32).nbytes
+            d2h += c.rain(interior=True).astype(np.float32).nbytes
+    c.sync()
+    el = time.perf_counter() - t0
+    cells = c.nx * c.ny * c.nz
+    c.close()
+    return cells * steps / el, h2d / steps, d2h / steps, el
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_setup(args.gpus)
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    import wfe_b200 as W
+
+    c = W.Case(CASE, precision="f32", device=local)
+    cells = c.nx * c.ny * c.nz
+    c.run(args.warmup, c.dt, 0.0)
+    c.sync()
+    sampler = ClockSampler(local)
+    time.sleep(0.3)
+    barrier(world)
+    sync_device(world)
+    ms = c.time_run(args.steps, c.dt, args.warmup * c.dt)
+    sync_device(world)
+    barrier(world)
+    clocks = sampler.stop()
+    ms_max = reduce_max(ms, world)
+    value = cells * args.steps * world / (ms_max / 1000.0)
+    launches = c.launches_per_step()
+
+    # per-kernel device times of one more step (CUDA events around each launch)
+    kt = c.kernel_times(c.dt, (args.warmup + args.steps) * c.dt)
+    step_kernel_ms = sum(v[0] for v in kt.values())
+    dom = max(kt.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n) = dom
+    avg_ms = dom_ms / dom_n
+    alg_bytes = KERNEL_FIELDS.get(dom_name, 0) * 4 * cells
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dom_name)
+    c.close()
+
+    e2e = None
+    if not args.no_e2e:
+        ev, h2d, d2h, el = e2e_run(W, CASE, args.steps, local)
+        ev = reduce_max(1.0 / ev, world)  # slowest rank
+        e2e = {"value": world / ev, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (analytic WK82 sounding and bubble, deterministic)",
+            "config": {"workload": "WK82 supercell 160x160x40, dx=1 km, 20 km stretched top, "
+                                   "moist + Kessler, dt=6 s, ns=6",
+                       "case": "cases/wk82_160.ini", "precision": "f32",
+                       "parallelism": f"replicas x{world} (one member per GPU)",
+                       "l2": "no flush: per-step working set ~270 MB > L2 (126 MB)",
+                       "timing": "CUDA events on the library stream around graph replays"},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+                         "launches_per_step": dom_n},
+            "step_roofline": {"alg_bytes_per_cell": STEP_FIELDS * 4,
+                              "achieved_gbs": STEP_FIELDS * 4 * cells / (ms_max / args.steps / 1e3) / 1e9,
+                              "frac": STEP_FIELDS * 4 * cells / (ms_max / args.steps / 1e3) / 1e9 / hbm},
+            "kernel_ms_per_step": {k: round(v[0], 4) for k, v in kt.items()},
+            "kernel_sum_ms": step_kernel_ms,
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+/* wfe_b200 -- B200-native (sm_100a) implementation of the WFE per-step
+ * dynamical core and column physics, behind a plain C ABI.
+ *
+ * The reference (Xassemblianist/WFE) has no plugin or FFI layer: its operator
+ * API is the C++ free-function surface of src/dynamics/kernels.hpp:14-71,
+ * src/physics/kessler.hpp:17-18 and src/physics/surface.hpp:20-44,
+ * orchestrated by Integrator (src/dynamics/integrator.hpp:18-42) and set up by
+ * src/main.cpp:245-383.  Each entry point below names the reference interface
+ * it replaces.  All functions return WFE_OK (0) or an error code; the library
+ * never exits the process (the reference prints and calls exit(1):
+ * src/core/cuda_check.hpp:7-39).  wfe_last_error() returns the message of the
+ * last failure on a context (or of the last failed creation for NULL).
+ *
+ * Layouts at the boundary are the reference's: WFE_LAYOUT_PADDED is the
+ * GDims buffer (NX = nx+6, NY = ny+6, NZ = nz+7, ng = 3, i fastest;
+ * src/core/grid.hpp:22-36); WFE_LAYOUT_INTERIOR is the Writer's interior
+ * float layout (nz, or nz+1 for w, x ny x nx; src/io/writer.cpp:89-107).
+ * Internally the fields are pitched for the B200; no device memory or torch
+ * types cross this boundary.
+ */
+#ifndef WFE_B200_H
+#define WFE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct wfe_ctx wfe_ctx;
+
+enum {
+  WFE_OK = 0,
+  WFE_ERR_ARG = 1,     /* bad argument */
+  WFE_ERR_CUDA = 2,    /* CUDA failure or no device (there is no CPU fallback) */
+  WFE_ERR_CONFIG = 3,  /* case configuration error (reference: exit 1) */
+  WFE_ERR_IO = 4,      /* input / boundary file error (reference: exit 1) */
+  WFE_ERR_NAN = 5,     /* non-finite state (reference main: exit 2) */
+  WFE_ERR_WABORT = 6   /* |w| above w_abort (reference main: exit 3) */
+};
+enum { WFE_F32 = 0, WFE_F64 = 1 };
+enum { WFE_U = 0, WFE_V, WFE_W, WFE_THP, WFE_PIP, WFE_QV, WFE_QC, WFE_QR };
+enum { WFE_ROLE_STATE = 0, WFE_ROLE_TEND = 1, WFE_ROLE_WORK = 2, WFE_ROLE_PIPREV = 3 };
+enum { WFE_LAYOUT_PADDED = 0, WFE_LAYOUT_INTERIOR = 1 };
+enum { WFE_DTYPE_F64 = 0, WFE_DTYPE_F32 = 1 };
+enum { WFE_2D_RAIN = 0, WFE_2D_TSK = 1, WFE_2D_PBLH = 2, WFE_2D_T2M = 3, WFE_2D_U10 = 4 };
+
+/* ------------------------------------------------------------- set-up */
+
+/* Reads a case .ini plus "key=value" overrides and builds everything
+ * src/main.cpp:248-383 builds before its time loop: grid, DynParams, Gal-Chen
+ * metric (Metric::build, src/core/metric.cpp:12-168), base state
+ * (BaseState::build, src/core/base_state.cpp:21-193), the initial state
+ * (idealised or file mode), the boundary manager and the surface physics,
+ * then uploads it to `device` (Integrator::init, integrator.cpp:43-69).
+ * precision: WFE_F32 or WFE_F64 (the reference's WFE_DOUBLE build).
+ * device < 0 builds the host set-up only (no GPU needed; the get_* calls
+ * work, every device call returns WFE_ERR_CUDA). */
+int wfe_case_create(const char* ini_path, const char* const* overrides, int n_overrides,
+                    int precision, int device, wfe_ctx** out);
+/* Same, from the text of a case file instead of a path. */
+int wfe_case_create_text(const char* ini_text, const char* const* overrides, int n_overrides,
+                         int precision, int device, wfe_ctx** out);
+int wfe_ctx_destroy(wfe_ctx* ctx);
+const char* wfe_last_error(const wfe_ctx* ctx);
+
+/* dims: nx ny nz ng NX NY NZ; spacing: dx dy dz dt t_end zt */
+int wfe_get_dims(const wfe_ctx* ctx, int dims[7]);
+int wfe_get_spacing(const wfe_ctx* ctx, double out[6]);
+/* flags: moisture microphysics pd_moist bc_x_open bc_y_open w_damping
+ *        file_mode physics_on boundary_on acoustic_ns */
+int wfe_get_flags(const wfe_ctx* ctx, int flags[10]);
+
+/* Host copies of the set-up arrays (reference padded layout, FP64):
+ * metric: 0..3 zeta_w zeta_c dzeta_c dzeta_w [NZ], 4..11 h hx hy hx_u hy_v
+ * jac fcor mapf [NX*NY] (DevMetric, src/core/metric.hpp:16-30);
+ * base: 0..8 thb pib rhob dthbdz thbw rhobw thvb thvbw qvb [NX*NY*NZ], 9 ub
+ * [NZ] (DevProf, src/core/base_state.hpp:16-27).  These never touch the GPU. */
+int wfe_get_metric(const wfe_ctx* ctx, int which, double* out);
+int wfe_get_base(const wfe_ctx* ctx, int which, double* out);
+
+/* --------------------------------------------------------- field I/O */
+
+/* Field3D::upload / download (src/core/field3d.hpp:38-43) of one prognostic
+ * field of a role: WFE_ROLE_STATE is Integrator::state() (time n),
+ * WFE_ROLE_TEND the slow tendencies (u v w thp pip qv qc qr), WFE_ROLE_WORK
+ * the acoustic work state, WFE_ROLE_PIPREV the pi' of the previous acoustic
+ * substep (field ignored).  dtype: WFE_DTYPE_F64 / F32 of the host buffer. */
+int wfe_field_upload(wfe_ctx* ctx, int role, int field, const void* host, int dtype, int layout);
+int wfe_field_download(wfe_ctx* ctx, int role, int field, void* host, int dtype, int layout);
+/* 2D fields (Integrator::rain, SfcPBL::tsk/pblh/t2m/u10) as padded NX*NY or
+ * interior ny*nx */
+int wfe_field2d_download(wfe_ctx* ctx, int which, void* host, int dtype, int layout);
+
+/* ----------------------------------------------------------- stepping */
+
+/* Integrator::step(dt, t) (src/dynamics/integrator.cpp:71-111): one
+ * Wicker-Skamarock RK3 large step with split-explicit acoustic substeps, then
+ * Kessler and the surface physics; boundary relaxation targets are switched
+ * as BdyManager::update (src/dynamics/boundary.cpp:83-89) does. */
+int wfe_step(wfe_ctx* ctx, double dt, double t);
+/* nsteps such steps from t0, replayed from captured CUDA graphs (the device
+ * clock advances inside the graph); asynchronous until wfe_sync. */
+int wfe_run(wfe_ctx* ctx, int nsteps, double dt, double t0);
+int wfe_sync(wfe_ctx* ctx);
+/* field_absmax (src/dynamics/kernels.cu:967-979): max |f| of a state field,
+ * NaN reported as a value above every finite one. */
+int wfe_absmax(wfe_ctx* ctx, int field, float* out);
+/* FP64 dry-air mass of the state [kg] (no reference counterpart). */
+int wfe_dry_mass(wfe_ctx* ctx, double* out);
+/* launches of the package's own kernels per large step in the last
+ * wfe_step / wfe_run */
+long wfe_launches_per_step(const wfe_ctx* ctx);
+
+/* nsteps graph-replayed steps timed with CUDA events recorded on the
+ * library's own stream; *ms = elapsed device time (no reference counterpart;
+ * the reference times sections with host clocks under WFE_PROF,
+ * src/dynamics/integrator.cpp:18-40). */
+int wfe_time_run(wfe_ctx* ctx, int nsteps, double dt, double t0, double* ms);
+/* One direct step with CUDA events around every kernel launch; per kernel
+ * name (comma-separated in names_csv) the summed device time and launch
+ * count.  Advances the state like wfe_step. */
+int wfe_kernel_times(wfe_ctx* ctx, double dt, double t, int cap, double* total_ms, int* counts,
+                     char* names_csv, int names_len, int* n_out);
+
+/* ------------------------------------------------- operator-level API */
+/* apply_bcs (src/dynamics/kernels.cu:805-835) on the state */
+int wfe_op_apply_bcs(wfe_ctx* ctx);
+/* compute_mass_fluxes + compute_divergence + compute_tendencies (+ bdy_relax
+ * when a boundary is set, at time t: BdyManager::tfrac) (kernels.cu:837-913,
+ * 981-995): state -> tend */
+int wfe_op_tendencies(wfe_ctx* ctx, double dt, double t);
+/* nsub x acoustic_substep (kernels.cu:929-965) starting from a copy of the
+ * state (as Integrator::step does at a stage): result in WFE_ROLE_WORK */
+int wfe_op_acoustic(wfe_ctx* ctx, double dtau, int nsub);
+/* update_moisture_stage (kernels.cu:997-1005): work.q = state.q + dt tend.q */
+int wfe_op_moisture_stage(wfe_ctx* ctx, double dt);
+/* kessler_step (src/physics/kessler.cu:143-149) on the state */
+int wfe_op_kessler(wfe_ctx* ctx, double dt);
+/* SfcPBL::step (src/physics/surface.cu:499-514) on the state, t = end of step */
+int wfe_op_sfc(wfe_ctx* ctx, double dt, double t);
+
+/* BdyManager with caller-supplied targets (u v thp pip qv, padded layout,
+ * FP64) and weights (padded NX*NY): lo/hi valid at t_lo/t_hi. */
+int wfe_set_boundary(wfe_ctx* ctx, const double* const lo[5], const double* const hi[5],
+                     const double* wgt, double t_lo, double t_hi);
+/* SfcPBL::init (surface.cu:440-482) from interior ny*nx FP64 arrays. */
+int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const double* lat,
+                    const double* lon, const double* soilw, double start_hour_utc, int doy,
+                    int nonlocal);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

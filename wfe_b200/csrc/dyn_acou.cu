@@ -1,0 +1,414 @@
+// Split-explicit acoustic substep on the B200 (src/dynamics/kernels.cu:445-688).
+//
+// Two launches per substep replace the reference's 9-11:
+//   k_acoustic_uv      forward u, v update with divergence damping, full
+//                      theta_v PGF, terrain cross term and map factor, plus the
+//                      Klemp-Wilhelmson radiation faces (open) or the periodic
+//                      face (u(nx) = u(0)) computed in the same thread;
+//   k_acoustic_column  the vertically implicit w - pi' system of a column
+//                      (off-centred, Thomas), theta' stratification update and
+//                      diagnostic surface w.  A CTA owns CX whole columns; the
+//                      column coefficients live in shared memory, the per-level
+//                      phases run in parallel over k and the Thomas sweep runs
+//                      in one lane per column (the reference keeps seven
+//                      320-deep arrays per thread in local memory).
+//
+// No ghost-fill launch is needed inside the acoustic loop: pi' at a ghost point
+// is read from the mapped interior point of the current buffer (the reference
+// refreshes pi' ghosts after every substep), while pi'_prev, theta' and qv at
+// lateral ghosts come from the time-n state (the reference's copies are made at
+// the stage start and never refreshed: kernels.cu:946-963, integrator.cpp:93-94).
+// u, v, theta' and pi' are double buffered by the integrator, so the column
+// kernel may read neighbours while the next substep's buffers are written.
+#include <cuda_runtime.h>
+
+#include "core.cuh"
+#include "kernels.cuh"
+
+namespace wfe {
+
+// ---------------------------------------------------- run-constant coefficients
+template <typename R>
+__global__ void k_coef_centre(Layout L, DBase<R> b, DMetric<R> m, R* rtjc, R* kt3, R* aw) {
+  // kernels.cu:452-464 over the whole padded grid
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - kOX;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - kOY;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z) - kOZ;
+  if (i + kOX >= L.px || j + kOY >= L.py || k + kOZ >= L.pz) return;
+  const size_t c = L.at(i, j, k);
+  R J = m.jac[L.at2(i, j)];
+  rtjc[c] = b.rhob[c] * b.thvb[c] * J;
+  kt3[c] = Phys<R>::Rd * b.pib[c] / (Phys<R>::cv * b.rhob[c] * b.thvb[c] * J);
+  aw[c] = b.rhobw[c] * b.thvbw[c];
+}
+
+template <typename R>
+__global__ void k_coef_face(Layout L, const R* rtjc, R* rtjx, R* rtjy) {
+  // kernels.cu:466-474: face averages; the first padded row/column of the
+  // reference layout (i = -3, j = -3) keeps the centre value
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - kOX;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - kOY;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z) - kOZ;
+  if (i + kOX >= L.px || j + kOY >= L.py || k + kOZ >= L.pz) return;
+  const size_t c = L.at(i, j, k);
+  rtjx[c] = (i > -kRefNG) ? (R)0.5 * (rtjc[c - 1] + rtjc[c]) : rtjc[c];
+  rtjy[c] = (j > -kRefNG) ? (R)0.5 * (rtjc[c - L.px] + rtjc[c]) : rtjc[c];
+}
+
+// ------------------------------------------------------------ forward u, v
+template <typename R>
+__device__ __forceinline__ R pistar(const AcouArgs<R>& a, int i, int j, int k) {
+  // pi* = pi' + smdiv (pi' - pi'_prev)  (kernels.cu:486-489)
+  const Layout& L = a.L;
+  const bool ghost = i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz;
+  R cur, prev;
+  if (!ghost) {
+    const size_t c = L.at(i, j, k);
+    cur = a.pi_cur[c];
+    prev = a.pi_prev[c];
+  } else {
+    const size_t c = L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open),
+                          map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), map_zc(k, L.nz));
+    cur = a.pi_cur[c];
+    prev = a.n_pip[c];
+  }
+  return cur + a.p.acoustic_smdiv * (cur - prev);
+}
+
+template <typename R>
+__device__ __forceinline__ R theta_v(const AcouArgs<R>& a, int i, int j, int k) {
+  // full virtual potential temperature at a cell centre (kernels.cu:490-495)
+  const Layout& L = a.L;
+  const bool lat = i < 0 || i >= L.nx || j < 0 || j >= L.ny;
+  const size_t c = L.at(i, j, k);
+  size_t s = c;
+  if (lat)
+    s = L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open), map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), k);
+  R t = a.b.thb[c] + (lat ? a.n_thp[s] : a.th_in[c]);
+  if (a.p.moisture) t *= (R)1 + Phys<R>::eps61 * a.qv[s];
+  return t;
+}
+
+template <typename R>
+__device__ __forceinline__ R u_forward(const AcouArgs<R>& a, int i, int j, int k) {
+  // kernels.cu:499-512
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const R zt = a.m.zt;
+  R thbu = (R)0.5 * (theta_v(a, i - 1, j, k) + theta_v(a, i, j, k));
+  R mu = (R)0.5 * (a.m.mapf[L.at2(i - 1, j)] + a.m.mapf[L.at2(i, j)]);
+  R grad = (pistar(a, i, j, k) - pistar(a, i - 1, j, k)) / a.dx;
+  R zxu = a.m.hx_u[L.at2(i, j)] * ((R)1 - a.m.zeta_c[kk] / zt);
+  if (zxu != (R)0) {
+    R dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
+    R ju = (R)0.5 * (a.m.jac[L.at2(i - 1, j)] + a.m.jac[L.at2(i, j)]);
+    R dpdz = (R)0.5 *
+             ((pistar(a, i - 1, j, k + 1) - pistar(a, i - 1, j, k - 1)) +
+              (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
+             dzc2;
+    grad -= zxu / ju * dpdz;
+  }
+  const size_t c = L.at(i, j, k);
+  return a.u_in[c] + a.dtau * (-Phys<R>::cp * thbu * mu * grad + a.tu[c]);
+}
+
+template <typename R>
+__device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k) {
+  // kernels.cu:513-526
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const R zt = a.m.zt;
+  R thbv = (R)0.5 * (theta_v(a, i, j - 1, k) + theta_v(a, i, j, k));
+  R mv = (R)0.5 * (a.m.mapf[L.at2(i, j - 1)] + a.m.mapf[L.at2(i, j)]);
+  R grad = (pistar(a, i, j, k) - pistar(a, i, j - 1, k)) / a.dy;
+  R zyv = a.m.hy_v[L.at2(i, j)] * ((R)1 - a.m.zeta_c[kk] / zt);
+  if (zyv != (R)0) {
+    R dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
+    R jv = (R)0.5 * (a.m.jac[L.at2(i, j - 1)] + a.m.jac[L.at2(i, j)]);
+    R dpdz = (R)0.5 *
+             ((pistar(a, i, j - 1, k + 1) - pistar(a, i, j - 1, k - 1)) +
+              (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
+             dzc2;
+    grad -= zyv / jv * dpdz;
+  }
+  const size_t c = L.at(i, j, k);
+  return a.v_in[c] + a.dtau * (-Phys<R>::cp * thbv * mv * grad + a.tv[c]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_acoustic_uv(AcouArgs<R> a) {
+  const Layout& L = a.L;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > L.nx || j > L.ny || k >= L.nz) return;
+  const int kk = L.at1(k);
+  const R cstar = a.p.cstar;
+  if (j < L.ny) {  // u on x faces 0..nx
+    R out;
+    if (a.p.bc_x_open) {
+      if (i == 0) {  // kernels.cu:654-660
+        R u0 = a.u_in[L.at(0, j, k)];
+        if (u0 >= (R)0) out = a.b.ub[kk];
+        else {
+          R cb = u0 - cstar;
+          out = u0 - a.dtau * cb * (u_forward(a, 1, j, k) - u0) / a.dx;
+        }
+      } else if (i == L.nx) {  // kernels.cu:661-667
+        R un = a.u_in[L.at(L.nx, j, k)];
+        if (un <= (R)0) out = a.b.ub[kk];
+        else {
+          R cb = un + cstar;
+          out = un - a.dtau * cb * (un - u_forward(a, L.nx - 1, j, k)) / a.dx;
+        }
+      } else {
+        out = u_forward(a, i, j, k);
+      }
+    } else {
+      out = u_forward(a, i == L.nx ? 0 : i, j, k);  // periodic face u(nx) = u(0)
+    }
+    a.u_out[L.at(i, j, k)] = out;
+  }
+  if (i < L.nx) {  // v on y faces 0..ny
+    R out;
+    if (a.p.bc_y_open) {
+      if (j == 0) {  // kernels.cu:674-680
+        R v0 = a.v_in[L.at(i, 0, k)];
+        if (v0 >= (R)0) out = 0;
+        else {
+          R cb = v0 - cstar;
+          out = v0 - a.dtau * cb * (v_forward(a, i, 1, k) - v0) / a.dy;
+        }
+      } else if (j == L.ny) {  // kernels.cu:681-687
+        R vn = a.v_in[L.at(i, L.ny, k)];
+        if (vn <= (R)0) out = 0;
+        else {
+          R cb = vn + cstar;
+          out = vn - a.dtau * cb * (vn - v_forward(a, i, L.ny - 1, k)) / a.dy;
+        }
+      } else {
+        out = v_forward(a, i, j, k);
+      }
+    } else {
+      out = v_forward(a, i, j == L.ny ? 0 : j, k);
+    }
+    a.v_out[L.at(i, j, k)] = out;
+  }
+}
+
+// ------------------------------------------------- implicit w - pi' columns
+// Shared-memory column arrays, level-major so that the CX lanes of a level
+// hit distinct banks: X(k, col) = base[k * CX + col].
+template <typename R, int CX>
+struct ColSmem {
+  R *Av, *Sv, *P, *E, *A, *B, *C, *D, *Wn;
+  __device__ ColSmem(R* s, int nz1) {
+    size_t n = (size_t)nz1 * CX;
+    Av = s; Sv = Av + n; P = Sv + n; E = P + n; A = E + n; B = A + n; C = B + n; D = C + n;
+    Wn = D + n;
+  }
+};
+
+template <typename R, int CX>
+__global__ void k_acoustic_column(AcouArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Layout& L = a.L;
+  const int nz = L.nz;
+  ColSmem<R, CX> S(reinterpret_cast<R*>(smem_raw), nz + 1);
+  const int tx = threadIdx.x;           // column within the CTA
+  const int lane_k = threadIdx.y;       // level lane
+  const int KL = blockDim.y;
+  const int i = blockIdx.x * CX + tx;
+  const int j = blockIdx.y;
+  const bool active = i < L.nx;
+  const R dtau = a.dtau, zt = a.m.zt;
+  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
+  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
+  const size_t c2d = L.at2(active ? i : 0, j);
+  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
+  const R* u = a.u_out;
+  const R* v = a.v_out;
+  const long sx = 1, sy = L.px;
+#define SM(X, k) S.X[(size_t)(k) * CX + tx]
+
+  // phase 1: Av = rho^w theta_v^w (0 at the rigid levels) and the explicit
+  // terrain cross flux Sv with the new u, v (kernels.cu:552-568)
+  if (active)
+    for (int k = lane_k; k <= nz; k += KL) {
+      R av = 0, sv = 0;
+      if (k >= 1 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = L.at(i, j, k);
+        av = a.co.aw[c];
+        R fac = (R)1 - a.m.zeta_w[kk] / zt;
+        const size_t cm = c - (size_t)L.plane();
+        R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+        R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+        sv = av * (uw * hxc + vw * hyc) * fac;
+      }
+      SM(Av, k) = av;
+      SM(Sv, k) = sv;
+    }
+  __syncthreads();
+  // phase 2: explicit part of the pi' equation (kernels.cu:570-587)
+  if (active)
+    for (int k = lane_k; k < nz; k += KL) {
+      const int kk = L.at1(k);
+      const size_t c = L.at(i, j, k);
+      R Kt = a.co.kt3[c];
+      R Dh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
+                   (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
+      R dzc = a.m.dzeta_c[kk];
+      R wk = a.w_in[c], wkp = a.w_in[c + L.plane()];
+      R tpi = a.tpi ? a.tpi[c] : (R)0;
+      SM(P, k) = a.pi_cur[c] + dtau * tpi -
+                 dtau * Kt *
+                     (Dh - (SM(Sv, k + 1) - SM(Sv, k)) / dzc +
+                      c2 * (SM(Av, k + 1) * wkp - SM(Av, k) * wk) / dzc);
+      SM(E, k) = dtau * Kt * c1 / dzc;
+    }
+  __syncthreads();
+  // phase 3: tridiagonal rows for w at inner levels (kernels.cu:589-611)
+  if (active)
+    for (int k = 1 + lane_k; k < nz; k += KL) {
+      const int kk = L.at1(k);
+      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+      R thc = a.th_in[c], thm = a.th_in[cm];
+      R thvw = a.b.thbw[c] + (R)0.5 * (thm + thc);
+      if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
+      R G = dtau * Phys<R>::cp * thvw * c1 / (J * a.m.dzeta_w[kk]);
+      R Em = SM(E, k - 1), Ek = SM(E, k);
+      SM(A, k) = -G * Em * SM(Av, k - 1);
+      SM(B, k) = (R)1 + G * SM(Av, k) * (Ek + Em);
+      SM(C, k) = -G * Ek * SM(Av, k + 1);
+      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / a.b.thbw[c];
+      if (a.p.moisture) {
+        R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
+        R qcr = (R)0.5 * (a.qc[cm] + a.qc[c]) + (R)0.5 * (a.qr[cm] + a.qr[c]);
+        buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
+      }
+      R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
+              dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) / (J * a.m.dzeta_w[kk]);
+      SM(D, k) = RHS - G * (SM(P, k) - SM(P, k - 1));
+    }
+  __syncthreads();
+  // phase 4: Thomas sweep, one lane per column (kernels.cu:612-634)
+  if (active && lane_k == 0) {
+    for (int k = 1; k < nz; ++k) {
+      R Ck = SM(C, k), Dk = SM(D, k), Bk = SM(B, k);
+      if (k == 1) {
+        SM(C, k) = Ck / Bk;
+        SM(D, k) = Dk / Bk;
+      } else {
+        R Ak = SM(A, k);
+        R mm = Bk - Ak * SM(C, k - 1);
+        SM(C, k) = Ck / mm;
+        SM(D, k) = (Dk - Ak * SM(D, k - 1)) / mm;
+      }
+    }
+    SM(Wn, nz) = 0;
+    R wabove = 0;
+    for (int k = nz - 1; k >= 1; --k) {
+      R wk = SM(D, k) - SM(C, k) * wabove;
+      SM(Wn, k) = wk;
+      wabove = wk;
+    }
+    const size_t c0 = L.at(i, j, 0);
+    R us = (R)0.5 * (u[c0] + u[c0 + sx]);
+    R vs = (R)0.5 * (v[c0] + v[c0 + sy]);
+    SM(Wn, 0) = us * hxc + vs * hyc;
+  }
+  __syncthreads();
+  // phase 5: pi', theta', w (kernels.cu:636-644)
+  if (active)
+    for (int k = lane_k; k <= nz; k += KL) {
+      const size_t c = L.at(i, j, k);
+      if (k < nz) {
+        R wn = SM(Wn, k), wn1 = SM(Wn, k + 1);
+        a.pi_next[c] = SM(P, k) - SM(E, k) * (SM(Av, k + 1) * wn1 - SM(Av, k) * wn);
+        R wc = (R)0.5 * (wn + wn1);
+        a.th_out[c] = a.th_in[c] + dtau * (a.tth[c] - wc * a.b.dthbdz[c]);
+        a.w_out[c] = wn;
+      } else {
+        a.w_out[c] = 0;
+      }
+    }
+#undef SM
+}
+
+// ------------------------------------------------------------ host launch
+template <typename R>
+void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,
+                          R* rtjx, R* rtjy, R* kt3, R* aw, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  dim3 grd((L.px + 31) / 32, (L.py + 3) / 4, (L.pz + 1) / 2);
+  k_coef_centre<R><<<grd, blk, 0, st>>>(L, b, m, scratch, kt3, aw);
+  k_coef_face<R><<<grd, blk, 0, st>>>(L, scratch, rtjx, rtjy);
+}
+
+template <typename R>
+void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  dim3 grd((a.L.nx + 1 + 31) / 32, (a.L.ny + 1 + 3) / 4, (a.L.nz + 1) / 2);
+  k_acoustic_uv<R><<<grd, blk, 0, st>>>(a);
+}
+
+template <typename R>
+size_t column_smem(int nz, int cx) {
+  return (size_t)9 * (nz + 1) * cx * sizeof(R);
+}
+
+template <typename R, int CX>
+static cudaError_t column_attr(size_t sm) {
+  return cudaFuncSetAttribute(k_acoustic_column<R, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm);
+}
+
+// columns per CTA: 32 while the column arrays fit in shared memory, else 16 or 8
+template <typename R>
+static int column_cx(int nz) {
+  const size_t lim = 200 * 1024;
+  if (column_smem<R>(nz, 32) <= lim) return 32;
+  if (column_smem<R>(nz, 16) <= lim) return 16;
+  if (column_smem<R>(nz, 8) <= lim) return 8;
+  return 0;
+}
+
+// Sets the dynamic shared-memory limit of the column kernel once, outside any
+// stream capture.
+template <typename R>
+int prepare_acoustic_column(int nz) {
+  int cx = column_cx<R>(nz);
+  if (!cx) return 2;
+  cudaError_t e = cx == 32   ? column_attr<R, 32>(column_smem<R>(nz, 32))
+                  : cx == 16 ? column_attr<R, 16>(column_smem<R>(nz, 16))
+                             : column_attr<R, 8>(column_smem<R>(nz, 8));
+  return e == cudaSuccess ? 0 : 1;
+}
+
+template <typename R>
+int launch_acoustic_column(const AcouArgs<R>& a, cudaStream_t st) {
+  const int nz = a.L.nz;
+  const int cx = column_cx<R>(nz);
+  if (cx == 32)
+    k_acoustic_column<R, 32><<<dim3((a.L.nx + 31) / 32, a.L.ny), dim3(32, 8), column_smem<R>(nz, 32), st>>>(a);
+  else if (cx == 16)
+    k_acoustic_column<R, 16><<<dim3((a.L.nx + 15) / 16, a.L.ny), dim3(16, 16), column_smem<R>(nz, 16), st>>>(a);
+  else if (cx == 8)
+    k_acoustic_column<R, 8><<<dim3((a.L.nx + 7) / 8, a.L.ny), dim3(8, 32), column_smem<R>(nz, 8), st>>>(a);
+  else
+    return 2;
+  return 0;
+}
+
+#define WFE_INST(R)                                                                            \
+  template void launch_acoustic_coef<R>(const Layout&, const DBase<R>&, const DMetric<R>&, R*, \
+                                        R*, R*, R*, R*, cudaStream_t);                         \
+  template void launch_acoustic_uv<R>(const AcouArgs<R>&, cudaStream_t);                       \
+  template int launch_acoustic_column<R>(const AcouArgs<R>&, cudaStream_t);                    \
+  template int prepare_acoustic_column<R>(int);
+WFE_INST(float)
+WFE_INST(double)
+#undef WFE_INST
+
+}  // namespace wfe

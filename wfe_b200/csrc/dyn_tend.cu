@@ -1,0 +1,455 @@
+// Slow-tendency path of one RK3 stage on the B200: one ghost-fill launch,
+// one mass-flux launch, an optional positive-definite-limiter launch and one
+// fused tendency launch that evaluates every prognostic tendency of a cell
+// (5th-order flux-form advection of u, v, w, theta', qv, qc, qr with the
+// Gal-Chen metric, Coriolis, Rayleigh sponge, w damping, constant-K diffusion
+// and Davies relaxation) and, in the integrator, writes the moisture stage
+// value q_n + dt_m * tq directly instead of storing tq.
+//
+// The arithmetic of every output value follows the reference expression by
+// expression (src/dynamics/kernels.cu:42-443, 292-304, 268-273) so that the
+// FP64 build agrees with the reference FP64 build to rounding.
+#include <cuda_runtime.h>
+
+#include "core.cuh"
+#include "kernels.cuh"
+
+namespace wfe {
+
+// ------------------------------------------------------------------ helpers
+template <typename R>
+__device__ __forceinline__ R sponge(R zeta, R zt, const DParams<R>& p) {
+  // src/dynamics/kernels.cu:42-48
+  if (p.rayleigh_zd < (R)0) return 0;
+  if (zeta <= p.rayleigh_zd || zt <= p.rayleigh_zd) return 0;
+  const R halfpi = (R)1.5707963267948966;
+  R s = sin(halfpi * (zeta - p.rayleigh_zd) / (zt - p.rayleigh_zd));
+  return p.rayleigh_alpha * s * s;
+}
+
+template <typename R>
+__device__ __forceinline__ R face5(R qm2, R qm1, R q0, R q1, R q2, R q3, R vel) {
+  // 5th-order upwind interface value (src/dynamics/kernels.cu:51-57)
+  const R c = (R)(1.0 / 60.0);
+  R cen = c * ((R)37 * (q0 + q1) - (R)8 * (qm1 + q2) + (qm2 + q3));
+  R upw = c * ((q3 - qm2) - (R)5 * (q2 - qm1) + (R)10 * (q1 - q0));
+  return (vel >= (R)0) ? (cen - upw) : (cen + upw);
+}
+
+// -------------------------------------------------------------- ghost fill
+// One launch fills the ghost rings of up to 8 fields with the composition of
+// the reference's fill order z -> x -> y (kernels.cu:692-835): a ghost value
+// is the z rule applied to the laterally mapped source column.  kind: 0 cell
+// scalar, 1 u (x faces 0..nx), 2 v (y faces 0..ny), 3 w (levels 0..nz,
+// w(nz) = 0, odd reflection about w(0) below, about w(nz) above).
+template <typename R>
+__global__ void k_fill_ghosts(Layout L, GhostJob<R> job, int open_x, int open_y) {
+  const int f = blockIdx.z;
+  if (f >= job.n) return;
+  R* a = job.f[f];
+  const int kind = job.kind[f];
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - kRefNG;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - kRefNG;
+  if (i > L.nx + 2 || j > L.ny + 2) return;
+  const int ilast = (kind == 1 && open_x) ? L.nx : L.nx - 1;
+  const int jlast = (kind == 2 && open_y) ? L.ny : L.ny - 1;
+  const int si = map_lat(i, L.nx, ilast, open_x);
+  const int sj = map_lat(j, L.ny, jlast, open_y);
+  const bool lateral_ghost = (si != i) || (sj != j);
+  const int k0 = -kRefNG, k1 = L.nz + kRefNG;  // inclusive
+  if (kind == 3) {
+    R w0 = a[L.at(si, sj, 0)];
+    for (int k = k0; k <= k1; ++k) {
+      R val;
+      if (k == L.nz) val = 0;
+      else if (k >= 0 && k < L.nz) {
+        if (!lateral_ghost) continue;
+        val = a[L.at(si, sj, k)];
+      } else if (k < 0) val = (R)2 * w0 - a[L.at(si, sj, -k)];
+      else val = -a[L.at(si, sj, 2 * L.nz - k)];
+      a[L.at(i, j, k)] = val;
+    }
+  } else {
+    for (int k = k0; k <= k1; ++k) {
+      int sk = map_zc(k, L.nz);
+      if (!lateral_ghost && sk == k) continue;
+      a[L.at(i, j, k)] = a[L.at(si, sj, sk)];
+    }
+  }
+}
+
+// ------------------------------------------------------------- mass fluxes
+// rho_b J weighted horizontal fluxes on the ring -2..n+2 and the
+// contravariant vertical flux on -2..n+1 (kernels.cu:68-97); w levels 0 and
+// nz carry Omega = 0.
+template <typename R>
+__global__ void k_mass_flux(Layout L, DBase<R> b, DMetric<R> m, const R* __restrict__ u,
+                            const R* __restrict__ v, const R* __restrict__ w, R* __restrict__ mfx,
+                            R* __restrict__ mfy, R* __restrict__ mfz) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 2;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 2;
+  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z);
+  if (i > L.nx + 2 || j > L.ny + 2 || k > L.nz) return;
+  const size_t c = L.at(i, j, k);
+  if (k < L.nz) {
+    R rjx = (R)0.5 * (b.rhob[L.at(i - 1, j, k)] * m.jac[L.at2(i - 1, j)] + b.rhob[c] * m.jac[L.at2(i, j)]);
+    mfx[c] = rjx * u[c];
+    R rjy = (R)0.5 * (b.rhob[L.at(i, j - 1, k)] * m.jac[L.at2(i, j - 1)] + b.rhob[c] * m.jac[L.at2(i, j)]);
+    mfy[c] = rjy * v[c];
+  }
+  if (i > L.nx + 1 || j > L.ny + 1) return;
+  if (k == 0 || k == L.nz) {
+    mfz[c] = 0;
+    return;
+  }
+  const int kk = L.at1(k);
+  R fac = (R)1 - m.zeta_w[kk] / m.zt;
+  R uw = (R)0.25 * (u[L.at(i, j, k - 1)] + u[L.at(i + 1, j, k - 1)] + u[c] + u[L.at(i + 1, j, k)]);
+  R vw = (R)0.25 * (v[L.at(i, j, k - 1)] + v[L.at(i, j + 1, k - 1)] + v[c] + v[L.at(i, j + 1, k)]);
+  R cross = (uw * m.hx[L.at2(i, j)] + vw * m.hy[L.at2(i, j)]) * fac;
+  mfz[c] = b.rhobw[c] * (w[c] - cross);
+}
+
+// divergence of the mass flux at cell (i,j,k) (kernels.cu:99-110), evaluated
+// where needed instead of being stored
+template <typename R>
+__device__ __forceinline__ R divergence(const TendArgs<R>& a, int i, int j, int k) {
+  const Layout& L = a.L;
+  return (a.mfx[L.at(i + 1, j, k)] - a.mfx[L.at(i, j, k)]) / a.dx +
+         (a.mfy[L.at(i, j + 1, k)] - a.mfy[L.at(i, j, k)]) / a.dy +
+         (a.mfz[L.at(i, j, k + 1)] - a.mfz[L.at(i, j, k)]) / a.m.dzeta_c[L.at1(k)];
+}
+
+// Flux-form advection of a cell-centred scalar (kernels.cu:114-179).
+template <typename R>
+__device__ __forceinline__ R scalar_adv(const TendArgs<R>& a, const R* __restrict__ q, int i, int j,
+                                        int k, R div) {
+  const Layout& L = a.L;
+  const size_t c = L.at(i, j, k);
+  const size_t sx = 1, sy = L.px, sz = L.plane();
+  const R* Q = q + c;
+  R fxL = a.mfx[c], fxR = a.mfx[c + sx];
+  R fyL = a.mfy[c], fyR = a.mfy[c + sy];
+  R fzB = a.mfz[c], fzT = a.mfz[c + sz];
+  R FxL = fxL * face5(Q[-3 * (long)sx], Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], fxL);
+  R FxR = fxR * face5(Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], Q[3 * sx], fxR);
+  R FyL = fyL * face5(Q[-3 * (long)sy], Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], fyL);
+  R FyR = fyR * face5(Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], Q[3 * sy], fyR);
+  R FzB = fzB * face5(Q[-3 * (long)sz], Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], fzB);
+  R FzT = fzT * face5(Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], Q[3 * sz], fzT);
+  R fdiv = (FxR - FxL) / a.dx + (FyR - FyL) / a.dy + (FzT - FzB) / a.m.dzeta_c[L.at1(k)];
+  R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
+  return (-fdiv + Q[0] * div) / rt;
+}
+
+// Face fluxes of a scalar used by the positive-definite limiter
+// (kernels.cu:187-218): F on the left/lower face of cell (i,j,k).
+template <typename R>
+__device__ __forceinline__ R qflux_x(const TendArgs<R>& a, const R* q, int i, int j, int k) {
+  const size_t c = a.L.at(i, j, k);
+  R f = a.mfx[c];
+  const R* Q = q + c;
+  return f * face5(Q[-3], Q[-2], Q[-1], Q[0], Q[1], Q[2], f);
+}
+template <typename R>
+__device__ __forceinline__ R qflux_y(const TendArgs<R>& a, const R* q, int i, int j, int k) {
+  const size_t c = a.L.at(i, j, k);
+  const long s = a.L.px;
+  R f = a.mfy[c];
+  const R* Q = q + c;
+  return f * face5(Q[-3 * s], Q[-2 * s], Q[-s], Q[0], Q[s], Q[2 * s], f);
+}
+template <typename R>
+__device__ __forceinline__ R qflux_z(const TendArgs<R>& a, const R* q, int i, int j, int k) {
+  const size_t c = a.L.at(i, j, k);
+  const long s = (long)a.L.plane();
+  R f = a.mfz[c];
+  const R* Q = q + c;
+  return f * face5(Q[-3 * s], Q[-2 * s], Q[-s], Q[0], Q[s], Q[2 * s], f);
+}
+
+// Outflow ratio min(1, available / outgoing) per species (kernels.cu:221-238).
+template <typename R>
+__global__ void k_pd_ratio(TendArgs<R> a, R* __restrict__ rv, R* __restrict__ rc,
+                           R* __restrict__ rr) {
+  const Layout& L = a.L;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+  const R dzc = a.m.dzeta_c[L.at1(k)];
+  const R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
+  const R* qs[3] = {a.qv, a.qc, a.qr};
+  R* outs[3] = {rv, rc, rr};
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const R* q = qs[s];
+    R out = fmax((R)0, qflux_x(a, q, i + 1, j, k)) / a.dx + fmax((R)0, -qflux_x(a, q, i, j, k)) / a.dx +
+            fmax((R)0, qflux_y(a, q, i, j + 1, k)) / a.dy + fmax((R)0, -qflux_y(a, q, i, j, k)) / a.dy +
+            fmax((R)0, qflux_z(a, q, i, j, k + 1)) / dzc + fmax((R)0, -qflux_z(a, q, i, j, k)) / dzc;
+    R avail = rt * fmax((R)0, q[L.at(i, j, k)]);
+    R r = (a.dt * out > (R)1e-20) ? avail / (a.dt * out) : (R)1;
+    outs[s][L.at(i, j, k)] = fmin((R)1, r);
+  }
+}
+
+// ratio at a possibly-ghost cell: lateral periodic / zero-gradient map
+// (kernels.cu:864-866); vertical neighbours only multiply a zero flux.
+template <typename R>
+__device__ __forceinline__ R ratio_at(const TendArgs<R>& a, const R* ratio, int i, int j, int k) {
+  const Layout& L = a.L;
+  int si = map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open);
+  int sj = map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open);
+  int sk = map_zc(k, L.nz);
+  return ratio[L.at(si, sj, sk)];
+}
+
+// Renormalised positive-definite advection (kernels.cu:241-264).
+template <typename R>
+__device__ __forceinline__ R pd_adv(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j,
+                                    int k, R div) {
+  const Layout& L = a.L;
+  R fxl = qflux_x(a, q, i, j, k), fxr = qflux_x(a, q, i + 1, j, k);
+  R fyl = qflux_y(a, q, i, j, k), fyr = qflux_y(a, q, i, j + 1, k);
+  R fzl = qflux_z(a, q, i, j, k), fzr = qflux_z(a, q, i, j, k + 1);
+  R sxl = fxl * ratio_at(a, ratio, fxl >= (R)0 ? i - 1 : i, j, k);
+  R sxr = fxr * ratio_at(a, ratio, fxr >= (R)0 ? i : i + 1, j, k);
+  R syl = fyl * ratio_at(a, ratio, i, fyl >= (R)0 ? j - 1 : j, k);
+  R syr = fyr * ratio_at(a, ratio, i, fyr >= (R)0 ? j : j + 1, k);
+  R szl = fzl * ratio_at(a, ratio, i, j, fzl >= (R)0 ? k - 1 : k);
+  R szr = fzr * ratio_at(a, ratio, i, j, fzr >= (R)0 ? k : k + 1);
+  R fdiv = (sxr - sxl) / a.dx + (syr - syl) / a.dy + (szr - szl) / a.m.dzeta_c[L.at1(k)];
+  R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
+  return (-fdiv + q[L.at(i, j, k)] * div) / rt;
+}
+
+// Constant-K Laplacian (kernels.cu:430-443).
+template <typename R>
+__device__ __forceinline__ R laplacian(const TendArgs<R>& a, const R* f, int i, int j, int k,
+                                       bool on_w) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  R dzl = (on_w ? a.m.dzeta_w[kk] : a.m.dzeta_c[kk]) * a.m.jac[L.at2(i, j)];
+  const size_t c = L.at(i, j, k);
+  R cc = f[c];
+  return (f[c + 1] - 2 * cc + f[c - 1]) / (a.dx * a.dx) +
+         (f[c + L.px] - 2 * cc + f[c - L.px]) / (a.dy * a.dy) +
+         (f[c + L.plane()] - 2 * cc + f[c - L.plane()]) / (dzl * dzl);
+}
+
+template <typename R>
+__device__ __forceinline__ R time_fraction(const double* clk) {
+  // BdyManager::tfrac (src/dynamics/boundary.cpp:91-97)
+  double t = clk[CLK_T], lo = clk[CLK_TLO], hi = clk[CLK_THI];
+  if (hi <= lo) return 0;
+  double f = (t - lo) / (hi - lo);
+  return (R)(f < 0 ? 0.0 : (f > 1 ? 1.0 : f));
+}
+
+template <typename R>
+__device__ __forceinline__ R davies(const TendArgs<R>& a, int v, const R* f, int i, int j, int k) {
+  const Layout& L = a.L;
+  const R tf = time_fraction<R>(a.clock);
+  int iw = i < L.nx ? i : L.nx - 1, jw = j < L.ny ? j : L.ny - 1;
+  R w = a.wgt[L.at2(iw, jw)];
+  if (w <= (R)0) return 0;
+  size_t c = L.at(i, j, k);
+  return w * (((R)1 - tf) * a.lo[v][c] + tf * a.hi[v][c] - f[c]);
+}
+
+// ------------------------------------------------------ fused tendencies
+template <typename R>
+__global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
+  const Layout& L = a.L;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  const long sx = 1, sy = L.px, sz = (long)L.plane();
+  const R zt = a.m.zt;
+  const bool bdy = a.lo[0] != nullptr;
+  const R* MX = a.mfx + c;
+  const R* MY = a.mfy + c;
+  const R* MZ = a.mfz + c;
+  const R div0 = divergence(a, i, j, k);
+
+  // ---- u on the x face i (kernels.cu:308-346)
+  {
+    const R* U = a.u + c;
+    R fcL = (R)0.5 * (MX[-sx] + MX[0]), fcR = (R)0.5 * (MX[0] + MX[sx]);
+    R FxL = fcL * face5(U[-3 * sx], U[-2 * sx], U[-sx], U[0], U[sx], U[2 * sx], fcL);
+    R FxR = fcR * face5(U[-2 * sx], U[-sx], U[0], U[sx], U[2 * sx], U[3 * sx], fcR);
+    R fyB = (R)0.5 * (MY[-sx] + MY[0]), fyT = (R)0.5 * (MY[sy - sx] + MY[sy]);
+    R FyB = fyB * face5(U[-3 * sy], U[-2 * sy], U[-sy], U[0], U[sy], U[2 * sy], fyB);
+    R FyT = fyT * face5(U[-2 * sy], U[-sy], U[0], U[sy], U[2 * sy], U[3 * sy], fyT);
+    R fzB = (R)0.5 * (MZ[-sx] + MZ[0]), fzT = (R)0.5 * (MZ[sz - sx] + MZ[sz]);
+    R FzB = fzB * face5(U[-3 * sz], U[-2 * sz], U[-sz], U[0], U[sz], U[2 * sz], fzB);
+    R FzT = fzT * face5(U[-2 * sz], U[-sz], U[0], U[sz], U[2 * sz], U[3 * sz], fzT);
+    R fdiv = (FxR - FxL) / a.dx + (FyT - FyB) / a.dy + (FzT - FzB) / a.m.dzeta_c[kk];
+    R dv = (R)0.5 * (divergence(a, i - 1, j, k) + div0);
+    R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+    const R* V = a.v + c;
+    R vavg = (R)0.25 * (V[-sx] + V[sy - sx] + V[0] + V[sy]);
+    R fc = (R)0.5 * (a.m.fcor[L.at2(i - 1, j)] + a.m.fcor[L.at2(i, j)]);
+    R relax = -sponge(a.m.zeta_c[kk], zt, a.p) * (U[0] - a.b.ub[kk]);
+    R t = (-fdiv + U[0] * dv) / ru + fc * vavg + relax;
+    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.u, i, j, k, false);
+    if (bdy) t += davies(a, 0, a.u, i, j, k);
+    a.tu[c] = t;
+  }
+  // ---- v on the y face j (kernels.cu:348-385)
+  {
+    const R* V = a.v + c;
+    R fcB = (R)0.5 * (MY[-sy] + MY[0]), fcT = (R)0.5 * (MY[0] + MY[sy]);
+    R FyB = fcB * face5(V[-3 * sy], V[-2 * sy], V[-sy], V[0], V[sy], V[2 * sy], fcB);
+    R FyT = fcT * face5(V[-2 * sy], V[-sy], V[0], V[sy], V[2 * sy], V[3 * sy], fcT);
+    R fxL = (R)0.5 * (MX[-sy] + MX[0]), fxR = (R)0.5 * (MX[sx - sy] + MX[sx]);
+    R FxL = fxL * face5(V[-3 * sx], V[-2 * sx], V[-sx], V[0], V[sx], V[2 * sx], fxL);
+    R FxR = fxR * face5(V[-2 * sx], V[-sx], V[0], V[sx], V[2 * sx], V[3 * sx], fxR);
+    R fzB = (R)0.5 * (MZ[-sy] + MZ[0]), fzT = (R)0.5 * (MZ[sz - sy] + MZ[sz]);
+    R FzB = fzB * face5(V[-3 * sz], V[-2 * sz], V[-sz], V[0], V[sz], V[2 * sz], fzB);
+    R FzT = fzT * face5(V[-2 * sz], V[-sz], V[0], V[sz], V[2 * sz], V[3 * sz], fzT);
+    R fdiv = (FxR - FxL) / a.dx + (FyT - FyB) / a.dy + (FzT - FzB) / a.m.dzeta_c[kk];
+    R dv = (R)0.5 * (divergence(a, i, j - 1, k) + div0);
+    R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+    const R* U = a.u + c;
+    R uavg = (R)0.25 * (U[-sy] + U[sx - sy] + U[0] + U[sx]);
+    R fc = (R)0.5 * (a.m.fcor[L.at2(i, j - 1)] + a.m.fcor[L.at2(i, j)]);
+    R uref = a.p.coriolis_use_ub ? a.b.ub[kk] : (R)0;
+    R relax = -sponge(a.m.zeta_c[kk], zt, a.p) * V[0];
+    R t = (-fdiv + V[0] * dv) / rv - fc * (uavg - uref) + relax;
+    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.v, i, j, k, false);
+    if (bdy) t += davies(a, 1, a.v, i, j, k);
+    a.tv[c] = t;
+  }
+  // ---- w on the inner level k >= 1 (kernels.cu:387-425)
+  if (k >= 1) {
+    const R* W = a.w + c;
+    R fxL = (R)0.5 * (MX[-sz] + MX[0]), fxR = (R)0.5 * (MX[sx - sz] + MX[sx]);
+    R FxL = fxL * face5(W[-3 * sx], W[-2 * sx], W[-sx], W[0], W[sx], W[2 * sx], fxL);
+    R FxR = fxR * face5(W[-2 * sx], W[-sx], W[0], W[sx], W[2 * sx], W[3 * sx], fxR);
+    R fyB = (R)0.5 * (MY[-sz] + MY[0]), fyT = (R)0.5 * (MY[sy - sz] + MY[sy]);
+    R FyB = fyB * face5(W[-3 * sy], W[-2 * sy], W[-sy], W[0], W[sy], W[2 * sy], fyB);
+    R FyT = fyT * face5(W[-2 * sy], W[-sy], W[0], W[sy], W[2 * sy], W[3 * sy], fyT);
+    R fzB = (R)0.5 * (MZ[-sz] + MZ[0]), fzT = (R)0.5 * (MZ[0] + MZ[sz]);
+    R FzB = fzB * face5(W[-3 * sz], W[-2 * sz], W[-sz], W[0], W[sz], W[2 * sz], fzB);
+    R FzT = fzT * face5(W[-2 * sz], W[-sz], W[0], W[sz], W[2 * sz], W[3 * sz], fzT);
+    R fdiv = (FxR - FxL) / a.dx + (FyT - FyB) / a.dy + (FzT - FzB) / a.m.dzeta_w[kk];
+    R dv = (R)0.5 * (divergence(a, i, j, k - 1) + div0);
+    R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
+    R relax = -sponge(a.m.zeta_w[kk], zt, a.p) * W[0];
+    R wk = W[0];
+    if (a.p.w_damping) {
+      R cr = fabs(wk) * a.dt / (a.m.dzeta_w[kk] * a.m.jac[L.at2(i, j)]);
+      if (cr > (R)1) relax -= (R)0.3 * (cr - (R)1) * wk / a.dt;
+    }
+    R t = (-fdiv + wk * dv) / rw + relax;
+    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.w, i, j, k, true);
+    a.tw[c] = t;
+  }
+  // ---- theta' (kernels.cu:114-146)
+  {
+    R t = scalar_adv(a, a.thp, i, j, k, div0) - sponge(a.m.zeta_c[kk], zt, a.p) * a.thp[c];
+    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.thp, i, j, k, false);
+    if (bdy) t += davies(a, 2, a.thp, i, j, k);
+    a.tth[c] = t;
+  }
+  // ---- pi': no slow advection; Davies only (kernels.cu:900-901)
+  if (a.tpi) a.tpi[c] = bdy ? davies(a, 3, a.pip, i, j, k) : (R)0;
+  // ---- moisture (kernels.cu:886-899) and its stage update (kernels.cu:268-273)
+  if (a.p.moisture) {
+    const R* qs[3] = {a.qv, a.qc, a.qr};
+    const R* rs[3] = {a.ratio_v, a.ratio_c, a.ratio_r};
+    R* ts[3] = {a.tqv, a.tqc, a.tqr};
+    const R* qn[3] = {a.qn_v, a.qn_c, a.qn_r};
+    R* qo[3] = {a.qo_v, a.qo_c, a.qo_r};
+#pragma unroll 1
+    for (int s = 0; s < 3; ++s) {
+      R t = (a.p.pd_moist && rs[s]) ? pd_adv(a, qs[s], rs[s], i, j, k, div0)
+                                     : scalar_adv(a, qs[s], i, j, k, div0);
+      if (s == 0 && bdy) t += davies(a, 4, a.qv, i, j, k);
+      if (qo[s]) qo[s][c] = qn[s][c] + a.dt_stage * t;
+      else ts[s][c] = t;
+    }
+  }
+}
+
+// ------------------------------------------------------- small utilities
+__global__ void k_clock(double* clk, double t, double t_lo, double t_hi, double dt, int advance) {
+  if (advance) {
+    clk[CLK_T] += clk[CLK_DT];
+  } else {
+    clk[CLK_T] = t;
+    clk[CLK_TLO] = t_lo;
+    clk[CLK_THI] = t_hi;
+    clk[CLK_DT] = dt;
+  }
+}
+
+void launch_clock(double* clock, double t, double t_lo, double t_hi, double dt, int advance,
+                  cudaStream_t st) {
+  k_clock<<<1, 1, 0, st>>>(clock, t, t_lo, t_hi, dt, advance);
+}
+
+// out = x + a * y over every stored point (src/dynamics/kernels.cu:268-273)
+template <typename R>
+__global__ void k_axpy(const R* __restrict__ x, const R* __restrict__ y, R a, R* __restrict__ out,
+                       size_t n) {
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x)
+    out[q] = x[q] + a * y[q];
+}
+
+template <typename R>
+void launch_axpy(const R* x, const R* y, R a, R* out, size_t n, cudaStream_t st) {
+  int grd = (int)((n + 255) / 256);
+  if (grd > 148 * 16) grd = 148 * 16;
+  k_axpy<R><<<grd, 256, 0, st>>>(x, y, a, out, n);
+}
+
+// ------------------------------------------------------------ host launch
+template <typename R>
+void launch_fill_ghosts(const Layout& L, const GhostJob<R>& job, int open_x, int open_y,
+                        cudaStream_t st) {
+  if (job.n == 0) return;
+  dim3 blk(32, 4);
+  dim3 grd((L.nx + 6 + 31) / 32, (L.ny + 6 + 3) / 4, job.n);
+  k_fill_ghosts<R><<<grd, blk, 0, st>>>(L, job, open_x, open_y);
+}
+
+template <typename R>
+void launch_mass_flux(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* u,
+                      const R* v, const R* w, R* mfx, R* mfy, R* mfz, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  dim3 grd((L.nx + 5 + 31) / 32, (L.ny + 5 + 3) / 4, (L.nz + 1 + 1) / 2);
+  k_mass_flux<R><<<grd, blk, 0, st>>>(L, b, m, u, v, w, mfx, mfy, mfz);
+}
+
+template <typename R>
+void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  dim3 grd((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
+  k_pd_ratio<R><<<grd, blk, 0, st>>>(a, rv, rc, rr);
+}
+
+template <typename R>
+void launch_tendencies(const TendArgs<R>& a, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  dim3 grd((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
+  k_tendencies<R><<<grd, blk, 0, st>>>(a);
+}
+
+#define WFE_INST(R)                                                                               \
+  template void launch_fill_ghosts<R>(const Layout&, const GhostJob<R>&, int, int, cudaStream_t); \
+  template void launch_mass_flux<R>(const Layout&, const DBase<R>&, const DMetric<R>&, const R*,  \
+                                    const R*, const R*, R*, R*, R*, cudaStream_t);                \
+  template void launch_pd_ratio<R>(const TendArgs<R>&, R*, R*, R*, cudaStream_t);                 \
+  template void launch_tendencies<R>(const TendArgs<R>&, cudaStream_t);                         \
+  template void launch_axpy<R>(const R*, const R*, R, R*, size_t, cudaStream_t);
+WFE_INST(float)
+WFE_INST(double)
+#undef WFE_INST
+
+}  // namespace wfe

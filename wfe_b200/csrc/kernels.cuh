@@ -1,0 +1,134 @@
+// Argument blocks and launch entry points of the wfe_b200 device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "core.cuh"
+
+namespace wfe {
+
+// Up to 8 fields whose ghost rings one launch fills (kind: 0 cell scalar,
+// 1 u, 2 v, 3 w).
+template <typename R>
+struct GhostJob {
+  R* f[8];
+  int kind[8];
+  int n;
+};
+
+template <typename R>
+struct TendArgs {
+  Layout L;
+  DBase<R> b;
+  DMetric<R> m;
+  DParams<R> p;
+  R dx, dy, dt;                                   // grid spacing, large step
+  const R *u, *v, *w, *thp, *pip, *qv, *qc, *qr;  // stage estimate, ghosts filled
+  const R *mfx, *mfy, *mfz;                       // mass fluxes on the ring
+  const R *ratio_v, *ratio_c, *ratio_r;           // PD outflow ratios or null
+  R *tu, *tv, *tw, *tth, *tpi;                    // tpi may be null
+  R *tqv, *tqc, *tqr;                             // used when qo_* are null
+  const R *qn_v, *qn_c, *qn_r;                    // time-n moisture
+  R *qo_v, *qo_c, *qo_r;                          // stage moisture q_n + dt_stage*tq
+  R dt_stage;
+  const R* lo[5];                                 // Davies targets, lo[0] null if off
+  const R* hi[5];
+  const R* wgt;
+  const double* clock;  // device clock: t (step start), t_lo, t_hi of the targets
+};
+
+// Device clock read by time-dependent terms (Davies time interpolation,
+// surface solar geometry) so that captured step graphs stay valid:
+// [0] t at the start of the step, [1] t_lo, [2] t_hi, [3] dt.
+enum { CLK_T = 0, CLK_TLO = 1, CLK_THI = 2, CLK_DT = 3, CLK_N = 4 };
+
+template <typename R>
+struct AcouArgs {
+  Layout L;
+  DBase<R> b;
+  DMetric<R> m;
+  DCoef<R> co;
+  DParams<R> p;
+  R dx, dy, dtau;
+  const R *u_in, *v_in;
+  R *u_out, *v_out;
+  const R* w_in;
+  R* w_out;
+  const R *pi_prev, *pi_cur;
+  R* pi_next;
+  const R* th_in;
+  R* th_out;
+  const R *n_pip, *n_thp;          // time-n pi', theta' (ghost values)
+  const R *qv, *qc, *qr;           // time-n moisture, stage constant
+  const R *tu, *tv, *tw, *tth, *tpi;  // tpi may be null (no slow pi' tendency)
+};
+
+template <typename R>
+struct KesArgs {
+  Layout L;
+  DBase<R> b;
+  DMetric<R> m;
+  R dt;
+  R *thp, *qv, *qc, *qr, *rain;
+  const R* pip;
+};
+
+// Surface layer, PBL, soil and radiation columns (src/physics/surface.cu).
+template <typename R>
+struct SfcArgs {
+  Layout L;
+  DBase<R> b;
+  DMetric<R> m;
+  R dt;
+  double start_hour;
+  int doy, nonlocal;
+  const double* clock;  // utc from clock[CLK_T] + clock[CLK_DT]
+  R *thp, *qv, *u, *v;
+  const R *pip, *qc;
+  R *tsk, *km, *cdv, *pblh, *t2m, *u10, *soilt;
+  const R *tdeep, *land, *lat, *lon, *soilw;
+  R* scratch;  // sfc_scratch_count(L) elements of column work arrays
+};
+
+template <typename R>
+int launch_sfc(const SfcArgs<R>& a, cudaStream_t st);
+template <typename R>
+size_t sfc_scratch_count(const Layout& L);
+void launch_clock(double* clock, double t, double t_lo, double t_hi, double dt, int advance,
+                  cudaStream_t st);
+template <typename R>
+void launch_axpy(const R* x, const R* y, R a, R* out, size_t n, cudaStream_t st);
+
+template <typename R>
+void launch_fill_ghosts(const Layout& L, const GhostJob<R>& job, int open_x, int open_y,
+                        cudaStream_t st);
+template <typename R>
+void launch_mass_flux(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* u,
+                      const R* v, const R* w, R* mfx, R* mfy, R* mfz, cudaStream_t st);
+template <typename R>
+void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st);
+template <typename R>
+void launch_tendencies(const TendArgs<R>& a, cudaStream_t st);
+
+template <typename R>
+void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,
+                          R* rtjx, R* rtjy, R* kt3, R* aw, cudaStream_t st);
+template <typename R>
+void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st);
+template <typename R>
+int launch_acoustic_column(const AcouArgs<R>& a, cudaStream_t st);  // returns 0 ok
+template <typename R>
+int prepare_acoustic_column(int nz);
+template <typename R>
+int prepare_kessler(int nz);
+
+template <typename R>
+int launch_kessler(const KesArgs<R>& a, cudaStream_t st);
+template <typename R>
+void launch_absmax(const R* f, size_t n, unsigned int* result, cudaStream_t st);
+template <typename R>
+void launch_dry_mass(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* pip,
+                     const R* thp, const R* qv, const R* qc, const R* qr, int moist, R dx, R dy,
+                     double* plane_sums, double* result, cudaStream_t st);
+
+}  // namespace wfe

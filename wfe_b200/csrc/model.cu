@@ -1,0 +1,827 @@
+// ModelT<R>: device buffers, the RK3 large step and its CUDA-graph replay,
+// and the operator-level entry points of one case on one B200.
+//
+// Buffer roles.  Three full states rotate with period three: at the start of
+// a step S[perm[0]] holds time n (N); stage 0 writes S[perm[1]], stage 1
+// reads it and writes S[perm[2]], stage 2 reads that and writes S[perm[1]],
+// which becomes the next N.  The reference instead copies time n into a work
+// state at every stage (integrator.cpp:93-94: nine device copies per stage)
+// and swaps pointers, which is why its CUDA-graph attempt was reverted; the
+// fixed rotation lets three captured graphs (one per phase) replay any number
+// of steps.  Inside a stage the acoustic loop reads time n from N on its first
+// substep and double-buffers u, v (U2, V2) and rotates pi' through three
+// buffers (X.pip, P1, P2), so the last substep lands in the stage output X
+// without any copy.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "core.cuh"
+#include "kernels.cuh"
+#include "model.hpp"
+
+namespace wfe {
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e__ = (call);                                                     \
+    if (e__ != cudaSuccess) return fail(std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+template <typename R>
+class ModelT final : public Model {
+ public:
+  ~ModelT() override { release(); }
+
+  int init(const CaseSetup& cs, int device) {
+    cs_ = &cs;
+    g_ = cs.g;
+    hp_ = cs.p;
+    L_ = make_layout(g_.nx, g_.ny, g_.nz);
+    dev_ = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    if (prepare_acoustic_column<R>(g_.nz) || prepare_kessler<R>(g_.nz))
+      return fail("nz too large for the column kernels' shared memory");
+    const size_t n3 = L_.n3(), n2 = L_.n2(), n1 = L_.pz;
+    // metric
+    R* mbuf = alloc(4 * n1 + 8 * n2);
+    if (!mbuf) return 1;
+    const std::vector<double>* m1[4] = {&cs.m.zeta_w, &cs.m.zeta_c, &cs.m.dzeta_c, &cs.m.dzeta_w};
+    const std::vector<double>* m2[8] = {&cs.m.h, &cs.m.hx, &cs.m.hy, &cs.m.hx_u,
+                                        &cs.m.hy_v, &cs.m.jac, &cs.m.fcor, &cs.m.mapf};
+    R* mp[12];
+    for (int q = 0; q < 4; ++q) {
+      mp[q] = mbuf + q * n1;
+      if (put1d(mp[q], *m1[q])) return 1;
+    }
+    for (int q = 0; q < 8; ++q) {
+      mp[4 + q] = mbuf + 4 * n1 + q * n2;
+      if (put2d(mp[4 + q], *m2[q])) return 1;
+    }
+    dm_ = DMetric<R>{mp[0], mp[1], mp[2], mp[3], mp[4], mp[5], mp[6], mp[7],
+                     mp[8], mp[9], mp[10], mp[11], (R)cs.m.zt};
+    // base state
+    const std::vector<double>* b3[9] = {&cs.b.thb, &cs.b.pib, &cs.b.rhob, &cs.b.dthbdz, &cs.b.thbw,
+                                        &cs.b.rhobw, &cs.b.thvb, &cs.b.thvbw, &cs.b.qvb};
+    R* bp[10];
+    for (int q = 0; q < 9; ++q) {
+      bp[q] = alloc(n3);
+      if (!bp[q] || put3d(bp[q], *b3[q])) return 1;
+    }
+    bp[9] = alloc(n1);
+    if (!bp[9] || put1d(bp[9], cs.b.ub)) return 1;
+    db_ = DBase<R>{bp[0], bp[1], bp[2], bp[3], bp[4], bp[5], bp[6], bp[7], bp[8], bp[9]};
+    // parameters
+    dp_.diff_K = (R)hp_.diff_K;
+    dp_.rayleigh_zd = (R)hp_.rayleigh_zd;
+    dp_.rayleigh_alpha = (R)hp_.rayleigh_alpha;
+    dp_.acoustic_beta = (R)hp_.acoustic_beta;
+    dp_.acoustic_smdiv = (R)hp_.acoustic_smdiv;
+    dp_.cstar = (R)hp_.cstar;
+    dp_.w_abort = (R)hp_.w_abort;
+    dp_.acoustic_ns = hp_.acoustic_ns;
+    dp_.coriolis_use_ub = hp_.coriolis_use_ub ? 1 : 0;
+    dp_.bc_x_open = hp_.bc_x_open;
+    dp_.bc_y_open = hp_.bc_y_open;
+    dp_.moisture = hp_.moisture;
+    dp_.microphysics = hp_.microphysics;
+    dp_.pd_moist = hp_.pd_moist;
+    dp_.w_damping = hp_.w_damping;
+    // prognostic states, tendencies, scratch
+    for (int s = 0; s < 3; ++s)
+      for (int f = 0; f < 8; ++f)
+        if (!(S_[s][f] = alloc(n3))) return 1;
+    for (int f = 0; f < 8; ++f)
+      if (!(T_[f] = alloc(n3))) return 1;
+    for (R** p : {&mfx_, &mfy_, &mfz_, &U2_, &V2_, &P1_, &P2_})
+      if (!(*p = alloc(n3))) return 1;
+    if (hp_.pd_moist)
+      for (int s = 0; s < 3; ++s)
+        if (!(ratio_[s] = alloc(n3))) return 1;
+    // run-constant acoustic coefficients (kernels.cu:915-927)
+    for (R** p : {&rtjx_, &rtjy_, &kt3_, &aw_})
+      if (!(*p = alloc(n3))) return 1;
+    R* scratch = alloc(n3);
+    if (!scratch) return 1;
+    launch_acoustic_coef<R>(L_, db_, dm_, scratch, rtjx_, rtjy_, kt3_, aw_, st_);
+    CK(cudaStreamSynchronize(st_));
+    CK(cudaGetLastError());
+    co_ = DCoef<R>{rtjx_, rtjy_, kt3_, aw_};
+    if (!(rain_ = alloc(n2))) return 1;
+    CK(cudaMalloc(&clock_, CLK_N * sizeof(double)));
+    CK(cudaMemset(clock_, 0, CLK_N * sizeof(double)));
+    CK(cudaMalloc(&wd_, sizeof(unsigned int)));
+    CK(cudaMalloc(&mass_planes_, (size_t)g_.nz * sizeof(double)));
+    CK(cudaMalloc(&mass_, sizeof(double)));
+    CK(cudaMallocHost(&stage_, n3 * sizeof(R)));
+    // initial state
+    for (int f = 0; f < 8; ++f)
+      if (upload(ROLE_STATE, f, cs.state[f].data())) return 1;
+    return 0;
+  }
+
+  const RefGrid& grid() const override { return g_; }
+  bool fp64() const override { return sizeof(R) == 8; }
+  size_t pitched_count() const override { return L_.n3(); }
+  void pitched_dims(int* px, int* py, int* pz) const override {
+    *px = L_.px;
+    *py = L_.py;
+    *pz = L_.pz;
+  }
+  long launches_per_step() const override { return launches_; }
+
+  // ------------------------------------------------------------ transfers
+  R* field_ptr(int role, int field) {
+    if (field < 0 || field > 7) return nullptr;
+    switch (role) {
+      case ROLE_STATE: return S_[perm_[0]][field];
+      case ROLE_TEND: return T_[field];
+      case ROLE_WORK: return S_[perm_[1]][field];
+      case ROLE_PIPREV: return piprev_ ? piprev_ : S_[perm_[0]][4];
+      default: return nullptr;
+    }
+  }
+
+  int upload(int role, int field, const double* ref) override {
+    R* d = field_ptr(role, field);
+    if (!d) return fail("bad role/field");
+    to_pitched(ref, stage_, true);
+    CK(cudaMemcpyAsync(d, stage_, L_.n3() * sizeof(R), cudaMemcpyHostToDevice, st_));
+    CK(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  int download(int role, int field, double* ref) override {
+    R* d = field_ptr(role, field);
+    if (!d) return fail("bad role/field");
+    CK(cudaMemcpyAsync(stage_, d, L_.n3() * sizeof(R), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    from_pitched(stage_, ref);
+    return 0;
+  }
+
+  int upload_state_raw(int field, const void* host) override {
+    if (field < 0 || field > 7) return fail("bad field");
+    CK(cudaMemcpyAsync(S_[perm_[0]][field], host, L_.n3() * sizeof(R), cudaMemcpyHostToDevice, st_));
+    return 0;
+  }
+  int download_state_raw(int field, void* host) override {
+    if (field < 0 || field > 7) return fail("bad field");
+    CK(cudaMemcpyAsync(host, S_[perm_[0]][field], L_.n3() * sizeof(R), cudaMemcpyDeviceToHost, st_));
+    return 0;
+  }
+
+  R* field2d(int which) {
+    switch (which) {
+      case F2_RAIN: return rain_;
+      case F2_TSK: return sf_.tsk;
+      case F2_PBLH: return sf_.pblh;
+      case F2_T2M: return sf_.t2m;
+      case F2_U10: return sf_.u10;
+      case F2_WGT: return wgt_;
+      default: return nullptr;
+    }
+  }
+
+  int download2d(int which, double* ref2) override {
+    R* d = field2d(which);
+    if (!d) return fail("2D field not available");
+    std::vector<R> h(L_.n2());
+    CK(cudaMemcpyAsync(h.data(), d, L_.n2() * sizeof(R), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    for (int j = -3; j < g_.ny + 3; ++j)
+      for (int i = -3; i < g_.nx + 3; ++i) ref2[g_.idx2(i, j)] = (double)h[L_.at2(i, j)];
+    return 0;
+  }
+
+  int upload2d(int which, const double* ref2) override {
+    R* d = field2d(which);
+    if (!d) return fail("2D field not available");
+    return put2d(d, std::vector<double>(ref2, ref2 + g_.n2()));
+  }
+
+  // ------------------------------------------------------------- stepping
+  int step(double dt, double t) override {
+    launch_clock(clock_, t, t_lo_, t_hi_, dt, 0, st_);
+    launches_ = 1;
+    if (enqueue_step((R)dt)) return 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  int run(int nsteps, double dt, double t0) override {
+    launch_clock(clock_, t0, t_lo_, t_hi_, dt, 0, st_);
+    if (!graphs_valid_ || graph_dt_ != dt) {
+      for (auto& ge : gexec_)
+        if (ge) {
+          cudaGraphExecDestroy(ge);
+          ge = nullptr;
+        }
+      graphs_valid_ = true;
+      graph_dt_ = dt;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+      int ph = phase_;
+      if (!gexec_[ph]) {
+        int saved[3] = {perm_[0], perm_[1], perm_[2]};
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        launches_ = 0;
+        int rc = enqueue_step((R)dt);
+        launch_clock(clock_, 0, 0, 0, 0, 1, st_);
+        ++launches_;
+        cudaError_t ce = cudaStreamEndCapture(st_, &gr);
+        if (rc) return 1;
+        if (ce != cudaSuccess) return fail(std::string("graph capture: ") + cudaGetErrorString(ce));
+        CK(cudaGraphInstantiate(&gexec_[ph], gr, 0));
+        cudaGraphDestroy(gr);
+        glaunches_ = launches_;
+        // enqueue_step advanced the rotation during capture; restore it
+        perm_[0] = saved[0];
+        perm_[1] = saved[1];
+        perm_[2] = saved[2];
+        phase_ = ph;
+      }
+      CK(cudaGraphLaunch(gexec_[ph], st_));
+      advance_rotation();
+    }
+    launches_ = glaunches_;
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  int time_run(int nsteps, double dt, double t0, double* ms) override {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st_));
+    int rc = run(nsteps, dt, t0);
+    CK(cudaEventRecord(e1, st_));
+    CK(cudaEventSynchronize(e1));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = f;
+    return rc;
+  }
+
+  int kernel_times(double dt, double t, std::vector<std::string>* names, std::vector<double>* ms,
+                   std::vector<int>* counts) override {
+    prof_.clear();
+    profiling_ = true;
+    int rc = step(dt, t);
+    profiling_ = false;
+    if (rc) return rc;
+    names->clear();
+    ms->clear();
+    counts->clear();
+    for (auto& pr : prof_) {
+      float f = 0;
+      CK(cudaEventElapsedTime(&f, pr.e0, pr.e1));
+      size_t q = 0;
+      while (q < names->size() && (*names)[q] != pr.name) ++q;
+      if (q == names->size()) {
+        names->push_back(pr.name);
+        ms->push_back(0);
+        counts->push_back(0);
+      }
+      (*ms)[q] += f;
+      (*counts)[q] += 1;
+      cudaEventDestroy(pr.e0);
+      cudaEventDestroy(pr.e1);
+    }
+    prof_.clear();
+    return 0;
+  }
+
+  int sync() override {
+    CK(cudaStreamSynchronize(st_));
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  int absmax(int field, float* out) override {
+    R* d = field_ptr(ROLE_STATE, field);
+    if (!d) return fail("bad field");
+    CK(cudaMemsetAsync(wd_, 0, sizeof(unsigned int), st_));
+    launch_absmax<R>(d, L_.n3(), wd_, st_);
+    unsigned int bits = 0;
+    CK(cudaMemcpyAsync(&bits, wd_, sizeof(bits), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    std::memcpy(out, &bits, sizeof(float));
+    return 0;
+  }
+
+  int dry_mass(double* out) override {
+    R** s = S_[perm_[0]];
+    launch_dry_mass<R>(L_, db_, dm_, s[4], s[3], s[5], s[6], s[7], dp_.moisture, (R)g_.dx,
+                       (R)g_.dy, mass_planes_, mass_, st_);
+    CK(cudaMemcpyAsync(out, mass_, sizeof(double), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  // ------------------------------------------------------------ boundary
+  int set_boundary(const double* const lo[5], const double* const hi[5], const double* wgt,
+                   double t_lo, double t_hi) override {
+    for (int v = 0; v < 5; ++v) {
+      if (!lo_[v] && !(lo_[v] = alloc(L_.n3()))) return 1;
+      if (!hi_[v] && !(hi_[v] = alloc(L_.n3()))) return 1;
+      if (put3d(lo_[v], std::vector<double>(lo[v], lo[v] + g_.npts()))) return 1;
+      if (put3d(hi_[v], std::vector<double>(hi[v], hi[v] + g_.npts()))) return 1;
+    }
+    if (!wgt_ && !(wgt_ = alloc(L_.n2()))) return 1;
+    if (put2d(wgt_, std::vector<double>(wgt, wgt + g_.n2()))) return 1;
+    t_lo_ = t_lo;
+    t_hi_ = t_hi;
+    bdy_on_ = true;
+    graphs_valid_ = false;
+    launch_clock(clock_, 0, t_lo, t_hi, 0, 0, st_);
+    return sync();
+  }
+
+  int set_boundary_hi(const double* const hi[5], double t_lo, double t_hi) override {
+    // BdyManager::update: the old upper targets become the lower ones
+    // (src/dynamics/boundary.cpp:83-89); buffers swap, so graphs recapture
+    if (!bdy_on_) return fail("boundary not set");
+    for (int v = 0; v < 5; ++v) {
+      std::swap(lo_[v], hi_[v]);
+      if (put3d(hi_[v], std::vector<double>(hi[v], hi[v] + g_.npts()))) return 1;
+    }
+    t_lo_ = t_lo;
+    t_hi_ = t_hi;
+    graphs_valid_ = false;
+    return 0;
+  }
+
+  int enable_physics(const double* tsk, const double* land, const double* lat, const double* lon,
+                     const double* soilw, double start_hour, int doy, bool nonlocal) override {
+    // SfcPBL::init (src/physics/surface.cu:440-482); inputs interior ny*nx
+    const size_t n2 = L_.n2();
+    for (R** p : {&sf_.tsk, &sf_.tdeep, &sf_.land, &sf_.lat, &sf_.lon, &sf_.soilw, &sf_.cdv,
+                  &sf_.pblh, &sf_.t2m, &sf_.u10})
+      if (!*p && !(*p = alloc(n2))) return 1;
+    if (!sf_.km && !(sf_.km = alloc(L_.n3()))) return 1;
+    if (!sf_.soilt && !(sf_.soilt = alloc(4 * n2))) return 1;
+    if (!sf_.scratch && !(sf_.scratch = alloc(sfc_scratch_count<R>(L_)))) return 1;
+    auto pad = [&](const double* in) {
+      std::vector<double> o(g_.n2(), 0.0);
+      for (int j = 0; j < g_.ny; ++j)
+        for (int i = 0; i < g_.nx; ++i) o[g_.idx2(i, j)] = in[(size_t)j * g_.nx + i];
+      return o;
+    };
+    if (put2d(sf_.tsk, pad(tsk)) || put2d(sf_.tdeep, pad(tsk)) || put2d(sf_.land, pad(land)) ||
+        put2d(sf_.lat, pad(lat)) || put2d(sf_.lon, pad(lon)) || put2d(sf_.soilw, pad(soilw)))
+      return 1;
+    for (int lyr = 0; lyr < 4; ++lyr)
+      if (put2d(sf_.soilt + lyr * n2, pad(tsk))) return 1;
+    sf_.start_hour = start_hour;
+    sf_.doy = doy;
+    sf_.nonlocal = nonlocal;
+    sfc_on_ = true;
+    graphs_valid_ = false;
+    return sync();
+  }
+
+  // ----------------------------------------------------------- operators
+  int op_apply_bcs() override {
+    GhostJob<R> job = ghost_job(S_[perm_[0]], true);
+    launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_);
+    return sync();
+  }
+
+  int op_tendencies(double dt, double t) override {
+    R** s = S_[perm_[0]];
+    launch_clock(clock_, t, t_lo_, t_hi_, dt, 0, st_);
+    tendencies(s, s, nullptr, (R)dt, (R)0, true);
+    return sync();
+  }
+
+  int op_acoustic(double dtau, int nsub) override {
+    R** N = S_[perm_[0]];
+    R** X = S_[perm_[1]];
+    if (acoustic(N, X, (R)dtau, nsub, true)) return 1;
+    return sync();
+  }
+
+  int op_moisture_stage(double dt) override {
+    R** N = S_[perm_[0]];
+    R** X = S_[perm_[1]];
+    for (int q = 5; q < 8; ++q) launch_axpy<R>(N[q], T_[q], (R)dt, X[q], L_.n3(), st_);
+    return sync();
+  }
+
+  int op_kessler(double dt) override {
+    if (kessler(S_[perm_[0]], (R)dt)) return 1;
+    return sync();
+  }
+
+  int op_sfc(double dt, double t) override {
+    if (!sfc_on_) return fail("surface physics not enabled");
+    launch_clock(clock_, t - dt, t_lo_, t_hi_, dt, 0, st_);
+    if (surface(S_[perm_[0]], (R)dt)) return 1;
+    return sync();
+  }
+
+ private:
+  // --------------------------------------------------------------- pieces
+  struct ProfRec {
+    std::string name;
+    cudaEvent_t e0, e1;
+  };
+  // wraps one launch: counted always, bracketed by events when profiling
+  template <class F>
+  void launch(const char* name, F&& f) {
+    ProfRec r{name, nullptr, nullptr};
+    if (profiling_) {
+      cudaEventCreate(&r.e0);
+      cudaEventCreate(&r.e1);
+      cudaEventRecord(r.e0, st_);
+    }
+    f();
+    ++launches_;
+    if (profiling_) {
+      cudaEventRecord(r.e1, st_);
+      prof_.push_back(r);
+    }
+  }
+
+  GhostJob<R> ghost_job(R** s, bool with_pip) {
+    GhostJob<R> j{};
+    auto add = [&](R* f, int kind) {
+      j.f[j.n] = f;
+      j.kind[j.n] = kind;
+      ++j.n;
+    };
+    add(s[0], 1);
+    add(s[1], 2);
+    add(s[2], 3);
+    add(s[3], 0);
+    if (with_pip) add(s[4], 0);
+    if (dp_.moisture) {
+      add(s[5], 0);
+      add(s[6], 0);
+      add(s[7], 0);
+    }
+    return j;
+  }
+
+  TendArgs<R> tend_args(R** est, R dt) {
+    TendArgs<R> a{};
+    a.L = L_;
+    a.b = db_;
+    a.m = dm_;
+    a.p = dp_;
+    a.dx = (R)g_.dx;
+    a.dy = (R)g_.dy;
+    a.dt = dt;
+    a.u = est[0];
+    a.v = est[1];
+    a.w = est[2];
+    a.thp = est[3];
+    a.pip = est[4];
+    a.qv = est[5];
+    a.qc = est[6];
+    a.qr = est[7];
+    a.mfx = mfx_;
+    a.mfy = mfy_;
+    a.mfz = mfz_;
+    a.clock = clock_;
+    if (bdy_on_) {
+      for (int v = 0; v < 5; ++v) {
+        a.lo[v] = lo_[v];
+        a.hi[v] = hi_[v];
+      }
+      a.wgt = wgt_;
+    }
+    return a;
+  }
+
+  // slow tendencies of est; moisture either into T_ (op) or into X as the
+  // stage value N.q + dt_stage * tq
+  void tendencies(R** est, R** N, R** X, R dt, R dt_stage, bool op) {
+    launch("mass_flux", [&] { launch_mass_flux<R>(L_, db_, dm_, est[0], est[1], est[2], mfx_, mfy_, mfz_, st_); });
+    TendArgs<R> a = tend_args(est, dt);
+    if (dp_.moisture && dp_.pd_moist) {
+      launch("pd_ratio", [&] { launch_pd_ratio<R>(a, ratio_[0], ratio_[1], ratio_[2], st_); });
+      a.ratio_v = ratio_[0];
+      a.ratio_c = ratio_[1];
+      a.ratio_r = ratio_[2];
+    }
+    a.tu = T_[0];
+    a.tv = T_[1];
+    a.tw = T_[2];
+    a.tth = T_[3];
+    a.tpi = (op || bdy_on_) ? T_[4] : nullptr;
+    a.tqv = T_[5];
+    a.tqc = T_[6];
+    a.tqr = T_[7];
+    if (!op && dp_.moisture) {
+      a.qn_v = N[5];
+      a.qn_c = N[6];
+      a.qn_r = N[7];
+      a.qo_v = X[5];
+      a.qo_c = X[6];
+      a.qo_r = X[7];
+      a.dt_stage = dt_stage;
+    }
+    launch("tendencies", [&] { launch_tendencies<R>(a, st_); });
+  }
+
+  // ns acoustic substeps from time n (N) into the stage output X
+  int acoustic(R** N, R** X, R dtau, int ns, bool op) {
+    AcouArgs<R> a{};
+    a.L = L_;
+    a.b = db_;
+    a.m = dm_;
+    a.co = co_;
+    a.p = dp_;
+    a.dx = (R)g_.dx;
+    a.dy = (R)g_.dy;
+    a.dtau = dtau;
+    a.n_pip = N[4];
+    a.n_thp = N[3];
+    a.qv = N[5];
+    a.qc = N[6];
+    a.qr = N[7];
+    a.tu = T_[0];
+    a.tv = T_[1];
+    a.tw = T_[2];
+    a.tth = T_[3];
+    a.tpi = (op || bdy_on_) ? T_[4] : nullptr;
+    R* pic[3] = {X[4], P1_, P2_};
+    auto pbuf = [&](int t) -> R* {  // pi' after substep t-1 (t >= 1), time n for t <= 0
+      if (t <= 0) return N[4];
+      return pic[(ns - t) % 3];
+    };
+    const R* uin = N[0];
+    const R* vin = N[1];
+    for (int t = 0; t < ns; ++t) {
+      R* uout = ((ns - 1 - t) % 2 == 0) ? X[0] : U2_;
+      R* vout = ((ns - 1 - t) % 2 == 0) ? X[1] : V2_;
+      a.u_in = uin;
+      a.v_in = vin;
+      a.u_out = uout;
+      a.v_out = vout;
+      a.w_in = t == 0 ? N[2] : X[2];
+      a.w_out = X[2];
+      a.th_in = t == 0 ? N[3] : X[3];
+      a.th_out = X[3];
+      a.pi_prev = pbuf(t - 1);
+      a.pi_cur = pbuf(t);
+      a.pi_next = pbuf(t + 1);
+      launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
+      int rc = 0;
+      launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, st_); });
+      if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
+      uin = uout;
+      vin = vout;
+      piprev_ = const_cast<R*>(a.pi_cur);
+    }
+    return 0;
+  }
+
+  int kessler(R** s, R dt) {
+    KesArgs<R> k{L_, db_, dm_, dt, s[3], s[5], s[6], s[7], rain_, s[4]};
+    int rc = 0;
+    launch("kessler", [&] { rc = launch_kessler<R>(k, st_); });
+    if (rc) return fail("Kessler launch");
+    return 0;
+  }
+
+  int surface(R** s, R dt) {
+    SfcArgs<R> a{};
+    a.L = L_;
+    a.b = db_;
+    a.m = dm_;
+    a.dt = dt;
+    a.start_hour = sf_.start_hour;
+    a.doy = sf_.doy;
+    a.nonlocal = sf_.nonlocal;
+    a.clock = clock_;
+    a.thp = s[3];
+    a.qv = s[5];
+    a.u = s[0];
+    a.v = s[1];
+    a.pip = s[4];
+    a.qc = s[6];
+    a.tsk = sf_.tsk;
+    a.km = sf_.km;
+    a.cdv = sf_.cdv;
+    a.pblh = sf_.pblh;
+    a.t2m = sf_.t2m;
+    a.u10 = sf_.u10;
+    a.soilt = sf_.soilt;
+    a.tdeep = sf_.tdeep;
+    a.land = sf_.land;
+    a.lat = sf_.lat;
+    a.lon = sf_.lon;
+    a.soilw = sf_.soilw;
+    a.scratch = sf_.scratch;
+    int rc = 0;
+    launch("surface", [&] { rc = launch_sfc<R>(a, st_); });
+    ++launches_;
+    if (rc) return fail("surface physics launch");
+    return 0;
+  }
+
+  // Integrator::step (src/dynamics/integrator.cpp:71-111) as launches on st_.
+  int enqueue_step(R dt) {
+    const int pN = perm_[0], pA = perm_[1], pB = perm_[2];
+    const R stage_dt[3] = {dt / 3, dt / 2, dt};
+    const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
+    const int nss[3] = {1, ns / 2 > 1 ? ns / 2 : 1, ns};
+    R** N = S_[pN];
+    for (int m = 0; m < 3; ++m) {
+      R** est = m == 0 ? N : S_[m == 1 ? pA : pB];
+      R** X = S_[m == 1 ? pB : pA];
+      GhostJob<R> job = ghost_job(est, false);
+      launch("fill_ghosts", [&] { launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_); });
+      tendencies(est, N, X, dt, stage_dt[m], false);
+      if (acoustic(N, X, stage_dt[m] / (R)nss[m], nss[m], false)) return 1;
+    }
+    R** Nn = S_[pA];
+    if (dp_.moisture && dp_.microphysics && kessler(Nn, dt)) return 1;
+    if (sfc_on_ && surface(Nn, dt)) return 1;
+    advance_rotation();
+    return 0;
+  }
+
+  void advance_rotation() {
+    int p0 = perm_[0];
+    perm_[0] = perm_[1];
+    perm_[1] = perm_[2];
+    perm_[2] = p0;
+    phase_ = (phase_ + 1) % 3;
+  }
+
+  // --------------------------------------------------------------- memory
+  R* alloc(size_t n) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(R));
+    if (e != cudaSuccess) {
+      fail(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return nullptr;
+    }
+    cudaMemset(p, 0, n * sizeof(R));
+    allocs_.push_back(p);
+    return (R*)p;
+  }
+
+  // reference padded layout -> pitched; columns/rows outside the reference's
+  // padded range replicate the nearest one so that no padding is uninitialised
+  void to_pitched(const double* ref, R* out, bool replicate) {
+    for (int k = -kOZ; k < L_.pz - kOZ; ++k)
+      for (int j = -kOY; j < L_.py - kOY; ++j) {
+        const double* row = ref + g_.idx(-3, j, k);
+        R* o = out + L_.at(-kOX, j, k);
+        for (int i = -kOX; i < L_.px - kOX; ++i) {
+          int ic = i < -3 ? -3 : (i > g_.nx + 2 ? g_.nx + 2 : i);
+          o[i + kOX] = (R)row[ic + 3];
+        }
+      }
+    (void)replicate;
+  }
+
+  void from_pitched(const R* in, double* ref) {
+    for (int k = -3; k < g_.nz + 4; ++k)
+      for (int j = -3; j < g_.ny + 3; ++j)
+        for (int i = -3; i < g_.nx + 3; ++i) ref[g_.idx(i, j, k)] = (double)in[L_.at(i, j, k)];
+  }
+
+  int put3d(R* d, const std::vector<double>& ref) {
+    to_pitched(ref.data(), stage_tmp(L_.n3()), true);
+    CK(cudaMemcpy(d, tmp_.data(), L_.n3() * sizeof(R), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int put2d(R* d, const std::vector<double>& ref2) {
+    R* o = stage_tmp(L_.n2());
+    for (int j = -kOY; j < L_.py - kOY; ++j)
+      for (int i = -kOX; i < L_.px - kOX; ++i) {
+        int ic = i < -3 ? -3 : (i > g_.nx + 2 ? g_.nx + 2 : i);
+        o[L_.at2(i, j)] = (R)ref2[g_.idx2(ic, j)];
+      }
+    CK(cudaMemcpy(d, o, L_.n2() * sizeof(R), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  int put1d(R* d, const std::vector<double>& v) {
+    R* o = stage_tmp(L_.pz);
+    for (int q = 0; q < L_.pz; ++q) o[q] = (R)v[q];
+    CK(cudaMemcpy(d, o, L_.pz * sizeof(R), cudaMemcpyHostToDevice));
+    return 0;
+  }
+  R* stage_tmp(size_t n) {
+    if (tmp_.size() < n) tmp_.resize(n);
+    return tmp_.data();
+  }
+
+  int fail(const std::string& m) {
+    err_ = m;
+    return 1;
+  }
+
+  void release() {
+    for (auto& ge : gexec_)
+      if (ge) cudaGraphExecDestroy(ge);
+    for (void* p : allocs_) cudaFree(p);
+    allocs_.clear();
+    if (clock_) cudaFree(clock_);
+    if (wd_) cudaFree(wd_);
+    if (mass_planes_) cudaFree(mass_planes_);
+    if (mass_) cudaFree(mass_);
+    if (stage_) cudaFreeHost(stage_);
+    if (st_) cudaStreamDestroy(st_);
+    clock_ = nullptr;
+    wd_ = nullptr;
+    mass_planes_ = nullptr;
+    mass_ = nullptr;
+    stage_ = nullptr;
+    st_ = nullptr;
+  }
+
+  struct SfcBufs {
+    R *tsk = nullptr, *tdeep = nullptr, *land = nullptr, *lat = nullptr, *lon = nullptr,
+      *soilw = nullptr, *cdv = nullptr, *pblh = nullptr, *t2m = nullptr, *u10 = nullptr,
+      *km = nullptr, *soilt = nullptr, *scratch = nullptr;
+    double start_hour = 0;
+    int doy = 1;
+    bool nonlocal = false;
+  };
+
+  const CaseSetup* cs_ = nullptr;
+  RefGrid g_{};
+  HostParams hp_{};
+  Layout L_{};
+  int dev_ = 0;
+  cudaStream_t st_ = nullptr;
+  DMetric<R> dm_{};
+  DBase<R> db_{};
+  DCoef<R> co_{};
+  DParams<R> dp_{};
+  R* S_[3][8] = {};
+  R* T_[8] = {};
+  R *mfx_ = nullptr, *mfy_ = nullptr, *mfz_ = nullptr;
+  R *U2_ = nullptr, *V2_ = nullptr, *P1_ = nullptr, *P2_ = nullptr;
+  R* ratio_[3] = {};
+  R *rtjx_ = nullptr, *rtjy_ = nullptr, *kt3_ = nullptr, *aw_ = nullptr;
+  R* rain_ = nullptr;
+  R* piprev_ = nullptr;
+  R* lo_[5] = {};
+  R* hi_[5] = {};
+  R* wgt_ = nullptr;
+  bool bdy_on_ = false, sfc_on_ = false;
+  double t_lo_ = 0, t_hi_ = 0;
+  SfcBufs sf_;
+  double* clock_ = nullptr;
+  unsigned int* wd_ = nullptr;
+  double *mass_planes_ = nullptr, *mass_ = nullptr;
+  R* stage_ = nullptr;
+  std::vector<R> tmp_;
+  std::vector<void*> allocs_;
+  int perm_[3] = {0, 1, 2};
+  int phase_ = 0;
+  cudaGraphExec_t gexec_[3] = {nullptr, nullptr, nullptr};
+  bool graphs_valid_ = false;
+  double graph_dt_ = 0;
+  long launches_ = 0, glaunches_ = 0;
+  bool profiling_ = false;
+  std::vector<ProfRec> prof_;
+};
+
+Model* Model::create(const CaseSetup& cs, bool fp64, int device, std::string* err) {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    *err = std::string("no CUDA device available: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  if (device < 0 || device >= ndev) {
+    *err = "device index out of range";
+    return nullptr;
+  }
+  Model* m = nullptr;
+  int rc;
+  if (fp64) {
+    auto* t = new ModelT<double>();
+    rc = t->init(cs, device);
+    m = t;
+  } else {
+    auto* t = new ModelT<float>();
+    rc = t->init(cs, device);
+    m = t;
+  }
+  if (rc) {
+    *err = m->error();
+    delete m;
+    return nullptr;
+  }
+  return m;
+}
+
+}  // namespace wfe

@@ -1,0 +1,73 @@
+// Precision-agnostic interface of a wfe_b200 model instance (one case on one
+// GPU).  ModelT<R> in model.cu implements it for float and double.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "setup.hpp"
+
+namespace wfe {
+
+enum Role { ROLE_STATE = 0, ROLE_TEND = 1, ROLE_WORK = 2, ROLE_PIPREV = 3 };
+enum Field2D { F2_RAIN = 0, F2_TSK = 1, F2_PBLH = 2, F2_T2M = 3, F2_U10 = 4, F2_WGT = 5 };
+
+class Model {
+ public:
+  virtual ~Model() = default;
+  // nullptr on failure with *err set
+  static Model* create(const CaseSetup& cs, bool fp64, int device, std::string* err);
+
+  virtual const RefGrid& grid() const = 0;
+  virtual bool fp64() const = 0;
+  const std::string& error() const { return err_; }
+
+  // field transfer in the reference padded layout (NX*NY*NZ doubles)
+  virtual int upload(int role, int field, const double* ref_padded) = 0;
+  virtual int download(int role, int field, double* ref_padded) = 0;
+  // 2D surface fields in the reference padded 2D layout (NX*NY doubles)
+  virtual int download2d(int which, double* ref_padded2d) = 0;
+  virtual int upload2d(int which, const double* ref_padded2d) = 0;
+  // raw device-layout transfers of the state (fast path, same precision)
+  virtual int upload_state_raw(int field, const void* host_pitched) = 0;
+  virtual int download_state_raw(int field, void* host_pitched) = 0;
+  virtual size_t pitched_count() const = 0;
+  virtual void pitched_dims(int* px, int* py, int* pz) const = 0;
+
+  // Integrator::step (src/dynamics/integrator.cpp:71-111): direct launches
+  virtual int step(double dt, double t) = 0;
+  // nsteps large steps replayed from captured CUDA graphs
+  virtual int run(int nsteps, double dt, double t0) = 0;
+  virtual int sync() = 0;
+  virtual int absmax(int field, float* out) = 0;
+  virtual int dry_mass(double* out) = 0;
+
+  // boundary relaxation targets, reference padded layout; t_lo < t_hi
+  virtual int set_boundary(const double* const lo[5], const double* const hi[5],
+                           const double* wgt_padded2d, double t_lo, double t_hi) = 0;
+  virtual int set_boundary_hi(const double* const hi[5], double t_lo, double t_hi) = 0;
+  virtual int enable_physics(const double* tsk, const double* land, const double* lat,
+                             const double* lon, const double* soilw, double start_hour, int doy,
+                             bool nonlocal) = 0;
+
+  // operator-level API (src/dynamics/kernels.hpp, physics/*.hpp)
+  virtual int op_apply_bcs() = 0;
+  virtual int op_tendencies(double dt, double t) = 0;
+  virtual int op_acoustic(double dtau, int nsub) = 0;
+  virtual int op_moisture_stage(double dt) = 0;
+  virtual int op_kessler(double dt) = 0;
+  virtual int op_sfc(double dt, double t) = 0;
+
+  // launches made by the last step()/run() call (device kernels only)
+  virtual long launches_per_step() const = 0;
+  // nsteps graph-replayed steps timed with CUDA events on the model's stream
+  virtual int time_run(int nsteps, double dt, double t0, double* ms) = 0;
+  // one direct step with CUDA events around every launch: per-kernel totals
+  virtual int kernel_times(double dt, double t, std::vector<std::string>* names,
+                           std::vector<double>* ms, std::vector<int>* counts) = 0;
+
+ protected:
+  std::string err_;
+};
+
+}  // namespace wfe

@@ -1,0 +1,309 @@
+// Kessler warm rain with the mixed-phase blend (src/physics/kessler.cu:22-149),
+// the |f| watchdog reduction (src/dynamics/kernels.cu:278-289) and an FP64
+// dry-air mass diagnostic, on the B200.
+//
+// The reference runs one thread per column with four 320-deep local arrays
+// (a 5 KB stack) and walks every level serially.  Here a CTA owns CX columns
+// with the column arrays in shared memory: the fall speeds, the flux
+// divergence of each sedimentation subcycle and the per-level conversions run
+// in parallel over the levels; only the rain accumulation is serial.  Every
+// value is computed with the reference's expressions, so subcycle counts and
+// branch decisions are the same.
+#include <cuda_runtime.h>
+
+#include "core.cuh"
+#include "kernels.cuh"
+
+namespace wfe {
+
+template <typename R>
+__device__ __forceinline__ R qsat_w(R p, R T) {  // src/core/thermo.hpp:11-17
+  R es = (R)610.78 * exp((R)17.269 * (T - (R)273.16) / (T - (R)35.86));
+  R den = p - es;
+  if (den < (R)1) den = (R)1;
+  return (R)0.622 * es / den;
+}
+template <typename R>
+__device__ __forceinline__ R qsat_i(R p, R T) {  // src/core/thermo.hpp:20-26
+  R es = (R)610.78 * exp((R)21.875 * (T - (R)273.16) / (T - (R)7.66));
+  R den = p - es;
+  if (den < (R)1) den = (R)1;
+  return (R)0.622 * es / den;
+}
+
+template <typename R>
+__device__ __forceinline__ R fall_speed(R rq, R rho_sfc, R rho, R T) {
+  // kessler.cu:195-211: 36.34 (rho qr)^0.1364 sqrt(rho0/rho), x0.35 below freezing
+  return rq > (R)1e-9 ? (R)36.34 * pow(rq, (R)0.1364) * sqrt(rho_sfc / rho) *
+                            (T < Phys<R>::Tfrz ? (R)0.35 : (R)1)
+                      : (R)0;
+}
+
+template <typename R, int CX>
+__global__ void k_kessler(KesArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Layout& L = a.L;
+  const int nz = L.nz;
+  const int tx = threadIdx.x, lane = threadIdx.y, KL = blockDim.y;
+  const int i = blockIdx.x * CX + tx, j = blockIdx.y;
+  const bool active = i < L.nx;
+  R* qrl = reinterpret_cast<R*>(smem_raw);
+  R* rhol = qrl + (size_t)nz * CX;
+  R* dzl = rhol + (size_t)nz * CX;
+  R* vr = dzl + (size_t)nz * CX;
+  R* F = vr + (size_t)nz * CX;                 // (nz + 1) * CX
+  R* red = F + (size_t)(nz + 1) * CX;          // KL * CX * 2 partial max/min
+  __shared__ int nsub_s[CX];
+  __shared__ R dts_s[CX];
+#define S(X, k) X[(size_t)(k) * CX + tx]
+  const R J = active ? a.m.jac[L.at2(i, j)] : (R)1;
+  const R rho_sfc = active ? a.b.rhob[L.at(i, j, 0)] : (R)1;
+
+  // 1) column set-up and the first fall speeds (kessler.cu:199-214)
+  R vmax = 0, dmin = (R)1e30;
+  if (active)
+    for (int k = lane; k < nz; k += KL) {
+      const size_t c = L.at(i, j, k);
+      R q = a.qr[c];
+      R qk = q > (R)0 ? q : (R)0;
+      R rh = a.b.rhob[c];
+      R dz = a.m.dzeta_c[L.at1(k)] * J;
+      R T = (a.b.thb[c] + a.thp[c]) * (a.b.pib[c] + a.pip[c]);
+      R vk = fall_speed(rh * qk, rho_sfc, rh, T);
+      S(qrl, k) = qk;
+      S(rhol, k) = rh;
+      S(dzl, k) = dz;
+      S(vr, k) = vk;
+      if (vk > vmax) vmax = vk;
+      if (dz < dmin) dmin = dz;
+    }
+  red[(size_t)lane * CX + tx] = vmax;
+  red[(size_t)(KL + lane) * CX + tx] = dmin;
+  __syncthreads();
+  if (lane == 0) {
+    R vm = 0, dm = (R)1e30;
+    for (int l = 0; l < KL; ++l) {
+      R x = red[(size_t)l * CX + tx], y = red[(size_t)(KL + l) * CX + tx];
+      if (x > vm) vm = x;
+      if (y < dm) dm = y;
+    }
+    int ns = active ? 1 + (int)(vm * a.dt / ((R)0.8 * dm)) : 0;
+    nsub_s[tx] = ns;
+    dts_s[tx] = active ? a.dt / (R)ns : (R)0;
+  }
+  __syncthreads();
+  int nsub_max = 0;
+  for (int c = 0; c < CX; ++c) nsub_max = max(nsub_max, nsub_s[c]);
+  const int nsub = nsub_s[tx];
+  const R dts = dts_s[tx];
+
+  // 2) upwind sedimentation subcycles (kessler.cu:215-236)
+  R acc = 0;
+  for (int s = 0; s < nsub_max; ++s) {
+    const bool on = active && s < nsub;
+    if (on)
+      for (int k = lane; k <= nz; k += KL) S(F, k) = (k < nz) ? S(rhol, k) * S(qrl, k) * S(vr, k) : (R)0;
+    __syncthreads();
+    if (on) {
+      if (lane == 0) acc += dts * S(F, 0);
+      for (int k = lane; k < nz; k += KL)
+        S(qrl, k) += dts * (S(F, k + 1) - S(F, k)) / (S(rhol, k) * S(dzl, k));
+    }
+    __syncthreads();
+    if (on && s + 1 < nsub)
+      for (int k = lane; k < nz; k += KL) {
+        const size_t c = L.at(i, j, k);
+        R q = S(qrl, k);
+        R rq = S(rhol, k) * (q > (R)0 ? q : (R)0);
+        R T = (a.b.thb[c] + a.thp[c]) * (a.b.pib[c] + a.pip[c]);
+        S(vr, k) = fall_speed(rq, rho_sfc, S(rhol, k), T);
+      }
+    __syncthreads();
+  }
+  if (active && lane == 0) a.rain[L.at2(i, j)] += acc;
+
+  // 3) conversions, evaporation and mixed-phase saturation adjustment,
+  //    independent per level (kessler.cu:239-297)
+  if (active)
+    for (int k = lane; k < nz; k += KL) {
+      const size_t c = L.at(i, j, k);
+      const R k1 = (R)0.001, qc0 = (R)0.001;
+      R qvk = a.qv[c] > (R)0 ? a.qv[c] : (R)0;
+      R qck = a.qc[c] > (R)0 ? a.qc[c] : (R)0;
+      R qrk = S(qrl, k) > (R)0 ? S(qrl, k) : (R)0;
+      R rh = S(rhol, k);
+      R pi = a.b.pib[c] + a.pip[c];
+      R thp = a.thp[c];
+      R th = a.b.thb[c] + thp;
+      R T = th * pi;
+      R pres = Phys<R>::p00 * pow(pi, Phys<R>::cp / Phys<R>::Rd);
+      R fl = (T - (R)233.15) / (R)40;
+      fl = fmax((R)0, fmin((R)1, fl));
+      R qsw = qsat_w(pres, T);
+      R qs = fl * qsw + ((R)1 - fl) * qsat_i(pres, T);
+      R Leff = fl * Phys<R>::Lv + ((R)1 - fl) * Phys<R>::Ls;
+      R dqauto = k1 * (qck > qc0 ? qck - qc0 : (R)0);
+      R dqacc = (R)2.2 * qck * pow(qrk > (R)1e-9 ? qrk : (R)1e-9, (R)0.875);
+      R dqr = a.dt * (dqauto + dqacc);
+      if (dqr > qck) dqr = qck;
+      qck -= dqr;
+      qrk += dqr;
+      if (qvk < qs && qrk > (R)0) {
+        R rq = rh * qrk;
+        R vent = (R)1.6 + (R)124.9 * pow(rq, (R)0.2046);
+        R ern = vent * pow(rq, (R)0.525) / ((R)2.55e8 / (pres * qs) + (R)5.4e5) * (qs - qvk) /
+                (rh * qs);
+        R dqe = a.dt * ern;
+        if (dqe > qrk) dqe = qrk;
+        if (dqe > qs - qvk) dqe = qs - qvk;
+        qrk -= dqe;
+        qvk += dqe;
+        thp -= Leff * dqe / (Phys<R>::cp * pi);
+        th = a.b.thb[c] + thp;
+        T = th * pi;
+        R fl2 = fmax((R)0, fmin((R)1, (T - (R)233.15) / (R)40));
+        qs = fl2 * qsat_w(pres, T) + ((R)1 - fl2) * qsat_i(pres, T);
+      }
+      R gam = Leff * Leff * qs / (Phys<R>::cp * Phys<R>::Rv * T * T);
+      R dq = (qvk - qs) / ((R)1 + gam);
+      if (dq < (R)0) {
+        R evap = -dq;
+        if (evap > qck) evap = qck;
+        dq = -evap;
+      }
+      qvk -= dq;
+      qck += dq;
+      thp += Leff * dq / (Phys<R>::cp * pi);
+      a.thp[c] = thp;
+      a.qv[c] = qvk > (R)0 ? qvk : (R)0;
+      a.qc[c] = qck > (R)0 ? qck : (R)0;
+      a.qr[c] = qrk > (R)0 ? qrk : (R)0;
+    }
+#undef S
+}
+
+template <typename R>
+static size_t kessler_smem(int nz, int cx, int kl) {
+  return ((size_t)4 * nz + (nz + 1) + 2 * kl) * cx * sizeof(R);
+}
+
+template <typename R>
+static int kessler_cx(int nz) {
+  const size_t lim = 200 * 1024;
+  if (kessler_smem<R>(nz, 32, 8) <= lim) return 32;
+  if (kessler_smem<R>(nz, 8, 32) <= lim) return 8;
+  return 0;
+}
+
+// Sets the dynamic shared-memory limit once, outside any stream capture.
+template <typename R>
+int prepare_kessler(int nz) {
+  int cx = kessler_cx<R>(nz);
+  cudaError_t e;
+  if (cx == 32)
+    e = cudaFuncSetAttribute(k_kessler<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kessler_smem<R>(nz, 32, 8));
+  else if (cx == 8)
+    e = cudaFuncSetAttribute(k_kessler<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kessler_smem<R>(nz, 8, 32));
+  else
+    return 2;
+  return e == cudaSuccess ? 0 : 1;
+}
+
+template <typename R>
+int launch_kessler(const KesArgs<R>& a, cudaStream_t st) {
+  const int nz = a.L.nz;
+  const int cx = kessler_cx<R>(nz);
+  if (cx == 32)
+    k_kessler<R, 32><<<dim3((a.L.nx + 31) / 32, a.L.ny), dim3(32, 8), kessler_smem<R>(nz, 32, 8), st>>>(a);
+  else if (cx == 8)
+    k_kessler<R, 8><<<dim3((a.L.nx + 7) / 8, a.L.ny), dim3(8, 32), kessler_smem<R>(nz, 8, 32), st>>>(a);
+  else
+    return 2;
+  return 0;
+}
+
+// ------------------------------------------------------------- watchdog
+// max |f| over the points the reference defines (interior cells, faces up to
+// nx / ny, w levels up to nz); as float bits so that NaN ranks above every
+// finite value (kernels.cu:275-289).
+template <typename R>
+__global__ void k_absmax(const R* __restrict__ f, size_t n, unsigned int* result) {
+  unsigned int best = 0;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    float v = fabsf((float)f[idx]);
+    unsigned int b = __float_as_uint(v);
+    best = b > best ? b : best;
+  }
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(result, best);
+}
+
+template <typename R>
+void launch_absmax(const R* f, size_t n, unsigned int* result, cudaStream_t st) {
+  int grd = (int)((n + 255) / 256);
+  if (grd > 148 * 8) grd = 148 * 8;
+  k_absmax<R><<<grd, 256, 0, st>>>(f, n, result);
+}
+
+// ---------------------------------------------------------- dry-air mass
+// sum over interior cells of rho / (1 + qv + qc + qr) * J * dzeta * dx * dy,
+// rho = p00 pi^(cv/Rd) / (Rd theta (1 + 0.61 qv)), accumulated in FP64 with a
+// fixed reduction order (one CTA per level, then the levels in order) so the
+// result is bit-reproducible run to run.
+template <typename R>
+__global__ void k_dry_mass_plane(Layout L, DBase<R> b, DMetric<R> m, const R* pip, const R* thp,
+                                 const R* qv, const R* qc, const R* qr, int moist,
+                                 double* plane_sums) {
+  __shared__ double part[256];
+  const int k = blockIdx.x;
+  double s = 0.0;
+  const int n2 = L.nx * L.ny;
+  for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+    int i = q % L.nx, j = q / L.nx;
+    size_t c = L.at(i, j, k);
+    double pi = (double)b.pib[c] + (double)pip[c];
+    double th = (double)b.thb[c] + (double)thp[c];
+    double v = moist ? (double)qv[c] : 0.0;
+    double qt = moist ? v + (double)qc[c] + (double)qr[c] : 0.0;
+    double rho = 1.0e5 * pow(pi, (1004.5 - 287.04) / 287.04) / (287.04 * th * (1.0 + 0.61 * v));
+    s += rho / (1.0 + qt) * (double)m.jac[L.at2(i, j)];
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) plane_sums[k] = part[0] * (double)m.dzeta_c[L.at1(k)];
+}
+
+__global__ void k_dry_mass_total(const double* plane_sums, int nz, double area, double* result) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double t = 0.0;
+  for (int k = 0; k < nz; ++k) t += plane_sums[k];
+  *result = t * area;
+}
+
+template <typename R>
+void launch_dry_mass(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* pip,
+                     const R* thp, const R* qv, const R* qc, const R* qr, int moist, R dx, R dy,
+                     double* plane_sums, double* result, cudaStream_t st) {
+  k_dry_mass_plane<R><<<L.nz, 256, 0, st>>>(L, b, m, pip, thp, qv, qc, qr, moist, plane_sums);
+  k_dry_mass_total<<<1, 32, 0, st>>>(plane_sums, L.nz, (double)dx * (double)dy, result);
+}
+
+#define WFE_INST(R)                                                                           \
+  template int launch_kessler<R>(const KesArgs<R>&, cudaStream_t);                            \
+  template int prepare_kessler<R>(int);                            \
+  template void launch_absmax<R>(const R*, size_t, unsigned int*, cudaStream_t);              \
+  template void launch_dry_mass<R>(const Layout&, const DBase<R>&, const DMetric<R>&, const R*, \
+                                   const R*, const R*, const R*, const R*, int, R, R, double*, \
+                                   double*, cudaStream_t);
+WFE_INST(float)
+WFE_INST(double)
+#undef WFE_INST
+
+}  // namespace wfe

@@ -1,0 +1,419 @@
+// Surface layer (Louis 1979), two-stream radiation, 4-layer soil, local-Ri or
+// Troen-Mahrt nonlocal PBL and implicit column mixing on the B200
+// (src/physics/surface.cu:28-514).
+//
+// One thread per column as in the reference, but the per-column work arrays
+// (the reference keeps 21 KB of them on the thread stack) live in an explicit
+// scratch buffer laid out column-fastest, so the 32 columns of a warp touch
+// consecutive addresses and no local-memory stack frame is needed; any column
+// depth works.  The momentum columns on u and v faces run in one launch.  Every
+// value follows the reference's expressions.
+#include <cuda_runtime.h>
+
+#include "core.cuh"
+#include "kernels.cuh"
+
+namespace wfe {
+
+namespace {
+
+template <typename R>
+__device__ __forceinline__ R qsat_tet(R p, R T) {  // src/core/thermo.hpp:11-17
+  R es = (R)610.78 * exp((R)17.269 * (T - (R)273.16) / (T - (R)35.86));
+  R den = p - es;
+  if (den < (R)1) den = (R)1;
+  return (R)0.622 * es / den;
+}
+
+template <typename R>
+__device__ __forceinline__ R psi_m(R zeta) {  // surface.cu:30-36
+  if (zeta >= (R)0) return (R)-5 * fmin(zeta, (R)2);
+  R x = pow((R)1 - (R)16 * zeta, (R)0.25);
+  const R halfpi = (R)1.5707963267948966;
+  return (R)2 * log(((R)1 + x) * (R)0.5) + log(((R)1 + x * x) * (R)0.5) - (R)2 * atan(x) + halfpi;
+}
+template <typename R>
+__device__ __forceinline__ R psi_h(R zeta) {  // surface.cu:37-41
+  if (zeta >= (R)0) return (R)-5 * fmin(zeta, (R)2);
+  R x = pow((R)1 - (R)16 * zeta, (R)0.25);
+  return (R)2 * log(((R)1 + x * x) * (R)0.5);
+}
+
+// One column of a scratch array: element k at p[k * s].
+template <typename R>
+struct Col {
+  R* p;
+  size_t s;
+  __device__ __forceinline__ R& operator[](int k) const { return p[(size_t)k * s]; }
+};
+
+// implicit column diffusion (Thomas), surface.cu:61-84; A..D are work columns
+template <typename R>
+__device__ void diffuse_col(int nz, R dt, Col<R> rho, Col<R> rhow, Col<R> dzc, Col<R> dzw,
+                            Col<R> Kw, R src0, Col<R> phi, const Col<R>* fcg, Col<R> A, Col<R> B,
+                            Col<R> C, Col<R> D) {
+  for (int k = 0; k < nz; ++k) {
+    R a = (k > 0) ? rhow[k] * Kw[k] / dzw[k] : (R)0;
+    R c = (k < nz - 1) ? rhow[k + 1] * Kw[k + 1] / dzw[k + 1] : (R)0;
+    R m = rho[k] * dzc[k] / dt;
+    A[k] = -a;
+    B[k] = m + a + c;
+    C[k] = -c;
+    D[k] = m * phi[k];
+    if (fcg) D[k] += (*fcg)[k] - (*fcg)[k + 1];
+  }
+  D[0] += src0;
+  for (int k = 1; k < nz; ++k) {
+    R w = A[k] / B[k - 1];
+    B[k] -= w * C[k - 1];
+    D[k] -= w * D[k - 1];
+  }
+  phi[nz - 1] = D[nz - 1] / B[nz - 1];
+  for (int k = nz - 2; k >= 0; --k) phi[k] = (D[k] - C[k] * phi[k + 1]) / B[k];
+}
+
+}  // namespace
+
+// scratch columns of the mass-column kernel
+enum { SC_RHO, SC_RHOW, SC_DZC, SC_DZW, SC_THV, SC_KW, SC_TH, SC_QV, SC_KLOC, SC_SH2, SC_TLEV,
+       SC_EPS, SC_FUP, SC_FDN, SC_RAD, SC_SW, SC_FCGT, SC_FCGQ, SC_A, SC_B, SC_C, SC_D, SC_N };
+// scratch columns of a momentum column
+enum { SM_RHO, SM_RHOW, SM_DZC, SM_DZW, SM_KW, SM_PHI, SM_A, SM_B, SM_C, SM_D, SM_N };
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_sfc_scalar(SfcArgs<R> a) {
+  const Layout& L = a.L;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= L.nx || j >= L.ny) return;
+  const int nz = L.nz;
+  using P = Phys<R>;
+  const R KAPPA = (R)0.4, SIGMA = (R)5.67e-8, S0 = (R)1361, KM_MAX = (R)1000, KM_MIN = (R)0.1;
+  const R SOIL_DZ[4] = {(R)0.1, (R)0.3, (R)0.6, (R)1.0};
+  const size_t c2 = L.at2(i, j);
+  const size_t n2 = L.n2();
+  const R J = a.m.jac[c2];
+  double tend_s = a.clock[CLK_T] + a.clock[CLK_DT];  // end of the step
+  R utc = (R)(a.start_hour + tend_s / 3600.0);
+  utc = utc - (R)24 * floor(utc / (R)24);
+
+  // work columns: array q of this column at scratch[(q * (nz + 1) + k) * ncol + col]
+  const size_t ncol = (size_t)L.nx * L.ny, col = (size_t)j * L.nx + i;
+  auto C_ = [&](int q) { return Col<R>{a.scratch + (size_t)q * (nz + 1) * ncol + col, ncol}; };
+  Col<R> rho = C_(SC_RHO), rhow = C_(SC_RHOW), dzc = C_(SC_DZC), dzw = C_(SC_DZW), thv = C_(SC_THV);
+  Col<R> Kw = C_(SC_KW), thcol = C_(SC_TH), qvcol = C_(SC_QV), Kloc = C_(SC_KLOC);
+  Col<R> shear2 = C_(SC_SH2);
+  R lwp = 0;
+  for (int k = 0; k < nz; ++k) {
+    const int kk = L.at1(k);
+    const size_t c = L.at(i, j, k);
+    rho[k] = a.b.rhob[c];
+    rhow[k] = a.b.rhobw[c];
+    dzc[k] = a.m.dzeta_c[kk] * J;
+    dzw[k] = a.m.dzeta_w[kk] * J;
+    thcol[k] = a.b.thb[c] + a.thp[c];
+    qvcol[k] = a.qv[c];
+    thv[k] = thcol[k] * ((R)1 + P::eps61 * qvcol[k]);
+    lwp += rho[k] * (a.qc[c] > (R)0 ? a.qc[c] : (R)0) * dzc[k] * (R)1000;
+  }
+  // The local-Ri diffusivity (surface.cu:285-298) and the bulk-Richardson shear
+  // of the PBL-height search (surface.cu:321) depend only on the column loaded
+  // above; they are evaluated here, with the reference's expressions, so that
+  // the wind columns are dead before the radiation arrays are live.
+  auto ucen = [&](int k) {  // cell-centre winds (surface.cu:112-113)
+    const size_t c = L.at(i, j, k);
+    return (R)0.5 * (a.u[c] + a.u[c + 1]);
+  };
+  auto vcen = [&](int k) {
+    const size_t c = L.at(i, j, k);
+    return (R)0.5 * (a.v[c] + a.v[c + L.px]);
+  };
+  for (int k = 1; k < nz; ++k) {
+    R dz = dzw[k];
+    R uk = ucen(k), vk = vcen(k);
+    R du = (uk - ucen(k - 1)) / dz, dv = (vk - vcen(k - 1)) / dz;
+    R S2 = du * du + dv * dv + (R)1e-8;
+    R thvw = (R)0.5 * (thv[k - 1] + thv[k]);
+    R N2 = P::grav / thvw * (thv[k] - thv[k - 1]) / dz;
+    R Ri = N2 / S2;
+    R zw = a.m.zeta_w[L.at1(k)] * J;
+    R l = KAPPA * zw / ((R)1 + KAPPA * zw / (R)150);
+    if (Ri < (R)0) {
+      Kloc[k] = l * l * sqrt(S2) * sqrt((R)1 - (R)16 * Ri);
+    } else {
+      R d = (R)1 + (R)5 * Ri;
+      Kloc[k] = l * l * sqrt(S2) / (d * d);
+    }
+    shear2[k] = uk * uk + vk * vk + (R)0.1;
+  }
+  // surface layer (surface.cu:120-161)
+  const bool onland = a.land[c2] > (R)0.5;
+  const R z0 = onland ? (R)0.1 : (R)2e-4;
+  const R alb = onland ? (R)0.2 : (R)0.08;
+  R beta;
+  if (onland) {
+    R f = (a.soilw[c2] - (R)0.08) / ((R)0.32 - (R)0.08);
+    f = fmin((R)1, fmax((R)0, f));
+    beta = fmax((R)0.05, f * f);
+  } else {
+    beta = (R)1;
+  }
+  R z1 = (R)0.5 * dzc[0];
+  const R u0 = ucen(0), v0 = vcen(0);
+  R V1 = sqrt(u0 * u0 + v0 * v0);
+  if (V1 < (R)0.5) V1 = (R)0.5;
+  const size_t c0 = L.at(i, j, 0);
+  R pi1 = a.b.pib[c0] + a.pip[c0];
+  R p1 = P::p00 * pow(pi1, P::cp / P::Rd);
+  R Ts = a.tsk[c2];
+  R pis = pi1 + P::grav * z1 / (P::cp * thv[0]);
+  R ths = Ts / pis;
+  R qs_s = qsat_tet(p1, Ts);
+  R thvs = ths * ((R)1 + P::eps61 * (beta * qs_s + ((R)1 - beta) * qvcol[0]));
+  R Rib = P::grav * z1 * (thv[0] - thvs) / (thvs * V1 * V1);
+  R a2 = KAPPA / log(z1 / z0);
+  a2 *= a2;
+  R Fm, Fh;
+  if (Rib < (R)0) {
+    R sq = sqrt(-Rib * z1 / z0);
+    Fm = (R)1 - (R)9.4 * Rib / ((R)1 + (R)7.4 * (R)9.4 * a2 * sq);
+    Fh = (R)1 - (R)9.4 * Rib / ((R)1 + (R)5.3 * (R)9.4 * a2 * sq);
+  } else {
+    R d = (R)1 + (R)4.7 * Rib;
+    Fm = Fh = (R)1 / (d * d);
+  }
+  R Cd = a2 * Fm, Ch = a2 * Fh;
+  a.cdv[c2] = Cd * V1;
+  // 2 m / 10 m diagnostics (surface.cu:163-182)
+  R z0h = z0 * (R)0.1;
+  R lnz1z0 = log(z1 / z0);
+  R zeta1 = (Rib >= (R)0) ? Rib * lnz1z0 / ((R)1 - (R)5 * fmin(Rib, (R)0.19)) : Rib * lnz1z0;
+  zeta1 = fmax((R)-8, fmin((R)2, zeta1));
+  R zol = zeta1 / z1;
+  R den_m = lnz1z0 - psi_m(zeta1) + psi_m(z0 * zol);
+  R num_m = log((R)10 / z0) - psi_m((R)10 * zol) + psi_m(z0 * zol);
+  R r10 = fmax((R)0, fmin((R)1.2, num_m / fmax(den_m, (R)0.1)));
+  a.u10[c2] = V1 * r10;
+  R den_h = log(z1 / z0h) - psi_h(zeta1) + psi_h(z0h * zol);
+  R num_h = log((R)2 / z0h) - psi_h((R)2 * zol) + psi_h(z0h * zol);
+  R r2 = fmax((R)0, fmin((R)1.2, num_h / fmax(den_h, (R)0.1)));
+  R th2 = ths + (thcol[0] - ths) * r2;
+  a.t2m[c2] = th2 * pi1;
+  R shf = Ch * V1 * (ths - thcol[0]);
+  R qflx = Ch * V1 * beta * (qs_s - qvcol[0]);
+  if (!onland && qflx < (R)0) qflx = 0;
+  // two-stream radiation (surface.cu:188-243)
+  R decl = (R)0.40928 * sin((R)6.2832 * ((R)284 + a.doy) / (R)365);
+  R latr = a.lat[c2] * (R)0.0174533;
+  R hsol = utc + a.lon[c2] / (R)15;
+  R H = (R)0.2618 * (hsol - (R)12);
+  R cosz = sin(latr) * sin(decl) + cos(latr) * cos(decl) * cos(H);
+  if (cosz < (R)0) cosz = 0;
+  Col<R> Tlev = C_(SC_TLEV), epslw = C_(SC_EPS), Fup = C_(SC_FUP), Fdn = C_(SC_FDN);
+  Col<R> radht = C_(SC_RAD);
+  for (int k = 0; k < nz; ++k) {
+    const size_t c = L.at(i, j, k);
+    R pik = a.b.pib[c] + a.pip[c];
+    Tlev[k] = thcol[k] * pik;
+    R du = rho[k] * qvcol[k] * dzc[k];
+    R dl = rho[k] * (a.qc[c] > (R)0 ? a.qc[c] : (R)0) * dzc[k] * (R)1000;
+    epslw[k] = (R)1 - exp(-((R)0.22 * du + (R)0.30 * dl));
+  }
+  Fdn[nz] = (R)0;
+  for (int k = nz - 1; k >= 0; --k)
+    Fdn[k] = Fdn[k + 1] * ((R)1 - epslw[k]) + epslw[k] * SIGMA * Tlev[k] * Tlev[k] * Tlev[k] * Tlev[k];
+  R lwd = Fdn[0];
+  Fup[0] = (R)0.97 * SIGMA * Ts * Ts * Ts * Ts + (R)0.03 * Fdn[0];
+  for (int k = 0; k < nz; ++k)
+    Fup[k + 1] = Fup[k] * ((R)1 - epslw[k]) + epslw[k] * SIGMA * Tlev[k] * Tlev[k] * Tlev[k] * Tlev[k];
+  R mu = fmax(cosz, (R)0.05);
+  R cldalb = lwp / (lwp + (R)60);
+  R Sdn = S0 * cosz * (R)0.95 * ((R)1 - cldalb);
+  Col<R> swabs = C_(SC_SW);
+  for (int k = nz - 1; k >= 0; --k) {
+    const size_t c = L.at(i, j, k);
+    R du = rho[k] * qvcol[k] * dzc[k];
+    R dl = rho[k] * (a.qc[c] > (R)0 ? a.qc[c] : (R)0) * dzc[k] * (R)1000;
+    R tau = exp(-((R)0.008 * du + (R)0.15 * dl) / mu);
+    R ab = Sdn * ((R)1 - tau);
+    swabs[k] = ab;
+    Sdn *= tau;
+  }
+  R swn = Sdn * ((R)1 - alb);
+  for (int k = 0; k < nz; ++k) {
+    const size_t c = L.at(i, j, k);
+    R pik = a.b.pib[c] + a.pip[c];
+    R lwconv = (Fdn[k + 1] - Fdn[k]) + (Fup[k] - Fup[k + 1]);
+    R net = lwconv + swabs[k];
+    radht[k] = net / (rho[k] * P::cp * dzc[k]) / pik;
+  }
+  // 4-layer soil (surface.cu:245-282)
+  R lwu = (R)0.97 * SIGMA * Ts * Ts * Ts * Ts;
+  R G = swn + (R)0.97 * lwd - lwu - rho[0] * P::cp * shf * pi1 - rho[0] * P::Lv * qflx;
+  if (onland) {
+    R w = a.soilw[c2];
+    R Cso = (R)1.2e6 + (R)3.2e6 * fmin(fmax(w, (R)0), (R)0.4);
+    R Kso = (R)0.25 + (R)3.0 * fmin(fmax(w, (R)0), (R)0.4);
+    R Tso[4], A[4], B[4], C[4], D[4];
+    for (int l = 0; l < 4; ++l) Tso[l] = a.soilt[(size_t)l * n2 + c2];
+    for (int l = 0; l < 4; ++l) {
+      R cap = Cso * SOIL_DZ[l] / a.dt;
+      R ku = (l > 0) ? Kso / ((R)0.5 * (SOIL_DZ[l - 1] + SOIL_DZ[l])) : (R)0;
+      R kl = (l < 3) ? Kso / ((R)0.5 * (SOIL_DZ[l] + SOIL_DZ[l + 1])) : Kso / SOIL_DZ[l];
+      A[l] = -ku;
+      C[l] = (l < 3) ? -kl : (R)0;
+      B[l] = cap + ku + kl;
+      D[l] = cap * Tso[l];
+    }
+    D[0] += G;
+    D[3] += (Kso / SOIL_DZ[3]) * a.tdeep[c2];
+    for (int l = 1; l < 4; ++l) {
+      R ww = A[l] / B[l - 1];
+      B[l] -= ww * C[l - 1];
+      D[l] -= ww * D[l - 1];
+    }
+    Tso[3] = D[3] / B[3];
+    for (int l = 2; l >= 0; --l) Tso[l] = (D[l] - C[l] * Tso[l + 1]) / B[l];
+    for (int l = 0; l < 4; ++l) {
+      if (Tso[l] < (R)200) Tso[l] = 200;
+      if (Tso[l] > (R)350) Tso[l] = 350;
+      a.soilt[(size_t)l * n2 + c2] = Tso[l];
+    }
+    a.tsk[c2] = Tso[0];
+  }
+  // eddy diffusivity: local Ri or nonlocal Troen-Mahrt (surface.cu:300-371)
+  Col<R> fcg_th = C_(SC_FCGT), fcg_qv = C_(SC_FCGQ);
+  Kw[0] = 0;
+  fcg_th[0] = fcg_qv[0] = fcg_th[nz] = fcg_qv[nz] = 0;
+  if (a.nonlocal) {
+    R ust = sqrt(Cd) * V1;
+    R thv1 = thv[0];
+    R wthv0 = shf * ((R)1 + P::eps61 * qvcol[0]) + P::eps61 * thcol[0] * qflx;
+    const R Ric = (R)0.25;
+    R hpbl = a.m.zeta_c[L.at1(nz - 1)] * J;
+    R ws = ust > (R)0.1 ? ust : (R)0.1;
+    for (int it = 0; it < 3; ++it) {
+      R exc = (wthv0 > (R)0) ? (R)6.8 * wthv0 / ws : (R)0;
+      R thv_s = thv1 + exc;
+      R prevRb = 0;
+      hpbl = a.m.zeta_c[L.at1(nz - 1)] * J;
+      for (int k = 1; k < nz; ++k) {
+        R zc = a.m.zeta_c[L.at1(k)] * J;
+        R Rbk = P::grav * (thv[k] - thv_s) * zc / (thv1 * shear2[k]);
+        if (Rbk >= Ric) {
+          R zcm = a.m.zeta_c[L.at1(k - 1)] * J;
+          R f = (Ric - prevRb) / (Rbk - prevRb + (R)1e-9);
+          f = fmin((R)1, fmax((R)0, f));
+          hpbl = zcm + f * (zc - zcm);
+          break;
+        }
+        prevRb = Rbk;
+      }
+      R zc0 = a.m.zeta_c[L.at1(0)] * J;
+      if (hpbl < zc0) hpbl = zc0;
+      R wstar = (wthv0 > (R)0) ? cbrt(P::grav / thv1 * wthv0 * hpbl) : (R)0;
+      ws = cbrt(ust * ust * ust + (R)0.6 * wstar * wstar * wstar);
+      if (ws < (R)0.1) ws = (R)0.1;
+    }
+    a.pblh[c2] = hpbl;
+    R gth = (wthv0 > (R)0) ? (R)6.8 * shf / (ws * hpbl) : (R)0;
+    R gqv = (wthv0 > (R)0) ? (R)6.8 * qflx / (ws * hpbl) : (R)0;
+    for (int k = 1; k < nz; ++k) {
+      R zw = a.m.zeta_w[L.at1(k)] * J;
+      R Kv;
+      if (wthv0 > (R)0 && zw < hpbl) {
+        R zf = zw / hpbl;
+        Kv = KAPPA * ws * zw * (1 - zf) * (1 - zf);
+        fcg_th[k] = rhow[k] * Kv * gth;
+        fcg_qv[k] = rhow[k] * Kv * gqv;
+      } else {
+        Kv = Kloc[k];
+        fcg_th[k] = fcg_qv[k] = 0;
+      }
+      if (Kv < KM_MIN) Kv = KM_MIN;
+      if (Kv > KM_MAX) Kv = KM_MAX;
+      Kw[k] = Kv;
+      a.km[L.at(i, j, k)] = Kv;
+    }
+  } else {
+    a.pblh[c2] = 0;
+    for (int k = 1; k < nz; ++k) {
+      R Kv = Kloc[k];
+      if (Kv < KM_MIN) Kv = KM_MIN;
+      if (Kv > KM_MAX) Kv = KM_MAX;
+      Kw[k] = Kv;
+      a.km[L.at(i, j, k)] = Kv;
+      fcg_th[k] = fcg_qv[k] = 0;
+    }
+  }
+  Col<R> tA = C_(SC_A), tB = C_(SC_B), tC = C_(SC_C), tD = C_(SC_D);
+  diffuse_col<R>(nz, a.dt, rho, rhow, dzc, dzw, Kw, rho[0] * shf, thcol, &fcg_th, tA, tB, tC, tD);
+  diffuse_col<R>(nz, a.dt, rho, rhow, dzc, dzw, Kw, rho[0] * qflx, qvcol, &fcg_qv, tA, tB, tC, tD);
+  for (int k = 0; k < nz; ++k) {
+    const size_t c = L.at(i, j, k);
+    R dth = a.dt * radht[k];
+    if (dth > (R)0.02) dth = (R)0.02;
+    if (dth < (R)-0.02) dth = (R)-0.02;
+    a.thp[c] = thcol[k] - a.b.thb[c] + dth;
+    R q = qvcol[k];
+    a.qv[c] = q > (R)0 ? q : (R)0;
+  }
+}
+
+// momentum columns: blockIdx.z = 0 for u faces i = 1..nx-1, 1 for v faces
+// j = 1..ny-1: surface drag + implicit mixing (surface.cu:390-436)
+template <typename R>
+__global__ void __launch_bounds__(128) k_sfc_momentum(SfcArgs<R> a) {
+  const Layout& L = a.L;
+  const bool on_v = blockIdx.z == 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + (on_v ? 0 : 1);
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + (on_v ? 1 : 0);
+  if (i >= L.nx || j >= L.ny) return;
+  const int nz = L.nz;
+  const int di = on_v ? 0 : 1, dj = on_v ? 1 : 0;
+  R* f = on_v ? a.v : a.u;
+  R J = (R)0.5 * (a.m.jac[L.at2(i - di, j - dj)] + a.m.jac[L.at2(i, j)]);
+  const size_t ncol = (size_t)L.nx * L.ny, col = (size_t)j * L.nx + i;
+  R* base = a.scratch + (on_v ? (size_t)SM_N * (nz + 1) * ncol : 0);
+  auto C_ = [&](int q) { return Col<R>{base + (size_t)q * (nz + 1) * ncol + col, ncol}; };
+  Col<R> rho = C_(SM_RHO), rhow = C_(SM_RHOW), dzc = C_(SM_DZC), dzw = C_(SM_DZW), Kw = C_(SM_KW);
+  Col<R> phi = C_(SM_PHI);
+  for (int k = 0; k < nz; ++k) {
+    const int kk = L.at1(k);
+    const size_t c = L.at(i, j, k), cb = L.at(i - di, j - dj, k);
+    rho[k] = (R)0.5 * (a.b.rhob[cb] + a.b.rhob[c]);
+    rhow[k] = (R)0.5 * (a.b.rhobw[cb] + a.b.rhobw[c]);
+    dzc[k] = a.m.dzeta_c[kk] * J;
+    dzw[k] = a.m.dzeta_w[kk] * J;
+    Kw[k] = (k > 0) ? (R)0.5 * (a.km[cb] + a.km[c]) : (R)0;
+    phi[k] = f[c];
+  }
+  R cdva = (R)0.5 * (a.cdv[L.at2(i - di, j - dj)] + a.cdv[L.at2(i, j)]);
+  R src0 = -rho[0] * cdva * phi[0];
+  diffuse_col<R>(nz, a.dt, rho, rhow, dzc, dzw, Kw, src0, phi, (const Col<R>*)nullptr, C_(SM_A),
+                 C_(SM_B), C_(SM_C), C_(SM_D));
+  for (int k = 0; k < nz; ++k) f[L.at(i, j, k)] = phi[k];
+}
+
+template <typename R>
+size_t sfc_scratch_count(const Layout& L) {
+  // the mass columns and, afterwards, two sets of momentum columns reuse it
+  size_t per = (size_t)(L.nz + 1) * L.nx * L.ny;
+  return per * (SC_N > 2 * SM_N ? SC_N : 2 * SM_N);
+}
+
+template <typename R>
+int launch_sfc(const SfcArgs<R>& a, cudaStream_t st) {
+  if (!a.scratch) return 2;
+  dim3 b(32, 4);
+  k_sfc_scalar<R><<<dim3((a.L.nx + 31) / 32, (a.L.ny + 3) / 4), b, 0, st>>>(a);
+  k_sfc_momentum<R><<<dim3((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, 2), b, 0, st>>>(a);
+  return 0;
+}
+
+template int launch_sfc<float>(const SfcArgs<float>&, cudaStream_t);
+template int launch_sfc<double>(const SfcArgs<double>&, cudaStream_t);
+template size_t sfc_scratch_count<float>(const Layout&);
+template size_t sfc_scratch_count<double>(const Layout&);
+
+}  // namespace wfe
