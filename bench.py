@@ -157,7 +157,7 @@ def sync_device(world):
         pass
 
 
-def cpu_baseline(steps_cap: float = 20.0):
+def cpu_baseline(seconds: float = 10.0):
     """CPU oracle (FP64, OpenMP over all host cores) on the same workload."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
@@ -171,7 +171,7 @@ def cpu_baseline(steps_cap: float = 20.0):
         it.step(o.dt, n * o.dt)
         n += 1
         el = time.perf_counter() - t0
-        if el > steps_cap or n >= 3:
+        if el > seconds or n >= 400:
             break
     return {"value": cells * n / el, "unit": "cell-updates/s", "cores": O.threads(),
             "kind": "port",
@@ -290,9 +290,12 @@ def main():
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
+    tf = ROOT / "profiles" / "traffic_wk82_160.txt"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dom_name)
+        for ln in tf.read_text().splitlines():
+            parts = ln.split()
+            if len(parts) == 2 and not ln.startswith("#") and parts[0] == dom_name:
+                traffic = int(parts[1])
     c.close()
 
     e2e = None

@@ -143,3 +143,24 @@ def test_watchdog_absmax_reports_nan():
     w[5, 5, 5] = np.nan
     c.set_field("w", w)
     assert c.field_absmax("w") > 1e30 or np.isnan(c.field_absmax("w"))
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_interior_transfers_roundtrip(prec):
+    """Writer-layout uploads/downloads (src/io/writer.cpp:89-107) keep ghosts
+    and agree with the padded transfers."""
+    c = W.Case(CASES / "bubble_open.ini", precision=prec)
+    rng = np.random.default_rng(3)
+    for k in ("u", "w", "qv"):
+        before = c.field(k)
+        nzl = c.nz + 1 if k == "w" else c.nz
+        a = rng.standard_normal((nzl, c.ny, c.nx)).astype(np.float32)
+        c.set_field(k, a, interior=True)
+        back = c.field(k, interior=True, dtype=np.float32)
+        assert np.array_equal(back, a)
+        pad = c.field(k)
+        g = c.ng
+        assert np.array_equal(pad[g:g + nzl, g:g + c.ny, g:g + c.nx].astype(np.float32), a)
+        mask = np.ones(c.shape, bool)
+        mask[g:g + nzl, g:g + c.ny, g:g + c.nx] = False
+        assert np.array_equal(pad[mask], before[mask])

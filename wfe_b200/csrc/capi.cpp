@@ -213,6 +213,9 @@ int wfe_get_base(const wfe_ctx* c, int which, double* out) {
 
 int wfe_field_upload(wfe_ctx* c, int role, int field, const void* host, int dtype, int layout) {
   NEED_MODEL(c);
+  if (host && field >= 0 && field <= 7 && layout == WFE_LAYOUT_INTERIOR)
+    return c->model->upload_interior(role, field, host, dtype == WFE_DTYPE_F32) ? model_err(c)
+                                                                                : WFE_OK;
   if (!c || !host || field < 0 || field > 7) return set_err(c, WFE_ERR_ARG, "bad argument");
   const RefGrid& g = c->cs.g;
   std::vector<double> pad(g.npts(), 0.0);
@@ -236,6 +239,9 @@ int wfe_field_upload(wfe_ctx* c, int role, int field, const void* host, int dtyp
 
 int wfe_field_download(wfe_ctx* c, int role, int field, void* host, int dtype, int layout) {
   NEED_MODEL(c);
+  if (host && field >= 0 && field <= 7 && layout == WFE_LAYOUT_INTERIOR)
+    return c->model->download_interior(role, field, host, dtype == WFE_DTYPE_F32) ? model_err(c)
+                                                                                  : WFE_OK;
   if (!c || !host || field < 0 || field > 7) return set_err(c, WFE_ERR_ARG, "bad argument");
   const RefGrid& g = c->cs.g;
   std::vector<double> pad(g.npts());

@@ -164,6 +164,60 @@ class ModelT final : public Model {
     return 0;
   }
 
+  int download_interior(int role, int field, void* host, bool f32) override {
+    R* d = field_ptr(role, field);
+    if (!d) return fail("bad role/field");
+    const int nzl = field == 2 ? g_.nz + 1 : g_.nz;
+    // only the interior planes cross PCIe
+    const size_t off = L_.at(-kOX, -kOY, 0), cnt = (size_t)nzl * L_.plane();
+    CK(cudaMemcpyAsync(stage_ + off, d + off, cnt * sizeof(R), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    const size_t row = (size_t)g_.nx;
+    for (int k = 0; k < nzl; ++k)
+      for (int j = 0; j < g_.ny; ++j) {
+        const R* src = stage_ + L_.at(0, j, k);
+        size_t o = ((size_t)k * g_.ny + j) * row;
+        if (f32 == (sizeof(R) == 4)) {
+          std::memcpy((char*)host + o * sizeof(R), src, row * sizeof(R));
+        } else if (f32) {
+          float* dst = (float*)host + o;
+          for (size_t i = 0; i < row; ++i) dst[i] = (float)src[i];
+        } else {
+          double* dst = (double*)host + o;
+          for (size_t i = 0; i < row; ++i) dst[i] = (double)src[i];
+        }
+      }
+    return 0;
+  }
+
+  int upload_interior(int role, int field, const void* host, bool f32) override {
+    R* d = field_ptr(role, field);
+    if (!d) return fail("bad role/field");
+    const int nzl = field == 2 ? g_.nz + 1 : g_.nz;
+    // read back the planes first so that ghosts and padding keep their values
+    const size_t off = L_.at(-kOX, -kOY, 0), cnt = (size_t)nzl * L_.plane();
+    CK(cudaMemcpyAsync(stage_ + off, d + off, cnt * sizeof(R), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    const size_t row = (size_t)g_.nx;
+    for (int k = 0; k < nzl; ++k)
+      for (int j = 0; j < g_.ny; ++j) {
+        R* dst = stage_ + L_.at(0, j, k);
+        size_t o = ((size_t)k * g_.ny + j) * row;
+        if (f32 == (sizeof(R) == 4)) {
+          std::memcpy(dst, (const char*)host + o * sizeof(R), row * sizeof(R));
+        } else if (f32) {
+          const float* src = (const float*)host + o;
+          for (size_t i = 0; i < row; ++i) dst[i] = (R)src[i];
+        } else {
+          const double* src = (const double*)host + o;
+          for (size_t i = 0; i < row; ++i) dst[i] = (R)src[i];
+        }
+      }
+    CK(cudaMemcpyAsync(d + off, stage_ + off, cnt * sizeof(R), cudaMemcpyHostToDevice, st_));
+    CK(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
   int upload_state_raw(int field, const void* host) override {
     if (field < 0 || field > 7) return fail("bad field");
     CK(cudaMemcpyAsync(S_[perm_[0]][field], host, L_.n3() * sizeof(R), cudaMemcpyHostToDevice, st_));

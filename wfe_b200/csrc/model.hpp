@@ -28,6 +28,10 @@ class Model {
   // 2D surface fields in the reference padded 2D layout (NX*NY doubles)
   virtual int download2d(int which, double* ref_padded2d) = 0;
   virtual int upload2d(int which, const double* ref_padded2d) = 0;
+  // interior (Writer layout) transfers straight between the device and a host
+  // buffer of float (dtype_f32) or double, without an FP64 padded copy
+  virtual int download_interior(int role, int field, void* host, bool dtype_f32) = 0;
+  virtual int upload_interior(int role, int field, const void* host, bool dtype_f32) = 0;
   // raw device-layout transfers of the state (fast path, same precision)
   virtual int upload_state_raw(int field, const void* host_pitched) = 0;
   virtual int download_state_raw(int field, void* host_pitched) = 0;
