@@ -149,6 +149,30 @@ int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const d
                     const double* lon, const double* soilw, double start_hour_utc, int doy,
                     int nonlocal);
 
+/* ------------------------------------------- allocation-free variant */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- a diagnostics hook running inside another framework's CUDA stream
+ * capture, where cudaMalloc is illegal, or a process whose device memory
+ * belongs to a fixed-budget pool allocator -- this computes the dry-air mass
+ * wfe_dry_mass reports, from device fields the caller owns, and allocates
+ * nothing: its per-level partial sums live in a file-scope __device__ array of
+ * WFE_NOALLOC_MAX_LEVELS doubles (8 KB, held by every GPU that loads the
+ * library until exit).  Inputs are FP64 device arrays in the reference padded
+ * layout (3D: (nx+6)*(ny+6)*(nz+7); jac: (nx+6)*(ny+6); dzeta_c: nz+7); qv, qc,
+ * qr may be NULL for a dry state; out is a device double.  The call is
+ * asynchronous on `stream` (a cudaStream_t, NULL for the legacy stream).
+ * nz > WFE_NOALLOC_MAX_LEVELS is rejected with WFE_ERR_ARG and a message in
+ * wfe_last_error(NULL).  The first call on a device looks up the array's
+ * device address (with that device current); make it before any stream
+ * capture.  All calls on a device share the array: calls that overlap on the
+ * GPU (different streams, or other host threads) race and must be serialised
+ * by the caller. */
+#define WFE_NOALLOC_MAX_LEVELS 1024
+int wfe_dry_mass_noalloc(int nx, int ny, int nz, double dx, double dy, const double* pib,
+                         const double* thb, const double* pip, const double* thp, const double* qv,
+                         const double* qc, const double* qr, const double* jac,
+                         const double* dzeta_c, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,7 @@ SYMBOLS = [
     "wfe_sync", "wfe_absmax", "wfe_dry_mass", "wfe_launches_per_step", "wfe_op_apply_bcs",
     "wfe_op_tendencies", "wfe_op_acoustic", "wfe_op_moisture_stage", "wfe_op_kessler",
     "wfe_op_sfc", "wfe_set_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
+    "wfe_dry_mass_noalloc",
 ]
 
 
@@ -99,6 +100,8 @@ def load_library(path: str | Path | None = None):
                                      C.c_double]
     lib.wfe_set_physics.argtypes = [vp, dp, dp, dp, dp, dp, C.c_double, C.c_int, C.c_int]
     lib.wfe_time_run.argtypes = [vp, C.c_int, C.c_double, C.c_double, dp]
+    lib.wfe_dry_mass_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double] + \
+        [vp] * 11
     lib.wfe_kernel_times.argtypes = [vp, C.c_double, C.c_double, C.c_int, dp, ip, C.c_char_p,
                                      C.c_int, ip]
     if path is None:

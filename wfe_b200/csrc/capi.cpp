@@ -137,6 +137,11 @@ size_t interior_count(const RefGrid& g, int field) {
 
 }  // namespace
 
+namespace wfe {
+// sets the message wfe_last_error(NULL) returns on this thread
+void set_thread_error(const std::string& m) { g_create_err = m; }
+}  // namespace wfe
+
 extern "C" {
 
 int wfe_case_create(const char* ini_path, const char* const* overrides, int n_overrides,
