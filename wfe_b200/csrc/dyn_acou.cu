@@ -89,10 +89,60 @@ __device__ __forceinline__ R theta_v(const AcouArgs<R>& a, int i, int j, int k) 
   return t;
 }
 
+// Interior points: every neighbour the forward step reads is an interior
+// point, so pi* and theta_v are plain offsets from the face (no ghost maps).
+template <typename R>
+__device__ __forceinline__ bool uv_interior(const Layout& L, int i, int j, int k) {
+  return i >= 1 && i < L.nx && j >= 1 && j < L.ny && k >= 1 && k < L.nz - 1;
+}
+
+template <typename R>
+__device__ __forceinline__ R pistar_at(const AcouArgs<R>& a, size_t c) {
+  R cur = a.pi_cur[c];
+  return cur + a.p.acoustic_smdiv * (cur - a.pi_prev[c]);
+}
+
+template <typename R>
+__device__ __forceinline__ R theta_v_at(const AcouArgs<R>& a, size_t c) {
+  R t = a.b.thb[c] + a.th_in[c];
+  if (a.p.moisture) t *= (R)1 + Phys<R>::eps61 * a.qv[c];
+  return t;
+}
+
+// u (d = 1) or v (d = L.px) forward step at an interior face, with the
+// reference's expressions (kernels.cu:499-526)
+template <typename R>
+__device__ __forceinline__ R uv_forward_interior(const AcouArgs<R>& a, int i, int j, int k, bool is_u) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  const size_t c2 = L.at2(i, j);
+  const int d = is_u ? 1 : L.px;
+  const int pl = (int)L.plane();
+  R thb_f = (R)0.5 * (theta_v_at(a, c - d) + theta_v_at(a, c));
+  R mf = (R)0.5 * (a.m.mapf[c2 - d] + a.m.mapf[c2]);
+  R p0 = pistar_at(a, c), pm = pistar_at(a, c - d);
+  R grad = (p0 - pm) / (is_u ? a.dx : a.dy);
+  R slope = (is_u ? a.m.hx_u[c2] : a.m.hy_v[c2]) * ((R)1 - a.m.zeta_c[kk] / a.m.zt);
+  if (slope != (R)0) {
+    R dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
+    R jf = (R)0.5 * (a.m.jac[c2 - d] + a.m.jac[c2]);
+    R dpdz = (R)0.5 *
+             ((pistar_at(a, c - d + pl) - pistar_at(a, c - d - pl)) +
+              (pistar_at(a, c + pl) - pistar_at(a, c - pl))) /
+             dzc2;
+    grad -= slope / jf * dpdz;
+  }
+  const R* tin = is_u ? a.tu : a.tv;
+  const R* vin = is_u ? a.u_in : a.v_in;
+  return vin[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin[c]);
+}
+
 template <typename R>
 __device__ __forceinline__ R u_forward(const AcouArgs<R>& a, int i, int j, int k) {
   // kernels.cu:499-512
   const Layout& L = a.L;
+  if (uv_interior<R>(L, i, j, k)) return uv_forward_interior(a, i, j, k, true);
   const int kk = L.at1(k);
   const R zt = a.m.zt;
   R thbu = (R)0.5 * (theta_v(a, i - 1, j, k) + theta_v(a, i, j, k));
@@ -116,6 +166,7 @@ template <typename R>
 __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k) {
   // kernels.cu:513-526
   const Layout& L = a.L;
+  if (uv_interior<R>(L, i, j, k)) return uv_forward_interior(a, i, j, k, false);
   const int kk = L.at1(k);
   const R zt = a.m.zt;
   R thbv = (R)0.5 * (theta_v(a, i, j - 1, k) + theta_v(a, i, j, k));
@@ -209,15 +260,14 @@ struct ColSmem {
   }
 };
 
-template <typename R, int CX>
-__global__ void k_acoustic_column(AcouArgs<R> a) {
+template <typename R, int CX, int KL>
+__global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Layout& L = a.L;
   const int nz = L.nz;
   ColSmem<R, CX> S(reinterpret_cast<R*>(smem_raw), nz + 1);
   const int tx = threadIdx.x;           // column within the CTA
   const int lane_k = threadIdx.y;       // level lane
-  const int KL = blockDim.y;
   const int i = blockIdx.x * CX + tx;
   const int j = blockIdx.y;
   const bool active = i < L.nx;
@@ -234,6 +284,7 @@ __global__ void k_acoustic_column(AcouArgs<R> a) {
   // phase 1: Av = rho^w theta_v^w (0 at the rigid levels) and the explicit
   // terrain cross flux Sv with the new u, v (kernels.cu:552-568)
   if (active)
+#pragma unroll 4
     for (int k = lane_k; k <= nz; k += KL) {
       R av = 0, sv = 0;
       if (k >= 1 && k < nz) {
@@ -252,6 +303,7 @@ __global__ void k_acoustic_column(AcouArgs<R> a) {
   __syncthreads();
   // phase 2: explicit part of the pi' equation (kernels.cu:570-587)
   if (active)
+#pragma unroll 4
     for (int k = lane_k; k < nz; k += KL) {
       const int kk = L.at1(k);
       const size_t c = L.at(i, j, k);
@@ -270,6 +322,7 @@ __global__ void k_acoustic_column(AcouArgs<R> a) {
   __syncthreads();
   // phase 3: tridiagonal rows for w at inner levels (kernels.cu:589-611)
   if (active)
+#pragma unroll 4
     for (int k = 1 + lane_k; k < nz; k += KL) {
       const int kk = L.at1(k);
       const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
@@ -321,6 +374,7 @@ __global__ void k_acoustic_column(AcouArgs<R> a) {
   __syncthreads();
   // phase 5: pi', theta', w (kernels.cu:636-644)
   if (active)
+#pragma unroll 4
     for (int k = lane_k; k <= nz; k += KL) {
       const size_t c = L.at(i, j, k);
       if (k < nz) {
@@ -358,46 +412,68 @@ size_t column_smem(int nz, int cx) {
   return (size_t)9 * (nz + 1) * cx * sizeof(R);
 }
 
-template <typename R, int CX>
+template <typename R, int CX, int KL>
 static cudaError_t column_attr(size_t sm) {
-  return cudaFuncSetAttribute(k_acoustic_column<R, CX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sm);
+  return cudaFuncSetAttribute(k_acoustic_column<R, CX, KL>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
 }
 
-// columns per CTA: 32 while the column arrays fit in shared memory, else 16 or 8
+// Tile shapes (columns x level lanes) the autotuner chooses from.
+static const int kColumnShapes[][2] = {{32, 8}, {16, 16}, {8, 32}, {32, 4}, {16, 8}, {8, 16}};
+constexpr int kNumColumnShapes = 6;
+
+int acoustic_column_shapes() { return kNumColumnShapes; }
+
 template <typename R>
-static int column_cx(int nz) {
-  const size_t lim = 200 * 1024;
-  if (column_smem<R>(nz, 32) <= lim) return 32;
-  if (column_smem<R>(nz, 16) <= lim) return 16;
-  if (column_smem<R>(nz, 8) <= lim) return 8;
-  return 0;
+static bool column_fits(int nz, int shape) {
+  return column_smem<R>(nz, kColumnShapes[shape][0]) <= 200 * 1024;
 }
 
-// Sets the dynamic shared-memory limit of the column kernel once, outside any
-// stream capture.
+// Sets the dynamic shared-memory limit of every tile shape that fits, once,
+// outside any stream capture.
 template <typename R>
 int prepare_acoustic_column(int nz) {
-  int cx = column_cx<R>(nz);
-  if (!cx) return 2;
-  cudaError_t e = cx == 32   ? column_attr<R, 32>(column_smem<R>(nz, 32))
-                  : cx == 16 ? column_attr<R, 16>(column_smem<R>(nz, 16))
-                             : column_attr<R, 8>(column_smem<R>(nz, 8));
-  return e == cudaSuccess ? 0 : 1;
+  bool any = false;
+  for (int s = 0; s < kNumColumnShapes; ++s) {
+    if (!column_fits<R>(nz, s)) continue;
+    any = true;
+    size_t sm = column_smem<R>(nz, kColumnShapes[s][0]);
+    cudaError_t e;
+    switch (s) {
+      case 0: e = column_attr<R, 32, 8>(sm); break;
+      case 1: e = column_attr<R, 16, 16>(sm); break;
+      case 2: e = column_attr<R, 8, 32>(sm); break;
+      case 3: e = column_attr<R, 32, 4>(sm); break;
+      case 4: e = column_attr<R, 16, 8>(sm); break;
+      default: e = column_attr<R, 8, 16>(sm); break;
+    }
+    if (e != cudaSuccess) return 1;
+  }
+  return any ? 0 : 2;
 }
 
+// shape: index into the tile shapes; out of range or too large for the
+// column picks the first shape that fits.  Returns 0 ok, 2 column too deep.
 template <typename R>
-int launch_acoustic_column(const AcouArgs<R>& a, cudaStream_t st) {
+int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st) {
   const int nz = a.L.nz;
-  const int cx = column_cx<R>(nz);
-  if (cx == 32)
-    k_acoustic_column<R, 32><<<dim3((a.L.nx + 31) / 32, a.L.ny), dim3(32, 8), column_smem<R>(nz, 32), st>>>(a);
-  else if (cx == 16)
-    k_acoustic_column<R, 16><<<dim3((a.L.nx + 15) / 16, a.L.ny), dim3(16, 16), column_smem<R>(nz, 16), st>>>(a);
-  else if (cx == 8)
-    k_acoustic_column<R, 8><<<dim3((a.L.nx + 7) / 8, a.L.ny), dim3(8, 32), column_smem<R>(nz, 8), st>>>(a);
-  else
-    return 2;
+  if (shape < 0 || shape >= kNumColumnShapes || !column_fits<R>(nz, shape)) {
+    shape = -1;
+    for (int s = 0; s < kNumColumnShapes && shape < 0; ++s)
+      if (column_fits<R>(nz, s)) shape = s;
+    if (shape < 0) return 2;
+  }
+  const int cx = kColumnShapes[shape][0], kl = kColumnShapes[shape][1];
+  const size_t sm = column_smem<R>(nz, cx);
+  const dim3 grd((a.L.nx + cx - 1) / cx, a.L.ny), blk(cx, kl);
+  switch (shape) {
+    case 0: k_acoustic_column<R, 32, 8><<<grd, blk, sm, st>>>(a); break;
+    case 1: k_acoustic_column<R, 16, 16><<<grd, blk, sm, st>>>(a); break;
+    case 2: k_acoustic_column<R, 8, 32><<<grd, blk, sm, st>>>(a); break;
+    case 3: k_acoustic_column<R, 32, 4><<<grd, blk, sm, st>>>(a); break;
+    case 4: k_acoustic_column<R, 16, 8><<<grd, blk, sm, st>>>(a); break;
+    default: k_acoustic_column<R, 8, 16><<<grd, blk, sm, st>>>(a); break;
+  }
   return 0;
 }
 
@@ -405,7 +481,7 @@ int launch_acoustic_column(const AcouArgs<R>& a, cudaStream_t st) {
   template void launch_acoustic_coef<R>(const Layout&, const DBase<R>&, const DMetric<R>&, R*, \
                                         R*, R*, R*, R*, cudaStream_t);                         \
   template void launch_acoustic_uv<R>(const AcouArgs<R>&, cudaStream_t);                       \
-  template int launch_acoustic_column<R>(const AcouArgs<R>&, cudaStream_t);                    \
+  template int launch_acoustic_column<R>(const AcouArgs<R>&, int, cudaStream_t);               \
   template int prepare_acoustic_column<R>(int);
 WFE_INST(float)
 WFE_INST(double)

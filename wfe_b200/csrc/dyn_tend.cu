@@ -42,8 +42,22 @@ __device__ __forceinline__ R face5(R qm2, R qm1, R q0, R q1, R q2, R q3, R vel) 
 // is the z rule applied to the laterally mapped source column.  kind: 0 cell
 // scalar, 1 u (x faces 0..nx), 2 v (y faces 0..ny), 3 w (levels 0..nz,
 // w(nz) = 0, odd reflection about w(0) below, about w(nz) above).
+// ghost value of (i, j, k) from the mapped source column (si, sj)
+template <typename R>
+__device__ __forceinline__ R ghost_value(const Layout& L, const R* a, int kind, int si, int sj,
+                                         int k) {
+  if (kind == 3) {  // w: rigid top, odd reflections (kernels.cu:710-723)
+    if (k == L.nz) return 0;
+    if (k >= 0 && k < L.nz) return a[L.at(si, sj, k)];
+    if (k < 0) return (R)2 * a[L.at(si, sj, 0)] - a[L.at(si, sj, -k)];
+    return -a[L.at(si, sj, 2 * L.nz - k)];
+  }
+  return a[L.at(si, sj, map_zc(k, L.nz))];
+}
+
 template <typename R>
 __global__ void k_fill_ghosts(Layout L, GhostJob<R> job, int open_x, int open_y) {
+  // one thread per padded column (i, j) of one field
   const int f = blockIdx.z;
   if (f >= job.n) return;
   R* a = job.f[f];
@@ -55,27 +69,31 @@ __global__ void k_fill_ghosts(Layout L, GhostJob<R> job, int open_x, int open_y)
   const int jlast = (kind == 2 && open_y) ? L.ny : L.ny - 1;
   const int si = map_lat(i, L.nx, ilast, open_x);
   const int sj = map_lat(j, L.ny, jlast, open_y);
-  const bool lateral_ghost = (si != i) || (sj != j);
   const int k0 = -kRefNG, k1 = L.nz + kRefNG;  // inclusive
-  if (kind == 3) {
-    R w0 = a[L.at(si, sj, 0)];
-    for (int k = k0; k <= k1; ++k) {
-      R val;
-      if (k == L.nz) val = 0;
-      else if (k >= 0 && k < L.nz) {
-        if (!lateral_ghost) continue;
-        val = a[L.at(si, sj, k)];
-      } else if (k < 0) val = (R)2 * w0 - a[L.at(si, sj, -k)];
-      else val = -a[L.at(si, sj, 2 * L.nz - k)];
-      a[L.at(i, j, k)] = val;
+  if ((si != i) || (sj != j)) {
+    // lateral ghost column: every level; sources are another column, so the
+    // loads of a chunk of levels are issued before its stores
+    for (int kb = k0; kb <= k1; kb += 8) {
+      R v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (kb + u <= k1) v[u] = ghost_value(L, a, kind, si, sj, kb + u);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (kb + u <= k1) a[L.at(i, j, kb + u)] = v[u];
     }
-  } else {
-    for (int k = k0; k <= k1; ++k) {
-      int sk = map_zc(k, L.nz);
-      if (!lateral_ghost && sk == k) continue;
-      a[L.at(i, j, k)] = a[L.at(si, sj, sk)];
-    }
+    return;
   }
+  // interior column: the levels below 0 and from nz up (w(nz) is the rigid lid)
+  R lo[kRefNG], hi[kRefNG + 1];
+#pragma unroll
+  for (int m = 1; m <= kRefNG; ++m) lo[m - 1] = ghost_value(L, a, kind, i, j, -m);
+#pragma unroll
+  for (int m = 0; m <= kRefNG; ++m) hi[m] = ghost_value(L, a, kind, i, j, L.nz + m);
+#pragma unroll
+  for (int m = 1; m <= kRefNG; ++m) a[L.at(i, j, -m)] = lo[m - 1];
+#pragma unroll
+  for (int m = 0; m <= kRefNG; ++m) a[L.at(i, j, L.nz + m)] = hi[m];
 }
 
 // ------------------------------------------------------------- mass fluxes
@@ -212,12 +230,25 @@ __device__ __forceinline__ R pd_adv(const TendArgs<R>& a, const R* q, const R* r
   R fxl = qflux_x(a, q, i, j, k), fxr = qflux_x(a, q, i + 1, j, k);
   R fyl = qflux_y(a, q, i, j, k), fyr = qflux_y(a, q, i, j + 1, k);
   R fzl = qflux_z(a, q, i, j, k), fzr = qflux_z(a, q, i, j, k + 1);
-  R sxl = fxl * ratio_at(a, ratio, fxl >= (R)0 ? i - 1 : i, j, k);
-  R sxr = fxr * ratio_at(a, ratio, fxr >= (R)0 ? i : i + 1, j, k);
-  R syl = fyl * ratio_at(a, ratio, i, fyl >= (R)0 ? j - 1 : j, k);
-  R syr = fyr * ratio_at(a, ratio, i, fyr >= (R)0 ? j : j + 1, k);
-  R szl = fzl * ratio_at(a, ratio, i, j, fzl >= (R)0 ? k - 1 : k);
-  R szr = fzr * ratio_at(a, ratio, i, j, fzr >= (R)0 ? k : k + 1);
+  R sxl, sxr, syl, syr, szl, szr;
+  if (i > 0 && i < L.nx - 1 && j > 0 && j < L.ny - 1 && k > 0 && k < L.nz - 1) {
+    // every upwind cell is interior: plain offsets from the cell
+    const R* r0 = ratio + L.at(i, j, k);
+    const int sy = L.px, sz = (int)L.plane();
+    sxl = fxl * r0[fxl >= (R)0 ? -1 : 0];
+    sxr = fxr * r0[fxr >= (R)0 ? 0 : 1];
+    syl = fyl * r0[fyl >= (R)0 ? -sy : 0];
+    syr = fyr * r0[fyr >= (R)0 ? 0 : sy];
+    szl = fzl * r0[fzl >= (R)0 ? -sz : 0];
+    szr = fzr * r0[fzr >= (R)0 ? 0 : sz];
+  } else {
+    sxl = fxl * ratio_at(a, ratio, fxl >= (R)0 ? i - 1 : i, j, k);
+    sxr = fxr * ratio_at(a, ratio, fxr >= (R)0 ? i : i + 1, j, k);
+    syl = fyl * ratio_at(a, ratio, i, fyl >= (R)0 ? j - 1 : j, k);
+    syr = fyr * ratio_at(a, ratio, i, fyr >= (R)0 ? j : j + 1, k);
+    szl = fzl * ratio_at(a, ratio, i, j, fzl >= (R)0 ? k - 1 : k);
+    szr = fzr * ratio_at(a, ratio, i, j, fzr >= (R)0 ? k : k + 1);
+  }
   R fdiv = (sxr - sxl) / a.dx + (syr - syl) / a.dy + (szr - szl) / a.m.dzeta_c[L.at1(k)];
   R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
   return (-fdiv + q[L.at(i, j, k)] * div) / rt;
@@ -257,8 +288,25 @@ __device__ __forceinline__ R davies(const TendArgs<R>& a, int v, const R* f, int
   return w * (((R)1 - tf) * a.lo[v][c] + tf * a.hi[v][c] - f[c]);
 }
 
-// ------------------------------------------------------ fused tendencies
+// One moisture species: tendency (op API) or stage value (integrator).
 template <typename R>
+__device__ __forceinline__ void moist_species(const TendArgs<R>& a, const R* q, const R* ratio,
+                                              R* tq, const R* qn, R* qo, bool davies_qv, int i,
+                                              int j, int k, size_t c, R div0) {
+  R t = (a.p.pd_moist && ratio) ? pd_adv(a, q, ratio, i, j, k, div0)
+                                : scalar_adv(a, q, i, j, k, div0);
+  if (davies_qv) t += davies(a, 4, q, i, j, k);
+  if (qo) qo[c] = qn[c] + a.dt_stage * t;
+  else tq[c] = t;
+}
+
+// ------------------------------------------------------ fused tendencies
+// PART selects the prognostics a launch computes: 1 = momentum (u, v, w),
+// 2 = scalars (theta', pi' relaxation, qv, qc, qr), 3 = all of them.  The
+// split variants need fewer registers (higher occupancy); the autotuner picks.
+enum { TEND_MOM = 1, TEND_SCAL = 2, TEND_ALL = 3 };
+
+template <typename R, int PART>
 __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
   const Layout& L = a.L;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -276,7 +324,7 @@ __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
   const R div0 = divergence(a, i, j, k);
 
   // ---- u on the x face i (kernels.cu:308-346)
-  {
+  if (PART & TEND_MOM) {
     const R* U = a.u + c;
     R fcL = (R)0.5 * (MX[-sx] + MX[0]), fcR = (R)0.5 * (MX[0] + MX[sx]);
     R FxL = fcL * face5(U[-3 * sx], U[-2 * sx], U[-sx], U[0], U[sx], U[2 * sx], fcL);
@@ -300,7 +348,7 @@ __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
     a.tu[c] = t;
   }
   // ---- v on the y face j (kernels.cu:348-385)
-  {
+  if (PART & TEND_MOM) {
     const R* V = a.v + c;
     R fcB = (R)0.5 * (MY[-sy] + MY[0]), fcT = (R)0.5 * (MY[0] + MY[sy]);
     R FyB = fcB * face5(V[-3 * sy], V[-2 * sy], V[-sy], V[0], V[sy], V[2 * sy], fcB);
@@ -325,7 +373,7 @@ __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
     a.tv[c] = t;
   }
   // ---- w on the inner level k >= 1 (kernels.cu:387-425)
-  if (k >= 1) {
+  if ((PART & TEND_MOM) && k >= 1) {
     const R* W = a.w + c;
     R fxL = (R)0.5 * (MX[-sz] + MX[0]), fxR = (R)0.5 * (MX[sx - sz] + MX[sx]);
     R FxL = fxL * face5(W[-3 * sx], W[-2 * sx], W[-sx], W[0], W[sx], W[2 * sx], fxL);
@@ -349,6 +397,7 @@ __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.w, i, j, k, true);
     a.tw[c] = t;
   }
+  if (!(PART & TEND_SCAL)) return;
   // ---- theta' (kernels.cu:114-146)
   {
     R t = scalar_adv(a, a.thp, i, j, k, div0) - sponge(a.m.zeta_c[kk], zt, a.p) * a.thp[c];
@@ -360,19 +409,9 @@ __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
   if (a.tpi) a.tpi[c] = bdy ? davies(a, 3, a.pip, i, j, k) : (R)0;
   // ---- moisture (kernels.cu:886-899) and its stage update (kernels.cu:268-273)
   if (a.p.moisture) {
-    const R* qs[3] = {a.qv, a.qc, a.qr};
-    const R* rs[3] = {a.ratio_v, a.ratio_c, a.ratio_r};
-    R* ts[3] = {a.tqv, a.tqc, a.tqr};
-    const R* qn[3] = {a.qn_v, a.qn_c, a.qn_r};
-    R* qo[3] = {a.qo_v, a.qo_c, a.qo_r};
-#pragma unroll 1
-    for (int s = 0; s < 3; ++s) {
-      R t = (a.p.pd_moist && rs[s]) ? pd_adv(a, qs[s], rs[s], i, j, k, div0)
-                                     : scalar_adv(a, qs[s], i, j, k, div0);
-      if (s == 0 && bdy) t += davies(a, 4, a.qv, i, j, k);
-      if (qo[s]) qo[s][c] = qn[s][c] + a.dt_stage * t;
-      else ts[s][c] = t;
-    }
+    moist_species(a, a.qv, a.ratio_v, a.tqv, a.qn_v, a.qo_v, bdy, i, j, k, c, div0);
+    moist_species(a, a.qc, a.ratio_c, a.tqc, a.qn_c, a.qo_c, false, i, j, k, c, div0);
+    moist_species(a, a.qr, a.ratio_r, a.tqr, a.qn_r, a.qo_r, false, i, j, k, c, div0);
   }
 }
 
@@ -435,10 +474,15 @@ void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st)
 }
 
 template <typename R>
-void launch_tendencies(const TendArgs<R>& a, cudaStream_t st) {
+void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
   dim3 blk(32, 4, 2);
   dim3 grd((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
-  k_tendencies<R><<<grd, blk, 0, st>>>(a);
+  if (variant == 1) {
+    k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);
+    k_tendencies<R, TEND_SCAL><<<grd, blk, 0, st>>>(a);
+  } else {
+    k_tendencies<R, TEND_ALL><<<grd, blk, 0, st>>>(a);
+  }
 }
 
 #define WFE_INST(R)                                                                               \
@@ -446,7 +490,7 @@ void launch_tendencies(const TendArgs<R>& a, cudaStream_t st) {
   template void launch_mass_flux<R>(const Layout&, const DBase<R>&, const DMetric<R>&, const R*,  \
                                     const R*, const R*, R*, R*, R*, cudaStream_t);                \
   template void launch_pd_ratio<R>(const TendArgs<R>&, R*, R*, R*, cudaStream_t);                 \
-  template void launch_tendencies<R>(const TendArgs<R>&, cudaStream_t);                         \
+  template void launch_tendencies<R>(const TendArgs<R>&, int, cudaStream_t);                         \
   template void launch_axpy<R>(const R*, const R*, R, R*, size_t, cudaStream_t);
 WFE_INST(float)
 WFE_INST(double)

@@ -107,16 +107,20 @@ void launch_mass_flux(const Layout& L, const DBase<R>& b, const DMetric<R>& m, c
                       const R* v, const R* w, R* mfx, R* mfy, R* mfz, cudaStream_t st);
 template <typename R>
 void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st);
+// variant 0: one fused launch; 1: momentum and scalar launches
 template <typename R>
-void launch_tendencies(const TendArgs<R>& a, cudaStream_t st);
+void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st);
 
 template <typename R>
 void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,
                           R* rtjx, R* rtjy, R* kt3, R* aw, cudaStream_t st);
 template <typename R>
 void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st);
+// shape: tile-shape index (columns x level lanes) in [0, acoustic_column_shapes());
+// one that does not fit the column depth falls back to the first that does
 template <typename R>
-int launch_acoustic_column(const AcouArgs<R>& a, cudaStream_t st);  // returns 0 ok
+int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st);
+int acoustic_column_shapes();
 template <typename R>
 int prepare_acoustic_column(int nz);
 template <typename R>

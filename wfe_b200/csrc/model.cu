@@ -16,14 +16,70 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <sstream>
 
 #include "core.cuh"
 #include "kernels.cuh"
 #include "model.hpp"
 
 namespace wfe {
+
+// Kernel variants picked by the autotuner.  Every variant computes the same
+// values with the same arithmetic; only launch shapes differ.
+struct Tune {
+  int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches
+  int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
+  bool done = false;
+};
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, Tune> g_tune_cache;
+
+std::string tune_cache_path() {
+  const char* p = std::getenv("WFE_TUNE_CACHE");
+  if (p && *p) return p;
+  const char* h = std::getenv("HOME");
+  return std::string(h && *h ? h : "/tmp") + "/.wfe_b200_tune.txt";
+}
+
+bool tune_lookup(const std::string& key, Tune* t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune_cache.find(key);
+  if (it != g_tune_cache.end()) {
+    *t = it->second;
+    return true;
+  }
+  std::ifstream f(tune_cache_path());
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream ss(line);
+    std::string k;
+    Tune v;
+    if (ss >> k >> v.tend_variant >> v.column_cx && k == key) {
+      v.done = true;
+      g_tune_cache[key] = v;
+      *t = v;
+      return true;
+    }
+  }
+  return false;
+}
+
+void tune_store(const std::string& key, const Tune& t) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = t;
+  // best effort: the cache file is an optimisation only (its directory must exist)
+  std::ofstream f(tune_cache_path(), std::ios::app);
+  if (f) f << key << " " << t.tend_variant << " " << t.column_cx << "\n";
+}
+}  // namespace
 
 #define CK(call)                                                                  \
   do {                                                                            \
@@ -260,6 +316,7 @@ class ModelT final : public Model {
 
   // ------------------------------------------------------------- stepping
   int step(double dt, double t) override {
+    if (autotune(dt)) return 1;
     launch_clock(clock_, t, t_lo_, t_hi_, dt, 0, st_);
     launches_ = 1;
     if (enqueue_step((R)dt)) return 1;
@@ -269,6 +326,7 @@ class ModelT final : public Model {
   }
 
   int run(int nsteps, double dt, double t0) override {
+    if (autotune(dt)) return 1;
     launch_clock(clock_, t0, t_lo_, t_hi_, dt, 0, st_);
     if (!graphs_valid_ || graph_dt_ != dt) {
       for (auto& ge : gexec_)
@@ -484,6 +542,88 @@ class ModelT final : public Model {
   }
 
  private:
+  // ------------------------------------------------------------ autotuner
+  // Times each kernel variant on the live buffers before the first step.  The
+  // trial launches read time n and write only scratch, tendencies and the
+  // stage-output state, which the step overwrites.  WFE_TUNE=0 keeps defaults.
+  std::string tune_key() const {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, dev_);
+    std::ostringstream k;
+    std::string name = prop.name;
+    for (char& ch : name)
+      if (ch == ' ') ch = '_';
+    k << "v2|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
+      << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0);
+    return k.str();
+  }
+
+  template <class F>
+  int time_ms(F&& f, float* best) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    *best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      CK(cudaEventRecord(e0, st_));
+      if (f()) return 1;
+      CK(cudaEventRecord(e1, st_));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < *best) *best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+  }
+
+  int autotune(double dt) {
+    if (tune_.done) return 0;
+    tune_.done = true;
+    const char* env = std::getenv("WFE_TUNE");
+    if (env && env[0] == '0') return 0;
+    const std::string key = tune_key();
+    Tune cached;
+    if (tune_lookup(key, &cached)) {
+      tune_ = cached;
+      return 0;
+    }
+    R** N = S_[perm_[0]];
+    R** X = S_[perm_[1]];
+    long saved = launches_;
+    GhostJob<R> job = ghost_job(N, false);
+    launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_);
+    float best = 1e30f;
+    for (int v = 0; v < 2; ++v) {
+      float ms;
+      tune_.tend_variant = v;
+      if (time_ms([&] { tendencies(N, N, X, (R)dt, (R)dt / 3, false); return 0; }, &ms)) return 1;
+      if (ms < best) {
+        best = ms;
+        cached.tend_variant = v;
+      }
+    }
+    best = 1e30f;
+    const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
+    for (int cx = 0; cx < acoustic_column_shapes(); ++cx) {
+      float ms;
+      tune_.column_cx = cx;
+      if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
+      if (ms < best) {
+        best = ms;
+        cached.column_cx = cx;
+      }
+    }
+    launches_ = saved;
+    CK(cudaStreamSynchronize(st_));
+    CK(cudaGetLastError());
+    cached.done = true;
+    tune_ = cached;
+    tune_store(key, tune_);
+    return 0;
+  }
+
   // --------------------------------------------------------------- pieces
   struct ProfRec {
     std::string name;
@@ -585,7 +725,7 @@ class ModelT final : public Model {
       a.qo_r = X[7];
       a.dt_stage = dt_stage;
     }
-    launch("tendencies", [&] { launch_tendencies<R>(a, st_); });
+    launch("tendencies", [&] { launch_tendencies<R>(a, tune_.tend_variant, st_); });
   }
 
   // ns acoustic substeps from time n (N) into the stage output X
@@ -632,7 +772,7 @@ class ModelT final : public Model {
       a.pi_next = pbuf(t + 1);
       launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
       int rc = 0;
-      launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, st_); });
+      launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, tune_.column_cx, st_); });
       if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
       uin = uout;
       vin = vout;
@@ -846,6 +986,7 @@ class ModelT final : public Model {
   long launches_ = 0, glaunches_ = 0;
   bool profiling_ = false;
   std::vector<ProfRec> prof_;
+  Tune tune_;
 };
 
 Model* Model::create(const CaseSetup& cs, bool fp64, int device, std::string* err) {
