@@ -458,3 +458,121 @@ class Integrator:
 
 def threads() -> int:
     return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+# ------------------------------------------------------------- file mode
+def load_prep(d, nx: int, ny: int, nz: int) -> dict:
+    """wfe_input.ini + wfe_init.bin of a prep directory (src/io/input.cpp:19-57)."""
+    d = Path(d)
+    meta = read_ini(d / "wfe_input.ini")
+    assert (int(meta["nx"]), int(meta["ny"]), int(meta["nz"])) == (nx, ny, nz), "grid mismatch"
+    assert int(meta.get("version", 1)) >= 3, "input version < 3"
+    npf = int(meta.get("np_prof", 0))
+    n2, n3 = nx * ny, nx * ny * nz
+    raw = np.fromfile(d / "wfe_init.bin", dtype=np.float32).astype(np.float64)
+    out, o = {}, 0
+    for k, n in (("prof_z", npf), ("prof_th", npf), ("prof_qv", npf), ("prof_u", npf),
+                 ("h", n2), ("fcor", n2), ("tsk", n2), ("land", n2), ("lat", n2),
+                 ("lon", n2), ("soilw", n2), ("u", n3), ("v", n3), ("th", n3), ("pi", n3),
+                 ("qv", n3)):
+        out[k] = raw[o:o + n].copy()
+        o += n
+    assert o == raw.size, "wfe_init.bin is short or corrupt"
+    out["dir"] = d
+    out["start"] = meta.get("start", "")
+    out["bdy_interval"] = _atof(meta.get("bdy_interval", "10800"))
+    out["n_bdy"] = int(meta.get("n_bdy", 0))
+    return out
+
+
+def load_bdy(inputs: dict, nx: int, ny: int, nz: int, idx: int) -> list:
+    """wfe_bdy_FFF.bin, FFF = idx * bdy_interval / 3600 (src/io/input.cpp:59-73)."""
+    fh = int(idx * inputs["bdy_interval"] / 3600)
+    raw = np.fromfile(Path(inputs["dir"]) / f"wfe_bdy_{fh:03d}.bin", dtype=np.float32)
+    n3 = nx * ny * nz
+    assert raw.size == 5 * n3, "boundary file is short or corrupt"
+    return [raw[v * n3:(v + 1) * n3].astype(np.float64).reshape(nz, ny, nx) for v in range(5)]
+
+
+class FileRun:
+    """A file-mode case set up and stepped as src/main.cpp:313-383 does: Lambert
+    map factor, base state from the profile tables, initial state from
+    wfe_init.bin (+ ic_perturb), Davies targets from the boundary files
+    (BdyManager, src/dynamics/boundary.cpp:9-97) and the surface scheme."""
+
+    def __init__(self, ini, overrides: dict | None = None):
+        kv = read_ini(ini)
+        kv.update({k: str(v) for k, v in (overrides or {}).items()})
+        c = Cfg(kv)
+        nx, ny, nz = c.int("nx", 100), c.int("ny", 100), c.int("nz", 50)
+        inp = load_prep(c.str("input_dir", ""), nx, ny, nz)
+        mapf = np.zeros(nx * ny)
+        lib().orc_lambert_mapf(nx * ny, ptr(np.ascontiguousarray(inp["lat"])),
+                               C.c_double(c.real("proj_lat1", 35)),
+                               C.c_double(c.real("proj_lat2", 43)), ptr(mapf))
+        inp["mapf"] = mapf
+        self.inputs = inp
+        self.case = cs = Case(kv=kv, inputs=inp)
+        g = cs.grid
+        s = cs.new_state()
+        st = cs.state_struct(s)
+        arrs = [np.ascontiguousarray(inp[k]) for k in ("u", "v", "th", "pi", "qv")]
+        lib().orc_ic_from_input(C.byref(g), C.byref(cs.base_s), *[ptr(a) for a in arrs],
+                                C.byref(st))
+        lib().orc_ic_perturb(C.byref(g), C.c_double(c.real("ic_perturb", 0)),
+                             C.c_uint(c.int("ens_seed", 0)), ptr(s["thp"]))
+        self.s0 = {k: v.copy() for k, v in s.items()}
+        self.it = cs.integrator()
+        self.it.set_state(s)
+        self.wgt = cs.bdy_weights(c.int("bdy_width", 8), c.real("bdy_tau", 600),
+                                  c.real("nudge_tau", 0))
+        self.idx_hi = 1
+        self.lo = self.targets(0)
+        self.hi = self.targets(min(1, inp["n_bdy"] - 1))
+        self.t_lo, self.t_hi = 0.0, inp["bdy_interval"]
+        self.it.set_boundary(self.lo, self.hi, self.wgt, self.t_lo, self.t_hi)
+        self.sfc = None
+        if c.str("physics", "none") == "simple":
+            st_ = inp["start"]
+            mo, dd, hh = int(st_[4:6]), int(st_[6:8]), int(st_[8:10])
+            cum = [0, 31, 59, 90, 120, 151, 181, 212, 243, 273, 304, 334]
+            self.sfc = cs.sfc(inp["tsk"], inp["land"], inp["lat"], inp["lon"], inp["soilw"],
+                              float(hh), cum[mo - 1] + dd, c.str("pbl", "local") == "nonlocal")
+            self.it.set_physics(self.sfc)
+
+    def targets(self, idx: int) -> list:
+        """Padded perturbation targets of boundary file idx (boundary.cpp:51-81)."""
+        cs, g = self.case, self.case.grid
+        nx, ny, nz = g.nx, g.ny, g.nz
+        f = load_bdy(self.inputs, nx, ny, nz, idx)
+        out = [cs.zeros() for _ in range(5)]
+        v3 = [cs.interior(a) for a in out]  # views (nz, ny, nx) into the padded arrays
+        a3 = [np.asarray(a).reshape(cs.shape) for a in out]
+        il = np.r_[0, np.arange(nx)]          # u faces 0..nx: centres (i-1, i) clamped
+        ir = np.r_[np.arange(nx), nx - 1]
+        a3[0][g.ng:g.ng + nz, g.ng:g.ng + ny, g.ng:g.ng + nx + 1] = 0.5 * (f[0][:, :, il] +
+                                                                             f[0][:, :, ir])
+        jl = np.r_[0, np.arange(ny - 1)]
+        v3[1][:] = 0.5 * (f[1][:, jl, :] + f[1])
+        v3[2][:] = f[2] - cs.interior(cs.base["thb"])
+        v3[3][:] = f[3] - cs.interior(cs.base["pib"])
+        v3[4][:] = f[4]
+        return out
+
+    def update(self, t: float) -> None:
+        """BdyManager::update (boundary.cpp:83-89)."""
+        n_bdy = self.inputs["n_bdy"]
+        changed = False
+        while t >= self.t_hi and self.idx_hi + 1 < n_bdy:
+            self.lo = self.hi
+            self.idx_hi += 1
+            self.hi = self.targets(self.idx_hi)
+            self.t_lo = self.t_hi
+            self.t_hi += self.inputs["bdy_interval"]
+            changed = True
+        if changed:
+            self.it.set_boundary(self.lo, self.hi, self.wgt, self.t_lo, self.t_hi)
+
+    def step(self, dt: float, t: float) -> None:
+        self.update(t)
+        self.it.step(dt, t)

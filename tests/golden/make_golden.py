@@ -16,6 +16,11 @@ Two steps, run from the repository root:
       (float64) and the unmodified executables' snapshots into
       tests/golden/<case>_wfe.npz (float32).
 
+  The file-mode case file_small (tests/helpers.py: seeded synthetic prep inputs
+  from wfe_b200.synth) runs through the unmodified executables only, for
+  FILE_STEPS steps; its snapshots at steps 0, 8 and FILE_STEPS, the logs and the
+  SHA-256 of the generated wfe_init.bin go to tests/golden/file_small_wfe.npz.
+
 The cases are small grids so that the pure-CPU oracle finishes in seconds.
 """
 
@@ -28,10 +33,14 @@ import subprocess
 import sys
 from pathlib import Path
 
+import hashlib
+
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
 CASES = HERE / "cases"
 REF = ROOT / "oracle" / "_ref"
 
@@ -39,6 +48,8 @@ RUN_CASES = ["bubble_open", "straka_periodic", "schaer_open", "wk82_small", "moi
 OPS_CASES = ["ops_open", "ops_periodic"]
 NSTEPS = 8
 DUMPS = "1,8"
+FILE_CASES = ["file_small"]
+FILE_STEPS = 65
 
 
 def read_ini(path: Path) -> dict:
@@ -82,6 +93,16 @@ def run(raw: Path) -> None:
                 sh([REF / f"wfe_{prec}", ini, f"out_dir={wout}", f"out_interval={dt}",
                     f"diag_interval={dt}", f"t_end={NSTEPS * dt}"],
                    raw / f"{case}_wfe{prec[1:]}.log")
+    from helpers import make_file_small
+    for case in FILE_CASES:
+        ini = make_file_small(raw / f"{case}_case")
+        dt = float(read_ini(ini)["dt"])
+        for prec in ("f64", "f32"):
+            wout = raw / f"{case}_wfe{prec[1:]}"
+            shutil.rmtree(wout, ignore_errors=True)
+            sh([REF / f"wfe_{prec}", ini, f"out_dir={wout}", f"out_interval={dt}",
+                f"diag_interval={dt}", f"t_end={FILE_STEPS * dt}"],
+               raw / f"{case}_wfe{prec[1:]}.log")
 
 
 def load_dump(d: Path) -> dict:
@@ -116,14 +137,32 @@ def pack(raw: Path) -> None:
                     (raw / f"{case}_wfe{prec}.log").read_bytes(), dtype=np.uint8)
             np.savez_compressed(HERE / f"{case}_wfe.npz", **snaps)
         print(case, "packed")
+    for case in FILE_CASES:
+        snaps = {}
+        for prec in ("64", "32"):
+            wdir = raw / f"{case}_wfe{prec}"
+            for step in (0, 8, FILE_STEPS):
+                for f in sorted(wdir.glob(f"*_{step:06d}.bin")):
+                    snaps[f"wfe{prec}_{f.stem}"] = np.fromfile(f, dtype=np.float32)
+            snaps[f"wfe{prec}_log"] = np.frombuffer(
+                (raw / f"{case}_wfe{prec}.log").read_bytes(), dtype=np.uint8)
+        init = raw / f"{case}_case" / f"{case}_prep" / "wfe_init.bin"
+        snaps["prep_sha256"] = np.frombuffer(hashlib.sha256(init.read_bytes()).digest(),
+                                             dtype=np.uint8)
+        np.savez_compressed(HERE / f"{case}_wfe.npz", **snaps)
+        print(case, "packed")
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["run", "pack"])
     ap.add_argument("--raw", default="gpurun_out/golden_raw")
+    ap.add_argument("--only-file", action="store_true", help="the file-mode cases only")
     a = ap.parse_args()
     os.chdir(ROOT)
+    if a.only_file:
+        RUN_CASES.clear()
+        OPS_CASES.clear()
     (run if a.what == "run" else pack)(Path(a.raw))
 
 

@@ -11,6 +11,21 @@ GOLDEN = ROOT / "tests" / "golden"
 CASES = GOLDEN / "cases"
 
 
+FILE_SMALL = dict(nx=24, ny=20, nz=12, dx=12000.0, dy=12000.0, dz=20000.0 / 12)
+FILE_SMALL_STEPS = 65  # crosses the first boundary-file switch at t = 3600 s
+
+
+def make_file_small(root: Path) -> Path:
+    """The small file-mode case of the goldens: 24 x 20 x 12, dx = 12 km, seeded
+    synthetic prep inputs (wfe_b200.synth, seed 7, u0 = 12 m/s) with 2 h of
+    hourly constant boundary files; returns the case .ini."""
+    from wfe_b200 import synth
+    root = Path(root)
+    prep = root / "file_small_prep"
+    synth.write_prep(prep, seed=7, u0=12.0, hours=2, bdy_interval=3600, **FILE_SMALL)
+    return synth.write_case(root / "file_small.ini", prep, dt=60.0, bdy_width=3, **FILE_SMALL)
+
+
 def golden(case: str):
     return np.load(GOLDEN / f"{case}.npz")
 

@@ -13,7 +13,8 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import CASES, GOLDEN, ghost_ok_mask, golden, scaled_err
+from helpers import (CASES, FILE_SMALL_STEPS, GOLDEN, ghost_ok_mask, golden, make_file_small,
+                     scaled_err)
 
 RUN_CASES = ["bubble_open", "straka_periodic", "schaer_open", "wk82_small", "moist_blob"]
 OPS_CASES = ["ops_open", "ops_periodic"]
@@ -183,3 +184,40 @@ def test_ops_surface_pbl(ops_case):
         _check_state(c, s, G, pre, fields=["u", "v", "thp", "qv"], tol=1e-11)
         for f in ("tsk", "pblh", "t2m", "u10"):
             assert scaled_err(ph.field(f), G[f"{pre}_{f}"]) <= 1e-11, (pre, f)
+
+
+def test_file_mode_matches_unmodified_reference_executable(tmp_path):
+    """file_small (seeded synthetic prep inputs; Davies boundaries with a
+    boundary-file switch at 3600 s, surface layer + nonlocal PBL + soil +
+    radiation, Kessler, positive-definite moisture, Lambert map factors) through
+    the unmodified wfe_f64 against the oracle's file-mode run."""
+    import hashlib
+    W = np.load(GOLDEN / "file_small_wfe.npz")
+    ini = make_file_small(tmp_path)
+    sha = hashlib.sha256((tmp_path / "file_small_prep" / "wfe_init.bin").read_bytes()).digest()
+    assert sha == bytes(W["prep_sha256"]), "the generator no longer writes the pinned inputs"
+    r = O.FileRun(ini)
+    c = r.case
+    for k in ("u", "v", "w", "thp", "pip", "qv"):
+        kind = "w" if k == "w" else "c"
+        got = c.interior(r.s0[k], kind).astype(np.float32).ravel()
+        assert np.array_equal(got, W[f"wfe64_{k}_000000"]), k
+    for step in range(1, FILE_SMALL_STEPS + 1):
+        r.step(c.dt, (step - 1) * c.dt)
+        if step in (8, FILE_SMALL_STEPS):
+            st = r.it.state()
+            for k in O.FIELDS:
+                kind = "w" if k == "w" else "c"
+                ref = W[f"wfe64_{k}_{step:06d}"].astype(np.float64)
+                got = c.interior(st[k], kind).ravel()
+                assert scaled_err(got, ref) <= 2.5e-7, (step, k, scaled_err(got, ref))
+            g2 = c.grid
+            for name in ("tsk", "pblh", "t2m", "u10"):
+                ref = W[f"wfe64_{name}_{step:06d}"].astype(np.float64)
+                got = r.sfc.field(name).reshape(g2.NY, g2.NX)[3:-3, 3:-3].ravel()
+                assert scaled_err(got, ref) <= 2.5e-7, (step, name)
+            ref = W[f"wfe64_rain_{step:06d}"].astype(np.float64)
+            got = r.it.rain().reshape(g2.NY, g2.NX)[3:-3, 3:-3].ravel()
+            assert np.abs(got - ref).max() <= 2.5e-7 * max(np.abs(ref).max(), 1e-12), step
+    log = bytes(W["wfe64_log"]).decode()
+    assert f"bitti: {FILE_SMALL_STEPS} adim" in log
