@@ -149,6 +149,35 @@ int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const d
                     const double* lon, const double* soilw, double start_hour_utc, int doy,
                     int nonlocal);
 
+/* --------------------------------------------------- batched ensembles */
+/* No counterpart in the reference, whose ensemble driver runs one process per
+ * member (tools/run_ensemble.py:61-64).  An ensemble advances member contexts
+ * of possibly different grid sizes together: every kernel of the RK3 step is
+ * one batched launch over a member x tile work list, and the whole step with
+ * its acoustic substeps is captured in one CUDA graph per rotation phase.
+ * Members are contexts created with a device (same device, same precision,
+ * same moisture / microphysics / positive-definite / boundary / surface /
+ * acoustic_ns settings, same step count so far); they stay owned by the
+ * caller, must outlive the ensemble, and keep serving field transfers,
+ * wfe_absmax, wfe_dry_mass and so on.  Errors are reported through
+ * wfe_last_error(NULL). */
+typedef struct wfe_ens wfe_ens;
+int wfe_ensemble_create(wfe_ctx* const* members, int n, wfe_ens** out);
+int wfe_ensemble_destroy(wfe_ens* ens);
+/* nsteps steps of every member from t0 with a common dt; boundary files of
+ * file-mode members are switched between graph replays as wfe_run does;
+ * asynchronous until wfe_ensemble_sync (member transfers wait for it too). */
+int wfe_ensemble_run(wfe_ens* ens, int nsteps, double dt, double t0);
+/* one step with direct batched launches (no graph) */
+int wfe_ensemble_step(wfe_ens* ens, double dt, double t);
+int wfe_ensemble_sync(wfe_ens* ens);
+/* nsteps graph-replayed steps timed with CUDA events on the ensemble's stream */
+int wfe_ensemble_time_run(wfe_ens* ens, int nsteps, double dt, double t0, double* ms);
+/* batched launches per step; tuned variants (tendencies split, acoustic
+ * column tile shape, persistent grid) */
+long wfe_ensemble_launches_per_step(const wfe_ens* ens);
+int wfe_ensemble_variants(const wfe_ens* ens, int out[3]);
+
 /* ------------------------------------------- allocation-free variant */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory -- a diagnostics hook running inside another framework's CUDA stream

@@ -26,7 +26,7 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["Case", "WfeError", "load_library", "FIELDS"]
+__all__ = ["Case", "Ensemble", "WfeError", "load_library", "FIELDS"]
 
 PKG = Path(__file__).resolve().parent
 LIBPATH = PKG / "libwfe_b200.so"
@@ -46,7 +46,9 @@ SYMBOLS = [
     "wfe_sync", "wfe_absmax", "wfe_dry_mass", "wfe_launches_per_step", "wfe_op_apply_bcs",
     "wfe_op_tendencies", "wfe_op_acoustic", "wfe_op_moisture_stage", "wfe_op_kessler",
     "wfe_op_sfc", "wfe_set_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
-    "wfe_dry_mass_noalloc",
+    "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
+    "wfe_ensemble_step", "wfe_ensemble_sync", "wfe_ensemble_time_run",
+    "wfe_ensemble_launches_per_step", "wfe_ensemble_variants",
 ]
 
 
@@ -104,6 +106,15 @@ def load_library(path: str | Path | None = None):
         [vp] * 11
     lib.wfe_kernel_times.argtypes = [vp, C.c_double, C.c_double, C.c_int, dp, ip, C.c_char_p,
                                      C.c_int, ip]
+    lib.wfe_ensemble_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
+    lib.wfe_ensemble_destroy.argtypes = [vp]
+    lib.wfe_ensemble_run.argtypes = [vp, C.c_int, C.c_double, C.c_double]
+    lib.wfe_ensemble_step.argtypes = [vp, C.c_double, C.c_double]
+    lib.wfe_ensemble_sync.argtypes = [vp]
+    lib.wfe_ensemble_time_run.argtypes = [vp, C.c_int, C.c_double, C.c_double, dp]
+    lib.wfe_ensemble_launches_per_step.argtypes = [vp]
+    lib.wfe_ensemble_launches_per_step.restype = C.c_long
+    lib.wfe_ensemble_variants.argtypes = [vp, ip]
     if path is None:
         _lib = lib
     return lib
@@ -304,3 +315,71 @@ class Case:
         g = self.ng
         nzl = self.nz + 1 if name == "w" else self.nz
         return a3[g:g + nzl, g:g + self.ny, g:g + self.nx]
+
+
+class Ensemble:
+    """Members (Case objects on one device, one precision, same physics
+    switches and substep count) advanced together by batched launches: each
+    kernel of the step runs once over a member x tile work list, and the step
+    is replayed from one CUDA graph per rotation phase.  Replaces the
+    reference's one-process-per-member loop (tools/run_ensemble.py:61-64).
+    The members stay usable (field(), rain(), dry_mass(), ...) and must stay
+    open while the ensemble is."""
+
+    def __init__(self, members: list):
+        self._lib = load_library()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m._h for m in self.members])
+        h = C.c_void_p()
+        rc = self._lib.wfe_ensemble_create(arr, len(self.members), C.byref(h))
+        if rc != 0:
+            raise WfeError(rc, self._lib.wfe_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise WfeError(rc, self._lib.wfe_last_error(None).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.wfe_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def cells(self) -> int:
+        return sum(m.nx * m.ny * m.nz for m in self.members)
+
+    def run(self, nsteps: int, dt: float, t0: float = 0.0) -> None:
+        self._check(self._lib.wfe_ensemble_run(self._h, nsteps, dt, t0))
+
+    def step(self, dt: float, t: float = 0.0) -> None:
+        self._check(self._lib.wfe_ensemble_step(self._h, dt, t))
+
+    def sync(self) -> None:
+        self._check(self._lib.wfe_ensemble_sync(self._h))
+
+    def time_run(self, nsteps: int, dt: float, t0: float = 0.0) -> float:
+        """device milliseconds of nsteps graph-replayed ensemble steps"""
+        ms = C.c_double()
+        self._check(self._lib.wfe_ensemble_time_run(self._h, nsteps, dt, t0, C.byref(ms)))
+        return float(ms.value)
+
+    def launches_per_step(self) -> int:
+        return int(self._lib.wfe_ensemble_launches_per_step(self._h))
+
+    def variants(self) -> dict:
+        out = (C.c_int * 3)()
+        self._check(self._lib.wfe_ensemble_variants(self._h, out))
+        return {"tendencies": out[0], "column_shape": out[1], "persistent": out[2]}

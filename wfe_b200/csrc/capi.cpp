@@ -440,3 +440,83 @@ int wfe_set_physics(wfe_ctx* c, const double* tsk, const double* land, const dou
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ ensembles
+struct wfe_ens {
+  std::unique_ptr<Ensemble> e;
+  std::vector<wfe_ctx*> members;
+};
+
+int wfe_ensemble_create(wfe_ctx* const* members, int n, wfe_ens** out) {
+  if (!out || !members || n < 1) return set_err(nullptr, WFE_ERR_ARG, "bad ensemble arguments");
+  *out = nullptr;
+  std::vector<Model*> ms;
+  for (int q = 0; q < n; ++q) {
+    if (!members[q] || !members[q]->model)
+      return set_err(nullptr, WFE_ERR_ARG, "ensemble member without a device model");
+    ms.push_back(members[q]->model.get());
+  }
+  std::string err;
+  Ensemble* e = Ensemble::create(ms, &err);
+  if (!e) return set_err(nullptr, WFE_ERR_ARG, err);
+  auto* h = new wfe_ens;
+  h->e.reset(e);
+  h->members.assign(members, members + n);
+  *out = h;
+  return WFE_OK;
+}
+
+int wfe_ensemble_destroy(wfe_ens* ens) {
+  delete ens;
+  return WFE_OK;
+}
+
+int wfe_ensemble_run(wfe_ens* ens, int nsteps, double dt, double t0) {
+  if (!ens || nsteps < 0) return set_err(nullptr, WFE_ERR_ARG, "bad ensemble arguments");
+  int done = 0;
+  while (done < nsteps) {
+    // replay up to the earliest boundary-file switch of any member, then switch
+    int chunk = nsteps - done;
+    const double t = t0 + done * dt;
+    for (wfe_ctx* c : ens->members) {
+      const CaseSetup& cs = c->cs;
+      if (!cs.bdy.on || c->bdy_idx_hi + 1 >= cs.input.n_bdy) continue;
+      if (boundary_update(c, t)) return set_err(nullptr, WFE_ERR_IO, c->err);
+      int until = (int)std::ceil((c->t_hi - t) / dt);
+      if (until < 1) until = 1;
+      if (until < chunk) chunk = until;
+    }
+    if (ens->e->run(chunk, dt, t)) return set_err(nullptr, WFE_ERR_CUDA, ens->e->error());
+    done += chunk;
+  }
+  return WFE_OK;
+}
+
+int wfe_ensemble_step(wfe_ens* ens, double dt, double t) {
+  if (!ens) return set_err(nullptr, WFE_ERR_ARG, "ensemble is NULL");
+  for (wfe_ctx* c : ens->members)
+    if (boundary_update(c, t)) return set_err(nullptr, WFE_ERR_IO, c->err);
+  if (ens->e->step(dt, t)) return set_err(nullptr, WFE_ERR_CUDA, ens->e->error());
+  return WFE_OK;
+}
+
+int wfe_ensemble_sync(wfe_ens* ens) {
+  if (!ens) return set_err(nullptr, WFE_ERR_ARG, "ensemble is NULL");
+  return ens->e->sync() ? set_err(nullptr, WFE_ERR_CUDA, ens->e->error()) : WFE_OK;
+}
+
+int wfe_ensemble_time_run(wfe_ens* ens, int nsteps, double dt, double t0, double* ms) {
+  if (!ens || !ms || nsteps < 1) return set_err(nullptr, WFE_ERR_ARG, "bad ensemble arguments");
+  return ens->e->time_run(nsteps, dt, t0, ms) ? set_err(nullptr, WFE_ERR_CUDA, ens->e->error())
+                                              : WFE_OK;
+}
+
+long wfe_ensemble_launches_per_step(const wfe_ens* ens) {
+  return ens ? ens->e->launches_per_step() : -1;
+}
+
+int wfe_ensemble_variants(const wfe_ens* ens, int out[3]) {
+  if (!ens || !out) return WFE_ERR_ARG;
+  ens->e->variants(&out[0], &out[1], &out[2]);
+  return WFE_OK;
+}

@@ -187,11 +187,11 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_acoustic_uv(AcouArgs<R> a) {
+__device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
   const Layout& L = a.L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
   if (i > L.nx || j > L.ny || k >= L.nz) return;
   const int kk = L.at1(k);
   const R cstar = a.p.cstar;
@@ -247,6 +247,15 @@ __global__ void __launch_bounds__(256) k_acoustic_uv(AcouArgs<R> a) {
   }
 }
 
+template <typename R>
+__global__ void __launch_bounds__(256) k_acoustic_uv(AcouArgs<R> a) {
+  uv_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_acoustic_uv_batch(Batch<AcouArgs<R>> b) {
+  for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int z) { uv_body(a, x, y, z); });
+}
+
 // ------------------------------------------------- implicit w - pi' columns
 // Shared-memory column arrays, level-major so that the CX lanes of a level
 // hit distinct banks: X(k, col) = base[k * CX + col].
@@ -261,15 +270,15 @@ struct ColSmem {
 };
 
 template <typename R, int CX, int KL>
-__global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
+__device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Layout& L = a.L;
   const int nz = L.nz;
   ColSmem<R, CX> S(reinterpret_cast<R*>(smem_raw), nz + 1);
   const int tx = threadIdx.x;           // column within the CTA
   const int lane_k = threadIdx.y;       // level lane
-  const int i = blockIdx.x * CX + tx;
-  const int j = blockIdx.y;
+  const int i = bx * CX + tx;
+  const int j = by;
   const bool active = i < L.nx;
   const R dtau = a.dtau, zt = a.m.zt;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
@@ -390,6 +399,17 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
 #undef SM
 }
 
+template <typename R, int CX, int KL>
+__global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
+  column_body<R, CX, KL>(a, blockIdx.x, blockIdx.y);
+}
+// the shared column arrays are reused by the next work item only after the
+// barrier that opens it
+template <typename R, int CX, int KL>
+__global__ void __launch_bounds__(CX * KL) k_acoustic_column_batch(Batch<AcouArgs<R>> b) {
+  for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int) { column_body<R, CX, KL>(a, x, y); });
+}
+
 // ------------------------------------------------------------ host launch
 template <typename R>
 void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,
@@ -401,10 +421,18 @@ void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& 
 }
 
 template <typename R>
+dim3 grid_uv(const Layout& L) {
+  return dim3((L.nx + 1 + 31) / 32, (L.ny + 1 + 3) / 4, (L.nz + 1) / 2);
+}
+
+template <typename R>
 void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 grd((a.L.nx + 1 + 31) / 32, (a.L.ny + 1 + 3) / 4, (a.L.nz + 1) / 2);
-  k_acoustic_uv<R><<<grd, blk, 0, st>>>(a);
+  k_acoustic_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a);
+}
+
+template <typename R>
+void batch_uv(const Batch<AcouArgs<R>>& b, int nblocks, cudaStream_t st) {
+  k_acoustic_uv_batch<R><<<nblocks, dim3(32, 4, 2), 0, st>>>(b);
 }
 
 template <typename R>
@@ -414,7 +442,10 @@ size_t column_smem(int nz, int cx) {
 
 template <typename R, int CX, int KL>
 static cudaError_t column_attr(size_t sm) {
-  return cudaFuncSetAttribute(k_acoustic_column<R, CX, KL>,
+  cudaError_t e = cudaFuncSetAttribute(k_acoustic_column<R, CX, KL>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_acoustic_column_batch<R, CX, KL>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
 }
 
@@ -427,6 +458,11 @@ int acoustic_column_shapes() { return kNumColumnShapes; }
 template <typename R>
 static bool column_fits(int nz, int shape) {
   return column_smem<R>(nz, kColumnShapes[shape][0]) <= 200 * 1024;
+}
+
+template <typename R>
+bool acoustic_column_fits(int nz, int shape) {
+  return shape >= 0 && shape < kNumColumnShapes && column_fits<R>(nz, shape);
 }
 
 // Sets the dynamic shared-memory limit of every tile shape that fits, once,
@@ -465,7 +501,7 @@ int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st) {
   }
   const int cx = kColumnShapes[shape][0], kl = kColumnShapes[shape][1];
   const size_t sm = column_smem<R>(nz, cx);
-  const dim3 grd((a.L.nx + cx - 1) / cx, a.L.ny), blk(cx, kl);
+  const dim3 grd = grid_column<R>(a.L, shape), blk(cx, kl);
   switch (shape) {
     case 0: k_acoustic_column<R, 32, 8><<<grd, blk, sm, st>>>(a); break;
     case 1: k_acoustic_column<R, 16, 16><<<grd, blk, sm, st>>>(a); break;
@@ -477,7 +513,56 @@ int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st) {
   return 0;
 }
 
+template <typename R>
+dim3 grid_column(const Layout& L, int shape) {
+  const int cx = kColumnShapes[shape][0];
+  return dim3((L.nx + cx - 1) / cx, L.ny, 1);
+}
+
+// Batched columns: the shared arrays are sized for the deepest member (nz_max)
+// and the tile shape must fit it (prepare_acoustic_column<R>(nz_max) done).
+template <typename R>
+int batch_column(const Batch<AcouArgs<R>>& b, int shape, int nz_max, int nblocks, cudaStream_t st) {
+  if (shape < 0 || shape >= kNumColumnShapes || !column_fits<R>(nz_max, shape)) return 2;
+  const int cx = kColumnShapes[shape][0], kl = kColumnShapes[shape][1];
+  const size_t sm = column_smem<R>(nz_max, cx);
+  const dim3 blk(cx, kl);
+  switch (shape) {
+    case 0: k_acoustic_column_batch<R, 32, 8><<<nblocks, blk, sm, st>>>(b); break;
+    case 1: k_acoustic_column_batch<R, 16, 16><<<nblocks, blk, sm, st>>>(b); break;
+    case 2: k_acoustic_column_batch<R, 8, 32><<<nblocks, blk, sm, st>>>(b); break;
+    case 3: k_acoustic_column_batch<R, 32, 4><<<nblocks, blk, sm, st>>>(b); break;
+    case 4: k_acoustic_column_batch<R, 16, 8><<<nblocks, blk, sm, st>>>(b); break;
+    default: k_acoustic_column_batch<R, 8, 16><<<nblocks, blk, sm, st>>>(b); break;
+  }
+  return 0;
+}
+
+template <typename R>
+int occupancy_column(int shape, int nz_max) {
+  if (shape < 0 || shape >= kNumColumnShapes || !column_fits<R>(nz_max, shape)) return 1;
+  const int cx = kColumnShapes[shape][0], kl = kColumnShapes[shape][1];
+  const size_t sm = column_smem<R>(nz_max, cx);
+  int n = 0;
+  cudaError_t e;
+  switch (shape) {
+    case 0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_acoustic_column_batch<R, 32, 8>, cx * kl, sm); break;
+    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_acoustic_column_batch<R, 16, 16>, cx * kl, sm); break;
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_acoustic_column_batch<R, 8, 32>, cx * kl, sm); break;
+    case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_acoustic_column_batch<R, 32, 4>, cx * kl, sm); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_acoustic_column_batch<R, 16, 8>, cx * kl, sm); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_acoustic_column_batch<R, 8, 16>, cx * kl, sm); break;
+  }
+  return e == cudaSuccess && n > 0 ? n : 1;
+}
+
 #define WFE_INST(R)                                                                            \
+  template dim3 grid_uv<R>(const Layout&);                                                     \
+  template dim3 grid_column<R>(const Layout&, int);                                            \
+  template void batch_uv<R>(const Batch<AcouArgs<R>>&, int, cudaStream_t);                     \
+  template int batch_column<R>(const Batch<AcouArgs<R>>&, int, int, int, cudaStream_t);        \
+  template int occupancy_column<R>(int, int);                                                  \
+  template bool acoustic_column_fits<R>(int, int);                                             \
   template void launch_acoustic_coef<R>(const Layout&, const DBase<R>&, const DMetric<R>&, R*, \
                                         R*, R*, R*, R*, cudaStream_t);                         \
   template void launch_acoustic_uv<R>(const AcouArgs<R>&, cudaStream_t);                       \

@@ -56,14 +56,16 @@ __device__ __forceinline__ R ghost_value(const Layout& L, const R* a, int kind, 
 }
 
 template <typename R>
-__global__ void k_fill_ghosts(Layout L, GhostJob<R> job, int open_x, int open_y) {
+__device__ __forceinline__ void fill_body(const FillArgs<R>& A, int bx, int by, int bz) {
   // one thread per padded column (i, j) of one field
-  const int f = blockIdx.z;
-  if (f >= job.n) return;
-  R* a = job.f[f];
-  const int kind = job.kind[f];
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - kRefNG;
-  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - kRefNG;
+  const Layout& L = A.L;
+  const int open_x = A.open_x, open_y = A.open_y;
+  const int f = bz;
+  if (f >= A.job.n) return;
+  R* a = A.job.f[f];
+  const int kind = A.job.kind[f];
+  const int i = (int)(bx * blockDim.x + threadIdx.x) - kRefNG;
+  const int j = (int)(by * blockDim.y + threadIdx.y) - kRefNG;
   if (i > L.nx + 2 || j > L.ny + 2) return;
   const int ilast = (kind == 1 && open_x) ? L.nx : L.nx - 1;
   const int jlast = (kind == 2 && open_y) ? L.ny : L.ny - 1;
@@ -96,17 +98,33 @@ __global__ void k_fill_ghosts(Layout L, GhostJob<R> job, int open_x, int open_y)
   for (int m = 0; m <= kRefNG; ++m) a[L.at(i, j, L.nz + m)] = hi[m];
 }
 
+template <typename R>
+__global__ void k_fill_ghosts(FillArgs<R> a) {
+  fill_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R>
+__global__ void k_fill_ghosts_batch(Batch<FillArgs<R>> b) {
+  for_each_work(b, [](const FillArgs<R>& a, int x, int y, int z) { fill_body(a, x, y, z); });
+}
+
 // ------------------------------------------------------------- mass fluxes
 // rho_b J weighted horizontal fluxes on the ring -2..n+2 and the
 // contravariant vertical flux on -2..n+1 (kernels.cu:68-97); w levels 0 and
 // nz carry Omega = 0.
 template <typename R>
-__global__ void k_mass_flux(Layout L, DBase<R> b, DMetric<R> m, const R* __restrict__ u,
-                            const R* __restrict__ v, const R* __restrict__ w, R* __restrict__ mfx,
-                            R* __restrict__ mfy, R* __restrict__ mfz) {
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 2;
-  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 2;
-  const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z);
+__device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, int bz) {
+  const Layout& L = A.L;
+  const DBase<R>& b = A.b;
+  const DMetric<R>& m = A.m;
+  const R* __restrict__ u = A.u;
+  const R* __restrict__ v = A.v;
+  const R* __restrict__ w = A.w;
+  R* __restrict__ mfx = A.mfx;
+  R* __restrict__ mfy = A.mfy;
+  R* __restrict__ mfz = A.mfz;
+  const int i = (int)(bx * blockDim.x + threadIdx.x) - 2;
+  const int j = (int)(by * blockDim.y + threadIdx.y) - 2;
+  const int k = (int)(bz * blockDim.z + threadIdx.z);
   if (i > L.nx + 2 || j > L.ny + 2 || k > L.nz) return;
   const size_t c = L.at(i, j, k);
   if (k < L.nz) {
@@ -126,6 +144,15 @@ __global__ void k_mass_flux(Layout L, DBase<R> b, DMetric<R> m, const R* __restr
   R vw = (R)0.25 * (v[L.at(i, j, k - 1)] + v[L.at(i, j + 1, k - 1)] + v[c] + v[L.at(i, j + 1, k)]);
   R cross = (uw * m.hx[L.at2(i, j)] + vw * m.hy[L.at2(i, j)]) * fac;
   mfz[c] = b.rhobw[c] * (w[c] - cross);
+}
+
+template <typename R>
+__global__ void k_mass_flux(FluxArgs<R> a) {
+  flux_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R>
+__global__ void k_mass_flux_batch(Batch<FluxArgs<R>> b) {
+  for_each_work(b, [](const FluxArgs<R>& a, int x, int y, int z) { flux_body(a, x, y, z); });
 }
 
 // divergence of the mass flux at cell (i,j,k) (kernels.cu:99-110), evaluated
@@ -188,12 +215,15 @@ __device__ __forceinline__ R qflux_z(const TendArgs<R>& a, const R* q, int i, in
 
 // Outflow ratio min(1, available / outgoing) per species (kernels.cu:221-238).
 template <typename R>
-__global__ void k_pd_ratio(TendArgs<R> a, R* __restrict__ rv, R* __restrict__ rc,
-                           R* __restrict__ rr) {
+__device__ __forceinline__ void pd_body(const PdArgs<R>& P, int bx, int by, int bz) {
+  const TendArgs<R>& a = P.t;
+  R* __restrict__ rv = P.rv;
+  R* __restrict__ rc = P.rc;
+  R* __restrict__ rr = P.rr;
   const Layout& L = a.L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
   const R dzc = a.m.dzeta_c[L.at1(k)];
   const R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
@@ -209,6 +239,15 @@ __global__ void k_pd_ratio(TendArgs<R> a, R* __restrict__ rv, R* __restrict__ rc
     R r = (a.dt * out > (R)1e-20) ? avail / (a.dt * out) : (R)1;
     outs[s][L.at(i, j, k)] = fmin((R)1, r);
   }
+}
+
+template <typename R>
+__global__ void k_pd_ratio(PdArgs<R> a) {
+  pd_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R>
+__global__ void k_pd_ratio_batch(Batch<PdArgs<R>> b) {
+  for_each_work(b, [](const PdArgs<R>& a, int x, int y, int z) { pd_body(a, x, y, z); });
 }
 
 // ratio at a possibly-ghost cell: lateral periodic / zero-gradient map
@@ -307,11 +346,11 @@ __device__ __forceinline__ void moist_species(const TendArgs<R>& a, const R* q, 
 enum { TEND_MOM = 1, TEND_SCAL = 2, TEND_ALL = 3 };
 
 template <typename R, int PART>
-__global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
+__device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, int bz) {
   const Layout& L = a.L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
   const int kk = L.at1(k);
   const size_t c = L.at(i, j, k);
@@ -415,21 +454,43 @@ __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
   }
 }
 
+template <typename R, int PART>
+__global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
+  tend_body<R, PART>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R, int PART>
+__global__ void __launch_bounds__(256) k_tendencies_batch(Batch<TendArgs<R>> b) {
+  for_each_work(b, [](const TendArgs<R>& a, int x, int y, int z) { tend_body<R, PART>(a, x, y, z); });
+}
+
 // ------------------------------------------------------- small utilities
-__global__ void k_clock(double* clk, double t, double t_lo, double t_hi, double dt, int advance) {
-  if (advance) {
+__device__ __forceinline__ void clock_body(const ClockArgs& a) {
+  if (threadIdx.x != 0) return;
+  double* clk = a.clk;
+  if (a.advance) {
     clk[CLK_T] += clk[CLK_DT];
   } else {
-    clk[CLK_T] = t;
-    clk[CLK_TLO] = t_lo;
-    clk[CLK_THI] = t_hi;
-    clk[CLK_DT] = dt;
+    clk[CLK_T] = a.t;
+    clk[CLK_TLO] = a.t_lo;
+    clk[CLK_THI] = a.t_hi;
+    clk[CLK_DT] = a.dt;
   }
+}
+
+__global__ void k_clock(ClockArgs a) { clock_body(a); }
+__global__ void k_clock_batch(Batch<ClockArgs> b) {
+  for_each_work(b, [](const ClockArgs& a, int, int, int) { clock_body(a); });
 }
 
 void launch_clock(double* clock, double t, double t_lo, double t_hi, double dt, int advance,
                   cudaStream_t st) {
-  k_clock<<<1, 1, 0, st>>>(clock, t, t_lo, t_hi, dt, advance);
+  k_clock<<<1, 32, 0, st>>>(ClockArgs{clock, t, t_lo, t_hi, dt, advance});
+}
+
+dim3 grid_clock() { return dim3(1, 1, 1); }
+
+void batch_clock(const Batch<ClockArgs>& b, int nblocks, cudaStream_t st) {
+  k_clock_batch<<<nblocks, 32, 0, st>>>(b);
 }
 
 // out = x + a * y over every stored point (src/dynamics/kernels.cu:268-273)
@@ -450,33 +511,59 @@ void launch_axpy(const R* x, const R* y, R a, R* out, size_t n, cudaStream_t st)
 
 // ------------------------------------------------------------ host launch
 template <typename R>
+dim3 grid_fill(const FillArgs<R>& a) {
+  return dim3((a.L.nx + 6 + 31) / 32, (a.L.ny + 6 + 3) / 4, a.job.n);
+}
+
+template <typename R>
 void launch_fill_ghosts(const Layout& L, const GhostJob<R>& job, int open_x, int open_y,
                         cudaStream_t st) {
   if (job.n == 0) return;
-  dim3 blk(32, 4);
-  dim3 grd((L.nx + 6 + 31) / 32, (L.ny + 6 + 3) / 4, job.n);
-  k_fill_ghosts<R><<<grd, blk, 0, st>>>(L, job, open_x, open_y);
+  FillArgs<R> a{L, job, open_x, open_y};
+  k_fill_ghosts<R><<<grid_fill(a), dim3(32, 4), 0, st>>>(a);
+}
+
+template <typename R>
+void batch_fill(const Batch<FillArgs<R>>& b, int nblocks, cudaStream_t st) {
+  k_fill_ghosts_batch<R><<<nblocks, dim3(32, 4), 0, st>>>(b);
+}
+
+template <typename R>
+dim3 grid_flux(const FluxArgs<R>& a) {
+  return dim3((a.L.nx + 5 + 31) / 32, (a.L.ny + 5 + 3) / 4, (a.L.nz + 1 + 1) / 2);
 }
 
 template <typename R>
 void launch_mass_flux(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* u,
                       const R* v, const R* w, R* mfx, R* mfy, R* mfz, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 grd((L.nx + 5 + 31) / 32, (L.ny + 5 + 3) / 4, (L.nz + 1 + 1) / 2);
-  k_mass_flux<R><<<grd, blk, 0, st>>>(L, b, m, u, v, w, mfx, mfy, mfz);
+  FluxArgs<R> a{L, b, m, u, v, w, mfx, mfy, mfz};
+  k_mass_flux<R><<<grid_flux(a), dim3(32, 4, 2), 0, st>>>(a);
+}
+
+template <typename R>
+void batch_flux(const Batch<FluxArgs<R>>& b, int nblocks, cudaStream_t st) {
+  k_mass_flux_batch<R><<<nblocks, dim3(32, 4, 2), 0, st>>>(b);
+}
+
+template <typename R>
+dim3 grid_cells(const Layout& L) {
+  return dim3((L.nx + 31) / 32, (L.ny + 3) / 4, (L.nz + 1) / 2);
 }
 
 template <typename R>
 void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 grd((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
-  k_pd_ratio<R><<<grd, blk, 0, st>>>(a, rv, rc, rr);
+  k_pd_ratio<R><<<grid_cells<R>(a.L), dim3(32, 4, 2), 0, st>>>(PdArgs<R>{a, rv, rc, rr});
+}
+
+template <typename R>
+void batch_pd(const Batch<PdArgs<R>>& b, int nblocks, cudaStream_t st) {
+  k_pd_ratio_batch<R><<<nblocks, dim3(32, 4, 2), 0, st>>>(b);
 }
 
 template <typename R>
 void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
   dim3 blk(32, 4, 2);
-  dim3 grd((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
+  dim3 grd = grid_cells<R>(a.L);
   if (variant == 1) {
     k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);
     k_tendencies<R, TEND_SCAL><<<grd, blk, 0, st>>>(a);
@@ -485,13 +572,46 @@ void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
   }
 }
 
+// variant 1 runs two subs (momentum, scalars); variant 0 one fused sub
+template <typename R>
+void batch_tend(const Batch<TendArgs<R>>& b, int variant, int sub, int nblocks, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  if (variant == 1) {
+    if (sub == 0) k_tendencies_batch<R, TEND_MOM><<<nblocks, blk, 0, st>>>(b);
+    else k_tendencies_batch<R, TEND_SCAL><<<nblocks, blk, 0, st>>>(b);
+  } else {
+    k_tendencies_batch<R, TEND_ALL><<<nblocks, blk, 0, st>>>(b);
+  }
+}
+
+template <typename R>
+int occupancy_tend(int variant, int sub) {
+  int n = 0;
+  cudaError_t e;
+  if (variant == 1 && sub == 0)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tendencies_batch<R, TEND_MOM>, 256, 0);
+  else if (variant == 1)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tendencies_batch<R, TEND_SCAL>, 256, 0);
+  else
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tendencies_batch<R, TEND_ALL>, 256, 0);
+  return e == cudaSuccess && n > 0 ? n : 1;
+}
+
 #define WFE_INST(R)                                                                               \
   template void launch_fill_ghosts<R>(const Layout&, const GhostJob<R>&, int, int, cudaStream_t); \
   template void launch_mass_flux<R>(const Layout&, const DBase<R>&, const DMetric<R>&, const R*,  \
                                     const R*, const R*, R*, R*, R*, cudaStream_t);                \
   template void launch_pd_ratio<R>(const TendArgs<R>&, R*, R*, R*, cudaStream_t);                 \
   template void launch_tendencies<R>(const TendArgs<R>&, int, cudaStream_t);                         \
-  template void launch_axpy<R>(const R*, const R*, R, R*, size_t, cudaStream_t);
+  template void launch_axpy<R>(const R*, const R*, R, R*, size_t, cudaStream_t);              \
+  template dim3 grid_fill<R>(const FillArgs<R>&);                                              \
+  template dim3 grid_flux<R>(const FluxArgs<R>&);                                              \
+  template dim3 grid_cells<R>(const Layout&);                                                   \
+  template void batch_fill<R>(const Batch<FillArgs<R>>&, int, cudaStream_t);                   \
+  template void batch_flux<R>(const Batch<FluxArgs<R>>&, int, cudaStream_t);                   \
+  template void batch_pd<R>(const Batch<PdArgs<R>>&, int, cudaStream_t);                       \
+  template void batch_tend<R>(const Batch<TendArgs<R>>&, int, int, int, cudaStream_t);         \
+  template int occupancy_tend<R>(int, int);
 WFE_INST(float)
 WFE_INST(double)
 #undef WFE_INST

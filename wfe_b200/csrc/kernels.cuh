@@ -90,6 +90,125 @@ struct SfcArgs {
   R* scratch;  // sfc_scratch_count(L) elements of column work arrays
 };
 
+// Argument blocks of the kernels whose single launches take loose arguments.
+template <typename R>
+struct FillArgs {
+  Layout L;
+  GhostJob<R> job;
+  int open_x, open_y;
+};
+template <typename R>
+struct FluxArgs {
+  Layout L;
+  DBase<R> b;
+  DMetric<R> m;
+  const R *u, *v, *w;
+  R *mfx, *mfy, *mfz;
+};
+template <typename R>
+struct PdArgs {
+  TendArgs<R> t;
+  R *rv, *rc, *rr;
+};
+struct ClockArgs {
+  double* clk;
+  double t, t_lo, t_hi, dt;
+  int advance;
+};
+
+// ------------------------------------------------------------------ batches
+// A batched launch runs one kernel over the blocks of several members (cases
+// of possibly different sizes advancing together): work[w] = (member, bx, by,
+// bz) names block w's member and its block coordinates in that member's own
+// grid.  Blocks walk the list with stride gridDim.x (a persistent grid when
+// the launch has fewer blocks than items).
+template <typename A>
+struct Batch {
+  const A* args;     // device array, one argument block per member
+  const int4* work;  // device work list
+  int nwork;
+};
+
+// Walks a batch's work list: for item w the block stages member work[w].x's
+// argument block in shared memory and runs body(args, bx, by, bz) with the
+// item's block coordinates.
+template <typename A, typename F>
+__device__ __forceinline__ void for_each_work(const Batch<A>& b, F&& body) {
+  static_assert(sizeof(A) % 4 == 0, "argument blocks are staged as 32-bit words");
+  __shared__ __align__(16) int raw[sizeof(A) / 4];
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nth = blockDim.x * blockDim.y * blockDim.z;
+  for (int w = blockIdx.x; w < b.nwork; w += gridDim.x) {
+    const int4 it = b.work[w];
+    __syncthreads();  // every thread is done with the previous item's arguments
+    const int* src = reinterpret_cast<const int*>(b.args + it.x);
+    for (int q = tid; q < (int)(sizeof(A) / 4); q += nth) raw[q] = src[q];
+    __syncthreads();
+    body(*reinterpret_cast<const A*>(raw), it.y, it.z, it.w);
+  }
+}
+
+// Kernel kinds of one RK3 step as recorded for batched replay.  variant is the
+// tuned launch variant (tendencies: 0 fused / 1 split; acoustic column: tile
+// shape); one kind may launch several kernels ("subs") over separate grids.
+enum Kind { K_FILL = 0, K_FLUX, K_PD, K_TEND, K_UV, K_COL, K_KES, K_SFC, K_CLOCK, K_NKIND };
+
+template <typename R>
+size_t kind_args_size(int kind);
+template <typename R>
+int kind_subs(int kind, int variant);
+// grid of sub-launch `sub` of one member (args: that member's argument block)
+template <typename R>
+dim3 kind_grid(int kind, int variant, int sub, const void* args, int nz_max);
+// resident blocks per SM of the batched kernel of sub-launch `sub`
+template <typename R>
+int kind_occupancy(int kind, int variant, int sub, int nz_max);
+// one batched launch of sub-launch `sub`; d_args holds one argument block of
+// the kind per member; nz_max sizes the shared memory of the column kernels
+template <typename R>
+int launch_kind_batch(int kind, int variant, int sub, const void* d_args, const int4* d_work,
+                      int nwork, int nblocks, int nz_max, cudaStream_t st);
+
+// Per-file batched launchers and grids behind the dispatch above.
+template <typename R>
+dim3 grid_fill(const FillArgs<R>& a);
+template <typename R>
+dim3 grid_flux(const FluxArgs<R>& a);
+template <typename R>
+dim3 grid_cells(const Layout& L);  // pd ratio and tendencies
+dim3 grid_clock();
+template <typename R>
+void batch_fill(const Batch<FillArgs<R>>& b, int nblocks, cudaStream_t st);
+template <typename R>
+void batch_flux(const Batch<FluxArgs<R>>& b, int nblocks, cudaStream_t st);
+template <typename R>
+void batch_pd(const Batch<PdArgs<R>>& b, int nblocks, cudaStream_t st);
+template <typename R>
+void batch_tend(const Batch<TendArgs<R>>& b, int variant, int sub, int nblocks, cudaStream_t st);
+void batch_clock(const Batch<ClockArgs>& b, int nblocks, cudaStream_t st);
+template <typename R>
+int occupancy_tend(int variant, int sub);
+template <typename R>
+dim3 grid_uv(const Layout& L);
+template <typename R>
+dim3 grid_column(const Layout& L, int shape);
+template <typename R>
+void batch_uv(const Batch<AcouArgs<R>>& b, int nblocks, cudaStream_t st);
+template <typename R>
+int batch_column(const Batch<AcouArgs<R>>& b, int shape, int nz_max, int nblocks, cudaStream_t st);
+template <typename R>
+int occupancy_column(int shape, int nz_max);
+template <typename R>
+dim3 grid_kessler(const Layout& L, int nz_max);
+template <typename R>
+int batch_kessler(const Batch<KesArgs<R>>& b, int nz_max, int nblocks, cudaStream_t st);
+template <typename R>
+int occupancy_kessler(int nz_max);
+template <typename R>
+dim3 grid_sfc(const Layout& L, int sub);
+template <typename R>
+void batch_sfc(const Batch<SfcArgs<R>>& b, int sub, int nblocks, cudaStream_t st);
+
 template <typename R>
 int launch_sfc(const SfcArgs<R>& a, cudaStream_t st);
 template <typename R>
@@ -121,6 +240,9 @@ void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st);
 template <typename R>
 int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st);
 int acoustic_column_shapes();
+// whether tile shape `shape` holds a column of nz levels in shared memory
+template <typename R>
+bool acoustic_column_fits(int nz, int shape);
 template <typename R>
 int prepare_acoustic_column(int nz);
 template <typename R>

@@ -35,7 +35,14 @@ namespace wfe {
 struct Tune {
   int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches
   int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
+  int persist = 0;       // batched launches: 0 one block per work item, 1 persistent grid
   bool done = false;
+};
+
+// One launch of a step recorded for batched replay: its kind and argument block.
+struct Rec {
+  int kind;
+  std::vector<unsigned char> args;
 };
 
 namespace {
@@ -63,6 +70,7 @@ bool tune_lookup(const std::string& key, Tune* t) {
     std::string k;
     Tune v;
     if (ss >> k >> v.tend_variant >> v.column_cx && k == key) {
+      if (!(ss >> v.persist)) v.persist = 0;
       v.done = true;
       g_tune_cache[key] = v;
       *t = v;
@@ -77,7 +85,7 @@ void tune_store(const std::string& key, const Tune& t) {
   g_tune_cache[key] = t;
   // best effort: the cache file is an optimisation only (its directory must exist)
   std::ofstream f(tune_cache_path(), std::ios::app);
-  if (f) f << key << " " << t.tend_variant << " " << t.column_cx << "\n";
+  if (f) f << key << " " << t.tend_variant << " " << t.column_cx << " " << t.persist << "\n";
 }
 }  // namespace
 
@@ -454,6 +462,7 @@ class ModelT final : public Model {
     t_hi_ = t_hi;
     bdy_on_ = true;
     graphs_valid_ = false;
+    ++gen_;
     launch_clock(clock_, 0, t_lo, t_hi, 0, 0, st_);
     return sync();
   }
@@ -469,6 +478,7 @@ class ModelT final : public Model {
     t_lo_ = t_lo;
     t_hi_ = t_hi;
     graphs_valid_ = false;
+    ++gen_;
     return 0;
   }
 
@@ -498,6 +508,7 @@ class ModelT final : public Model {
     sf_.nonlocal = nonlocal;
     sfc_on_ = true;
     graphs_valid_ = false;
+    ++gen_;
     return sync();
   }
 
@@ -539,6 +550,40 @@ class ModelT final : public Model {
     launch_clock(clock_, t - dt, t_lo_, t_hi_, dt, 0, st_);
     if (surface(S_[perm_[0]], (R)dt)) return 1;
     return sync();
+  }
+
+  // ----------------------------------------------------- batched ensembles
+  // The launches of one step from the current rotation phase, recorded
+  // instead of issued; the rotation is left unchanged.
+  int record_step(double dt, std::vector<Rec>* out) {
+    const int saved[3] = {perm_[0], perm_[1], perm_[2]};
+    const int ph = phase_;
+    const long l = launches_;
+    rec_ = out;
+    int rc = enqueue_step((R)dt);
+    rec_ = nullptr;
+    launches_ = l;
+    perm_[0] = saved[0];
+    perm_[1] = saved[1];
+    perm_[2] = saved[2];
+    phase_ = ph;
+    return rc;
+  }
+  void rotate() { advance_rotation(); }
+  int phase() const { return phase_; }
+  long generation() const { return gen_; }
+  double* clock_ptr() const { return clock_; }
+  double bdy_t_lo() const { return t_lo_; }
+  double bdy_t_hi() const { return t_hi_; }
+  cudaStream_t stream() const { return st_; }
+  int device() const { return dev_; }
+  const Layout& layout() const { return L_; }
+  // members whose signatures match record the same launch sequence
+  std::string batch_signature() const {
+    std::ostringstream k;
+    k << "m" << dp_.moisture << "mp" << dp_.microphysics << "pd" << dp_.pd_moist << "b" << bdy_on_
+      << "s" << sfc_on_ << "ns" << hp_.acoustic_ns;
+    return k.str();
   }
 
  private:
@@ -629,6 +674,20 @@ class ModelT final : public Model {
     std::string name;
     cudaEvent_t e0, e1;
   };
+  // Record mode (batched ensembles): a launch site appends its kind and
+  // argument block to rec_ instead of launching.
+  template <class A>
+  bool record(int kind, const A& a) {
+    if (!rec_) return false;
+    Rec r;
+    r.kind = kind;
+    r.args.resize(sizeof(A));
+    std::memcpy(r.args.data(), &a, sizeof(A));
+    rec_->push_back(std::move(r));
+    ++launches_;
+    return true;
+  }
+
   // wraps one launch: counted always, bracketed by events when profiling
   template <class F>
   void launch(const char* name, F&& f) {
@@ -700,10 +759,12 @@ class ModelT final : public Model {
   // slow tendencies of est; moisture either into T_ (op) or into X as the
   // stage value N.q + dt_stage * tq
   void tendencies(R** est, R** N, R** X, R dt, R dt_stage, bool op) {
-    launch("mass_flux", [&] { launch_mass_flux<R>(L_, db_, dm_, est[0], est[1], est[2], mfx_, mfy_, mfz_, st_); });
+    if (!record(K_FLUX, FluxArgs<R>{L_, db_, dm_, est[0], est[1], est[2], mfx_, mfy_, mfz_}))
+      launch("mass_flux", [&] { launch_mass_flux<R>(L_, db_, dm_, est[0], est[1], est[2], mfx_, mfy_, mfz_, st_); });
     TendArgs<R> a = tend_args(est, dt);
     if (dp_.moisture && dp_.pd_moist) {
-      launch("pd_ratio", [&] { launch_pd_ratio<R>(a, ratio_[0], ratio_[1], ratio_[2], st_); });
+      if (!record(K_PD, PdArgs<R>{a, ratio_[0], ratio_[1], ratio_[2]}))
+        launch("pd_ratio", [&] { launch_pd_ratio<R>(a, ratio_[0], ratio_[1], ratio_[2], st_); });
       a.ratio_v = ratio_[0];
       a.ratio_c = ratio_[1];
       a.ratio_r = ratio_[2];
@@ -725,7 +786,8 @@ class ModelT final : public Model {
       a.qo_r = X[7];
       a.dt_stage = dt_stage;
     }
-    launch("tendencies", [&] { launch_tendencies<R>(a, tune_.tend_variant, st_); });
+    if (!record(K_TEND, a))
+      launch("tendencies", [&] { launch_tendencies<R>(a, tune_.tend_variant, st_); });
   }
 
   // ns acoustic substeps from time n (N) into the stage output X
@@ -770,9 +832,10 @@ class ModelT final : public Model {
       a.pi_prev = pbuf(t - 1);
       a.pi_cur = pbuf(t);
       a.pi_next = pbuf(t + 1);
-      launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
       int rc = 0;
-      launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, tune_.column_cx, st_); });
+      if (!record(K_UV, a)) launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
+      if (!record(K_COL, a))
+        launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, tune_.column_cx, st_); });
       if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
       uin = uout;
       vin = vout;
@@ -784,7 +847,7 @@ class ModelT final : public Model {
   int kessler(R** s, R dt) {
     KesArgs<R> k{L_, db_, dm_, dt, s[3], s[5], s[6], s[7], rain_, s[4]};
     int rc = 0;
-    launch("kessler", [&] { rc = launch_kessler<R>(k, st_); });
+    if (!record(K_KES, k)) launch("kessler", [&] { rc = launch_kessler<R>(k, st_); });
     if (rc) return fail("Kessler launch");
     return 0;
   }
@@ -819,6 +882,10 @@ class ModelT final : public Model {
     a.soilw = sf_.soilw;
     a.scratch = sf_.scratch;
     int rc = 0;
+    if (record(K_SFC, a)) {
+      ++launches_;  // two kernels
+      return 0;
+    }
     launch("surface", [&] { rc = launch_sfc<R>(a, st_); });
     ++launches_;
     if (rc) return fail("surface physics launch");
@@ -836,7 +903,8 @@ class ModelT final : public Model {
       R** est = m == 0 ? N : S_[m == 1 ? pA : pB];
       R** X = S_[m == 1 ? pB : pA];
       GhostJob<R> job = ghost_job(est, false);
-      launch("fill_ghosts", [&] { launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_); });
+      if (!record(K_FILL, FillArgs<R>{L_, job, dp_.bc_x_open, dp_.bc_y_open}))
+        launch("fill_ghosts", [&] { launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_); });
       tendencies(est, N, X, dt, stage_dt[m], false);
       if (acoustic(N, X, stage_dt[m] / (R)nss[m], nss[m], false)) return 1;
     }
@@ -982,12 +1050,425 @@ class ModelT final : public Model {
   int phase_ = 0;
   cudaGraphExec_t gexec_[3] = {nullptr, nullptr, nullptr};
   bool graphs_valid_ = false;
+  long gen_ = 0;  // changes whenever buffer roles or physics switches change
+  std::vector<Rec>* rec_ = nullptr;  // record mode when set
   double graph_dt_ = 0;
   long launches_ = 0, glaunches_ = 0;
   bool profiling_ = false;
   std::vector<ProfRec> prof_;
   Tune tune_;
 };
+
+// --------------------------------------------------------------- ensembles
+template <typename R>
+class EnsembleT final : public Ensemble {
+ public:
+  ~EnsembleT() override { release(); }
+
+  int init(const std::vector<ModelT<R>*>& m) {
+    mem_ = m;
+    if (mem_.empty()) return fail("an ensemble needs at least one member");
+    dev_ = mem_[0]->device();
+    const std::string sig = mem_[0]->batch_signature();
+    for (auto* x : mem_) {
+      if (x->device() != dev_) return fail("ensemble members must share one device");
+      if (x->batch_signature() != sig)
+        return fail("ensemble members must share moisture, microphysics, positive-definite "
+                    "moisture, boundary, surface-physics and substep settings");
+      if (x->phase() != mem_[0]->phase())
+        return fail("ensemble members must be at the same step phase");
+      nz_max_ = std::max(nz_max_, x->layout().nz);
+    }
+    CK(cudaSetDevice(dev_));
+    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_));
+    sms_ = sms;
+    if (prepare_acoustic_column<R>(nz_max_) || prepare_kessler<R>(nz_max_))
+      return fail("nz too large for the column kernels' shared memory");
+    gens_.assign(mem_.size(), -1);
+    return 0;
+  }
+
+  int run(int nsteps, double dt, double t0) override {
+    CK(cudaSetDevice(dev_));
+    if (begin(dt)) return 1;
+    for (auto* x : mem_) launch_clock(x->clock_ptr(), t0, x->bdy_t_lo(), x->bdy_t_hi(), dt, 0, st_);
+    for (int s = 0; s < nsteps; ++s) {
+      Phase& P = ph_[mem_[0]->phase()];
+      if (!P.ge) {
+        if (build(P, dt)) return 1;
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        int rc = issue(P, (int)P.pos.size());
+        cudaError_t ce = cudaStreamEndCapture(st_, &gr);
+        if (rc) return 1;
+        if (ce != cudaSuccess) return fail(std::string("graph capture: ") + cudaGetErrorString(ce));
+        CK(cudaGraphInstantiate(&P.ge, gr, 0));
+        cudaGraphDestroy(gr);
+      }
+      CK(cudaGraphLaunch(P.ge, st_));
+      for (auto* x : mem_) x->rotate();
+    }
+    return finish();
+  }
+
+  int step(double dt, double t) override {
+    CK(cudaSetDevice(dev_));
+    if (begin(dt)) return 1;
+    for (auto* x : mem_) launch_clock(x->clock_ptr(), t, x->bdy_t_lo(), x->bdy_t_hi(), dt, 0, st_);
+    Phase& P = ph_[mem_[0]->phase()];
+    if (!P.built && build(P, dt)) return 1;
+    if (issue(P, (int)P.pos.size())) return 1;
+    for (auto* x : mem_) x->rotate();
+    if (finish()) return 1;
+    return sync();
+  }
+
+  int sync() override {
+    CK(cudaStreamSynchronize(st_));
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  int time_run(int nsteps, double dt, double t0, double* ms) override {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    if (begin(dt)) return 1;  // tuning and member ordering outside the timed region
+    CK(cudaEventRecord(e0, st_));
+    int rc = run(nsteps, dt, t0);
+    CK(cudaEventRecord(e1, st_));
+    CK(cudaEventSynchronize(e1));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = f;
+    return rc;
+  }
+
+  long launches_per_step() const override { return launches_; }
+  void variants(int* tend, int* column, int* persist) const override {
+    *tend = tune_.tend_variant;
+    *column = tune_.column_cx;
+    *persist = tune_.persist;
+  }
+
+ private:
+  struct Work {
+    int4* d = nullptr;
+    int n = 0;
+  };
+  struct Pos {
+    int kind;
+    size_t off;                // member argument blocks at arena + off
+    std::vector<Work*> subs;   // work list of each sub-launch
+  };
+  struct Phase {
+    std::vector<Pos> pos;
+    unsigned char* d_args = nullptr;
+    size_t cap = 0;
+    cudaGraphExec_t ge = nullptr;
+    bool built = false;
+  };
+
+  int variant_of(int kind) const {
+    return kind == K_TEND ? tune_.tend_variant : (kind == K_COL ? tune_.column_cx : 0);
+  }
+
+  // Orders the ensemble stream after the members' streams, tunes once and
+  // drops phases whose members changed buffers or whose dt changed.
+  int begin(double dt) {
+    for (auto* x : mem_) {
+      CK(cudaEventRecord(ev_, x->stream()));
+      CK(cudaStreamWaitEvent(st_, ev_, 0));
+    }
+    bool stale = dt != dt_;
+    for (size_t m = 0; m < mem_.size(); ++m)
+      if (gens_[m] != mem_[m]->generation()) stale = true;
+    if (stale) {
+      for (auto& P : ph_) drop(P);
+      for (size_t m = 0; m < mem_.size(); ++m) gens_[m] = mem_[m]->generation();
+      dt_ = dt;
+    }
+    return autotune(dt);
+  }
+
+  // Orders the members' streams after the ensemble's work.
+  int finish() {
+    CK(cudaEventRecord(ev_, st_));
+    for (auto* x : mem_) CK(cudaStreamWaitEvent(x->stream(), ev_, 0));
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  void drop(Phase& P) {
+    if (P.ge) cudaGraphExecDestroy(P.ge);
+    P.ge = nullptr;
+    P.built = false;
+    P.pos.clear();
+  }
+
+  // Records every member's step from the current phase, checks that the
+  // launch sequences agree, uploads the argument blocks and builds the work
+  // lists for the current variants.
+  int build(Phase& P, double dt) {
+    const size_t M = mem_.size();
+    std::vector<std::vector<Rec>> recs(M);
+    for (size_t m = 0; m < M; ++m) {
+      if (mem_[m]->record_step(dt, &recs[m])) return fail(mem_[m]->error());
+      Rec c;
+      c.kind = K_CLOCK;
+      ClockArgs ca{mem_[m]->clock_ptr(), 0, 0, 0, 0, 1};
+      c.args.resize(sizeof(ca));
+      std::memcpy(c.args.data(), &ca, sizeof(ca));
+      recs[m].push_back(std::move(c));
+    }
+    const size_t n = recs[0].size();
+    for (size_t m = 1; m < M; ++m) {
+      if (recs[m].size() != n) return fail("ensemble members record different steps");
+      for (size_t p = 0; p < n; ++p)
+        if (recs[m][p].kind != recs[0][p].kind) return fail("ensemble members record different steps");
+    }
+    P.pos.clear();
+    size_t total = 0;
+    for (size_t p = 0; p < n; ++p) {
+      const size_t sz = kind_args_size<R>(recs[0][p].kind);
+      P.pos.push_back(Pos{recs[0][p].kind, total, {}});
+      total += (M * sz + 255) / 256 * 256;
+    }
+    std::vector<unsigned char> host(total);
+    for (size_t p = 0; p < n; ++p) {
+      const size_t sz = kind_args_size<R>(P.pos[p].kind);
+      for (size_t m = 0; m < M; ++m) {
+        if (recs[m][p].args.size() != sz) return fail("argument block size mismatch");
+        std::memcpy(host.data() + P.pos[p].off + m * sz, recs[m][p].args.data(), sz);
+      }
+      const int kind = P.pos[p].kind, var = variant_of(kind);
+      for (int sub = 0; sub < kind_subs<R>(kind, var); ++sub) {
+        std::vector<const void*> args(M);
+        for (size_t m = 0; m < M; ++m) args[m] = recs[m][p].args.data();
+        Work* w = work_for(kind, var, sub, args);
+        if (!w) return 1;
+        P.pos[p].subs.push_back(w);
+      }
+    }
+    if (P.cap < total) {
+      if (P.d_args) cudaFree(P.d_args);
+      P.d_args = nullptr;
+      P.cap = 0;
+      CK(cudaMalloc(&P.d_args, total));
+      P.cap = total;
+    }
+    CK(cudaMemcpyAsync(P.d_args, host.data(), total, cudaMemcpyHostToDevice, st_));
+    CK(cudaStreamSynchronize(st_));
+    long l = 0;
+    for (auto& q : P.pos) l += (long)q.subs.size();
+    launches_ = l;
+    P.built = true;
+    return 0;
+  }
+
+  // work list of one sub-launch over all members, shared by every position
+  // with the same kind, variant and member grids
+  Work* work_for(int kind, int var, int sub, const std::vector<const void*>& args) {
+    std::ostringstream key;
+    key << kind << "/" << var << "/" << sub;
+    std::vector<dim3> grids(args.size());
+    for (size_t m = 0; m < args.size(); ++m) {
+      grids[m] = kind_grid<R>(kind, var, sub, args[m], nz_max_);
+      key << "|" << grids[m].x << "x" << grids[m].y << "x" << grids[m].z;
+    }
+    auto it = work_.find(key.str());
+    if (it != work_.end()) return &it->second;
+    std::vector<int4> items;
+    for (size_t m = 0; m < args.size(); ++m)
+      for (unsigned z = 0; z < grids[m].z; ++z)
+        for (unsigned y = 0; y < grids[m].y; ++y)
+          for (unsigned x = 0; x < grids[m].x; ++x)
+            items.push_back(make_int4((int)m, (int)x, (int)y, (int)z));
+    Work w;
+    w.n = (int)items.size();
+    if (w.n > 0) {
+      cudaError_t e = cudaMalloc(&w.d, items.size() * sizeof(int4));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(w.d, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        fail(std::string("work list: ") + cudaGetErrorString(e));
+        return nullptr;
+      }
+    }
+    return &(work_[key.str()] = w);
+  }
+
+  // issues the first npos positions of a built phase on st_
+  int issue(const Phase& P, int npos) {
+    for (int p = 0; p < npos; ++p) {
+      const Pos& q = P.pos[p];
+      const int var = variant_of(q.kind);
+      for (int sub = 0; sub < (int)q.subs.size(); ++sub) {
+        const Work* w = q.subs[sub];
+        int nblocks = w->n;
+        if (tune_.persist) {
+          int occ = kind_occupancy<R>(q.kind, var, sub, nz_max_);
+          nblocks = std::min(w->n, occ * sms_);
+        }
+        if (launch_kind_batch<R>(q.kind, var, sub, P.d_args + q.off, w->d, w->n, nblocks, nz_max_,
+                                 st_))
+          return fail("batched launch: tile shape does not fit the deepest member");
+      }
+    }
+    CK(cudaGetLastError());
+    return 0;
+  }
+
+  std::string tune_key() const {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, dev_);
+    std::ostringstream k;
+    std::string name = prop.name;
+    for (char& ch : name)
+      if (ch == ' ') ch = '_';
+    k << "ens1|" << name << "|" << (sizeof(R) * 8) << "|" << mem_[0]->batch_signature();
+    for (auto* x : mem_) k << "|" << x->layout().nx << "x" << x->layout().ny << "x" << x->layout().nz;
+    return k.str();
+  }
+
+  // Times the variants on the first stage's launches up to its acoustic
+  // column (they read time n and write only scratch, tendencies and the
+  // stage output, which the step overwrites).  WFE_TUNE=0 keeps defaults.
+  int autotune(double dt) {
+    if (tune_.done) return 0;
+    tune_.done = true;
+    const char* env = std::getenv("WFE_TUNE");
+    if (env && env[0] == '0') return 0;
+    const std::string key = tune_key();
+    Tune cached;
+    if (tune_lookup(key, &cached)) {
+      tune_ = cached;
+      return 0;
+    }
+    int upto = -1;
+    auto stage0 = [&](float* ms) -> int {
+      Phase T;
+      if (build(T, dt)) return 1;
+      if (upto < 0)
+        for (int p = 0; p < (int)T.pos.size() && upto < 0; ++p)
+          if (T.pos[p].kind == K_COL) upto = p + 1;
+      cudaEvent_t e0, e1;
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      *ms = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        CK(cudaEventRecord(e0, st_));
+        if (issue(T, upto)) return 1;
+        CK(cudaEventRecord(e1, st_));
+        CK(cudaEventSynchronize(e1));
+        float f = 0;
+        CK(cudaEventElapsedTime(&f, e0, e1));
+        *ms = std::min(*ms, f);
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (T.d_args) cudaFree(T.d_args);
+      return 0;
+    };
+    Tune best = tune_;
+    float bt = 1e30f, ms;
+    for (int v = 0; v < 2; ++v) {
+      tune_.tend_variant = v;
+      if (stage0(&ms)) return 1;
+      if (ms < bt) bt = ms, best.tend_variant = v;
+    }
+    tune_.tend_variant = best.tend_variant;
+    bt = 1e30f;
+    for (int c = 0; c < acoustic_column_shapes(); ++c) {
+      if (!acoustic_column_fits<R>(nz_max_, c)) continue;
+      tune_.column_cx = c;
+      if (stage0(&ms)) return 1;
+      if (ms < bt) bt = ms, best.column_cx = c;
+    }
+    tune_.column_cx = best.column_cx;
+    bt = 1e30f;
+    for (int pz = 0; pz < 2; ++pz) {
+      tune_.persist = pz;
+      if (stage0(&ms)) return 1;
+      if (ms < bt) bt = ms, best.persist = pz;
+    }
+    CK(cudaStreamSynchronize(st_));
+    best.done = true;
+    tune_ = best;
+    tune_store(key, tune_);
+    return 0;
+  }
+
+  int fail(const std::string& m) {
+    err_ = m;
+    return 1;
+  }
+
+  void release() {
+    for (auto& P : ph_) {
+      drop(P);
+      if (P.d_args) cudaFree(P.d_args);
+      P.d_args = nullptr;
+    }
+    for (auto& kv : work_)
+      if (kv.second.d) cudaFree(kv.second.d);
+    work_.clear();
+    if (ev_) cudaEventDestroy(ev_);
+    if (st_) cudaStreamDestroy(st_);
+    ev_ = nullptr;
+    st_ = nullptr;
+  }
+
+  std::vector<ModelT<R>*> mem_;
+  std::vector<long> gens_;
+  int dev_ = 0, sms_ = 148, nz_max_ = 0;
+  cudaStream_t st_ = nullptr;
+  cudaEvent_t ev_ = nullptr;
+  Phase ph_[3];
+  std::map<std::string, Work> work_;
+  Tune tune_;
+  double dt_ = -1;
+  long launches_ = 0;
+};
+
+Ensemble* Ensemble::create(const std::vector<Model*>& members, std::string* err) {
+  if (members.empty()) {
+    *err = "an ensemble needs at least one member";
+    return nullptr;
+  }
+  const bool f64 = members[0]->fp64();
+  for (Model* m : members)
+    if (!m || m->fp64() != f64) {
+      *err = "ensemble members must share one precision";
+      return nullptr;
+    }
+  Ensemble* e = nullptr;
+  int rc;
+  if (f64) {
+    std::vector<ModelT<double>*> v;
+    for (Model* m : members) v.push_back(static_cast<ModelT<double>*>(m));
+    auto* t = new EnsembleT<double>();
+    rc = t->init(v);
+    e = t;
+  } else {
+    std::vector<ModelT<float>*> v;
+    for (Model* m : members) v.push_back(static_cast<ModelT<float>*>(m));
+    auto* t = new EnsembleT<float>();
+    rc = t->init(v);
+    e = t;
+  }
+  if (rc) {
+    *err = e->error();
+    delete e;
+    return nullptr;
+  }
+  return e;
+}
 
 Model* Model::create(const CaseSetup& cs, bool fp64, int device, std::string* err) {
   int ndev = 0;

@@ -74,4 +74,32 @@ class Model {
   std::string err_;
 };
 
+// Members of uneven sizes advancing together: every launch of the RK3 step is
+// one batched launch over a member x block work list (kernels.cuh: Batch),
+// and the whole step with its acoustic substeps is captured in one CUDA graph
+// per rotation phase.  Members are Model instances of one precision on one
+// device with the same physics switches and substep count; they stay owned by
+// the caller and must outlive the ensemble.  Member state is read and written
+// through the members; their streams are ordered after the ensemble's work.
+class Ensemble {
+ public:
+  virtual ~Ensemble() = default;
+  // nullptr on failure with *err set
+  static Ensemble* create(const std::vector<Model*>& members, std::string* err);
+  const std::string& error() const { return err_; }
+
+  // nsteps large steps of every member, t0 the time of the first
+  virtual int run(int nsteps, double dt, double t0) = 0;
+  // one step with direct batched launches (no graph)
+  virtual int step(double dt, double t) = 0;
+  virtual int sync() = 0;
+  virtual int time_run(int nsteps, double dt, double t0, double* ms) = 0;
+  virtual long launches_per_step() const = 0;
+  // tuned variants: tendencies variant, acoustic column shape, persistent grid
+  virtual void variants(int* tend, int* column, int* persist) const = 0;
+
+ protected:
+  std::string err_;
+};
+
 }  // namespace wfe

@@ -40,12 +40,12 @@ __device__ __forceinline__ R fall_speed(R rq, R rho_sfc, R rho, R T) {
 }
 
 template <typename R, int CX>
-__global__ void k_kessler(KesArgs<R> a) {
+__device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Layout& L = a.L;
   const int nz = L.nz;
   const int tx = threadIdx.x, lane = threadIdx.y, KL = blockDim.y;
-  const int i = blockIdx.x * CX + tx, j = blockIdx.y;
+  const int i = bx * CX + tx, j = by;
   const bool active = i < L.nx;
   R* qrl = reinterpret_cast<R*>(smem_raw);
   R* rhol = qrl + (size_t)nz * CX;
@@ -182,6 +182,15 @@ __global__ void k_kessler(KesArgs<R> a) {
 #undef S
 }
 
+template <typename R, int CX>
+__global__ void k_kessler(KesArgs<R> a) {
+  kessler_body<R, CX>(a, blockIdx.x, blockIdx.y);
+}
+template <typename R, int CX>
+__global__ void k_kessler_batch(Batch<KesArgs<R>> b) {
+  for_each_work(b, [](const KesArgs<R>& a, int x, int y, int) { kessler_body<R, CX>(a, x, y); });
+}
+
 template <typename R>
 static size_t kessler_smem(int nz, int cx, int kl) {
   return ((size_t)4 * nz + (nz + 1) + 2 * kl) * cx * sizeof(R);
@@ -200,15 +209,54 @@ template <typename R>
 int prepare_kessler(int nz) {
   int cx = kessler_cx<R>(nz);
   cudaError_t e;
+  if (cx == 32) {
+    const int sm = (int)kessler_smem<R>(nz, 32, 8);
+    e = cudaFuncSetAttribute(k_kessler<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_kessler_batch<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  } else if (cx == 8) {
+    const int sm = (int)kessler_smem<R>(nz, 8, 32);
+    e = cudaFuncSetAttribute(k_kessler<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_kessler_batch<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  } else {
+    return 2;
+  }
+  return e == cudaSuccess ? 0 : 1;
+}
+
+// Batched columns use the tile of the deepest member (nz_max); the shared
+// arrays are sized for it (prepare_kessler<R>(nz_max) done).
+template <typename R>
+dim3 grid_kessler(const Layout& L, int nz_max) {
+  const int cx = kessler_cx<R>(nz_max);
+  return cx ? dim3((L.nx + cx - 1) / cx, L.ny, 1) : dim3(0, 0, 0);
+}
+
+template <typename R>
+int batch_kessler(const Batch<KesArgs<R>>& b, int nz_max, int nblocks, cudaStream_t st) {
+  const int cx = kessler_cx<R>(nz_max);
   if (cx == 32)
-    e = cudaFuncSetAttribute(k_kessler<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kessler_smem<R>(nz, 32, 8));
+    k_kessler_batch<R, 32><<<nblocks, dim3(32, 8), kessler_smem<R>(nz_max, 32, 8), st>>>(b);
   else if (cx == 8)
-    e = cudaFuncSetAttribute(k_kessler<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kessler_smem<R>(nz, 8, 32));
+    k_kessler_batch<R, 8><<<nblocks, dim3(8, 32), kessler_smem<R>(nz_max, 8, 32), st>>>(b);
   else
     return 2;
-  return e == cudaSuccess ? 0 : 1;
+  return 0;
+}
+
+template <typename R>
+int occupancy_kessler(int nz_max) {
+  const int cx = kessler_cx<R>(nz_max);
+  int n = 0;
+  cudaError_t e = cudaErrorInvalidValue;
+  if (cx == 32)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_kessler_batch<R, 32>, 256,
+                                                      kessler_smem<R>(nz_max, 32, 8));
+  else if (cx == 8)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_kessler_batch<R, 8>, 256,
+                                                      kessler_smem<R>(nz_max, 8, 32));
+  return e == cudaSuccess && n > 0 ? n : 1;
 }
 
 template <typename R>
@@ -297,7 +345,10 @@ void launch_dry_mass(const Layout& L, const DBase<R>& b, const DMetric<R>& m, co
 
 #define WFE_INST(R)                                                                           \
   template int launch_kessler<R>(const KesArgs<R>&, cudaStream_t);                            \
-  template int prepare_kessler<R>(int);                            \
+  template int prepare_kessler<R>(int);                                                        \
+  template dim3 grid_kessler<R>(const Layout&, int);                                           \
+  template int batch_kessler<R>(const Batch<KesArgs<R>>&, int, int, cudaStream_t);             \
+  template int occupancy_kessler<R>(int);                            \
   template void launch_absmax<R>(const R*, size_t, unsigned int*, cudaStream_t);              \
   template void launch_dry_mass<R>(const Layout&, const DBase<R>&, const DMetric<R>&, const R*, \
                                    const R*, const R*, const R*, const R*, int, R, R, double*, \

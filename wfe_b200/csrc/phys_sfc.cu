@@ -81,10 +81,10 @@ enum { SC_RHO, SC_RHOW, SC_DZC, SC_DZW, SC_THV, SC_KW, SC_TH, SC_QV, SC_KLOC, SC
 enum { SM_RHO, SM_RHOW, SM_DZC, SM_DZW, SM_KW, SM_PHI, SM_A, SM_B, SM_C, SM_D, SM_N };
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_sfc_scalar(SfcArgs<R> a) {
+__device__ __forceinline__ void sfc_scalar_body(const SfcArgs<R>& a, int bx, int by) {
   const Layout& L = a.L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
   if (i >= L.nx || j >= L.ny) return;
   const int nz = L.nz;
   using P = Phys<R>;
@@ -360,14 +360,23 @@ __global__ void __launch_bounds__(128) k_sfc_scalar(SfcArgs<R> a) {
   }
 }
 
-// momentum columns: blockIdx.z = 0 for u faces i = 1..nx-1, 1 for v faces
+template <typename R>
+__global__ void __launch_bounds__(128) k_sfc_scalar(SfcArgs<R> a) {
+  sfc_scalar_body(a, blockIdx.x, blockIdx.y);
+}
+template <typename R>
+__global__ void __launch_bounds__(128) k_sfc_scalar_batch(Batch<SfcArgs<R>> b) {
+  for_each_work(b, [](const SfcArgs<R>& a, int x, int y, int) { sfc_scalar_body(a, x, y); });
+}
+
+// momentum columns: block z = 0 for u faces i = 1..nx-1, 1 for v faces
 // j = 1..ny-1: surface drag + implicit mixing (surface.cu:390-436)
 template <typename R>
-__global__ void __launch_bounds__(128) k_sfc_momentum(SfcArgs<R> a) {
+__device__ __forceinline__ void sfc_momentum_body(const SfcArgs<R>& a, int bx, int by, int bz) {
   const Layout& L = a.L;
-  const bool on_v = blockIdx.z == 1;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + (on_v ? 0 : 1);
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + (on_v ? 1 : 0);
+  const bool on_v = bz == 1;
+  const int i = bx * blockDim.x + threadIdx.x + (on_v ? 0 : 1);
+  const int j = by * blockDim.y + threadIdx.y + (on_v ? 1 : 0);
   if (i >= L.nx || j >= L.ny) return;
   const int nz = L.nz;
   const int di = on_v ? 0 : 1, dj = on_v ? 1 : 0;
@@ -396,23 +405,48 @@ __global__ void __launch_bounds__(128) k_sfc_momentum(SfcArgs<R> a) {
 }
 
 template <typename R>
+__global__ void __launch_bounds__(128) k_sfc_momentum(SfcArgs<R> a) {
+  sfc_momentum_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R>
+__global__ void __launch_bounds__(128) k_sfc_momentum_batch(Batch<SfcArgs<R>> b) {
+  for_each_work(b, [](const SfcArgs<R>& a, int x, int y, int z) { sfc_momentum_body(a, x, y, z); });
+}
+
+template <typename R>
 size_t sfc_scratch_count(const Layout& L) {
   // the mass columns and, afterwards, two sets of momentum columns reuse it
   size_t per = (size_t)(L.nz + 1) * L.nx * L.ny;
   return per * (SC_N > 2 * SM_N ? SC_N : 2 * SM_N);
 }
 
+// sub 0: scalar columns; sub 1: u and v momentum columns (after sub 0)
+template <typename R>
+dim3 grid_sfc(const Layout& L, int sub) {
+  return dim3((L.nx + 31) / 32, (L.ny + 3) / 4, sub == 0 ? 1 : 2);
+}
+
 template <typename R>
 int launch_sfc(const SfcArgs<R>& a, cudaStream_t st) {
   if (!a.scratch) return 2;
   dim3 b(32, 4);
-  k_sfc_scalar<R><<<dim3((a.L.nx + 31) / 32, (a.L.ny + 3) / 4), b, 0, st>>>(a);
-  k_sfc_momentum<R><<<dim3((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, 2), b, 0, st>>>(a);
+  k_sfc_scalar<R><<<grid_sfc<R>(a.L, 0), b, 0, st>>>(a);
+  k_sfc_momentum<R><<<grid_sfc<R>(a.L, 1), b, 0, st>>>(a);
   return 0;
+}
+
+template <typename R>
+void batch_sfc(const Batch<SfcArgs<R>>& b, int sub, int nblocks, cudaStream_t st) {
+  if (sub == 0) k_sfc_scalar_batch<R><<<nblocks, dim3(32, 4), 0, st>>>(b);
+  else k_sfc_momentum_batch<R><<<nblocks, dim3(32, 4), 0, st>>>(b);
 }
 
 template int launch_sfc<float>(const SfcArgs<float>&, cudaStream_t);
 template int launch_sfc<double>(const SfcArgs<double>&, cudaStream_t);
+template dim3 grid_sfc<float>(const Layout&, int);
+template dim3 grid_sfc<double>(const Layout&, int);
+template void batch_sfc<float>(const Batch<SfcArgs<float>>&, int, int, cudaStream_t);
+template void batch_sfc<double>(const Batch<SfcArgs<double>>&, int, int, cudaStream_t);
 template size_t sfc_scratch_count<float>(const Layout&);
 template size_t sfc_scratch_count<double>(const Layout&);
 
