@@ -19,6 +19,20 @@ ours       K steps replayed from captured CUDA graphs, timed with CUDA events on
 reference  the reference's own CUDA implementation, compiled from its sources
            (oracle/_ref/refdump_f32, its Integrator::step through its C++ API)
            on the same GPU, same case, K steps after W warm-up steps.
+
+--workload ensemble24 measures the batched ensemble instead: 24 members in
+three groups of 8 on 120x90x45, 220x150x45 and 300x200x45 grids (dx = 12 km,
+20 km top, 37 368 000 cells), seeded synthetic prep inputs (wfe_b200.synth:
+Gaussian ridges, standard-atmosphere sounding, u0 ~ U(5, 20) m/s, theta' and
+qv' noise), full physics (surface layer, nonlocal PBL, soil, radiation,
+Kessler), Davies relaxation over 5 rows, positive-definite moisture, dt = 60 s,
+6 acoustic substeps, FP32.  value = all members' cells x K / device time of K
+graph-replayed batched steps (max over ranks; N > 1 shards members over GPUs
+by cell count, no collective on the data path).  The same members stepped one
+after another through their own graphs give the serial figure; with
+--impl reference the unmodified reference executable (oracle/_ref/wfe_f32)
+runs each member for K steps, one after another, and the sum of its own step-
+loop wall times is the reference figure.
 """
 
 from __future__ import annotations
@@ -245,6 +259,157 @@ def e2e_run(W, case_ini, steps: int, device: int):
     return cells * steps / el, h2d / steps, d2h / steps, el
 
 
+ENS_DIR = Path(tempfile.gettempdir()) / "wfe_b200_ensemble24"
+ENS_CELLS = 8 * (120 * 90 + 220 * 150 + 300 * 200) * 45
+ENS_FIELDS = 3 * 29 + 10 * 27 + 12 + 23  # full physics + Davies + PD, fields per cell-update
+
+
+def ensemble_members():
+    """The 24 member cases (generated once per machine into a temp dir)."""
+    from wfe_b200 import synth
+
+    done = ENS_DIR / "done"
+    if not done.exists():
+        paths = synth.write_ensemble(ENS_DIR, seed=2024, hours=24)
+        done.write_text("\n".join(str(p) for p in paths))
+    return [Path(p) for p in done.read_text().split()]
+
+
+ENS_CONFIG = {
+    "workload": "batched ensemble: 24 members, 8 each on 120x90x45, 220x150x45, 300x200x45, "
+                "dx=12 km, 20 km top, full physics + Kessler + Davies(5) + PD, dt=60 s, ns=6",
+    "members": 24, "cells": ENS_CELLS, "precision": "f32",
+    "inputs": "wfe_b200.synth.write_ensemble(seed=2024): seeded synthetic prep files",
+    "l2": "no flush: per-step working set ~10 GB > L2 (126 MB)",
+    "timing": "CUDA events on the ensemble stream around graph replays",
+}
+
+
+def run_reference_ensemble(args) -> dict:
+    exe = ROOT / "oracle" / "_ref" / "wfe_f32"
+    if not exe.exists():
+        return {"impl": "reference", "unavailable": "oracle/_ref/wfe_f32 not built"}
+    total_s, cells = 0.0, 0
+    for p in ensemble_members():
+        kv = dict(ln.split(" = ", 1) for ln in p.read_text().splitlines() if " = " in ln)
+        dt = float(kv["dt"])
+        r = subprocess.run([str(exe), str(p), f"out_dir=/tmp/wfe_refens/{p.stem}",
+                            "out_interval=1e9", "diag_interval=1e9", f"t_end={args.steps * dt}"],
+                           capture_output=True, text=True, timeout=1800)
+        m = re.search(r"bitti: (\d+) adim, ([\d.]+) s", r.stdout)
+        if r.returncode != 0 or not m:
+            return {"impl": "reference", "unavailable": f"reference member run failed: {p.name}"}
+        total_s += float(m.group(2))
+        cells += int(kv["nx"]) * int(kv["ny"]) * int(kv["nz"])
+    v = cells * args.steps / total_s
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": 0, "ms_per_step": total_s * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded prep inputs)", "config": ENS_CONFIG,
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                         "sample": "the unmodified reference executable run once per member, "
+                                   "members one after another (its ensemble pattern, "
+                                   "tools/run_ensemble.py); wall time of its step loop"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def ensemble_bench(args, rank, world, local):
+    import numpy as np
+    import wfe_b200 as W
+    from wfe_b200 import shard
+
+    paths = ensemble_members()
+    sizes = []
+    for p in paths:
+        kv = dict(ln.split(" = ", 1) for ln in p.read_text().splitlines() if " = " in ln)
+        sizes.append(int(kv["nx"]) * int(kv["ny"]) * int(kv["nz"]))
+    mine = shard.partition(sizes, world)[rank]
+    mem = [W.Case(paths[q], precision="f32", device=local) for q in mine]
+    dt = mem[0].dt
+    cells = sum(sizes[q] for q in mine)
+    ens = W.Ensemble(mem)
+    ens.run(args.warmup, dt, 0.0)
+    ens.sync()
+    sampler = ClockSampler(local)
+    time.sleep(0.3)
+    barrier(world)
+    sync_device(world)
+    ms = ens.time_run(args.steps, dt, args.warmup * dt)
+    sync_device(world)
+    barrier(world)
+    clocks = sampler.stop()
+    ms_max = reduce_max(ms, world)
+    value = sum(sizes) * args.steps / (ms_max / 1000.0)
+    launches = ens.launches_per_step()
+    variants = ens.variants()
+
+    # serial: the same members stepped one after another through their own graphs
+    serial_ms = 0.0
+    t_now = (args.warmup + args.steps) * dt
+    for m in mem:
+        serial_ms += m.time_run(args.steps, dt, t_now)
+    serial_ms = reduce_max(serial_ms, world)
+    serial_value = sum(sizes) * args.steps / (serial_ms / 1000.0)
+
+    # end to end: initial states from pinned host buffers, the |w| watchdog of
+    # every member each 10 steps, the final states back to the host
+    e2e = None
+    if not args.no_e2e:
+        host = [{k: m.field(k, interior=True, dtype=np.float32) for k in W.FIELDS} for m in mem]
+        h2d = d2h = 0
+        sync_device(world)
+        t0 = time.perf_counter()
+        for m, hs in zip(mem, host):
+            for k, a in hs.items():
+                m.set_field(k, a, interior=True)
+                h2d += a.nbytes
+        t = 0.0
+        for s in range(0, args.steps, 10):
+            n = min(10, args.steps - s)
+            ens.run(n, dt, t)
+            t += n * dt
+            for m in mem:
+                if not m.field_absmax("w") < 150.0:
+                    raise RuntimeError("|w| watchdog tripped")
+                d2h += 4
+        for m in mem:
+            for k in W.FIELDS:
+                d2h += m.field(k, interior=True, dtype=np.float32).nbytes
+        ens.sync()
+        el = reduce_max(time.perf_counter() - t0, world)
+        e2e = {"value": sum(sizes) * args.steps / el, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps}
+    stats = {q: shard.member_stats(m) for q, m in zip(mine, mem)}
+    allstats = shard.gather_stats(stats, world, device="cuda" if world > 1 else None)
+    ens.close()
+    for m in mem:
+        m.close()
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        gbs = ENS_FIELDS * 4 * sum(sizes) / (ms_max / args.steps / 1e3) / 1e9 / world
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded prep inputs)",
+            "config": dict(ENS_CONFIG, parallelism=f"members sharded over {world} GPU(s)"),
+            "step_roofline": {"alg_bytes_per_cell": ENS_FIELDS * 4, "achieved_gbs_per_gpu": gbs,
+                              "peak": hbm, "peak_kind": peak_kind, "frac": gbs / hbm},
+            "serial": {"value": serial_value, "ms_per_step": serial_ms / args.steps,
+                       "what": "the same members stepped one after another, each from its own "
+                               "captured graphs"},
+            "speedup_vs_serial": value / serial_value,
+            "variants": variants,
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks, "e2e": e2e,
+            "members_w_max": max(st["w_max"] for st in allstats.values()),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -253,13 +418,27 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["wk82", "ensemble24"], default="wk82")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_setup(args.gpus)
 
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)), flush=True)
+            ref = run_reference_ensemble if args.workload == "ensemble24" else run_reference
+            print(json.dumps(ref(args)), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "ensemble24":
+        ensemble_bench(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
         return
 
     import wfe_b200 as W

@@ -22,6 +22,7 @@ library or a CUDA device every GPU call raises WfeError.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -62,11 +63,13 @@ _lib = None
 
 
 def load_library(path: str | Path | None = None):
-    """Load libwfe_b200.so (raises if it has not been built)."""
+    """Load libwfe_b200.so (raises if it has not been built).  The environment
+    variable WFE_B200_LIB names another build of the library to load."""
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIBPATH
+    env = os.environ.get("WFE_B200_LIB")
+    p = Path(path) if path else (Path(env) if env else LIBPATH)
     if not p.exists():
         raise WfeError(2, f"{p} not built; run `python -m wfe_b200.build`")
     lib = C.CDLL(str(p))

@@ -135,6 +135,7 @@ struct Batch {
 template <typename A, typename F>
 __device__ __forceinline__ void for_each_work(const Batch<A>& b, F&& body) {
   static_assert(sizeof(A) % 4 == 0, "argument blocks are staged as 32-bit words");
+
   __shared__ __align__(16) int raw[sizeof(A) / 4];
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nth = blockDim.x * blockDim.y * blockDim.z;
