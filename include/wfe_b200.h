@@ -40,7 +40,9 @@ enum {
 };
 enum { WFE_F32 = 0, WFE_F64 = 1 };
 enum { WFE_U = 0, WFE_V, WFE_W, WFE_THP, WFE_PIP, WFE_QV, WFE_QC, WFE_QR };
-enum { WFE_ROLE_STATE = 0, WFE_ROLE_TEND = 1, WFE_ROLE_WORK = 2, WFE_ROLE_PIPREV = 3 };
+/* WFE_ROLE_LIN: the tangent-linear / adjoint field of the state (wfe_lin_enable) */
+enum { WFE_ROLE_STATE = 0, WFE_ROLE_TEND = 1, WFE_ROLE_WORK = 2, WFE_ROLE_PIPREV = 3,
+       WFE_ROLE_LIN = 4 };
 enum { WFE_LAYOUT_PADDED = 0, WFE_LAYOUT_INTERIOR = 1 };
 enum { WFE_DTYPE_F64 = 0, WFE_DTYPE_F32 = 1 };
 enum { WFE_2D_RAIN = 0, WFE_2D_TSK = 1, WFE_2D_PBLH = 2, WFE_2D_T2M = 3, WFE_2D_U10 = 4 };
@@ -148,6 +150,25 @@ int wfe_set_boundary(wfe_ctx* ctx, const double* const lo[5], const double* cons
 int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const double* lat,
                     const double* lon, const double* soilw, double start_hour_utc, int doy,
                     int nonlocal);
+
+/* ------------------------------------- tangent-linear and adjoint runs */
+/* No counterpart in the reference.  Linearisation of the dry dynamics (5th-
+ * order advection with the Gal-Chen metric, Rayleigh sponge, constant-K
+ * diffusion, Coriolis, the split-explicit acoustic step with its implicit
+ * w - pi' columns, open and periodic lateral boundaries) about the forward
+ * trajectory; moist, Davies-relaxed, surface-physics and w-damping cases are
+ * refused.  wfe_lin_enable gives the context a linearised field for every
+ * prognostic (WFE_ROLE_LIN in wfe_field_upload / wfe_field_download), all
+ * zero.  wfe_tl_run advances the state x0 -> xN and the linearised field
+ * dx0 -> dxN = M dx0 (M: the Jacobian of the N steps at x0).  wfe_ad_run
+ * advances the state x0 -> xN with checkpoints of the state every
+ * `checkpoint_every` steps, then sweeps back, recomputing between
+ * checkpoints: the linearised field holds dJ/dxN on entry and M^T dJ/dxN =
+ * dJ/dx0 on exit. */
+int wfe_lin_enable(wfe_ctx* ctx);
+int wfe_lin_zero(wfe_ctx* ctx);
+int wfe_tl_run(wfe_ctx* ctx, int nsteps, double dt, double t0);
+int wfe_ad_run(wfe_ctx* ctx, int nsteps, double dt, double t0, int checkpoint_every);
 
 /* --------------------------------------------------- batched ensembles */
 /* No counterpart in the reference, whose ensemble driver runs one process per

@@ -33,7 +33,7 @@ PKG = Path(__file__).resolve().parent
 LIBPATH = PKG / "libwfe_b200.so"
 FIELDS = ["u", "v", "w", "thp", "pip", "qv", "qc", "qr"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
-ROLES = {"state": 0, "tend": 1, "work": 2, "piprev": 3}
+ROLES = {"state": 0, "tend": 1, "work": 2, "piprev": 3, "lin": 4}
 F2D = {"rain": 0, "tsk": 1, "pblh": 2, "t2m": 3, "u10": 4}
 METRIC = ["zeta_w", "zeta_c", "dzeta_c", "dzeta_w", "h", "hx", "hy", "hx_u", "hy_v", "jac",
           "fcor", "mapf"]
@@ -49,7 +49,8 @@ SYMBOLS = [
     "wfe_op_sfc", "wfe_set_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
     "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
     "wfe_ensemble_step", "wfe_ensemble_sync", "wfe_ensemble_time_run",
-    "wfe_ensemble_launches_per_step", "wfe_ensemble_variants",
+    "wfe_ensemble_launches_per_step", "wfe_ensemble_variants", "wfe_lin_enable", "wfe_lin_zero",
+    "wfe_tl_run", "wfe_ad_run",
 ]
 
 
@@ -109,6 +110,10 @@ def load_library(path: str | Path | None = None):
         [vp] * 11
     lib.wfe_kernel_times.argtypes = [vp, C.c_double, C.c_double, C.c_int, dp, ip, C.c_char_p,
                                      C.c_int, ip]
+    lib.wfe_lin_enable.argtypes = [vp]
+    lib.wfe_lin_zero.argtypes = [vp]
+    lib.wfe_tl_run.argtypes = [vp, C.c_int, C.c_double, C.c_double]
+    lib.wfe_ad_run.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_int]
     lib.wfe_ensemble_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
     lib.wfe_ensemble_destroy.argtypes = [vp]
     lib.wfe_ensemble_run.argtypes = [vp, C.c_int, C.c_double, C.c_double]
@@ -311,6 +316,24 @@ class Case:
                 (tsk, land, lat, lon, soilw)]
         self._check(self._lib.wfe_set_physics(self._h, *[_dptr(a) for a in arrs], start_hour,
                                               int(doy), int(nonlocal_pbl)))
+
+    # ---------------------------------------- tangent-linear / adjoint
+    def lin_enable(self) -> None:
+        """Linearised fields (role "lin") for the tangent-linear and adjoint runs."""
+        self._check(self._lib.wfe_lin_enable(self._h))
+
+    def lin_zero(self) -> None:
+        self._check(self._lib.wfe_lin_zero(self._h))
+
+    def tl_run(self, nsteps: int, dt: float | None = None, t0: float = 0.0) -> None:
+        """state x0 -> xN and lin field dx0 -> M dx0"""
+        self._check(self._lib.wfe_tl_run(self._h, nsteps, self.dt if dt is None else dt, t0))
+
+    def ad_run(self, nsteps: int, dt: float | None = None, t0: float = 0.0,
+               checkpoint_every: int = 30) -> None:
+        """state x0 -> xN; lin field dJ/dxN -> M^T dJ/dxN = dJ/dx0"""
+        self._check(self._lib.wfe_ad_run(self._h, nsteps, self.dt if dt is None else dt, t0,
+                                         checkpoint_every))
 
     # -------------------------------------------------------------- index
     def interior(self, a, name: str = "c") -> np.ndarray:

@@ -15,6 +15,7 @@ using namespace wfe;
 struct wfe_ctx {
   CaseSetup cs;
   std::unique_ptr<Model> model;
+  std::unique_ptr<Lin> lin;  // declared after model: released first
   std::string err;
   int bdy_idx_hi = 1;  // BdyManager::idx_hi_
   double t_lo = 0, t_hi = 0;
@@ -519,4 +520,35 @@ int wfe_ensemble_variants(const wfe_ens* ens, int out[3]) {
   if (!ens || !out) return WFE_ERR_ARG;
   ens->e->variants(&out[0], &out[1], &out[2]);
   return WFE_OK;
+}
+
+// ------------------------------------------------- tangent-linear / adjoint
+int wfe_lin_enable(wfe_ctx* c) {
+  NEED_MODEL(c);
+  if (c->lin) return WFE_OK;
+  std::string err;
+  c->lin.reset(Lin::create(c->model.get(), &err));
+  if (!c->lin) return set_err(c, WFE_ERR_CONFIG, err);
+  return WFE_OK;
+}
+
+int wfe_lin_zero(wfe_ctx* c) {
+  NEED_MODEL(c);
+  if (!c->lin) return set_err(c, WFE_ERR_ARG, "linearisation not enabled");
+  return c->lin->zero() ? set_err(c, WFE_ERR_CUDA, c->lin->error()) : WFE_OK;
+}
+
+int wfe_tl_run(wfe_ctx* c, int nsteps, double dt, double t0) {
+  NEED_MODEL(c);
+  if (!c->lin) return set_err(c, WFE_ERR_ARG, "linearisation not enabled");
+  if (nsteps < 0) return set_err(c, WFE_ERR_ARG, "nsteps < 0");
+  return c->lin->tl_run(nsteps, dt, t0) ? set_err(c, WFE_ERR_CUDA, c->lin->error()) : WFE_OK;
+}
+
+int wfe_ad_run(wfe_ctx* c, int nsteps, double dt, double t0, int checkpoint_every) {
+  NEED_MODEL(c);
+  if (!c->lin) return set_err(c, WFE_ERR_ARG, "linearisation not enabled");
+  if (nsteps < 0) return set_err(c, WFE_ERR_ARG, "nsteps < 0");
+  return c->lin->ad_run(nsteps, dt, t0, checkpoint_every) ? set_err(c, WFE_ERR_CUDA, c->lin->error())
+                                                           : WFE_OK;
 }

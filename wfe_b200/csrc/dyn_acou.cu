@@ -24,6 +24,7 @@
 
 #include "core.cuh"
 #include "kernels.cuh"
+#include "dyn_common.cuh"
 
 namespace wfe {
 
@@ -56,39 +57,6 @@ __global__ void k_coef_face(Layout L, const R* rtjc, R* rtjx, R* rtjy) {
 }
 
 // ------------------------------------------------------------ forward u, v
-template <typename R>
-__device__ __forceinline__ R pistar(const AcouArgs<R>& a, int i, int j, int k) {
-  // pi* = pi' + smdiv (pi' - pi'_prev)  (kernels.cu:486-489)
-  const Layout& L = a.L;
-  const bool ghost = i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz;
-  R cur, prev;
-  if (!ghost) {
-    const size_t c = L.at(i, j, k);
-    cur = a.pi_cur[c];
-    prev = a.pi_prev[c];
-  } else {
-    const size_t c = L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open),
-                          map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), map_zc(k, L.nz));
-    cur = a.pi_cur[c];
-    prev = a.n_pip[c];
-  }
-  return cur + a.p.acoustic_smdiv * (cur - prev);
-}
-
-template <typename R>
-__device__ __forceinline__ R theta_v(const AcouArgs<R>& a, int i, int j, int k) {
-  // full virtual potential temperature at a cell centre (kernels.cu:490-495)
-  const Layout& L = a.L;
-  const bool lat = i < 0 || i >= L.nx || j < 0 || j >= L.ny;
-  const size_t c = L.at(i, j, k);
-  size_t s = c;
-  if (lat)
-    s = L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open), map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), k);
-  R t = a.b.thb[c] + (lat ? a.n_thp[s] : a.th_in[c]);
-  if (a.p.moisture) t *= (R)1 + Phys<R>::eps61 * a.qv[s];
-  return t;
-}
-
 // Interior points: every neighbour the forward step reads is an interior
 // point, so pi* and theta_v are plain offsets from the face (no ghost maps).
 template <typename R>

@@ -13,28 +13,9 @@
 
 #include "core.cuh"
 #include "kernels.cuh"
+#include "dyn_common.cuh"
 
 namespace wfe {
-
-// ------------------------------------------------------------------ helpers
-template <typename R>
-__device__ __forceinline__ R sponge(R zeta, R zt, const DParams<R>& p) {
-  // src/dynamics/kernels.cu:42-48
-  if (p.rayleigh_zd < (R)0) return 0;
-  if (zeta <= p.rayleigh_zd || zt <= p.rayleigh_zd) return 0;
-  const R halfpi = (R)1.5707963267948966;
-  R s = sin(halfpi * (zeta - p.rayleigh_zd) / (zt - p.rayleigh_zd));
-  return p.rayleigh_alpha * s * s;
-}
-
-template <typename R>
-__device__ __forceinline__ R face5(R qm2, R qm1, R q0, R q1, R q2, R q3, R vel) {
-  // 5th-order upwind interface value (src/dynamics/kernels.cu:51-57)
-  const R c = (R)(1.0 / 60.0);
-  R cen = c * ((R)37 * (q0 + q1) - (R)8 * (qm1 + q2) + (qm2 + q3));
-  R upw = c * ((q3 - qm2) - (R)5 * (q2 - qm1) + (R)10 * (q1 - q0));
-  return (vel >= (R)0) ? (cen - upw) : (cen + upw);
-}
 
 // -------------------------------------------------------------- ghost fill
 // One launch fills the ghost rings of up to 8 fields with the composition of

@@ -210,6 +210,33 @@ dim3 grid_sfc(const Layout& L, int sub);
 template <typename R>
 void batch_sfc(const Batch<SfcArgs<R>>& b, int sub, int nblocks, cudaStream_t st);
 
+// Tangent-linear (tl_) and adjoint (ad_) launches of the dry dynamics
+// (lin.cu): a is the forward argument block of the linearised launch, d the
+// same block over the tangent or adjoint buffers.  The TL of the ghost fill
+// and of the mass fluxes is the forward launch on d.  The column launches
+// return 2 when nz exceeds lin_max_levels().
+template <typename R>
+void ad_fill(const FillArgs<R>& d, cudaStream_t st);
+template <typename R>
+void ad_flux(const FluxArgs<R>& d, cudaStream_t st);
+template <typename R>
+void tl_tend(const TendArgs<R>& a, const TendArgs<R>& d, cudaStream_t st);
+template <typename R>
+void ad_tend(const TendArgs<R>& a, const TendArgs<R>& d, cudaStream_t st);
+template <typename R>
+void tl_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+template <typename R>
+void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+template <typename R>
+int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+template <typename R>
+int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+int lin_max_levels();
+// zero a cell field outside the interior cells (the pi' ghost ring, which no
+// launch of a step reads or writes)
+template <typename R>
+void zero_ring(R* f, const Layout& L, cudaStream_t st);
+
 template <typename R>
 int launch_sfc(const SfcArgs<R>& a, cudaStream_t st);
 template <typename R>

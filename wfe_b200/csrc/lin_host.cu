@@ -1,0 +1,459 @@
+// Tangent-linear and adjoint runs of the dry dynamics (Lin, model.hpp).
+//
+// The step is taken from the model's own recorded launch sequence, so the
+// linearised runs follow the forward's buffer rotation exactly: every
+// state-like forward buffer has a linearised mirror, and each recorded
+// argument block is translated to the mirrors to drive the TL / AD kernel of
+// that launch (lin.cu).
+//
+// TL:  per launch, the TL kernel (forward values still in place) and then the
+//      forward launch.
+// AD:  the forward pass stores the time-n state every `every` steps.  The
+//      reverse sweep takes the segments last to first: it recomputes the
+//      segment storing every step's time-n state, then for each step (last
+//      first) restores its state, replays the step forward while saving the
+//      buffers each launch overwrites (an undo log), and walks the launches
+//      backwards: restore the launch's outputs, run its AD kernel.  A step is
+//      a function of its time-n state alone (every other buffer is written
+//      before it is read), so restoring that state reproduces the step.
+// Cost per step: three forward steps (run, segment recompute, replay), the
+// undo-log copies and the AD kernels.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "model.hpp"
+
+namespace wfe {
+namespace {
+
+#define LCK(call)                                                                 \
+  do {                                                                            \
+    cudaError_t e__ = (call);                                                     \
+    if (e__ != cudaSuccess) return fail(std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+template <typename R>
+class LinT final : public Lin {
+ public:
+  ~LinT() override { release(); }
+
+  int init(Model* m) {
+    m_ = m;
+    std::string why;
+    if (!m->linearisable(&why)) return fail(why);
+    st_ = static_cast<cudaStream_t>(m->stream_handle());
+    for (auto& b : m->state_buffers()) {
+      void* p = nullptr;
+      LCK(cudaMalloc(&p, b.second * sizeof(R)));
+      LCK(cudaMemsetAsync(p, 0, b.second * sizeof(R), st_));
+      map_[b.first] = p;
+      bufs_.push_back({static_cast<R*>(p), b.second});
+      fwd_.push_back({static_cast<R*>(b.first), b.second});
+    }
+    n3_ = bufs_.empty() ? 0 : bufs_[0].second;
+    std::vector<Rec> recs;
+    if (m->record_step(1.0, &recs)) return fail(m->error());
+    learn_layout(recs);
+    m->set_lin_map([this](const void* p) -> void* {
+      auto it = map_.find(p);
+      return it == map_.end() ? nullptr : it->second;
+    });
+    LCK(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  int zero() override {
+    for (auto& b : bufs_) LCK(cudaMemsetAsync(b.first, 0, b.second * sizeof(R), st_));
+    LCK(cudaStreamSynchronize(st_));
+    return 0;
+  }
+
+  int tl_run(int nsteps, double dt, double t0) override {
+    (void)t0;
+    if (keep_only_state()) return 1;
+    for (int s = 0; s < nsteps; ++s) {
+      std::vector<Rec> recs;
+      if (m_->record_step(dt, &recs)) return fail(m_->error());
+      for (const Rec& r : recs) {
+        if (tl(r) || fwd(r)) return 1;
+      }
+      m_->rotate();
+    }
+    // pi' ghosts are outputs of nothing: the tangent has none there
+    if (L_.nx) zero_ring<R>(D(static_cast<R*>(m_->state_field(4))), L_, st_);
+    LCK(cudaStreamSynchronize(st_));
+    LCK(cudaGetLastError());
+    return 0;
+  }
+
+  int ad_run(int nsteps, double dt, double t0, int every) override {
+    (void)t0;
+    if (nsteps <= 0) return 0;
+    if (every < 1) every = 1;
+    // the adjoint of x_N, uploaded in the slot of the current time-n state;
+    // pi' ghosts are no state, so adjoint values there are dropped
+    if (L_.nx) zero_ring<R>(D(static_cast<R*>(m_->state_field(4))), L_, st_);
+    std::vector<R*> bar;
+    if (save_lin_state(&bar)) return 1;
+    // forward pass with segment checkpoints; x_N kept to restore at the end
+    const int nseg = (nsteps + every - 1) / every;
+    std::vector<Snap> segs(nseg);
+    for (int s = 0; s < nsteps; ++s) {
+      if (s % every == 0 && snap(&segs[s / every])) return 1;
+      if (step_fwd(dt)) return 1;
+    }
+    Snap last;
+    if (snap(&last)) return 1;
+    if (zero() || load_lin_state(bar)) return 1;
+    std::vector<Snap> steps(every);
+    for (int g = nseg - 1; g >= 0; --g) {
+      const int s0 = g * every, s1 = std::min(nsteps, s0 + every);
+      if (restore(segs[g])) return 1;
+      for (int s = s0; s < s1; ++s) {
+        if (snap(&steps[s - s0])) return 1;
+        if (s + 1 < s1 && step_fwd(dt)) return 1;
+      }
+      for (int s = s1 - 1; s >= s0; --s) {
+        if (restore(steps[s - s0])) return 1;
+        if (step_ad(dt)) return 1;
+      }
+    }
+    // dJ/dx0 sits in the slot of x0; move it to the slot of x_N
+    if (save_lin_state(&bar)) return 1;
+    if (restore(last) || zero() || load_lin_state(bar)) return 1;
+    for (auto& s : segs) free_snap(&s);
+    for (auto& s : steps) free_snap(&s);
+    free_snap(&last);
+    for (R* p : bar) cudaFree(p);
+    LCK(cudaStreamSynchronize(st_));
+    LCK(cudaGetLastError());
+    return 0;
+  }
+
+ private:
+  struct Snap {
+    int phase = -1;
+    R* d = nullptr;  // 8 fields of the time-n state
+  };
+
+  R* D(const R* p) const {
+    if (!p) return nullptr;
+    auto it = map_.find(p);
+    return it == map_.end() ? nullptr : static_cast<R*>(it->second);
+  }
+
+  template <class A>
+  static const A& as(const Rec& r) {
+    return *reinterpret_cast<const A*>(r.args.data());
+  }
+
+  FillArgs<R> tr(const FillArgs<R>& a) const {
+    FillArgs<R> d = a;
+    for (int q = 0; q < a.job.n; ++q) d.job.f[q] = D(a.job.f[q]);
+    return d;
+  }
+  FluxArgs<R> tr(const FluxArgs<R>& a) const {
+    FluxArgs<R> d = a;
+    d.u = D(a.u);
+    d.v = D(a.v);
+    d.w = D(a.w);
+    d.mfx = D(a.mfx);
+    d.mfy = D(a.mfy);
+    d.mfz = D(a.mfz);
+    return d;
+  }
+  TendArgs<R> tr(const TendArgs<R>& a) const {
+    TendArgs<R> d = a;
+    for (const R** p : {&d.u, &d.v, &d.w, &d.thp, &d.pip, &d.qv, &d.qc, &d.qr, &d.mfx, &d.mfy,
+                        &d.mfz})
+      *p = D(*p);
+    for (R** p : {&d.tu, &d.tv, &d.tw, &d.tth, &d.tpi}) *p = D(*p);
+    return d;
+  }
+  AcouArgs<R> tr(const AcouArgs<R>& a) const {
+    AcouArgs<R> d = a;
+    for (const R** p : {&d.u_in, &d.v_in, &d.w_in, &d.pi_prev, &d.pi_cur, &d.th_in, &d.n_pip,
+                        &d.n_thp, &d.qv, &d.qc, &d.qr, &d.tu, &d.tv, &d.tw, &d.tth, &d.tpi})
+      *p = D(*p);
+    for (R** p : {&d.u_out, &d.v_out, &d.w_out, &d.pi_next, &d.th_out}) *p = D(*p);
+    return d;
+  }
+
+  int unsupported(int kind) { return fail("launch kind " + std::to_string(kind) + " is not linearised"); }
+
+  int fwd(const Rec& r) {
+    switch (r.kind) {
+      case K_FILL: {
+        const auto& a = as<FillArgs<R>>(r);
+        launch_fill_ghosts<R>(a.L, a.job, a.open_x, a.open_y, st_);
+        break;
+      }
+      case K_FLUX: {
+        const auto& a = as<FluxArgs<R>>(r);
+        launch_mass_flux<R>(a.L, a.b, a.m, a.u, a.v, a.w, a.mfx, a.mfy, a.mfz, st_);
+        break;
+      }
+      case K_TEND: launch_tendencies<R>(as<TendArgs<R>>(r), 0, st_); break;
+      case K_UV: launch_acoustic_uv<R>(as<AcouArgs<R>>(r), st_); break;
+      case K_COL:
+        if (launch_acoustic_column<R>(as<AcouArgs<R>>(r), m_->column_shape(), st_))
+          return fail("acoustic column launch");
+        break;
+      default: return unsupported(r.kind);
+    }
+    return 0;
+  }
+
+  int tl(const Rec& r) {
+    switch (r.kind) {
+      case K_FILL: {
+        const FillArgs<R> d = tr(as<FillArgs<R>>(r));
+        launch_fill_ghosts<R>(d.L, d.job, d.open_x, d.open_y, st_);
+        break;
+      }
+      case K_FLUX: {
+        const FluxArgs<R> d = tr(as<FluxArgs<R>>(r));
+        launch_mass_flux<R>(d.L, d.b, d.m, d.u, d.v, d.w, d.mfx, d.mfy, d.mfz, st_);
+        break;
+      }
+      case K_TEND: {
+        const auto& a = as<TendArgs<R>>(r);
+        tl_tend<R>(a, tr(a), st_);
+        break;
+      }
+      case K_UV: {
+        const auto& a = as<AcouArgs<R>>(r);
+        tl_uv<R>(a, tr(a), st_);
+        break;
+      }
+      case K_COL: {
+        const auto& a = as<AcouArgs<R>>(r);
+        if (tl_column<R>(a, tr(a), st_)) return fail("column deeper than the linearised kernels hold");
+        break;
+      }
+      default: return unsupported(r.kind);
+    }
+    return 0;
+  }
+
+  int ad(const Rec& r) {
+    switch (r.kind) {
+      case K_FILL: ad_fill<R>(tr(as<FillArgs<R>>(r)), st_); break;
+      case K_FLUX: ad_flux<R>(tr(as<FluxArgs<R>>(r)), st_); break;
+      case K_TEND: {
+        const auto& a = as<TendArgs<R>>(r);
+        ad_tend<R>(a, tr(a), st_);
+        break;
+      }
+      case K_UV: {
+        const auto& a = as<AcouArgs<R>>(r);
+        ad_uv<R>(a, tr(a), st_);
+        break;
+      }
+      case K_COL: {
+        const auto& a = as<AcouArgs<R>>(r);
+        if (ad_column<R>(a, tr(a), st_)) return fail("column deeper than the linearised kernels hold");
+        break;
+      }
+      default: return unsupported(r.kind);
+    }
+    return 0;
+  }
+
+  // forward buffers a launch overwrites (saved before it runs)
+  static void outputs(const Rec& r, std::vector<R*>* o) {
+    o->clear();
+    switch (r.kind) {
+      case K_FILL: {
+        const auto& a = as<FillArgs<R>>(r);
+        for (int q = 0; q < a.job.n; ++q) o->push_back(a.job.f[q]);
+        break;
+      }
+      case K_FLUX: {
+        const auto& a = as<FluxArgs<R>>(r);
+        *o = {a.mfx, a.mfy, a.mfz};
+        break;
+      }
+      case K_TEND: {
+        const auto& a = as<TendArgs<R>>(r);
+        *o = {a.tu, a.tv, a.tw, a.tth};
+        if (a.tpi) o->push_back(a.tpi);
+        break;
+      }
+      case K_UV: {
+        const auto& a = as<AcouArgs<R>>(r);
+        *o = {a.u_out, a.v_out};
+        break;
+      }
+      case K_COL: {
+        const auto& a = as<AcouArgs<R>>(r);
+        *o = {a.w_out, a.pi_next, a.th_out};
+        break;
+      }
+      default: break;
+    }
+  }
+
+  // the layout of the case, taken from the first recorded fill
+  void learn_layout(const std::vector<Rec>& recs) {
+    if (L_.nx) return;
+    for (const Rec& r : recs)
+      if (r.kind == K_FILL) {
+        L_ = as<FillArgs<R>>(r).L;
+        return;
+      }
+  }
+
+  int step_fwd(double dt) {
+    std::vector<Rec> recs;
+    if (m_->record_step(dt, &recs)) return fail(m_->error());
+    for (const Rec& r : recs)
+      if (fwd(r)) return 1;
+    m_->rotate();
+    return 0;
+  }
+
+  int step_ad(double dt) {
+    std::vector<Rec> recs;
+    if (m_->record_step(dt, &recs)) return fail(m_->error());
+    size_t need = 0;
+    std::vector<R*> o;
+    for (const Rec& r : recs) {
+      outputs(r, &o);
+      need += o.size();
+    }
+    if (need > log_cap_) {
+      if (log_) cudaFree(log_);
+      log_ = nullptr;
+      log_cap_ = 0;
+      LCK(cudaMalloc(&log_, need * n3_ * sizeof(R)));
+      log_cap_ = need;
+    }
+    size_t slot = 0;
+    for (const Rec& r : recs) {
+      outputs(r, &o);
+      for (R* p : o) {
+        LCK(cudaMemcpyAsync(log_ + slot * n3_, p, n3_ * sizeof(R), cudaMemcpyDeviceToDevice, st_));
+        ++slot;
+      }
+      if (fwd(r)) return 1;
+    }
+    for (size_t q = recs.size(); q-- > 0;) {
+      outputs(recs[q], &o);
+      for (size_t z = o.size(); z-- > 0;) {
+        --slot;
+        LCK(cudaMemcpyAsync(o[z], log_ + slot * n3_, n3_ * sizeof(R), cudaMemcpyDeviceToDevice, st_));
+      }
+      if (ad(recs[q])) return 1;
+    }
+    LCK(cudaGetLastError());
+    return 0;
+  }
+
+  int snap(Snap* s) {
+    if (!s->d) LCK(cudaMalloc(&s->d, 8 * n3_ * sizeof(R)));
+    s->phase = m_->phase();
+    for (int f = 0; f < 8; ++f)
+      LCK(cudaMemcpyAsync(s->d + f * n3_, m_->state_field(f), n3_ * sizeof(R),
+                          cudaMemcpyDeviceToDevice, st_));
+    return 0;
+  }
+
+  int restore(const Snap& s) {
+    if (s.phase < 0 || s.phase > 2 || !s.d) return fail("restore of a state never saved");
+    while (m_->phase() != s.phase) m_->rotate();
+    for (int f = 0; f < 8; ++f)
+      LCK(cudaMemcpyAsync(m_->state_field(f), s.d + f * n3_, n3_ * sizeof(R),
+                          cudaMemcpyDeviceToDevice, st_));
+    return 0;
+  }
+
+  void free_snap(Snap* s) {
+    if (s->d) cudaFree(s->d);
+    s->d = nullptr;
+  }
+
+  // copies of the linearised time-n state (8 fields)
+  int save_lin_state(std::vector<R*>* out) {
+    for (R* p : *out) cudaFree(p);
+    out->assign(8, nullptr);
+    for (int f = 0; f < 8; ++f) {
+      LCK(cudaMalloc(&(*out)[f], n3_ * sizeof(R)));
+      LCK(cudaMemcpyAsync((*out)[f], D(static_cast<R*>(m_->state_field(f))), n3_ * sizeof(R),
+                          cudaMemcpyDeviceToDevice, st_));
+    }
+    return 0;
+  }
+
+  int load_lin_state(const std::vector<R*>& in) {
+    for (int f = 0; f < 8; ++f)
+      LCK(cudaMemcpyAsync(D(static_cast<R*>(m_->state_field(f))), in[f], n3_ * sizeof(R),
+                          cudaMemcpyDeviceToDevice, st_));
+    return 0;
+  }
+
+  // zero every linearised buffer but the time-n state's
+  int keep_only_state() {
+    std::vector<R*> keep;
+    if (save_lin_state(&keep) || zero() || load_lin_state(keep)) return 1;
+    LCK(cudaStreamSynchronize(st_));
+    for (R* p : keep) cudaFree(p);
+    return 0;
+  }
+
+  int fail(const std::string& m) {
+    err_ = m;
+    return 1;
+  }
+
+  void release() {
+    if (m_) m_->set_lin_map(nullptr);
+    for (auto& b : bufs_) cudaFree(b.first);
+    bufs_.clear();
+    if (log_) cudaFree(log_);
+    log_ = nullptr;
+  }
+
+  Model* m_ = nullptr;
+  cudaStream_t st_ = nullptr;
+  std::map<const void*, void*> map_;
+  std::vector<std::pair<R*, size_t>> bufs_, fwd_;
+  size_t n3_ = 0;
+  Layout L_{};
+  R* log_ = nullptr;
+  size_t log_cap_ = 0;
+};
+
+}  // namespace
+
+Lin* Lin::create(Model* m, std::string* err) {
+  if (!m) {
+    *err = "no model";
+    return nullptr;
+  }
+  Lin* l = nullptr;
+  int rc;
+  if (m->fp64()) {
+    auto* t = new LinT<double>();
+    rc = t->init(m);
+    l = t;
+  } else {
+    auto* t = new LinT<float>();
+    rc = t->init(m);
+    l = t;
+  }
+  if (rc) {
+    *err = l->error();
+    delete l;
+    return nullptr;
+  }
+  return l;
+}
+
+}  // namespace wfe

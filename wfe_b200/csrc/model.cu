@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -39,11 +40,6 @@ struct Tune {
   bool done = false;
 };
 
-// One launch of a step recorded for batched replay: its kind and argument block.
-struct Rec {
-  int kind;
-  std::vector<unsigned char> args;
-};
 
 namespace {
 std::mutex g_tune_mu;
@@ -206,6 +202,7 @@ class ModelT final : public Model {
       case ROLE_TEND: return T_[field];
       case ROLE_WORK: return S_[perm_[1]][field];
       case ROLE_PIPREV: return piprev_ ? piprev_ : S_[perm_[0]][4];
+      case ROLE_LIN: return lin_map_ ? static_cast<R*>(lin_map_(S_[perm_[0]][field])) : nullptr;
       default: return nullptr;
     }
   }
@@ -555,7 +552,7 @@ class ModelT final : public Model {
   // ----------------------------------------------------- batched ensembles
   // The launches of one step from the current rotation phase, recorded
   // instead of issued; the rotation is left unchanged.
-  int record_step(double dt, std::vector<Rec>* out) {
+  int record_step(double dt, std::vector<Rec>* out) override {
     const int saved[3] = {perm_[0], perm_[1], perm_[2]};
     const int ph = phase_;
     const long l = launches_;
@@ -569,8 +566,31 @@ class ModelT final : public Model {
     phase_ = ph;
     return rc;
   }
-  void rotate() { advance_rotation(); }
-  int phase() const { return phase_; }
+  void rotate() override { advance_rotation(); }
+  int phase() const override { return phase_; }
+  std::vector<std::pair<void*, size_t>> state_buffers() const override {
+    std::vector<std::pair<void*, size_t>> v;
+    const size_t n3 = L_.n3();
+    for (int s = 0; s < 3; ++s)
+      for (int f = 0; f < 8; ++f) v.push_back({S_[s][f], n3});
+    for (int f = 0; f < 8; ++f) v.push_back({T_[f], n3});
+    for (R* p : {mfx_, mfy_, mfz_, U2_, V2_, P1_, P2_}) v.push_back({p, n3});
+    return v;
+  }
+  void* state_field(int field) override {
+    return (field >= 0 && field < 8) ? S_[perm_[0]][field] : nullptr;
+  }
+  void* stream_handle() const override { return st_; }
+  int column_shape() const override { return tune_.column_cx; }
+  void set_lin_map(std::function<void*(const void*)> map) override { lin_map_ = std::move(map); }
+  bool linearisable(std::string* why) const override {
+    if (dp_.moisture) *why = "moist cases are not linearised";
+    else if (bdy_on_) *why = "Davies relaxation is not linearised";
+    else if (sfc_on_) *why = "the surface physics is not linearised";
+    else if (dp_.w_damping) *why = "w damping is not linearised";
+    else return true;
+    return false;
+  }
   long generation() const { return gen_; }
   double* clock_ptr() const { return clock_; }
   double bdy_t_lo() const { return t_lo_; }
@@ -1052,6 +1072,7 @@ class ModelT final : public Model {
   bool graphs_valid_ = false;
   long gen_ = 0;  // changes whenever buffer roles or physics switches change
   std::vector<Rec>* rec_ = nullptr;  // record mode when set
+  std::function<void*(const void*)> lin_map_;
   double graph_dt_ = 0;
   long launches_ = 0, glaunches_ = 0;
   bool profiling_ = false;

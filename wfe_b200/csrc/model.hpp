@@ -2,14 +2,24 @@
 // GPU).  ModelT<R> in model.cu implements it for float and double.
 #pragma once
 
+#include <functional>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "setup.hpp"
 
 namespace wfe {
 
-enum Role { ROLE_STATE = 0, ROLE_TEND = 1, ROLE_WORK = 2, ROLE_PIPREV = 3 };
+// ROLE_LIN: the tangent-linear / adjoint field of the time-n state (Lin)
+enum Role { ROLE_STATE = 0, ROLE_TEND = 1, ROLE_WORK = 2, ROLE_PIPREV = 3, ROLE_LIN = 4 };
+
+// One launch of a step recorded instead of issued: its kind (kernels.cuh
+// Kind) and argument block.
+struct Rec {
+  int kind;
+  std::vector<unsigned char> args;
+};
 enum Field2D { F2_RAIN = 0, F2_TSK = 1, F2_PBLH = 2, F2_T2M = 3, F2_U10 = 4, F2_WGT = 5 };
 
 class Model {
@@ -69,6 +79,40 @@ class Model {
   // one direct step with CUDA events around every launch: per-kernel totals
   virtual int kernel_times(double dt, double t, std::vector<std::string>* names,
                            std::vector<double>* ms, std::vector<int>* counts) = 0;
+
+  // ------------------------------------- access for batched / linearised steps
+  // the launches of one step from the current rotation phase, not issued
+  virtual int record_step(double dt, std::vector<Rec>* out) = 0;
+  virtual void rotate() = 0;  // what a step does to the buffer roles
+  virtual int phase() const = 0;
+  // state-like device buffers (states, tendencies, mass fluxes, acoustic
+  // scratch): base pointer and element count
+  virtual std::vector<std::pair<void*, size_t>> state_buffers() const = 0;
+  virtual void* state_field(int field) = 0;  // time-n device buffer of a field
+  virtual void* stream_handle() const = 0;
+  virtual int column_shape() const = 0;      // acoustic column tile in use
+  // buffer -> linearised buffer map behind ROLE_LIN (empty function: none)
+  virtual void set_lin_map(std::function<void*(const void*)> map) = 0;
+  // whether the step is one the linearised kernels cover (why not, if not)
+  virtual bool linearisable(std::string* why) const = 0;
+
+ protected:
+  std::string err_;
+};
+
+// Tangent-linear and adjoint runs of a Model's dry dynamics (lin_host.cu).
+// The linearised field of the time-n state is the model's ROLE_LIN field.
+class Lin {
+ public:
+  virtual ~Lin() = default;
+  static Lin* create(Model* m, std::string* err);
+  const std::string& error() const { return err_; }
+  // forward and tangent together: state x0 -> xN, ROLE_LIN dx0 -> dxN
+  virtual int tl_run(int nsteps, double dt, double t0) = 0;
+  // state x0 -> xN (forward with checkpoints every `every` steps), then the
+  // adjoint sweep: ROLE_LIN dJ/dxN on entry -> dJ/dx0 on exit
+  virtual int ad_run(int nsteps, double dt, double t0, int every) = 0;
+  virtual int zero() = 0;  // every linearised buffer to 0
 
  protected:
   std::string err_;
