@@ -94,6 +94,12 @@ int wfe_field_download(wfe_ctx* ctx, int role, int field, void* host, int dtype,
  * interior ny*nx */
 int wfe_field2d_download(wfe_ctx* ctx, int which, void* host, int dtype, int layout);
 
+/* The driver settings src/main.cpp reads besides the case (main.cpp:262-275,
+ * 418-420): out_interval, diag_interval and w_abort [s, s, m/s] into
+ * out[3]; out_dir into a caller buffer of out_dir_len bytes (truncated,
+ * always terminated). */
+int wfe_get_run_config(const wfe_ctx* ctx, double out[3], char* out_dir, int out_dir_len);
+
 /* ----------------------------------------------------------- stepping */
 
 /* Integrator::step(dt, t) (src/dynamics/integrator.cpp:71-111): one

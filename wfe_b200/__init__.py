@@ -50,7 +50,7 @@ SYMBOLS = [
     "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
     "wfe_ensemble_step", "wfe_ensemble_sync", "wfe_ensemble_time_run",
     "wfe_ensemble_launches_per_step", "wfe_ensemble_variants", "wfe_lin_enable", "wfe_lin_zero",
-    "wfe_tl_run", "wfe_ad_run",
+    "wfe_tl_run", "wfe_ad_run", "wfe_get_run_config",
 ]
 
 

@@ -187,6 +187,19 @@ int wfe_get_spacing(const wfe_ctx* c, double out[6]) {
   return WFE_OK;
 }
 
+int wfe_get_run_config(const wfe_ctx* c, double out[3], char* out_dir, int out_dir_len) {
+  if (!c || !out) return WFE_ERR_ARG;
+  const CaseSetup& cs = c->cs;
+  out[0] = cs.out_every;
+  out[1] = cs.diag_every;
+  out[2] = cs.p.w_abort;
+  if (out_dir && out_dir_len > 0) {
+    std::strncpy(out_dir, cs.out_dir.c_str(), (size_t)out_dir_len - 1);
+    out_dir[out_dir_len - 1] = 0;
+  }
+  return WFE_OK;
+}
+
 int wfe_get_flags(const wfe_ctx* c, int flags[10]) {
   if (!c || !flags) return WFE_ERR_ARG;
   const CaseSetup& cs = c->cs;
