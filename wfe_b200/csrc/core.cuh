@@ -72,6 +72,11 @@ struct DBase {
 template <typename R>
 struct DCoef {
   const R *rtjx, *rtjy, *kt3, *aw;
+  // per level (pz entries): 1/dzeta_c, 1/dzeta_w, 1 - zeta_w/zt, 1 - zeta_c/zt,
+  // 1/(zeta_c[k+1] - zeta_c[k-1]); the step multiplies by these instead of
+  // dividing by the metric in every substep
+  const R *inv_dzc, *inv_dzw, *fac_w, *fac_c, *inv_dzc2;
+  R inv_dx, inv_dy;
 };
 
 // Dynamics parameters (src/dynamics/params.hpp:8-25).

@@ -154,6 +154,50 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
   return a.v_in[c] + a.dtau * (-Phys<R>::cp * thbv * mv * grad + a.tv[c]);
 }
 
+// Both faces of an interior point: the cell values at (i,j), (i-1,j) and
+// (i,j-1) are computed once for the u and the v face (kernels.cu:499-526).
+template <typename R>
+__device__ __forceinline__ void uv_pair_interior(const AcouArgs<R>& a, int i, int j, int k) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k), c2 = L.at2(i, j);
+  const size_t sy = L.px, pl = L.plane();
+  const R tv0 = theta_v_at(a, c), tvx = theta_v_at(a, c - 1), tvy = theta_v_at(a, c - sy);
+  const R ps0 = pistar_at(a, c), psx = pistar_at(a, c - 1), psy = pistar_at(a, c - sy);
+  const R m0 = a.m.mapf[c2];
+  const R fc = a.co.fac_c[kk];
+  {
+    R thb_f = (R)0.5 * (tvx + tv0);
+    R mf = (R)0.5 * (a.m.mapf[c2 - 1] + m0);
+    R grad = (ps0 - psx) * a.co.inv_dx;
+    R slope = a.m.hx_u[c2] * fc;
+    if (slope != (R)0) {
+      R jf = (R)0.5 * (a.m.jac[c2 - 1] + a.m.jac[c2]);
+      R dpdz = (R)0.5 *
+               ((pistar_at(a, c - 1 + pl) - pistar_at(a, c - 1 - pl)) +
+                (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
+               a.co.inv_dzc2[kk];
+      grad -= slope / jf * dpdz;
+    }
+    a.u_out[c] = a.u_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tu[c]);
+  }
+  {
+    R thb_f = (R)0.5 * (tvy + tv0);
+    R mf = (R)0.5 * (a.m.mapf[c2 - sy] + m0);
+    R grad = (ps0 - psy) * a.co.inv_dy;
+    R slope = a.m.hy_v[c2] * fc;
+    if (slope != (R)0) {
+      R jf = (R)0.5 * (a.m.jac[c2 - sy] + a.m.jac[c2]);
+      R dpdz = (R)0.5 *
+               ((pistar_at(a, c - sy + pl) - pistar_at(a, c - sy - pl)) +
+                (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
+               a.co.inv_dzc2[kk];
+      grad -= slope / jf * dpdz;
+    }
+    a.v_out[c] = a.v_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tv[c]);
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
   const Layout& L = a.L;
@@ -161,6 +205,10 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   const int j = by * blockDim.y + threadIdx.y;
   const int k = bz * blockDim.z + threadIdx.z;
   if (i > L.nx || j > L.ny || k >= L.nz) return;
+  if (i >= 1 && i < L.nx && j >= 1 && j < L.ny && k >= 1 && k < L.nz - 1) {
+    uv_pair_interior(a, i, j, k);
+    return;
+  }
   const int kk = L.at1(k);
   const R cstar = a.p.cstar;
   if (j < L.ny) {  // u on x faces 0..nx
@@ -248,14 +296,18 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
   const int i = bx * CX + tx;
   const int j = by;
   const bool active = i < L.nx;
-  const R dtau = a.dtau, zt = a.m.zt;
+  const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
   const size_t c2d = L.at2(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
-  const R* u = a.u_out;
-  const R* v = a.v_out;
-  const long sx = 1, sy = L.px;
+  const R invJ = (R)1 / J;
+  const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
+  const bool terrain = hxc != (R)0 || hyc != (R)0;
+  const R* __restrict__ u = a.u_out;
+  const R* __restrict__ v = a.v_out;
+  const size_t sx = 1, sy = L.px, pl = L.plane();
+  const size_t c0 = L.at(active ? i : 0, j, 0);  // level k at c0 + k * pl
 #define SM(X, k) S.X[(size_t)(k) * CX + tx]
 
   // phase 1: Av = rho^w theta_v^w (0 at the rigid levels) and the explicit
@@ -265,14 +317,13 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
     for (int k = lane_k; k <= nz; k += KL) {
       R av = 0, sv = 0;
       if (k >= 1 && k < nz) {
-        const int kk = L.at1(k);
-        const size_t c = L.at(i, j, k);
+        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
         av = a.co.aw[c];
-        R fac = (R)1 - a.m.zeta_w[kk] / zt;
-        const size_t cm = c - (size_t)L.plane();
-        R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
-        R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
-        sv = av * (uw * hxc + vw * hyc) * fac;
+        if (terrain) {
+          R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+          R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+          sv = av * (uw * hxc + vw * hyc) * a.co.fac_w[L.at1(k)];
+        }
       }
       SM(Av, k) = av;
       SM(Sv, k) = sv;
@@ -283,18 +334,18 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
 #pragma unroll 4
     for (int k = lane_k; k < nz; k += KL) {
       const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const size_t c = c0 + (size_t)k * pl;
       R Kt = a.co.kt3[c];
-      R Dh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
-                   (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
-      R dzc = a.m.dzeta_c[kk];
-      R wk = a.w_in[c], wkp = a.w_in[c + L.plane()];
+      R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * mcx +
+             (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * mcy;
+      R idz = a.co.inv_dzc[kk];
+      R wk = a.w_in[c], wkp = a.w_in[c + pl];
       R tpi = a.tpi ? a.tpi[c] : (R)0;
       SM(P, k) = a.pi_cur[c] + dtau * tpi -
                  dtau * Kt *
-                     (Dh - (SM(Sv, k + 1) - SM(Sv, k)) / dzc +
-                      c2 * (SM(Av, k + 1) * wkp - SM(Av, k) * wk) / dzc);
-      SM(E, k) = dtau * Kt * c1 / dzc;
+                     (Dh - (SM(Sv, k + 1) - SM(Sv, k)) * idz +
+                      c2 * (SM(Av, k + 1) * wkp - SM(Av, k) * wk) * idz);
+      SM(E, k) = dtau * Kt * c1 * idz;
     }
   __syncthreads();
   // phase 3: tridiagonal rows for w at inner levels (kernels.cu:589-611)
@@ -302,39 +353,57 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
 #pragma unroll 4
     for (int k = 1 + lane_k; k < nz; k += KL) {
       const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+      const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+      const R iJdz = invJ * a.co.inv_dzw[kk];
       R thc = a.th_in[c], thm = a.th_in[cm];
-      R thvw = a.b.thbw[c] + (R)0.5 * (thm + thc);
+      R thbw = a.b.thbw[c];
+      R thvw = thbw + (R)0.5 * (thm + thc);
       if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
-      R G = dtau * Phys<R>::cp * thvw * c1 / (J * a.m.dzeta_w[kk]);
+      R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
       R Em = SM(E, k - 1), Ek = SM(E, k);
       SM(A, k) = -G * Em * SM(Av, k - 1);
       SM(B, k) = (R)1 + G * SM(Av, k) * (Ek + Em);
       SM(C, k) = -G * Ek * SM(Av, k + 1);
-      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / a.b.thbw[c];
+      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
       if (a.p.moisture) {
         R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
         R qcr = (R)0.5 * (a.qc[cm] + a.qc[c]) + (R)0.5 * (a.qr[cm] + a.qr[c]);
         buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
       }
       R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
-              dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) / (J * a.m.dzeta_w[kk]);
+              dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) * iJdz;
       SM(D, k) = RHS - G * (SM(P, k) - SM(P, k - 1));
     }
   __syncthreads();
-  // phase 4: Thomas sweep, one lane per column (kernels.cu:612-634)
+  // phase 4: Thomas sweep, one lane per column (kernels.cu:612-634), one
+  // reciprocal per level; the next level's row is read before this level's
+  // results are stored
   if (active && lane_k == 0) {
+    R cprev = 0, dprev = 0;
+    R Ak = SM(A, 1), Bk = SM(B, 1), Ck = SM(C, 1), Dk = SM(D, 1);
     for (int k = 1; k < nz; ++k) {
-      R Ck = SM(C, k), Dk = SM(D, k), Bk = SM(B, k);
-      if (k == 1) {
-        SM(C, k) = Ck / Bk;
-        SM(D, k) = Dk / Bk;
-      } else {
-        R Ak = SM(A, k);
-        R mm = Bk - Ak * SM(C, k - 1);
-        SM(C, k) = Ck / mm;
-        SM(D, k) = (Dk - Ak * SM(D, k - 1)) / mm;
+      R An = 0, Bn = 1, Cn = 0, Dn = 0;
+      if (k + 1 < nz) {
+        An = SM(A, k + 1);
+        Bn = SM(B, k + 1);
+        Cn = SM(C, k + 1);
+        Dn = SM(D, k + 1);
       }
+      R r, ck, dk;
+      if (k == 1) {
+        r = (R)1 / Bk;
+        ck = Ck * r;
+        dk = Dk * r;
+      } else {
+        r = (R)1 / (Bk - Ak * cprev);
+        ck = Ck * r;
+        dk = (Dk - Ak * dprev) * r;
+      }
+      SM(C, k) = ck;
+      SM(D, k) = dk;
+      cprev = ck;
+      dprev = dk;
+      Ak = An, Bk = Bn, Ck = Cn, Dk = Dn;
     }
     SM(Wn, nz) = 0;
     R wabove = 0;
@@ -343,7 +412,6 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
       SM(Wn, k) = wk;
       wabove = wk;
     }
-    const size_t c0 = L.at(i, j, 0);
     R us = (R)0.5 * (u[c0] + u[c0 + sx]);
     R vs = (R)0.5 * (v[c0] + v[c0 + sy]);
     SM(Wn, 0) = us * hxc + vs * hyc;
@@ -353,7 +421,7 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
   if (active)
 #pragma unroll 4
     for (int k = lane_k; k <= nz; k += KL) {
-      const size_t c = L.at(i, j, k);
+      const size_t c = c0 + (size_t)k * pl;
       if (k < nz) {
         R wn = SM(Wn, k), wn1 = SM(Wn, k + 1);
         a.pi_next[c] = SM(P, k) - SM(E, k) * (SM(Av, k + 1) * wn1 - SM(Av, k) * wn);
@@ -368,13 +436,13 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
 }
 
 template <typename R, int CX, int KL>
-__global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
+__global__ void __launch_bounds__(CX * KL, 1024 / (CX * KL)) k_acoustic_column(AcouArgs<R> a) {
   column_body<R, CX, KL>(a, blockIdx.x, blockIdx.y);
 }
 // the shared column arrays are reused by the next work item only after the
 // barrier that opens it
 template <typename R, int CX, int KL>
-__global__ void __launch_bounds__(CX * KL) k_acoustic_column_batch(Batch<AcouArgs<R>> b) {
+__global__ void __launch_bounds__(CX * KL, 1024 / (CX * KL)) k_acoustic_column_batch(Batch<AcouArgs<R>> b) {
   for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int) { column_body<R, CX, KL>(a, x, y); });
 }
 

@@ -170,7 +170,29 @@ class ModelT final : public Model {
     launch_acoustic_coef<R>(L_, db_, dm_, scratch, rtjx_, rtjy_, kt3_, aw_, st_);
     CK(cudaStreamSynchronize(st_));
     CK(cudaGetLastError());
-    co_ = DCoef<R>{rtjx_, rtjy_, kt3_, aw_};
+    {
+      // per-level reciprocals and terrain-following factors of the metric
+      std::vector<double> lv[5];
+      for (auto& v : lv) v.assign(n1, 0.0);
+      const double zt = cs.m.zt;
+      for (size_t q = 0; q < n1; ++q) {
+        const double dzc = cs.m.dzeta_c[q], dzw = cs.m.dzeta_w[q];
+        lv[0][q] = dzc != 0 ? 1.0 / dzc : 0.0;
+        lv[1][q] = dzw != 0 ? 1.0 / dzw : 0.0;
+        lv[2][q] = 1.0 - cs.m.zeta_w[q] / zt;
+        lv[3][q] = 1.0 - cs.m.zeta_c[q] / zt;
+        if (q >= 1 && q + 1 < n1) {
+          const double d2 = cs.m.zeta_c[q + 1] - cs.m.zeta_c[q - 1];
+          lv[4][q] = d2 != 0 ? 1.0 / d2 : 0.0;
+        }
+      }
+      R* lb = alloc(5 * n1);
+      if (!lb) return 1;
+      for (int q = 0; q < 5; ++q)
+        if (put1d(lb + q * n1, lv[q])) return 1;
+      co_ = DCoef<R>{rtjx_, rtjy_, kt3_, aw_, lb, lb + n1, lb + 2 * n1, lb + 3 * n1, lb + 4 * n1,
+                     (R)(1.0 / g_.dx), (R)(1.0 / g_.dy)};
+    }
     if (!(rain_ = alloc(n2))) return 1;
     CK(cudaMalloc(&clock_, CLK_N * sizeof(double)));
     CK(cudaMemset(clock_, 0, CLK_N * sizeof(double)));
