@@ -76,6 +76,7 @@ struct DCoef {
   // 1/(zeta_c[k+1] - zeta_c[k-1]); the step multiplies by these instead of
   // dividing by the metric in every substep
   const R *inv_dzc, *inv_dzw, *fac_w, *fac_c, *inv_dzc2;
+  const R *spg_c, *spg_w;  // Rayleigh coefficient at the cell / w levels
   R inv_dx, inv_dy;
 };
 

@@ -141,9 +141,9 @@ __global__ void k_mass_flux_batch(Batch<FluxArgs<R>> b) {
 template <typename R>
 __device__ __forceinline__ R divergence(const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
-  return (a.mfx[L.at(i + 1, j, k)] - a.mfx[L.at(i, j, k)]) / a.dx +
-         (a.mfy[L.at(i, j + 1, k)] - a.mfy[L.at(i, j, k)]) / a.dy +
-         (a.mfz[L.at(i, j, k + 1)] - a.mfz[L.at(i, j, k)]) / a.m.dzeta_c[L.at1(k)];
+  const size_t c = L.at(i, j, k);
+  return (a.mfx[c + 1] - a.mfx[c]) * a.co.inv_dx + (a.mfy[c + L.px] - a.mfy[c]) * a.co.inv_dy +
+         (a.mfz[c + L.plane()] - a.mfz[c]) * a.co.inv_dzc[L.at1(k)];
 }
 
 // Flux-form advection of a cell-centred scalar (kernels.cu:114-179).
@@ -163,7 +163,7 @@ __device__ __forceinline__ R scalar_adv(const TendArgs<R>& a, const R* __restric
   R FyR = fyR * face5(Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], Q[3 * sy], fyR);
   R FzB = fzB * face5(Q[-3 * (long)sz], Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], fzB);
   R FzT = fzT * face5(Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], Q[3 * sz], fzT);
-  R fdiv = (FxR - FxL) / a.dx + (FyR - FyL) / a.dy + (FzT - FzB) / a.m.dzeta_c[L.at1(k)];
+  R fdiv = (FxR - FxL) * a.co.inv_dx + (FyR - FyL) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[L.at1(k)];
   R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
   return (-fdiv + Q[0] * div) / rt;
 }
@@ -269,7 +269,7 @@ __device__ __forceinline__ R pd_adv(const TendArgs<R>& a, const R* q, const R* r
     szl = fzl * ratio_at(a, ratio, i, j, fzl >= (R)0 ? k - 1 : k);
     szr = fzr * ratio_at(a, ratio, i, j, fzr >= (R)0 ? k : k + 1);
   }
-  R fdiv = (sxr - sxl) / a.dx + (syr - syl) / a.dy + (szr - szl) / a.m.dzeta_c[L.at1(k)];
+  R fdiv = (sxr - sxl) * a.co.inv_dx + (syr - syl) * a.co.inv_dy + (szr - szl) * a.co.inv_dzc[L.at1(k)];
   R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
   return (-fdiv + q[L.at(i, j, k)] * div) / rt;
 }
@@ -336,7 +336,6 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
   const int kk = L.at1(k);
   const size_t c = L.at(i, j, k);
   const long sx = 1, sy = L.px, sz = (long)L.plane();
-  const R zt = a.m.zt;
   const bool bdy = a.lo[0] != nullptr;
   const R* MX = a.mfx + c;
   const R* MY = a.mfy + c;
@@ -355,13 +354,13 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     R fzB = (R)0.5 * (MZ[-sx] + MZ[0]), fzT = (R)0.5 * (MZ[sz - sx] + MZ[sz]);
     R FzB = fzB * face5(U[-3 * sz], U[-2 * sz], U[-sz], U[0], U[sz], U[2 * sz], fzB);
     R FzT = fzT * face5(U[-2 * sz], U[-sz], U[0], U[sz], U[2 * sz], U[3 * sz], fzT);
-    R fdiv = (FxR - FxL) / a.dx + (FyT - FyB) / a.dy + (FzT - FzB) / a.m.dzeta_c[kk];
+    R fdiv = (FxR - FxL) * a.co.inv_dx + (FyT - FyB) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[kk];
     R dv = (R)0.5 * (divergence(a, i - 1, j, k) + div0);
     R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
     const R* V = a.v + c;
     R vavg = (R)0.25 * (V[-sx] + V[sy - sx] + V[0] + V[sy]);
     R fc = (R)0.5 * (a.m.fcor[L.at2(i - 1, j)] + a.m.fcor[L.at2(i, j)]);
-    R relax = -sponge(a.m.zeta_c[kk], zt, a.p) * (U[0] - a.b.ub[kk]);
+    R relax = -a.co.spg_c[kk] * (U[0] - a.b.ub[kk]);
     R t = (-fdiv + U[0] * dv) / ru + fc * vavg + relax;
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.u, i, j, k, false);
     if (bdy) t += davies(a, 0, a.u, i, j, k);
@@ -379,14 +378,14 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     R fzB = (R)0.5 * (MZ[-sy] + MZ[0]), fzT = (R)0.5 * (MZ[sz - sy] + MZ[sz]);
     R FzB = fzB * face5(V[-3 * sz], V[-2 * sz], V[-sz], V[0], V[sz], V[2 * sz], fzB);
     R FzT = fzT * face5(V[-2 * sz], V[-sz], V[0], V[sz], V[2 * sz], V[3 * sz], fzT);
-    R fdiv = (FxR - FxL) / a.dx + (FyT - FyB) / a.dy + (FzT - FzB) / a.m.dzeta_c[kk];
+    R fdiv = (FxR - FxL) * a.co.inv_dx + (FyT - FyB) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[kk];
     R dv = (R)0.5 * (divergence(a, i, j - 1, k) + div0);
     R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
     const R* U = a.u + c;
     R uavg = (R)0.25 * (U[-sy] + U[sx - sy] + U[0] + U[sx]);
     R fc = (R)0.5 * (a.m.fcor[L.at2(i, j - 1)] + a.m.fcor[L.at2(i, j)]);
     R uref = a.p.coriolis_use_ub ? a.b.ub[kk] : (R)0;
-    R relax = -sponge(a.m.zeta_c[kk], zt, a.p) * V[0];
+    R relax = -a.co.spg_c[kk] * V[0];
     R t = (-fdiv + V[0] * dv) / rv - fc * (uavg - uref) + relax;
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.v, i, j, k, false);
     if (bdy) t += davies(a, 1, a.v, i, j, k);
@@ -404,10 +403,10 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     R fzB = (R)0.5 * (MZ[-sz] + MZ[0]), fzT = (R)0.5 * (MZ[0] + MZ[sz]);
     R FzB = fzB * face5(W[-3 * sz], W[-2 * sz], W[-sz], W[0], W[sz], W[2 * sz], fzB);
     R FzT = fzT * face5(W[-2 * sz], W[-sz], W[0], W[sz], W[2 * sz], W[3 * sz], fzT);
-    R fdiv = (FxR - FxL) / a.dx + (FyT - FyB) / a.dy + (FzT - FzB) / a.m.dzeta_w[kk];
+    R fdiv = (FxR - FxL) * a.co.inv_dx + (FyT - FyB) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzw[kk];
     R dv = (R)0.5 * (divergence(a, i, j, k - 1) + div0);
     R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
-    R relax = -sponge(a.m.zeta_w[kk], zt, a.p) * W[0];
+    R relax = -a.co.spg_w[kk] * W[0];
     R wk = W[0];
     if (a.p.w_damping) {
       R cr = fabs(wk) * a.dt / (a.m.dzeta_w[kk] * a.m.jac[L.at2(i, j)]);
@@ -420,7 +419,7 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
   if (!(PART & TEND_SCAL)) return;
   // ---- theta' (kernels.cu:114-146)
   {
-    R t = scalar_adv(a, a.thp, i, j, k, div0) - sponge(a.m.zeta_c[kk], zt, a.p) * a.thp[c];
+    R t = scalar_adv(a, a.thp, i, j, k, div0) - a.co.spg_c[kk] * a.thp[c];
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.thp, i, j, k, false);
     if (bdy) t += davies(a, 2, a.thp, i, j, k);
     a.tth[c] = t;

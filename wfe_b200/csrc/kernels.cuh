@@ -22,6 +22,7 @@ struct TendArgs {
   DBase<R> b;
   DMetric<R> m;
   DParams<R> p;
+  DCoef<R> co;  // per-level reciprocals and Rayleigh coefficients
   R dx, dy, dt;                                   // grid spacing, large step
   const R *u, *v, *w, *thp, *pip, *qv, *qc, *qr;  // stage estimate, ghosts filled
   const R *mfx, *mfy, *mfz;                       // mass fluxes on the ring

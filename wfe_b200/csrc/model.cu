@@ -172,9 +172,16 @@ class ModelT final : public Model {
     CK(cudaGetLastError());
     {
       // per-level reciprocals and terrain-following factors of the metric
-      std::vector<double> lv[5];
+      std::vector<double> lv[7];
       for (auto& v : lv) v.assign(n1, 0.0);
       const double zt = cs.m.zt;
+      // Rayleigh sponge coefficient (src/dynamics/kernels.cu:42-48)
+      auto sponge = [&](double zeta) {
+        const double zd = hp_.rayleigh_zd;
+        if (zd < 0 || zeta <= zd || zt <= zd) return 0.0;
+        double sn = std::sin(1.5707963267948966 * (zeta - zd) / (zt - zd));
+        return hp_.rayleigh_alpha * sn * sn;
+      };
       for (size_t q = 0; q < n1; ++q) {
         const double dzc = cs.m.dzeta_c[q], dzw = cs.m.dzeta_w[q];
         lv[0][q] = dzc != 0 ? 1.0 / dzc : 0.0;
@@ -185,13 +192,16 @@ class ModelT final : public Model {
           const double d2 = cs.m.zeta_c[q + 1] - cs.m.zeta_c[q - 1];
           lv[4][q] = d2 != 0 ? 1.0 / d2 : 0.0;
         }
+        lv[5][q] = sponge(cs.m.zeta_c[q]);
+        lv[6][q] = sponge(cs.m.zeta_w[q]);
       }
-      R* lb = alloc(5 * n1);
+      R* lb = alloc(7 * n1);
       if (!lb) return 1;
-      for (int q = 0; q < 5; ++q)
+      for (int q = 0; q < 7; ++q)
         if (put1d(lb + q * n1, lv[q])) return 1;
-      co_ = DCoef<R>{rtjx_, rtjy_, kt3_, aw_, lb, lb + n1, lb + 2 * n1, lb + 3 * n1, lb + 4 * n1,
-                     (R)(1.0 / g_.dx), (R)(1.0 / g_.dy)};
+      co_ = DCoef<R>{rtjx_,      rtjy_,      kt3_,       aw_,        lb,
+                     lb + n1,    lb + 2 * n1, lb + 3 * n1, lb + 4 * n1, lb + 5 * n1,
+                     lb + 6 * n1, (R)(1.0 / g_.dx), (R)(1.0 / g_.dy)};
     }
     if (!(rain_ = alloc(n2))) return 1;
     CK(cudaMalloc(&clock_, CLK_N * sizeof(double)));
@@ -773,6 +783,7 @@ class ModelT final : public Model {
     a.b = db_;
     a.m = dm_;
     a.p = dp_;
+    a.co = co_;
     a.dx = (R)g_.dx;
     a.dy = (R)g_.dy;
     a.dt = dt;
