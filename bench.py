@@ -224,13 +224,19 @@ def run_reference(args) -> dict:
 
 def e2e_run(W, case_ini, steps: int, device: int):
     """End to end through the public API with host buffers, at the reference
-    driver's cadence (src/main.cpp:425-467): initial state uploaded from host,
-    every step the |w| watchdog read back, diagnostics (w, theta', pi', qc, qr)
-    every diag_interval and the full state every out_interval downloaded."""
+    driver's cadence (src/main.cpp:425-467): initial state uploaded from
+    page-locked host buffers, every step the |w| watchdog read back,
+    diagnostics (w, theta', pi', qc, qr) every diag_interval and the full state
+    and rain every out_interval downloaded as asynchronous snapshots (packed on
+    the device, copied to page-locked buffers while the next steps run)."""
     import numpy as np
 
     c = W.Case(case_ini, precision="f32", device=device)
-    host = {k: c.field(k, interior=True, dtype=np.float32) for k in W.FIELDS}
+    host = c.snapshot_buffers(W.FIELDS)  # page-locked, interior layout
+    for k in W.FIELDS:
+        host[k][...] = c.field(k, interior=True, dtype=np.float32)
+    diag = c.snapshot_buffers(("w", "thp", "pip", "qc", "qr"))
+    full = c.snapshot_buffers(list(W.FIELDS) + ["rain"])
     diag_every = max(1, round(120.0 / c.dt))
     out_every = max(1, round(600.0 / c.dt))
     h2d = d2h = 0
@@ -245,13 +251,14 @@ def e2e_run(W, case_ini, steps: int, device: int):
         d2h += 4
         if not wmax < 150.0:
             raise RuntimeError(f"|w| watchdog tripped at step {s}: {wmax}")
+        # snapshots are packed on the device and copied while later steps run
         if s % diag_every == 0:
-            for k in ("w", "thp", "pip", "qc", "qr"):
-                d2h += c.field(k, interior=True, dtype=np.float32).nbytes
+            c.snapshot_begin(diag)
+            d2h += sum(a.nbytes for a in diag.values())
         if s % out_every == 0 or s == steps:
-            for k in W.FIELDS:
-                d2h += c.field(k, interior=True, dtype=np.float32).nbytes
-            d2h += c.rain(interior=True).astype(np.float32).nbytes
+            c.snapshot_begin(full)
+            d2h += sum(a.nbytes for a in full.values())
+    c.snapshot_wait()
     c.sync()
     el = time.perf_counter() - t0
     cells = c.nx * c.ny * c.nz

@@ -131,6 +131,22 @@ int wfe_time_run(wfe_ctx* ctx, int nsteps, double dt, double t0, double* ms);
 int wfe_kernel_times(wfe_ctx* ctx, double dt, double t, int cap, double* total_ms, int* counts,
                      char* names_csv, int names_len, int* n_out);
 
+/* Asynchronous snapshot (no reference counterpart; replaces the Writer's
+ * blocking cudaMemcpy of a padded field and its host repack,
+ * src/io/writer.cpp:89-107).  Each requested field -- WFE_U..WFE_QR, or
+ * WFE_SNAP_2D + WFE_2D_* -- is packed on the device into the interior layout
+ * (float32 for WFE_DTYPE_F32, else float64) on the library's stream, in order
+ * with the steps already issued, then copied into host[q] on a separate copy
+ * stream, so steps issued afterwards overlap the transfer.  The host buffers
+ * (interior_count elements each) are complete after wfe_snapshot_wait; a new
+ * wfe_snapshot_begin waits for the previous one first.  For the copies to be
+ * asynchronous the buffers must be page-locked: wfe_host_alloc. */
+enum { WFE_SNAP_2D = 100 };
+int wfe_snapshot_begin(wfe_ctx* ctx, int n, const int* fields, void* const* host, int dtype);
+int wfe_snapshot_wait(wfe_ctx* ctx);
+void* wfe_host_alloc(size_t bytes); /* page-locked host memory, NULL on failure */
+int wfe_host_free(void* p);
+
 /* ------------------------------------------------- operator-level API */
 /* apply_bcs (src/dynamics/kernels.cu:805-835) on the state */
 int wfe_op_apply_bcs(wfe_ctx* ctx);

@@ -21,7 +21,7 @@ RUN_CASES = ["bubble_open", "straka_periodic", "schaer_open", "wk82_small", "moi
 
 def header_symbols():
     text = (ROOT / "include" / "wfe_b200.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|long|const char\*)\s+(wfe_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long|const char\*|void\*)\s+(wfe_\w+)\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():

@@ -164,3 +164,27 @@ def test_interior_transfers_roundtrip(prec):
         mask = np.ones(c.shape, bool)
         mask[g:g + nzl, g:g + c.ny, g:g + c.nx] = False
         assert np.array_equal(pad[mask], before[mask])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_async_snapshot_equals_interior_download(prec):
+    c = W.Case(CASES / "wk82_small.ini", precision=prec)
+    c.run(3)
+    names = list(W.FIELDS) + ["rain"]
+    for dt in (np.float32, np.float64):
+        bufs = c.snapshot_buffers(names, dtype=dt)
+        c.snapshot_begin(bufs)
+        c.run(2)  # steps issued after the snapshot do not change it
+        c.snapshot_wait()
+        c2 = None
+        for k in names:
+            assert bufs[k].dtype == dt
+        # the state 2 steps ago: redo on a twin case for the reference values
+        c2 = W.Case(CASES / "wk82_small.ini", precision=prec)
+        c2.run(3 if dt is np.float32 else 5)
+        for k in W.FIELDS:
+            assert np.array_equal(bufs[k], c2.field(k, interior=True, dtype=dt)), k
+        assert np.array_equal(bufs["rain"], c2.rain(interior=True).astype(dt))
+        c2.close()
+    c.close()

@@ -50,7 +50,8 @@ SYMBOLS = [
     "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
     "wfe_ensemble_step", "wfe_ensemble_sync", "wfe_ensemble_time_run",
     "wfe_ensemble_launches_per_step", "wfe_ensemble_variants", "wfe_lin_enable", "wfe_lin_zero",
-    "wfe_tl_run", "wfe_ad_run", "wfe_get_run_config",
+    "wfe_tl_run", "wfe_ad_run", "wfe_get_run_config", "wfe_snapshot_begin", "wfe_snapshot_wait",
+    "wfe_host_alloc", "wfe_host_free",
 ]
 
 
@@ -110,6 +111,11 @@ def load_library(path: str | Path | None = None):
         [vp] * 11
     lib.wfe_kernel_times.argtypes = [vp, C.c_double, C.c_double, C.c_int, dp, ip, C.c_char_p,
                                      C.c_int, ip]
+    lib.wfe_snapshot_begin.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.c_int]
+    lib.wfe_snapshot_wait.argtypes = [vp]
+    lib.wfe_host_alloc.argtypes = [C.c_size_t]
+    lib.wfe_host_alloc.restype = vp
+    lib.wfe_host_free.argtypes = [vp]
     lib.wfe_lin_enable.argtypes = [vp]
     lib.wfe_lin_zero.argtypes = [vp]
     lib.wfe_tl_run.argtypes = [vp, C.c_int, C.c_double, C.c_double]
@@ -126,6 +132,22 @@ def load_library(path: str | Path | None = None):
     if path is None:
         _lib = lib
     return lib
+
+
+class _PinnedArray:
+    """numpy array over page-locked memory from wfe_host_alloc (freed with it)"""
+
+    def __init__(self, lib, shape, dtype):
+        self._lib = lib
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self._p = lib.wfe_host_alloc(max(n, 1))
+        if not self._p:
+            raise WfeError(2, "wfe_host_alloc failed")
+        buf = (C.c_char * max(n, 1)).from_address(self._p)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+        self.array.flags.writeable = True
+        # the array keeps this owner alive
+        self._finalizer = __import__("weakref").finalize(self.array, lib.wfe_host_free, self._p)
 
 
 def _dptr(a: np.ndarray):
@@ -316,6 +338,29 @@ class Case:
                 (tsk, land, lat, lon, soilw)]
         self._check(self._lib.wfe_set_physics(self._h, *[_dptr(a) for a in arrs], start_hour,
                                               int(doy), int(nonlocal_pbl)))
+
+    # ------------------------------------------------- async snapshots
+    def snapshot_buffers(self, names, dtype=np.float32) -> dict:
+        """page-locked host arrays (interior layout) for snapshot_begin"""
+        out = {}
+        for k in names:
+            shape = ((self.ny, self.nx) if k in F2D else
+                     ((self.nz + 1 if k == "w" else self.nz), self.ny, self.nx))
+            out[k] = _PinnedArray(self._lib, shape, dtype).array
+        return out
+
+    def snapshot_begin(self, bufs: dict) -> None:
+        """pack the named fields on the device and start their copies into the
+        arrays of snapshot_buffers (complete after snapshot_wait)"""
+        names = list(bufs)
+        ids = (C.c_int * len(names))(*[(100 + F2D[k]) if k in F2D else FIELD_ID[k]
+                                       for k in names])
+        ptrs = (C.c_void_p * len(names))(*[bufs[k].ctypes.data for k in names])
+        dt = 1 if next(iter(bufs.values())).dtype == np.float32 else 0
+        self._check(self._lib.wfe_snapshot_begin(self._h, len(names), ids, ptrs, dt))
+
+    def snapshot_wait(self) -> None:
+        self._check(self._lib.wfe_snapshot_wait(self._h))
 
     # ---------------------------------------- tangent-linear / adjoint
     def lin_enable(self) -> None:

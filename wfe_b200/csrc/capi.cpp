@@ -1,6 +1,8 @@
 // C-ABI of wfe_b200 (include/wfe_b200.h).
 #include "wfe_b200.h"
 
+#include <cuda_runtime.h>
+
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -564,4 +566,27 @@ int wfe_ad_run(wfe_ctx* c, int nsteps, double dt, double t0, int checkpoint_ever
   if (nsteps < 0) return set_err(c, WFE_ERR_ARG, "nsteps < 0");
   return c->lin->ad_run(nsteps, dt, t0, checkpoint_every) ? set_err(c, WFE_ERR_CUDA, c->lin->error())
                                                            : WFE_OK;
+}
+
+// ------------------------------------------------------------- snapshots
+int wfe_snapshot_begin(wfe_ctx* c, int n, const int* fields, void* const* host, int dtype) {
+  NEED_MODEL(c);
+  if (n < 0 || (n > 0 && (!fields || !host))) return set_err(c, WFE_ERR_ARG, "bad snapshot arguments");
+  for (int q = 0; q < n; ++q)
+    if (!host[q]) return set_err(c, WFE_ERR_ARG, "snapshot host buffer is NULL");
+  return c->model->snapshot_begin(n, fields, host, dtype == WFE_DTYPE_F32) ? model_err(c) : WFE_OK;
+}
+
+int wfe_snapshot_wait(wfe_ctx* c) {
+  NEED_MODEL(c);
+  return c->model->snapshot_wait() ? model_err(c) : WFE_OK;
+}
+
+void* wfe_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  return cudaMallocHost(&p, bytes) == cudaSuccess ? p : nullptr;
+}
+
+int wfe_host_free(void* p) {
+  return cudaFreeHost(p) == cudaSuccess ? WFE_OK : WFE_ERR_CUDA;
 }

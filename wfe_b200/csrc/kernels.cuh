@@ -279,6 +279,13 @@ int prepare_kessler(int nz);
 
 template <typename R>
 int launch_kessler(const KesArgs<R>& a, cudaStream_t st);
+// interior of a 3D field (nzl levels) or of a 2D field into a contiguous
+// float32 (f32) or float64 device buffer in the Writer's layout (io.cu)
+template <typename R>
+void launch_pack_interior(const R* src, const Layout& L, int nzl, void* dst, bool f32,
+                          cudaStream_t st);
+template <typename R>
+void launch_pack_interior2d(const R* src, const Layout& L, void* dst, bool f32, cudaStream_t st);
 template <typename R>
 void launch_absmax(const R* f, size_t n, unsigned int* result, cudaStream_t st);
 template <typename R>

@@ -311,6 +311,50 @@ class ModelT final : public Model {
     return 0;
   }
 
+  int snapshot_begin(int n, const int* fields, void* const* host, bool f32) override {
+    if (snapshot_wait()) return 1;
+    if (!cs_st_) CK(cudaStreamCreateWithFlags(&cs_st_, cudaStreamNonBlocking));
+    if (!snap_ev_) CK(cudaEventCreateWithFlags(&snap_ev_, cudaEventDisableTiming));
+    const size_t es = f32 ? 4 : 8;
+    std::vector<size_t> off(n), bytes(n);
+    size_t total = 0;
+    for (int q = 0; q < n; ++q) {
+      const int f = fields[q];
+      size_t cnt;
+      if (f >= 0 && f < 8) cnt = (size_t)(f == 2 ? g_.nz + 1 : g_.nz) * g_.ny * g_.nx;
+      else if (f >= 100 && field2d(f - 100)) cnt = (size_t)g_.ny * g_.nx;
+      else return fail("snapshot: bad field " + std::to_string(f));
+      off[q] = total;
+      bytes[q] = cnt * es;
+      total += (bytes[q] + 255) / 256 * 256;
+    }
+    if (total > snap_cap_) {
+      if (snap_buf_) cudaFree(snap_buf_);
+      snap_buf_ = nullptr;
+      snap_cap_ = 0;
+      CK(cudaMalloc(&snap_buf_, total));
+      snap_cap_ = total;
+    }
+    for (int q = 0; q < n; ++q) {
+      const int f = fields[q];
+      char* dst = static_cast<char*>(snap_buf_) + off[q];
+      if (f < 8) launch_pack_interior<R>(S_[perm_[0]][f], L_, f == 2 ? g_.nz + 1 : g_.nz, dst, f32, st_);
+      else launch_pack_interior2d<R>(field2d(f - 100), L_, dst, f32, st_);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(snap_ev_, st_));
+    CK(cudaStreamWaitEvent(cs_st_, snap_ev_, 0));
+    for (int q = 0; q < n; ++q)
+      CK(cudaMemcpyAsync(host[q], static_cast<char*>(snap_buf_) + off[q], bytes[q],
+                         cudaMemcpyDeviceToHost, cs_st_));
+    return 0;
+  }
+
+  int snapshot_wait() override {
+    if (cs_st_) CK(cudaStreamSynchronize(cs_st_));
+    return 0;
+  }
+
   int upload_state_raw(int field, const void* host) override {
     if (field < 0 || field > 7) return fail("bad field");
     CK(cudaMemcpyAsync(S_[perm_[0]][field], host, L_.n3() * sizeof(R), cudaMemcpyHostToDevice, st_));
@@ -1051,6 +1095,15 @@ class ModelT final : public Model {
     if (mass_planes_) cudaFree(mass_planes_);
     if (mass_) cudaFree(mass_);
     if (stage_) cudaFreeHost(stage_);
+    if (cs_st_) {
+      cudaStreamSynchronize(cs_st_);
+      cudaStreamDestroy(cs_st_);
+    }
+    if (snap_ev_) cudaEventDestroy(snap_ev_);
+    if (snap_buf_) cudaFree(snap_buf_);
+    cs_st_ = nullptr;
+    snap_ev_ = nullptr;
+    snap_buf_ = nullptr;
     if (st_) cudaStreamDestroy(st_);
     clock_ = nullptr;
     wd_ = nullptr;
@@ -1105,6 +1158,10 @@ class ModelT final : public Model {
   bool graphs_valid_ = false;
   long gen_ = 0;  // changes whenever buffer roles or physics switches change
   std::vector<Rec>* rec_ = nullptr;  // record mode when set
+  cudaStream_t cs_st_ = nullptr;     // snapshot copy stream
+  cudaEvent_t snap_ev_ = nullptr;
+  void* snap_buf_ = nullptr;         // packed snapshot staging
+  size_t snap_cap_ = 0;
   std::function<void*(const void*)> lin_map_;
   double graph_dt_ = 0;
   long launches_ = 0, glaunches_ = 0;

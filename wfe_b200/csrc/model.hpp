@@ -48,6 +48,13 @@ class Model {
   virtual size_t pitched_count() const = 0;
   virtual void pitched_dims(int* px, int* py, int* pz) const = 0;
 
+  // Asynchronous snapshot: fields 0..7 (state) and 100 + Field2D (2D fields)
+  // packed on the device in step order, copied to the host buffers on a copy
+  // stream; the buffers are complete after snapshot_wait (which a new
+  // snapshot_begin also does first)
+  virtual int snapshot_begin(int n, const int* fields, void* const* host, bool f32) = 0;
+  virtual int snapshot_wait() = 0;
+
   // Integrator::step (src/dynamics/integrator.cpp:71-111): direct launches
   virtual int step(double dt, double t) = 0;
   // nsteps large steps replayed from captured CUDA graphs
