@@ -579,218 +579,266 @@ __global__ void __launch_bounds__(256) k_ad_uv(AcouArgs<R> a, AcouArgs<R> d) {
 }
 
 // ================================================================ w - pi' column
-constexpr int kLinNZ = 80;  // deepest column (+1) the linearised column kernels hold
+// A CTA owns LCX columns of one row with LKL level lanes; the column arrays
+// live in shared memory ([level * LCX + column]); the sweeps run in one lane
+// per column, everything else in parallel over the levels.
+constexpr int LCX = 8, LKL = 16;
 
-// tridiagonal solve rows 1..n-1 (row 1 without A, row n-1 without C), the
-// forward's elimination order (kernels.cu:612-634)
+// rows 1..n-1 of a tridiagonal system (row 1 without A, row n-1 without C),
+// the forward's elimination order (kernels.cu:612-634); arrays strided by LCX
 template <typename R>
-__device__ void thomas(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds, R* x) {
+__device__ void thomas_s(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds, R* x) {
+  R cp = 0, dp = 0;
   for (int k = 1; k < n; ++k) {
+    const int q = k * LCX;
     if (k == 1) {
-      cs[k] = C[k] / B[k];
-      ds[k] = D[k] / B[k];
+      cp = C[q] / B[q];
+      dp = D[q] / B[q];
     } else {
-      R m = B[k] - A[k] * cs[k - 1];
-      cs[k] = C[k] / m;
-      ds[k] = (D[k] - A[k] * ds[k - 1]) / m;
+      const R m = B[q] - A[q] * cp;
+      cp = C[q] / m;
+      dp = (D[q] - A[q] * dp) / m;
     }
+    cs[q] = cp;
+    ds[q] = dp;
   }
-  x[n] = 0;
+  x[n * LCX] = 0;
   R above = 0;
   for (int k = n - 1; k >= 1; --k) {
-    R v = ds[k] - cs[k] * above;
-    x[k] = v;
-    above = v;
+    above = ds[k * LCX] - cs[k * LCX] * above;
+    x[k * LCX] = above;
   }
 }
 
-// the transposed system: (M^T)_{k,k-1} = C[k-1], (M^T)_{k,k} = B[k],
-// (M^T)_{k,k+1} = A[k+1] over rows 1..n-1
+// the transposed system: (M^T)_{k,k-1} = C[k-1], (M^T)_{k,k+1} = A[k+1]
 template <typename R>
-__device__ void thomas_t(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds, R* x) {
+__device__ void thomas_ts(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds, R* x) {
+  R cp = 0, dp = 0;
   for (int k = 1; k < n; ++k) {
-    const R sub = k > 1 ? C[k - 1] : (R)0;
-    const R sup = k < n - 1 ? A[k + 1] : (R)0;
+    const int q = k * LCX;
+    const R sub = k > 1 ? C[q - LCX] : (R)0;
+    const R sup = k < n - 1 ? A[q + LCX] : (R)0;
     if (k == 1) {
-      cs[k] = sup / B[k];
-      ds[k] = D[k] / B[k];
+      cp = sup / B[q];
+      dp = D[q] / B[q];
     } else {
-      R m = B[k] - sub * cs[k - 1];
-      cs[k] = sup / m;
-      ds[k] = (D[k] - sub * ds[k - 1]) / m;
+      const R m = B[q] - sub * cp;
+      cp = sup / m;
+      dp = (D[q] - sub * dp) / m;
     }
+    cs[q] = cp;
+    ds[q] = dp;
   }
-  x[n] = 0;
+  x[n * LCX] = 0;
+  x[0] = 0;
   R above = 0;
   for (int k = n - 1; k >= 1; --k) {
-    R v = ds[k] - cs[k] * above;
-    x[k] = v;
-    above = v;
+    above = ds[k * LCX] - cs[k * LCX] * above;
+    x[k * LCX] = above;
   }
 }
 
-// Forward values of one column (kernels.cu:552-634), as the column kernel
-// computes them: Av, Sv, P, E on levels, A, B, C, D, G, thvw on inner levels,
-// and the solution w.
+// shared column arrays: a fixed set of (nz + 1)-level arrays
 template <typename R>
-struct ColVals {
-  R Av[kLinNZ + 1], Sv[kLinNZ + 1], P[kLinNZ], E[kLinNZ];
-  R A[kLinNZ], B[kLinNZ], C[kLinNZ], D[kLinNZ], G[kLinNZ], thvw[kLinNZ];
-  R w[kLinNZ + 1], cs[kLinNZ], ds[kLinNZ];
+struct ColArr {
+  R* base;
+  int n1;  // nz + 1
+  __device__ R* operator[](int q) const { return base + (size_t)q * n1 * LCX; }
 };
 
+// Forward values of one column (kernels.cu:552-634) as the column kernel
+// computes them, into shared arrays: Av, Sv, P, E on levels; G, A, B, C, D on
+// the inner levels; the solution w (with the surface w at level 0).
+enum { V_AV, V_SV, V_P, V_E, V_G, V_A, V_B, V_C, V_D, V_W, V_CS, V_DS, V_N };
+
 template <typename R>
-__device__ void column_values(const AcouArgs<R>& a, int i, int j, ColVals<R>& V) {
+__device__ void column_values_s(const AcouArgs<R>& a, int i, int j, bool active, const ColArr<R>& S) {
   const Layout& L = a.L;
-  const int nz = L.nz;
+  const int nz = L.nz, tx = threadIdx.x, lane = threadIdx.y;
   const R dtau = a.dtau, zt = a.m.zt;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(i, j);
+  const size_t c2d = L.at2(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   const R* u = a.u_out;
   const R* v = a.v_out;
   const long sx = 1, sy = L.px;
-  for (int k = 0; k <= nz; ++k) {
-    R av = 0, sv = 0;
-    if (k >= 1 && k < nz) {
+  R *Av = S[V_AV] + tx, *Sv = S[V_SV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx;
+  R *G = S[V_G] + tx, *A = S[V_A] + tx, *B = S[V_B] + tx, *C = S[V_C] + tx, *D = S[V_D] + tx;
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      R av = 0, sv = 0;
+      if (k >= 1 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = L.at(i, j, k);
+        av = a.co.aw[c];
+        R fac = (R)1 - a.m.zeta_w[kk] / zt;
+        const size_t cm = c - (size_t)L.plane();
+        R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+        R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+        sv = av * (uw * hxc + vw * hyc) * fac;
+      }
+      Av[k * LCX] = av;
+      Sv[k * LCX] = sv;
+    }
+  __syncthreads();
+  if (active)
+    for (int k = lane; k < nz; k += LKL) {
       const int kk = L.at1(k);
       const size_t c = L.at(i, j, k);
-      av = a.co.aw[c];
-      R fac = (R)1 - a.m.zeta_w[kk] / zt;
-      const size_t cm = c - (size_t)L.plane();
-      R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
-      R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
-      sv = av * (uw * hxc + vw * hyc) * fac;
+      R Kt = a.co.kt3[c];
+      R Dh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
+                   (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
+      R dzc = a.m.dzeta_c[kk];
+      R wk = a.w_in[c], wkp = a.w_in[c + L.plane()];
+      R tpi = a.tpi ? a.tpi[c] : (R)0;
+      P[k * LCX] = a.pi_cur[c] + dtau * tpi -
+                   dtau * Kt *
+                       (Dh - (Sv[(k + 1) * LCX] - Sv[k * LCX]) / dzc +
+                        c2 * (Av[(k + 1) * LCX] * wkp - Av[k * LCX] * wk) / dzc);
+      E[k * LCX] = dtau * Kt * c1 / dzc;
     }
-    V.Av[k] = av;
-    V.Sv[k] = sv;
+  __syncthreads();
+  if (active)
+    for (int k = 1 + lane; k < nz; k += LKL) {
+      const int kk = L.at1(k);
+      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+      R thc = a.th_in[c], thm = a.th_in[cm];
+      R thvw = a.b.thbw[c] + (R)0.5 * (thm + thc);
+      R g = dtau * Phys<R>::cp * thvw * c1 / (J * a.m.dzeta_w[kk]);
+      const int q = k * LCX;
+      G[q] = g;
+      A[q] = -g * E[q - LCX] * Av[q - LCX];
+      B[q] = (R)1 + g * Av[q] * (E[q] + E[q - LCX]);
+      C[q] = -g * E[q] * Av[q + LCX];
+      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / a.b.thbw[c];
+      R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
+              dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) / (J * a.m.dzeta_w[kk]);
+      D[q] = RHS - g * (P[q] - P[q - LCX]);
+    }
+  __syncthreads();
+  if (active && lane == 0) {
+    R* W = S[V_W] + tx;
+    thomas_s(nz, A, B, C, D, S[V_CS] + tx, S[V_DS] + tx, W);
+    const size_t c0 = L.at(i, j, 0);
+    W[0] = (R)0.5 * (u[c0] + u[c0 + sx]) * hxc + (R)0.5 * (v[c0] + v[c0 + sy]) * hyc;
   }
-  for (int k = 0; k < nz; ++k) {
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k);
-    R Kt = a.co.kt3[c];
-    R Dh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
-                 (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
-    R dzc = a.m.dzeta_c[kk];
-    R wk = a.w_in[c], wkp = a.w_in[c + L.plane()];
-    R tpi = a.tpi ? a.tpi[c] : (R)0;
-    V.P[k] = a.pi_cur[c] + dtau * tpi -
-             dtau * Kt * (Dh - (V.Sv[k + 1] - V.Sv[k]) / dzc + c2 * (V.Av[k + 1] * wkp - V.Av[k] * wk) / dzc);
-    V.E[k] = dtau * Kt * c1 / dzc;
-  }
-  for (int k = 1; k < nz; ++k) {
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-    R thc = a.th_in[c], thm = a.th_in[cm];
-    R thvw = a.b.thbw[c] + (R)0.5 * (thm + thc);
-    R G = dtau * Phys<R>::cp * thvw * c1 / (J * a.m.dzeta_w[kk]);
-    V.thvw[k] = thvw;
-    V.G[k] = G;
-    V.A[k] = -G * V.E[k - 1] * V.Av[k - 1];
-    V.B[k] = (R)1 + G * V.Av[k] * (V.E[k] + V.E[k - 1]);
-    V.C[k] = -G * V.E[k] * V.Av[k + 1];
-    R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / a.b.thbw[c];
-    R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
-            dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) / (J * a.m.dzeta_w[kk]);
-    V.D[k] = RHS - G * (V.P[k] - V.P[k - 1]);
-  }
-  thomas(nz, V.A, V.B, V.C, V.D, V.cs, V.ds, V.w);
-  const size_t c0 = L.at(i, j, 0);
-  V.w[0] = (R)0.5 * (u[c0] + u[c0 + sx]) * hxc + (R)0.5 * (v[c0] + v[c0 + sy]) * hyc;
+  __syncthreads();
 }
 
+enum { T_DSV = V_N, T_DTH, T_DP, T_DG, T_RHS, T_DW, T_NARR };
+
 template <typename R>
-__global__ void k_tl_column(AcouArgs<R> a, AcouArgs<R> d) {
+__global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs<R> d) {
+  extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= L.nx || j >= L.ny) return;
-  const int nz = L.nz;
-  ColVals<R> V;
-  column_values(a, i, j, V);
+  const int nz = L.nz, tx = threadIdx.x, lane = threadIdx.y;
+  const int i = blockIdx.x * LCX + tx, j = blockIdx.y;
+  const bool active = i < L.nx;
+  const ColArr<R> S{reinterpret_cast<R*>(lin_smem), nz + 1};
   const R dtau = a.dtau, zt = a.m.zt;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(i, j);
+  const size_t c2d = L.at2(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   const R* u = d.u_out;
   const R* v = d.v_out;
   const long sx = 1, sy = L.px;
-  R dSv[kLinNZ + 1], dP[kLinNZ], rhs[kLinNZ], dw[kLinNZ + 1], dth[kLinNZ];
-  for (int k = 0; k < nz; ++k) dth[k] = d.th_in[L.at(i, j, k)];  // before any in-place write
-  for (int k = 0; k <= nz; ++k) {
-    R s = 0;
-    if (k >= 1 && k < nz) {
+  R *dSv = S[T_DSV] + tx, *dth = S[T_DTH] + tx, *dP = S[T_DP] + tx, *dG = S[T_DG] + tx;
+  R *rhs = S[T_RHS] + tx, *dw = S[T_DW] + tx;
+  // the tangent theta' in, before any in-place write of this launch
+  if (active)
+    for (int k = lane; k < nz; k += LKL) dth[k * LCX] = d.th_in[L.at(i, j, k)];
+  column_values_s(a, i, j, active, S);  // ends with a barrier
+  const R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *G = S[V_G] + tx;
+  const R *W = S[V_W] + tx;
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      R s = 0;
+      if (k >= 1 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+        R fac = (R)1 - a.m.zeta_w[kk] / zt;
+        R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+        R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+        s = Av[k * LCX] * (uw * hxc + vw * hyc) * fac;
+      }
+      dSv[k * LCX] = s;
+    }
+  __syncthreads();
+  if (active)
+    for (int k = lane; k < nz; k += LKL) {
+      const int kk = L.at1(k);
+      const size_t c = L.at(i, j, k);
+      R Kt = a.co.kt3[c];
+      R dDh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
+                    (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
+      R dzc = a.m.dzeta_c[kk];
+      R dwk = d.w_in[c], dwkp = d.w_in[c + L.plane()];
+      R dtpi = d.tpi ? d.tpi[c] : (R)0;
+      const int q = k * LCX;
+      dP[q] = d.pi_cur[c] + dtau * dtpi -
+              dtau * Kt * (dDh - (dSv[q + LCX] - dSv[q]) / dzc + c2 * (Av[q + LCX] * dwkp - Av[q] * dwk) / dzc);
+    }
+  __syncthreads();
+  if (active)
+    for (int k = 1 + lane; k < nz; k += LKL) {
       const int kk = L.at1(k);
       const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-      R fac = (R)1 - a.m.zeta_w[kk] / zt;
-      R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
-      R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
-      s = V.Av[k] * (uw * hxc + vw * hyc) * fac;
+      const int q = k * LCX;
+      const R jdz = J * a.m.dzeta_w[kk];
+      const R thvw = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      R dthvw = (R)0.5 * (dth[q - LCX] + dth[q]);
+      R g = dtau * Phys<R>::cp * dthvw * c1 / jdz;
+      R dbuoy = Phys<R>::grav * (R)0.5 * (dth[q - LCX] + dth[q]) / a.b.thbw[c];
+      R dpi = d.pi_cur[c] - d.pi_cur[cm], pi = a.pi_cur[c] - a.pi_cur[cm];
+      R dRHS = d.w_in[c] + dtau * (dbuoy + d.tw[c]) -
+               dtau * Phys<R>::cp * c2 * (dthvw * pi + thvw * dpi) / jdz;
+      R dD = dRHS - g * (P[q] - P[q - LCX]) - G[q] * (dP[q] - dP[q - LCX]);
+      R dA = -g * E[q - LCX] * Av[q - LCX];
+      R dB = g * Av[q] * (E[q] + E[q - LCX]);
+      R dC = -g * E[q] * Av[q + LCX];
+      R mw = dB * W[q];
+      if (k > 1) mw += dA * W[q - LCX];
+      if (k < nz - 1) mw += dC * W[q + LCX];
+      rhs[q] = dD - mw;
+      dG[q] = g;
     }
-    dSv[k] = s;
+  __syncthreads();
+  if (active && lane == 0) {
+    thomas_s(nz, S[V_A] + tx, S[V_B] + tx, S[V_C] + tx, rhs, S[V_CS] + tx, S[V_DS] + tx, dw);
+    const size_t c0 = L.at(i, j, 0);
+    dw[0] = (R)0.5 * (u[c0] + u[c0 + sx]) * hxc + (R)0.5 * (v[c0] + v[c0 + sy]) * hyc;
   }
-  for (int k = 0; k < nz; ++k) {
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k);
-    R Kt = a.co.kt3[c];
-    R dDh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
-                  (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
-    R dzc = a.m.dzeta_c[kk];
-    R dwk = d.w_in[c], dwkp = d.w_in[c + L.plane()];
-    R dtpi = d.tpi ? d.tpi[c] : (R)0;
-    dP[k] = d.pi_cur[c] + dtau * dtpi -
-            dtau * Kt * (dDh - (dSv[k + 1] - dSv[k]) / dzc + c2 * (V.Av[k + 1] * dwkp - V.Av[k] * dwk) / dzc);
-  }
-  for (int k = 1; k < nz; ++k) {
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-    const R jdz = J * a.m.dzeta_w[kk];
-    R dthvw = (R)0.5 * (dth[k - 1] + dth[k]);
-    R dG = dtau * Phys<R>::cp * dthvw * c1 / jdz;
-    R dA = -dG * V.E[k - 1] * V.Av[k - 1];
-    R dB = dG * V.Av[k] * (V.E[k] + V.E[k - 1]);
-    R dC = -dG * V.E[k] * V.Av[k + 1];
-    R dbuoy = Phys<R>::grav * (R)0.5 * (dth[k - 1] + dth[k]) / a.b.thbw[c];
-    R dpi = d.pi_cur[c] - d.pi_cur[cm], pi = a.pi_cur[c] - a.pi_cur[cm];
-    R dRHS = d.w_in[c] + dtau * (dbuoy + d.tw[c]) -
-             dtau * Phys<R>::cp * c2 * (dthvw * pi + V.thvw[k] * dpi) / jdz;
-    R dD = dRHS - dG * (V.P[k] - V.P[k - 1]) - V.G[k] * (dP[k] - dP[k - 1]);
-    R mw = dB * V.w[k];
-    if (k > 1) mw += dA * V.w[k - 1];
-    if (k < nz - 1) mw += dC * V.w[k + 1];
-    rhs[k] = dD - mw;
-  }
-  R cs[kLinNZ], ds[kLinNZ];
-  thomas(nz, V.A, V.B, V.C, rhs, cs, ds, dw);
-  const size_t c0 = L.at(i, j, 0);
-  dw[0] = (R)0.5 * (u[c0] + u[c0 + sx]) * hxc + (R)0.5 * (v[c0] + v[c0 + sy]) * hyc;
-  for (int k = 0; k <= nz; ++k) {
-    const size_t c = L.at(i, j, k);
-    if (k < nz) {
-      d.pi_next[c] = dP[k] - V.E[k] * (V.Av[k + 1] * dw[k + 1] - V.Av[k] * dw[k]);
-      d.th_out[c] = dth[k] + dtau * (d.tth[c] - (R)0.5 * (dw[k] + dw[k + 1]) * a.b.dthbdz[c]);
-      d.w_out[c] = dw[k];
-    } else {
-      d.w_out[c] = 0;
+  __syncthreads();
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      const size_t c = L.at(i, j, k);
+      const int q = k * LCX;
+      if (k < nz) {
+        d.pi_next[c] = dP[q] - E[q] * (Av[q + LCX] * dw[q + LCX] - Av[q] * dw[q]);
+        d.th_out[c] = dth[q] + dtau * (d.tth[c] - (R)0.5 * (dw[q] + dw[q + LCX]) * a.b.dthbdz[c]);
+        d.w_out[c] = dw[q];
+      } else {
+        d.w_out[c] = 0;
+      }
     }
-  }
 }
 
+enum { A_WB = V_N, A_PB, A_TB, A_WS, A_LAM, A_GL, A_PIB, A_THB, A_KTD, A_NARR };
+
 template <typename R>
-__global__ void k_ad_column(AcouArgs<R> a, AcouArgs<R> d) {
+__global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs<R> d) {
+  extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= L.nx || j >= L.ny) return;
-  const int nz = L.nz;
-  ColVals<R> V;
-  column_values(a, i, j, V);
+  const int nz = L.nz, tx = threadIdx.x, lane = threadIdx.y;
+  const int i = blockIdx.x * LCX + tx, j = blockIdx.y;
+  const bool active = i < L.nx;
+  const ColArr<R> S{reinterpret_cast<R*>(lin_smem), nz + 1};
   const R dtau = a.dtau, zt = a.m.zt;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(i, j);
+  const size_t c2d = L.at2(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   R* ub = d.u_out;
   R* vb = d.v_out;
@@ -801,126 +849,143 @@ __global__ void k_ad_column(AcouArgs<R> a, AcouArgs<R> d) {
   R* tthB = const_cast<R*>(d.tth);
   R* tpiB = const_cast<R*>(d.tpi);
   const long sx = 1, sy = L.px;
+  R *wb = S[A_WB] + tx, *pb = S[A_PB] + tx, *tb = S[A_TB] + tx, *ws = S[A_WS] + tx;
+  R *lam = S[A_LAM] + tx, *GL = S[A_GL] + tx, *PIB = S[A_PIB] + tx, *THB = S[A_THB] + tx;
+  R *KTD = S[A_KTD] + tx;
   // output adjoints, read and cleared before the (possibly aliased) inputs gain theirs
-  R wb[kLinNZ + 1], pb[kLinNZ], tb[kLinNZ];
-  for (int k = 0; k <= nz; ++k) {
-    const size_t c = L.at(i, j, k);
-    wb[k] = d.w_out[c];
-    d.w_out[c] = 0;
-    if (k < nz) {
-      pb[k] = d.pi_next[c];
-      tb[k] = d.th_out[c];
-      d.pi_next[c] = 0;
-      d.th_out[c] = 0;
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      const size_t c = L.at(i, j, k);
+      const int q = k * LCX;
+      wb[q] = d.w_out[c];
+      d.w_out[c] = 0;
+      if (k < nz) {
+        pb[q] = d.pi_next[c];
+        tb[q] = d.th_out[c];
+        d.pi_next[c] = 0;
+        d.th_out[c] = 0;
+      }
     }
-  }
-  R wsb[kLinNZ + 1], Pb[kLinNZ], Svb[kLinNZ + 1], thb[kLinNZ];
-  for (int k = 0; k <= nz; ++k) {
-    wsb[k] = 0;
-    Svb[k] = 0;
-  }
-  for (int k = 0; k < nz; ++k) {
-    Pb[k] = 0;
-    thb[k] = 0;
-  }
-  for (int k = 0; k < nz; ++k) {
-    const size_t c = L.at(i, j, k);
-    // theta_out = theta_in + dtau (tth - 0.5 (w_k + w_k+1) dthbdz)
-    thb[k] += tb[k];
-    tthB[c] += dtau * tb[k];
-    R h = -(R)0.5 * dtau * a.b.dthbdz[c] * tb[k];
-    wsb[k] += h;
-    wsb[k + 1] += h;
-    // pi_next = P - E (Av_k+1 w_k+1 - Av_k w_k)
-    Pb[k] += pb[k];
-    wsb[k + 1] += -V.E[k] * V.Av[k + 1] * pb[k];
-    wsb[k] += V.E[k] * V.Av[k] * pb[k];
-    // w_out = w
-    wsb[k] += wb[k];
-  }
-  // surface w = us hx + vs hy
-  {
+  column_values_s(a, i, j, active, S);  // ends with a barrier
+  const R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *G = S[V_G] + tx;
+  const R *W = S[V_W] + tx;
+  // adjoint of the column solution w (level 0: surface w, level nz: the lid)
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      const int q = k * LCX;
+      R g = 0;
+      if (k < nz) {
+        const size_t c = L.at(i, j, k);
+        g += wb[q] - (R)0.5 * dtau * a.b.dthbdz[c] * tb[q] + E[q] * Av[q] * pb[q];
+      }
+      if (k >= 1) {
+        const size_t cm = L.at(i, j, k - 1);
+        g += -(R)0.5 * dtau * a.b.dthbdz[cm] * tb[q - LCX] - E[q - LCX] * Av[q] * pb[q - LCX];
+      }
+      ws[q] = g;
+    }
+  __syncthreads();
+  if (active && lane == 0) {
     const size_t c0 = L.at(i, j, 0);
-    R g = wsb[0];
+    const R g = ws[0];
     if (g != (R)0) {
       atomicAdd(ub + c0, (R)0.5 * hxc * g);
       atomicAdd(ub + c0 + sx, (R)0.5 * hxc * g);
       atomicAdd(vb + c0, (R)0.5 * hyc * g);
       atomicAdd(vb + c0 + sy, (R)0.5 * hyc * g);
     }
+    thomas_ts(nz, S[V_A] + tx, S[V_B] + tx, S[V_C] + tx, ws, S[V_CS] + tx, S[V_DS] + tx, lam);
   }
-  // lambda = M^-T wsb on rows 1..nz-1
-  R lam[kLinNZ + 1];
-  thomas_t(nz, V.A, V.B, V.C, wsb, V.cs, V.ds, lam);
-  for (int k = 1; k < nz; ++k) {
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-    const R jdz = J * a.m.dzeta_w[kk];
-    const R Db = lam[k];
-    const R Ab = k > 1 ? -lam[k] * V.w[k - 1] : (R)0;
-    const R Bb = -lam[k] * V.w[k];
-    const R Cb = k < nz - 1 ? -lam[k] * V.w[k + 1] : (R)0;
-    R Gb = Ab * (-V.E[k - 1] * V.Av[k - 1]) + Bb * (V.Av[k] * (V.E[k] + V.E[k - 1])) +
-           Cb * (-V.E[k] * V.Av[k + 1]) - Db * (V.P[k] - V.P[k - 1]);
-    Pb[k] += -V.G[k] * Db;
-    Pb[k - 1] += V.G[k] * Db;
-    const R RHSb = Db;
-    wI[c] += RHSb;
-    twB[c] += dtau * RHSb;
-    const R buoyb = dtau * RHSb;
-    const R pi = a.pi_cur[c] - a.pi_cur[cm];
-    R thvwb = -dtau * Phys<R>::cp * c2 * pi / jdz * RHSb;
-    const R pib = -dtau * Phys<R>::cp * V.thvw[k] * c2 / jdz * RHSb;
-    piC[c] += pib;
-    piC[cm] -= pib;
-    const R bt = Phys<R>::grav * (R)0.5 / a.b.thbw[c] * buoyb;
-    thb[k - 1] += bt;
-    thb[k] += bt;
-    thvwb += Gb * dtau * Phys<R>::cp * c1 / jdz;
-    thb[k - 1] += (R)0.5 * thvwb;
-    thb[k] += (R)0.5 * thvwb;
-  }
-  for (int k = 0; k < nz; ++k) {
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k);
-    const R Kt = a.co.kt3[c];
-    const R dzc = a.m.dzeta_c[kk];
-    const R g = Pb[k];
-    piC[c] += g;
-    if (tpiB) tpiB[c] += dtau * g;
-    const R Dhb = -dtau * Kt * g;
-    Svb[k + 1] += dtau * Kt / dzc * g;
-    Svb[k] -= dtau * Kt / dzc * g;
-    wI[c + L.plane()] += -dtau * Kt * c2 * V.Av[k + 1] / dzc * g;
-    wI[c] += dtau * Kt * c2 * V.Av[k] / dzc * g;
-    if (Dhb != (R)0) {
-      atomicAdd(ub + c + sx, mc * a.co.rtjx[c + sx] / a.dx * Dhb);
-      atomicAdd(ub + c, -mc * a.co.rtjx[c] / a.dx * Dhb);
-      atomicAdd(vb + c + sy, mc * a.co.rtjy[c + sy] / a.dy * Dhb);
-      atomicAdd(vb + c, -mc * a.co.rtjy[c] / a.dy * Dhb);
+  __syncthreads();
+  // per inner level: what its row sends to neighbouring levels
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      const int q = k * LCX;
+      if (k < 1 || k >= nz) {
+        GL[q] = 0;
+        PIB[q] = 0;
+        THB[q] = 0;
+        continue;
+      }
+      const int kk = L.at1(k);
+      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+      const R jdz = J * a.m.dzeta_w[kk];
+      const R lm = lam[q];
+      const R Ab = k > 1 ? -lm * W[q - LCX] : (R)0;
+      const R Bb = -lm * W[q];
+      const R Cb = k < nz - 1 ? -lm * W[q + LCX] : (R)0;
+      const R Gb = Ab * (-E[q - LCX] * Av[q - LCX]) + Bb * (Av[q] * (E[q] + E[q - LCX])) +
+                   Cb * (-E[q] * Av[q + LCX]) - lm * (P[q] - P[q - LCX]);
+      const R thvw = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      const R pi = a.pi_cur[c] - a.pi_cur[cm];
+      GL[q] = G[q] * lm;
+      PIB[q] = -dtau * Phys<R>::cp * thvw * c2 / jdz * lm;
+      const R thvwb = -dtau * Phys<R>::cp * c2 * pi / jdz * lm + Gb * dtau * Phys<R>::cp * c1 / jdz;
+      const R bt = Phys<R>::grav * (R)0.5 / a.b.thbw[c] * dtau * lm;
+      THB[q] = (R)0.5 * thvwb + bt;
+      twB[c] += dtau * lm;
     }
-  }
-  for (int k = 1; k < nz; ++k) {
-    const R g = Svb[k];
-    if (g == (R)0) continue;
-    const int kk = L.at1(k);
-    const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-    const R fac = (R)1 - a.m.zeta_w[kk] / zt;
-    const R cu = (R)0.25 * V.Av[k] * hxc * fac * g, cv = (R)0.25 * V.Av[k] * hyc * fac * g;
-    if (cu != (R)0) {
-      atomicAdd(ub + cm, cu);
-      atomicAdd(ub + cm + sx, cu);
-      atomicAdd(ub + c, cu);
-      atomicAdd(ub + c + sx, cu);
+  __syncthreads();
+  if (active)
+    for (int k = lane; k < nz; k += LKL) {
+      const int kk = L.at1(k);
+      const size_t c = L.at(i, j, k);
+      const int q = k * LCX;
+      R Pb = pb[q];
+      if (k >= 1) Pb -= GL[q];
+      if (k + 1 < nz) Pb += GL[q + LCX];
+      R pic = Pb;
+      if (k >= 1) pic += PIB[q];
+      if (k + 1 < nz) pic -= PIB[q + LCX];
+      piC[c] += pic;
+      if (tpiB) tpiB[c] += dtau * Pb;
+      const R Kt = a.co.kt3[c];
+      const R Dhb = -dtau * Kt * Pb;
+      if (Dhb != (R)0) {
+        atomicAdd(ub + c + sx, mc * a.co.rtjx[c + sx] / a.dx * Dhb);
+        atomicAdd(ub + c, -mc * a.co.rtjx[c] / a.dx * Dhb);
+        atomicAdd(vb + c + sy, mc * a.co.rtjy[c + sy] / a.dy * Dhb);
+        atomicAdd(vb + c, -mc * a.co.rtjy[c] / a.dy * Dhb);
+      }
+      R th = tb[q];
+      if (k >= 1) th += THB[q];
+      if (k + 1 < nz) th += THB[q + LCX];
+      thI[c] += th;
+      tthB[c] += dtau * tb[q];
+      KTD[q] = Kt / a.m.dzeta_c[kk] * Pb;
     }
-    if (cv != (R)0) {
-      atomicAdd(vb + cm, cv);
-      atomicAdd(vb + cm + sy, cv);
-      atomicAdd(vb + c, cv);
-      atomicAdd(vb + c + sy, cv);
+  __syncthreads();
+  if (active)
+    for (int k = lane; k <= nz; k += LKL) {
+      const int q = k * LCX;
+      const size_t c = L.at(i, j, k);
+      R wsum = 0;
+      if (k >= 1 && k < nz) wsum += lam[q];
+      R kd = (k < nz ? KTD[q] : (R)0) - (k >= 1 ? KTD[q - LCX] : (R)0);
+      wsum += dtau * c2 * Av[q] * kd;
+      wI[c] += wsum;
+      if (k >= 1 && k < nz) {
+        const R svb = -dtau * kd;  // adjoint of Sv(k)
+        if (svb != (R)0) {
+          const int kk = L.at1(k);
+          const size_t cm = c - (size_t)L.plane();
+          const R fac = (R)1 - a.m.zeta_w[kk] / zt;
+          const R cu = (R)0.25 * Av[q] * hxc * fac * svb, cv = (R)0.25 * Av[q] * hyc * fac * svb;
+          if (cu != (R)0) {
+            atomicAdd(ub + cm, cu);
+            atomicAdd(ub + cm + sx, cu);
+            atomicAdd(ub + c, cu);
+            atomicAdd(ub + c + sx, cu);
+          }
+          if (cv != (R)0) {
+            atomicAdd(vb + cm, cv);
+            atomicAdd(vb + cm + sy, cv);
+            atomicAdd(vb + c, cv);
+            atomicAdd(vb + c + sy, cv);
+          }
+        }
+      }
     }
-  }
-  for (int k = 0; k < nz; ++k) thI[L.at(i, j, k)] += thb[k];
 }
 
 // zero every stored point of a cell field outside the interior cells
@@ -975,21 +1040,32 @@ void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
   k_ad_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d);
 }
 
-int lin_max_levels() { return kLinNZ - 1; }
+int lin_max_levels() { return 160; }  // FP64 adjoint column arrays within 227 KB
+
+template <typename R, int NARR>
+static size_t lin_col_smem(int nz) {
+  return (size_t)NARR * (nz + 1) * LCX * sizeof(R);
+}
 
 template <typename R>
 int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
-  if (a.L.nz > kLinNZ - 1) return 2;
-  dim3 blk(32, 2);
-  k_tl_column<R><<<dim3((a.L.nx + 31) / 32, (a.L.ny + 1) / 2), blk, 0, st>>>(a, d);
+  if (a.L.nz > lin_max_levels()) return 2;
+  const size_t sm = lin_col_smem<R, T_NARR>(a.L.nz);
+  if (sm > 48 * 1024 &&
+      cudaFuncSetAttribute(k_tl_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    return 2;
+  k_tl_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d);
   return 0;
 }
 
 template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
-  if (a.L.nz > kLinNZ - 1) return 2;
-  dim3 blk(32, 2);
-  k_ad_column<R><<<dim3((a.L.nx + 31) / 32, (a.L.ny + 1) / 2), blk, 0, st>>>(a, d);
+  if (a.L.nz > lin_max_levels()) return 2;
+  const size_t sm = lin_col_smem<R, A_NARR>(a.L.nz);
+  if (sm > 48 * 1024 &&
+      cudaFuncSetAttribute(k_ad_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    return 2;
+  k_ad_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d);
   return 0;
 }
 
