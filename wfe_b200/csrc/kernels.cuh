@@ -233,6 +233,10 @@ int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
 template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
 int lin_max_levels();
+// shared-memory limits of the linearised column kernels for nz levels (once,
+// outside any stream capture); 2 when nz exceeds lin_max_levels()
+template <typename R>
+int lin_prepare(int nz);
 // zero a cell field outside the interior cells (the pi' ghost ring, which no
 // launch of a step reads or writes)
 template <typename R>

@@ -303,11 +303,13 @@ __global__ void __launch_bounds__(256) k_ad_tend(TendArgs<R> a, TendArgs<R> d) {
 
 // ================================================================ ghost fill
 // Adjoint of the ghost fill (forward: dyn_tend.cu fill_body): every written
-// ghost value moves its adjoint onto its interior sources and is zeroed.
+// ghost value moves its adjoint onto its interior sources and is zeroed.  One
+// thread per (padded column, level, field); interior points return at once.
 template <typename R>
-__global__ void k_ad_fill(FillArgs<R> A) {
+__global__ void k_ad_fill(FillArgs<R> A, int nk) {
   const Layout& L = A.L;
-  const int f = blockIdx.z;
+  const int f = blockIdx.z / nk;
+  const int k = (int)(blockIdx.z % nk) - kRefNG;
   if (f >= A.job.n) return;
   R* a = A.job.f[f];
   const int kind = A.job.kind[f];
@@ -319,24 +321,22 @@ __global__ void k_ad_fill(FillArgs<R> A) {
   const int si = map_lat(i, L.nx, ilast, A.open_x);
   const int sj = map_lat(j, L.ny, jlast, A.open_y);
   const bool lateral = (si != i) || (sj != j);
-  for (int k = -kRefNG; k <= L.nz + kRefNG; ++k) {
-    if (!lateral && k >= 0 && k < L.nz) continue;  // interior levels of an interior column
-    const size_t q = L.at(i, j, k);
-    const R g = a[q];
-    a[q] = 0;
-    if (g == (R)0) continue;
-    if (kind == 3) {
-      if (k == L.nz) continue;
-      if (k >= 0 && k < L.nz) atomicAdd(a + L.at(si, sj, k), g);
-      else if (k < 0) {
-        atomicAdd(a + L.at(si, sj, 0), (R)2 * g);
-        atomicAdd(a + L.at(si, sj, -k), -g);
-      } else {
-        atomicAdd(a + L.at(si, sj, 2 * L.nz - k), -g);
-      }
+  if (!lateral && k >= 0 && k < L.nz) return;  // interior level of an interior column
+  const size_t q = L.at(i, j, k);
+  const R g = a[q];
+  a[q] = 0;
+  if (g == (R)0) return;
+  if (kind == 3) {
+    if (k == L.nz) return;
+    if (k >= 0 && k < L.nz) atomicAdd(a + L.at(si, sj, k), g);
+    else if (k < 0) {
+      atomicAdd(a + L.at(si, sj, 0), (R)2 * g);
+      atomicAdd(a + L.at(si, sj, -k), -g);
     } else {
-      atomicAdd(a + L.at(si, sj, map_zc(k, L.nz)), g);
+      atomicAdd(a + L.at(si, sj, 2 * L.nz - k), -g);
     }
+  } else {
+    atomicAdd(a + L.at(si, sj, map_zc(k, L.nz)), g);
   }
 }
 
@@ -1012,7 +1012,10 @@ void zero_ring(R* f, const Layout& L, cudaStream_t st) {
 template <typename R>
 void ad_fill(const FillArgs<R>& d, cudaStream_t st) {
   if (d.job.n == 0) return;
-  k_ad_fill<R><<<grid_fill(d), dim3(32, 4), 0, st>>>(d);
+  const int nk = d.L.nz + 1 + 2 * kRefNG;  // levels -3 .. nz+3
+  dim3 g = grid_fill(d);
+  g.z = (unsigned)(d.job.n * nk);
+  k_ad_fill<R><<<g, dim3(32, 4), 0, st>>>(d, nk);
 }
 
 template <typename R>
@@ -1047,13 +1050,23 @@ static size_t lin_col_smem(int nz) {
   return (size_t)NARR * (nz + 1) * LCX * sizeof(R);
 }
 
+// Sets the dynamic shared-memory limits of the column kernels for nz levels,
+// once, outside any stream capture.
+template <typename R>
+int lin_prepare(int nz) {
+  if (nz > lin_max_levels()) return 2;
+  if (cudaFuncSetAttribute(k_tl_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)lin_col_smem<R, T_NARR>(nz)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_ad_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)lin_col_smem<R, A_NARR>(nz)) != cudaSuccess)
+    return 1;
+  return 0;
+}
+
 template <typename R>
 int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
   if (a.L.nz > lin_max_levels()) return 2;
   const size_t sm = lin_col_smem<R, T_NARR>(a.L.nz);
-  if (sm > 48 * 1024 &&
-      cudaFuncSetAttribute(k_tl_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-    return 2;
   k_tl_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d);
   return 0;
 }
@@ -1062,9 +1075,6 @@ template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
   if (a.L.nz > lin_max_levels()) return 2;
   const size_t sm = lin_col_smem<R, A_NARR>(a.L.nz);
-  if (sm > 48 * 1024 &&
-      cudaFuncSetAttribute(k_ad_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-    return 2;
   k_ad_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d);
   return 0;
 }
@@ -1078,7 +1088,8 @@ int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
   template void ad_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t);   \
   template int tl_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t); \
   template int ad_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t);  \
-  template void zero_ring<R>(R*, const Layout&, cudaStream_t);
+  template void zero_ring<R>(R*, const Layout&, cudaStream_t);                        \
+  template int lin_prepare<R>(int);
 WFE_INST(float)
 WFE_INST(double)
 #undef WFE_INST

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <memory>
 #include <string>
@@ -60,6 +61,9 @@ class LinT final : public Lin {
     std::vector<Rec> recs;
     if (m->record_step(1.0, &recs)) return fail(m->error());
     learn_layout(recs);
+    const int pr = lin_prepare<R>(L_.nz);
+    if (pr == 2) return fail("column deeper than the linearised kernels hold");
+    if (pr) return fail("linearised column kernels: shared memory limit");
     m->set_lin_map([this](const void* p) -> void* {
       auto it = map_.find(p);
       return it == map_.end() ? nullptr : it->second;
@@ -77,12 +81,22 @@ class LinT final : public Lin {
   int tl_run(int nsteps, double dt, double t0) override {
     (void)t0;
     if (keep_only_state()) return 1;
+    if (dt != dt_) drop_graphs(dt);
     for (int s = 0; s < nsteps; ++s) {
-      std::vector<Rec> recs;
-      if (m_->record_step(dt, &recs)) return fail(m_->error());
-      for (const Rec& r : recs) {
-        if (tl(r) || fwd(r)) return 1;
+      // one captured graph per rotation phase: [TL kernel, forward launch] per launch
+      const int ph = m_->phase();
+      cudaGraphExec_t& ge = tl_graph_[ph];
+      if (!ge) {
+        std::vector<Rec> recs;
+        if (m_->record_step(dt, &recs)) return fail(m_->error());
+        if (capture(&ge, [&] {
+              for (const Rec& r : recs)
+                if (tl(r) || fwd(r)) return 1;
+              return 0;
+            }))
+          return 1;
       }
+      LCK(cudaGraphLaunch(ge, st_));
       m_->rotate();
     }
     // pi' ghosts are outputs of nothing: the tangent has none there
@@ -93,45 +107,45 @@ class LinT final : public Lin {
   }
 
   int ad_run(int nsteps, double dt, double t0, int every) override {
-    (void)t0;
     if (nsteps <= 0) return 0;
     if (every < 1) every = 1;
+    if (dt != dt_) drop_graphs(dt);
     // the adjoint of x_N, uploaded in the slot of the current time-n state;
     // pi' ghosts are no state, so adjoint values there are dropped
     if (L_.nx) zero_ring<R>(D(static_cast<R*>(m_->state_field(4))), L_, st_);
     std::vector<R*> bar;
     if (save_lin_state(&bar)) return 1;
-    // forward pass with segment checkpoints; x_N kept to restore at the end
+    // forward pass (the model's own graphs) with segment checkpoints; x_N kept
+    // to restore at the end
     const int nseg = (nsteps + every - 1) / every;
     std::vector<Snap> segs(nseg);
-    for (int s = 0; s < nsteps; ++s) {
-      if (s % every == 0 && snap(&segs[s / every])) return 1;
-      if (step_fwd(dt)) return 1;
+    for (int g = 0; g < nseg; ++g) {
+      const int s0 = g * every, len = std::min(nsteps, s0 + every) - s0;
+      if (snap(&segs[g])) return 1;
+      if (m_->run(len, dt, t0 + s0 * dt)) return fail(m_->error());
     }
     Snap last;
     if (snap(&last)) return 1;
     if (zero() || load_lin_state(bar)) return 1;
-    std::vector<Snap> steps(every);
+    // reverse sweep: per segment (last first) one graph replays the segment
+    // forward saving every buffer each launch overwrites (the undo log), one
+    // graph walks the launches backwards (restore outputs, adjoint kernel);
+    // both depend only on the segment's start phase and length
     for (int g = nseg - 1; g >= 0; --g) {
-      const int s0 = g * every, s1 = std::min(nsteps, s0 + every);
+      const int s0 = g * every, len = std::min(nsteps, s0 + every) - s0;
       if (restore(segs[g])) return 1;
-      for (int s = s0; s < s1; ++s) {
-        if (snap(&steps[s - s0])) return 1;
-        if (s + 1 < s1 && step_fwd(dt)) return 1;
-      }
-      for (int s = s1 - 1; s >= s0; --s) {
-        if (restore(steps[s - s0])) return 1;
-        if (step_ad(dt)) return 1;
-      }
+      SegGraphs* sg = nullptr;
+      if (segment_graphs(segs[g].phase, len, dt, &sg)) return 1;
+      LCK(cudaGraphLaunch(sg->fwd, st_));
+      LCK(cudaGraphLaunch(sg->rev, st_));
     }
     // dJ/dx0 sits in the slot of x0; move it to the slot of x_N
     if (save_lin_state(&bar)) return 1;
     if (restore(last) || zero() || load_lin_state(bar)) return 1;
     for (auto& s : segs) free_snap(&s);
-    for (auto& s : steps) free_snap(&s);
     free_snap(&last);
-    for (R* p : bar) cudaFree(p);
     LCK(cudaStreamSynchronize(st_));
+    for (R* p : bar) cudaFree(p);
     LCK(cudaGetLastError());
     return 0;
   }
@@ -310,49 +324,112 @@ class LinT final : public Lin {
       }
   }
 
-  int step_fwd(double dt) {
-    std::vector<Rec> recs;
-    if (m_->record_step(dt, &recs)) return fail(m_->error());
-    for (const Rec& r : recs)
-      if (fwd(r)) return 1;
-    m_->rotate();
+  struct SegGraphs {
+    cudaGraphExec_t fwd = nullptr, rev = nullptr;
+  };
+
+  template <class F>
+  int capture(cudaGraphExec_t* out, F&& issue) {
+    cudaGraph_t gr = nullptr;
+    LCK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    const int rc = issue();
+    cudaError_t ce = cudaStreamEndCapture(st_, &gr);
+    if (rc) {
+      if (gr) cudaGraphDestroy(gr);
+      return 1;
+    }
+    if (ce != cudaSuccess) return fail(std::string("graph capture: ") + cudaGetErrorString(ce));
+    cudaError_t ie = cudaGraphInstantiate(out, gr, 0);
+    cudaGraphDestroy(gr);
+    if (ie != cudaSuccess) return fail(std::string("graph instantiate: ") + cudaGetErrorString(ie));
     return 0;
   }
 
-  int step_ad(double dt) {
-    std::vector<Rec> recs;
-    if (m_->record_step(dt, &recs)) return fail(m_->error());
-    size_t need = 0;
-    std::vector<R*> o;
-    for (const Rec& r : recs) {
-      outputs(r, &o);
-      need += o.size();
+  void drop_graphs(double dt) {
+    for (auto& ge : tl_graph_)
+      if (ge) {
+        cudaGraphExecDestroy(ge);
+        ge = nullptr;
+      }
+    for (auto& kv : seg_) {
+      if (kv.second.fwd) cudaGraphExecDestroy(kv.second.fwd);
+      if (kv.second.rev) cudaGraphExecDestroy(kv.second.rev);
     }
-    if (need > log_cap_) {
+    seg_.clear();
+    dt_ = dt;
+  }
+
+  // the launches of `len` steps from rotation phase `phase` (the model is
+  // left at its current phase)
+  int record_segment(int phase, int len, double dt, std::vector<std::vector<Rec>>* recs) {
+    const int keep = m_->phase();
+    while (m_->phase() != phase) m_->rotate();
+    recs->assign(len, {});
+    for (int s = 0; s < len; ++s) {
+      if (m_->record_step(dt, &(*recs)[s])) return fail(m_->error());
+      m_->rotate();
+    }
+    while (m_->phase() != keep) m_->rotate();
+    return 0;
+  }
+
+  int segment_graphs(int phase, int len, double dt, SegGraphs** out) {
+    const long key = (long)phase * 1000000L + len;
+    auto it = seg_.find(key);
+    if (it != seg_.end()) {
+      *out = &it->second;
+      return 0;
+    }
+    std::vector<std::vector<Rec>> recs;
+    if (record_segment(phase, len, dt, &recs)) return 1;
+    size_t slots = 0;
+    std::vector<R*> o;
+    for (auto& st : recs)
+      for (const Rec& r : st) {
+        outputs(r, &o);
+        slots += o.size();
+      }
+    if (slots > log_cap_) {  // outside any capture
       if (log_) cudaFree(log_);
       log_ = nullptr;
       log_cap_ = 0;
-      LCK(cudaMalloc(&log_, need * n3_ * sizeof(R)));
-      log_cap_ = need;
+      LCK(cudaMalloc(&log_, slots * n3_ * sizeof(R)));
+      log_cap_ = slots;
     }
-    size_t slot = 0;
-    for (const Rec& r : recs) {
-      outputs(r, &o);
-      for (R* p : o) {
-        LCK(cudaMemcpyAsync(log_ + slot * n3_, p, n3_ * sizeof(R), cudaMemcpyDeviceToDevice, st_));
-        ++slot;
-      }
-      if (fwd(r)) return 1;
-    }
-    for (size_t q = recs.size(); q-- > 0;) {
-      outputs(recs[q], &o);
-      for (size_t z = o.size(); z-- > 0;) {
-        --slot;
-        LCK(cudaMemcpyAsync(o[z], log_ + slot * n3_, n3_ * sizeof(R), cudaMemcpyDeviceToDevice, st_));
-      }
-      if (ad(recs[q])) return 1;
-    }
-    LCK(cudaGetLastError());
+    SegGraphs g;
+    if (capture(&g.fwd, [&] {
+          size_t slot = 0;
+          std::vector<R*> oo;
+          for (auto& st : recs)
+            for (const Rec& r : st) {
+              outputs(r, &oo);
+              for (R* p : oo) {
+                LCK(cudaMemcpyAsync(log_ + slot * n3_, p, n3_ * sizeof(R), cudaMemcpyDeviceToDevice,
+                                    st_));
+                ++slot;
+              }
+              if (fwd(r)) return 1;
+            }
+          return 0;
+        }))
+      return 1;
+    if (capture(&g.rev, [&] {
+          size_t slot = slots;
+          std::vector<R*> oo;
+          for (size_t s = recs.size(); s-- > 0;)
+            for (size_t q = recs[s].size(); q-- > 0;) {
+              outputs(recs[s][q], &oo);
+              for (size_t z = oo.size(); z-- > 0;) {
+                --slot;
+                LCK(cudaMemcpyAsync(oo[z], log_ + slot * n3_, n3_ * sizeof(R),
+                                    cudaMemcpyDeviceToDevice, st_));
+              }
+              if (ad(recs[s][q])) return 1;
+            }
+          return 0;
+        }))
+      return 1;
+    *out = &(seg_[key] = g);
     return 0;
   }
 
@@ -413,6 +490,7 @@ class LinT final : public Lin {
   }
 
   void release() {
+    drop_graphs(0);
     if (m_) m_->set_lin_map(nullptr);
     for (auto& b : bufs_) cudaFree(b.first);
     bufs_.clear();
@@ -428,6 +506,9 @@ class LinT final : public Lin {
   Layout L_{};
   R* log_ = nullptr;
   size_t log_cap_ = 0;
+  double dt_ = -1;
+  cudaGraphExec_t tl_graph_[3] = {nullptr, nullptr, nullptr};
+  std::map<long, SegGraphs> seg_;
 };
 
 }  // namespace
