@@ -188,3 +188,21 @@ def test_async_snapshot_equals_interior_download(prec):
         assert np.array_equal(bufs["rain"], c2.rain(interior=True).astype(dt))
         c2.close()
     c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "bubble_open", "straka_periodic"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_tma_column_variant_equals_tile_variants(name, prec, monkeypatch):
+    """The TMA-staged acoustic column kernel (variant 6) computes the same
+    values, bit for bit, as the shared-memory tile kernel (variant 0)."""
+    out = {}
+    for v in ("0", "6"):
+        monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
+        c = W.Case(CASES / f"{name}.ini", precision=prec)
+        for s in range(4):
+            c.step(c.dt, s * c.dt)
+        out[v] = {k: c.field(k) for k in W.FIELDS}
+        c.close()
+    for k in W.FIELDS:
+        assert np.array_equal(out["0"][k], out["6"][k]), k

@@ -25,6 +25,7 @@
 #include "core.cuh"
 #include "kernels.cuh"
 #include "dyn_common.cuh"
+#include "tma.cuh"
 
 namespace wfe {
 
@@ -446,6 +447,246 @@ __global__ void __launch_bounds__(CX * KL, 1024 / (CX * KL)) k_acoustic_column_b
   for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int) { column_body<R, CX, KL>(a, x, y); });
 }
 
+// --------------------------------------------- TMA-staged column variant
+constexpr int kTmaKL = 32;
+
+// shared-memory layout: the barrier, then each field's box (levels -1..nz,
+// x fastest), then the nine column work arrays
+template <typename R>
+struct TmaColLayout {
+  size_t field[TC_N];
+  size_t work, total;
+  __host__ __device__ TmaColLayout(int nz) {
+    const int nzs = nz + 2;
+    size_t o = 128;  // the mbarrier lives in the first 8 bytes
+    for (int f = 0; f < TC_N; ++f) {
+      int bx, by;
+      tma_col_box(f, &bx, &by);
+      field[f] = o;
+      o += ((size_t)bx * by * nzs * sizeof(R) + 127) / 128 * 128;
+    }
+    work = o;
+    total = o + (size_t)9 * (nz + 1) * kTmaCX * sizeof(R);
+  }
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kTmaCX * kTmaKL)
+    k_acoustic_column_tma(const __grid_constant__ TmaColParams<R> p) {
+  extern __shared__ __align__(128) unsigned char smem_tma[];
+  const AcouArgs<R>& a = p.a;
+  const Layout& L = a.L;
+  const int nz = L.nz, nzs = nz + 2;
+  const int tx = threadIdx.x, lane_k = threadIdx.y;
+  const int tid = tx + kTmaCX * lane_k;
+  const int i0 = blockIdx.x * kTmaCX, i = i0 + tx, j = blockIdx.y;
+  const bool active = i < L.nx;
+  const bool moist = a.p.moisture != 0;
+  const TmaColLayout<R> lay(nz);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_tma);
+  auto fld = [&](int f) { return reinterpret_cast<R*>(smem_tma + lay.field[f]); };
+
+  if (tid == 0) {
+    tma::mbar_init(bar, 1);
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t bytes = 0;
+    for (int f = 0; f < TC_N; ++f) {
+      if (f == TC_TPI && !p.has_tpi) continue;
+      if (f >= TC_QV && !moist) continue;
+      int bx, by;
+      tma_col_box(f, &bx, &by);
+      bytes += (uint32_t)((size_t)bx * by * nzs * sizeof(R));
+    }
+    tma::mbar_arrive_expect_tx(bar, bytes);
+    const int x = i0 + kOX, y = j + kOY, z = kOZ - 1;
+    for (int f = 0; f < TC_N; ++f) {
+      if (f == TC_TPI && !p.has_tpi) continue;
+      if (f >= TC_QV && !moist) continue;
+      tma::load_3d(fld(f), &p.map[f], x, y, z, bar);
+    }
+  }
+  // one thread polls the barrier (bounded) while the others sleep in the CTA
+  // barrier; on a timeout every thread leaves after the copies drain
+  bool ok = true;
+  if (tid == 0) ok = tma::mbar_wait(bar, 0, 1u << 24);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) {
+      atomicExch(p.err, 1u);
+      tma::mbar_wait(bar, 0, 1u << 22);
+    }
+    return;
+  }
+
+  const R* sU = fld(TC_U);
+  const R* sRX = fld(TC_RTJX);
+  const R* sV = fld(TC_V);
+  const R* sRY = fld(TC_RTJY);
+#define UF(k, d) sU[((k) + 1) * (kTmaCX + 4) + tx + (d)]
+#define RXF(k, d) sRX[((k) + 1) * (kTmaCX + 4) + tx + (d)]
+#define VF(k, r) sV[(((k) + 1) * 2 + (r)) * kTmaCX + tx]
+#define RYF(k, r) sRY[(((k) + 1) * 2 + (r)) * kTmaCX + tx]
+#define CF(f, k) fld(f)[((k) + 1) * kTmaCX + tx]
+  ColSmem<R, kTmaCX> S(reinterpret_cast<R*>(smem_tma + lay.work), nz + 1);
+#define SM(X, k) S.X[(k) * kTmaCX + tx]
+  const R dtau = a.dtau;
+  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
+  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
+  const size_t c2d = L.at2(active ? i : 0, j);
+  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
+  const R invJ = (R)1 / J;
+  const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
+  const bool terrain = hxc != (R)0 || hyc != (R)0;
+
+  // phase 1: Av and the terrain cross flux Sv (kernels.cu:552-568)
+  if (active)
+    for (int k = lane_k; k <= nz; k += kTmaKL) {
+      R av = 0, sv = 0;
+      if (k >= 1 && k < nz) {
+        av = CF(TC_AW, k);
+        if (terrain) {
+          R uw = (R)0.25 * (UF(k - 1, 0) + UF(k - 1, 1) + UF(k, 0) + UF(k, 1));
+          R vw = (R)0.25 * (VF(k - 1, 0) + VF(k - 1, 1) + VF(k, 0) + VF(k, 1));
+          sv = av * (uw * hxc + vw * hyc) * a.co.fac_w[L.at1(k)];
+        }
+      }
+      SM(Av, k) = av;
+      SM(Sv, k) = sv;
+    }
+  __syncthreads();
+  // phase 2: explicit pi' (kernels.cu:570-587)
+  if (active)
+    for (int k = lane_k; k < nz; k += kTmaKL) {
+      R Kt = CF(TC_KT3, k);
+      R Dh = (RXF(k, 1) * UF(k, 1) - RXF(k, 0) * UF(k, 0)) * mcx +
+             (RYF(k, 1) * VF(k, 1) - RYF(k, 0) * VF(k, 0)) * mcy;
+      R idz = a.co.inv_dzc[L.at1(k)];
+      R wk = CF(TC_W, k), wkp = CF(TC_W, k + 1);
+      R tpi = p.has_tpi ? CF(TC_TPI, k) : (R)0;
+      SM(P, k) = CF(TC_PI, k) + dtau * tpi -
+                 dtau * Kt *
+                     (Dh - (SM(Sv, k + 1) - SM(Sv, k)) * idz +
+                      c2 * (SM(Av, k + 1) * wkp - SM(Av, k) * wk) * idz);
+      SM(E, k) = dtau * Kt * c1 * idz;
+    }
+  __syncthreads();
+  // phase 3: tridiagonal rows (kernels.cu:589-611)
+  if (active)
+    for (int k = 1 + lane_k; k < nz; k += kTmaKL) {
+      const R iJdz = invJ * a.co.inv_dzw[L.at1(k)];
+      R thc = CF(TC_TH, k), thm = CF(TC_TH, k - 1);
+      R thbw = CF(TC_THBW, k);
+      R thvw = thbw + (R)0.5 * (thm + thc);
+      if (moist) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (CF(TC_QV, k - 1) + CF(TC_QV, k));
+      R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
+      R Em = SM(E, k - 1), Ek = SM(E, k);
+      SM(A, k) = -G * Em * SM(Av, k - 1);
+      SM(B, k) = (R)1 + G * SM(Av, k) * (Ek + Em);
+      SM(C, k) = -G * Ek * SM(Av, k + 1);
+      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
+      if (moist) {
+        R dqv = (R)0.5 * (CF(TC_QV, k - 1) + CF(TC_QV, k)) -
+                (R)0.5 * (CF(TC_QVB, k - 1) + CF(TC_QVB, k));
+        R qcr = (R)0.5 * (CF(TC_QC, k - 1) + CF(TC_QC, k)) + (R)0.5 * (CF(TC_QR, k - 1) + CF(TC_QR, k));
+        buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
+      }
+      R RHS = CF(TC_W, k) + dtau * (buoy + CF(TC_TW, k)) -
+              dtau * Phys<R>::cp * thvw * c2 * (CF(TC_PI, k) - CF(TC_PI, k - 1)) * iJdz;
+      SM(D, k) = RHS - G * (SM(P, k) - SM(P, k - 1));
+    }
+  __syncthreads();
+  // phase 4: Thomas sweep, one lane per column (kernels.cu:612-634)
+  if (active && lane_k == 0) {
+    R cprev = 0, dprev = 0;
+    R Ak = SM(A, 1), Bk = SM(B, 1), Ck = SM(C, 1), Dk = SM(D, 1);
+    for (int k = 1; k < nz; ++k) {
+      R An = 0, Bn = 1, Cn = 0, Dn = 0;
+      if (k + 1 < nz) {
+        An = SM(A, k + 1);
+        Bn = SM(B, k + 1);
+        Cn = SM(C, k + 1);
+        Dn = SM(D, k + 1);
+      }
+      R r, ck, dk;
+      if (k == 1) {
+        r = (R)1 / Bk;
+        ck = Ck * r;
+        dk = Dk * r;
+      } else {
+        r = (R)1 / (Bk - Ak * cprev);
+        ck = Ck * r;
+        dk = (Dk - Ak * dprev) * r;
+      }
+      SM(C, k) = ck;
+      SM(D, k) = dk;
+      cprev = ck;
+      dprev = dk;
+      Ak = An, Bk = Bn, Ck = Cn, Dk = Dn;
+    }
+    SM(Wn, nz) = 0;
+    R wabove = 0;
+    for (int k = nz - 1; k >= 1; --k) {
+      R wk = SM(D, k) - SM(C, k) * wabove;
+      SM(Wn, k) = wk;
+      wabove = wk;
+    }
+    R us = (R)0.5 * (UF(0, 0) + UF(0, 1));
+    R vs = (R)0.5 * (VF(0, 0) + VF(0, 1));
+    SM(Wn, 0) = us * hxc + vs * hyc;
+  }
+  __syncthreads();
+  // phase 5: pi', theta', w (kernels.cu:636-644)
+  if (active) {
+    const size_t c0 = L.at(i, j, 0), pl = L.plane();
+    for (int k = lane_k; k <= nz; k += kTmaKL) {
+      const size_t c = c0 + (size_t)k * pl;
+      if (k < nz) {
+        R wn = SM(Wn, k), wn1 = SM(Wn, k + 1);
+        a.pi_next[c] = SM(P, k) - SM(E, k) * (SM(Av, k + 1) * wn1 - SM(Av, k) * wn);
+        R wc = (R)0.5 * (wn + wn1);
+        a.th_out[c] = CF(TC_TH, k) + dtau * (CF(TC_TTH, k) - wc * CF(TC_DTHB, k));
+        a.w_out[c] = wn;
+      } else {
+        a.w_out[c] = 0;
+      }
+    }
+  }
+#undef UF
+#undef RXF
+#undef VF
+#undef RYF
+#undef CF
+#undef SM
+}
+
+template <typename R>
+size_t acoustic_column_tma_smem(int nz) {
+  if (nz + 2 > 256) return 0;  // a box extent is at most 256 elements
+  const size_t t = TmaColLayout<R>(nz).total;
+  return t <= 227 * 1024 ? t : 0;
+}
+
+template <typename R>
+int prepare_acoustic_column_tma(int nz) {
+  const size_t sm = acoustic_column_tma_smem<R>(nz);
+  if (!sm) return 2;
+  return cudaFuncSetAttribute(k_acoustic_column_tma<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm) == cudaSuccess
+             ? 0
+             : 1;
+}
+
+template <typename R>
+int launch_acoustic_column_tma(const TmaColParams<R>& p, cudaStream_t st) {
+  const size_t sm = acoustic_column_tma_smem<R>(p.a.L.nz);
+  if (!sm) return 2;
+  dim3 grd((p.a.L.nx + kTmaCX - 1) / kTmaCX, p.a.L.ny), blk(kTmaCX, kTmaKL);
+  k_acoustic_column_tma<R><<<grd, blk, sm, st>>>(p);
+  return 0;
+}
+
 // ------------------------------------------------------------ host launch
 template <typename R>
 void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,
@@ -593,6 +834,9 @@ int occupancy_column(int shape, int nz_max) {
 }
 
 #define WFE_INST(R)                                                                            \
+  template size_t acoustic_column_tma_smem<R>(int);                                            \
+  template int prepare_acoustic_column_tma<R>(int);                                            \
+  template int launch_acoustic_column_tma<R>(const TmaColParams<R>&, cudaStream_t);            \
   template dim3 grid_uv<R>(const Layout&);                                                     \
   template dim3 grid_column<R>(const Layout&, int);                                            \
   template void batch_uv<R>(const Batch<AcouArgs<R>>&, int, cudaStream_t);                     \

@@ -1,6 +1,7 @@
 // Argument blocks and launch entry points of the wfe_b200 device kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "core.cuh"
@@ -268,6 +269,36 @@ void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& 
                           R* rtjx, R* rtjy, R* kt3, R* aw, cudaStream_t st);
 template <typename R>
 void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st);
+// TMA variant of the column kernel (dyn_acou.cu): a CTA owns kTmaCX columns of
+// one row; every input column block (levels -1..nz) arrives in shared memory
+// by one bulk tensor load per field, then the five phases run from shared
+// memory.  Tensor maps, one per input field, in this order:
+enum {
+  TC_U = 0, TC_RTJX, TC_V, TC_RTJY,  // faces: u, rtjx (x faces i0..), v, rtjy (rows j, j+1)
+  TC_W, TC_PI, TC_TH, TC_TW, TC_TTH, TC_TPI, TC_AW, TC_KT3, TC_THBW, TC_DTHB,
+  TC_QV, TC_QC, TC_QR, TC_QVB, TC_N
+};
+constexpr int kTmaCX = 16;
+// box (x, y) extents of map f; the z extent is nz + 2 (levels -1 .. nz)
+WFE_HD void tma_col_box(int f, int* bx, int* by) {
+  *bx = (f == TC_U || f == TC_RTJX) ? kTmaCX + 4 : kTmaCX;
+  *by = (f == TC_V || f == TC_RTJY) ? 2 : 1;
+}
+template <typename R>
+struct TmaColParams {
+  AcouArgs<R> a;
+  unsigned* err;   // set to 1 when a tile's loads did not arrive in time
+  int has_tpi;     // TC_TPI map valid
+  CUtensorMap map[TC_N];
+};
+// shared memory of the TMA column kernel for nz levels (0: does not fit)
+template <typename R>
+size_t acoustic_column_tma_smem(int nz);
+template <typename R>
+int prepare_acoustic_column_tma(int nz);
+template <typename R>
+int launch_acoustic_column_tma(const TmaColParams<R>& p, cudaStream_t st);
+
 // shape: tile-shape index (columns x level lanes) in [0, acoustic_column_shapes());
 // one that does not fit the column depth falls back to the first that does
 template <typename R>

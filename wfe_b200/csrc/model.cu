@@ -12,6 +12,8 @@
 // substep and double-buffers u, v (U2, V2) and rotates pi' through three
 // buffers (X.pip, P1, P2), so the last substep lands in the stage output X
 // without any copy.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -85,6 +87,22 @@ void tune_store(const std::string& key, const Tune& t) {
 }
 }  // namespace
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda
+// link); null when the driver does not provide it
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
 #define CK(call)                                                                  \
   do {                                                                            \
     cudaError_t e__ = (call);                                                     \
@@ -106,6 +124,9 @@ class ModelT final : public Model {
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     if (prepare_acoustic_column<R>(g_.nz) || prepare_kessler<R>(g_.nz))
       return fail("nz too large for the column kernels' shared memory");
+    tma_ok_ = tensor_map_encoder() && prepare_acoustic_column_tma<R>(g_.nz) == 0;
+    CK(cudaMalloc(&tma_err_, sizeof(unsigned)));
+    CK(cudaMemset(tma_err_, 0, sizeof(unsigned)));
     const size_t n3 = L_.n3(), n2 = L_.n2(), n1 = L_.pz;
     // metric
     R* mbuf = alloc(4 * n1 + 8 * n2);
@@ -403,7 +424,7 @@ class ModelT final : public Model {
     if (enqueue_step((R)dt)) return 1;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st_));
-    return 0;
+    return check_tma();
   }
 
   int run(int nsteps, double dt, double t0) override {
@@ -496,6 +517,15 @@ class ModelT final : public Model {
   int sync() override {
     CK(cudaStreamSynchronize(st_));
     CK(cudaGetLastError());
+    return check_tma();
+  }
+
+  // a TMA tile that did not arrive in time leaves the flag set
+  int check_tma() {
+    if (!tma_err_) return 0;
+    unsigned e = 0;
+    CK(cudaMemcpy(&e, tma_err_, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) return fail("acoustic column: a TMA tile load timed out");
     return 0;
   }
 
@@ -694,7 +724,7 @@ class ModelT final : public Model {
     std::string name = prop.name;
     for (char& ch : name)
       if (ch == ' ') ch = '_';
-    k << "v2|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
+    k << "v3|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
       << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0);
     return k.str();
   }
@@ -719,7 +749,21 @@ class ModelT final : public Model {
     return 0;
   }
 
+  // WFE_COLUMN_VARIANT=<n> forces the acoustic column variant (0..5 tile
+  // shapes, 6 the TMA-staged kernel) after tuning, for tests and experiments
   int autotune(double dt) {
+    const bool first = !tune_.done;
+    int rc = autotune_variants(dt);
+    const char* cv = std::getenv("WFE_COLUMN_VARIANT");
+    if (first && cv && *cv) {
+      const int v = std::atoi(cv);
+      if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_)))
+        tune_.column_cx = v;
+    }
+    return rc;
+  }
+
+  int autotune_variants(double dt) {
     if (tune_.done) return 0;
     tune_.done = true;
     const char* env = std::getenv("WFE_TUNE");
@@ -747,7 +791,8 @@ class ModelT final : public Model {
     }
     best = 1e30f;
     const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
-    for (int cx = 0; cx < acoustic_column_shapes(); ++cx) {
+    const int nvar = acoustic_column_shapes() + (tma_ok_ ? 1 : 0);  // last: TMA-staged
+    for (int cx = 0; cx < nvar; ++cx) {
       float ms;
       tune_.column_cx = cx;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -931,12 +976,62 @@ class ModelT final : public Model {
       a.pi_next = pbuf(t + 1);
       int rc = 0;
       if (!record(K_UV, a)) launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
-      if (!record(K_COL, a))
-        launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, tune_.column_cx, st_); });
+      if (!record(K_COL, a)) {
+        if (tma_ok_ && tune_.column_cx == acoustic_column_shapes()) {
+          TmaColParams<R> tp;
+          if (tma_params(a, &tp)) return 1;
+          launch("acoustic_column", [&] { rc = launch_acoustic_column_tma<R>(tp, st_); });
+        } else {
+          launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, tune_.column_cx, st_); });
+        }
+      }
       if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
       uin = uout;
       vin = vout;
       piprev_ = const_cast<R*>(a.pi_cur);
+    }
+    return 0;
+  }
+
+  // tensor map of a pitched field for box f of the TMA column kernel (cached)
+  const CUtensorMap* tmap(const R* ptr, int f) {
+    int bx, by;
+    tma_col_box(f, &bx, &by);
+    const auto key = std::make_pair(static_cast<const void*>(ptr), bx * 16 + by);
+    auto it = tmaps_.find(key);
+    if (it != tmaps_.end()) return &it->second;
+    CUtensorMap m;
+    std::memset(&m, 0, sizeof(m));
+    const cuuint64_t dims[3] = {(cuuint64_t)L_.px, (cuuint64_t)L_.py, (cuuint64_t)L_.pz};
+    const cuuint64_t strides[2] = {(cuuint64_t)L_.px * sizeof(R), (cuuint64_t)L_.plane() * sizeof(R)};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)(g_.nz + 2)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = tensor_map_encoder()(
+        &m, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+        const_cast<R*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      fail("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+      return nullptr;
+    }
+    return &(tmaps_[key] = m);
+  }
+
+  int tma_params(const AcouArgs<R>& a, TmaColParams<R>* tp) {
+    std::memset(static_cast<void*>(tp), 0, sizeof(*tp));
+    tp->a = a;
+    tp->err = tma_err_;
+    tp->has_tpi = a.tpi != nullptr;
+    const R* src[TC_N] = {a.u_out,  a.co.rtjx, a.v_out, a.co.rtjy, a.w_in,   a.pi_cur,
+                          a.th_in,  a.tw,      a.tth,   a.tpi,     a.co.aw,  a.co.kt3,
+                          a.b.thbw, a.b.dthbdz, a.qv,   a.qc,      a.qr,     a.b.qvb};
+    for (int f = 0; f < TC_N; ++f) {
+      if (f == TC_TPI && !a.tpi) continue;
+      if (f >= TC_QV && !a.p.moisture) continue;
+      const CUtensorMap* m = tmap(src[f], f);
+      if (!m) return 1;
+      tp->map[f] = *m;
     }
     return 0;
   }
@@ -1094,6 +1189,8 @@ class ModelT final : public Model {
     if (wd_) cudaFree(wd_);
     if (mass_planes_) cudaFree(mass_planes_);
     if (mass_) cudaFree(mass_);
+    if (tma_err_) cudaFree(tma_err_);
+    tma_err_ = nullptr;
     if (stage_) cudaFreeHost(stage_);
     if (cs_st_) {
       cudaStreamSynchronize(cs_st_);
@@ -1158,6 +1255,9 @@ class ModelT final : public Model {
   bool graphs_valid_ = false;
   long gen_ = 0;  // changes whenever buffer roles or physics switches change
   std::vector<Rec>* rec_ = nullptr;  // record mode when set
+  bool tma_ok_ = false;              // TMA column variant usable
+  unsigned* tma_err_ = nullptr;      // set by a TMA tile load that timed out
+  std::map<std::pair<const void*, int>, CUtensorMap> tmaps_;
   cudaStream_t cs_st_ = nullptr;     // snapshot copy stream
   cudaEvent_t snap_ev_ = nullptr;
   void* snap_buf_ = nullptr;         // packed snapshot staging
