@@ -140,10 +140,3 @@ def test_autograd_function_gradient():
         assert np.linalg.norm(a - b) <= 1e-10 * max(np.linalg.norm(b), 1e-300), k
     assert np.linalg.norm(g["w"]) > 0
     c.close()
-
-
-def test_refuses_moist_cases():
-    c = W.Case(CASES / "wk82_small.ini", precision="f64")
-    with pytest.raises(W.WfeError, match="moist"):
-        c.lin_enable()
-    c.close()

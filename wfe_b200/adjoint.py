@@ -1,8 +1,9 @@
 """Forecast gradients through the tangent-linear and adjoint runs.
 
-``Forecast`` is a torch.autograd.Function over a dry Case: its forward maps
-the initial state x0 = (u, v, w, theta', pi') to the state after ``nsteps``
-large steps; its backward runs the adjoint (wfe_ad_run: checkpoints of the
+``Forecast`` is a torch.autograd.Function over a Case: its forward maps
+the initial state x0 = (u, v, w, theta', pi'[, qv, qc, qr]) -- the moisture
+species when the case carries them -- to the state after ``nsteps`` large
+steps; its backward runs the adjoint (wfe_ad_run: checkpoints of the
 state every ``every`` steps, recomputation in between) on the incoming
 gradients and returns dJ/dx0.  Fields are in the reference's padded layout
 (NZ, NY, NX) = (nz+7, ny+6, nx+6), which holds every prognostic point (with
@@ -17,6 +18,12 @@ from __future__ import annotations
 import numpy as np
 
 FIELDS5 = ("u", "v", "w", "thp", "pip")
+FIELDS8 = FIELDS5 + ("qv", "qc", "qr")
+
+
+def state_names(case) -> tuple:
+    """the prognostic fields of the case's state vector"""
+    return FIELDS8 if case.moisture else FIELDS5
 
 
 def set_fields(case, fields: dict, role: str = "state") -> None:
@@ -24,8 +31,8 @@ def set_fields(case, fields: dict, role: str = "state") -> None:
         case.set_field(k, np.ascontiguousarray(a, dtype=np.float64).reshape(case.shape), role=role)
 
 
-def get_fields(case, role: str = "state", names=FIELDS5) -> dict:
-    return {k: case.field(k, role=role) for k in names}
+def get_fields(case, role: str = "state", names=None) -> dict:
+    return {k: case.field(k, role=role) for k in (names or state_names(case))}
 
 
 def w_box_mask(case, x0: float, x1: float, z0: float, z1: float) -> np.ndarray:
@@ -74,27 +81,28 @@ try:
         """x0 -> xN of a dry Case; gradients through the adjoint run."""
 
         @staticmethod
-        def forward(ctx, case, nsteps, every, u, v, w, thp, pip):
-            x0 = {k: t.detach().to("cpu", torch.float64).numpy()
-                  for k, t in zip(FIELDS5, (u, v, w, thp, pip))}
-            ctx.case, ctx.nsteps, ctx.every, ctx.x0 = case, int(nsteps), int(every), x0
+        def forward(ctx, case, nsteps, every, *fields):
+            names = state_names(case)
+            x0 = {k: t.detach().to("cpu", torch.float64).numpy() for k, t in zip(names, fields)}
+            ctx.case, ctx.nsteps, ctx.every, ctx.x0, ctx.names = case, int(nsteps), int(every), x0, names
             case.lin_enable()
             set_fields(case, x0)
             case.run(ctx.nsteps)
             out = get_fields(case)
-            return tuple(torch.from_numpy(out[k]).to(u.device, u.dtype) for k in FIELDS5)
+            ref = fields[0]
+            return tuple(torch.from_numpy(out[k]).to(ref.device, ref.dtype) for k in names)
 
         @staticmethod
         def backward(ctx, *grads):
             ybar = {k: (g.detach().to("cpu", torch.float64).numpy() if g is not None
-                        else np.zeros_like(ctx.x0[k])) for k, g in zip(FIELDS5, grads)}
+                        else np.zeros_like(ctx.x0[k])) for k, g in zip(ctx.names, grads)}
             gx = adjoint(ctx.case, ctx.x0, ybar, ctx.nsteps, ctx.every)
-            dev = grads[0].device if grads[0] is not None else "cpu"
-            return (None, None, None) + tuple(torch.from_numpy(gx[k]).to(dev) for k in FIELDS5)
+            dev = next((g.device for g in grads if g is not None), "cpu")
+            return (None, None, None) + tuple(torch.from_numpy(gx[k]).to(dev) for k in ctx.names)
 
     def forecast(case, nsteps: int, x0: dict, every: int = 30):
-        """dict of torch tensors x0 -> tuple of the five final fields (autograd)."""
-        return Forecast.apply(case, nsteps, every, *[x0[k] for k in FIELDS5])
+        """dict of torch tensors x0 -> tuple of the final state fields (autograd)."""
+        return Forecast.apply(case, nsteps, every, *[x0[k] for k in state_names(case)])
 
 except ImportError:  # torch is optional for the numpy entry points
     Forecast = None

@@ -212,11 +212,12 @@ dim3 grid_sfc(const Layout& L, int sub);
 template <typename R>
 void batch_sfc(const Batch<SfcArgs<R>>& b, int sub, int nblocks, cudaStream_t st);
 
-// Tangent-linear (tl_) and adjoint (ad_) launches of the dry dynamics
-// (lin.cu): a is the forward argument block of the linearised launch, d the
-// same block over the tangent or adjoint buffers.  The TL of the ghost fill
-// and of the mass fluxes is the forward launch on d.  The column launches
-// return 2 when nz exceeds lin_max_levels().
+// Tangent-linear (tl_) and adjoint (ad_) launches of the dynamics (lin.cu)
+// and of the Kessler column (lin_kessler.cu): a is the forward argument block
+// of the linearised launch, d the same block over the tangent or adjoint
+// buffers.  The TL of the ghost fill and of the mass fluxes is the forward
+// launch on d.  The column launches return 2 when nz exceeds
+// lin_max_levels().
 template <typename R>
 void ad_fill(const FillArgs<R>& d, cudaStream_t st);
 template <typename R>
@@ -233,11 +234,17 @@ template <typename R>
 int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
 template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+template <typename R>
+void tl_kessler(const KesArgs<R>& a, const KesArgs<R>& d, cudaStream_t st);
+template <typename R>
+void ad_kessler(const KesArgs<R>& a, const KesArgs<R>& d, cudaStream_t st);
 int lin_max_levels();
 // shared-memory limits of the linearised column kernels for nz levels (once,
 // outside any stream capture); 2 when nz exceeds lin_max_levels()
 template <typename R>
 int lin_prepare(int nz);
+template <typename R>
+int lin_kessler_prepare(int nz);
 // zero a cell field outside the interior cells (the pi' ghost ring, which no
 // launch of a step reads or writes)
 template <typename R>

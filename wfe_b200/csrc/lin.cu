@@ -1,4 +1,4 @@
-// Tangent-linear (TL) and adjoint (AD) kernels of the dry dynamics, linearised
+// Tangent-linear (TL) and adjoint (AD) kernels of the dynamics, linearised
 // about the forward trajectory (the forward buffers hold the values of the
 // step being linearised when these run).
 //
@@ -18,8 +18,11 @@
 //
 // Upwind selections, the radiation-boundary branch and the w(nz) = 0 lid are
 // frozen at the trajectory (the derivative of a piecewise-smooth step almost
-// everywhere).  Moisture, the positive-definite limiter, Davies relaxation,
-// w damping and the physics columns are not linearised here; the host refuses
+// everywhere).  Moisture enters as advected species (tendency rows with
+// their stage update), through theta_v in the pressure-gradient terms and
+// through the moist buoyancy of the column; the Kessler column has its own
+// TL/AD (lin_kessler.cu).  The positive-definite limiter, Davies relaxation,
+// w damping and the surface physics are not linearised; the host refuses
 // cases that use them.
 #include <cuda_runtime.h>
 
@@ -66,7 +69,7 @@ __device__ __forceinline__ void face5_weights(R vel, R w[6]) {
 __device__ __forceinline__ size_t off(size_t c, long d) { return (size_t)((long)c + d); }
 
 // ================================================================ tendencies
-enum { T_U = 0, T_V, T_W, T_TH, T_MFX, T_MFY, T_MFZ, T_N };
+enum { T_U = 0, T_V, T_W, T_TH, T_MFX, T_MFY, T_MFZ, T_QV, T_QC, T_QR, T_N };
 
 // Contribution cF * dF of one flux F = fv face5(Q[c + (b + n) s], fv): fv is
 // 0.5 (MF[ma] + MF[mb]) (avg) or MF[ma].
@@ -230,11 +233,31 @@ __device__ void row_tth(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   if (a.p.diff_K > (R)0) emit_lap(acc, a, T_TH, i, j, k, false, a.p.diff_K);
 }
 
+// moisture species tendency row: flux-form advection only (kernels.cu:886-899)
+template <typename R, class Acc>
+__device__ void row_tq(Acc& acc, const TendArgs<R>& a, const R* q, int qid, int i, int j, int k) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  const long sx = 1, sy = L.px, sz = (long)L.plane();
+  const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
+  const R dzc = a.m.dzeta_c[kk];
+  emit_face(acc, (R)1 / (a.dx * rt), a.mfx, T_MFX, c, c, false, q, qid, c, sx, -3);
+  emit_face(acc, -(R)1 / (a.dx * rt), a.mfx, T_MFX, off(c, sx), 0, false, q, qid, c, sx, -2);
+  emit_face(acc, (R)1 / (a.dy * rt), a.mfy, T_MFY, c, c, false, q, qid, c, sy, -3);
+  emit_face(acc, -(R)1 / (a.dy * rt), a.mfy, T_MFY, off(c, sy), 0, false, q, qid, c, sy, -2);
+  emit_face(acc, (R)1 / (dzc * rt), a.mfz, T_MFZ, c, c, false, q, qid, c, sz, -3);
+  emit_face(acc, -(R)1 / (dzc * rt), a.mfz, T_MFZ, off(c, sz), 0, false, q, qid, c, sz, -2);
+  emit_div(acc, a, i, j, k, q[c] / rt);
+  acc(qid, c, div_value(a, i, j, k) / rt);
+}
+
 template <typename R>
 __device__ __forceinline__ Ptrs<R, T_N> tend_ptrs(const TendArgs<R>& d) {
   return Ptrs<R, T_N>{{const_cast<R*>(d.u), const_cast<R*>(d.v), const_cast<R*>(d.w),
                        const_cast<R*>(d.thp), const_cast<R*>(d.mfx), const_cast<R*>(d.mfy),
-                       const_cast<R*>(d.mfz)}};
+                       const_cast<R*>(d.mfz), const_cast<R*>(d.qv), const_cast<R*>(d.qc),
+                       const_cast<R*>(d.qr)}};
 }
 
 template <typename R>
@@ -267,6 +290,18 @@ __global__ void __launch_bounds__(256) k_tl_tend(TendArgs<R> a, TendArgs<R> d) {
     d.tth[c] = acc.sum;
   }
   if (d.tpi) d.tpi[c] = 0;  // pi' has no slow tendency without Davies relaxation
+  if (a.p.moisture) {
+    const R* qf[3] = {a.qv, a.qc, a.qr};
+    R* qo[3] = {d.qo_v, d.qo_c, d.qo_r};
+    const R* qn[3] = {d.qn_v, d.qn_c, d.qn_r};
+    R* tq[3] = {d.tqv, d.tqc, d.tqr};
+    for (int sp = 0; sp < 3; ++sp) {
+      TLAcc<R, T_N> acc{P, 0};
+      row_tq(acc, a, qf[sp], T_QV + sp, i, j, k);
+      if (qo[sp]) qo[sp][c] = qn[sp][c] + a.dt_stage * acc.sum;  // stage value (kernels.cu:268-273)
+      else tq[sp][c] = acc.sum;
+    }
+  }
 }
 
 template <typename R>
@@ -299,6 +334,26 @@ __global__ void __launch_bounds__(256) k_ad_tend(TendArgs<R> a, TendArgs<R> d) {
     if (acc.ybar != (R)0) row_tth(acc, a, i, j, k);
   }
   if (d.tpi) d.tpi[c] = 0;
+  if (a.p.moisture) {
+    const R* qf[3] = {a.qv, a.qc, a.qr};
+    R* qo[3] = {d.qo_v, d.qo_c, d.qo_r};
+    R* qn[3] = {const_cast<R*>(d.qn_v), const_cast<R*>(d.qn_c), const_cast<R*>(d.qn_r)};
+    R* tq[3] = {d.tqv, d.tqc, d.tqr};
+    for (int sp = 0; sp < 3; ++sp) {
+      R g;
+      if (qo[sp]) {
+        const R gq = qo[sp][c];
+        qo[sp][c] = 0;
+        if (gq != (R)0) atomicAdd(qn[sp] + c, gq);
+        g = a.dt_stage * gq;
+      } else {
+        g = tq[sp][c];
+        tq[sp][c] = 0;
+      }
+      ADAcc<R, T_N> acc{P, g};
+      if (g != (R)0) row_tq(acc, a, qf[sp], T_QV + sp, i, j, k);
+    }
+  }
 }
 
 // ================================================================ ghost fill
@@ -389,13 +444,14 @@ __global__ void k_ad_flux(FluxArgs<R> A) {
 }
 
 // ============================================================== acoustic u, v
-enum { A_UIN = 0, A_VIN, A_PICUR, A_PIPREV, A_NPIP, A_THIN, A_NTHP, A_TU, A_TV, A_N };
+enum { A_UIN = 0, A_VIN, A_PICUR, A_PIPREV, A_NPIP, A_THIN, A_NTHP, A_TU, A_TV, A_QV, A_N };
 
 template <typename R>
 __device__ __forceinline__ Ptrs<R, A_N> acou_ptrs(const AcouArgs<R>& d) {
   return Ptrs<R, A_N>{{const_cast<R*>(d.u_in), const_cast<R*>(d.v_in), const_cast<R*>(d.pi_cur),
                        const_cast<R*>(d.pi_prev), const_cast<R*>(d.n_pip), const_cast<R*>(d.th_in),
-                       const_cast<R*>(d.n_thp), const_cast<R*>(d.tu), const_cast<R*>(d.tv)}};
+                       const_cast<R*>(d.n_thp), const_cast<R*>(d.tu), const_cast<R*>(d.tv),
+                       const_cast<R*>(d.qv)}};
 }
 
 // coef * d pi*(i, j, k) (dyn_common.cuh pistar)
@@ -416,16 +472,22 @@ __device__ __forceinline__ void emit_pistar(Acc& acc, const AcouArgs<R>& a, int 
   }
 }
 
-// coef * d theta_v(i, j, k) of the dry state (dyn_common.cuh theta_v)
+// coef * d theta_v(i, j, k) (dyn_common.cuh theta_v): theta' and, moist, qv
 template <typename R, class Acc>
 __device__ __forceinline__ void emit_thv(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R coef) {
   const Layout& L = a.L;
   const bool lat = i < 0 || i >= L.nx || j < 0 || j >= L.ny;
-  if (lat)
-    acc(A_NTHP, L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open), map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), k),
-        coef);
-  else
-    acc(A_THIN, L.at(i, j, k), coef);
+  const size_t c = L.at(i, j, k);
+  const size_t s =
+      lat ? L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open), map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), k)
+          : c;
+  R f = coef;
+  if (a.p.moisture) {
+    const R th = a.b.thb[c] + (lat ? a.n_thp[s] : a.th_in[c]);
+    f = coef * ((R)1 + Phys<R>::eps61 * a.qv[s]);
+    acc(A_QV, s, coef * th * Phys<R>::eps61);
+  }
+  acc(lat ? A_NTHP : A_THIN, s, f);
 }
 
 // forward u (is_u) or v step at a face and, when acc is given, coef times
@@ -705,6 +767,7 @@ __device__ void column_values_s(const AcouArgs<R>& a, int i, int j, bool active,
       const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
       R thc = a.th_in[c], thm = a.th_in[cm];
       R thvw = a.b.thbw[c] + (R)0.5 * (thm + thc);
+      if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
       R g = dtau * Phys<R>::cp * thvw * c1 / (J * a.m.dzeta_w[kk]);
       const int q = k * LCX;
       G[q] = g;
@@ -712,6 +775,11 @@ __device__ void column_values_s(const AcouArgs<R>& a, int i, int j, bool active,
       B[q] = (R)1 + g * Av[q] * (E[q] + E[q - LCX]);
       C[q] = -g * E[q] * Av[q + LCX];
       R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / a.b.thbw[c];
+      if (a.p.moisture) {
+        R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
+        R qcr = (R)0.5 * (a.qc[cm] + a.qc[c]) + (R)0.5 * (a.qr[cm] + a.qr[c]);
+        buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
+      }
       R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
               dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) / (J * a.m.dzeta_w[kk]);
       D[q] = RHS - g * (P[q] - P[q - LCX]);
@@ -787,10 +855,20 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
       const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
       const int q = k * LCX;
       const R jdz = J * a.m.dzeta_w[kk];
-      const R thvw = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      R thvw = thd;
       R dthvw = (R)0.5 * (dth[q - LCX] + dth[q]);
-      R g = dtau * Phys<R>::cp * dthvw * c1 / jdz;
       R dbuoy = Phys<R>::grav * (R)0.5 * (dth[q - LCX] + dth[q]) / a.b.thbw[c];
+      if (a.p.moisture) {
+        // theta_v = theta (1 + 0.61 qv); buoyancy + g (0.61 qv' - qc - qr)
+        const R mq = (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
+        const R dqv = (R)0.5 * (d.qv[cm] + d.qv[c]);
+        thvw = thd * mq;
+        dthvw = dthvw * mq + thd * Phys<R>::eps61 * dqv;
+        dbuoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - (R)0.5 * (d.qc[cm] + d.qc[c]) -
+                                  (R)0.5 * (d.qr[cm] + d.qr[c]));
+      }
+      R g = dtau * Phys<R>::cp * dthvw * c1 / jdz;
       R dpi = d.pi_cur[c] - d.pi_cur[cm], pi = a.pi_cur[c] - a.pi_cur[cm];
       R dRHS = d.w_in[c] + dtau * (dbuoy + d.tw[c]) -
                dtau * Phys<R>::cp * c2 * (dthvw * pi + thvw * dpi) / jdz;
@@ -848,10 +926,16 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   R* twB = const_cast<R*>(d.tw);
   R* tthB = const_cast<R*>(d.tth);
   R* tpiB = const_cast<R*>(d.tpi);
+  R* qvI = const_cast<R*>(d.qv);
+  R* qcI = const_cast<R*>(d.qc);
+  R* qrI = const_cast<R*>(d.qr);
+  const bool moist = a.p.moisture != 0;
   const long sx = 1, sy = L.px;
   R *wb = S[A_WB] + tx, *pb = S[A_PB] + tx, *tb = S[A_TB] + tx, *ws = S[A_WS] + tx;
   R *lam = S[A_LAM] + tx, *GL = S[A_GL] + tx, *PIB = S[A_PIB] + tx, *THB = S[A_THB] + tx;
   R *KTD = S[A_KTD] + tx;
+  // the sweep's scratch rows, free once the transposed solve is done
+  R *QVB = S[V_CS] + tx, *QCB = S[V_DS] + tx;
   // output adjoints, read and cleared before the (possibly aliased) inputs gain theirs
   if (active)
     for (int k = lane; k <= nz; k += LKL) {
@@ -905,6 +989,8 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
         GL[q] = 0;
         PIB[q] = 0;
         THB[q] = 0;
+        QVB[q] = 0;
+        QCB[q] = 0;
         continue;
       }
       const int kk = L.at1(k);
@@ -916,13 +1002,18 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
       const R Cb = k < nz - 1 ? -lm * W[q + LCX] : (R)0;
       const R Gb = Ab * (-E[q - LCX] * Av[q - LCX]) + Bb * (Av[q] * (E[q] + E[q - LCX])) +
                    Cb * (-E[q] * Av[q + LCX]) - lm * (P[q] - P[q - LCX]);
-      const R thvw = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      const R mq = moist ? (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]) : (R)1;
+      const R thvw = thd * mq;
       const R pi = a.pi_cur[c] - a.pi_cur[cm];
       GL[q] = G[q] * lm;
       PIB[q] = -dtau * Phys<R>::cp * thvw * c2 / jdz * lm;
       const R thvwb = -dtau * Phys<R>::cp * c2 * pi / jdz * lm + Gb * dtau * Phys<R>::cp * c1 / jdz;
       const R bt = Phys<R>::grav * (R)0.5 / a.b.thbw[c] * dtau * lm;
-      THB[q] = (R)0.5 * thvwb + bt;
+      THB[q] = (R)0.5 * thvwb * mq + bt;
+      // per level of the pair (k-1, k): qv through theta_v and buoyancy, qc and qr through buoyancy
+      QVB[q] = (R)0.5 * Phys<R>::eps61 * (thvwb * thd + Phys<R>::grav * dtau * lm);
+      QCB[q] = -(R)0.5 * Phys<R>::grav * dtau * lm;
       twB[c] += dtau * lm;
     }
   __syncthreads();
@@ -951,6 +1042,14 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
       if (k >= 1) th += THB[q];
       if (k + 1 < nz) th += THB[q + LCX];
       thI[c] += th;
+      if (moist) {
+        R qvs = 0, qcs = 0;
+        if (k >= 1) qvs += QVB[q], qcs += QCB[q];
+        if (k + 1 < nz) qvs += QVB[q + LCX], qcs += QCB[q + LCX];
+        qvI[c] += qvs;
+        qcI[c] += qcs;
+        qrI[c] += qcs;
+      }
       tthB[c] += dtau * tb[q];
       KTD[q] = Kt / a.m.dzeta_c[kk] * Pb;
     }
@@ -1060,7 +1159,7 @@ int lin_prepare(int nz) {
       cudaFuncSetAttribute(k_ad_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)lin_col_smem<R, A_NARR>(nz)) != cudaSuccess)
     return 1;
-  return 0;
+  return lin_kessler_prepare<R>(nz);
 }
 
 template <typename R>

@@ -1,4 +1,5 @@
-// Tangent-linear and adjoint runs of the dry dynamics (Lin, model.hpp).
+// Tangent-linear and adjoint runs of the model step (Lin, model.hpp): the
+// dynamics with moisture and the Kessler column.
 //
 // The step is taken from the model's own recorded launch sequence, so the
 // linearised runs follow the forward's buffer rotation exactly: every
@@ -187,7 +188,17 @@ class LinT final : public Lin {
     for (const R** p : {&d.u, &d.v, &d.w, &d.thp, &d.pip, &d.qv, &d.qc, &d.qr, &d.mfx, &d.mfy,
                         &d.mfz})
       *p = D(*p);
-    for (R** p : {&d.tu, &d.tv, &d.tw, &d.tth, &d.tpi}) *p = D(*p);
+    for (R** p : {&d.tu, &d.tv, &d.tw, &d.tth, &d.tpi, &d.tqv, &d.tqc, &d.tqr, &d.qo_v, &d.qo_c,
+                  &d.qo_r})
+      *p = D(*p);
+    for (const R** p : {&d.qn_v, &d.qn_c, &d.qn_r}) *p = D(*p);
+    return d;
+  }
+  KesArgs<R> tr(const KesArgs<R>& a) const {
+    KesArgs<R> d = a;
+    for (R** p : {&d.thp, &d.qv, &d.qc, &d.qr}) *p = D(*p);
+    d.pip = D(a.pip);
+    d.rain = nullptr;  // a diagnostic, not linearised
     return d;
   }
   AcouArgs<R> tr(const AcouArgs<R>& a) const {
@@ -201,7 +212,8 @@ class LinT final : public Lin {
 
   int unsupported(int kind) { return fail("launch kind " + std::to_string(kind) + " is not linearised"); }
 
-  int fwd(const Rec& r) {
+  // replay: a recomputation inside the adjoint sweep, whose rain goes to scratch
+  int fwd(const Rec& r, bool replay = false) {
     switch (r.kind) {
       case K_FILL: {
         const auto& a = as<FillArgs<R>>(r);
@@ -219,6 +231,12 @@ class LinT final : public Lin {
         if (launch_acoustic_column<R>(as<AcouArgs<R>>(r), m_->column_shape(), st_))
           return fail("acoustic column launch");
         break;
+      case K_KES: {
+        KesArgs<R> a = as<KesArgs<R>>(r);
+        if (replay) a.rain = rain_scratch_;
+        if (launch_kessler<R>(a, st_)) return fail("Kessler launch");
+        break;
+      }
       default: return unsupported(r.kind);
     }
     return 0;
@@ -251,6 +269,11 @@ class LinT final : public Lin {
         if (tl_column<R>(a, tr(a), st_)) return fail("column deeper than the linearised kernels hold");
         break;
       }
+      case K_KES: {
+        const auto& a = as<KesArgs<R>>(r);
+        tl_kessler<R>(a, tr(a), st_);
+        break;
+      }
       default: return unsupported(r.kind);
     }
     return 0;
@@ -273,6 +296,11 @@ class LinT final : public Lin {
       case K_COL: {
         const auto& a = as<AcouArgs<R>>(r);
         if (ad_column<R>(a, tr(a), st_)) return fail("column deeper than the linearised kernels hold");
+        break;
+      }
+      case K_KES: {
+        const auto& a = as<KesArgs<R>>(r);
+        ad_kessler<R>(a, tr(a), st_);
         break;
       }
       default: return unsupported(r.kind);
@@ -298,6 +326,12 @@ class LinT final : public Lin {
         const auto& a = as<TendArgs<R>>(r);
         *o = {a.tu, a.tv, a.tw, a.tth};
         if (a.tpi) o->push_back(a.tpi);
+        if (a.p.moisture) {
+          const bool stage = a.qo_v != nullptr;
+          o->push_back(stage ? a.qo_v : a.tqv);
+          o->push_back(stage ? a.qo_c : a.tqc);
+          o->push_back(stage ? a.qo_r : a.tqr);
+        }
         break;
       }
       case K_UV: {
@@ -308,6 +342,11 @@ class LinT final : public Lin {
       case K_COL: {
         const auto& a = as<AcouArgs<R>>(r);
         *o = {a.w_out, a.pi_next, a.th_out};
+        break;
+      }
+      case K_KES: {
+        const auto& a = as<KesArgs<R>>(r);
+        *o = {a.thp, a.qv, a.qc, a.qr};
         break;
       }
       default: break;
@@ -389,6 +428,7 @@ class LinT final : public Lin {
         outputs(r, &o);
         slots += o.size();
       }
+    if (!rain_scratch_) LCK(cudaMalloc(&rain_scratch_, L_.n2() * sizeof(R)));
     if (slots > log_cap_) {  // outside any capture
       if (log_) cudaFree(log_);
       log_ = nullptr;
@@ -408,7 +448,7 @@ class LinT final : public Lin {
                                     st_));
                 ++slot;
               }
-              if (fwd(r)) return 1;
+              if (fwd(r, true)) return 1;
             }
           return 0;
         }))
@@ -496,6 +536,8 @@ class LinT final : public Lin {
     bufs_.clear();
     if (log_) cudaFree(log_);
     log_ = nullptr;
+    if (rain_scratch_) cudaFree(rain_scratch_);
+    rain_scratch_ = nullptr;
   }
 
   Model* m_ = nullptr;
@@ -506,6 +548,7 @@ class LinT final : public Lin {
   Layout L_{};
   R* log_ = nullptr;
   size_t log_cap_ = 0;
+  R* rain_scratch_ = nullptr;  // rain of the adjoint sweep's forward replays
   double dt_ = -1;
   cudaGraphExec_t tl_graph_[3] = {nullptr, nullptr, nullptr};
   std::map<long, SegGraphs> seg_;

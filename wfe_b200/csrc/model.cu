@@ -690,7 +690,7 @@ class ModelT final : public Model {
   int column_shape() const override { return tune_.column_cx; }
   void set_lin_map(std::function<void*(const void*)> map) override { lin_map_ = std::move(map); }
   bool linearisable(std::string* why) const override {
-    if (dp_.moisture) *why = "moist cases are not linearised";
+    if (dp_.moisture && dp_.pd_moist) *why = "the positive-definite moisture limiter is not linearised";
     else if (bdy_on_) *why = "Davies relaxation is not linearised";
     else if (sfc_on_) *why = "the surface physics is not linearised";
     else if (dp_.w_damping) *why = "w damping is not linearised";

@@ -13,31 +13,9 @@
 
 #include "core.cuh"
 #include "kernels.cuh"
+#include "phys_common.cuh"
 
 namespace wfe {
-
-template <typename R>
-__device__ __forceinline__ R qsat_w(R p, R T) {  // src/core/thermo.hpp:11-17
-  R es = (R)610.78 * exp((R)17.269 * (T - (R)273.16) / (T - (R)35.86));
-  R den = p - es;
-  if (den < (R)1) den = (R)1;
-  return (R)0.622 * es / den;
-}
-template <typename R>
-__device__ __forceinline__ R qsat_i(R p, R T) {  // src/core/thermo.hpp:20-26
-  R es = (R)610.78 * exp((R)21.875 * (T - (R)273.16) / (T - (R)7.66));
-  R den = p - es;
-  if (den < (R)1) den = (R)1;
-  return (R)0.622 * es / den;
-}
-
-template <typename R>
-__device__ __forceinline__ R fall_speed(R rq, R rho_sfc, R rho, R T) {
-  // kessler.cu:195-211: 36.34 (rho qr)^0.1364 sqrt(rho0/rho), x0.35 below freezing
-  return rq > (R)1e-9 ? (R)36.34 * pow(rq, (R)0.1364) * sqrt(rho_sfc / rho) *
-                            (T < Phys<R>::Tfrz ? (R)0.35 : (R)1)
-                      : (R)0;
-}
 
 template <typename R, int CX>
 __device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by) {
@@ -123,61 +101,17 @@ __device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by
   if (active && lane == 0) a.rain[L.at2(i, j)] += acc;
 
   // 3) conversions, evaporation and mixed-phase saturation adjustment,
-  //    independent per level (kessler.cu:239-297)
+  //    independent per level (kessler.cu:239-297; phys_common.cuh)
   if (active)
     for (int k = lane; k < nz; k += KL) {
       const size_t c = L.at(i, j, k);
-      const R k1 = (R)0.001, qc0 = (R)0.001;
-      R qvk = a.qv[c] > (R)0 ? a.qv[c] : (R)0;
-      R qck = a.qc[c] > (R)0 ? a.qc[c] : (R)0;
-      R qrk = S(qrl, k) > (R)0 ? S(qrl, k) : (R)0;
-      R rh = S(rhol, k);
-      R pi = a.b.pib[c] + a.pip[c];
-      R thp = a.thp[c];
-      R th = a.b.thb[c] + thp;
-      R T = th * pi;
-      R pres = Phys<R>::p00 * pow(pi, Phys<R>::cp / Phys<R>::Rd);
-      R fl = (T - (R)233.15) / (R)40;
-      fl = fmax((R)0, fmin((R)1, fl));
-      R qsw = qsat_w(pres, T);
-      R qs = fl * qsw + ((R)1 - fl) * qsat_i(pres, T);
-      R Leff = fl * Phys<R>::Lv + ((R)1 - fl) * Phys<R>::Ls;
-      R dqauto = k1 * (qck > qc0 ? qck - qc0 : (R)0);
-      R dqacc = (R)2.2 * qck * pow(qrk > (R)1e-9 ? qrk : (R)1e-9, (R)0.875);
-      R dqr = a.dt * (dqauto + dqacc);
-      if (dqr > qck) dqr = qck;
-      qck -= dqr;
-      qrk += dqr;
-      if (qvk < qs && qrk > (R)0) {
-        R rq = rh * qrk;
-        R vent = (R)1.6 + (R)124.9 * pow(rq, (R)0.2046);
-        R ern = vent * pow(rq, (R)0.525) / ((R)2.55e8 / (pres * qs) + (R)5.4e5) * (qs - qvk) /
-                (rh * qs);
-        R dqe = a.dt * ern;
-        if (dqe > qrk) dqe = qrk;
-        if (dqe > qs - qvk) dqe = qs - qvk;
-        qrk -= dqe;
-        qvk += dqe;
-        thp -= Leff * dqe / (Phys<R>::cp * pi);
-        th = a.b.thb[c] + thp;
-        T = th * pi;
-        R fl2 = fmax((R)0, fmin((R)1, (T - (R)233.15) / (R)40));
-        qs = fl2 * qsat_w(pres, T) + ((R)1 - fl2) * qsat_i(pres, T);
-      }
-      R gam = Leff * Leff * qs / (Phys<R>::cp * Phys<R>::Rv * T * T);
-      R dq = (qvk - qs) / ((R)1 + gam);
-      if (dq < (R)0) {
-        R evap = -dq;
-        if (evap > qck) evap = qck;
-        dq = -evap;
-      }
-      qvk -= dq;
-      qck += dq;
-      thp += Leff * dq / (Phys<R>::cp * pi);
+      R thp = a.thp[c], qv = a.qv[c], qc = a.qc[c], qr = S(qrl, k);
+      const R pip = a.pip[c];
+      kessler_convert<R, R>(thp, qv, qc, qr, pip, S(rhol, k), a.b.thb[c], a.b.pib[c], a.dt);
       a.thp[c] = thp;
-      a.qv[c] = qvk > (R)0 ? qvk : (R)0;
-      a.qc[c] = qck > (R)0 ? qck : (R)0;
-      a.qr[c] = qrk > (R)0 ? qrk : (R)0;
+      a.qv[c] = qv;
+      a.qc[c] = qc;
+      a.qr[c] = qr;
     }
 #undef S
 }
