@@ -228,12 +228,17 @@ template <typename R>
 void ad_tend(const TendArgs<R>& a, const TendArgs<R>& d, cudaStream_t st);
 template <typename R>
 void tl_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+// scratch cell fields of the gather-form adjoints (six, n3 each)
 template <typename R>
-void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+struct LinScratch {
+  R* f[6];
+};
+template <typename R>
+void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st);
 template <typename R>
 int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
 template <typename R>
-int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st);
 template <typename R>
 void tl_kessler(const KesArgs<R>& a, const KesArgs<R>& d, cudaStream_t st);
 template <typename R>

@@ -304,7 +304,12 @@ __global__ void __launch_bounds__(256) k_tl_tend(TendArgs<R> a, TendArgs<R> d) {
   }
 }
 
-template <typename R>
+// The adjoint runs as one launch per output group (PART: AD_U, AD_V, AD_W,
+// AD_TH with the pi' tendency, AD_Q for the three species): each launch is a
+// small kernel, where the fused one stalled on instruction fetch.
+enum { AD_U = 0, AD_V, AD_W, AD_TH, AD_Q };
+
+template <typename R, int PART>
 __global__ void __launch_bounds__(256) k_ad_tend(TendArgs<R> a, TendArgs<R> d) {
   const Layout& L = a.L;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -313,45 +318,59 @@ __global__ void __launch_bounds__(256) k_ad_tend(TendArgs<R> a, TendArgs<R> d) {
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
   const size_t c = L.at(i, j, k);
   const Ptrs<R, T_N> P = tend_ptrs(d);
-  {
+  // each output adjoint is cleared once it has been read and used (a store
+  // issued while the load of the same address is in flight stalls the
+  // memory pipeline)
+  if (PART == AD_U) {
     ADAcc<R, T_N> acc{P, d.tu[c]};
-    d.tu[c] = 0;
-    if (acc.ybar != (R)0) row_tu(acc, a, i, j, k);
-  }
-  {
+    if (acc.ybar != (R)0) {
+      row_tu(acc, a, i, j, k);
+      d.tu[c] = 0;
+    }
+  } else if (PART == AD_V) {
     ADAcc<R, T_N> acc{P, d.tv[c]};
-    d.tv[c] = 0;
-    if (acc.ybar != (R)0) row_tv(acc, a, i, j, k);
-  }
-  if (k >= 1) {
-    ADAcc<R, T_N> acc{P, d.tw[c]};
-    d.tw[c] = 0;
-    if (acc.ybar != (R)0) row_tw(acc, a, i, j, k);
-  }
-  {
+    if (acc.ybar != (R)0) {
+      row_tv(acc, a, i, j, k);
+      d.tv[c] = 0;
+    }
+  } else if (PART == AD_W) {
+    if (k >= 1) {
+      ADAcc<R, T_N> acc{P, d.tw[c]};
+      if (acc.ybar != (R)0) {
+        row_tw(acc, a, i, j, k);
+        d.tw[c] = 0;
+      }
+    }
+  } else if (PART == AD_TH) {
     ADAcc<R, T_N> acc{P, d.tth[c]};
-    d.tth[c] = 0;
-    if (acc.ybar != (R)0) row_tth(acc, a, i, j, k);
-  }
-  if (d.tpi) d.tpi[c] = 0;
-  if (a.p.moisture) {
+    if (acc.ybar != (R)0) {
+      row_tth(acc, a, i, j, k);
+      d.tth[c] = 0;
+    }
+    if (d.tpi && d.tpi[c] != (R)0) d.tpi[c] = 0;
+  } else {
     const R* qf[3] = {a.qv, a.qc, a.qr};
     R* qo[3] = {d.qo_v, d.qo_c, d.qo_r};
     R* qn[3] = {const_cast<R*>(d.qn_v), const_cast<R*>(d.qn_c), const_cast<R*>(d.qn_r)};
     R* tq[3] = {d.tqv, d.tqc, d.tqr};
+#pragma unroll 1
     for (int sp = 0; sp < 3; ++sp) {
-      R g;
+      R* y = qo[sp] ? qo[sp] : tq[sp];
+      const R gy = y[c];
+      if (gy == (R)0) continue;
+      R g = gy;
       if (qo[sp]) {
-        const R gq = qo[sp][c];
-        qo[sp][c] = 0;
-        if (gq != (R)0) atomicAdd(qn[sp] + c, gq);
-        g = a.dt_stage * gq;
+        // stage value q_n + dt_stage * tq: q_n takes gy (in place: keeps it)
+        g = a.dt_stage * gy;
+        if (qn[sp] != qo[sp]) {
+          atomicAdd(qn[sp] + c, gy);
+          y[c] = 0;
+        }
       } else {
-        g = tq[sp][c];
-        tq[sp][c] = 0;
+        y[c] = 0;
       }
       ADAcc<R, T_N> acc{P, g};
-      if (g != (R)0) row_tq(acc, a, qf[sp], T_QV + sp, i, j, k);
+      row_tq(acc, a, qf[sp], T_QV + sp, i, j, k);
     }
   }
 }
@@ -378,9 +397,12 @@ __global__ void k_ad_fill(FillArgs<R> A, int nk) {
   const bool lateral = (si != i) || (sj != j);
   if (!lateral && k >= 0 && k < L.nz) return;  // interior level of an interior column
   const size_t q = L.at(i, j, k);
+  // the ghost's adjoint moves to its sources; it is cleared only once read
+  // (a store issued while the load of the same address is in flight stalls
+  // the memory pipeline)
   const R g = a[q];
-  a[q] = 0;
   if (g == (R)0) return;
+  a[q] = 0;
   if (kind == 3) {
     if (k == L.nz) return;
     if (k >= 0 && k < L.nz) atomicAdd(a + L.at(si, sj, k), g);
@@ -409,20 +431,25 @@ __global__ void k_ad_flux(FluxArgs<R> A) {
   R* vb = const_cast<R*>(A.v);
   R* wb = const_cast<R*>(A.w);
   if (k < L.nz) {
-    R gx = A.mfx[c], gy = A.mfy[c];
-    A.mfx[c] = 0;
-    A.mfy[c] = 0;
+    const R gx = A.mfx[c], gy = A.mfy[c];
     R rjx = (R)0.5 * (A.b.rhob[L.at(i - 1, j, k)] * A.m.jac[L.at2(i - 1, j)] +
                       A.b.rhob[c] * A.m.jac[L.at2(i, j)]);
     R rjy = (R)0.5 * (A.b.rhob[L.at(i, j - 1, k)] * A.m.jac[L.at2(i, j - 1)] +
                       A.b.rhob[c] * A.m.jac[L.at2(i, j)]);
-    if (gx != (R)0) atomicAdd(ub + c, rjx * gx);
-    if (gy != (R)0) atomicAdd(vb + c, rjy * gy);
+    if (gx != (R)0) {
+      atomicAdd(ub + c, rjx * gx);
+      A.mfx[c] = 0;
+    }
+    if (gy != (R)0) {
+      atomicAdd(vb + c, rjy * gy);
+      A.mfy[c] = 0;
+    }
   }
   if (i > L.nx + 1 || j > L.ny + 1) return;
-  R gz = A.mfz[c];
+  const R gz = A.mfz[c];
+  if (gz == (R)0) return;
   A.mfz[c] = 0;
-  if (k == 0 || k == L.nz || gz == (R)0) return;
+  if (k == 0 || k == L.nz) return;
   const int kk = L.at1(k);
   R fac = (R)1 - A.m.zeta_w[kk] / A.m.zt;
   R rw = A.b.rhobw[c];
@@ -490,43 +517,61 @@ __device__ __forceinline__ void emit_thv(Acc& acc, const AcouArgs<R>& a, int i, 
   acc(lat ? A_NTHP : A_THIN, s, f);
 }
 
+// The pressure-gradient terms of the u (is_u) or v step at a face
+// (kernels.cu:499-526): face theta_v and map factor, the horizontal pi*
+// gradient with its terrain correction, and what the correction is made of.
+template <typename R>
+struct UvFace {
+  R thf, mf, h, grad, slope, jf, dzc2;
+};
+
+template <typename R>
+__device__ __forceinline__ UvFace<R> uv_face_terms(const AcouArgs<R>& a, int i, int j, int k, bool is_u) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const int di = is_u ? 1 : 0, dj = is_u ? 0 : 1;
+  UvFace<R> f;
+  f.thf = (R)0.5 * (theta_v(a, i - di, j - dj, k) + theta_v(a, i, j, k));
+  f.mf = (R)0.5 * (a.m.mapf[L.at2(i - di, j - dj)] + a.m.mapf[L.at2(i, j)]);
+  f.h = is_u ? a.dx : a.dy;
+  f.grad = (pistar(a, i, j, k) - pistar(a, i - di, j - dj, k)) / f.h;
+  f.slope = (is_u ? a.m.hx_u[L.at2(i, j)] : a.m.hy_v[L.at2(i, j)]) * ((R)1 - a.m.zeta_c[kk] / a.m.zt);
+  f.dzc2 = 1;
+  f.jf = 1;
+  if (f.slope != (R)0) {
+    f.dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
+    f.jf = (R)0.5 * (a.m.jac[L.at2(i - di, j - dj)] + a.m.jac[L.at2(i, j)]);
+    R dpdz = (R)0.5 *
+             ((pistar(a, i - di, j - dj, k + 1) - pistar(a, i - di, j - dj, k - 1)) +
+              (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
+             f.dzc2;
+    f.grad -= f.slope / f.jf * dpdz;
+  }
+  return f;
+}
+
 // forward u (is_u) or v step at a face and, when acc is given, coef times
 // its Jacobian row (kernels.cu:499-526)
 template <typename R, class Acc>
 __device__ R uv_face(Acc* acc, const AcouArgs<R>& a, int i, int j, int k, bool is_u, R coef) {
   const Layout& L = a.L;
-  const int kk = L.at1(k);
   const int di = is_u ? 1 : 0, dj = is_u ? 0 : 1;
-  const R thf = (R)0.5 * (theta_v(a, i - di, j - dj, k) + theta_v(a, i, j, k));
-  const R mf = (R)0.5 * (a.m.mapf[L.at2(i - di, j - dj)] + a.m.mapf[L.at2(i, j)]);
-  const R h = is_u ? a.dx : a.dy;
-  R grad = (pistar(a, i, j, k) - pistar(a, i - di, j - dj, k)) / h;
-  const R slope = (is_u ? a.m.hx_u[L.at2(i, j)] : a.m.hy_v[L.at2(i, j)]) * ((R)1 - a.m.zeta_c[kk] / a.m.zt);
-  R dzc2 = 1, jf = 1;
-  if (slope != (R)0) {
-    dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
-    jf = (R)0.5 * (a.m.jac[L.at2(i - di, j - dj)] + a.m.jac[L.at2(i, j)]);
-    R dpdz = (R)0.5 *
-             ((pistar(a, i - di, j - dj, k + 1) - pistar(a, i - di, j - dj, k - 1)) +
-              (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
-             dzc2;
-    grad -= slope / jf * dpdz;
-  }
+  const UvFace<R> f = uv_face_terms(a, i, j, k, is_u);
   const size_t c = L.at(i, j, k);
   const R* tin = is_u ? a.tu : a.tv;
   const R* vin = is_u ? a.u_in : a.v_in;
-  const R out = vin[c] + a.dtau * (-Phys<R>::cp * thf * mf * grad + tin[c]);
+  const R out = vin[c] + a.dtau * (-Phys<R>::cp * f.thf * f.mf * f.grad + tin[c]);
   if (acc) {
     (*acc)(is_u ? A_UIN : A_VIN, c, coef);
     (*acc)(is_u ? A_TU : A_TV, c, coef * a.dtau);
-    const R g1 = -coef * a.dtau * Phys<R>::cp * mf;
-    emit_thv(*acc, a, i - di, j - dj, k, g1 * grad * (R)0.5);
-    emit_thv(*acc, a, i, j, k, g1 * grad * (R)0.5);
-    const R g2 = g1 * thf;
-    emit_pistar(*acc, a, i, j, k, g2 / h);
-    emit_pistar(*acc, a, i - di, j - dj, k, -g2 / h);
-    if (slope != (R)0) {
-      const R g3 = -g2 * slope / jf * (R)0.5 / dzc2;
+    const R g1 = -coef * a.dtau * Phys<R>::cp * f.mf;
+    emit_thv(*acc, a, i - di, j - dj, k, g1 * f.grad * (R)0.5);
+    emit_thv(*acc, a, i, j, k, g1 * f.grad * (R)0.5);
+    const R g2 = g1 * f.thf;
+    emit_pistar(*acc, a, i, j, k, g2 / f.h);
+    emit_pistar(*acc, a, i - di, j - dj, k, -g2 / f.h);
+    if (f.slope != (R)0) {
+      const R g3 = -g2 * f.slope / f.jf * (R)0.5 / f.dzc2;
       emit_pistar(*acc, a, i - di, j - dj, k + 1, g3);
       emit_pistar(*acc, a, i - di, j - dj, k - 1, -g3);
       emit_pistar(*acc, a, i, j, k + 1, g3);
@@ -616,28 +661,180 @@ __global__ void __launch_bounds__(256) k_tl_uv(AcouArgs<R> a, AcouArgs<R> d) {
   }
 }
 
+// Adjoint of the u, v step in gather form, two launches and no atomics.
+// (1) Per face: the face's own output adjoint, plus what a radiation face
+//     (open boundaries) or the periodic face nx adds to the face it was
+//     computed from, gives the coefficient of that face's uv_face row; the
+//     face writes its u_in / tendency adjoint and three coefficients -- of
+//     the pi* difference (gp), of the terrain pi* correction (gs) and of the
+//     two theta_v values (gt) -- into scratch.
+// (2) Per cell: gathers the coefficients of the faces around the cell (and
+//     of the ghost cells the cell is the source of) into pi', pi'_prev /
+//     time-n pi', theta' / time-n theta' and qv adjoints, and clears the face
+//     output adjoints.
 template <typename R>
-__global__ void __launch_bounds__(256) k_ad_uv(AcouArgs<R> a, AcouArgs<R> d) {
+struct UvScr {
+  R *gp_u, *gs_u, *gt_u, *gp_v, *gs_v, *gt_v;
+};
+
+template <typename R>
+__device__ __forceinline__ void ad_uv_face(const AcouArgs<R>& a, const AcouArgs<R>& d, int i, int j, int k,
+                                           bool is_u, R* gp, R* gs, R* gt) {
+  const Layout& L = a.L;
+  const int n = is_u ? L.nx : L.ny;       // faces 0..n along the face normal
+  const int f = is_u ? i : j;             // this face's index along it
+  const bool open = is_u ? a.p.bc_x_open : a.p.bc_y_open;
+  const R h = is_u ? a.dx : a.dy;
+  const R cstar = a.p.cstar;
+  const R* yb = is_u ? d.u_out : d.v_out;
+  const R* xin = is_u ? a.u_in : a.v_in;
+  R* xb = const_cast<R*>(is_u ? d.u_in : d.v_in);
+  R* tb = const_cast<R*>(is_u ? d.tu : d.tv);
+  auto at_f = [&](int q) { return is_u ? L.at(q, j, k) : L.at(i, q, k); };
+  const size_t c = L.at(i, j, k);
+  R ce = 0;  // coefficient of the uv_face row at this face
+  if (open) {
+    if (f == 0 || f == n) {
+      // radiation face (kernels.cu:654-667, 674-687): its own u_in term
+      const R x0 = xin[c], g = yb[c];
+      if (g != (R)0 && (f == 0 ? x0 < (R)0 : x0 > (R)0)) {
+        const R cb = f == 0 ? x0 - cstar : x0 + cstar;
+        const R xf = uv_face<R, ADAcc<R, A_N>>(nullptr, a, is_u ? (f == 0 ? 1 : n - 1) : i,
+                                                is_u ? j : (f == 0 ? 1 : n - 1), k, is_u, 0);
+        const R dd = f == 0 ? (xf - x0 - cb) : (x0 - xf + cb);
+        xb[c] += g * ((R)1 - a.dtau / h * dd);
+      }
+    } else {
+      ce = yb[c];
+      if (f == 1) {
+        const size_t c0 = at_f(0);
+        const R x0 = xin[c0];
+        if (x0 < (R)0) ce += -yb[c0] * a.dtau * (x0 - cstar) / h;
+      }
+      if (f == n - 1) {
+        const size_t cn = at_f(n);
+        const R xn = xin[cn];
+        if (xn > (R)0) ce += yb[cn] * a.dtau * (xn + cstar) / h;
+      }
+    }
+  } else if (f < n) {
+    ce = yb[c];
+    if (f == 0) ce += yb[at_f(n)];  // face n repeats face 0
+  }
+  R p = 0, s = 0, t = 0;
+  if (ce != (R)0) {
+    const UvFace<R> u = uv_face_terms(a, i, j, k, is_u);
+    xb[c] += ce;
+    tb[c] += ce * a.dtau;
+    const R g1 = -ce * a.dtau * Phys<R>::cp * u.mf;
+    t = g1 * u.grad * (R)0.5;
+    const R g2 = g1 * u.thf;
+    p = g2 / u.h;
+    if (u.slope != (R)0) s = -g2 * u.slope / u.jf * (R)0.5 / u.dzc2;
+  }
+  gp[c] = p;
+  gs[c] = s;
+  gt[c] = t;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_ad_uv_faces(AcouArgs<R> a, AcouArgs<R> d, UvScr<R> w) {
   const Layout& L = a.L;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i > L.nx || j > L.ny || k >= L.nz) return;
-  const Ptrs<R, A_N> P = acou_ptrs(d);
-  if (j < L.ny) {
-    const size_t c = L.at(i, j, k);
-    ADAcc<R, A_N> acc{P, (R)1};
-    const R g = d.u_out[c];
-    d.u_out[c] = 0;
-    if (g != (R)0) row_u_out(acc, a, i, j, k, g);
+  if (j < L.ny) ad_uv_face(a, d, i, j, k, true, w.gp_u, w.gs_u, w.gt_u);
+  if (i < L.nx) ad_uv_face(a, d, i, j, k, false, w.gp_v, w.gs_v, w.gt_v);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_ad_uv_cells(AcouArgs<R> a, AcouArgs<R> d, UvScr<R> w) {
+  const Layout& L = a.L;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  if (i >= nx || j >= ny || k >= nz) return;
+  // face coefficients, zero outside the faces that exist
+  auto U = [&](const R* g, int fi, int fj, int fk) -> R {
+    return (fi >= 0 && fi <= nx && fj >= 0 && fj < ny && fk >= 0 && fk < nz) ? g[L.at(fi, fj, fk)] : (R)0;
+  };
+  auto V = [&](const R* g, int fi, int fj, int fk) -> R {
+    return (fi >= 0 && fi < nx && fj >= 0 && fj <= ny && fk >= 0 && fk < nz) ? g[L.at(fi, fj, fk)] : (R)0;
+  };
+  // adjoint of pi* at cell (ci, cj, ck), interior or ghost (emit_pistar)
+  auto pbar = [&](int ci, int cj, int ck) -> R {
+    return U(w.gp_u, ci, cj, ck) - U(w.gp_u, ci + 1, cj, ck) + V(w.gp_v, ci, cj, ck) -
+           V(w.gp_v, ci, cj + 1, ck) + U(w.gs_u, ci, cj, ck - 1) - U(w.gs_u, ci, cj, ck + 1) +
+           U(w.gs_u, ci + 1, cj, ck - 1) - U(w.gs_u, ci + 1, cj, ck + 1) + V(w.gs_v, ci, cj, ck - 1) -
+           V(w.gs_v, ci, cj, ck + 1) + V(w.gs_v, ci, cj + 1, ck - 1) - V(w.gs_v, ci, cj + 1, ck + 1);
+  };
+  const size_t c = L.at(i, j, k);
+  const R sm = a.p.acoustic_smdiv;
+  R* piC = const_cast<R*>(d.pi_cur);
+  R* piP = const_cast<R*>(d.pi_prev);
+  R* npB = const_cast<R*>(d.n_pip);
+  R* thB = const_cast<R*>(d.th_in);
+  R* ntB = const_cast<R*>(d.n_thp);
+  R* qvB = const_cast<R*>(d.qv);
+  // periodic ghosts whose source is this cell: column -1 (row -1) maps to nx - 1 (ny - 1)
+  const bool gx = !a.p.bc_x_open && i == nx - 1;
+  const bool gy = !a.p.bc_y_open && j == ny - 1;
+  {
+    const R X = pbar(i, j, k);
+    R Xg = 0;
+    if (k == 0) Xg += pbar(i, j, -1);
+    if (k == nz - 1) Xg += pbar(i, j, nz);
+    if (gx) {
+      Xg += pbar(-1, j, k);
+      if (k == 0) Xg += pbar(-1, j, -1);
+      if (k == nz - 1) Xg += pbar(-1, j, nz);
+    }
+    if (gy) {
+      Xg += pbar(i, -1, k);
+      if (k == 0) Xg += pbar(i, -1, -1);
+      if (k == nz - 1) Xg += pbar(i, -1, nz);
+    }
+    // pi' and the three pi'_prev / time-n pi' buffers may coincide: one
+    // update after another in this thread
+    if (X != (R)0) {
+      piC[c] += ((R)1 + sm) * X;
+      piP[c] += -sm * X;
+    }
+    if (Xg != (R)0) {
+      piC[c] += ((R)1 + sm) * Xg;
+      npB[c] += -sm * Xg;
+    }
   }
-  if (i < L.nx) {
-    const size_t c = L.at(i, j, k);
-    ADAcc<R, A_N> acc{P, (R)1};
-    const R g = d.v_out[c];
-    d.v_out[c] = 0;
-    if (g != (R)0) row_v_out(acc, a, i, j, k, g);
+  {
+    const bool moist = a.p.moisture != 0;
+    const R T = U(w.gt_u, i, j, k) + U(w.gt_u, i + 1, j, k) + V(w.gt_v, i, j, k) + V(w.gt_v, i, j + 1, k);
+    if (T != (R)0) {
+      if (moist) {
+        thB[c] += T * ((R)1 + Phys<R>::eps61 * a.qv[c]);
+        qvB[c] += T * (a.b.thb[c] + a.th_in[c]) * Phys<R>::eps61;
+      } else {
+        thB[c] += T;
+      }
+    }
+    R Tg[2] = {gx ? U(w.gt_u, 0, j, k) : (R)0, gy ? V(w.gt_v, i, 0, k) : (R)0};
+    const size_t gc[2] = {L.at(-1, j, k), L.at(i, -1, k)};
+    for (int q = 0; q < 2; ++q) {
+      if (Tg[q] == (R)0) continue;
+      if (moist) {
+        ntB[c] += Tg[q] * ((R)1 + Phys<R>::eps61 * a.qv[c]);
+        qvB[c] += Tg[q] * (a.b.thb[gc[q]] + a.n_thp[c]) * Phys<R>::eps61;
+      } else {
+        ntB[c] += Tg[q];
+      }
+    }
   }
+  // the output adjoints are consumed
+  d.u_out[c] = 0;
+  d.v_out[c] = 0;
+  if (i == nx - 1) d.u_out[L.at(nx, j, k)] = 0;
+  if (j == ny - 1) d.v_out[L.at(i, ny, k)] = 0;
 }
 
 // ================================================================ w - pi' column
@@ -647,19 +844,22 @@ __global__ void __launch_bounds__(256) k_ad_uv(AcouArgs<R> a, AcouArgs<R> d) {
 constexpr int LCX = 8, LKL = 16;
 
 // rows 1..n-1 of a tridiagonal system (row 1 without A, row n-1 without C),
-// the forward's elimination order (kernels.cu:612-634); arrays strided by LCX
+// the forward's elimination (kernels.cu:612-634; dyn_acou.cu phase 4: one
+// reciprocal per row); arrays strided by LCX
 template <typename R>
-__device__ void thomas_s(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds, R* x) {
+__device__ __forceinline__ void thomas_s(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds,
+                                         R* x) {
   R cp = 0, dp = 0;
   for (int k = 1; k < n; ++k) {
     const int q = k * LCX;
     if (k == 1) {
-      cp = C[q] / B[q];
-      dp = D[q] / B[q];
+      const R r = (R)1 / B[q];
+      cp = C[q] * r;
+      dp = D[q] * r;
     } else {
-      const R m = B[q] - A[q] * cp;
-      cp = C[q] / m;
-      dp = (D[q] - A[q] * dp) / m;
+      const R r = (R)1 / (B[q] - A[q] * cp);
+      cp = C[q] * r;
+      dp = (D[q] - A[q] * dp) * r;
     }
     cs[q] = cp;
     ds[q] = dp;
@@ -674,19 +874,21 @@ __device__ void thomas_s(int n, const R* A, const R* B, const R* C, const R* D, 
 
 // the transposed system: (M^T)_{k,k-1} = C[k-1], (M^T)_{k,k+1} = A[k+1]
 template <typename R>
-__device__ void thomas_ts(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds, R* x) {
+__device__ __forceinline__ void thomas_ts(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds,
+                                          R* x) {
   R cp = 0, dp = 0;
   for (int k = 1; k < n; ++k) {
     const int q = k * LCX;
     const R sub = k > 1 ? C[q - LCX] : (R)0;
     const R sup = k < n - 1 ? A[q + LCX] : (R)0;
     if (k == 1) {
-      cp = sup / B[q];
-      dp = D[q] / B[q];
+      const R r = (R)1 / B[q];
+      cp = sup * r;
+      dp = D[q] * r;
     } else {
-      const R m = B[q] - sub * cp;
-      cp = sup / m;
-      dp = (D[q] - sub * dp) / m;
+      const R r = (R)1 / (B[q] - sub * cp);
+      cp = sup * r;
+      dp = (D[q] - sub * dp) * r;
     }
     cs[q] = cp;
     ds[q] = dp;
@@ -708,153 +910,183 @@ struct ColArr {
   __device__ R* operator[](int q) const { return base + (size_t)q * n1 * LCX; }
 };
 
-// Forward values of one column (kernels.cu:552-634) as the column kernel
-// computes them, into shared arrays: Av, Sv, P, E on levels; G, A, B, C, D on
-// the inner levels; the solution w (with the surface w at level 0).
+// What the TL and AD kernels of one column share: the column's geometry and
+// its level k at c0 + k * pl, as the forward column kernel addresses it.
+template <typename R>
+struct ColGeom {
+  int nz;
+  R dtau, c1, c2, J, invJ, hxc, hyc, mc, mcx, mcy;
+  bool terrain;
+  size_t c0, sx, sy, pl;
+  __device__ ColGeom(const AcouArgs<R>& a, int i, int j, bool active) {
+    const Layout& L = a.L;
+    nz = L.nz;
+    dtau = a.dtau;
+    c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
+    c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
+    const size_t c2d = L.at2(active ? i : 0, j);
+    J = a.m.jac[c2d];
+    hxc = a.m.hx[c2d];
+    hyc = a.m.hy[c2d];
+    mc = a.m.mapf[c2d];
+    invJ = (R)1 / J;
+    mcx = mc * a.co.inv_dx;
+    mcy = mc * a.co.inv_dy;
+    terrain = hxc != (R)0 || hyc != (R)0;
+    sx = 1;
+    sy = L.px;
+    pl = L.plane();
+    c0 = L.at(active ? i : 0, j, 0);
+  }
+  __device__ size_t at(int k) const { return c0 + (size_t)k * pl; }
+};
+
+// Forward values of one column (kernels.cu:552-634) with the forward column
+// kernel's expressions (dyn_acou.cu phases 1-4), into shared arrays: Av, Sv,
+// P, E on levels; G, A, B, C, D on the inner levels; the solution w (with the
+// surface w at level 0).  Ends with a barrier.
 enum { V_AV, V_SV, V_P, V_E, V_G, V_A, V_B, V_C, V_D, V_W, V_CS, V_DS, V_N };
 
 template <typename R>
-__device__ void column_values_s(const AcouArgs<R>& a, int i, int j, bool active, const ColArr<R>& S) {
+__device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColGeom<R>& g, bool active,
+                                                const ColArr<R>& S) {
   const Layout& L = a.L;
-  const int nz = L.nz, tx = threadIdx.x, lane = threadIdx.y;
-  const R dtau = a.dtau, zt = a.m.zt;
-  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
-  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
-  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
-  const R* u = a.u_out;
-  const R* v = a.v_out;
-  const long sx = 1, sy = L.px;
+  const int nz = g.nz, tx = threadIdx.x, lane = threadIdx.y;
+  const R dtau = g.dtau, c1 = g.c1, c2 = g.c2;
+  const R* __restrict__ u = a.u_out;
+  const R* __restrict__ v = a.v_out;
+  const size_t sx = g.sx, sy = g.sy, pl = g.pl;
   R *Av = S[V_AV] + tx, *Sv = S[V_SV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx;
   R *G = S[V_G] + tx, *A = S[V_A] + tx, *B = S[V_B] + tx, *C = S[V_C] + tx, *D = S[V_D] + tx;
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
       R av = 0, sv = 0;
       if (k >= 1 && k < nz) {
-        const int kk = L.at1(k);
-        const size_t c = L.at(i, j, k);
+        const size_t c = g.at(k), cm = c - pl;
         av = a.co.aw[c];
-        R fac = (R)1 - a.m.zeta_w[kk] / zt;
-        const size_t cm = c - (size_t)L.plane();
-        R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
-        R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
-        sv = av * (uw * hxc + vw * hyc) * fac;
+        if (g.terrain) {
+          R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+          R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+          sv = av * (uw * g.hxc + vw * g.hyc) * a.co.fac_w[L.at1(k)];
+        }
       }
       Av[k * LCX] = av;
       Sv[k * LCX] = sv;
     }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = lane; k < nz; k += LKL) {
-      const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const size_t c = g.at(k);
       R Kt = a.co.kt3[c];
-      R Dh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
-                   (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
-      R dzc = a.m.dzeta_c[kk];
-      R wk = a.w_in[c], wkp = a.w_in[c + L.plane()];
+      R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * g.mcx +
+             (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * g.mcy;
+      R idz = a.co.inv_dzc[L.at1(k)];
+      R wk = a.w_in[c], wkp = a.w_in[c + pl];
       R tpi = a.tpi ? a.tpi[c] : (R)0;
-      P[k * LCX] = a.pi_cur[c] + dtau * tpi -
-                   dtau * Kt *
-                       (Dh - (Sv[(k + 1) * LCX] - Sv[k * LCX]) / dzc +
-                        c2 * (Av[(k + 1) * LCX] * wkp - Av[k * LCX] * wk) / dzc);
-      E[k * LCX] = dtau * Kt * c1 / dzc;
+      const int q = k * LCX;
+      P[q] = a.pi_cur[c] + dtau * tpi -
+             dtau * Kt * (Dh - (Sv[q + LCX] - Sv[q]) * idz + c2 * (Av[q + LCX] * wkp - Av[q] * wk) * idz);
+      E[q] = dtau * Kt * c1 * idz;
     }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = 1 + lane; k < nz; k += LKL) {
-      const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+      const size_t c = g.at(k), cm = c - pl;
+      const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       R thc = a.th_in[c], thm = a.th_in[cm];
-      R thvw = a.b.thbw[c] + (R)0.5 * (thm + thc);
+      R thbw = a.b.thbw[c];
+      R thvw = thbw + (R)0.5 * (thm + thc);
       if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
-      R g = dtau * Phys<R>::cp * thvw * c1 / (J * a.m.dzeta_w[kk]);
+      R Gk = dtau * Phys<R>::cp * thvw * c1 * iJdz;
       const int q = k * LCX;
-      G[q] = g;
-      A[q] = -g * E[q - LCX] * Av[q - LCX];
-      B[q] = (R)1 + g * Av[q] * (E[q] + E[q - LCX]);
-      C[q] = -g * E[q] * Av[q + LCX];
-      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / a.b.thbw[c];
+      const R Em = E[q - LCX], Ek = E[q];
+      G[q] = Gk;
+      A[q] = -Gk * Em * Av[q - LCX];
+      B[q] = (R)1 + Gk * Av[q] * (Ek + Em);
+      C[q] = -Gk * Ek * Av[q + LCX];
+      R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
       if (a.p.moisture) {
         R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
         R qcr = (R)0.5 * (a.qc[cm] + a.qc[c]) + (R)0.5 * (a.qr[cm] + a.qr[c]);
         buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
       }
       R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
-              dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) / (J * a.m.dzeta_w[kk]);
-      D[q] = RHS - g * (P[q] - P[q - LCX]);
+              dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) * iJdz;
+      D[q] = RHS - Gk * (P[q] - P[q - LCX]);
     }
   __syncthreads();
   if (active && lane == 0) {
     R* W = S[V_W] + tx;
     thomas_s(nz, A, B, C, D, S[V_CS] + tx, S[V_DS] + tx, W);
-    const size_t c0 = L.at(i, j, 0);
-    W[0] = (R)0.5 * (u[c0] + u[c0 + sx]) * hxc + (R)0.5 * (v[c0] + v[c0 + sy]) * hyc;
+    R us = (R)0.5 * (u[g.c0] + u[g.c0 + sx]);
+    R vs = (R)0.5 * (v[g.c0] + v[g.c0 + sy]);
+    W[0] = us * g.hxc + vs * g.hyc;
   }
   __syncthreads();
 }
 
-enum { T_DSV = V_N, T_DTH, T_DP, T_DG, T_RHS, T_DW, T_NARR };
+enum { T_DSV = V_N, T_DTH, T_DP, T_RHS, T_DW, T_NARR };
 
 template <typename R>
 __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs<R> d) {
   extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
-  const int nz = L.nz, tx = threadIdx.x, lane = threadIdx.y;
+  const int tx = threadIdx.x, lane = threadIdx.y;
   const int i = blockIdx.x * LCX + tx, j = blockIdx.y;
   const bool active = i < L.nx;
-  const ColArr<R> S{reinterpret_cast<R*>(lin_smem), nz + 1};
-  const R dtau = a.dtau, zt = a.m.zt;
-  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
-  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
-  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
-  const R* u = d.u_out;
-  const R* v = d.v_out;
-  const long sx = 1, sy = L.px;
-  R *dSv = S[T_DSV] + tx, *dth = S[T_DTH] + tx, *dP = S[T_DP] + tx, *dG = S[T_DG] + tx;
+  const ColArr<R> S{reinterpret_cast<R*>(lin_smem), L.nz + 1};
+  const ColGeom<R> g(a, i, j, active);
+  const int nz = g.nz;
+  const R dtau = g.dtau, c1 = g.c1, c2 = g.c2;
+  const R* __restrict__ du = d.u_out;
+  const R* __restrict__ dv = d.v_out;
+  const size_t sx = g.sx, sy = g.sy, pl = g.pl;
+  R *dSv = S[T_DSV] + tx, *dth = S[T_DTH] + tx, *dP = S[T_DP] + tx;
   R *rhs = S[T_RHS] + tx, *dw = S[T_DW] + tx;
   // the tangent theta' in, before any in-place write of this launch
   if (active)
-    for (int k = lane; k < nz; k += LKL) dth[k * LCX] = d.th_in[L.at(i, j, k)];
-  column_values_s(a, i, j, active, S);  // ends with a barrier
+#pragma unroll 4
+    for (int k = lane; k < nz; k += LKL) dth[k * LCX] = d.th_in[g.at(k)];
+  column_values_s(a, g, active, S);
   const R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *G = S[V_G] + tx;
-  const R *W = S[V_W] + tx;
+  const R* W = S[V_W] + tx;
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
-      R s = 0;
-      if (k >= 1 && k < nz) {
-        const int kk = L.at1(k);
-        const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-        R fac = (R)1 - a.m.zeta_w[kk] / zt;
-        R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
-        R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
-        s = Av[k * LCX] * (uw * hxc + vw * hyc) * fac;
+      R sv = 0;
+      if (g.terrain && k >= 1 && k < nz) {
+        const size_t c = g.at(k), cm = c - pl;
+        R uw = (R)0.25 * (du[cm] + du[cm + sx] + du[c] + du[c + sx]);
+        R vw = (R)0.25 * (dv[cm] + dv[cm + sy] + dv[c] + dv[c + sy]);
+        sv = Av[k * LCX] * (uw * g.hxc + vw * g.hyc) * a.co.fac_w[L.at1(k)];
       }
-      dSv[k * LCX] = s;
+      dSv[k * LCX] = sv;
     }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = lane; k < nz; k += LKL) {
-      const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const size_t c = g.at(k);
       R Kt = a.co.kt3[c];
-      R dDh = mc * ((a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) / a.dx +
-                    (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) / a.dy);
-      R dzc = a.m.dzeta_c[kk];
-      R dwk = d.w_in[c], dwkp = d.w_in[c + L.plane()];
+      R dDh = (a.co.rtjx[c + sx] * du[c + sx] - a.co.rtjx[c] * du[c]) * g.mcx +
+              (a.co.rtjy[c + sy] * dv[c + sy] - a.co.rtjy[c] * dv[c]) * g.mcy;
+      R idz = a.co.inv_dzc[L.at1(k)];
+      R dwk = d.w_in[c], dwkp = d.w_in[c + pl];
       R dtpi = d.tpi ? d.tpi[c] : (R)0;
       const int q = k * LCX;
       dP[q] = d.pi_cur[c] + dtau * dtpi -
-              dtau * Kt * (dDh - (dSv[q + LCX] - dSv[q]) / dzc + c2 * (Av[q + LCX] * dwkp - Av[q] * dwk) / dzc);
+              dtau * Kt * (dDh - (dSv[q + LCX] - dSv[q]) * idz + c2 * (Av[q + LCX] * dwkp - Av[q] * dwk) * idz);
     }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = 1 + lane; k < nz; k += LKL) {
-      const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
+      const size_t c = g.at(k), cm = c - pl;
       const int q = k * LCX;
-      const R jdz = J * a.m.dzeta_w[kk];
+      const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
       R thvw = thd;
       R dthvw = (R)0.5 * (dth[q - LCX] + dth[q]);
@@ -868,30 +1100,28 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
         dbuoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - (R)0.5 * (d.qc[cm] + d.qc[c]) -
                                   (R)0.5 * (d.qr[cm] + d.qr[c]));
       }
-      R g = dtau * Phys<R>::cp * dthvw * c1 / jdz;
+      const R dG = dtau * Phys<R>::cp * dthvw * c1 * iJdz;
       R dpi = d.pi_cur[c] - d.pi_cur[cm], pi = a.pi_cur[c] - a.pi_cur[cm];
-      R dRHS = d.w_in[c] + dtau * (dbuoy + d.tw[c]) -
-               dtau * Phys<R>::cp * c2 * (dthvw * pi + thvw * dpi) / jdz;
-      R dD = dRHS - g * (P[q] - P[q - LCX]) - G[q] * (dP[q] - dP[q - LCX]);
-      R dA = -g * E[q - LCX] * Av[q - LCX];
-      R dB = g * Av[q] * (E[q] + E[q - LCX]);
-      R dC = -g * E[q] * Av[q + LCX];
+      R dRHS = d.w_in[c] + dtau * (dbuoy + d.tw[c]) - dtau * Phys<R>::cp * c2 * (dthvw * pi + thvw * dpi) * iJdz;
+      R dD = dRHS - dG * (P[q] - P[q - LCX]) - G[q] * (dP[q] - dP[q - LCX]);
+      R dA = -dG * E[q - LCX] * Av[q - LCX];
+      R dB = dG * Av[q] * (E[q] + E[q - LCX]);
+      R dC = -dG * E[q] * Av[q + LCX];
       R mw = dB * W[q];
       if (k > 1) mw += dA * W[q - LCX];
       if (k < nz - 1) mw += dC * W[q + LCX];
       rhs[q] = dD - mw;
-      dG[q] = g;
     }
   __syncthreads();
   if (active && lane == 0) {
     thomas_s(nz, S[V_A] + tx, S[V_B] + tx, S[V_C] + tx, rhs, S[V_CS] + tx, S[V_DS] + tx, dw);
-    const size_t c0 = L.at(i, j, 0);
-    dw[0] = (R)0.5 * (u[c0] + u[c0 + sx]) * hxc + (R)0.5 * (v[c0] + v[c0 + sy]) * hyc;
+    dw[0] = (R)0.5 * (du[g.c0] + du[g.c0 + sx]) * g.hxc + (R)0.5 * (dv[g.c0] + dv[g.c0 + sy]) * g.hyc;
   }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
-      const size_t c = L.at(i, j, k);
+      const size_t c = g.at(k);
       const int q = k * LCX;
       if (k < nz) {
         d.pi_next[c] = dP[q] - E[q] * (Av[q + LCX] * dw[q + LCX] - Av[q] * dw[q]);
@@ -905,21 +1135,22 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
 
 enum { A_WB = V_N, A_PB, A_TB, A_WS, A_LAM, A_GL, A_PIB, A_THB, A_KTD, A_NARR };
 
+// Adjoint of the column.  dhB (per cell, levels < nz) receives mc times the
+// adjoint of the horizontal divergence, svB the u, v weight of level k (the
+// surface w at level 0, Sv(k) at levels 1..nz-1); k_ad_column_uv takes both
+// to the faces.
 template <typename R>
-__global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs<R> d) {
+__global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs<R> d, R* dhB, R* svB) {
   extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
-  const int nz = L.nz, tx = threadIdx.x, lane = threadIdx.y;
+  const int tx = threadIdx.x, lane = threadIdx.y;
   const int i = blockIdx.x * LCX + tx, j = blockIdx.y;
   const bool active = i < L.nx;
-  const ColArr<R> S{reinterpret_cast<R*>(lin_smem), nz + 1};
-  const R dtau = a.dtau, zt = a.m.zt;
-  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
-  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
-  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
-  R* ub = d.u_out;
-  R* vb = d.v_out;
+  const ColArr<R> S{reinterpret_cast<R*>(lin_smem), L.nz + 1};
+  const ColGeom<R> g(a, i, j, active);
+  const int nz = g.nz;
+  const R dtau = g.dtau, c1 = g.c1, c2 = g.c2;
+  const size_t pl = g.pl;
   R* wI = const_cast<R*>(d.w_in);
   R* piC = const_cast<R*>(d.pi_cur);
   R* thI = const_cast<R*>(d.th_in);
@@ -930,59 +1161,50 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   R* qcI = const_cast<R*>(d.qc);
   R* qrI = const_cast<R*>(d.qr);
   const bool moist = a.p.moisture != 0;
-  const long sx = 1, sy = L.px;
   R *wb = S[A_WB] + tx, *pb = S[A_PB] + tx, *tb = S[A_TB] + tx, *ws = S[A_WS] + tx;
   R *lam = S[A_LAM] + tx, *GL = S[A_GL] + tx, *PIB = S[A_PIB] + tx, *THB = S[A_THB] + tx;
-  R *KTD = S[A_KTD] + tx;
+  R* KTD = S[A_KTD] + tx;
   // the sweep's scratch rows, free once the transposed solve is done
   R *QVB = S[V_CS] + tx, *QCB = S[V_DS] + tx;
-  // output adjoints, read and cleared before the (possibly aliased) inputs gain theirs
+  // the output adjoints; w and theta' update in place after the first
+  // substep (w_out = w_in, th_out = th_in), so the inputs' adjoints replace
+  // the outputs' there, and are added to the input's elsewhere while the
+  // output's are cleared -- at the end, long after these loads (a store
+  // issued while the load of the same address is in flight stalls the
+  // memory pipeline)
+  const bool w_alias = d.w_out == d.w_in, th_alias = d.th_out == d.th_in;
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
-      const size_t c = L.at(i, j, k);
+      const size_t c = g.at(k);
       const int q = k * LCX;
       wb[q] = d.w_out[c];
-      d.w_out[c] = 0;
       if (k < nz) {
         pb[q] = d.pi_next[c];
         tb[q] = d.th_out[c];
-        d.pi_next[c] = 0;
-        d.th_out[c] = 0;
       }
     }
-  column_values_s(a, i, j, active, S);  // ends with a barrier
+  column_values_s(a, g, active, S);
   const R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *G = S[V_G] + tx;
-  const R *W = S[V_W] + tx;
+  const R* W = S[V_W] + tx;
   // adjoint of the column solution w (level 0: surface w, level nz: the lid)
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
       const int q = k * LCX;
-      R g = 0;
-      if (k < nz) {
-        const size_t c = L.at(i, j, k);
-        g += wb[q] - (R)0.5 * dtau * a.b.dthbdz[c] * tb[q] + E[q] * Av[q] * pb[q];
-      }
-      if (k >= 1) {
-        const size_t cm = L.at(i, j, k - 1);
-        g += -(R)0.5 * dtau * a.b.dthbdz[cm] * tb[q - LCX] - E[q - LCX] * Av[q] * pb[q - LCX];
-      }
-      ws[q] = g;
+      const size_t c = g.at(k);
+      R s = 0;
+      if (k < nz) s += wb[q] - (R)0.5 * dtau * a.b.dthbdz[c] * tb[q] + E[q] * Av[q] * pb[q];
+      if (k >= 1) s += -(R)0.5 * dtau * a.b.dthbdz[c - pl] * tb[q - LCX] - E[q - LCX] * Av[q] * pb[q - LCX];
+      ws[q] = s;
     }
   __syncthreads();
-  if (active && lane == 0) {
-    const size_t c0 = L.at(i, j, 0);
-    const R g = ws[0];
-    if (g != (R)0) {
-      atomicAdd(ub + c0, (R)0.5 * hxc * g);
-      atomicAdd(ub + c0 + sx, (R)0.5 * hxc * g);
-      atomicAdd(vb + c0, (R)0.5 * hyc * g);
-      atomicAdd(vb + c0 + sy, (R)0.5 * hyc * g);
-    }
+  if (active && lane == 0)
     thomas_ts(nz, S[V_A] + tx, S[V_B] + tx, S[V_C] + tx, ws, S[V_CS] + tx, S[V_DS] + tx, lam);
-  }
   __syncthreads();
   // per inner level: what its row sends to neighbouring levels
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
       const int q = k * LCX;
       if (k < 1 || k >= nz) {
@@ -993,9 +1215,8 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
         QCB[q] = 0;
         continue;
       }
-      const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k), cm = c - (size_t)L.plane();
-      const R jdz = J * a.m.dzeta_w[kk];
+      const size_t c = g.at(k), cm = c - pl;
+      const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       const R lm = lam[q];
       const R Ab = k > 1 ? -lm * W[q - LCX] : (R)0;
       const R Bb = -lm * W[q];
@@ -1004,11 +1225,11 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
                    Cb * (-E[q] * Av[q + LCX]) - lm * (P[q] - P[q - LCX]);
       const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
       const R mq = moist ? (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]) : (R)1;
-      const R thvw = thd * mq;
+      const R thvw = moist ? thd * mq : thd;
       const R pi = a.pi_cur[c] - a.pi_cur[cm];
       GL[q] = G[q] * lm;
-      PIB[q] = -dtau * Phys<R>::cp * thvw * c2 / jdz * lm;
-      const R thvwb = -dtau * Phys<R>::cp * c2 * pi / jdz * lm + Gb * dtau * Phys<R>::cp * c1 / jdz;
+      PIB[q] = -dtau * Phys<R>::cp * thvw * c2 * iJdz * lm;
+      const R thvwb = -dtau * Phys<R>::cp * c2 * pi * iJdz * lm + Gb * dtau * Phys<R>::cp * c1 * iJdz;
       const R bt = Phys<R>::grav * (R)0.5 / a.b.thbw[c] * dtau * lm;
       THB[q] = (R)0.5 * thvwb * mq + bt;
       // per level of the pair (k-1, k): qv through theta_v and buoyancy, qc and qr through buoyancy
@@ -1018,73 +1239,107 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
     }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = lane; k < nz; k += LKL) {
-      const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const size_t c = g.at(k);
       const int q = k * LCX;
+      // the adjoints this level accumulates into, all read first
+      const R pic0 = piC[c];
+      const R tpi0 = tpiB ? tpiB[c] : (R)0;
+      const R th0 = th_alias ? (R)0 : thI[c];
+      const R tth0 = tthB[c];
+      R qv0 = 0, qc0 = 0, qr0 = 0;
+      if (moist) {
+        qv0 = qvI[c];
+        qc0 = qcI[c];
+        qr0 = qrI[c];
+      }
+      const R Kt = a.co.kt3[c];
       R Pb = pb[q];
       if (k >= 1) Pb -= GL[q];
       if (k + 1 < nz) Pb += GL[q + LCX];
       R pic = Pb;
       if (k >= 1) pic += PIB[q];
       if (k + 1 < nz) pic -= PIB[q + LCX];
-      piC[c] += pic;
-      if (tpiB) tpiB[c] += dtau * Pb;
-      const R Kt = a.co.kt3[c];
-      const R Dhb = -dtau * Kt * Pb;
-      if (Dhb != (R)0) {
-        atomicAdd(ub + c + sx, mc * a.co.rtjx[c + sx] / a.dx * Dhb);
-        atomicAdd(ub + c, -mc * a.co.rtjx[c] / a.dx * Dhb);
-        atomicAdd(vb + c + sy, mc * a.co.rtjy[c + sy] / a.dy * Dhb);
-        atomicAdd(vb + c, -mc * a.co.rtjy[c] / a.dy * Dhb);
-      }
       R th = tb[q];
       if (k >= 1) th += THB[q];
       if (k + 1 < nz) th += THB[q + LCX];
-      thI[c] += th;
+      piC[c] = pic0 + pic;
+      if (tpiB) tpiB[c] = tpi0 + dtau * Pb;
+      dhB[c] = -dtau * Kt * Pb * g.mc;  // adjoint of the map-factor-scaled divergence
+      thI[c] = th0 + th;
+      if (!th_alias) d.th_out[c] = 0;
       if (moist) {
         R qvs = 0, qcs = 0;
         if (k >= 1) qvs += QVB[q], qcs += QCB[q];
         if (k + 1 < nz) qvs += QVB[q + LCX], qcs += QCB[q + LCX];
-        qvI[c] += qvs;
-        qcI[c] += qcs;
-        qrI[c] += qcs;
+        qvI[c] = qv0 + qvs;
+        qcI[c] = qc0 + qcs;
+        qrI[c] = qr0 + qcs;
       }
-      tthB[c] += dtau * tb[q];
-      KTD[q] = Kt / a.m.dzeta_c[kk] * Pb;
+      tthB[c] = tth0 + dtau * tb[q];
+      d.pi_next[c] = 0;
+      KTD[q] = Kt * a.co.inv_dzc[L.at1(k)] * Pb;
     }
   __syncthreads();
   if (active)
+#pragma unroll 4
     for (int k = lane; k <= nz; k += LKL) {
       const int q = k * LCX;
-      const size_t c = L.at(i, j, k);
+      const size_t c = g.at(k);
+      const R w0 = w_alias ? (R)0 : wI[c];
       R wsum = 0;
       if (k >= 1 && k < nz) wsum += lam[q];
       R kd = (k < nz ? KTD[q] : (R)0) - (k >= 1 ? KTD[q - LCX] : (R)0);
       wsum += dtau * c2 * Av[q] * kd;
-      wI[c] += wsum;
-      if (k >= 1 && k < nz) {
-        const R svb = -dtau * kd;  // adjoint of Sv(k)
-        if (svb != (R)0) {
-          const int kk = L.at1(k);
-          const size_t cm = c - (size_t)L.plane();
-          const R fac = (R)1 - a.m.zeta_w[kk] / zt;
-          const R cu = (R)0.25 * Av[q] * hxc * fac * svb, cv = (R)0.25 * Av[q] * hyc * fac * svb;
-          if (cu != (R)0) {
-            atomicAdd(ub + cm, cu);
-            atomicAdd(ub + cm + sx, cu);
-            atomicAdd(ub + c, cu);
-            atomicAdd(ub + c + sx, cu);
-          }
-          if (cv != (R)0) {
-            atomicAdd(vb + cm, cv);
-            atomicAdd(vb + cm + sy, cv);
-            atomicAdd(vb + c, cv);
-            atomicAdd(vb + c + sy, cv);
-          }
-        }
-      }
+      wI[c] = w0 + wsum;
+      if (!w_alias) d.w_out[c] = 0;
+      // the u, v weight of level k: surface w (level 0) or Sv(k) over the
+      // faces of levels k - 1 and k (k_ad_column_uv takes them to the faces)
+      if (k == 0)
+        svB[c] = (R)0.5 * ws[0];
+      else if (k < nz)
+        svB[c] = (R)0.25 * Av[q] * a.co.fac_w[L.at1(k)] * (-dtau * kd);
     }
+}
+
+// The u, v adjoints the column sends to the faces around it, gathered per
+// face from the two columns beside it (no atomics): dh holds mc * (adjoint
+// of the horizontal divergence) per cell, sv the weight of the surface w
+// (level 0) or of Sv(k) (levels 1..nz-1), which reaches the faces of levels
+// k - 1 and k times the column's terrain slope hx (hy).
+template <typename R>
+__global__ void __launch_bounds__(256) k_ad_column_uv(AcouArgs<R> a, AcouArgs<R> d, const R* __restrict__ dh,
+                                                      const R* __restrict__ sv) {
+  const Layout& L = a.L;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  if (i > nx || j > ny || k >= nz) return;
+  const size_t c = L.at(i, j, k), pl = L.plane();
+  // a column's weight at level k for the faces of level k: its own level and the one above
+  auto wsv = [&](size_t cc) { return sv[cc] + (k + 1 < nz ? sv[cc + pl] : (R)0); };
+  if (j < ny) {  // u face i: columns i - 1 and i
+    R g = 0;
+    const R rj = a.co.rtjx[c] * a.co.inv_dx;
+    if (i >= 1) {
+      const size_t cl = c - 1;
+      g += rj * dh[cl] + a.m.hx[L.at2(i - 1, j)] * wsv(cl);
+    }
+    if (i < nx) g += -rj * dh[c] + a.m.hx[L.at2(i, j)] * wsv(c);
+    if (g != (R)0) d.u_out[c] += g;
+  }
+  if (i < nx) {  // v face j: rows j - 1 and j
+    R g = 0;
+    const R rj = a.co.rtjy[c] * a.co.inv_dy;
+    if (j >= 1) {
+      const size_t cl = c - L.px;
+      g += rj * dh[cl] + a.m.hy[L.at2(i, j - 1)] * wsv(cl);
+    }
+    if (j < ny) g += -rj * dh[c] + a.m.hy[L.at2(i, j)] * wsv(c);
+    if (g != (R)0) d.v_out[c] += g;
+  }
 }
 
 // zero every stored point of a cell field outside the interior cells
@@ -1129,7 +1384,12 @@ void tl_tend(const TendArgs<R>& a, const TendArgs<R>& d, cudaStream_t st) {
 
 template <typename R>
 void ad_tend(const TendArgs<R>& a, const TendArgs<R>& d, cudaStream_t st) {
-  k_ad_tend<R><<<grid_cells<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d);
+  const dim3 g = grid_cells<R>(a.L), b(32, 4, 2);
+  k_ad_tend<R, AD_U><<<g, b, 0, st>>>(a, d);
+  k_ad_tend<R, AD_V><<<g, b, 0, st>>>(a, d);
+  k_ad_tend<R, AD_W><<<g, b, 0, st>>>(a, d);
+  k_ad_tend<R, AD_TH><<<g, b, 0, st>>>(a, d);
+  if (a.p.moisture) k_ad_tend<R, AD_Q><<<g, b, 0, st>>>(a, d);
 }
 
 template <typename R>
@@ -1138,8 +1398,10 @@ void tl_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
 }
 
 template <typename R>
-void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
-  k_ad_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d);
+void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st) {
+  const UvScr<R> w{scr.f[0], scr.f[1], scr.f[2], scr.f[3], scr.f[4], scr.f[5]};
+  k_ad_uv_faces<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d, w);
+  k_ad_uv_cells<R><<<grid_cells<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d, w);
 }
 
 int lin_max_levels() { return 160; }  // FP64 adjoint column arrays within 227 KB
@@ -1171,10 +1433,11 @@ int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
 }
 
 template <typename R>
-int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
+int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st) {
   if (a.L.nz > lin_max_levels()) return 2;
   const size_t sm = lin_col_smem<R, A_NARR>(a.L.nz);
-  k_ad_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d);
+  k_ad_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d, scr.f[0], scr.f[1]);
+  k_ad_column_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d, scr.f[0], scr.f[1]);
   return 0;
 }
 
@@ -1184,9 +1447,9 @@ int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
   template void tl_tend<R>(const TendArgs<R>&, const TendArgs<R>&, cudaStream_t); \
   template void ad_tend<R>(const TendArgs<R>&, const TendArgs<R>&, cudaStream_t); \
   template void tl_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t);   \
-  template void ad_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t);   \
+  template void ad_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
   template int tl_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t); \
-  template int ad_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t);  \
+  template int ad_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
   template void zero_ring<R>(R*, const Layout&, cudaStream_t);                        \
   template int lin_prepare<R>(int);
 WFE_INST(float)

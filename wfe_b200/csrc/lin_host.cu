@@ -59,6 +59,10 @@ class LinT final : public Lin {
       fwd_.push_back({static_cast<R*>(b.first), b.second});
     }
     n3_ = bufs_.empty() ? 0 : bufs_[0].second;
+    for (R*& f : scr_.f) {
+      LCK(cudaMalloc(&f, n3_ * sizeof(R)));
+      LCK(cudaMemsetAsync(f, 0, n3_ * sizeof(R), st_));
+    }
     std::vector<Rec> recs;
     if (m->record_step(1.0, &recs)) return fail(m->error());
     learn_layout(recs);
@@ -290,12 +294,12 @@ class LinT final : public Lin {
       }
       case K_UV: {
         const auto& a = as<AcouArgs<R>>(r);
-        ad_uv<R>(a, tr(a), st_);
+        ad_uv<R>(a, tr(a), scr_, st_);
         break;
       }
       case K_COL: {
         const auto& a = as<AcouArgs<R>>(r);
-        if (ad_column<R>(a, tr(a), st_)) return fail("column deeper than the linearised kernels hold");
+        if (ad_column<R>(a, tr(a), scr_, st_)) return fail("column deeper than the linearised kernels hold");
         break;
       }
       case K_KES: {
@@ -538,6 +542,10 @@ class LinT final : public Lin {
     log_ = nullptr;
     if (rain_scratch_) cudaFree(rain_scratch_);
     rain_scratch_ = nullptr;
+    for (R*& f : scr_.f) {
+      if (f) cudaFree(f);
+      f = nullptr;
+    }
   }
 
   Model* m_ = nullptr;
@@ -549,6 +557,7 @@ class LinT final : public Lin {
   R* log_ = nullptr;
   size_t log_cap_ = 0;
   R* rain_scratch_ = nullptr;  // rain of the adjoint sweep's forward replays
+  LinScratch<R> scr_{};        // work fields of the gather-form adjoints
   double dt_ = -1;
   cudaGraphExec_t tl_graph_[3] = {nullptr, nullptr, nullptr};
   std::map<long, SegGraphs> seg_;
