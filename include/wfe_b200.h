@@ -174,12 +174,14 @@ int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const d
                     int nonlocal);
 
 /* ------------------------------------- tangent-linear and adjoint runs */
-/* No counterpart in the reference.  Linearisation of the dry dynamics (5th-
- * order advection with the Gal-Chen metric, Rayleigh sponge, constant-K
- * diffusion, Coriolis, the split-explicit acoustic step with its implicit
- * w - pi' columns, open and periodic lateral boundaries) about the forward
- * trajectory; moist, Davies-relaxed, surface-physics and w-damping cases are
- * refused.  wfe_lin_enable gives the context a linearised field for every
+/* No counterpart in the reference.  Linearisation of the model step (5th-
+ * order advection of momentum, theta' and the moisture species with the
+ * Gal-Chen metric, Rayleigh sponge, constant-K diffusion, Coriolis, the
+ * split-explicit acoustic step with its implicit w - pi' columns and moist
+ * buoyancy, open and periodic lateral boundaries, the Kessler column with the
+ * mixed-phase blend) about the forward trajectory; cases with the
+ * positive-definite moisture limiter, Davies relaxation, surface physics or
+ * w damping are refused.  wfe_lin_enable gives the context a linearised field for every
  * prognostic (WFE_ROLE_LIN in wfe_field_upload / wfe_field_download), all
  * zero.  wfe_tl_run advances the state x0 -> xN and the linearised field
  * dx0 -> dxN = M dx0 (M: the Jacobian of the N steps at x0).  wfe_ad_run
