@@ -437,13 +437,13 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
 }
 
 template <typename R, int CX, int KL>
-__global__ void __launch_bounds__(CX * KL, 1024 / (CX * KL)) k_acoustic_column(AcouArgs<R> a) {
+__global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
   column_body<R, CX, KL>(a, blockIdx.x, blockIdx.y);
 }
 // the shared column arrays are reused by the next work item only after the
 // barrier that opens it
 template <typename R, int CX, int KL>
-__global__ void __launch_bounds__(CX * KL, 1024 / (CX * KL)) k_acoustic_column_batch(Batch<AcouArgs<R>> b) {
+__global__ void __launch_bounds__(CX * KL) k_acoustic_column_batch(Batch<AcouArgs<R>> b) {
   for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int) { column_body<R, CX, KL>(a, x, y); });
 }
 
