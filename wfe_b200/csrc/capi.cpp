@@ -238,6 +238,8 @@ int wfe_field_upload(wfe_ctx* c, int role, int field, const void* host, int dtyp
     return c->model->upload_interior(role, field, host, dtype == WFE_DTYPE_F32) ? model_err(c)
                                                                                 : WFE_OK;
   if (!c || !host || field < 0 || field > 7) return set_err(c, WFE_ERR_ARG, "bad argument");
+  if (dtype != WFE_DTYPE_F32 && layout != WFE_LAYOUT_INTERIOR)  // FP64 padded: no host copies
+    return c->model->upload(role, field, static_cast<const double*>(host)) ? model_err(c) : WFE_OK;
   const RefGrid& g = c->cs.g;
   std::vector<double> pad(g.npts(), 0.0);
   size_t n = layout == WFE_LAYOUT_INTERIOR ? interior_count(g, field) : g.npts();
@@ -264,6 +266,8 @@ int wfe_field_download(wfe_ctx* c, int role, int field, void* host, int dtype, i
     return c->model->download_interior(role, field, host, dtype == WFE_DTYPE_F32) ? model_err(c)
                                                                                   : WFE_OK;
   if (!c || !host || field < 0 || field > 7) return set_err(c, WFE_ERR_ARG, "bad argument");
+  if (dtype != WFE_DTYPE_F32 && layout != WFE_LAYOUT_INTERIOR)  // FP64 padded: no host copies
+    return c->model->download(role, field, static_cast<double*>(host)) ? model_err(c) : WFE_OK;
   const RefGrid& g = c->cs.g;
   std::vector<double> pad(g.npts());
   if (c->model->download(role, field, pad.data())) return model_err(c);

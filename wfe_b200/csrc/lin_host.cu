@@ -118,20 +118,20 @@ class LinT final : public Lin {
     // the adjoint of x_N, uploaded in the slot of the current time-n state;
     // pi' ghosts are no state, so adjoint values there are dropped
     if (L_.nx) zero_ring<R>(D(static_cast<R*>(m_->state_field(4))), L_, st_);
-    std::vector<R*> bar;
-    if (save_lin_state(&bar)) return 1;
+    if (save_lin_state()) return 1;
     // forward pass (the model's own graphs) with segment checkpoints; x_N kept
-    // to restore at the end
+    // to restore at the end (checkpoint buffers persist across calls)
     const int nseg = (nsteps + every - 1) / every;
-    std::vector<Snap> segs(nseg);
+    if ((int)snaps_.size() < nseg + 1) snaps_.resize(nseg + 1);
+    std::vector<Snap>& segs = snaps_;
     for (int g = 0; g < nseg; ++g) {
       const int s0 = g * every, len = std::min(nsteps, s0 + every) - s0;
       if (snap(&segs[g])) return 1;
       if (m_->run(len, dt, t0 + s0 * dt)) return fail(m_->error());
     }
-    Snap last;
+    Snap& last = snaps_[nseg];
     if (snap(&last)) return 1;
-    if (zero() || load_lin_state(bar)) return 1;
+    if (zero() || load_lin_state()) return 1;
     // reverse sweep: per segment (last first) one graph replays the segment
     // forward saving every buffer each launch overwrites (the undo log), one
     // graph walks the launches backwards (restore outputs, adjoint kernel);
@@ -145,12 +145,9 @@ class LinT final : public Lin {
       LCK(cudaGraphLaunch(sg->rev, st_));
     }
     // dJ/dx0 sits in the slot of x0; move it to the slot of x_N
-    if (save_lin_state(&bar)) return 1;
-    if (restore(last) || zero() || load_lin_state(bar)) return 1;
-    for (auto& s : segs) free_snap(&s);
-    free_snap(&last);
+    if (save_lin_state()) return 1;
+    if (restore(last) || zero() || load_lin_state()) return 1;
     LCK(cudaStreamSynchronize(st_));
-    for (R* p : bar) cudaFree(p);
     LCK(cudaGetLastError());
     return 0;
   }
@@ -500,31 +497,27 @@ class LinT final : public Lin {
     s->d = nullptr;
   }
 
-  // copies of the linearised time-n state (8 fields)
-  int save_lin_state(std::vector<R*>* out) {
-    for (R* p : *out) cudaFree(p);
-    out->assign(8, nullptr);
-    for (int f = 0; f < 8; ++f) {
-      LCK(cudaMalloc(&(*out)[f], n3_ * sizeof(R)));
-      LCK(cudaMemcpyAsync((*out)[f], D(static_cast<R*>(m_->state_field(f))), n3_ * sizeof(R),
+  // a copy of the linearised time-n state (8 fields) in a buffer kept for
+  // the context's lifetime
+  int save_lin_state() {
+    if (!hold_) LCK(cudaMalloc(&hold_, 8 * n3_ * sizeof(R)));
+    for (int f = 0; f < 8; ++f)
+      LCK(cudaMemcpyAsync(hold_ + f * n3_, D(static_cast<R*>(m_->state_field(f))), n3_ * sizeof(R),
                           cudaMemcpyDeviceToDevice, st_));
-    }
     return 0;
   }
 
-  int load_lin_state(const std::vector<R*>& in) {
+  int load_lin_state() {
     for (int f = 0; f < 8; ++f)
-      LCK(cudaMemcpyAsync(D(static_cast<R*>(m_->state_field(f))), in[f], n3_ * sizeof(R),
+      LCK(cudaMemcpyAsync(D(static_cast<R*>(m_->state_field(f))), hold_ + f * n3_, n3_ * sizeof(R),
                           cudaMemcpyDeviceToDevice, st_));
     return 0;
   }
 
   // zero every linearised buffer but the time-n state's
   int keep_only_state() {
-    std::vector<R*> keep;
-    if (save_lin_state(&keep) || zero() || load_lin_state(keep)) return 1;
+    if (save_lin_state() || zero() || load_lin_state()) return 1;
     LCK(cudaStreamSynchronize(st_));
-    for (R* p : keep) cudaFree(p);
     return 0;
   }
 
@@ -546,6 +539,10 @@ class LinT final : public Lin {
       if (f) cudaFree(f);
       f = nullptr;
     }
+    for (auto& sn : snaps_) free_snap(&sn);
+    snaps_.clear();
+    if (hold_) cudaFree(hold_);
+    hold_ = nullptr;
   }
 
   Model* m_ = nullptr;
@@ -558,6 +555,8 @@ class LinT final : public Lin {
   size_t log_cap_ = 0;
   R* rain_scratch_ = nullptr;  // rain of the adjoint sweep's forward replays
   LinScratch<R> scr_{};        // work fields of the gather-form adjoints
+  std::vector<Snap> snaps_;    // adjoint checkpoints, kept across calls
+  R* hold_ = nullptr;          // a saved linearised time-n state
   double dt_ = -1;
   cudaGraphExec_t tl_graph_[3] = {nullptr, nullptr, nullptr};
   std::map<long, SegGraphs> seg_;
