@@ -33,6 +33,16 @@ after another through their own graphs give the serial figure; with
 --impl reference the unmodified reference executable (oracle/_ref/wfe_f32)
 runs each member for K steps, one after another, and the sum of its own step-
 loop wall times is the reference figure.
+
+--workload adjoint measures the cost of the adjoint (and tangent-linear) run
+against the forward run on the same WK82 case with the linearised Kessler
+column (positive-definite limiter and w damping off, neither linearised):
+after W spin-up steps, value = wall time of wfe_ad_run over K steps
+(checkpoints every 30 steps, the fields already on the device; the second of
+two runs, the first captures the sweep's graphs) / CUDA-event time of the same
+K forward steps.  The line also gives the tangent-linear ratio and the
+dot-product gap <M dx, y> - <dx, M^T y> over min(K, 10) steps.  --fp64 runs the
+FP64 state.
 """
 
 from __future__ import annotations
@@ -417,6 +427,61 @@ def ensemble_bench(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def adjoint_bench(args, device: int) -> dict:
+    """Adjoint and tangent-linear cost over the forward on the WK82 case."""
+    import numpy as np
+    import wfe_b200 as W
+    from wfe_b200 import adjoint as A
+
+    prec = "f64" if args.fp64 else "f32"
+    K = args.steps
+    c = W.Case(CASE, overrides={"pd_moist": "off", "w_damping": "off"}, precision=prec, device=device)
+    c.run(args.warmup)
+    c.sync()
+    x0 = A.get_fields(c)
+    A.set_fields(c, x0)
+    c.sync()
+    fwd_ms = c.time_run(K)
+    rng = np.random.default_rng(2)
+    sc = {"qv": 1e-3, "qc": 1e-3, "qr": 1e-3}
+    dx = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in A.FIELDS8}
+    y = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in A.FIELDS8}
+    c.lin_enable()
+    times = {}
+    for name in ("ad", "tl"):
+        t = []
+        for rep in range(2):
+            A.set_fields(c, x0)
+            c.lin_zero()
+            A.set_fields(c, y if name == "ad" else dx, role="lin")
+            c.sync()
+            t0 = time.perf_counter()
+            if name == "ad":
+                c.ad_run(K, checkpoint_every=30)
+            else:
+                c.tl_run(K)
+            t.append(time.perf_counter() - t0)
+        times[name] = t[-1] * 1e3
+    m = min(K, 10)
+    mdx = A.tangent(c, x0, dx, m)
+    mty = A.adjoint(c, x0, y, m, every=5)
+    lhs = sum(float(np.sum(mdx[k] * y[k])) for k in A.FIELDS8)
+    rhs = sum(float(np.sum(dx[k] * mty[k])) for k in A.FIELDS8)
+    c.close()
+    return {
+        "metric": "adjoint_cost_over_forward", "value": times["ad"] / fwd_ms, "unit": "x",
+        "higher_is_better": False, "n_gpus": 1, "steps": K, "warmup": args.warmup, "dtype": prec,
+        "data": "synthetic (analytic WK82 sounding and bubble, deterministic)",
+        "config": {"workload": "WK82 supercell 160x160x40, moist + linearised Kessler, dt=6 s, ns=6, "
+                               "pd_moist=off, w_damping=off", "case": "cases/wk82_160.ini",
+                   "checkpoint_every": 30},
+        "fwd_ms_per_step": fwd_ms / K, "ad_ms_per_step": times["ad"] / K,
+        "tl_ms_per_step": times["tl"] / K, "tl_cost_over_forward": times["tl"] / fwd_ms,
+        "dot_test": {"steps": m, "lhs": lhs, "rhs": rhs,
+                     "rel_gap": abs(lhs - rhs) / max(abs(lhs), abs(rhs))},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,7 +490,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["wk82", "ensemble24"], default="wk82")
+    ap.add_argument("--workload", choices=["wk82", "ensemble24", "adjoint"], default="wk82")
+    ap.add_argument("--fp64", action="store_true", help="adjoint workload: FP64 state")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_setup(args.gpus)
@@ -434,6 +500,15 @@ def main():
         if rank == 0:
             ref = run_reference_ensemble if args.workload == "ensemble24" else run_reference
             print(json.dumps(ref(args)), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "adjoint":
+        if rank == 0:
+            print(json.dumps(adjoint_bench(args, local)), flush=True)
         if world > 1:
             import torch.distributed as dist
 
