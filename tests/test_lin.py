@@ -140,3 +140,19 @@ def test_autograd_function_gradient():
         assert np.linalg.norm(a - b) <= 1e-10 * max(np.linalg.norm(b), 1e-300), k
     assert np.linalg.norm(g["w"]) > 0
     c.close()
+
+
+@pytest.mark.parametrize("name", ["schaer_open", "straka_periodic"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_tangent_run_advances_the_state_like_the_forward(name, prec):
+    """tl_run takes the state x0 -> xN exactly as run does: the column's TL
+    launch writes the forward column's outputs itself, bit for bit."""
+    c, x0 = _spinup(name, prec)
+    A.set_fields(c, x0)
+    c.run(4)
+    ref = A.get_fields(c)
+    A.tangent(c, x0, _rand_fields(c, np.random.default_rng(1)), 4)
+    got = A.get_fields(c)
+    for k in A.FIELDS5:
+        assert np.array_equal(ref[k], got[k]), k
+    c.close()

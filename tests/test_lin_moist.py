@@ -120,6 +120,19 @@ def test_moist_gradient_matches_central_differences():
     c.close()
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_moist_tangent_run_advances_the_state_like_the_forward(prec):
+    c, x0 = _moist_state(prec, OV)
+    c.run(4)
+    ref = A.get_fields(c)
+    rng = np.random.default_rng(9)
+    A.tangent(c, x0, _rand(c, rng, A.FIELDS8, {"qv": 1e-3, "qc": 1e-3, "qr": 1e-3}), 4)
+    got = A.get_fields(c)
+    for k in A.FIELDS8:
+        assert np.array_equal(ref[k], got[k]), k
+    c.close()
+
+
 def test_refuses_positive_definite_moisture():
     c = W.Case(CASES / "wk82_small.ini", precision="f64")
     with pytest.raises(W.WfeError, match="positive-definite"):

@@ -236,7 +236,9 @@ struct LinScratch {
 template <typename R>
 void ad_uv(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st);
 template <typename R>
-int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st);
+// with_forward: the launch also writes the forward column's outputs (the
+// values the forward launch would write, bit for bit)
+int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, bool with_forward, cudaStream_t st);
 template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st);
 template <typename R>

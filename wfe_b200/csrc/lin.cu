@@ -838,20 +838,25 @@ __global__ void __launch_bounds__(256) k_ad_uv_cells(AcouArgs<R> a, AcouArgs<R> 
 }
 
 // ================================================================ w - pi' column
-// A CTA owns LCX columns of one row with LKL level lanes; the column arrays
-// live in shared memory ([level * LCX + column]); the sweeps run in one lane
+// A CTA owns kLcx columns of one row with kLkl level lanes; the column arrays
+// live in shared memory ([level * kLcx + column]); the sweeps run in one lane
 // per column, everything else in parallel over the levels.
-constexpr int LCX = 8, LKL = 16;
+// FP32 tiles hold 16 columns x 8 level lanes; FP64 keeps 8 columns x 16 lanes
+// so that the adjoint's arrays for lin_max_levels() levels fit in shared memory
+template <typename R>
+constexpr int kLcx = sizeof(R) == 4 ? 16 : 8;
+template <typename R>
+constexpr int kLkl = sizeof(R) == 4 ? 8 : 16;
 
 // rows 1..n-1 of a tridiagonal system (row 1 without A, row n-1 without C),
 // the forward's elimination (kernels.cu:612-634; dyn_acou.cu phase 4: one
-// reciprocal per row); arrays strided by LCX
+// reciprocal per row); arrays strided by kLcx<R>
 template <typename R>
 __device__ __forceinline__ void thomas_s(int n, const R* A, const R* B, const R* C, const R* D, R* cs, R* ds,
                                          R* x) {
   R cp = 0, dp = 0;
   for (int k = 1; k < n; ++k) {
-    const int q = k * LCX;
+    const int q = k * kLcx<R>;
     if (k == 1) {
       const R r = (R)1 / B[q];
       cp = C[q] * r;
@@ -864,11 +869,11 @@ __device__ __forceinline__ void thomas_s(int n, const R* A, const R* B, const R*
     cs[q] = cp;
     ds[q] = dp;
   }
-  x[n * LCX] = 0;
+  x[n * kLcx<R>] = 0;
   R above = 0;
   for (int k = n - 1; k >= 1; --k) {
-    above = ds[k * LCX] - cs[k * LCX] * above;
-    x[k * LCX] = above;
+    above = ds[k * kLcx<R>] - cs[k * kLcx<R>] * above;
+    x[k * kLcx<R>] = above;
   }
 }
 
@@ -878,9 +883,9 @@ __device__ __forceinline__ void thomas_ts(int n, const R* A, const R* B, const R
                                           R* x) {
   R cp = 0, dp = 0;
   for (int k = 1; k < n; ++k) {
-    const int q = k * LCX;
-    const R sub = k > 1 ? C[q - LCX] : (R)0;
-    const R sup = k < n - 1 ? A[q + LCX] : (R)0;
+    const int q = k * kLcx<R>;
+    const R sub = k > 1 ? C[q - kLcx<R>] : (R)0;
+    const R sup = k < n - 1 ? A[q + kLcx<R>] : (R)0;
     if (k == 1) {
       const R r = (R)1 / B[q];
       cp = sup * r;
@@ -893,12 +898,12 @@ __device__ __forceinline__ void thomas_ts(int n, const R* A, const R* B, const R
     cs[q] = cp;
     ds[q] = dp;
   }
-  x[n * LCX] = 0;
+  x[n * kLcx<R>] = 0;
   x[0] = 0;
   R above = 0;
   for (int k = n - 1; k >= 1; --k) {
-    above = ds[k * LCX] - cs[k * LCX] * above;
-    x[k * LCX] = above;
+    above = ds[k * kLcx<R>] - cs[k * kLcx<R>] * above;
+    x[k * kLcx<R>] = above;
   }
 }
 
@@ -907,7 +912,7 @@ template <typename R>
 struct ColArr {
   R* base;
   int n1;  // nz + 1
-  __device__ R* operator[](int q) const { return base + (size_t)q * n1 * LCX; }
+  __device__ R* operator[](int q) const { return base + (size_t)q * n1 * kLcx<R>; }
 };
 
 // What the TL and AD kernels of one column share: the column's geometry and
@@ -960,7 +965,7 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
   R *G = S[V_G] + tx, *A = S[V_A] + tx, *B = S[V_B] + tx, *C = S[V_C] + tx, *D = S[V_D] + tx;
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
+    for (int k = lane; k <= nz; k += kLkl<R>) {
       R av = 0, sv = 0;
       if (k >= 1 && k < nz) {
         const size_t c = g.at(k), cm = c - pl;
@@ -971,13 +976,13 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
           sv = av * (uw * g.hxc + vw * g.hyc) * a.co.fac_w[L.at1(k)];
         }
       }
-      Av[k * LCX] = av;
-      Sv[k * LCX] = sv;
+      Av[k * kLcx<R>] = av;
+      Sv[k * kLcx<R>] = sv;
     }
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = lane; k < nz; k += LKL) {
+    for (int k = lane; k < nz; k += kLkl<R>) {
       const size_t c = g.at(k);
       R Kt = a.co.kt3[c];
       R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * g.mcx +
@@ -985,15 +990,15 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
       R idz = a.co.inv_dzc[L.at1(k)];
       R wk = a.w_in[c], wkp = a.w_in[c + pl];
       R tpi = a.tpi ? a.tpi[c] : (R)0;
-      const int q = k * LCX;
+      const int q = k * kLcx<R>;
       P[q] = a.pi_cur[c] + dtau * tpi -
-             dtau * Kt * (Dh - (Sv[q + LCX] - Sv[q]) * idz + c2 * (Av[q + LCX] * wkp - Av[q] * wk) * idz);
+             dtau * Kt * (Dh - (Sv[q + kLcx<R>] - Sv[q]) * idz + c2 * (Av[q + kLcx<R>] * wkp - Av[q] * wk) * idz);
       E[q] = dtau * Kt * c1 * idz;
     }
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = 1 + lane; k < nz; k += LKL) {
+    for (int k = 1 + lane; k < nz; k += kLkl<R>) {
       const size_t c = g.at(k), cm = c - pl;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       R thc = a.th_in[c], thm = a.th_in[cm];
@@ -1001,12 +1006,12 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
       R thvw = thbw + (R)0.5 * (thm + thc);
       if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
       R Gk = dtau * Phys<R>::cp * thvw * c1 * iJdz;
-      const int q = k * LCX;
-      const R Em = E[q - LCX], Ek = E[q];
+      const int q = k * kLcx<R>;
+      const R Em = E[q - kLcx<R>], Ek = E[q];
       G[q] = Gk;
-      A[q] = -Gk * Em * Av[q - LCX];
+      A[q] = -Gk * Em * Av[q - kLcx<R>];
       B[q] = (R)1 + Gk * Av[q] * (Ek + Em);
-      C[q] = -Gk * Ek * Av[q + LCX];
+      C[q] = -Gk * Ek * Av[q + kLcx<R>];
       R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
       if (a.p.moisture) {
         R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
@@ -1015,7 +1020,7 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
       }
       R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
               dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) * iJdz;
-      D[q] = RHS - Gk * (P[q] - P[q - LCX]);
+      D[q] = RHS - Gk * (P[q] - P[q - kLcx<R>]);
     }
   __syncthreads();
   if (active && lane == 0) {
@@ -1031,11 +1036,11 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
 enum { T_DSV = V_N, T_DTH, T_DP, T_RHS, T_DW, T_NARR };
 
 template <typename R>
-__global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs<R> d) {
+__global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_tl_column(AcouArgs<R> a, AcouArgs<R> d, int with_forward) {
   extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
   const int tx = threadIdx.x, lane = threadIdx.y;
-  const int i = blockIdx.x * LCX + tx, j = blockIdx.y;
+  const int i = blockIdx.x * kLcx<R> + tx, j = blockIdx.y;
   const bool active = i < L.nx;
   const ColArr<R> S{reinterpret_cast<R*>(lin_smem), L.nz + 1};
   const ColGeom<R> g(a, i, j, active);
@@ -1049,26 +1054,26 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
   // the tangent theta' in, before any in-place write of this launch
   if (active)
 #pragma unroll 4
-    for (int k = lane; k < nz; k += LKL) dth[k * LCX] = d.th_in[g.at(k)];
+    for (int k = lane; k < nz; k += kLkl<R>) dth[k * kLcx<R>] = d.th_in[g.at(k)];
   column_values_s(a, g, active, S);
   const R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *G = S[V_G] + tx;
   const R* W = S[V_W] + tx;
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
+    for (int k = lane; k <= nz; k += kLkl<R>) {
       R sv = 0;
       if (g.terrain && k >= 1 && k < nz) {
         const size_t c = g.at(k), cm = c - pl;
         R uw = (R)0.25 * (du[cm] + du[cm + sx] + du[c] + du[c + sx]);
         R vw = (R)0.25 * (dv[cm] + dv[cm + sy] + dv[c] + dv[c + sy]);
-        sv = Av[k * LCX] * (uw * g.hxc + vw * g.hyc) * a.co.fac_w[L.at1(k)];
+        sv = Av[k * kLcx<R>] * (uw * g.hxc + vw * g.hyc) * a.co.fac_w[L.at1(k)];
       }
-      dSv[k * LCX] = sv;
+      dSv[k * kLcx<R>] = sv;
     }
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = lane; k < nz; k += LKL) {
+    for (int k = lane; k < nz; k += kLkl<R>) {
       const size_t c = g.at(k);
       R Kt = a.co.kt3[c];
       R dDh = (a.co.rtjx[c + sx] * du[c + sx] - a.co.rtjx[c] * du[c]) * g.mcx +
@@ -1076,21 +1081,21 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
       R idz = a.co.inv_dzc[L.at1(k)];
       R dwk = d.w_in[c], dwkp = d.w_in[c + pl];
       R dtpi = d.tpi ? d.tpi[c] : (R)0;
-      const int q = k * LCX;
+      const int q = k * kLcx<R>;
       dP[q] = d.pi_cur[c] + dtau * dtpi -
-              dtau * Kt * (dDh - (dSv[q + LCX] - dSv[q]) * idz + c2 * (Av[q + LCX] * dwkp - Av[q] * dwk) * idz);
+              dtau * Kt * (dDh - (dSv[q + kLcx<R>] - dSv[q]) * idz + c2 * (Av[q + kLcx<R>] * dwkp - Av[q] * dwk) * idz);
     }
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = 1 + lane; k < nz; k += LKL) {
+    for (int k = 1 + lane; k < nz; k += kLkl<R>) {
       const size_t c = g.at(k), cm = c - pl;
-      const int q = k * LCX;
+      const int q = k * kLcx<R>;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
       R thvw = thd;
-      R dthvw = (R)0.5 * (dth[q - LCX] + dth[q]);
-      R dbuoy = Phys<R>::grav * (R)0.5 * (dth[q - LCX] + dth[q]) / a.b.thbw[c];
+      R dthvw = (R)0.5 * (dth[q - kLcx<R>] + dth[q]);
+      R dbuoy = Phys<R>::grav * (R)0.5 * (dth[q - kLcx<R>] + dth[q]) / a.b.thbw[c];
       if (a.p.moisture) {
         // theta_v = theta (1 + 0.61 qv); buoyancy + g (0.61 qv' - qc - qr)
         const R mq = (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
@@ -1103,13 +1108,13 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
       const R dG = dtau * Phys<R>::cp * dthvw * c1 * iJdz;
       R dpi = d.pi_cur[c] - d.pi_cur[cm], pi = a.pi_cur[c] - a.pi_cur[cm];
       R dRHS = d.w_in[c] + dtau * (dbuoy + d.tw[c]) - dtau * Phys<R>::cp * c2 * (dthvw * pi + thvw * dpi) * iJdz;
-      R dD = dRHS - dG * (P[q] - P[q - LCX]) - G[q] * (dP[q] - dP[q - LCX]);
-      R dA = -dG * E[q - LCX] * Av[q - LCX];
-      R dB = dG * Av[q] * (E[q] + E[q - LCX]);
-      R dC = -dG * E[q] * Av[q + LCX];
+      R dD = dRHS - dG * (P[q] - P[q - kLcx<R>]) - G[q] * (dP[q] - dP[q - kLcx<R>]);
+      R dA = -dG * E[q - kLcx<R>] * Av[q - kLcx<R>];
+      R dB = dG * Av[q] * (E[q] + E[q - kLcx<R>]);
+      R dC = -dG * E[q] * Av[q + kLcx<R>];
       R mw = dB * W[q];
-      if (k > 1) mw += dA * W[q - LCX];
-      if (k < nz - 1) mw += dC * W[q + LCX];
+      if (k > 1) mw += dA * W[q - kLcx<R>];
+      if (k < nz - 1) mw += dC * W[q + kLcx<R>];
       rhs[q] = dD - mw;
     }
   __syncthreads();
@@ -1120,15 +1125,28 @@ __global__ void __launch_bounds__(LCX * LKL) k_tl_column(AcouArgs<R> a, AcouArgs
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
+    for (int k = lane; k <= nz; k += kLkl<R>) {
       const size_t c = g.at(k);
-      const int q = k * LCX;
+      const int q = k * kLcx<R>;
       if (k < nz) {
-        d.pi_next[c] = dP[q] - E[q] * (Av[q + LCX] * dw[q + LCX] - Av[q] * dw[q]);
-        d.th_out[c] = dth[q] + dtau * (d.tth[c] - (R)0.5 * (dw[q] + dw[q + LCX]) * a.b.dthbdz[c]);
+        d.pi_next[c] = dP[q] - E[q] * (Av[q + kLcx<R>] * dw[q + kLcx<R>] - Av[q] * dw[q]);
+        d.th_out[c] = dth[q] + dtau * (d.tth[c] - (R)0.5 * (dw[q] + dw[q + kLcx<R>]) * a.b.dthbdz[c]);
         d.w_out[c] = dw[q];
       } else {
         d.w_out[c] = 0;
+      }
+      // the forward launch's outputs (dyn_acou.cu phase 5, the same
+      // expressions on the same values): the forward column need not run
+      if (with_forward) {
+        if (k < nz) {
+          R wn = W[q], wn1 = W[q + kLcx<R>];
+          a.pi_next[c] = P[q] - E[q] * (Av[q + kLcx<R>] * wn1 - Av[q] * wn);
+          R wc = (R)0.5 * (wn + wn1);
+          a.th_out[c] = a.th_in[c] + dtau * (a.tth[c] - wc * a.b.dthbdz[c]);
+          a.w_out[c] = wn;
+        } else {
+          a.w_out[c] = 0;
+        }
       }
     }
 }
@@ -1140,11 +1158,11 @@ enum { A_WB = V_N, A_PB, A_TB, A_WS, A_LAM, A_GL, A_PIB, A_THB, A_KTD, A_NARR };
 // surface w at level 0, Sv(k) at levels 1..nz-1); k_ad_column_uv takes both
 // to the faces.
 template <typename R>
-__global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs<R> d, R* dhB, R* svB) {
+__global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, AcouArgs<R> d, R* dhB, R* svB) {
   extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
   const int tx = threadIdx.x, lane = threadIdx.y;
-  const int i = blockIdx.x * LCX + tx, j = blockIdx.y;
+  const int i = blockIdx.x * kLcx<R> + tx, j = blockIdx.y;
   const bool active = i < L.nx;
   const ColArr<R> S{reinterpret_cast<R*>(lin_smem), L.nz + 1};
   const ColGeom<R> g(a, i, j, active);
@@ -1175,9 +1193,9 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   const bool w_alias = d.w_out == d.w_in, th_alias = d.th_out == d.th_in;
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
+    for (int k = lane; k <= nz; k += kLkl<R>) {
       const size_t c = g.at(k);
-      const int q = k * LCX;
+      const int q = k * kLcx<R>;
       wb[q] = d.w_out[c];
       if (k < nz) {
         pb[q] = d.pi_next[c];
@@ -1190,12 +1208,12 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   // adjoint of the column solution w (level 0: surface w, level nz: the lid)
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
-      const int q = k * LCX;
+    for (int k = lane; k <= nz; k += kLkl<R>) {
+      const int q = k * kLcx<R>;
       const size_t c = g.at(k);
       R s = 0;
       if (k < nz) s += wb[q] - (R)0.5 * dtau * a.b.dthbdz[c] * tb[q] + E[q] * Av[q] * pb[q];
-      if (k >= 1) s += -(R)0.5 * dtau * a.b.dthbdz[c - pl] * tb[q - LCX] - E[q - LCX] * Av[q] * pb[q - LCX];
+      if (k >= 1) s += -(R)0.5 * dtau * a.b.dthbdz[c - pl] * tb[q - kLcx<R>] - E[q - kLcx<R>] * Av[q] * pb[q - kLcx<R>];
       ws[q] = s;
     }
   __syncthreads();
@@ -1205,8 +1223,8 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   // per inner level: what its row sends to neighbouring levels
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
-      const int q = k * LCX;
+    for (int k = lane; k <= nz; k += kLkl<R>) {
+      const int q = k * kLcx<R>;
       if (k < 1 || k >= nz) {
         GL[q] = 0;
         PIB[q] = 0;
@@ -1218,11 +1236,11 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
       const size_t c = g.at(k), cm = c - pl;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       const R lm = lam[q];
-      const R Ab = k > 1 ? -lm * W[q - LCX] : (R)0;
+      const R Ab = k > 1 ? -lm * W[q - kLcx<R>] : (R)0;
       const R Bb = -lm * W[q];
-      const R Cb = k < nz - 1 ? -lm * W[q + LCX] : (R)0;
-      const R Gb = Ab * (-E[q - LCX] * Av[q - LCX]) + Bb * (Av[q] * (E[q] + E[q - LCX])) +
-                   Cb * (-E[q] * Av[q + LCX]) - lm * (P[q] - P[q - LCX]);
+      const R Cb = k < nz - 1 ? -lm * W[q + kLcx<R>] : (R)0;
+      const R Gb = Ab * (-E[q - kLcx<R>] * Av[q - kLcx<R>]) + Bb * (Av[q] * (E[q] + E[q - kLcx<R>])) +
+                   Cb * (-E[q] * Av[q + kLcx<R>]) - lm * (P[q] - P[q - kLcx<R>]);
       const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
       const R mq = moist ? (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]) : (R)1;
       const R thvw = moist ? thd * mq : thd;
@@ -1240,9 +1258,9 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = lane; k < nz; k += LKL) {
+    for (int k = lane; k < nz; k += kLkl<R>) {
       const size_t c = g.at(k);
-      const int q = k * LCX;
+      const int q = k * kLcx<R>;
       // the adjoints this level accumulates into, all read first
       const R pic0 = piC[c];
       const R tpi0 = tpiB ? tpiB[c] : (R)0;
@@ -1257,13 +1275,13 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
       const R Kt = a.co.kt3[c];
       R Pb = pb[q];
       if (k >= 1) Pb -= GL[q];
-      if (k + 1 < nz) Pb += GL[q + LCX];
+      if (k + 1 < nz) Pb += GL[q + kLcx<R>];
       R pic = Pb;
       if (k >= 1) pic += PIB[q];
-      if (k + 1 < nz) pic -= PIB[q + LCX];
+      if (k + 1 < nz) pic -= PIB[q + kLcx<R>];
       R th = tb[q];
       if (k >= 1) th += THB[q];
-      if (k + 1 < nz) th += THB[q + LCX];
+      if (k + 1 < nz) th += THB[q + kLcx<R>];
       piC[c] = pic0 + pic;
       if (tpiB) tpiB[c] = tpi0 + dtau * Pb;
       dhB[c] = -dtau * Kt * Pb * g.mc;  // adjoint of the map-factor-scaled divergence
@@ -1272,7 +1290,7 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
       if (moist) {
         R qvs = 0, qcs = 0;
         if (k >= 1) qvs += QVB[q], qcs += QCB[q];
-        if (k + 1 < nz) qvs += QVB[q + LCX], qcs += QCB[q + LCX];
+        if (k + 1 < nz) qvs += QVB[q + kLcx<R>], qcs += QCB[q + kLcx<R>];
         qvI[c] = qv0 + qvs;
         qcI[c] = qc0 + qcs;
         qrI[c] = qr0 + qcs;
@@ -1284,13 +1302,13 @@ __global__ void __launch_bounds__(LCX * LKL) k_ad_column(AcouArgs<R> a, AcouArgs
   __syncthreads();
   if (active)
 #pragma unroll 4
-    for (int k = lane; k <= nz; k += LKL) {
-      const int q = k * LCX;
+    for (int k = lane; k <= nz; k += kLkl<R>) {
+      const int q = k * kLcx<R>;
       const size_t c = g.at(k);
       const R w0 = w_alias ? (R)0 : wI[c];
       R wsum = 0;
       if (k >= 1 && k < nz) wsum += lam[q];
-      R kd = (k < nz ? KTD[q] : (R)0) - (k >= 1 ? KTD[q - LCX] : (R)0);
+      R kd = (k < nz ? KTD[q] : (R)0) - (k >= 1 ? KTD[q - kLcx<R>] : (R)0);
       wsum += dtau * c2 * Av[q] * kd;
       wI[c] = w0 + wsum;
       if (!w_alias) d.w_out[c] = 0;
@@ -1408,7 +1426,7 @@ int lin_max_levels() { return 160; }  // FP64 adjoint column arrays within 227 K
 
 template <typename R, int NARR>
 static size_t lin_col_smem(int nz) {
-  return (size_t)NARR * (nz + 1) * LCX * sizeof(R);
+  return (size_t)NARR * (nz + 1) * kLcx<R> * sizeof(R);
 }
 
 // Sets the dynamic shared-memory limits of the column kernels for nz levels,
@@ -1425,10 +1443,11 @@ int lin_prepare(int nz) {
 }
 
 template <typename R>
-int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, cudaStream_t st) {
+int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, bool with_forward, cudaStream_t st) {
   if (a.L.nz > lin_max_levels()) return 2;
   const size_t sm = lin_col_smem<R, T_NARR>(a.L.nz);
-  k_tl_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d);
+  k_tl_column<R><<<dim3((a.L.nx + kLcx<R> - 1) / kLcx<R>, a.L.ny), dim3(kLcx<R>, kLkl<R>), sm, st>>>(
+      a, d, with_forward ? 1 : 0);
   return 0;
 }
 
@@ -1436,7 +1455,7 @@ template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st) {
   if (a.L.nz > lin_max_levels()) return 2;
   const size_t sm = lin_col_smem<R, A_NARR>(a.L.nz);
-  k_ad_column<R><<<dim3((a.L.nx + LCX - 1) / LCX, a.L.ny), dim3(LCX, LKL), sm, st>>>(a, d, scr.f[0], scr.f[1]);
+  k_ad_column<R><<<dim3((a.L.nx + kLcx<R> - 1) / kLcx<R>, a.L.ny), dim3(kLcx<R>, kLkl<R>), sm, st>>>(a, d, scr.f[0], scr.f[1]);
   k_ad_column_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d, scr.f[0], scr.f[1]);
   return 0;
 }
@@ -1448,7 +1467,7 @@ int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& s
   template void ad_tend<R>(const TendArgs<R>&, const TendArgs<R>&, cudaStream_t); \
   template void tl_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t);   \
   template void ad_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
-  template int tl_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, cudaStream_t); \
+  template int tl_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, bool, cudaStream_t); \
   template int ad_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
   template void zero_ring<R>(R*, const Layout&, cudaStream_t);                        \
   template int lin_prepare<R>(int);

@@ -8,7 +8,8 @@
 // that launch (lin.cu).
 //
 // TL:  per launch, the TL kernel (forward values still in place) and then the
-//      forward launch.
+//      forward launch; the column's TL launch writes the forward column's
+//      outputs itself, bit for bit.
 // AD:  the forward pass stores the time-n state every `every` steps.  The
 //      reverse sweep takes the segments last to first: it recomputes the
 //      segment storing every step's time-n state, then for each step (last
@@ -95,8 +96,10 @@ class LinT final : public Lin {
         std::vector<Rec> recs;
         if (m_->record_step(dt, &recs)) return fail(m_->error());
         if (capture(&ge, [&] {
-              for (const Rec& r : recs)
-                if (tl(r) || fwd(r)) return 1;
+              for (const Rec& r : recs) {
+                bool done = false;  // the TL launch also did the forward one
+                if (tl(r, &done) || (!done && fwd(r))) return 1;
+              }
               return 0;
             }))
           return 1;
@@ -243,7 +246,8 @@ class LinT final : public Lin {
     return 0;
   }
 
-  int tl(const Rec& r) {
+  int tl(const Rec& r, bool* did_forward) {
+    *did_forward = false;
     switch (r.kind) {
       case K_FILL: {
         const FillArgs<R> d = tr(as<FillArgs<R>>(r));
@@ -267,7 +271,8 @@ class LinT final : public Lin {
       }
       case K_COL: {
         const auto& a = as<AcouArgs<R>>(r);
-        if (tl_column<R>(a, tr(a), st_)) return fail("column deeper than the linearised kernels hold");
+        if (tl_column<R>(a, tr(a), true, st_)) return fail("column deeper than the linearised kernels hold");
+        *did_forward = true;
         break;
       }
       case K_KES: {
