@@ -264,12 +264,17 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   }
 }
 
+// FP32: 32 registers, eight CTAs per SM -- the kernel waits on loads, and the
+// extra resident warps hide more of that than the few spills cost
 template <typename R>
-__global__ void __launch_bounds__(256) k_acoustic_uv(AcouArgs<R> a) {
+constexpr int kUvMinBlocks = sizeof(R) == 4 ? 8 : 1;
+
+template <typename R>
+__global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv(AcouArgs<R> a) {
   uv_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R>
-__global__ void __launch_bounds__(256) k_acoustic_uv_batch(Batch<AcouArgs<R>> b) {
+__global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv_batch(Batch<AcouArgs<R>> b) {
   for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int z) { uv_body(a, x, y, z); });
 }
 

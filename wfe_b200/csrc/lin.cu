@@ -641,8 +641,12 @@ __device__ void row_v_out(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R
   }
 }
 
+// FP32: eight CTAs per SM (32 registers) for the load-bound u, v kernels
 template <typename R>
-__global__ void __launch_bounds__(256) k_tl_uv(AcouArgs<R> a, AcouArgs<R> d) {
+constexpr int kUvLinMinBlocks = sizeof(R) == 4 ? 8 : 1;
+
+template <typename R>
+__global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_tl_uv(AcouArgs<R> a, AcouArgs<R> d) {
   const Layout& L = a.L;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -738,7 +742,7 @@ __device__ __forceinline__ void ad_uv_face(const AcouArgs<R>& a, const AcouArgs<
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_ad_uv_faces(AcouArgs<R> a, AcouArgs<R> d, UvScr<R> w) {
+__global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_ad_uv_faces(AcouArgs<R> a, AcouArgs<R> d, UvScr<R> w) {
   const Layout& L = a.L;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -749,7 +753,7 @@ __global__ void __launch_bounds__(256) k_ad_uv_faces(AcouArgs<R> a, AcouArgs<R> 
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_ad_uv_cells(AcouArgs<R> a, AcouArgs<R> d, UvScr<R> w) {
+__global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_ad_uv_cells(AcouArgs<R> a, AcouArgs<R> d, UvScr<R> w) {
   const Layout& L = a.L;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
