@@ -252,6 +252,18 @@ template <typename R>
 int lin_prepare(int nz);
 template <typename R>
 int lin_kessler_prepare(int nz);
+// copy `count` whole fields of n elements each (src[f] -> dst[f]) in one
+// launch; 16-byte aligned pointers and n * sizeof(R) a multiple of 16, else
+// nothing is launched and 1 is returned
+constexpr int kCopyMax = 8;
+template <typename R>
+struct CopyJob {
+  const R* src[kCopyMax];
+  R* dst[kCopyMax];
+  int count;
+};
+template <typename R>
+int copy_fields(const CopyJob<R>& job, size_t n, cudaStream_t st);
 // zero a cell field outside the interior cells (the pi' ghost ring, which no
 // launch of a step reads or writes)
 template <typename R>

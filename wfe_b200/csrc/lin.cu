@@ -1364,6 +1364,21 @@ __global__ void __launch_bounds__(256) k_ad_column_uv(AcouArgs<R> a, AcouArgs<R>
   }
 }
 
+// Undo-log copies: up to kCopyMax whole fields (n elements each) in one
+// launch, 16-byte vectors, grid-stride over fields x chunks.
+template <typename R>
+__global__ void __launch_bounds__(256) k_copy_fields(CopyJob<R> job, size_t n) {
+  const size_t nv = n * sizeof(R) / 16;  // n * sizeof(R) is a multiple of 16 (copy_fields)
+  const size_t total = nv * (size_t)job.count;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(q / nv);
+    const size_t e = q - (size_t)f * nv;
+    reinterpret_cast<uint4*>(job.dst[f])[e] = reinterpret_cast<const uint4*>(job.src[f])[e];
+  }
+}
+
+
 // zero every stored point of a cell field outside the interior cells
 template <typename R>
 __global__ void k_zero_ring(R* f, Layout L) {
@@ -1380,6 +1395,16 @@ __global__ void k_zero_ring(R* f, Layout L) {
 }  // namespace
 
 // ------------------------------------------------------------ host launch
+template <typename R>
+int copy_fields(const CopyJob<R>& job, size_t n, cudaStream_t st) {
+  if (job.count < 1) return 0;
+  if (job.count > kCopyMax || (n * sizeof(R)) % 16) return 1;
+  for (int f = 0; f < job.count; ++f)
+    if ((reinterpret_cast<uintptr_t>(job.src[f]) | reinterpret_cast<uintptr_t>(job.dst[f])) % 16) return 1;
+  k_copy_fields<R><<<148 * 8, 256, 0, st>>>(job, n);
+  return 0;
+}
+
 template <typename R>
 void zero_ring(R* f, const Layout& L, cudaStream_t st) {
   k_zero_ring<R><<<1184, 256, 0, st>>>(f, L);
@@ -1474,6 +1499,7 @@ int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& s
   template int tl_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, bool, cudaStream_t); \
   template int ad_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
   template void zero_ring<R>(R*, const Layout&, cudaStream_t);                        \
+  template int copy_fields<R>(const CopyJob<R>&, size_t, cudaStream_t);               \
   template int lin_prepare<R>(int);
 WFE_INST(float)
 WFE_INST(double)

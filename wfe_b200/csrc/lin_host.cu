@@ -449,11 +449,13 @@ class LinT final : public Lin {
           for (auto& st : recs)
             for (const Rec& r : st) {
               outputs(r, &oo);
+              CopyJob<R> job{};
               for (R* p : oo) {
-                LCK(cudaMemcpyAsync(log_ + slot * n3_, p, n3_ * sizeof(R), cudaMemcpyDeviceToDevice,
-                                    st_));
+                job.src[job.count] = p;
+                job.dst[job.count++] = log_ + slot * n3_;
                 ++slot;
               }
+              if (copy_fields<R>(job, n3_, st_)) return fail("undo-log copy");
               if (fwd(r, true)) return 1;
             }
           return 0;
@@ -465,11 +467,13 @@ class LinT final : public Lin {
           for (size_t s = recs.size(); s-- > 0;)
             for (size_t q = recs[s].size(); q-- > 0;) {
               outputs(recs[s][q], &oo);
+              CopyJob<R> job{};
               for (size_t z = oo.size(); z-- > 0;) {
                 --slot;
-                LCK(cudaMemcpyAsync(oo[z], log_ + slot * n3_, n3_ * sizeof(R),
-                                    cudaMemcpyDeviceToDevice, st_));
+                job.src[job.count] = log_ + slot * n3_;
+                job.dst[job.count++] = oo[z];
               }
+              if (copy_fields<R>(job, n3_, st_)) return fail("undo-log copy");
               if (ad(recs[s][q])) return 1;
             }
           return 0;
