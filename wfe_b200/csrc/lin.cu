@@ -71,26 +71,42 @@ __device__ __forceinline__ size_t off(size_t c, long d) { return (size_t)((long)
 // ================================================================ tendencies
 enum { T_U = 0, T_V, T_W, T_TH, T_MFX, T_MFY, T_MFZ, T_QV, T_QC, T_QR, T_N };
 
-// Contribution cF * dF of one flux F = fv face5(Q[c + (b + n) s], fv): fv is
-// 0.5 (MF[ma] + MF[mb]) (avg) or MF[ma].
+// The two faces of one direction of a cell, cL dF_L + cR dF_R, with the
+// face-5 stencils (offsets -3..2 of the left face, -2..3 of the right) merged
+// into one weight per point: seven q terms instead of up to twelve.  Left
+// face mass flux: 0.5 (MF[maL] + MF[mbL]) (avg) or MF[maL]; right likewise.
 template <typename R, class Acc>
-__device__ __forceinline__ void emit_face(Acc& acc, R cF, const R* MF, int mfid, size_t ma, size_t mb,
-                                          bool avg, const R* Q, int qid, size_t c, long s, int b) {
-  const R fv = avg ? (R)0.5 * (MF[ma] + MF[mb]) : MF[ma];
+__device__ __forceinline__ void emit_face_pair(Acc& acc, R cL, R cR, const R* MF, int mfid, size_t maL,
+                                               size_t mbL, size_t maR, size_t mbR, bool avg, const R* Q,
+                                               int qid, size_t c, long s) {
+  const R fvL = avg ? (R)0.5 * (MF[maL] + MF[mbL]) : MF[maL];
+  const R fvR = avg ? (R)0.5 * (MF[maR] + MF[mbR]) : MF[maR];
   const R* Qc = Q + c;
-  const R face = face5(Qc[(long)b * s], Qc[(long)(b + 1) * s], Qc[(long)(b + 2) * s],
-                       Qc[(long)(b + 3) * s], Qc[(long)(b + 4) * s], Qc[(long)(b + 5) * s], fv);
-  if (avg) {
-    acc(mfid, ma, cF * (R)0.5 * face);
-    acc(mfid, mb, cF * (R)0.5 * face);
-  } else {
-    acc(mfid, ma, cF * face);
-  }
-  R w[6];
-  face5_weights(fv, w);
+  R q[7];
 #pragma unroll
-  for (int n = 0; n < 6; ++n)
-    if (w[n] != (R)0) acc(qid, off(c, (long)(b + n) * s), cF * fv * w[n]);
+  for (int n = 0; n < 7; ++n) q[n] = Qc[(long)(n - 3) * s];
+  const R faceL = face5(q[0], q[1], q[2], q[3], q[4], q[5], fvL);
+  const R faceR = face5(q[1], q[2], q[3], q[4], q[5], q[6], fvR);
+  if (avg) {
+    acc(mfid, maL, cL * (R)0.5 * faceL);
+    acc(mfid, mbL, cL * (R)0.5 * faceL);
+    acc(mfid, maR, cR * (R)0.5 * faceR);
+    acc(mfid, mbR, cR * (R)0.5 * faceR);
+  } else {
+    acc(mfid, maL, cL * faceL);
+    acc(mfid, maR, cR * faceR);
+  }
+  R wL[6], wR[6];
+  face5_weights(fvL, wL);
+  face5_weights(fvR, wR);
+  const R gL = cL * fvL, gR = cR * fvR;
+#pragma unroll
+  for (int n = 0; n < 7; ++n) {
+    R wgt = 0;
+    if (n < 6) wgt += gL * wL[n];
+    if (n >= 1) wgt += gR * wR[n - 1];
+    if (wgt != (R)0) acc(qid, off(c, (long)(n - 3) * s), wgt);
+  }
 }
 
 // coef * d divergence(i, j, k) (src/dynamics/kernels.cu:99-110)
@@ -142,12 +158,12 @@ __device__ void row_tu(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const long sx = 1, sy = L.px, sz = (long)L.plane();
   const R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
   const R dzc = a.m.dzeta_c[kk];
-  emit_face(acc, (R)1 / (a.dx * ru), a.mfx, T_MFX, off(c, -sx), c, true, a.u, T_U, c, sx, -3);
-  emit_face(acc, -(R)1 / (a.dx * ru), a.mfx, T_MFX, c, off(c, sx), true, a.u, T_U, c, sx, -2);
-  emit_face(acc, (R)1 / (a.dy * ru), a.mfy, T_MFY, off(c, -sx), c, true, a.u, T_U, c, sy, -3);
-  emit_face(acc, -(R)1 / (a.dy * ru), a.mfy, T_MFY, off(c, sy - sx), off(c, sy), true, a.u, T_U, c, sy, -2);
-  emit_face(acc, (R)1 / (dzc * ru), a.mfz, T_MFZ, off(c, -sx), c, true, a.u, T_U, c, sz, -3);
-  emit_face(acc, -(R)1 / (dzc * ru), a.mfz, T_MFZ, off(c, sz - sx), off(c, sz), true, a.u, T_U, c, sz, -2);
+  emit_face_pair(acc, (R)1 / (a.dx * ru), -(R)1 / (a.dx * ru), a.mfx, T_MFX, off(c, -sx), c,
+                 c, off(c, sx), true, a.u, T_U, c, sx);
+  emit_face_pair(acc, (R)1 / (a.dy * ru), -(R)1 / (a.dy * ru), a.mfy, T_MFY, off(c, -sx), c,
+                 off(c, sy - sx), off(c, sy), true, a.u, T_U, c, sy);
+  emit_face_pair(acc, (R)1 / (dzc * ru), -(R)1 / (dzc * ru), a.mfz, T_MFZ, off(c, -sx), c,
+                 off(c, sz - sx), off(c, sz), true, a.u, T_U, c, sz);
   const R dv = (R)0.5 * (div_value(a, i - 1, j, k) + div_value(a, i, j, k));
   const R u0 = a.u[c];
   emit_div(acc, a, i - 1, j, k, u0 * (R)0.5 / ru);
@@ -170,12 +186,12 @@ __device__ void row_tv(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const long sx = 1, sy = L.px, sz = (long)L.plane();
   const R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
   const R dzc = a.m.dzeta_c[kk];
-  emit_face(acc, (R)1 / (a.dy * rv), a.mfy, T_MFY, off(c, -sy), c, true, a.v, T_V, c, sy, -3);
-  emit_face(acc, -(R)1 / (a.dy * rv), a.mfy, T_MFY, c, off(c, sy), true, a.v, T_V, c, sy, -2);
-  emit_face(acc, (R)1 / (a.dx * rv), a.mfx, T_MFX, off(c, -sy), c, true, a.v, T_V, c, sx, -3);
-  emit_face(acc, -(R)1 / (a.dx * rv), a.mfx, T_MFX, off(c, sx - sy), off(c, sx), true, a.v, T_V, c, sx, -2);
-  emit_face(acc, (R)1 / (dzc * rv), a.mfz, T_MFZ, off(c, -sy), c, true, a.v, T_V, c, sz, -3);
-  emit_face(acc, -(R)1 / (dzc * rv), a.mfz, T_MFZ, off(c, sz - sy), off(c, sz), true, a.v, T_V, c, sz, -2);
+  emit_face_pair(acc, (R)1 / (a.dy * rv), -(R)1 / (a.dy * rv), a.mfy, T_MFY, off(c, -sy), c,
+                 c, off(c, sy), true, a.v, T_V, c, sy);
+  emit_face_pair(acc, (R)1 / (a.dx * rv), -(R)1 / (a.dx * rv), a.mfx, T_MFX, off(c, -sy), c,
+                 off(c, sx - sy), off(c, sx), true, a.v, T_V, c, sx);
+  emit_face_pair(acc, (R)1 / (dzc * rv), -(R)1 / (dzc * rv), a.mfz, T_MFZ, off(c, -sy), c,
+                 off(c, sz - sy), off(c, sz), true, a.v, T_V, c, sz);
   const R dv = (R)0.5 * (div_value(a, i, j - 1, k) + div_value(a, i, j, k));
   const R v0 = a.v[c];
   emit_div(acc, a, i, j - 1, k, v0 * (R)0.5 / rv);
@@ -198,12 +214,12 @@ __device__ void row_tw(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const long sx = 1, sy = L.px, sz = (long)L.plane();
   const R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
   const R dzw = a.m.dzeta_w[kk];
-  emit_face(acc, (R)1 / (a.dx * rw), a.mfx, T_MFX, off(c, -sz), c, true, a.w, T_W, c, sx, -3);
-  emit_face(acc, -(R)1 / (a.dx * rw), a.mfx, T_MFX, off(c, sx - sz), off(c, sx), true, a.w, T_W, c, sx, -2);
-  emit_face(acc, (R)1 / (a.dy * rw), a.mfy, T_MFY, off(c, -sz), c, true, a.w, T_W, c, sy, -3);
-  emit_face(acc, -(R)1 / (a.dy * rw), a.mfy, T_MFY, off(c, sy - sz), off(c, sy), true, a.w, T_W, c, sy, -2);
-  emit_face(acc, (R)1 / (dzw * rw), a.mfz, T_MFZ, off(c, -sz), c, true, a.w, T_W, c, sz, -3);
-  emit_face(acc, -(R)1 / (dzw * rw), a.mfz, T_MFZ, c, off(c, sz), true, a.w, T_W, c, sz, -2);
+  emit_face_pair(acc, (R)1 / (a.dx * rw), -(R)1 / (a.dx * rw), a.mfx, T_MFX, off(c, -sz), c,
+                 off(c, sx - sz), off(c, sx), true, a.w, T_W, c, sx);
+  emit_face_pair(acc, (R)1 / (a.dy * rw), -(R)1 / (a.dy * rw), a.mfy, T_MFY, off(c, -sz), c,
+                 off(c, sy - sz), off(c, sy), true, a.w, T_W, c, sy);
+  emit_face_pair(acc, (R)1 / (dzw * rw), -(R)1 / (dzw * rw), a.mfz, T_MFZ, off(c, -sz), c,
+                 c, off(c, sz), true, a.w, T_W, c, sz);
   const R dv = (R)0.5 * (div_value(a, i, j, k - 1) + div_value(a, i, j, k));
   const R w0 = a.w[c];
   emit_div(acc, a, i, j, k - 1, w0 * (R)0.5 / rw);
@@ -221,12 +237,12 @@ __device__ void row_tth(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const long sx = 1, sy = L.px, sz = (long)L.plane();
   const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
   const R dzc = a.m.dzeta_c[kk];
-  emit_face(acc, (R)1 / (a.dx * rt), a.mfx, T_MFX, c, c, false, a.thp, T_TH, c, sx, -3);
-  emit_face(acc, -(R)1 / (a.dx * rt), a.mfx, T_MFX, off(c, sx), 0, false, a.thp, T_TH, c, sx, -2);
-  emit_face(acc, (R)1 / (a.dy * rt), a.mfy, T_MFY, c, c, false, a.thp, T_TH, c, sy, -3);
-  emit_face(acc, -(R)1 / (a.dy * rt), a.mfy, T_MFY, off(c, sy), 0, false, a.thp, T_TH, c, sy, -2);
-  emit_face(acc, (R)1 / (dzc * rt), a.mfz, T_MFZ, c, c, false, a.thp, T_TH, c, sz, -3);
-  emit_face(acc, -(R)1 / (dzc * rt), a.mfz, T_MFZ, off(c, sz), 0, false, a.thp, T_TH, c, sz, -2);
+  emit_face_pair(acc, (R)1 / (a.dx * rt), -(R)1 / (a.dx * rt), a.mfx, T_MFX, c, c,
+                 off(c, sx), 0, false, a.thp, T_TH, c, sx);
+  emit_face_pair(acc, (R)1 / (a.dy * rt), -(R)1 / (a.dy * rt), a.mfy, T_MFY, c, c,
+                 off(c, sy), 0, false, a.thp, T_TH, c, sy);
+  emit_face_pair(acc, (R)1 / (dzc * rt), -(R)1 / (dzc * rt), a.mfz, T_MFZ, c, c,
+                 off(c, sz), 0, false, a.thp, T_TH, c, sz);
   const R div = div_value(a, i, j, k);
   emit_div(acc, a, i, j, k, a.thp[c] / rt);
   acc(T_TH, c, div / rt - sponge(a.m.zeta_c[kk], a.m.zt, a.p));
@@ -242,12 +258,12 @@ __device__ void row_tq(Acc& acc, const TendArgs<R>& a, const R* q, int qid, int 
   const long sx = 1, sy = L.px, sz = (long)L.plane();
   const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
   const R dzc = a.m.dzeta_c[kk];
-  emit_face(acc, (R)1 / (a.dx * rt), a.mfx, T_MFX, c, c, false, q, qid, c, sx, -3);
-  emit_face(acc, -(R)1 / (a.dx * rt), a.mfx, T_MFX, off(c, sx), 0, false, q, qid, c, sx, -2);
-  emit_face(acc, (R)1 / (a.dy * rt), a.mfy, T_MFY, c, c, false, q, qid, c, sy, -3);
-  emit_face(acc, -(R)1 / (a.dy * rt), a.mfy, T_MFY, off(c, sy), 0, false, q, qid, c, sy, -2);
-  emit_face(acc, (R)1 / (dzc * rt), a.mfz, T_MFZ, c, c, false, q, qid, c, sz, -3);
-  emit_face(acc, -(R)1 / (dzc * rt), a.mfz, T_MFZ, off(c, sz), 0, false, q, qid, c, sz, -2);
+  emit_face_pair(acc, (R)1 / (a.dx * rt), -(R)1 / (a.dx * rt), a.mfx, T_MFX, c, c,
+                 off(c, sx), 0, false, q, qid, c, sx);
+  emit_face_pair(acc, (R)1 / (a.dy * rt), -(R)1 / (a.dy * rt), a.mfy, T_MFY, c, c,
+                 off(c, sy), 0, false, q, qid, c, sy);
+  emit_face_pair(acc, (R)1 / (dzc * rt), -(R)1 / (dzc * rt), a.mfz, T_MFZ, c, c,
+                 off(c, sz), 0, false, q, qid, c, sz);
   emit_div(acc, a, i, j, k, q[c] / rt);
   acc(qid, c, div_value(a, i, j, k) / rt);
 }
