@@ -127,14 +127,14 @@ class LinT final : public Lin {
     const int nseg = (nsteps + every - 1) / every;
     if ((int)snaps_.size() < nseg + 1) snaps_.resize(nseg + 1);
     std::vector<Snap>& segs = snaps_;
+    // (the last segment is not run here: its logged replay below is its
+    // forward run, and x_N is taken right after it)
     for (int g = 0; g < nseg; ++g) {
       const int s0 = g * every, len = std::min(nsteps, s0 + every) - s0;
       if (snap(&segs[g])) return 1;
-      if (m_->run(len, dt, t0 + s0 * dt)) return fail(m_->error());
+      if (g + 1 < nseg && m_->run(len, dt, t0 + s0 * dt)) return fail(m_->error());
     }
     Snap& last = snaps_[nseg];
-    if (snap(&last)) return 1;
-    if (zero() || load_lin_state()) return 1;
     // reverse sweep: per segment (last first) one graph replays the segment
     // forward saving every buffer each launch overwrites (the undo log), one
     // graph walks the launches backwards (restore outputs, adjoint kernel);
@@ -145,6 +145,13 @@ class LinT final : public Lin {
       SegGraphs* sg = nullptr;
       if (segment_graphs(segs[g].phase, len, dt, &sg)) return 1;
       LCK(cudaGraphLaunch(sg->fwd, st_));
+      if (g == nseg - 1) {
+        // the replay ends at x_N, one rotation phase per step further on:
+        // keep x_N, and put the adjoint of x_N in the slot of its time-n state
+        for (int q = 0; q < len; ++q) m_->rotate();
+        if (snap(&last) || zero() || load_lin_state()) return 1;
+        for (int q = 0; q < len; ++q) m_->rotate(), m_->rotate();
+      }
       LCK(cudaGraphLaunch(sg->rev, st_));
     }
     // dJ/dx0 sits in the slot of x0; move it to the slot of x_N
