@@ -156,3 +156,27 @@ def test_tangent_run_advances_the_state_like_the_forward(name, prec):
     for k in A.FIELDS5:
         assert np.array_equal(ref[k], got[k]), k
     c.close()
+
+
+@pytest.mark.parametrize("every", [1, 4, 5, 8])
+def test_dot_product_any_checkpoint_interval(every):
+    """The adjoint sweep is exact for every checkpoint interval: one step per
+    segment, segments of uneven length, and a single segment (no separate
+    forward run at all)."""
+    c, x0 = _spinup("schaer_open", "f64")
+    rng = np.random.default_rng(17)
+    dx, y = _rand_fields(c, rng), _rand_fields(c, rng)
+    n = 5
+    mdx = A.tangent(c, x0, dx, n)
+    mty = A.adjoint(c, x0, y, n, every=every)
+    lhs, rhs = _dot(mdx, y), _dot(dx, mty)
+    assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+    # the state ends at x_N either way
+    A.set_fields(c, x0)
+    c.run(n)
+    ref = A.get_fields(c)
+    A.adjoint(c, x0, y, n, every=every)
+    got = A.get_fields(c)
+    for k in A.FIELDS5:
+        assert np.array_equal(ref[k], got[k]), k
+    c.close()
