@@ -40,9 +40,10 @@ column (positive-definite limiter and w damping off, neither linearised):
 after W spin-up steps, value = wall time of wfe_ad_run over K steps
 (checkpoints every 30 steps, the fields already on the device; the second of
 two runs, the first captures the sweep's graphs) / CUDA-event time of the same
-K forward steps.  The line also gives the tangent-linear ratio and the
-dot-product gap <M dx, y> - <dx, M^T y> over min(K, 10) steps.  --fp64 runs the
-FP64 state.
+K forward steps.  The line also gives the tangent-linear ratio, the adjoint's
+with checkpoint_every = 0 (the longest interval the device memory holds: no
+recomputation when the whole undo log fits) and the dot-product gap
+<M dx, y> - <dx, M^T y> over min(K, 10) steps.  --fp64 runs the FP64 state.
 """
 
 from __future__ import annotations
@@ -448,16 +449,18 @@ def adjoint_bench(args, device: int) -> dict:
     y = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in A.FIELDS8}
     c.lin_enable()
     times = {}
-    for name in ("ad", "tl"):
+    for name in ("ad", "tl", "ad_auto"):
         t = []
         for rep in range(2):
             A.set_fields(c, x0)
             c.lin_zero()
-            A.set_fields(c, y if name == "ad" else dx, role="lin")
+            A.set_fields(c, dx if name == "tl" else y, role="lin")
             c.sync()
             t0 = time.perf_counter()
             if name == "ad":
                 c.ad_run(K, checkpoint_every=30)
+            elif name == "ad_auto":
+                c.ad_run(K, checkpoint_every=0)
             else:
                 c.tl_run(K)
             t.append(time.perf_counter() - t0)
@@ -477,6 +480,7 @@ def adjoint_bench(args, device: int) -> dict:
                    "checkpoint_every": 30},
         "fwd_ms_per_step": fwd_ms / K, "ad_ms_per_step": times["ad"] / K,
         "tl_ms_per_step": times["tl"] / K, "tl_cost_over_forward": times["tl"] / fwd_ms,
+        "ad_auto_checkpoint_cost_over_forward": times["ad_auto"] / fwd_ms,
         "dot_test": {"steps": m, "lhs": lhs, "rhs": rhs,
                      "rel_gap": abs(lhs - rhs) / max(abs(lhs), abs(rhs))},
     }

@@ -192,6 +192,9 @@ int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const d
 int wfe_lin_enable(wfe_ctx* ctx);
 int wfe_lin_zero(wfe_ctx* ctx);
 int wfe_tl_run(wfe_ctx* ctx, int nsteps, double dt, double t0);
+/* checkpoint_every <= 0: the longest interval whose undo log (every buffer
+ * each launch of a step overwrites) fits in 80 % of the free device memory;
+ * when the whole run fits, nothing is recomputed. */
 int wfe_ad_run(wfe_ctx* ctx, int nsteps, double dt, double t0, int checkpoint_every);
 
 /* --------------------------------------------------- batched ensembles */

@@ -158,11 +158,12 @@ def test_tangent_run_advances_the_state_like_the_forward(name, prec):
     c.close()
 
 
-@pytest.mark.parametrize("every", [1, 4, 5, 8])
+@pytest.mark.parametrize("every", [1, 4, 5, 8, 0])
 def test_dot_product_any_checkpoint_interval(every):
     """The adjoint sweep is exact for every checkpoint interval: one step per
-    segment, segments of uneven length, and a single segment (no separate
-    forward run at all)."""
+    segment, segments of uneven length, a single segment (no separate forward
+    run at all), and 0 (the longest interval the device memory holds: here a
+    single segment)."""
     c, x0 = _spinup("schaer_open", "f64")
     rng = np.random.default_rng(17)
     dx, y = _rand_fields(c, rng), _rand_fields(c, rng)
@@ -179,4 +180,22 @@ def test_dot_product_any_checkpoint_interval(every):
     got = A.get_fields(c)
     for k in A.FIELDS5:
         assert np.array_equal(ref[k], got[k]), k
+    c.close()
+
+
+def test_adjoint_across_growing_checkpoint_intervals():
+    """Longer segments need a larger undo log; the segment graphs captured for
+    the old log are retired with it, so a later call reusing a short segment
+    still runs on valid memory and gives the same gradient."""
+    c, x0 = _spinup("schaer_open", "f64")
+    rng = np.random.default_rng(23)
+    y = _rand_fields(c, rng)
+    n = 7
+    ref = None
+    for every in (2, 3, 7, 3, 2):
+        g = A.adjoint(c, x0, y, n, every=every)
+        if ref is None:
+            ref = g
+        for k in A.FIELDS5:
+            assert np.linalg.norm(g[k] - ref[k]) <= 1e-12 * max(np.linalg.norm(ref[k]), 1e-300), (every, k)
     c.close()

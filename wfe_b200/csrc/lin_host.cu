@@ -116,8 +116,10 @@ class LinT final : public Lin {
 
   int ad_run(int nsteps, double dt, double t0, int every) override {
     if (nsteps <= 0) return 0;
-    if (every < 1) every = 1;
     if (dt != dt_) drop_graphs(dt);
+    if (every < 1 && auto_interval(nsteps, dt, &every)) return 1;
+    // the undo log for the longest segment, before any segment graph runs
+    if (ensure_log(std::min(every, nsteps), dt)) return 1;
     // the adjoint of x_N, uploaded in the slot of the current time-n state;
     // pi' ghosts are no state, so adjoint values there are dropped
     if (L_.nx) zero_ring<R>(D(static_cast<R*>(m_->state_field(4))), L_, st_);
@@ -403,12 +405,48 @@ class LinT final : public Lin {
         cudaGraphExecDestroy(ge);
         ge = nullptr;
       }
+    drop_segment_graphs();
+    dt_ = dt;
+  }
+
+  void drop_segment_graphs() {
     for (auto& kv : seg_) {
       if (kv.second.fwd) cudaGraphExecDestroy(kv.second.fwd);
       if (kv.second.rev) cudaGraphExecDestroy(kv.second.rev);
     }
     seg_.clear();
-    dt_ = dt;
+  }
+
+  // undo-log slots (whole fields) one step needs: the outputs of its launches
+  int slots_per_step(double dt, size_t* out) {
+    std::vector<std::vector<Rec>> recs;
+    if (record_segment(m_->phase(), 1, dt, &recs)) return 1;
+    size_t slots = 0;
+    std::vector<R*> o;
+    for (const Rec& r : recs[0]) {
+      outputs(r, &o);
+      slots += o.size();
+    }
+    *out = slots;
+    return 0;
+  }
+
+  // An undo log for segments of up to `len` steps.  The segment graphs hold
+  // the log's address, so a new log first retires every one of them (after
+  // the stream has drained): none may run on a freed log.
+  int ensure_log(int len, double dt) {
+    size_t per = 0;
+    if (slots_per_step(dt, &per)) return 1;
+    const size_t slots = per * (size_t)len;
+    if (slots <= log_cap_) return 0;
+    LCK(cudaStreamSynchronize(st_));
+    drop_segment_graphs();
+    if (log_) cudaFree(log_);
+    log_ = nullptr;
+    log_cap_ = 0;
+    LCK(cudaMalloc(&log_, slots * n3_ * sizeof(R)));
+    log_cap_ = slots;
+    return 0;
   }
 
   // the launches of `len` steps from rotation phase `phase` (the model is
@@ -422,6 +460,22 @@ class LinT final : public Lin {
       m_->rotate();
     }
     while (m_->phase() != keep) m_->rotate();
+    return 0;
+  }
+
+  // The longest checkpoint interval whose undo log fits in 80 % of the free
+  // device memory (plus the log already held): with one segment the sweep
+  // recomputes nothing (the logged replay is the only forward run).
+  int auto_interval(int nsteps, double dt, int* every) {
+    size_t slots = 0;
+    if (slots_per_step(dt, &slots)) return 1;
+    size_t free_b = 0, total_b = 0;
+    LCK(cudaMemGetInfo(&free_b, &total_b));
+    const double per_step = (double)slots * n3_ * sizeof(R);
+    const double room = 0.8 * (double)free_b + (double)log_cap_ * n3_ * sizeof(R);
+    long n = per_step > 0 ? (long)(room / per_step) : nsteps;
+    if (n > nsteps) n = nsteps;
+    *every = n < 1 ? 1 : (int)n;
     return 0;
   }
 
@@ -442,13 +496,7 @@ class LinT final : public Lin {
         slots += o.size();
       }
     if (!rain_scratch_) LCK(cudaMalloc(&rain_scratch_, L_.n2() * sizeof(R)));
-    if (slots > log_cap_) {  // outside any capture
-      if (log_) cudaFree(log_);
-      log_ = nullptr;
-      log_cap_ = 0;
-      LCK(cudaMalloc(&log_, slots * n3_ * sizeof(R)));
-      log_cap_ = slots;
-    }
+    if (slots > log_cap_) return fail("undo log smaller than the segment (ensure_log not called)");
     SegGraphs g;
     if (capture(&g.fwd, [&] {
           size_t slot = 0;
