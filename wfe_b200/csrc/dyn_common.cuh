@@ -17,6 +17,12 @@ __device__ __forceinline__ R sponge(R zeta, R zt, const DParams<R>& p) {
   return p.rayleigh_alpha * s * s;
 }
 
+// a product the compiler may not fuse into a following add: face fluxes are
+// rounded once, wherever they are combined (so kernels that keep them in
+// registers and kernels that stage them in shared memory agree bit for bit)
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <typename R>
 __device__ __forceinline__ R face5(R qm2, R qm1, R q0, R q1, R q2, R q3, R vel) {
   // 5th-order upwind interface value (src/dynamics/kernels.cu:51-57)
@@ -24,6 +30,27 @@ __device__ __forceinline__ R face5(R qm2, R qm1, R q0, R q1, R q2, R q3, R vel) 
   R cen = c * ((R)37 * (q0 + q1) - (R)8 * (qm1 + q2) + (qm2 + q3));
   R upw = c * ((q3 - qm2) - (R)5 * (q2 - qm1) + (R)10 * (q1 - q0));
   return (vel >= (R)0) ? (cen - upw) : (cen + upw);
+}
+
+// ------------------------------------------------------ Davies relaxation
+template <typename R>
+__device__ __forceinline__ R time_fraction(const double* clk) {
+  // BdyManager::tfrac (src/dynamics/boundary.cpp:91-97)
+  double t = clk[CLK_T], lo = clk[CLK_TLO], hi = clk[CLK_THI];
+  if (hi <= lo) return 0;
+  double f = (t - lo) / (hi - lo);
+  return (R)(f < 0 ? 0.0 : (f > 1 ? 1.0 : f));
+}
+
+template <typename R>
+__device__ __forceinline__ R davies(const TendArgs<R>& a, int v, const R* f, int i, int j, int k) {
+  const Layout& L = a.L;
+  const R tf = time_fraction<R>(a.clock);
+  int iw = i < L.nx ? i : L.nx - 1, jw = j < L.ny ? j : L.ny - 1;
+  R w = a.wgt[L.at2(iw, jw)];
+  if (w <= (R)0) return 0;
+  size_t c = L.at(i, j, k);
+  return w * (((R)1 - tf) * a.lo[v][c] + tf * a.hi[v][c] - f[c]);
 }
 
 // ------------------------------------------------------ acoustic helpers

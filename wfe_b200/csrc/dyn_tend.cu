@@ -157,12 +157,12 @@ __device__ __forceinline__ R scalar_adv(const TendArgs<R>& a, const R* __restric
   R fxL = a.mfx[c], fxR = a.mfx[c + sx];
   R fyL = a.mfy[c], fyR = a.mfy[c + sy];
   R fzB = a.mfz[c], fzT = a.mfz[c + sz];
-  R FxL = fxL * face5(Q[-3 * (long)sx], Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], fxL);
-  R FxR = fxR * face5(Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], Q[3 * sx], fxR);
-  R FyL = fyL * face5(Q[-3 * (long)sy], Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], fyL);
-  R FyR = fyR * face5(Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], Q[3 * sy], fyR);
-  R FzB = fzB * face5(Q[-3 * (long)sz], Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], fzB);
-  R FzT = fzT * face5(Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], Q[3 * sz], fzT);
+  R FxL = mul_rn(fxL, face5(Q[-3 * (long)sx], Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], fxL));
+  R FxR = mul_rn(fxR, face5(Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], Q[3 * sx], fxR));
+  R FyL = mul_rn(fyL, face5(Q[-3 * (long)sy], Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], fyL));
+  R FyR = mul_rn(fyR, face5(Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], Q[3 * sy], fyR));
+  R FzB = mul_rn(fzB, face5(Q[-3 * (long)sz], Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], fzB));
+  R FzT = mul_rn(fzT, face5(Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], Q[3 * sz], fzT));
   R fdiv = (FxR - FxL) * a.co.inv_dx + (FyR - FyL) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[L.at1(k)];
   R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
   return (-fdiv + Q[0] * div) / rt;
@@ -288,25 +288,6 @@ __device__ __forceinline__ R laplacian(const TendArgs<R>& a, const R* f, int i, 
          (f[c + L.plane()] - 2 * cc + f[c - L.plane()]) / (dzl * dzl);
 }
 
-template <typename R>
-__device__ __forceinline__ R time_fraction(const double* clk) {
-  // BdyManager::tfrac (src/dynamics/boundary.cpp:91-97)
-  double t = clk[CLK_T], lo = clk[CLK_TLO], hi = clk[CLK_THI];
-  if (hi <= lo) return 0;
-  double f = (t - lo) / (hi - lo);
-  return (R)(f < 0 ? 0.0 : (f > 1 ? 1.0 : f));
-}
-
-template <typename R>
-__device__ __forceinline__ R davies(const TendArgs<R>& a, int v, const R* f, int i, int j, int k) {
-  const Layout& L = a.L;
-  const R tf = time_fraction<R>(a.clock);
-  int iw = i < L.nx ? i : L.nx - 1, jw = j < L.ny ? j : L.ny - 1;
-  R w = a.wgt[L.at2(iw, jw)];
-  if (w <= (R)0) return 0;
-  size_t c = L.at(i, j, k);
-  return w * (((R)1 - tf) * a.lo[v][c] + tf * a.hi[v][c] - f[c]);
-}
 
 // One moisture species: tendency (op API) or stage value (integrator).
 template <typename R>
@@ -544,7 +525,9 @@ template <typename R>
 void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
   dim3 blk(32, 4, 2);
   dim3 grd = grid_cells<R>(a.L);
-  if (variant == 1) {
+  if (variant == 3) {  // momentum only (beside the TMA-staged scalar kernel)
+    k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);
+  } else if (variant == 1) {
     k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);
     k_tendencies<R, TEND_SCAL><<<grd, blk, 0, st>>>(a);
   } else {

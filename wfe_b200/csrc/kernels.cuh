@@ -287,8 +287,29 @@ void launch_mass_flux(const Layout& L, const DBase<R>& b, const DMetric<R>& m, c
 template <typename R>
 void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st);
 // variant 0: one fused launch; 1: momentum and scalar launches
+// variant: 0 fused, 1 momentum + scalar launches, 3 momentum only (the
+// scalars then come from launch_tend_scal_tma)
 template <typename R>
 void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st);
+// TMA-staged scalar tendencies (dyn_tend_tma.cu): a CTA per tile of
+// kTtX x kTtY x kTtZ cells; tensor maps over the pitched fields with boxes
+// mfx (kTtX + 4) x kTtY x kTtZ, mfy kTtX x (kTtY + 1) x kTtZ, mfz
+// kTtX x kTtY x (kTtZ + 1), scalars (kTtX + 8) x (kTtY + 6) x (kTtZ + 6) for
+// theta', qv, qc, qr (q[1..3] only with moisture).  No positive-definite
+// moisture.
+constexpr int kTtX = 32, kTtY = 4, kTtZ = 4;
+template <typename R>
+struct TendTmaParams {
+  TendArgs<R> a;
+  unsigned* err;  // set to 1 when a tile's loads did not arrive in time
+  CUtensorMap mfx, mfy, mfz, q[4];
+};
+template <typename R>
+size_t tend_scal_tma_smem();
+template <typename R>
+int prepare_tend_scal_tma();
+template <typename R>
+void launch_tend_scal_tma(const TendTmaParams<R>& p, cudaStream_t st);
 
 template <typename R>
 void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,

@@ -36,7 +36,7 @@ namespace wfe {
 // Kernel variants picked by the autotuner.  Every variant computes the same
 // values with the same arithmetic; only launch shapes differ.
 struct Tune {
-  int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches
+  int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches, 2 with TMA-staged scalars
   int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
   int persist = 0;       // batched launches: 0 one block per work item, 1 persistent grid
   bool done = false;
@@ -125,6 +125,8 @@ class ModelT final : public Model {
     if (prepare_acoustic_column<R>(g_.nz) || prepare_kessler<R>(g_.nz))
       return fail("nz too large for the column kernels' shared memory");
     tma_ok_ = tensor_map_encoder() && prepare_acoustic_column_tma<R>(g_.nz) == 0;
+    tend_tma_ok_ = tensor_map_encoder() && tend_scal_tma_smem<R>() <= 227 * 1024 &&
+                   prepare_tend_scal_tma<R>() == 0;
     CK(cudaMalloc(&tma_err_, sizeof(unsigned)));
     CK(cudaMemset(tma_err_, 0, sizeof(unsigned)));
     const size_t n3 = L_.n3(), n2 = L_.n2(), n1 = L_.pz;
@@ -724,7 +726,7 @@ class ModelT final : public Model {
     std::string name = prop.name;
     for (char& ch : name)
       if (ch == ' ') ch = '_';
-    k << "v3|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
+    k << "v4|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
       << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0);
     return k.str();
   }
@@ -750,7 +752,9 @@ class ModelT final : public Model {
   }
 
   // WFE_COLUMN_VARIANT=<n> forces the acoustic column variant (0..5 tile
-  // shapes, 6 the TMA-staged kernel) after tuning, for tests and experiments
+  // shapes, 6 the TMA-staged kernel) and WFE_TEND_VARIANT=<n> the tendency
+  // variant (0 fused, 1 split, 2 momentum + TMA-staged scalars) after tuning,
+  // for tests and experiments
   int autotune(double dt) {
     const bool first = !tune_.done;
     int rc = autotune_variants(dt);
@@ -759,6 +763,11 @@ class ModelT final : public Model {
       const int v = std::atoi(cv);
       if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_)))
         tune_.column_cx = v;
+    }
+    const char* tv = std::getenv("WFE_TEND_VARIANT");
+    if (first && tv && *tv) {
+      const int v = std::atoi(tv);
+      if (v >= 0 && (v < 2 || (v == 2 && tend_tma_usable()))) tune_.tend_variant = v;
     }
     return rc;
   }
@@ -780,7 +789,8 @@ class ModelT final : public Model {
     GhostJob<R> job = ghost_job(N, false);
     launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_);
     float best = 1e30f;
-    for (int v = 0; v < 2; ++v) {
+    const int ntend = tend_tma_usable() ? 3 : 2;  // 2: momentum + TMA-staged scalars
+    for (int v = 0; v < ntend; ++v) {
       float ms;
       tune_.tend_variant = v;
       if (time_ms([&] { tendencies(N, N, X, (R)dt, (R)dt / 3, false); return 0; }, &ms)) return 1;
@@ -928,8 +938,17 @@ class ModelT final : public Model {
       a.qo_r = X[7];
       a.dt_stage = dt_stage;
     }
-    if (!record(K_TEND, a))
-      launch("tendencies", [&] { launch_tendencies<R>(a, tune_.tend_variant, st_); });
+    if (!record(K_TEND, a)) {
+      TendTmaParams<R> tp;
+      if (tune_.tend_variant == 2 && tend_tma_usable() && tend_tma_params(a, &tp) == 0) {
+        launch("tendencies", [&] {
+          launch_tendencies<R>(a, 3, st_);
+          launch_tend_scal_tma<R>(tp, st_);
+        });
+      } else {
+        launch("tendencies", [&] { launch_tendencies<R>(a, tune_.tend_variant == 1 ? 1 : 0, st_); });
+      }
+    }
   }
 
   // ns acoustic substeps from time n (N) into the stage output X
@@ -1016,6 +1035,51 @@ class ModelT final : public Model {
       return nullptr;
     }
     return &(tmaps_[key] = m);
+  }
+
+  bool tend_tma_usable() const { return tend_tma_ok_ && !(dp_.moisture && dp_.pd_moist); }
+
+  // tensor map of a pitched field with box (bx, by, bz) (cached per pointer and box)
+  const CUtensorMap* tmap3(const R* ptr, int bx, int by, int bz) {
+    const auto key = std::make_pair(static_cast<const void*>(ptr), ((bx * 512) + by) * 512 + bz + 1000000000);
+    auto it = tmaps_.find(key);
+    if (it != tmaps_.end()) return &it->second;
+    CUtensorMap m;
+    std::memset(&m, 0, sizeof(m));
+    const cuuint64_t dims[3] = {(cuuint64_t)L_.px, (cuuint64_t)L_.py, (cuuint64_t)L_.pz};
+    const cuuint64_t strides[2] = {(cuuint64_t)L_.px * sizeof(R), (cuuint64_t)L_.plane() * sizeof(R)};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = tensor_map_encoder()(
+        &m, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+        const_cast<R*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      fail("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+      return nullptr;
+    }
+    return &(tmaps_[key] = m);
+  }
+
+  int tend_tma_params(const TendArgs<R>& a, TendTmaParams<R>* tp) {
+    std::memset(static_cast<void*>(tp), 0, sizeof(*tp));
+    tp->a = a;
+    tp->err = tma_err_;
+    const CUtensorMap* m[3] = {tmap3(a.mfx, kTtX + 4, kTtY, kTtZ), tmap3(a.mfy, kTtX, kTtY + 1, kTtZ),
+                               tmap3(a.mfz, kTtX, kTtY, kTtZ + 1)};
+    for (auto* x : m)
+      if (!x) return 1;
+    tp->mfx = *m[0];
+    tp->mfy = *m[1];
+    tp->mfz = *m[2];
+    const R* q[4] = {a.thp, a.qv, a.qc, a.qr};
+    for (int f = 0; f < (dp_.moisture ? 4 : 1); ++f) {
+      const CUtensorMap* x = tmap3(q[f], kTtX + 8, kTtY + 6, kTtZ + 6);
+      if (!x) return 1;
+      tp->q[f] = *x;
+    }
+    return 0;
   }
 
   int tma_params(const AcouArgs<R>& a, TmaColParams<R>* tp) {
@@ -1256,6 +1320,7 @@ class ModelT final : public Model {
   long gen_ = 0;  // changes whenever buffer roles or physics switches change
   std::vector<Rec>* rec_ = nullptr;  // record mode when set
   bool tma_ok_ = false;              // TMA column variant usable
+  bool tend_tma_ok_ = false;         // TMA-staged scalar tendencies usable
   unsigned* tma_err_ = nullptr;      // set by a TMA tile load that timed out
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps_;
   cudaStream_t cs_st_ = nullptr;     // snapshot copy stream
