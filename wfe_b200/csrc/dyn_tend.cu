@@ -36,12 +36,22 @@ __device__ __forceinline__ R ghost_value(const Layout& L, const R* a, int kind, 
   return a[L.at(si, sj, map_zc(k, L.nz))];
 }
 
+// levels of a lateral ghost column one thread fills (one batch of loads)
+constexpr int kFillChunk = 8;
+__host__ __device__ inline int fill_chunks(int nz) {
+  return (nz + 2 * kRefNG + 1 + kFillChunk - 1) / kFillChunk;
+}
+
 template <typename R>
 __device__ __forceinline__ void fill_body(const FillArgs<R>& A, int bx, int by, int bz) {
-  // one thread per padded column (i, j) of one field
+  // one thread per padded column (i, j) of one field and part: part 0 fills
+  // the ghost levels of the interior columns, part p >= 1 the p-th chunk of
+  // kFillChunk levels of the lateral ghost columns (so that no thread walks a
+  // whole column)
   const Layout& L = A.L;
   const int open_x = A.open_x, open_y = A.open_y;
-  const int f = bz;
+  const int nparts = 1 + fill_chunks(L.nz);
+  const int f = bz / nparts, part = bz % nparts;
   if (f >= A.job.n) return;
   R* a = A.job.f[f];
   const int kind = A.job.kind[f];
@@ -54,19 +64,20 @@ __device__ __forceinline__ void fill_body(const FillArgs<R>& A, int bx, int by, 
   const int sj = map_lat(j, L.ny, jlast, open_y);
   const int k0 = -kRefNG, k1 = L.nz + kRefNG;  // inclusive
   if ((si != i) || (sj != j)) {
-    // lateral ghost column: every level; sources are another column, so the
-    // loads of a chunk of levels are issued before its stores
-    for (int kb = k0; kb <= k1; kb += 8) {
-      R v[8];
+    // lateral ghost column, levels of this part; the sources are another
+    // column, so the loads are issued before the stores
+    if (part == 0) return;
+    const int kb = k0 + (part - 1) * kFillChunk;
+    R v[kFillChunk];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (kb + u <= k1) v[u] = ghost_value(L, a, kind, si, sj, kb + u);
+    for (int u = 0; u < kFillChunk; ++u)
+      if (kb + u <= k1) v[u] = ghost_value(L, a, kind, si, sj, kb + u);
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (kb + u <= k1) a[L.at(i, j, kb + u)] = v[u];
-    }
+    for (int u = 0; u < kFillChunk; ++u)
+      if (kb + u <= k1) a[L.at(i, j, kb + u)] = v[u];
     return;
   }
+  if (part != 0) return;
   // interior column: the levels below 0 and from nz up (w(nz) is the rigid lid)
   R lo[kRefNG], hi[kRefNG + 1];
 #pragma unroll
@@ -473,7 +484,7 @@ void launch_axpy(const R* x, const R* y, R a, R* out, size_t n, cudaStream_t st)
 // ------------------------------------------------------------ host launch
 template <typename R>
 dim3 grid_fill(const FillArgs<R>& a) {
-  return dim3((a.L.nx + 6 + 31) / 32, (a.L.ny + 6 + 3) / 4, a.job.n);
+  return dim3((a.L.nx + 6 + 31) / 32, (a.L.ny + 6 + 3) / 4, a.job.n * (1 + fill_chunks(a.L.nz)));
 }
 
 template <typename R>
