@@ -6,15 +6,22 @@
 // kernel's recorded argument block `a` (forward values) plus the same block
 // `d` with the state-like pointers replaced by tangent (TL) or adjoint (AD)
 // buffers.  The ghost fill and the mass fluxes are linear, so their TL is the
-// forward kernel applied to the tangent buffers.  For the tendencies and the
-// forward u, v step one "row" function per output enumerates the nonzeros of
-// the output's Jacobian row -- (input array, index, coefficient) -- from the
-// forward values; TL gathers sum(coef * dx[index]) and AD scatters
-// coef * ybar into the adjoint arrays (atomics), so TL and AD are transposes
-// of each other by construction.  The implicit w - pi' column gets its own
-// TL (a second Thomas sweep with the same matrix, right-hand side
-// dD - dM w) and AD (the transposed tridiagonal solve M^T lambda = wbar,
-// then dDbar = lambda, dMbar = -lambda w^T on the three diagonals).
+// forward kernel applied to the tangent buffers.  For the tendencies one
+// "row" function per output enumerates the nonzeros of the output's Jacobian
+// row -- (input array, index, coefficient) -- from the forward values; TL
+// gathers sum(coef * dx[index]) and AD scatters coef * ybar into the adjoint
+// arrays (atomics), so TL and AD are transposes of each other by
+// construction.  The forward u, v step's TL gathers its rows the same way;
+// its AD is gather-form (per-face coefficients, then a per-cell gather, no
+// atomics).  The implicit w - pi' column gets its own TL (a second Thomas
+// sweep with the same matrix, right-hand side dD - dM w; the launch also
+// writes the forward column's outputs) and AD (the transposed tridiagonal
+// solve M^T lambda = wbar, then dDbar = lambda, dMbar = -lambda w^T on the
+// three diagonals; its u, v adjoints are gathered per face).
+//
+// Output adjoints are cleared only after their values have been used: a
+// store issued while the load of the same address is in flight stalls the
+// memory pipeline.
 //
 // Upwind selections, the radiation-boundary branch and the w(nz) = 0 lid are
 // frozen at the trajectory (the derivative of a piecewise-smooth step almost
