@@ -114,6 +114,14 @@ int wfe_sync(wfe_ctx* ctx);
 /* field_absmax (src/dynamics/kernels.cu:967-979): max |f| of a state field,
  * NaN reported as a value above every finite one. */
 int wfe_absmax(wfe_ctx* ctx, int field, float* out);
+/* The same value without stopping the stream (no counterpart in the
+ * reference): wfe_absmax_begin enqueues the reduction and its copy into
+ * page-locked slot `slot` (0 or 1) behind the work already queued;
+ * wfe_absmax_end waits for that slot and returns the value.  A driver loop
+ * can enqueue step s + 1 before reading step s's |w|, so the GPU never waits
+ * for the host; its watchdog then trips one step later. */
+int wfe_absmax_begin(wfe_ctx* ctx, int field, int slot);
+int wfe_absmax_end(wfe_ctx* ctx, int slot, float* out);
 /* FP64 dry-air mass of the state [kg] (no reference counterpart). */
 int wfe_dry_mass(wfe_ctx* ctx, double* out);
 /* launches of the package's own kernels per large step in the last

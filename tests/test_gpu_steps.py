@@ -227,3 +227,20 @@ def test_tendency_variants_are_bit_identical(name, prec, monkeypatch):
     for v in ("1", "2"):
         for k in W.FIELDS:
             assert np.array_equal(out["0"][k], out[v][k]), (v, k)
+
+
+@pytest.mark.gpu
+def test_watchdog_absmax_begin_end_matches_blocking_call():
+    """The non-blocking watchdog (two page-locked slots, read one step behind)
+    returns exactly what the blocking field_absmax returns for each step."""
+    c = W.Case(CASES / "wk82_small.ini", precision="f32")
+    seen = []
+    for s in range(1, 5):
+        c.run(1, c.dt, (s - 1) * c.dt)
+        c.absmax_begin("w", s & 1)
+        ref = c.field_absmax("w")
+        seen.append((s, ref))
+        if s > 1:
+            assert c.absmax_end((s - 1) & 1) == seen[-2][1]
+    assert c.absmax_end(4 & 1) == seen[-1][1]
+    c.close()

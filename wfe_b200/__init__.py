@@ -44,7 +44,7 @@ SYMBOLS = [
     "wfe_case_create", "wfe_case_create_text", "wfe_ctx_destroy", "wfe_last_error",
     "wfe_get_dims", "wfe_get_spacing", "wfe_get_flags", "wfe_get_metric", "wfe_get_base",
     "wfe_field_upload", "wfe_field_download", "wfe_field2d_download", "wfe_step", "wfe_run",
-    "wfe_sync", "wfe_absmax", "wfe_dry_mass", "wfe_launches_per_step", "wfe_op_apply_bcs",
+    "wfe_sync", "wfe_absmax", "wfe_absmax_begin", "wfe_absmax_end", "wfe_dry_mass", "wfe_launches_per_step", "wfe_op_apply_bcs",
     "wfe_op_tendencies", "wfe_op_acoustic", "wfe_op_moisture_stage", "wfe_op_kessler",
     "wfe_op_sfc", "wfe_set_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
     "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
@@ -94,6 +94,8 @@ def load_library(path: str | Path | None = None):
     lib.wfe_run.argtypes = [vp, C.c_int, C.c_double, C.c_double]
     lib.wfe_sync.argtypes = [vp]
     lib.wfe_absmax.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
+    lib.wfe_absmax_begin.argtypes = [vp, C.c_int, C.c_int]
+    lib.wfe_absmax_end.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
     lib.wfe_dry_mass.argtypes = [vp, dp]
     lib.wfe_launches_per_step.argtypes = [vp]
     lib.wfe_launches_per_step.restype = C.c_long
@@ -275,6 +277,16 @@ class Case:
     def field_absmax(self, name: str = "w") -> float:
         out = C.c_float()
         self._check(self._lib.wfe_absmax(self._h, FIELD_ID[name], C.byref(out)))
+        return float(out.value)
+
+    def absmax_begin(self, name: str = "w", slot: int = 0) -> None:
+        """enqueue max |field| into page-locked slot 0 or 1 without waiting"""
+        self._check(self._lib.wfe_absmax_begin(self._h, FIELD_ID[name], slot))
+
+    def absmax_end(self, slot: int = 0) -> float:
+        """wait for slot `slot` of absmax_begin and return its value"""
+        out = C.c_float()
+        self._check(self._lib.wfe_absmax_end(self._h, slot, C.byref(out)))
         return float(out.value)
 
     def dry_mass(self) -> float:

@@ -371,6 +371,17 @@ int wfe_absmax(wfe_ctx* c, int field, float* out) {
   return c->model->absmax(field, out) ? model_err(c) : WFE_OK;
 }
 
+int wfe_absmax_begin(wfe_ctx* c, int field, int slot) {
+  NEED_MODEL(c);
+  return c->model->absmax_begin(field, slot) ? model_err(c) : WFE_OK;
+}
+
+int wfe_absmax_end(wfe_ctx* c, int slot, float* out) {
+  NEED_MODEL(c);
+  if (!out) return set_err(c, WFE_ERR_ARG, "bad argument");
+  return c->model->absmax_end(slot, out) ? model_err(c) : WFE_OK;
+}
+
 int wfe_dry_mass(wfe_ctx* c, double* out) {
   NEED_MODEL(c);
   if (!c || !out) return WFE_ERR_ARG;

@@ -543,6 +543,29 @@ class ModelT final : public Model {
     return 0;
   }
 
+  int absmax_begin(int field, int slot) override {
+    if (slot < 0 || slot > 1) return fail("absmax slot must be 0 or 1");
+    R* d = field_ptr(ROLE_STATE, field);
+    if (!d) return fail("bad field");
+    if (!wd_async_) {
+      CK(cudaMalloc(&wd_async_, 2 * sizeof(unsigned int)));
+      CK(cudaHostAlloc(&wd_host_, 2 * sizeof(unsigned int), cudaHostAllocDefault));
+      for (auto& e : wd_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    CK(cudaMemsetAsync(wd_async_ + slot, 0, sizeof(unsigned int), st_));
+    launch_absmax<R>(d, L_.n3(), wd_async_ + slot, st_);
+    CK(cudaMemcpyAsync(wd_host_ + slot, wd_async_ + slot, sizeof(unsigned int), cudaMemcpyDeviceToHost, st_));
+    CK(cudaEventRecord(wd_ev_[slot], st_));
+    return 0;
+  }
+
+  int absmax_end(int slot, float* out) override {
+    if (slot < 0 || slot > 1 || !wd_async_) return fail("absmax_end without absmax_begin");
+    CK(cudaEventSynchronize(wd_ev_[slot]));
+    std::memcpy(out, wd_host_ + slot, sizeof(float));
+    return 0;
+  }
+
   int dry_mass(double* out) override {
     R** s = S_[perm_[0]];
     launch_dry_mass<R>(L_, db_, dm_, s[4], s[3], s[5], s[6], s[7], dp_.moisture, (R)g_.dx,
@@ -1268,6 +1291,15 @@ class ModelT final : public Model {
     if (st_) cudaStreamDestroy(st_);
     clock_ = nullptr;
     wd_ = nullptr;
+    if (wd_async_) cudaFree(wd_async_);
+    wd_async_ = nullptr;
+    if (wd_host_) cudaFreeHost(wd_host_);
+    wd_host_ = nullptr;
+    for (auto& e : wd_ev_)
+      if (e) {
+        cudaEventDestroy(e);
+        e = nullptr;
+      }
     mass_planes_ = nullptr;
     mass_ = nullptr;
     stage_ = nullptr;
@@ -1309,6 +1341,9 @@ class ModelT final : public Model {
   SfcBufs sf_;
   double* clock_ = nullptr;
   unsigned int* wd_ = nullptr;
+  unsigned int* wd_async_ = nullptr;   // two watchdog slots (absmax_begin / end)
+  unsigned int* wd_host_ = nullptr;    // their page-locked copies
+  cudaEvent_t wd_ev_[2] = {nullptr, nullptr};
   double *mass_planes_ = nullptr, *mass_ = nullptr;
   R* stage_ = nullptr;
   std::vector<R> tmp_;

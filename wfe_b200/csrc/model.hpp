@@ -61,6 +61,10 @@ class Model {
   virtual int run(int nsteps, double dt, double t0) = 0;
   virtual int sync() = 0;
   virtual int absmax(int field, float* out) = 0;
+  // the same, split: begin enqueues the reduction and its copy into page-locked
+  // slot `slot` (0 or 1) on the model's stream; end waits for that slot
+  virtual int absmax_begin(int field, int slot) = 0;
+  virtual int absmax_end(int slot, float* out) = 0;
   virtual int dry_mass(double* out) = 0;
 
   // boundary relaxation targets, reference padded layout; t_lo < t_hi
