@@ -176,6 +176,17 @@ int wfe_op_sfc(wfe_ctx* ctx, double dt, double t);
  * FP64) and weights (padded NX*NY): lo/hi valid at t_lo/t_hi. */
 int wfe_set_boundary(wfe_ctx* ctx, const double* const lo[5], const double* const hi[5],
                      const double* wgt, double t_lo, double t_hi);
+/* BdyManager::init's relaxation weights (src/dynamics/boundary.cpp:24-39),
+ * padded NX*NY FP64 into `out`: cos^2 ramp over `width` rows next to the
+ * open edges with 1/tau at the edge, and 1/nudge_tau (0: none) everywhere
+ * as the interior analysis-nudging floor.  Host only: works on a context
+ * created without a device. */
+int wfe_bdy_weights(const wfe_ctx* ctx, int width, double tau, double nudge_tau, double* out);
+/* No counterpart in the reference: switches the relaxation of
+ * wfe_set_boundary off again (the next step has no Davies / nudging term),
+ * e.g. to run the tangent-linear and adjoint runs of the next analysis
+ * cycle after a nudged forecast. */
+int wfe_clear_boundary(wfe_ctx* ctx);
 /* SfcPBL::init (surface.cu:440-482) from interior ny*nx FP64 arrays. */
 int wfe_set_physics(wfe_ctx* ctx, const double* tsk, const double* land, const double* lat,
                     const double* lon, const double* soilw, double start_hour_utc, int doy,

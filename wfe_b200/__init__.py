@@ -46,7 +46,7 @@ SYMBOLS = [
     "wfe_field_upload", "wfe_field_download", "wfe_field2d_download", "wfe_step", "wfe_run",
     "wfe_sync", "wfe_absmax", "wfe_absmax_begin", "wfe_absmax_end", "wfe_dry_mass", "wfe_launches_per_step", "wfe_op_apply_bcs",
     "wfe_op_tendencies", "wfe_op_acoustic", "wfe_op_moisture_stage", "wfe_op_kessler",
-    "wfe_op_sfc", "wfe_set_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
+    "wfe_op_sfc", "wfe_set_boundary", "wfe_bdy_weights", "wfe_clear_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
     "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
     "wfe_ensemble_step", "wfe_ensemble_sync", "wfe_ensemble_time_run",
     "wfe_ensemble_launches_per_step", "wfe_ensemble_variants", "wfe_lin_enable", "wfe_lin_zero",
@@ -108,6 +108,8 @@ def load_library(path: str | Path | None = None):
     lib.wfe_set_boundary.argtypes = [vp, C.POINTER(dp), C.POINTER(dp), dp, C.c_double,
                                      C.c_double]
     lib.wfe_set_physics.argtypes = [vp, dp, dp, dp, dp, dp, C.c_double, C.c_int, C.c_int]
+    lib.wfe_bdy_weights.argtypes = [vp, C.c_int, C.c_double, C.c_double, dp]
+    lib.wfe_clear_boundary.argtypes = [vp]
     lib.wfe_time_run.argtypes = [vp, C.c_int, C.c_double, C.c_double, dp]
     lib.wfe_dry_mass_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double] + \
         [vp] * 11
@@ -343,6 +345,18 @@ class Case:
         plo = (DP * 5)(*[_dptr(a) for a in keep[:5]])
         phi = (DP * 5)(*[_dptr(a) for a in keep[5:]])
         self._check(self._lib.wfe_set_boundary(self._h, plo, phi, _dptr(w), t_lo, t_hi))
+
+    def bdy_weights(self, width: int, tau: float, nudge_tau: float = 0.0) -> np.ndarray:
+        """BdyManager::init's relaxation weights (padded NY x NX): Davies ramp
+        of `width` rows with 1/tau at open edges, 1/nudge_tau inside"""
+        out = np.zeros(self.NY * self.NX, dtype=np.float64)
+        self._check(self._lib.wfe_bdy_weights(self._h, int(width), float(tau), float(nudge_tau),
+                                              _dptr(out)))
+        return out.reshape(self.NY, self.NX)
+
+    def clear_boundary(self) -> None:
+        """switch the relaxation of set_boundary off"""
+        self._check(self._lib.wfe_clear_boundary(self._h))
 
     def set_physics(self, tsk, land, lat, lon, soilw, start_hour: float, doy: int,
                     nonlocal_pbl: bool) -> None:

@@ -1,0 +1,303 @@
+"""Variational analysis and analysis nudging driven by the adjoint.
+
+Strong-constraint 4D-Var over a window of large steps:
+
+    J(x0) = 1/2 sum_f |(x0_f - xb_f) / sb_f|^2
+          + 1/2 sum_k |(H_k x(t_k) - y_k) / so_k|^2
+
+x(t) is the model trajectory from x0 (the forward step), xb the background,
+sb_f one background standard deviation per prognostic field (diagonal B),
+H_k point sampling of one prognostic field at large step t_k and so_k the
+observation standard deviation.  The gradient is one chained adjoint sweep:
+backwards from the last observation time, H_k^T R_k^-1 (H_k x - y_k) is added
+to the adjoint at each observation time and carried to the previous one by
+the adjoint run of the steps in between (wfe_ad_run: dJ/dx_end -> dJ/dx_start).
+
+``FourDVar.minimise`` is incremental (Gauss-Newton) 4D-Var: each outer loop
+relinearises about the current x0; its inner loop minimises the quadratic
+cost of the increment in the control variable chi = B^-1/2 dx by conjugate
+gradients, one tangent-linear and one adjoint sweep per iteration (the
+Hessian I + B^1/2 M^T H^T R^-1 H M B^1/2 is symmetric positive definite, and
+the tangent and adjoint runs are exact transposes of each other).
+
+The reference has no analysis step: it ingests analyses as boundary files and
+relaxes toward them with the BdyManager weights, the cos^2 Davies ramp at the
+open edges and 1/nudge_tau as the interior analysis-nudging floor
+(src/dynamics/boundary.cpp:24-39; the relaxation term of compute_tendencies,
+src/dynamics/kernels.cu:292-304, 981-995).  ``nudge`` feeds an analysis back
+through that same path: targets lo = hi = xa for (u, v, theta', pi', qv) and
+the BdyManager weights, so a forecast from the background relaxes toward the
+analysis instead of restarting from it.
+
+Fields are dicts of numpy arrays in the reference's padded layout; the
+control points (``control_mask``) are the prognostic points of each field.
+The solver only talks to a model object with ``names``, ``mask(name)``,
+``forecast(x0, n)``, ``tangent(x0, dx, n)`` and ``adjoint(x0, lam, n)``
+(``CaseModel`` wraps a Case), so its algebra is testable without a device.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import adjoint as A
+
+BDY_FIELDS = ("u", "v", "thp", "pip", "qv")
+
+
+# ------------------------------------------------------------------ model
+def control_mask(case, name: str) -> np.ndarray:
+    """Prognostic points of one field in the padded layout: cells for the
+    scalars, faces i = 0..nx for u, j = 0..ny for v, levels k = 0..nz for w
+    (src/core/grid.hpp:22-36).  Ghost points are refilled by each step and are
+    inputs of nothing."""
+    g = case.ng
+    m = np.zeros(case.shape, dtype=bool)
+    ex = 1 if name == "u" else 0
+    ey = 1 if name == "v" else 0
+    ez = 1 if name == "w" else 0
+    m[g:g + case.nz + ez, g:g + case.ny + ey, g:g + case.nx + ex] = True
+    return m
+
+
+class CaseModel:
+    """The forward, tangent-linear and adjoint runs of a Case as the solver
+    sees them.  ``every`` is the adjoint's checkpoint interval (0: the
+    largest the device memory allows)."""
+
+    def __init__(self, case, every: int = 0):
+        self.case = case
+        self.every = int(every)
+        self.names = A.state_names(case)
+        self._masks = {k: control_mask(case, k) for k in self.names}
+        case.lin_enable()
+
+    def mask(self, name: str) -> np.ndarray:
+        return self._masks[name]
+
+    def forecast(self, x0: dict, n: int) -> dict:
+        A.set_fields(self.case, x0)
+        if n > 0:
+            self.case.run(n)
+        return A.get_fields(self.case, names=self.names)
+
+    def tangent(self, x0: dict, dx: dict, n: int) -> dict:
+        if n == 0:
+            return {k: np.array(v, dtype=np.float64) for k, v in dx.items()}
+        return A.tangent(self.case, x0, dx, n)
+
+    def adjoint(self, x0: dict, lam: dict, n: int) -> dict:
+        if n == 0:
+            return {k: np.array(v, dtype=np.float64) for k, v in lam.items()}
+        return A.adjoint(self.case, x0, lam, n, every=self.every)
+
+
+# ----------------------------------------------------------- observations
+@dataclass
+class Obs:
+    """Point observations of one prognostic field after `step` large steps
+    (0 = the start of the window): flat indices into the padded layout,
+    values and standard deviation(s)."""
+
+    step: int
+    field: str
+    index: np.ndarray
+    value: np.ndarray
+    sigma: float | np.ndarray = 1.0
+
+    def __post_init__(self):
+        self.index = np.asarray(self.index, dtype=np.int64).ravel()
+        self.value = np.asarray(self.value, dtype=np.float64).ravel()
+        if self.index.shape != self.value.shape:
+            raise ValueError("one value per observed point")
+        s = np.broadcast_to(np.asarray(self.sigma, dtype=np.float64), self.value.shape)
+        if np.any(s <= 0):
+            raise ValueError("observation standard deviations must be positive")
+        self.sigma = np.array(s)
+
+    @staticmethod
+    def at(case, step: int, field: str, i, j, k, value, sigma=1.0) -> "Obs":
+        """observations at interior indices (i, j, k) of `field`"""
+        g = case.ng
+        i, j, k = (np.asarray(a, dtype=np.int64) for a in (i, j, k))
+        idx = ((k + g) * case.NY + (j + g)) * case.NX + (i + g)
+        return Obs(step, field, idx, value, sigma)
+
+    def sample(self, x: dict) -> np.ndarray:
+        return x[self.field].ravel()[self.index]
+
+    def scatter_into(self, lam: dict, r: np.ndarray) -> None:
+        """lam[field] += H^T r (repeated indices accumulate)"""
+        np.add.at(lam[self.field].reshape(-1), self.index, r)
+
+
+@dataclass
+class Result:
+    x: dict
+    cost: list = field(default_factory=list)       # J at the start of each outer loop, then at xa
+    inner_residual: list = field(default_factory=list)  # CG residual norms, one list per outer loop
+
+
+# ---------------------------------------------------------------- 4D-Var
+class FourDVar:
+    def __init__(self, model, xb: dict, sigma_b: dict | float, obs: list):
+        self.m = model
+        self.names = tuple(model.names)
+        self.xb = {k: np.asarray(xb[k], dtype=np.float64) for k in self.names}
+        sb = sigma_b if isinstance(sigma_b, dict) else {k: float(sigma_b) for k in self.names}
+        self.sb = {k: float(sb[k]) for k in self.names}
+        if any(v <= 0 for v in self.sb.values()):
+            raise ValueError("background standard deviations must be positive")
+        self.obs = list(obs)
+        for o in self.obs:
+            if o.field not in self.names:
+                raise ValueError(f"observed field {o.field!r} is not prognostic here")
+            if o.step < 0:
+                raise ValueError("observation steps count from the start of the window")
+            n = self.xb[o.field].size
+            if o.index.size and (o.index.min() < 0 or o.index.max() >= n):
+                raise ValueError("observation index outside the field")
+        # segment boundaries: the window start and every observation time
+        self.times = sorted({0} | {o.step for o in self.obs})
+        self._mask = {k: np.asarray(model.mask(k), dtype=bool) for k in self.names}
+
+    # ---- control vector <-> fields (prognostic points only)
+    def pack(self, x: dict) -> np.ndarray:
+        return np.concatenate([np.asarray(x[k]).reshape(-1)[self._mask[k].ravel()]
+                               for k in self.names])
+
+    def unpack(self, v: np.ndarray) -> dict:
+        out, o = {}, 0
+        for k in self.names:
+            m = self._mask[k]
+            a = np.zeros(m.shape)
+            n = int(m.sum())
+            a[m] = v[o:o + n]
+            out[k] = a
+            o += n
+        return out
+
+    def _sb_vec(self) -> np.ndarray:
+        return np.concatenate([np.full(int(self._mask[k].sum()), self.sb[k]) for k in self.names])
+
+    def _zeros(self) -> dict:
+        return {k: np.zeros_like(self.xb[k]) for k in self.names}
+
+    # ---- nonlinear pieces
+    def trajectory(self, x0: dict) -> dict:
+        """states at every segment boundary (step -> fields)"""
+        traj = {0: {k: np.asarray(x0[k], dtype=np.float64) for k in self.names}}
+        x = traj[0]
+        for a, b in zip(self.times[:-1], self.times[1:]):
+            x = self.m.forecast(x, b - a)
+            traj[b] = x
+        return traj
+
+    def _obs_at(self, t: int) -> list:
+        return [o for o in self.obs if o.step == t]
+
+    def cost(self, x0: dict, traj: dict | None = None) -> float:
+        traj = traj or self.trajectory(x0)
+        jb = sum(float(np.sum(((np.asarray(x0[k]) - self.xb[k])[self._mask[k]] / self.sb[k]) ** 2))
+                 for k in self.names)
+        jo = sum(float(np.sum(((o.sample(traj[o.step]) - o.value) / o.sigma) ** 2)) for o in self.obs)
+        return 0.5 * (jb + jo)
+
+    def _adjoint_sweep(self, traj: dict, forcing) -> dict:
+        """sum_k M_k^T H_k^T forcing(o) over the observations: forcing(o) is the
+        weighted residual of each observation set"""
+        lam = self._zeros()
+        for ti in range(len(self.times) - 1, -1, -1):
+            t = self.times[ti]
+            for o in self._obs_at(t):
+                o.scatter_into(lam, forcing(o))
+            if ti > 0:
+                t0 = self.times[ti - 1]
+                lam = self.m.adjoint(traj[t0], lam, t - t0)
+        return lam
+
+    def gradient(self, x0: dict) -> tuple:
+        """(J, dJ/dx0) with dJ/dx0 zero off the control points"""
+        traj = self.trajectory(x0)
+        lam = self._adjoint_sweep(traj, lambda o: (o.sample(traj[o.step]) - o.value) / o.sigma ** 2)
+        g = {k: np.where(self._mask[k], lam[k] + (np.asarray(x0[k]) - self.xb[k]) / self.sb[k] ** 2,
+                         0.0) for k in self.names}
+        return self.cost(x0, traj), g
+
+    # ---- linearised pieces about a trajectory
+    def _tangent_sweep(self, traj: dict, dx0: dict) -> dict:
+        """H_k M_k dx0 for every observation set (obs id -> values)"""
+        out, dx = {}, dx0
+        for ti, t in enumerate(self.times):
+            if ti > 0:
+                t0 = self.times[ti - 1]
+                dx = self.m.tangent(traj[t0], dx, t - t0)
+            for o in self._obs_at(t):
+                out[id(o)] = o.sample(dx)
+        return out
+
+    def minimise(self, x0: dict | None = None, outer: int = 2, inner: int = 10,
+                 rtol: float = 1e-3) -> Result:
+        """Incremental 4D-Var from x0 (default: the background).  Each inner
+        loop stops after `inner` CG iterations or when the residual falls
+        below rtol times its initial norm."""
+        x = {k: np.asarray((x0 or self.xb)[k], dtype=np.float64).copy() for k in self.names}
+        res = Result(x=x)
+        sbv = self._sb_vec()
+        for _ in range(outer):
+            traj = self.trajectory(x)
+            res.cost.append(self.cost(x, traj))
+            # innovations d_k = y_k - H_k x(t_k); background departure b = x - xb
+            d = {id(o): o.value - o.sample(traj[o.step]) for o in self.obs}
+            bvec = self.pack({k: x[k] - self.xb[k] for k in self.names}) / sbv
+
+            def hess(v):
+                hm = self._tangent_sweep(traj, self.unpack(sbv * v))
+                lam = self._adjoint_sweep(traj, lambda o: hm[id(o)] / o.sigma ** 2)
+                return v + sbv * self.pack(lam)
+
+            # A chi = -b + B^1/2 M^T H^T R^-1 d
+            lam = self._adjoint_sweep(traj, lambda o: d[id(o)] / o.sigma ** 2)
+            rhs = -bvec + sbv * self.pack(lam)
+            chi = np.zeros_like(rhs)
+            r = rhs.copy()
+            p = r.copy()
+            rr = float(r @ r)
+            norms = [np.sqrt(rr)]
+            r0 = norms[0]
+            for _ in range(inner):
+                if r0 == 0 or np.sqrt(rr) <= rtol * r0:
+                    break
+                ap = hess(p)
+                alpha = rr / float(p @ ap)
+                chi += alpha * p
+                r -= alpha * ap
+                rr_new = float(r @ r)
+                norms.append(np.sqrt(rr_new))
+                p = r + (rr_new / rr) * p
+                rr = rr_new
+            res.inner_residual.append(norms)
+            dx = self.unpack(sbv * chi)
+            x = {k: x[k] + dx[k] for k in self.names}
+        res.x = x
+        res.cost.append(self.cost(x))
+        return res
+
+
+# --------------------------------------------------------------- nudging
+def nudge(case, xa: dict, tau: float, width: int = 0, bdy_tau: float | None = None) -> np.ndarray:
+    """Relax the case's forecast toward the analysis xa: BdyManager targets
+    lo = hi = xa for (u, v, theta', pi', qv) (absent fields: 0) and the
+    reference's weights, 1/tau everywhere with the cos^2 Davies ramp of
+    `width` rows and 1/bdy_tau at the open edges.  Returns the weights.
+    ``case.clear_boundary()`` switches the relaxation off again (the tangent-
+    linear and adjoint runs refuse a case that relaxes)."""
+    if not tau > 0:
+        raise ValueError("the nudging time scale must be positive")
+    w = case.bdy_weights(width, bdy_tau if bdy_tau is not None else tau, tau)
+    tg = [np.ascontiguousarray(xa[k], dtype=np.float64) if k in xa else np.zeros(case.shape)
+          for k in BDY_FIELDS]
+    case.set_boundary(tg, tg, w, 0.0, 1.0)
+    return w

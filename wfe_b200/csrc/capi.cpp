@@ -460,6 +460,19 @@ int wfe_set_boundary(wfe_ctx* c, const double* const lo[5], const double* const 
   return c->model->set_boundary(lo, hi, wgt, t_lo, t_hi) ? model_err(c) : WFE_OK;
 }
 
+int wfe_bdy_weights(const wfe_ctx* c, int width, double tau, double nudge_tau, double* out) {
+  if (!c || !out || width < 0 || (width > 0 && !(tau > 0)) || nudge_tau < 0) return WFE_ERR_ARG;
+  std::vector<double> w;
+  bdy_weights(c->cs.g, c->cs.p, width, tau, nudge_tau, &w);
+  std::memcpy(out, w.data(), w.size() * sizeof(double));
+  return WFE_OK;
+}
+
+int wfe_clear_boundary(wfe_ctx* c) {
+  NEED_MODEL(c);
+  return c->model->clear_boundary() ? model_err(c) : WFE_OK;
+}
+
 int wfe_set_physics(wfe_ctx* c, const double* tsk, const double* land, const double* lat,
                     const double* lon, const double* soilw, double start_hour, int doy,
                     int nonlocal) {

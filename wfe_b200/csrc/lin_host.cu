@@ -86,7 +86,7 @@ class LinT final : public Lin {
 
   int tl_run(int nsteps, double dt, double t0) override {
     (void)t0;
-    if (keep_only_state()) return 1;
+    if (check_linearisable() || keep_only_state()) return 1;
     if (dt != dt_) drop_graphs(dt);
     for (int s = 0; s < nsteps; ++s) {
       // one captured graph per rotation phase: [TL kernel, forward launch] per launch
@@ -116,6 +116,7 @@ class LinT final : public Lin {
 
   int ad_run(int nsteps, double dt, double t0, int every) override {
     if (nsteps <= 0) return 0;
+    if (check_linearisable()) return 1;
     if (dt != dt_) drop_graphs(dt);
     if (every < 1 && auto_interval(nsteps, dt, &every)) return 1;
     // the undo log for the longest segment, before any segment graph runs
@@ -588,6 +589,13 @@ class LinT final : public Lin {
   int fail(const std::string& m) {
     err_ = m;
     return 1;
+  }
+
+  // switches turned on after wfe_lin_enable (a boundary relaxation, surface
+  // physics) make the recorded step one the kernels do not linearise
+  int check_linearisable() {
+    std::string why;
+    return m_->linearisable(&why) ? 0 : fail(why);
   }
 
   void release() {

@@ -610,6 +610,14 @@ class ModelT final : public Model {
     return 0;
   }
 
+  int clear_boundary() override {
+    if (!bdy_on_) return 0;
+    bdy_on_ = false;
+    graphs_valid_ = false;
+    ++gen_;
+    return 0;
+  }
+
   int enable_physics(const double* tsk, const double* land, const double* lat, const double* lon,
                      const double* soilw, double start_hour, int doy, bool nonlocal) override {
     // SfcPBL::init (src/physics/surface.cu:440-482); inputs interior ny*nx

@@ -71,6 +71,8 @@ class Model {
   virtual int set_boundary(const double* const lo[5], const double* const hi[5],
                            const double* wgt_padded2d, double t_lo, double t_hi) = 0;
   virtual int set_boundary_hi(const double* const hi[5], double t_lo, double t_hi) = 0;
+  // relaxation off again (targets and weights kept, unused)
+  virtual int clear_boundary() = 0;
   virtual int enable_physics(const double* tsk, const double* land, const double* lat,
                              const double* lon, const double* soilw, double start_hour, int doy,
                              bool nonlocal) = 0;
