@@ -191,21 +191,29 @@ def test_async_snapshot_equals_interior_download(prec):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "bubble_open", "straka_periodic"])
+@pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "bubble_open", "straka_periodic",
+                                  "ops_periodic", "moist_blob"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_tma_column_variant_equals_tile_variants(name, prec, monkeypatch):
-    """The TMA-staged acoustic column kernel (variant 6) computes the same
-    values, bit for bit, as the shared-memory tile kernel (variant 0)."""
+def test_acoustic_variants_are_bit_identical(name, prec, monkeypatch):
+    """The TMA-staged acoustic column kernel (variant 6) and the fused substep
+    kernel that computes its tile's u, v faces itself (variants 7-9: three tile
+    shapes, ragged tiles where nx is no multiple of the tile width) give the
+    same values, bit for bit, as the u, v kernel + shared-memory column tile
+    kernel (variant 0)."""
     out = {}
-    for v in ("0", "6"):
+    for v in ("0", "6", "7", "8", "9"):
         monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
         c = W.Case(CASES / f"{name}.ini", precision=prec)
         for s in range(4):
             c.step(c.dt, s * c.dt)
+        c.run(3, t0=4 * c.dt)
         out[v] = {k: c.field(k) for k in W.FIELDS}
+        kt = c.kernel_times()  # one more step, timed per kernel: which kernels ran
+        assert ("acoustic_fused" in kt) == (v in ("7", "8", "9")), (v, sorted(kt))
         c.close()
-    for k in W.FIELDS:
-        assert np.array_equal(out["0"][k], out["6"][k]), k
+    for v in ("6", "7", "8", "9"):
+        for k in W.FIELDS:
+            assert np.array_equal(out["0"][k], out[v][k]), (v, k)
 
 
 @pytest.mark.gpu

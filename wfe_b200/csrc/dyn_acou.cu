@@ -155,48 +155,106 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
   return a.v_in[c] + a.dtau * (-Phys<R>::cp * thbv * mv * grad + a.tv[c]);
 }
 
+// u (v) at an interior face from the cell values beside it: theta_v and pi*
+// at the face's two cells (kernels.cu:499-526)
+template <typename R>
+__device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
+                                            R ps0, R psx) {
+  const size_t pl = a.L.plane();
+  R thb_f = (R)0.5 * (tvx + tv0);
+  R mf = (R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]);
+  R grad = (ps0 - psx) * a.co.inv_dx;
+  R slope = a.m.hx_u[c2] * a.co.fac_c[kk];
+  if (slope != (R)0) {
+    R jf = (R)0.5 * (a.m.jac[c2 - 1] + a.m.jac[c2]);
+    R dpdz = (R)0.5 *
+             ((pistar_at(a, c - 1 + pl) - pistar_at(a, c - 1 - pl)) +
+              (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
+             a.co.inv_dzc2[kk];
+    grad -= slope / jf * dpdz;
+  }
+  return a.u_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tu[c]);
+}
+
+template <typename R>
+__device__ __forceinline__ R v_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
+                                            R ps0, R psy) {
+  const size_t sy = a.L.px, pl = a.L.plane();
+  R thb_f = (R)0.5 * (tvy + tv0);
+  R mf = (R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]);
+  R grad = (ps0 - psy) * a.co.inv_dy;
+  R slope = a.m.hy_v[c2] * a.co.fac_c[kk];
+  if (slope != (R)0) {
+    R jf = (R)0.5 * (a.m.jac[c2 - sy] + a.m.jac[c2]);
+    R dpdz = (R)0.5 *
+             ((pistar_at(a, c - sy + pl) - pistar_at(a, c - sy - pl)) +
+              (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
+             a.co.inv_dzc2[kk];
+    grad -= slope / jf * dpdz;
+  }
+  return a.v_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tv[c]);
+}
+
 // Both faces of an interior point: the cell values at (i,j), (i-1,j) and
-// (i,j-1) are computed once for the u and the v face (kernels.cu:499-526).
+// (i,j-1) are loaded once for the u and the v face.
 template <typename R>
 __device__ __forceinline__ void uv_pair_interior(const AcouArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
   const size_t c = L.at(i, j, k), c2 = L.at2(i, j);
-  const size_t sy = L.px, pl = L.plane();
+  const size_t sy = L.px;
   const R tv0 = theta_v_at(a, c), tvx = theta_v_at(a, c - 1), tvy = theta_v_at(a, c - sy);
   const R ps0 = pistar_at(a, c), psx = pistar_at(a, c - 1), psy = pistar_at(a, c - sy);
-  const R m0 = a.m.mapf[c2];
-  const R fc = a.co.fac_c[kk];
-  {
-    R thb_f = (R)0.5 * (tvx + tv0);
-    R mf = (R)0.5 * (a.m.mapf[c2 - 1] + m0);
-    R grad = (ps0 - psx) * a.co.inv_dx;
-    R slope = a.m.hx_u[c2] * fc;
-    if (slope != (R)0) {
-      R jf = (R)0.5 * (a.m.jac[c2 - 1] + a.m.jac[c2]);
-      R dpdz = (R)0.5 *
-               ((pistar_at(a, c - 1 + pl) - pistar_at(a, c - 1 - pl)) +
-                (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
-               a.co.inv_dzc2[kk];
-      grad -= slope / jf * dpdz;
+  a.u_out[c] = u_interior_val(a, c, c2, kk, tv0, tvx, ps0, psx);
+  a.v_out[c] = v_interior_val(a, c, c2, kk, tv0, tvy, ps0, psy);
+}
+
+// u on an x face (0..nx) of a row j < ny that is not an interior point:
+// radiation faces (open) or the periodic face u(nx) = u(0)
+template <typename R>
+__device__ __forceinline__ R u_face_edge(const AcouArgs<R>& a, int i, int j, int k) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const R cstar = a.p.cstar;
+  if (a.p.bc_x_open) {
+    if (i == 0) {  // kernels.cu:654-660
+      R u0 = a.u_in[L.at(0, j, k)];
+      if (u0 >= (R)0) return a.b.ub[kk];
+      R cb = u0 - cstar;
+      return u0 - a.dtau * cb * (u_forward(a, 1, j, k) - u0) / a.dx;
     }
-    a.u_out[c] = a.u_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tu[c]);
-  }
-  {
-    R thb_f = (R)0.5 * (tvy + tv0);
-    R mf = (R)0.5 * (a.m.mapf[c2 - sy] + m0);
-    R grad = (ps0 - psy) * a.co.inv_dy;
-    R slope = a.m.hy_v[c2] * fc;
-    if (slope != (R)0) {
-      R jf = (R)0.5 * (a.m.jac[c2 - sy] + a.m.jac[c2]);
-      R dpdz = (R)0.5 *
-               ((pistar_at(a, c - sy + pl) - pistar_at(a, c - sy - pl)) +
-                (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
-               a.co.inv_dzc2[kk];
-      grad -= slope / jf * dpdz;
+    if (i == L.nx) {  // kernels.cu:661-667
+      R un = a.u_in[L.at(L.nx, j, k)];
+      if (un <= (R)0) return a.b.ub[kk];
+      R cb = un + cstar;
+      return un - a.dtau * cb * (un - u_forward(a, L.nx - 1, j, k)) / a.dx;
     }
-    a.v_out[c] = a.v_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tv[c]);
+    return u_forward(a, i, j, k);
   }
+  return u_forward(a, i == L.nx ? 0 : i, j, k);  // periodic face u(nx) = u(0)
+}
+
+// v on a y face (0..ny) of a column i < nx that is not an interior point
+template <typename R>
+__device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int k) {
+  const Layout& L = a.L;
+  const R cstar = a.p.cstar;
+  if (a.p.bc_y_open) {
+    if (j == 0) {  // kernels.cu:674-680
+      R v0 = a.v_in[L.at(i, 0, k)];
+      if (v0 >= (R)0) return 0;
+      R cb = v0 - cstar;
+      return v0 - a.dtau * cb * (v_forward(a, i, 1, k) - v0) / a.dy;
+    }
+    if (j == L.ny) {  // kernels.cu:681-687
+      R vn = a.v_in[L.at(i, L.ny, k)];
+      if (vn <= (R)0) return 0;
+      R cb = vn + cstar;
+      return vn - a.dtau * cb * (vn - v_forward(a, i, L.ny - 1, k)) / a.dy;
+    }
+    return v_forward(a, i, j, k);
+  }
+  return v_forward(a, i, j == L.ny ? 0 : j, k);
 }
 
 template <typename R>
@@ -206,62 +264,36 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   const int j = by * blockDim.y + threadIdx.y;
   const int k = bz * blockDim.z + threadIdx.z;
   if (i > L.nx || j > L.ny || k >= L.nz) return;
-  if (i >= 1 && i < L.nx && j >= 1 && j < L.ny && k >= 1 && k < L.nz - 1) {
+  if (uv_interior<R>(L, i, j, k)) {
     uv_pair_interior(a, i, j, k);
     return;
   }
-  const int kk = L.at1(k);
-  const R cstar = a.p.cstar;
-  if (j < L.ny) {  // u on x faces 0..nx
-    R out;
-    if (a.p.bc_x_open) {
-      if (i == 0) {  // kernels.cu:654-660
-        R u0 = a.u_in[L.at(0, j, k)];
-        if (u0 >= (R)0) out = a.b.ub[kk];
-        else {
-          R cb = u0 - cstar;
-          out = u0 - a.dtau * cb * (u_forward(a, 1, j, k) - u0) / a.dx;
-        }
-      } else if (i == L.nx) {  // kernels.cu:661-667
-        R un = a.u_in[L.at(L.nx, j, k)];
-        if (un <= (R)0) out = a.b.ub[kk];
-        else {
-          R cb = un + cstar;
-          out = un - a.dtau * cb * (un - u_forward(a, L.nx - 1, j, k)) / a.dx;
-        }
-      } else {
-        out = u_forward(a, i, j, k);
-      }
-    } else {
-      out = u_forward(a, i == L.nx ? 0 : i, j, k);  // periodic face u(nx) = u(0)
-    }
-    a.u_out[L.at(i, j, k)] = out;
+  if (j < L.ny) a.u_out[L.at(i, j, k)] = u_face_edge(a, i, j, k);
+  if (i < L.nx) a.v_out[L.at(i, j, k)] = v_face_edge(a, i, j, k);
+}
+
+// One face with uv_body's arithmetic (the fused substep kernel computes a
+// tile's faces itself)
+template <typename R>
+__device__ __forceinline__ R u_face(const AcouArgs<R>& a, int i, int j, int k) {
+  const Layout& L = a.L;
+  if (uv_interior<R>(L, i, j, k)) {
+    const size_t c = L.at(i, j, k);
+    return u_interior_val(a, c, L.at2(i, j), L.at1(k), theta_v_at(a, c), theta_v_at(a, c - 1),
+                          pistar_at(a, c), pistar_at(a, c - 1));
   }
-  if (i < L.nx) {  // v on y faces 0..ny
-    R out;
-    if (a.p.bc_y_open) {
-      if (j == 0) {  // kernels.cu:674-680
-        R v0 = a.v_in[L.at(i, 0, k)];
-        if (v0 >= (R)0) out = 0;
-        else {
-          R cb = v0 - cstar;
-          out = v0 - a.dtau * cb * (v_forward(a, i, 1, k) - v0) / a.dy;
-        }
-      } else if (j == L.ny) {  // kernels.cu:681-687
-        R vn = a.v_in[L.at(i, L.ny, k)];
-        if (vn <= (R)0) out = 0;
-        else {
-          R cb = vn + cstar;
-          out = vn - a.dtau * cb * (vn - v_forward(a, i, L.ny - 1, k)) / a.dy;
-        }
-      } else {
-        out = v_forward(a, i, j, k);
-      }
-    } else {
-      out = v_forward(a, i, j == L.ny ? 0 : j, k);
-    }
-    a.v_out[L.at(i, j, k)] = out;
+  return u_face_edge(a, i, j, k);
+}
+
+template <typename R>
+__device__ __forceinline__ R v_face(const AcouArgs<R>& a, int i, int j, int k) {
+  const Layout& L = a.L;
+  if (uv_interior<R>(L, i, j, k)) {
+    const size_t c = L.at(i, j, k), sy = L.px;
+    return v_interior_val(a, c, L.at2(i, j), L.at1(k), theta_v_at(a, c), theta_v_at(a, c - sy),
+                          pistar_at(a, c), pistar_at(a, c - sy));
   }
+  return v_face_edge(a, i, j, k);
 }
 
 // FP32: 32 registers, eight CTAs per SM -- the kernel waits on loads, and the
@@ -291,12 +323,33 @@ struct ColSmem {
   }
 };
 
-template <typename R, int CX, int KL>
-__device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// Where a column reads the new u, v: the substep's output fields, or the
+// fused kernel's shared tiles.  u_at(k, 0|1): the column's west | east face
+// at level k; v_at(k, 0|1): its south | north face.
+template <typename R>
+struct UvGlobal {
+  const R* __restrict__ u;
+  const R* __restrict__ v;
+  size_t c0, pl, sy;
+  __device__ R u_at(int k, int dx) const { return u[c0 + (size_t)k * pl + dx]; }
+  __device__ R v_at(int k, int dy) const { return v[c0 + (size_t)k * pl + (size_t)dy * sy]; }
+};
+
+// tiles: us[k * (CX + 1) + face], vs[(k * 2 + row) * CX + column]
+template <typename R, int CX>
+struct UvTile {
+  const R* us;
+  const R* vs;
+  int tx;
+  __device__ R u_at(int k, int dx) const { return us[k * (CX + 1) + tx + dx]; }
+  __device__ R v_at(int k, int dy) const { return vs[(k * 2 + dy) * CX + tx]; }
+};
+
+template <typename R, int CX, int KL, typename UV>
+__device__ __forceinline__ void column_core(const AcouArgs<R>& a, int bx, int by, R* smem, const UV& uv) {
   const Layout& L = a.L;
   const int nz = L.nz;
-  ColSmem<R, CX> S(reinterpret_cast<R*>(smem_raw), nz + 1);
+  ColSmem<R, CX> S(smem, nz + 1);
   const int tx = threadIdx.x;           // column within the CTA
   const int lane_k = threadIdx.y;       // level lane
   const int i = bx * CX + tx;
@@ -310,8 +363,6 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
   const R invJ = (R)1 / J;
   const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
   const bool terrain = hxc != (R)0 || hyc != (R)0;
-  const R* __restrict__ u = a.u_out;
-  const R* __restrict__ v = a.v_out;
   const size_t sx = 1, sy = L.px, pl = L.plane();
   const size_t c0 = L.at(active ? i : 0, j, 0);  // level k at c0 + k * pl
 #define SM(X, k) S.X[(size_t)(k) * CX + tx]
@@ -326,8 +377,8 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
         const size_t c = c0 + (size_t)k * pl, cm = c - pl;
         av = a.co.aw[c];
         if (terrain) {
-          R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
-          R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+          R uw = (R)0.25 * (uv.u_at(k - 1, 0) + uv.u_at(k - 1, 1) + uv.u_at(k, 0) + uv.u_at(k, 1));
+          R vw = (R)0.25 * (uv.v_at(k - 1, 0) + uv.v_at(k - 1, 1) + uv.v_at(k, 0) + uv.v_at(k, 1));
           sv = av * (uw * hxc + vw * hyc) * a.co.fac_w[L.at1(k)];
         }
       }
@@ -342,8 +393,8 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
       const int kk = L.at1(k);
       const size_t c = c0 + (size_t)k * pl;
       R Kt = a.co.kt3[c];
-      R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * mcx +
-             (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * mcy;
+      R Dh = (a.co.rtjx[c + sx] * uv.u_at(k, 1) - a.co.rtjx[c] * uv.u_at(k, 0)) * mcx +
+             (a.co.rtjy[c + sy] * uv.v_at(k, 1) - a.co.rtjy[c] * uv.v_at(k, 0)) * mcy;
       R idz = a.co.inv_dzc[kk];
       R wk = a.w_in[c], wkp = a.w_in[c + pl];
       R tpi = a.tpi ? a.tpi[c] : (R)0;
@@ -418,8 +469,8 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
       SM(Wn, k) = wk;
       wabove = wk;
     }
-    R us = (R)0.5 * (u[c0] + u[c0 + sx]);
-    R vs = (R)0.5 * (v[c0] + v[c0 + sy]);
+    R us = (R)0.5 * (uv.u_at(0, 0) + uv.u_at(0, 1));
+    R vs = (R)0.5 * (uv.v_at(0, 0) + uv.v_at(0, 1));
     SM(Wn, 0) = us * hxc + vs * hyc;
   }
   __syncthreads();
@@ -442,8 +493,58 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
 }
 
 template <typename R, int CX, int KL>
+__device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Layout& L = a.L;
+  const int i = bx * CX + (int)threadIdx.x;
+  const UvGlobal<R> uv{a.u_out, a.v_out, L.at(i < L.nx ? i : 0, by, 0), L.plane(), (size_t)L.px};
+  column_core<R, CX, KL>(a, bx, by, reinterpret_cast<R*>(smem_raw), uv);
+}
+
+template <typename R, int CX, int KL>
 __global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
   column_body<R, CX, KL>(a, blockIdx.x, blockIdx.y);
+}
+
+// The whole substep in one launch: a CTA first computes the u faces
+// i0..i0+CX of its row and the v faces of rows j and j+1 of its columns with
+// uv_body's arithmetic into shared tiles (storing the faces it owns: u faces
+// of its columns and u(nx), v faces of row j and v(ny)), then solves its
+// columns from the tiles.  A face beside the tile is computed by both CTAs
+// that need it.  Every CTA reads theta' and pi' of neighbouring columns that
+// other CTAs update in the same launch, so the integrator gives this kernel
+// distinct theta'_in / theta'_out buffers (pi' and u, v already are).
+template <typename R, int CX, int KL>
+__global__ void __launch_bounds__(CX * KL) k_acoustic_fused(AcouArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Layout& L = a.L;
+  const int nz = L.nz;
+  R* cols = reinterpret_cast<R*>(smem_raw);
+  R* us = cols + (size_t)9 * (nz + 1) * CX;
+  R* vs = us + (size_t)nz * (CX + 1);
+  const int i0 = blockIdx.x * CX, j = blockIdx.y;
+  const int tid = threadIdx.y * CX + threadIdx.x;
+  const int nu = (CX + 1) * nz, nv = 2 * CX * nz;
+  for (int e = tid; e < nu + nv; e += CX * KL) {
+    if (e < nu) {
+      const int f = e % (CX + 1), k = e / (CX + 1), i = i0 + f;
+      if (i <= L.nx) {
+        const R val = u_face(a, i, j, k);
+        us[e] = val;
+        if (f < CX || i == L.nx) a.u_out[L.at(i, j, k)] = val;
+      }
+    } else {
+      const int e2 = e - nu, col = e2 % CX, row = (e2 / CX) & 1, k = e2 / (2 * CX);
+      const int i = i0 + col, jj = j + row;
+      if (i < L.nx) {
+        const R val = v_face(a, i, jj, k);
+        vs[e2] = val;
+        if (row == 0 || jj == L.ny) a.v_out[L.at(i, jj, k)] = val;
+      }
+    }
+  }
+  __syncthreads();
+  column_core<R, CX, KL>(a, blockIdx.x, j, cols, UvTile<R, CX>{us, vs, (int)threadIdx.x});
 }
 // the shared column arrays are reused by the next work item only after the
 // barrier that opens it
@@ -820,6 +921,65 @@ int batch_column(const Batch<AcouArgs<R>>& b, int shape, int nz_max, int nblocks
   return 0;
 }
 
+// Tile shapes of the fused substep kernel (indices into kColumnShapes)
+static const int kFusedShapes[] = {0, 4, 1};
+constexpr int kNumFusedShapes = 3;
+
+int acoustic_fused_shapes() { return kNumFusedShapes; }
+
+template <typename R>
+size_t fused_smem(int nz, int cx) {
+  return column_smem<R>(nz, cx) + ((size_t)nz * (cx + 1) + (size_t)2 * cx * nz) * sizeof(R);
+}
+
+template <typename R>
+static bool fused_fits(int nz, int f) {
+  return f >= 0 && f < kNumFusedShapes && fused_smem<R>(nz, kColumnShapes[kFusedShapes[f]][0]) <= 200 * 1024;
+}
+
+template <typename R>
+bool acoustic_fused_fits(int nz, int f) {
+  return fused_fits<R>(nz, f);
+}
+
+template <typename R>
+int prepare_acoustic_fused(int nz) {
+  for (int f = 0; f < kNumFusedShapes; ++f) {
+    if (!fused_fits<R>(nz, f)) continue;
+    const int sm = (int)fused_smem<R>(nz, kColumnShapes[kFusedShapes[f]][0]);
+    cudaError_t e;
+    switch (kFusedShapes[f]) {
+      case 0: e = cudaFuncSetAttribute(k_acoustic_fused<R, 32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      case 4: e = cudaFuncSetAttribute(k_acoustic_fused<R, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      default: e = cudaFuncSetAttribute(k_acoustic_fused<R, 16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+    }
+    if (e != cudaSuccess) return 1;
+  }
+  return 0;
+}
+
+// f: index into the fused tile shapes.  Returns 0 ok, 2 the column does not fit.
+template <typename R>
+int launch_acoustic_fused(const AcouArgs<R>& a, int f, cudaStream_t st) {
+  const int nz = a.L.nz;
+  if (!fused_fits<R>(nz, f)) return 2;
+  const int shape = kFusedShapes[f];
+  const int cx = kColumnShapes[shape][0], kl = kColumnShapes[shape][1];
+  const size_t sm = fused_smem<R>(nz, cx);
+  const dim3 grd((a.L.nx + cx - 1) / cx, a.L.ny, 1), blk(cx, kl);
+  switch (shape) {
+    case 0: k_acoustic_fused<R, 32, 8><<<grd, blk, sm, st>>>(a); break;
+    case 4: k_acoustic_fused<R, 16, 8><<<grd, blk, sm, st>>>(a); break;
+    default: k_acoustic_fused<R, 16, 16><<<grd, blk, sm, st>>>(a); break;
+  }
+  return 0;
+}
+
+// the plain column tile shape of fused shape f
+int acoustic_fused_column_shape(int f) {
+  return (f >= 0 && f < kNumFusedShapes) ? kFusedShapes[f] : 0;
+}
+
 template <typename R>
 int occupancy_column(int shape, int nz_max) {
   if (shape < 0 || shape >= kNumColumnShapes || !column_fits<R>(nz_max, shape)) return 1;
@@ -852,7 +1012,10 @@ int occupancy_column(int shape, int nz_max) {
                                         R*, R*, R*, R*, cudaStream_t);                         \
   template void launch_acoustic_uv<R>(const AcouArgs<R>&, cudaStream_t);                       \
   template int launch_acoustic_column<R>(const AcouArgs<R>&, int, cudaStream_t);               \
-  template int prepare_acoustic_column<R>(int);
+  template int prepare_acoustic_column<R>(int);                                                 \
+  template bool acoustic_fused_fits<R>(int, int);                                              \
+  template int prepare_acoustic_fused<R>(int);                                                 \
+  template int launch_acoustic_fused<R>(const AcouArgs<R>&, int, cudaStream_t);
 WFE_INST(float)
 WFE_INST(double)
 #undef WFE_INST

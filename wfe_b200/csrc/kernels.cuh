@@ -351,6 +351,17 @@ int launch_acoustic_column_tma(const TmaColParams<R>& p, cudaStream_t st);
 template <typename R>
 int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st);
 int acoustic_column_shapes();
+// The fused substep kernel (u, v faces of the tile, then its columns), in
+// acoustic_fused_shapes() tile shapes; theta'_in and theta'_out must be
+// distinct buffers (pi', u and v always are).  Returns 0 ok, 2 too deep.
+template <typename R>
+int launch_acoustic_fused(const AcouArgs<R>& a, int f, cudaStream_t st);
+int acoustic_fused_shapes();
+int acoustic_fused_column_shape(int f);
+template <typename R>
+bool acoustic_fused_fits(int nz, int f);
+template <typename R>
+int prepare_acoustic_fused(int nz);
 // whether tile shape `shape` holds a column of nz levels in shared memory
 template <typename R>
 bool acoustic_column_fits(int nz, int shape);

@@ -125,6 +125,7 @@ class ModelT final : public Model {
     if (prepare_acoustic_column<R>(g_.nz) || prepare_kessler<R>(g_.nz))
       return fail("nz too large for the column kernels' shared memory");
     tma_ok_ = tensor_map_encoder() && prepare_acoustic_column_tma<R>(g_.nz) == 0;
+    fused_ok_ = prepare_acoustic_fused<R>(g_.nz) == 0;
     tend_tma_ok_ = tensor_map_encoder() && tend_scal_tma_smem<R>() <= 227 * 1024 &&
                    prepare_tend_scal_tma<R>() == 0;
     CK(cudaMalloc(&tma_err_, sizeof(unsigned)));
@@ -180,7 +181,7 @@ class ModelT final : public Model {
         if (!(S_[s][f] = alloc(n3))) return 1;
     for (int f = 0; f < 8; ++f)
       if (!(T_[f] = alloc(n3))) return 1;
-    for (R** p : {&mfx_, &mfy_, &mfz_, &U2_, &V2_, &P1_, &P2_})
+    for (R** p : {&mfx_, &mfy_, &mfz_, &U2_, &V2_, &P1_, &P2_, &TH2_})
       if (!(*p = alloc(n3))) return 1;
     if (hp_.pd_moist)
       for (int s = 0; s < 3; ++s)
@@ -720,7 +721,16 @@ class ModelT final : public Model {
     return (field >= 0 && field < 8) ? S_[perm_[0]][field] : nullptr;
   }
   void* stream_handle() const override { return st_; }
-  int column_shape() const override { return tune_.column_cx; }
+  // the plain column tile shape of the variant in use (the linearised runs
+  // launch the unfused kernels)
+  int column_shape() const override {
+    const int f = tune_.column_cx - acoustic_column_shapes() - 1;
+    return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
+  }
+  bool fused_usable(int v) const {
+    const int f = v - acoustic_column_shapes() - 1;
+    return fused_ok_ && f >= 0 && f < acoustic_fused_shapes() && acoustic_fused_fits<R>(g_.nz, f);
+  }
   void set_lin_map(std::function<void*(const void*)> map) override { lin_map_ = std::move(map); }
   bool linearisable(std::string* why) const override {
     if (dp_.moisture && dp_.pd_moist) *why = "the positive-definite moisture limiter is not linearised";
@@ -757,7 +767,7 @@ class ModelT final : public Model {
     std::string name = prop.name;
     for (char& ch : name)
       if (ch == ' ') ch = '_';
-    k << "v4|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
+    k << "v5|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
       << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0);
     return k.str();
   }
@@ -782,8 +792,9 @@ class ModelT final : public Model {
     return 0;
   }
 
-  // WFE_COLUMN_VARIANT=<n> forces the acoustic column variant (0..5 tile
-  // shapes, 6 the TMA-staged kernel) and WFE_TEND_VARIANT=<n> the tendency
+  // WFE_COLUMN_VARIANT=<n> forces the acoustic variant (0..5 column tile
+  // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
+  // tile shapes) and WFE_TEND_VARIANT=<n> the tendency
   // variant (0 fused, 1 split, 2 momentum + TMA-staged scalars) after tuning,
   // for tests and experiments
   int autotune(double dt) {
@@ -792,7 +803,8 @@ class ModelT final : public Model {
     const char* cv = std::getenv("WFE_COLUMN_VARIANT");
     if (first && cv && *cv) {
       const int v = std::atoi(cv);
-      if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_)))
+      if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_) ||
+                     fused_usable(v)))
         tune_.column_cx = v;
     }
     const char* tv = std::getenv("WFE_TEND_VARIANT");
@@ -832,8 +844,11 @@ class ModelT final : public Model {
     }
     best = 1e30f;
     const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
-    const int nvar = acoustic_column_shapes() + (tma_ok_ ? 1 : 0);  // last: TMA-staged
+    // tile shapes, the TMA-staged column, the fused substep kernels
+    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes();
     for (int cx = 0; cx < nvar; ++cx) {
+      if (cx == acoustic_column_shapes() && !tma_ok_) continue;
+      if (cx > acoustic_column_shapes() && !fused_usable(cx)) continue;
       float ms;
       tune_.column_cx = cx;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -1010,23 +1025,35 @@ class ModelT final : public Model {
     };
     const R* uin = N[0];
     const R* vin = N[1];
+    // the fused kernel reads theta' of neighbouring columns that other CTAs
+    // update: theta' alternates between X and a second buffer like u, v (the
+    // last substep writes X); recorded launches keep the two-kernel form
+    const bool fuse = !rec_ && fused_usable(tune_.column_cx);
+    const R* thin = N[3];
     for (int t = 0; t < ns; ++t) {
-      R* uout = ((ns - 1 - t) % 2 == 0) ? X[0] : U2_;
-      R* vout = ((ns - 1 - t) % 2 == 0) ? X[1] : V2_;
+      const bool last_parity = (ns - 1 - t) % 2 == 0;
+      R* uout = last_parity ? X[0] : U2_;
+      R* vout = last_parity ? X[1] : V2_;
+      R* thout = (fuse && !last_parity) ? TH2_ : X[3];
       a.u_in = uin;
       a.v_in = vin;
       a.u_out = uout;
       a.v_out = vout;
       a.w_in = t == 0 ? N[2] : X[2];
       a.w_out = X[2];
-      a.th_in = t == 0 ? N[3] : X[3];
-      a.th_out = X[3];
+      a.th_in = thin;
+      a.th_out = thout;
       a.pi_prev = pbuf(t - 1);
       a.pi_cur = pbuf(t);
       a.pi_next = pbuf(t + 1);
       int rc = 0;
-      if (!record(K_UV, a)) launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
-      if (!record(K_COL, a)) {
+      if (fuse) {
+        const int f = tune_.column_cx - acoustic_column_shapes() - 1;
+        launch("acoustic_fused", [&] { rc = launch_acoustic_fused<R>(a, f, st_); });
+      } else if (!record(K_UV, a)) {
+        launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
+      }
+      if (!fuse && !record(K_COL, a)) {
         if (tma_ok_ && tune_.column_cx == acoustic_column_shapes()) {
           TmaColParams<R> tp;
           if (tma_params(a, &tp)) return 1;
@@ -1038,6 +1065,7 @@ class ModelT final : public Model {
       if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
       uin = uout;
       vin = vout;
+      thin = thout;
       piprev_ = const_cast<R*>(a.pi_cur);
     }
     return 0;
@@ -1336,7 +1364,7 @@ class ModelT final : public Model {
   R* S_[3][8] = {};
   R* T_[8] = {};
   R *mfx_ = nullptr, *mfy_ = nullptr, *mfz_ = nullptr;
-  R *U2_ = nullptr, *V2_ = nullptr, *P1_ = nullptr, *P2_ = nullptr;
+  R *U2_ = nullptr, *V2_ = nullptr, *P1_ = nullptr, *P2_ = nullptr, *TH2_ = nullptr;
   R* ratio_[3] = {};
   R *rtjx_ = nullptr, *rtjy_ = nullptr, *kt3_ = nullptr, *aw_ = nullptr;
   R* rain_ = nullptr;
@@ -1363,6 +1391,7 @@ class ModelT final : public Model {
   long gen_ = 0;  // changes whenever buffer roles or physics switches change
   std::vector<Rec>* rec_ = nullptr;  // record mode when set
   bool tma_ok_ = false;              // TMA column variant usable
+  bool fused_ok_ = false;            // fused substep kernels prepared
   bool tend_tma_ok_ = false;         // TMA-staged scalar tendencies usable
   unsigned* tma_err_ = nullptr;      // set by a TMA tile load that timed out
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps_;
