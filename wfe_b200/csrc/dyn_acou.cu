@@ -506,6 +506,180 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column(AcouArgs<R> a) {
   column_body<R, CX, KL>(a, blockIdx.x, blockIdx.y);
 }
 
+// Column variant with contiguous level chunks: level lane l owns levels
+// l*ch .. l*ch+ch-1 (ch = ceil((nz+1)/KL)) and runs phases 1-3 of column_core
+// for them in registers without barriers, recomputing Av, Sv, P and E of the
+// level below its chunk (its first row needs them) and Av, Sv of the level
+// above; it loads phase 5's inputs before the sweep, so their latency
+// overlaps it, and keeps theta' of its levels.  Only the rows A, B, C, D and
+// the solution pass through shared memory (two barriers instead of four).
+// The same expressions on the same values as column_core: bit-identical.
+// KCH: the largest chunk (nz + 1 <= KL * KCH).
+template <typename R, int CX, int KL, int KCH>
+__global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Layout& L = a.L;
+  const int nz = L.nz;
+  const size_t n1 = (size_t)(nz + 1) * CX;
+  R* sA = reinterpret_cast<R*>(smem_raw);
+  R* sB = sA + n1;
+  R* sC = sB + n1;
+  R* sD = sC + n1;
+  R* sW = sD + n1;
+  const int tx = threadIdx.x, lane = threadIdx.y;
+  const int i = blockIdx.x * CX + tx, j = blockIdx.y;
+  const bool active = i < L.nx;
+  const R dtau = a.dtau;
+  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
+  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
+  const size_t c2d = L.at2(active ? i : 0, j);
+  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
+  const R invJ = (R)1 / J;
+  const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
+  const bool terrain = hxc != (R)0 || hyc != (R)0;
+  const size_t sx = 1, sy = L.px, pl = L.plane();
+  const size_t c0 = L.at(active ? i : 0, j, 0);
+  const R* __restrict__ u = a.u_out;
+  const R* __restrict__ v = a.v_out;
+  const int ch = (nz + KL) / KL;
+  const int klo = lane * ch;  // first level of the chunk; s = k - klo + 1
+  R av[KCH + 2], sv[KCH + 2], P[KCH + 1], E[KCH + 1], th[KCH + 1], tt[KCH + 1], db[KCH + 1];
+#define SQ(X, k) X[(size_t)(k) * CX + tx]
+  if (active) {
+    // phase 1 on levels klo-1 .. klo+ch
+#pragma unroll
+    for (int s = 0; s < KCH + 2; ++s) {
+      const int k = klo - 1 + s;
+      R avk = 0, svk = 0;
+      if (s <= ch + 1 && k >= 1 && k < nz) {
+        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        avk = a.co.aw[c];
+        if (terrain) {
+          R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+          R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+          svk = avk * (uw * hxc + vw * hyc) * a.co.fac_w[L.at1(k)];
+        }
+      }
+      av[s] = avk;
+      sv[s] = svk;
+    }
+    // phase 2 on levels klo-1 .. klo+ch-1
+#pragma unroll
+    for (int s = 0; s < KCH + 1; ++s) {
+      const int k = klo - 1 + s;
+      R pk = 0, ek = 0;
+      if (s <= ch && k >= 0 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = c0 + (size_t)k * pl;
+        R Kt = a.co.kt3[c];
+        R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * mcx +
+               (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * mcy;
+        R idz = a.co.inv_dzc[kk];
+        R wk = a.w_in[c], wkp = a.w_in[c + pl];
+        R tpi = a.tpi ? a.tpi[c] : (R)0;
+        pk = a.pi_cur[c] + dtau * tpi -
+             dtau * Kt * (Dh - (sv[s + 1] - sv[s]) * idz + c2 * (av[s + 1] * wkp - av[s] * wk) * idz);
+        ek = dtau * Kt * c1 * idz;
+      }
+      P[s] = pk;
+      E[s] = ek;
+    }
+    // phase 3 on the inner levels of the chunk, and phase 5's inputs
+#pragma unroll
+    for (int s = 1; s < KCH + 1; ++s) {
+      const int k = klo - 1 + s;
+      if (s <= ch && k < nz) {
+        const size_t c = c0 + (size_t)k * pl;
+        th[s] = a.th_in[c];
+        tt[s] = a.tth[c];
+        db[s] = a.b.dthbdz[c];
+      }
+      if (s <= ch && k >= 1 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const R iJdz = invJ * a.co.inv_dzw[kk];
+        R thc = th[s], thm = a.th_in[cm];
+        R thbw = a.b.thbw[c];
+        R thvw = thbw + (R)0.5 * (thm + thc);
+        if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
+        R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
+        R Em = E[s - 1], Ek = E[s];
+        SQ(sA, k) = -G * Em * av[s - 1];
+        SQ(sB, k) = (R)1 + G * av[s] * (Ek + Em);
+        SQ(sC, k) = -G * Ek * av[s + 1];
+        R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
+        if (a.p.moisture) {
+          R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
+          R qcr = (R)0.5 * (a.qc[cm] + a.qc[c]) + (R)0.5 * (a.qr[cm] + a.qr[c]);
+          buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
+        }
+        R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
+                dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) * iJdz;
+        SQ(sD, k) = RHS - G * (P[s] - P[s - 1]);
+      }
+    }
+  }
+  __syncthreads();
+  // phase 4: the Thomas sweep of column_core
+  if (active && lane == 0) {
+    R cprev = 0, dprev = 0;
+    R Ak = SQ(sA, 1), Bk = SQ(sB, 1), Ck = SQ(sC, 1), Dk = SQ(sD, 1);
+    for (int k = 1; k < nz; ++k) {
+      R An = 0, Bn = 1, Cn = 0, Dn = 0;
+      if (k + 1 < nz) {
+        An = SQ(sA, k + 1);
+        Bn = SQ(sB, k + 1);
+        Cn = SQ(sC, k + 1);
+        Dn = SQ(sD, k + 1);
+      }
+      R r, ck, dk;
+      if (k == 1) {
+        r = (R)1 / Bk;
+        ck = Ck * r;
+        dk = Dk * r;
+      } else {
+        r = (R)1 / (Bk - Ak * cprev);
+        ck = Ck * r;
+        dk = (Dk - Ak * dprev) * r;
+      }
+      SQ(sC, k) = ck;
+      SQ(sD, k) = dk;
+      cprev = ck;
+      dprev = dk;
+      Ak = An, Bk = Bn, Ck = Cn, Dk = Dn;
+    }
+    SQ(sW, nz) = 0;
+    R wabove = 0;
+    for (int k = nz - 1; k >= 1; --k) {
+      R wk = SQ(sD, k) - SQ(sC, k) * wabove;
+      SQ(sW, k) = wk;
+      wabove = wk;
+    }
+    R us = (R)0.5 * (u[c0] + u[c0 + sx]);
+    R vs = (R)0.5 * (v[c0] + v[c0 + sy]);
+    SQ(sW, 0) = us * hxc + vs * hyc;
+  }
+  __syncthreads();
+  // phase 5 on the chunk's levels
+  if (active)
+#pragma unroll
+    for (int s = 1; s < KCH + 1; ++s) {
+      const int k = klo - 1 + s;
+      if (s > ch || k > nz) continue;
+      const size_t c = c0 + (size_t)k * pl;
+      if (k < nz) {
+        R wn = SQ(sW, k), wn1 = SQ(sW, k + 1);
+        a.pi_next[c] = P[s] - E[s] * (av[s + 1] * wn1 - av[s] * wn);
+        R wc = (R)0.5 * (wn + wn1);
+        a.th_out[c] = th[s] + dtau * (tt[s] - wc * db[s]);
+        a.w_out[c] = wn;
+      } else {
+        a.w_out[c] = 0;
+      }
+    }
+#undef SQ
+}
+
 // The whole substep in one launch: a CTA first computes the u faces
 // i0..i0+CX of its row and the v faces of rows j and j+1 of its columns with
 // uv_body's arithmetic into shared tiles (storing the faces it owns: u faces
@@ -975,6 +1149,39 @@ int launch_acoustic_fused(const AcouArgs<R>& a, int f, cudaStream_t st) {
   return 0;
 }
 
+// Shapes of the chunked column kernel: columns, level lanes, largest chunk
+static const int kChunkShapes[][3] = {{32, 8, 8}, {16, 16, 4}, {32, 16, 4}};
+constexpr int kNumChunkShapes = 3;
+
+int acoustic_chunked_shapes() { return kNumChunkShapes; }
+
+template <typename R>
+size_t chunked_smem(int nz, int cx) {
+  return (size_t)5 * (nz + 1) * cx * sizeof(R);
+}
+
+template <typename R>
+bool acoustic_chunked_fits(int nz, int f) {
+  return f >= 0 && f < kNumChunkShapes && nz + 1 <= kChunkShapes[f][1] * kChunkShapes[f][2] &&
+         chunked_smem<R>(nz, kChunkShapes[f][0]) <= 48 * 1024;
+}
+
+// f: index into the chunked shapes.  Returns 0 ok, 2 the column does not fit.
+template <typename R>
+int launch_acoustic_column_chunked(const AcouArgs<R>& a, int f, cudaStream_t st) {
+  const int nz = a.L.nz;
+  if (!acoustic_chunked_fits<R>(nz, f)) return 2;
+  const int cx = kChunkShapes[f][0], kl = kChunkShapes[f][1];
+  const size_t sm = chunked_smem<R>(nz, cx);
+  const dim3 grd((a.L.nx + cx - 1) / cx, a.L.ny, 1), blk(cx, kl);
+  switch (f) {
+    case 0: k_acoustic_column_chunked<R, 32, 8, 8><<<grd, blk, sm, st>>>(a); break;
+    case 1: k_acoustic_column_chunked<R, 16, 16, 4><<<grd, blk, sm, st>>>(a); break;
+    default: k_acoustic_column_chunked<R, 32, 16, 4><<<grd, blk, sm, st>>>(a); break;
+  }
+  return 0;
+}
+
 // the plain column tile shape of fused shape f
 int acoustic_fused_column_shape(int f) {
   return (f >= 0 && f < kNumFusedShapes) ? kFusedShapes[f] : 0;
@@ -1015,7 +1222,9 @@ int occupancy_column(int shape, int nz_max) {
   template int prepare_acoustic_column<R>(int);                                                 \
   template bool acoustic_fused_fits<R>(int, int);                                              \
   template int prepare_acoustic_fused<R>(int);                                                 \
-  template int launch_acoustic_fused<R>(const AcouArgs<R>&, int, cudaStream_t);
+  template int launch_acoustic_fused<R>(const AcouArgs<R>&, int, cudaStream_t);                \
+  template bool acoustic_chunked_fits<R>(int, int);                                            \
+  template int launch_acoustic_column_chunked<R>(const AcouArgs<R>&, int, cudaStream_t);
 WFE_INST(float)
 WFE_INST(double)
 #undef WFE_INST

@@ -362,6 +362,13 @@ template <typename R>
 bool acoustic_fused_fits(int nz, int f);
 template <typename R>
 int prepare_acoustic_fused(int nz);
+// The column kernel with contiguous level chunks per lane (fewer barriers),
+// acoustic_chunked_shapes() shapes; same values as launch_acoustic_column.
+template <typename R>
+int launch_acoustic_column_chunked(const AcouArgs<R>& a, int f, cudaStream_t st);
+int acoustic_chunked_shapes();
+template <typename R>
+bool acoustic_chunked_fits(int nz, int f);
 // whether tile shape `shape` holds a column of nz levels in shared memory
 template <typename R>
 bool acoustic_column_fits(int nz, int shape);

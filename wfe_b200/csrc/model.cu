@@ -724,8 +724,18 @@ class ModelT final : public Model {
   // the plain column tile shape of the variant in use (the linearised runs
   // launch the unfused kernels)
   int column_shape() const override {
+    if (chunked_index(tune_.column_cx) >= 0) return 0;
     const int f = tune_.column_cx - acoustic_column_shapes() - 1;
     return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
+  }
+  // chunked column variants follow the fused ones; -1 for other variants
+  int chunked_index(int v) const {
+    const int f = v - acoustic_column_shapes() - 1 - acoustic_fused_shapes();
+    return (f >= 0 && f < acoustic_chunked_shapes()) ? f : -1;
+  }
+  bool chunked_usable(int v) const {
+    const int f = chunked_index(v);
+    return f >= 0 && acoustic_chunked_fits<R>(g_.nz, f);
   }
   bool fused_usable(int v) const {
     const int f = v - acoustic_column_shapes() - 1;
@@ -794,7 +804,8 @@ class ModelT final : public Model {
 
   // WFE_COLUMN_VARIANT=<n> forces the acoustic variant (0..5 column tile
   // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
-  // tile shapes) and WFE_TEND_VARIANT=<n> the tendency
+  // tile shapes, 10..12 the chunked column kernel) and WFE_TEND_VARIANT=<n>
+  // the tendency
   // variant (0 fused, 1 split, 2 momentum + TMA-staged scalars) after tuning,
   // for tests and experiments
   int autotune(double dt) {
@@ -804,7 +815,7 @@ class ModelT final : public Model {
     if (first && cv && *cv) {
       const int v = std::atoi(cv);
       if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_) ||
-                     fused_usable(v)))
+                     fused_usable(v) || chunked_usable(v)))
         tune_.column_cx = v;
     }
     const char* tv = std::getenv("WFE_TEND_VARIANT");
@@ -845,10 +856,10 @@ class ModelT final : public Model {
     best = 1e30f;
     const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
     // tile shapes, the TMA-staged column, the fused substep kernels
-    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes();
+    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() + acoustic_chunked_shapes();
     for (int cx = 0; cx < nvar; ++cx) {
       if (cx == acoustic_column_shapes() && !tma_ok_) continue;
-      if (cx > acoustic_column_shapes() && !fused_usable(cx)) continue;
+      if (cx > acoustic_column_shapes() && !fused_usable(cx) && !chunked_usable(cx)) continue;
       float ms;
       tune_.column_cx = cx;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -1054,7 +1065,10 @@ class ModelT final : public Model {
         launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
       }
       if (!fuse && !record(K_COL, a)) {
-        if (tma_ok_ && tune_.column_cx == acoustic_column_shapes()) {
+        if (chunked_usable(tune_.column_cx)) {
+          const int f = chunked_index(tune_.column_cx);
+          launch("acoustic_column", [&] { rc = launch_acoustic_column_chunked<R>(a, f, st_); });
+        } else if (tma_ok_ && tune_.column_cx == acoustic_column_shapes()) {
           TmaColParams<R> tp;
           if (tma_params(a, &tp)) return 1;
           launch("acoustic_column", [&] { rc = launch_acoustic_column_tma<R>(tp, st_); });
