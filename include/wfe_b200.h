@@ -240,8 +240,12 @@ int wfe_ensemble_step(wfe_ens* ens, double dt, double t);
 int wfe_ensemble_sync(wfe_ens* ens);
 /* nsteps graph-replayed steps timed with CUDA events on the ensemble's stream */
 int wfe_ensemble_time_run(wfe_ens* ens, int nsteps, double dt, double t0, double* ms);
-/* batched launches per step; tuned variants (tendencies split, acoustic
- * column tile shape, persistent grid) */
+/* launches per step; tuned variants: tendencies split, acoustic column tile
+ * shape, and the mode (0 batched launches, one block per work item; 1
+ * batched on a persistent grid; 2 every member's own graph on its own
+ * stream, the members running concurrently).  The first run of 8 or more
+ * steps times one step of each mode (after three warm-up steps of each) and
+ * keeps the faster: both give the same values, bit for bit. */
 long wfe_ensemble_launches_per_step(const wfe_ens* ens);
 int wfe_ensemble_variants(const wfe_ens* ens, int out[3]);
 

@@ -65,13 +65,19 @@ def _alone(path, prec, n):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_ensemble_equals_members_alone(member_cases, prec):
+@pytest.mark.parametrize("mode", ["batched", "members", ""])
+def test_ensemble_equals_members_alone(member_cases, prec, mode, monkeypatch):
+    """batched launches, the members' own graphs on concurrent streams, and
+    the mode the first run picks by timing one step of each ("")"""
+    monkeypatch.setenv("WFE_ENSEMBLE_MODE", mode)
     n = 65  # crosses the boundary-file switch at 3600 s
     mem = [W.Case(p, precision=prec) for p in member_cases]
     ens = W.Ensemble(mem)
     ens.run(n, mem[0].dt)
     ens.sync()
     assert ens.launches_per_step() > 0
+    if mode:
+        assert ens.variants()["mode"] == mode
     for p, m in zip(member_cases, mem):
         alone = _alone(p, prec, n)
         for k in W.FIELDS:

@@ -253,3 +253,25 @@ def test_watchdog_absmax_begin_end_matches_blocking_call():
             assert c.absmax_end((s - 1) & 1) == seen[-2][1]
     assert c.absmax_end(4 & 1) == seen[-1][1]
     c.close()
+
+
+@pytest.mark.gpu
+def test_cases_of_different_depths_share_the_kernels(monkeypatch):
+    """A shallower case set up after a deeper one must not lower the shared-
+    memory limit of the kernels the deeper case launches (FP64 column tiles
+    of 30 levels need more than the default 48 KB)."""
+    monkeypatch.setenv("WFE_COLUMN_VARIANT", "0")
+    deep = {"nz": "30"}
+    a = W.Case(CASES / "bubble_open.ini", deep, precision="f64")
+    ref = W.Case(CASES / "bubble_open.ini", deep, precision="f64")
+    ref.run(2)
+    ref.sync()
+    shallow = W.Case(CASES / "bubble_open.ini", {"nz": "8"}, precision="f64")
+    shallow.run(2)
+    shallow.sync()
+    for s in range(2):
+        a.step(a.dt, s * a.dt)
+    for k in W.FIELDS:
+        assert np.array_equal(a.field(k), ref.field(k)), k
+    for c in (a, ref, shallow):
+        c.close()

@@ -22,6 +22,10 @@
 // kernel may read neighbours while the next substep's buffers are written.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "core.cuh"
 #include "kernels.cuh"
 #include "dyn_common.cuh"
@@ -952,8 +956,7 @@ template <typename R>
 int prepare_acoustic_column_tma(int nz) {
   const size_t sm = acoustic_column_tma_smem<R>(nz);
   if (!sm) return 2;
-  return cudaFuncSetAttribute(k_acoustic_column_tma<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sm) == cudaSuccess
+  return raise_smem_limit(k_acoustic_column_tma<R>, sm) == cudaSuccess
              ? 0
              : 1;
 }
@@ -999,11 +1002,24 @@ size_t column_smem(int nz, int cx) {
 
 template <typename R, int CX, int KL>
 static cudaError_t column_attr(size_t sm) {
-  cudaError_t e = cudaFuncSetAttribute(k_acoustic_column<R, CX, KL>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = raise_smem_limit(k_acoustic_column<R, CX, KL>, sm);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_acoustic_column_batch<R, CX, KL>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  return raise_smem_limit(k_acoustic_column_batch<R, CX, KL>, sm);
+}
+
+cudaError_t raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> limits;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(func, dev);
+  auto it = limits.find(key);
+  if (it != limits.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) limits[key] = bytes;
+  return e;
 }
 
 // Tile shapes (columns x level lanes) the autotuner chooses from.
@@ -1120,12 +1136,12 @@ template <typename R>
 int prepare_acoustic_fused(int nz) {
   for (int f = 0; f < kNumFusedShapes; ++f) {
     if (!fused_fits<R>(nz, f)) continue;
-    const int sm = (int)fused_smem<R>(nz, kColumnShapes[kFusedShapes[f]][0]);
+    const size_t sm = fused_smem<R>(nz, kColumnShapes[kFusedShapes[f]][0]);
     cudaError_t e;
     switch (kFusedShapes[f]) {
-      case 0: e = cudaFuncSetAttribute(k_acoustic_fused<R, 32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-      case 4: e = cudaFuncSetAttribute(k_acoustic_fused<R, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-      default: e = cudaFuncSetAttribute(k_acoustic_fused<R, 16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      case 0: e = raise_smem_limit(k_acoustic_fused<R, 32, 8>, sm); break;
+      case 4: e = raise_smem_limit(k_acoustic_fused<R, 16, 8>, sm); break;
+      default: e = raise_smem_limit(k_acoustic_fused<R, 16, 16>, sm); break;
     }
     if (e != cudaSuccess) return 1;
   }

@@ -225,8 +225,7 @@ size_t tend_scal_tma_smem() {
 
 template <typename R>
 int prepare_tend_scal_tma() {
-  return cudaFuncSetAttribute(k_tend_scal_tma<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)tend_scal_tma_smem<R>()) == cudaSuccess
+  return raise_smem_limit(k_tend_scal_tma<R>, tend_scal_tma_smem<R>()) == cudaSuccess
              ? 0
              : 1;
 }

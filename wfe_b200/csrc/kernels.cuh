@@ -351,6 +351,15 @@ int launch_acoustic_column_tma(const TmaColParams<R>& p, cudaStream_t st);
 template <typename R>
 int launch_acoustic_column(const AcouArgs<R>& a, int shape, cudaStream_t st);
 int acoustic_column_shapes();
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) that never lowers the
+// limit an earlier call set for the same kernel on the current device: cases
+// of different depths in one process share the kernels, and a shallower
+// case's set-up must not cut the limit a deeper case relies on
+cudaError_t raise_smem_limit(const void* func, size_t bytes);
+template <typename K>
+cudaError_t raise_smem_limit(K* func, size_t bytes) {
+  return raise_smem_limit(reinterpret_cast<const void*>(func), bytes);
+}
 // The fused substep kernel (u, v faces of the tile, then its columns), in
 // acoustic_fused_shapes() tile shapes; theta'_in and theta'_out must be
 // distinct buffers (pi', u and v always are).  Returns 0 ok, 2 too deep.

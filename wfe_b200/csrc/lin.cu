@@ -1486,10 +1486,8 @@ static size_t lin_col_smem(int nz) {
 template <typename R>
 int lin_prepare(int nz) {
   if (nz > lin_max_levels()) return 2;
-  if (cudaFuncSetAttribute(k_tl_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)lin_col_smem<R, T_NARR>(nz)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_ad_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)lin_col_smem<R, A_NARR>(nz)) != cudaSuccess)
+  if (raise_smem_limit(k_tl_column<R>, lin_col_smem<R, T_NARR>(nz)) != cudaSuccess ||
+      raise_smem_limit(k_ad_column<R>, lin_col_smem<R, A_NARR>(nz)) != cudaSuccess)
     return 1;
   return lin_kessler_prepare<R>(nz);
 }

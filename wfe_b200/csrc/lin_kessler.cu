@@ -295,10 +295,8 @@ size_t ad_kessler_smem(int nz) {
 
 template <typename R>
 int lin_kessler_prepare(int nz) {
-  if (cudaFuncSetAttribute(k_tl_kessler<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)tl_kessler_smem<R>(nz)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_ad_kessler<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)ad_kessler_smem<R>(nz)) != cudaSuccess)
+  if (raise_smem_limit(k_tl_kessler<R>, tl_kessler_smem<R>(nz)) != cudaSuccess ||
+      raise_smem_limit(k_ad_kessler<R>, ad_kessler_smem<R>(nz)) != cudaSuccess)
     return 1;
   return 0;
 }

@@ -38,7 +38,7 @@ namespace wfe {
 struct Tune {
   int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches, 2 with TMA-staged scalars
   int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
-  int persist = 0;       // batched launches: 0 one block per work item, 1 persistent grid
+  int persist = 0;       // ensembles: 0 one block per work item, 1 persistent grid, 2 members' own graphs
   bool done = false;
 };
 
@@ -433,6 +433,12 @@ class ModelT final : public Model {
   int run(int nsteps, double dt, double t0) override {
     if (autotune(dt)) return 1;
     launch_clock(clock_, t0, t_lo_, t_hi_, dt, 0, st_);
+    return graph_steps(nsteps, dt);
+  }
+
+  // nsteps graph-replayed steps on the member's stream, the clock running on
+  // from its last value (the ensemble's concurrent mode; run() sets it first)
+  int graph_steps(int nsteps, double dt) {
     if (!graphs_valid_ || graph_dt_ != dt) {
       for (auto& ge : gexec_)
         if (ge) {
@@ -752,6 +758,7 @@ class ModelT final : public Model {
   }
   long generation() const { return gen_; }
   double* clock_ptr() const { return clock_; }
+  int tune_for(double dt) { return autotune(dt); }
   double bdy_t_lo() const { return t_lo_; }
   double bdy_t_hi() const { return t_hi_; }
   cudaStream_t stream() const { return st_; }
@@ -791,10 +798,17 @@ class ModelT final : public Model {
     for (int rep = 0; rep < 3; ++rep) {
       CK(cudaEventRecord(e0, st_));
       if (f()) return 1;
+      // a variant whose launch is refused (its resources do not fit) is
+      // never the fastest
+      const bool refused = cudaGetLastError() != cudaSuccess;
       CK(cudaEventRecord(e1, st_));
       CK(cudaEventSynchronize(e1));
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (refused) {
+        *best = 1e30f;
+        break;
+      }
       if (ms < *best) *best = ms;
     }
     cudaEventDestroy(e0);
@@ -1457,6 +1471,70 @@ class EnsembleT final : public Ensemble {
     CK(cudaSetDevice(dev_));
     if (begin(dt)) return 1;
     for (auto* x : mem_) launch_clock(x->clock_ptr(), t0, x->bdy_t_lo(), x->bdy_t_hi(), dt, 0, st_);
+    int s = 0;
+    const char* em = std::getenv("WFE_ENSEMBLE_MODE");  // "members" | "batched": no timing
+    if (em && *em) {
+      mode_done_ = true;
+      tune_.persist = std::string(em) == "members" ? 2 : ((tune_.persist & 1) | 4);
+    }
+    if (!mode_done_ && nsteps >= 8) {
+      // pick between the batched launches and the members' own graphs on
+      // their own streams on real steps (both give the same values, bit for
+      // bit): three warm-up steps of each mode capture every phase's graphs,
+      // then one timed step each
+      float tb = 0, tc = 0;
+      if (batched_steps(3, dt) || timed([&] { return batched_steps(1, dt); }, &tb)) return 1;
+      if (member_steps(3, dt) || timed([&] { return member_steps(1, dt); }, &tc)) return 1;
+      s = 8;
+      mode_done_ = true;
+      tune_.persist = tc < tb ? 2 : ((tune_.persist & 1) | 4);
+      tune_store(tune_key(), tune_);
+    }
+    if (tune_.persist == 2) {
+      if (member_steps(nsteps - s, dt)) return 1;
+      return 0;
+    }
+    if (batched_steps(nsteps - s, dt)) return 1;
+    return finish();
+  }
+
+  // members' own graphs, each on its own stream, interleaved step by step;
+  // ordered after the ensemble stream's work, and the ensemble stream after them
+  int member_steps(int nsteps, double dt) {
+    CK(cudaEventRecord(ev_, st_));
+    for (auto* x : mem_) {
+      CK(cudaStreamWaitEvent(x->stream(), ev_, 0));
+      if (x->tune_for(dt)) return fail(x->error());
+    }
+    for (int s = 0; s < nsteps; ++s)
+      for (auto* x : mem_)
+        if (x->graph_steps(1, dt)) return fail(x->error());
+    long l = 0;
+    for (auto* x : mem_) {
+      CK(cudaEventRecord(ev_, x->stream()));
+      CK(cudaStreamWaitEvent(st_, ev_, 0));
+      l += x->launches_per_step();
+    }
+    if (tune_.persist == 2) launches_ = l;
+    return 0;
+  }
+
+  template <typename F>
+  int timed(F&& f, float* ms) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st_));
+    int rc = f();
+    CK(cudaEventRecord(e1, st_));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+  }
+
+  int batched_steps(int nsteps, double dt) {
     for (int s = 0; s < nsteps; ++s) {
       Phase& P = ph_[mem_[0]->phase()];
       if (!P.ge) {
@@ -1473,7 +1551,7 @@ class EnsembleT final : public Ensemble {
       CK(cudaGraphLaunch(P.ge, st_));
       for (auto* x : mem_) x->rotate();
     }
-    return finish();
+    return 0;
   }
 
   int step(double dt, double t) override {
@@ -1515,10 +1593,13 @@ class EnsembleT final : public Ensemble {
   void variants(int* tend, int* column, int* persist) const override {
     *tend = tune_.tend_variant;
     *column = tune_.column_cx;
-    *persist = tune_.persist;
+    *persist = tune_.persist & 3;
   }
 
  private:
+  // tune_.persist: bit 0 the persistent grid of the batched launches, 4 the
+  // batched mode chosen on real steps; 2 the members' own graphs chosen
+  bool mode_done_ = false;  // batched vs members' own graphs decided
   struct Work {
     int4* d = nullptr;
     int n = 0;
@@ -1673,7 +1754,7 @@ class EnsembleT final : public Ensemble {
       for (int sub = 0; sub < (int)q.subs.size(); ++sub) {
         const Work* w = q.subs[sub];
         int nblocks = w->n;
-        if (tune_.persist) {
+        if (tune_.persist & 1) {
           int occ = kind_occupancy<R>(q.kind, var, sub, nz_max_);
           nblocks = std::min(w->n, occ * sms_);
         }
@@ -1710,6 +1791,7 @@ class EnsembleT final : public Ensemble {
     Tune cached;
     if (tune_lookup(key, &cached)) {
       tune_ = cached;
+      mode_done_ = tune_.persist == 2 || (tune_.persist & 4);
       return 0;
     }
     int upto = -1;

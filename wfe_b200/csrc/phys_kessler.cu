@@ -144,15 +144,13 @@ int prepare_kessler(int nz) {
   int cx = kessler_cx<R>(nz);
   cudaError_t e;
   if (cx == 32) {
-    const int sm = (int)kessler_smem<R>(nz, 32, 8);
-    e = cudaFuncSetAttribute(k_kessler<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_kessler_batch<R, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    const size_t sm = kessler_smem<R>(nz, 32, 8);
+    e = raise_smem_limit(k_kessler<R, 32>, sm);
+    if (e == cudaSuccess) e = raise_smem_limit(k_kessler_batch<R, 32>, sm);
   } else if (cx == 8) {
-    const int sm = (int)kessler_smem<R>(nz, 8, 32);
-    e = cudaFuncSetAttribute(k_kessler<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_kessler_batch<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    const size_t sm = kessler_smem<R>(nz, 8, 32);
+    e = raise_smem_limit(k_kessler<R, 8>, sm);
+    if (e == cudaSuccess) e = raise_smem_limit(k_kessler_batch<R, 8>, sm);
   } else {
     return 2;
   }
