@@ -235,7 +235,8 @@ def run_reference(args) -> dict:
 
 def e2e_run(W, case_ini, steps: int, device: int):
     """End to end through the public API with host buffers, at the reference
-    driver's cadence (src/main.cpp:425-467): initial state uploaded from
+    driver's cadence (src/main.cpp:425-467), after three untimed warm-up
+    steps through the same calls: initial state uploaded from
     page-locked host buffers, every step the |w| watchdog read back (one step
     behind: wfe_absmax_begin queues step s's reduction, and step s's value is
     read once step s + 1 is queued, so the GPU never waits for the host),
@@ -252,6 +253,16 @@ def e2e_run(W, case_ini, steps: int, device: int):
     full = c.snapshot_buffers(list(W.FIELDS) + ["rain"])
     diag_every = max(1, round(120.0 / c.dt))
     out_every = max(1, round(600.0 / c.dt))
+    # untimed warm-up through the same calls: the first steps capture the
+    # three rotation phases' graphs (one-time set-up, like the warm-up steps
+    # of the device-resident measurement); the timed run restarts from the
+    # host copy of the initial state
+    c.run(3, c.dt, 0.0)
+    c.absmax_begin("w", 0)
+    c.absmax_end(0)
+    c.snapshot_begin(diag)
+    c.snapshot_wait()
+    c.sync()
     h2d = d2h = 0
     sync_device(1)
     t0 = time.perf_counter()
@@ -572,10 +583,15 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        ev, h2d, d2h, el = e2e_run(W, CASE, args.steps, local)
+        # three runs, the median: the wall clock of a host-driven loop also
+        # sees the host's own scheduling (one stalled host thread idles the GPU)
+        runs = [e2e_run(W, CASE, args.steps, local) for _ in range(3)]
+        vals = sorted(r[0] for r in runs)
+        ev, h2d, d2h = vals[1], runs[0][1], runs[0][2]
         ev = reduce_max(1.0 / ev, world)  # slowest rank
         e2e = {"value": world / ev, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h}
+               "d2h_bytes_per_step": d2h, "runs": [round(v) for v in vals],
+               "statistic": "median of 3 runs"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
