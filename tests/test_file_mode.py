@@ -140,3 +140,26 @@ def test_file_mode_fp32_within_reference_spread(file_case, n):
     for k in ("qv", "qc", "qr"):
         assert np.all(c.interior(c.field(k)) >= 0), k
     c.close()
+
+
+@pytest.mark.gpu
+def test_boundary_switch_waits_for_queued_steps(tmp_path):
+    """wfe_run replays the steps up to a boundary-file switch asynchronously,
+    then swaps the targets and uploads the next file: the upload must not
+    overwrite targets the queued steps still read.  A member large enough
+    that the GPU is still busy when the host reaches the switch, run in one
+    call, against the same steps taken one at a time (each synchronised)."""
+    from test_ensemble import make_members
+
+    (p,) = make_members(tmp_path, members=[(160, 128, 24, 5, 14.0)], hours=2, bdy_interval=3600)
+    n = 62  # the switch at 3600 s = step 60
+    a = W.Case(p, precision="f32")
+    a.run(n)
+    a.sync()
+    b = W.Case(p, precision="f32")
+    for s in range(n):
+        b.step(b.dt, s * b.dt)
+    for k in W.FIELDS:
+        assert np.array_equal(a.field(k), b.field(k)), k
+    a.close()
+    b.close()

@@ -395,8 +395,18 @@ void launch_pack_interior(const R* src, const Layout& L, int nzl, void* dst, boo
                           cudaStream_t st);
 template <typename R>
 void launch_pack_interior2d(const R* src, const Layout& L, void* dst, bool f32, cudaStream_t st);
+// a contiguous float32 (f32) or float64 interior block into a field's
+// interior points (io.cu)
+template <typename R>
+void launch_unpack_interior(const void* src, const Layout& L, int nzl, R* dst, bool f32,
+                            cudaStream_t st);
 template <typename R>
 void launch_absmax(const R* f, size_t n, unsigned int* result, cudaStream_t st);
+// max |f| as float bits into mapped host memory; acc: two device words, zero
+// before the first call and left zero by every call (phys_kessler.cu)
+template <typename R>
+void launch_absmax_to_host(const R* f, size_t n, unsigned int* acc, unsigned int* host_out,
+                           cudaStream_t st);
 template <typename R>
 void launch_dry_mass(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* pip,
                      const R* thp, const R* qv, const R* qc, const R* qr, int moist, R dx, R dy,

@@ -311,26 +311,20 @@ class ModelT final : public Model {
     R* d = field_ptr(role, field);
     if (!d) return fail("bad role/field");
     const int nzl = field == 2 ? g_.nz + 1 : g_.nz;
-    // read back the planes first so that ghosts and padding keep their values
-    const size_t off = L_.at(-kOX, -kOY, 0), cnt = (size_t)nzl * L_.plane();
-    CK(cudaMemcpyAsync(stage_ + off, d + off, cnt * sizeof(R), cudaMemcpyDeviceToHost, st_));
-    CK(cudaStreamSynchronize(st_));
-    const size_t row = (size_t)g_.nx;
-    for (int k = 0; k < nzl; ++k)
-      for (int j = 0; j < g_.ny; ++j) {
-        R* dst = stage_ + L_.at(0, j, k);
-        size_t o = ((size_t)k * g_.ny + j) * row;
-        if (f32 == (sizeof(R) == 4)) {
-          std::memcpy(dst, (const char*)host + o * sizeof(R), row * sizeof(R));
-        } else if (f32) {
-          const float* src = (const float*)host + o;
-          for (size_t i = 0; i < row; ++i) dst[i] = (R)src[i];
-        } else {
-          const double* src = (const double*)host + o;
-          for (size_t i = 0; i < row; ++i) dst[i] = (R)src[i];
-        }
-      }
-    CK(cudaMemcpyAsync(d + off, stage_ + off, cnt * sizeof(R), cudaMemcpyHostToDevice, st_));
+    // the block crosses the host link as one copy into a device staging
+    // buffer; a kernel scatters it into the interior points (ghosts and
+    // padding keep their values).  Synchronous: the caller may reuse `host`.
+    const size_t bytes = (size_t)nzl * g_.ny * g_.nx * (f32 ? 4 : 8);
+    if (up_cap_ < bytes) {
+      if (up_buf_) cudaFree(up_buf_);
+      up_buf_ = nullptr;
+      up_cap_ = 0;
+      CK(cudaMalloc(&up_buf_, bytes));
+      up_cap_ = bytes;
+    }
+    CK(cudaMemcpyAsync(up_buf_, host, bytes, cudaMemcpyHostToDevice, st_));
+    launch_unpack_interior<R>(up_buf_, L_, nzl, d, f32, st_);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st_));
     return 0;
   }
@@ -555,13 +549,16 @@ class ModelT final : public Model {
     R* d = field_ptr(ROLE_STATE, field);
     if (!d) return fail("bad field");
     if (!wd_async_) {
-      CK(cudaMalloc(&wd_async_, 2 * sizeof(unsigned int)));
-      CK(cudaHostAlloc(&wd_host_, 2 * sizeof(unsigned int), cudaHostAllocDefault));
+      // per slot: the blocks' maximum and their count (left zero by every
+      // launch); the result lands in mapped page-locked memory
+      CK(cudaMalloc(&wd_async_, 4 * sizeof(unsigned int)));
+      CK(cudaMemset(wd_async_, 0, 4 * sizeof(unsigned int)));
+      CK(cudaHostAlloc(&wd_host_, 2 * sizeof(unsigned int), cudaHostAllocMapped));
+      CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&wd_host_dev_), wd_host_, 0));
       for (auto& e : wd_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    CK(cudaMemsetAsync(wd_async_ + slot, 0, sizeof(unsigned int), st_));
-    launch_absmax<R>(d, L_.n3(), wd_async_ + slot, st_);
-    CK(cudaMemcpyAsync(wd_host_ + slot, wd_async_ + slot, sizeof(unsigned int), cudaMemcpyDeviceToHost, st_));
+    launch_absmax_to_host<R>(d, L_.n3(), wd_async_ + 2 * slot, wd_host_dev_ + slot, st_);
+    CK(cudaGetLastError());
     CK(cudaEventRecord(wd_ev_[slot], st_));
     return 0;
   }
@@ -569,7 +566,8 @@ class ModelT final : public Model {
   int absmax_end(int slot, float* out) override {
     if (slot < 0 || slot > 1 || !wd_async_) return fail("absmax_end without absmax_begin");
     CK(cudaEventSynchronize(wd_ev_[slot]));
-    std::memcpy(out, wd_host_ + slot, sizeof(float));
+    unsigned int bits = *reinterpret_cast<volatile unsigned int*>(wd_host_ + slot);
+    std::memcpy(out, &bits, sizeof(float));
     return 0;
   }
 
@@ -1300,12 +1298,18 @@ class ModelT final : public Model {
         for (int i = -3; i < g_.nx + 3; ++i) ref[g_.idx(i, j, k)] = (double)in[L_.at(i, j, k)];
   }
 
+  // put3d / put2d / put1d overwrite buffers that queued steps may still read
+  // (boundary targets switched between runs, surface fields): the model's
+  // stream is drained first (the copies themselves are not stream-ordered,
+  // and an ensemble orders its members' streams after its own work)
   int put3d(R* d, const std::vector<double>& ref) {
     to_pitched(ref.data(), stage_tmp(L_.n3()), true);
+    CK(cudaStreamSynchronize(st_));
     CK(cudaMemcpy(d, tmp_.data(), L_.n3() * sizeof(R), cudaMemcpyHostToDevice));
     return 0;
   }
   int put2d(R* d, const std::vector<double>& ref2) {
+    CK(cudaStreamSynchronize(st_));
     R* o = stage_tmp(L_.n2());
     for (int j = -kOY; j < L_.py - kOY; ++j)
       for (int i = -kOX; i < L_.px - kOX; ++i) {
@@ -1316,6 +1320,7 @@ class ModelT final : public Model {
     return 0;
   }
   int put1d(R* d, const std::vector<double>& v) {
+    CK(cudaStreamSynchronize(st_));
     R* o = stage_tmp(L_.pz);
     for (int q = 0; q < L_.pz; ++q) o[q] = (R)v[q];
     CK(cudaMemcpy(d, o, L_.pz * sizeof(R), cudaMemcpyHostToDevice));
@@ -1349,6 +1354,9 @@ class ModelT final : public Model {
     }
     if (snap_ev_) cudaEventDestroy(snap_ev_);
     if (snap_buf_) cudaFree(snap_buf_);
+    if (up_buf_) cudaFree(up_buf_);
+    up_buf_ = nullptr;
+    up_cap_ = 0;
     cs_st_ = nullptr;
     snap_ev_ = nullptr;
     snap_buf_ = nullptr;
@@ -1406,7 +1414,8 @@ class ModelT final : public Model {
   double* clock_ = nullptr;
   unsigned int* wd_ = nullptr;
   unsigned int* wd_async_ = nullptr;   // two watchdog slots (absmax_begin / end)
-  unsigned int* wd_host_ = nullptr;    // their page-locked copies
+  unsigned int* wd_host_ = nullptr;    // mapped page-locked results, one per slot
+  unsigned int* wd_host_dev_ = nullptr;  // the same words as the device sees them
   cudaEvent_t wd_ev_[2] = {nullptr, nullptr};
   double *mass_planes_ = nullptr, *mass_ = nullptr;
   R* stage_ = nullptr;
@@ -1426,6 +1435,8 @@ class ModelT final : public Model {
   cudaStream_t cs_st_ = nullptr;     // snapshot copy stream
   cudaEvent_t snap_ev_ = nullptr;
   void* snap_buf_ = nullptr;         // packed snapshot staging
+  void* up_buf_ = nullptr;           // interior upload staging
+  size_t up_cap_ = 0;
   size_t snap_cap_ = 0;
   std::function<void*(const void*)> lin_map_;
   double graph_dt_ = 0;

@@ -209,7 +209,11 @@ int launch_kessler(const KesArgs<R>& a, cudaStream_t st) {
 // nx / ny, w levels up to nz); as float bits so that NaN ranks above every
 // finite value (kernels.cu:275-289).
 template <typename R>
-__global__ void k_absmax(const R* __restrict__ f, size_t n, unsigned int* result) {
+__global__ void __launch_bounds__(256) k_absmax(const R* __restrict__ f, size_t n, unsigned int* result) {
+  // |f| as float bits: the unsigned order of non-negative floats, NaN above
+  // every finite value; one atomic per block (the blocks' atomics on one
+  // address serialise in L2)
+  __shared__ unsigned int warp_best[8];
   unsigned int best = 0;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
        idx += (size_t)gridDim.x * blockDim.x) {
@@ -218,13 +222,61 @@ __global__ void k_absmax(const R* __restrict__ f, size_t n, unsigned int* result
     best = b > best ? b : best;
   }
   for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(result, best);
+  if ((threadIdx.x & 31) == 0) warp_best[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    best = threadIdx.x < (blockDim.x >> 5) ? warp_best[threadIdx.x] : 0u;
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (threadIdx.x == 0) atomicMax(result, best);
+  }
+}
+
+// The watchdog's pipelined form: the blocks' maxima meet in acc[0]; the last
+// block to finish (counted in acc[1]) writes the result straight into mapped
+// page-locked host memory and resets acc for the next call, so one launch is
+// all a step's watchdog adds to the stream (no memset, no copy).
+template <typename R>
+__global__ void __launch_bounds__(256) k_absmax_to_host(const R* __restrict__ f, size_t n, unsigned int* acc,
+                                                        unsigned int* host_out) {
+  __shared__ unsigned int warp_best[8];
+  unsigned int best = 0;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    float v = fabsf((float)f[idx]);
+    unsigned int b = __float_as_uint(v);
+    best = b > best ? b : best;
+  }
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) warp_best[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    best = threadIdx.x < (blockDim.x >> 5) ? warp_best[threadIdx.x] : 0u;
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (threadIdx.x == 0) {
+      atomicMax(acc, best);
+      __threadfence();
+      if (atomicAdd(acc + 1, 1u) == gridDim.x - 1) {
+        const unsigned int v = atomicExch(acc, 0u);
+        acc[1] = 0;
+        *reinterpret_cast<volatile unsigned int*>(host_out) = v;
+        __threadfence_system();
+      }
+    }
+  }
+}
+
+template <typename R>
+void launch_absmax_to_host(const R* f, size_t n, unsigned int* acc, unsigned int* host_out,
+                           cudaStream_t st) {
+  int grd = (int)((n + 255) / 256);
+  if (grd > 148 * 2) grd = 148 * 2;
+  k_absmax_to_host<R><<<grd, 256, 0, st>>>(f, n, acc, host_out);
 }
 
 template <typename R>
 void launch_absmax(const R* f, size_t n, unsigned int* result, cudaStream_t st) {
   int grd = (int)((n + 255) / 256);
-  if (grd > 148 * 8) grd = 148 * 8;
+  if (grd > 148 * 2) grd = 148 * 2;
   k_absmax<R><<<grd, 256, 0, st>>>(f, n, result);
 }
 
@@ -282,6 +334,7 @@ void launch_dry_mass(const Layout& L, const DBase<R>& b, const DMetric<R>& m, co
   template int batch_kessler<R>(const Batch<KesArgs<R>>&, int, int, cudaStream_t);             \
   template int occupancy_kessler<R>(int);                            \
   template void launch_absmax<R>(const R*, size_t, unsigned int*, cudaStream_t);              \
+  template void launch_absmax_to_host<R>(const R*, size_t, unsigned int*, unsigned int*, cudaStream_t); \
   template void launch_dry_mass<R>(const Layout&, const DBase<R>&, const DMetric<R>&, const R*, \
                                    const R*, const R*, const R*, const R*, int, R, R, double*, \
                                    double*, cudaStream_t);
