@@ -201,3 +201,71 @@ def test_control_mask_and_obs_indexing_on_host_case():
     with pytest.raises(W.WfeError):  # the relaxation needs the device model
         c.clear_boundary()
     c.close()
+
+
+def _linear_field(c, field, a, b, cy, d):
+    """a + b x + cy y + d zeta at the field's own points, padded layout"""
+    g = c.ng
+    ex = 0.0 if field == "u" else 0.5
+    ey = 0.0 if field == "v" else 0.5
+    zeta = c.metric("zeta_w" if field == "w" else "zeta_c")
+    x = (np.arange(c.NX) - g + ex) * c.dx
+    y = (np.arange(c.NY) - g + ey) * c.dy
+    return a + b * x[None, None, :] + cy * y[None, :, None] + d * zeta[:, None, None]
+
+
+@pytest.mark.parametrize("field", ["thp", "u", "v", "w"])
+def test_interp_obs_reproduce_trilinear_fields(field):
+    """Trilinear interpolation is exact for a field linear in (x, y, zeta);
+    over flat terrain zeta is the height z."""
+    c = W.Case(CASES / "bubble_open.ini", precision="f64", device=-1)
+    assert np.all(c.metric("h") == 0)
+    f = _linear_field(c, field, 1.5, 2e-4, -3e-4, 1e-3)
+    rng = np.random.default_rng(4)
+    ex = 0.0 if field == "u" else 0.5
+    ey = 0.0 if field == "v" else 0.5
+    nxp = c.nx + (field == "u")
+    nyp = c.ny + (field == "v")
+    zl = c.metric("zeta_w" if field == "w" else "zeta_c")[c.ng:c.ng + c.nz + (field == "w")]
+    x = (ex + rng.uniform(0, nxp - 1, 50)) * c.dx
+    y = (ey + rng.uniform(0, nyp - 1, 50)) * c.dy
+    z = rng.uniform(zl[0], zl[-1], 50)
+    o = AN.Obs.interp(c, 3, field, x, y, z, np.zeros(50), 0.5)
+    assert o.index.shape == (50, 8) and np.allclose(o.weight.sum(axis=1), 1.0)
+    expect = 1.5 + 2e-4 * x - 3e-4 * y + 1e-3 * z
+    assert np.allclose(o.sample({field: f}), expect, rtol=1e-12, atol=1e-12)
+    # the transpose: <H f, r> = <f, H^T r>
+    r = rng.standard_normal(50)
+    lam = {field: np.zeros(c.shape)}
+    o.scatter_into(lam, r)
+    assert abs(float(o.sample({field: f}) @ r) - float(np.sum(f * lam[field]))) <= 1e-12 * np.sum(np.abs(f))
+    with pytest.raises(ValueError):
+        AN.Obs.interp(c, 3, field, [-c.dx], [y[0]], [z[0]], [0.0])
+    with pytest.raises(ValueError):
+        AN.Obs.interp(c, 3, field, [x[0]], [y[0]], [c.zt * 2], [0.0])
+    c.close()
+
+
+def test_gradient_with_interpolated_observations():
+    """weighted observations (rows of points and weights) in the chained
+    adjoint gradient, against central differences"""
+    m = QuadMap(c=0.15)
+    rng = np.random.default_rng(13)
+    xb = {k: 0.5 * rng.standard_normal(m.n) for k in m.names}
+    idx = np.array([[0, 1], [3, 4], [5, 6], [2, 2]])
+    w = np.array([[0.25, 0.75], [0.5, 0.5], [0.9, 0.1], [0.3, 0.7]])
+    obs = [AN.Obs(2, "a", idx, rng.standard_normal(4), 0.1, w),
+           AN.Obs(4, "b", idx[:3], rng.standard_normal(3), 0.2, w[:3]),
+           AN.Obs(4, "a", [1, 7], rng.standard_normal(2), 0.1)]
+    v = AN.FourDVar(m, xb, 0.3, obs)
+    x0 = {k: xb[k] + 0.1 * rng.standard_normal(m.n) for k in m.names}
+    _, g = v.gradient(x0)
+    for _ in range(4):
+        d = {k: np.where(m.mask(k), rng.standard_normal(m.n), 0.0) for k in m.names}
+        eps = 1e-6
+        fd = (v.cost({k: x0[k] + eps * d[k] for k in m.names}) -
+              v.cost({k: x0[k] - eps * d[k] for k in m.names})) / (2 * eps)
+        an = sum(float(g[k] @ d[k]) for k in m.names)
+        assert abs(fd - an) <= 1e-7 * max(1.0, abs(an)), (fd, an)
+    with pytest.raises(ValueError):
+        AN.Obs(1, "a", idx, [1.0, 2.0], 1.0, w)  # one row per observation

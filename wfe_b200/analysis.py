@@ -97,21 +97,32 @@ class CaseModel:
 # ----------------------------------------------------------- observations
 @dataclass
 class Obs:
-    """Point observations of one prognostic field after `step` large steps
-    (0 = the start of the window): flat indices into the padded layout,
-    values and standard deviation(s)."""
+    """Observations of one prognostic field after `step` large steps (0 = the
+    start of the window).  Each observation is a point value (`index`: flat
+    indices into the padded layout, one per observation) or a weighted sum of
+    field values (`index` and `weight` of shape (n_obs, n_points), e.g. the
+    trilinear interpolation weights of ``Obs.interp``); values and standard
+    deviation(s)."""
 
     step: int
     field: str
     index: np.ndarray
     value: np.ndarray
     sigma: float | np.ndarray = 1.0
+    weight: np.ndarray | None = None
 
     def __post_init__(self):
-        self.index = np.asarray(self.index, dtype=np.int64).ravel()
         self.value = np.asarray(self.value, dtype=np.float64).ravel()
-        if self.index.shape != self.value.shape:
-            raise ValueError("one value per observed point")
+        idx = np.asarray(self.index, dtype=np.int64)
+        if self.weight is None:
+            self.index = idx.ravel()
+            if self.index.shape != self.value.shape:
+                raise ValueError("one value per observed point")
+        else:
+            w = np.asarray(self.weight, dtype=np.float64)
+            if idx.ndim != 2 or w.shape != idx.shape or idx.shape[0] != self.value.size:
+                raise ValueError("index and weight: one row of points per observation")
+            self.index, self.weight = idx, w
         s = np.broadcast_to(np.asarray(self.sigma, dtype=np.float64), self.value.shape)
         if np.any(s <= 0):
             raise ValueError("observation standard deviations must be positive")
@@ -125,12 +136,69 @@ class Obs:
         idx = ((k + g) * case.NY + (j + g)) * case.NX + (i + g)
         return Obs(step, field, idx, value, sigma)
 
+    @staticmethod
+    def interp(case, step: int, field: str, x, y, z, value, sigma=1.0) -> "Obs":
+        """Observations at physical positions (x, y in m from the domain's
+        corner, z in m above sea level): trilinear interpolation between the
+        field's own points in (x, y, zeta), zeta = zt (z - h) / (zt - h) with
+        the terrain height h interpolated bilinearly at (x, y) (the Gal-Chen
+        map, src/core/metric.cpp).  Cell-centred fields sit at ((i + 1/2) dx,
+        (j + 1/2) dy, zeta_c), u on x faces (i dx), v on y faces (j dy), w on
+        the zeta_w levels.  Positions outside the field's points raise."""
+        g = case.ng
+        x, y, z = (np.atleast_1d(np.asarray(a, dtype=np.float64)).ravel() for a in (x, y, z))
+        if not (x.shape == y.shape == z.shape):
+            raise ValueError("one x, y, z per observation")
+        ex = 0.0 if field == "u" else 0.5
+        ey = 0.0 if field == "v" else 0.5
+        nxp = case.nx + 1 if field == "u" else case.nx
+        nyp = case.ny + 1 if field == "v" else case.ny
+        zeta = case.metric("zeta_w" if field == "w" else "zeta_c")
+        nzp = case.nz + 1 if field == "w" else case.nz
+        zlev = zeta[g:g + nzp]
+
+        def axis(pos, d, e, n, name):
+            f = pos / d - e
+            if np.any(f < 0) or np.any(f > n - 1):
+                raise ValueError(f"observation {name} outside the field's points")
+            i0 = np.minimum(np.floor(f).astype(np.int64), max(n - 2, 0))
+            return i0, f - i0
+
+        i0, tx = axis(x, case.dx, ex, nxp, "x")
+        j0, ty = axis(y, case.dy, ey, nyp, "y")
+        # terrain height at (x, y) from the cell-centre h (ghost ring included)
+        h2 = case.metric("h").reshape(case.NY, case.NX)
+        fi, fj = x / case.dx - 0.5, y / case.dy - 0.5
+        hi0, hj0 = np.floor(fi).astype(np.int64), np.floor(fj).astype(np.int64)
+        hx, hy = fi - hi0, fj - hj0
+        hi0, hj0 = hi0 + g, hj0 + g
+        h = ((1 - hx) * (1 - hy) * h2[hj0, hi0] + hx * (1 - hy) * h2[hj0, hi0 + 1] +
+             (1 - hx) * hy * h2[hj0 + 1, hi0] + hx * hy * h2[hj0 + 1, hi0 + 1])
+        zt = case.zt
+        zc = zt * (z - h) / (zt - h)
+        if np.any(zc < zlev[0]) or np.any(zc > zlev[-1]):
+            raise ValueError("observation z outside the field's levels")
+        k0 = np.clip(np.searchsorted(zlev, zc, side="right") - 1, 0, nzp - 2)
+        tz = (zc - zlev[k0]) / (zlev[k0 + 1] - zlev[k0])
+        idx, wts = [], []
+        for dk, wk in ((0, 1 - tz), (1, tz)):
+            for dj, wj in ((0, 1 - ty), (1, ty)):
+                for di, wi in ((0, 1 - tx), (1, tx)):
+                    idx.append(((k0 + dk + g) * case.NY + (j0 + dj + g)) * case.NX + (i0 + di + g))
+                    wts.append(wk * wj * wi)
+        return Obs(step, field, np.stack(idx, axis=1), value, sigma, np.stack(wts, axis=1))
+
     def sample(self, x: dict) -> np.ndarray:
-        return x[self.field].ravel()[self.index]
+        v = x[self.field].ravel()[self.index]
+        return v if self.weight is None else np.sum(v * self.weight, axis=1)
 
     def scatter_into(self, lam: dict, r: np.ndarray) -> None:
         """lam[field] += H^T r (repeated indices accumulate)"""
-        np.add.at(lam[self.field].reshape(-1), self.index, r)
+        if self.weight is None:
+            np.add.at(lam[self.field].reshape(-1), self.index, r)
+        else:
+            np.add.at(lam[self.field].reshape(-1), self.index.ravel(),
+                      (self.weight * np.asarray(r)[:, None]).ravel())
 
 
 @dataclass
