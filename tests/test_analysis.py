@@ -1,8 +1,9 @@
 """Variational analysis and analysis nudging on the device (GPU).
 
   * the 4D-Var gradient (background term + point observations of w and
-    theta' at two times, chained adjoint runs) against central differences
-    of the cost along seeded directions (FP64);
+    theta' at two times and u, theta' interpolated at positions over the
+    terrain, chained adjoint runs) against central differences of the cost
+    along seeded directions (FP64);
   * incremental 4D-Var recovers a warm bubble missing from the background
     from observations of its evolution: the cost falls by an order of
     magnitude and theta' moves toward the truth;
@@ -70,6 +71,15 @@ def test_4dvar_gradient_matches_central_differences():
     xt = {k: xb[k] + (_bubble(c, 0.5, 8000.0, 2000.0, 1500.0) if k == "thp" else 0.0)
           for k in m.names}
     obs = _obs_from(c, m, xt, [2, 5], ["w", "thp"], {"w": 0.05, "thp": 0.1}, rng, every_k=2)
+    # and u, theta' interpolated at positions over the terrain
+    xs = rng.uniform(2 * c.dx, (c.nx - 2) * c.dx, 20)
+    ys = rng.uniform(1.0 * c.dy, (c.ny - 1) * c.dy, 20)
+    zs = rng.uniform(1500.0, 4000.0, 20)
+    traj5 = m.forecast(xt, 5)
+    for f, sg in (("u", 0.2), ("thp", 0.1)):
+        o = AN.Obs.interp(c, 5, f, xs, ys, zs, np.zeros(20), sg)
+        o.value = o.sample(traj5) + 0.05 * rng.standard_normal(20)
+        obs.append(o)
     v = AN.FourDVar(m, xb, SIGMA_B, obs)
     x0 = {k: xb[k] + 0.1 * SIGMA_B[k] * rng.standard_normal(c.shape) * m.mask(k)
           for k in m.names}
