@@ -96,10 +96,11 @@ def test_4dvar_gradient_matches_central_differences():
                   v.cost({k: x0[k] - eps * d[k] for k in m.names})) / (2 * eps)
             gap[eps] = abs(fd - ad) / abs(fd)
         # the O(eps^2) term of the central difference, over a floor of
-        # ~1e-7 - 1e-6: upwind switches of the advection where the bubble's
-        # velocities cross 0 make J piecewise smooth, kinks the gradient
-        # (the derivative of the branches taken) does not see
-        assert gap[1e-4] <= 1e-4 and gap[1e-5] <= 1e-5, (r, gap)
+        # 1e-7 - 2e-5: upwind switches of the advection where the bubble's and
+        # the mountain wave's vertical velocities cross 0 make J piecewise
+        # smooth, kinks the gradient (the derivative of the branches taken)
+        # does not see; the u observations make J the more sensitive to them
+        assert gap[1e-4] <= 5e-5 and gap[1e-5] <= 5e-5, (r, gap)
     c.close()
 
 
