@@ -261,15 +261,42 @@ __device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int
   return v_forward(a, i, j == L.ny ? 0 : j, k);
 }
 
+// Launched as (32, 4, 2) blocks.  Each thread computes theta_v and pi* of
+// its own cell once and shares them through shared memory: an interior
+// point takes its x (y) neighbour's values from the thread beside it in the
+// block when there is one, instead of loading the neighbour's five fields.
+constexpr int kUvBx = 32, kUvBy = 4, kUvBz = 2;
+
 template <typename R>
 __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
+  __shared__ R s_tv[kUvBz][kUvBy][kUvBx], s_ps[kUvBz][kUvBy][kUvBx];
   const Layout& L = a.L;
-  const int i = bx * blockDim.x + threadIdx.x;
-  const int j = by * blockDim.y + threadIdx.y;
-  const int k = bz * blockDim.z + threadIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
+  const int i = bx * kUvBx + tx;
+  const int j = by * kUvBy + ty;
+  const int k = bz * kUvBz + tz;
+  const bool has_cell = i < L.nx && j < L.ny && k < L.nz;
+  const size_t c = has_cell ? L.at(i, j, k) : 0;
+  R tv0 = 0, ps0 = 0;
+  if (has_cell) {
+    tv0 = theta_v_at(a, c);
+    ps0 = pistar_at(a, c);
+  }
+  s_tv[tz][ty][tx] = tv0;
+  s_ps[tz][ty][tx] = ps0;
+  __syncthreads();
   if (i > L.nx || j > L.ny || k >= L.nz) return;
   if (uv_interior<R>(L, i, j, k)) {
-    uv_pair_interior(a, i, j, k);
+    // the same values uv_pair_interior loads (kernels.cu:499-526)
+    const size_t sy = L.px;
+    const R tvx = tx > 0 ? s_tv[tz][ty][tx - 1] : theta_v_at(a, c - 1);
+    const R psx = tx > 0 ? s_ps[tz][ty][tx - 1] : pistar_at(a, c - 1);
+    const R tvy = ty > 0 ? s_tv[tz][ty - 1][tx] : theta_v_at(a, c - sy);
+    const R psy = ty > 0 ? s_ps[tz][ty - 1][tx] : pistar_at(a, c - sy);
+    const int kk = L.at1(k);
+    const size_t c2 = L.at2(i, j);
+    a.u_out[c] = u_interior_val(a, c, c2, kk, tv0, tvx, ps0, psx);
+    a.v_out[c] = v_interior_val(a, c, c2, kk, tv0, tvy, ps0, psy);
     return;
   }
   if (j < L.ny) a.u_out[L.at(i, j, k)] = u_face_edge(a, i, j, k);
@@ -987,12 +1014,12 @@ dim3 grid_uv(const Layout& L) {
 
 template <typename R>
 void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st) {
-  k_acoustic_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a);
+  k_acoustic_uv<R><<<grid_uv<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
 }
 
 template <typename R>
 void batch_uv(const Batch<AcouArgs<R>>& b, int nblocks, cudaStream_t st) {
-  k_acoustic_uv_batch<R><<<nblocks, dim3(32, 4, 2), 0, st>>>(b);
+  k_acoustic_uv_batch<R><<<nblocks, dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(b);
 }
 
 template <typename R>
