@@ -2,7 +2,7 @@
 
 Two steps, run from the repository root:
 
-  python tests/golden/make_golden.py run  --raw gpurun_out/golden_raw
+  python tests/golden/make_golden.py run  --raw <raw dir>
       On a machine with a B200 and the reference built by `make -C oracle ref`
       (oracle/_ref/).  Runs, for every case in tests/golden/cases/:
         * oracle/_ref/refdump_f64 / refdump_f32 (the reference's own kernels and
@@ -11,8 +11,8 @@ Two steps, run from the repository root:
           (its src/main.cpp), writing its float32 snapshots every step.
       Raw output goes to --raw.
 
-  python tests/golden/make_golden.py pack --raw gpurun_out/golden_raw
-      Here.  Packs a selection of the raw arrays into tests/golden/<case>.npz
+  python tests/golden/make_golden.py pack --raw <raw dir>
+      On any machine, with the raw directory copied back.  Packs a selection of the raw arrays into tests/golden/<case>.npz
       (float64) and the unmodified executables' snapshots into
       tests/golden/<case>_wfe.npz (float32).
 
