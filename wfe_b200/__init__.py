@@ -12,7 +12,16 @@ in-tree by wfe_b200.build).  It mirrors the reference's operator interface:
 * ``apply_bcs``, ``compute_tendencies``, ``acoustic_substeps``,
   ``update_moisture_stage``, ``kessler_step``, ``sfc_step``,
   ``set_boundary``, ``set_physics``, ``field_absmax`` -- the kernel API of
-  src/dynamics/kernels.hpp:14-71 and src/physics/*.hpp.
+  src/dynamics/kernels.hpp:14-71 and src/physics/*.hpp;
+* ``Ensemble(members)`` -- members of different grids stepped together
+  (batched launches, or the members' own graphs on concurrent streams);
+* ``bdy_weights``, ``clear_boundary`` -- BdyManager's relaxation weights
+  (src/dynamics/boundary.cpp:24-39) and switching the relaxation off.
+
+Beside it: ``wfe_b200.adjoint`` (tangent-linear and adjoint runs, the
+torch.autograd.Function), ``wfe_b200.analysis`` (4D-Var and analysis
+nudging), ``wfe_b200.synth`` (prep-format inputs), ``wfe_b200.shard``
+(ensemble members over ranks).
 
 Arrays are numpy, in the reference's padded layout (NZ, NY, NX) with ng = 3,
 or the Writer's interior layout.  There is no CPU fallback: without the
