@@ -241,6 +241,10 @@ template <typename R>
 int tl_column(const AcouArgs<R>& a, const AcouArgs<R>& d, bool with_forward, cudaStream_t st);
 template <typename R>
 int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st);
+// the same adjoint from the forward launch's outputs still in place (w_out,
+// pi_next) with a.w_in / a.th_in pointing at the launch's inputs
+template <typename R>
+int ad_column_stored(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st);
 template <typename R>
 void tl_kessler(const KesArgs<R>& a, const KesArgs<R>& d, cudaStream_t st);
 template <typename R>

@@ -1060,6 +1060,57 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
   __syncthreads();
 }
 
+// The same values from the forward launch's outputs, for the adjoint sweep
+// when they are still in place (the adjoint runs before the launch's outputs
+// are restored): W is the forward w_out (its level 0 the surface w), P follows
+// from pi_next = P - E (Av(k+1) W(k+1) - Av(k) W(k)) up to rounding, and the
+// rows A, B, C, G from the inputs as before; no Thomas sweep, no right-hand
+// side.  a.w_in and a.th_in must hold the launch's inputs (the undo log's
+// copies where the launch updated them in place).  Ends with a barrier.
+template <typename R>
+__device__ __forceinline__ void column_values_stored_s(const AcouArgs<R>& a, const ColGeom<R>& g, bool active,
+                                                       const ColArr<R>& S) {
+  const Layout& L = a.L;
+  const int nz = g.nz, tx = threadIdx.x, lane = threadIdx.y;
+  const R dtau = g.dtau, c1 = g.c1;
+  R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *W = S[V_W] + tx;
+  R *G = S[V_G] + tx, *A = S[V_A] + tx, *B = S[V_B] + tx, *C = S[V_C] + tx;
+  if (active)
+#pragma unroll 4
+    for (int k = lane; k <= nz; k += kLkl<R>) {
+      const size_t c = g.at(k);
+      Av[k * kLcx<R>] = (k >= 1 && k < nz) ? a.co.aw[c] : (R)0;
+      W[k * kLcx<R>] = k < nz ? a.w_out[c] : (R)0;
+    }
+  __syncthreads();
+  if (active)
+#pragma unroll 4
+    for (int k = lane; k < nz; k += kLkl<R>) {
+      const size_t c = g.at(k);
+      const int q = k * kLcx<R>;
+      const R e = dtau * a.co.kt3[c] * c1 * a.co.inv_dzc[L.at1(k)];
+      E[q] = e;
+      P[q] = a.pi_next[c] + e * (Av[q + kLcx<R>] * W[q + kLcx<R>] - Av[q] * W[q]);
+    }
+  __syncthreads();
+  if (active)
+#pragma unroll 4
+    for (int k = 1 + lane; k < nz; k += kLkl<R>) {
+      const size_t c = g.at(k), cm = c - g.pl;
+      const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
+      R thvw = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
+      if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
+      const R Gk = dtau * Phys<R>::cp * thvw * c1 * iJdz;
+      const int q = k * kLcx<R>;
+      const R Em = E[q - kLcx<R>], Ek = E[q];
+      G[q] = Gk;
+      A[q] = -Gk * Em * Av[q - kLcx<R>];
+      B[q] = (R)1 + Gk * Av[q] * (Ek + Em);
+      C[q] = -Gk * Ek * Av[q + kLcx<R>];
+    }
+  __syncthreads();
+}
+
 enum { T_DSV = V_N, T_DTH, T_DP, T_RHS, T_DW, T_NARR };
 
 template <typename R>
@@ -1184,7 +1235,9 @@ enum { A_WB = V_N, A_PB, A_TB, A_WS, A_LAM, A_GL, A_PIB, A_THB, A_KTD, A_NARR };
 // adjoint of the horizontal divergence, svB the u, v weight of level k (the
 // surface w at level 0, Sv(k) at levels 1..nz-1); k_ad_column_uv takes both
 // to the faces.
-template <typename R>
+// STORED: the forward values from the launch's outputs (column_values_stored_s)
+// instead of recomputing the forward column
+template <typename R, bool STORED = false>
 __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, AcouArgs<R> d, R* dhB, R* svB) {
   extern __shared__ __align__(16) unsigned char lin_smem[];
   const Layout& L = a.L;
@@ -1229,7 +1282,10 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
         tb[q] = d.th_out[c];
       }
     }
-  column_values_s(a, g, active, S);
+  if (STORED)
+    column_values_stored_s(a, g, active, S);
+  else
+    column_values_s(a, g, active, S);
   const R *Av = S[V_AV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx, *G = S[V_G] + tx;
   const R* W = S[V_W] + tx;
   // adjoint of the column solution w (level 0: surface w, level nz: the lid)
@@ -1487,7 +1543,8 @@ template <typename R>
 int lin_prepare(int nz) {
   if (nz > lin_max_levels()) return 2;
   if (raise_smem_limit(k_tl_column<R>, lin_col_smem<R, T_NARR>(nz)) != cudaSuccess ||
-      raise_smem_limit(k_ad_column<R>, lin_col_smem<R, A_NARR>(nz)) != cudaSuccess)
+      raise_smem_limit(k_ad_column<R>, lin_col_smem<R, A_NARR>(nz)) != cudaSuccess ||
+      raise_smem_limit(k_ad_column<R, true>, lin_col_smem<R, A_NARR>(nz)) != cudaSuccess)
     return 1;
   return lin_kessler_prepare<R>(nz);
 }
@@ -1510,6 +1567,16 @@ int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& s
   return 0;
 }
 
+template <typename R>
+int ad_column_stored(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& scr, cudaStream_t st) {
+  if (a.L.nz > lin_max_levels()) return 2;
+  const size_t sm = lin_col_smem<R, A_NARR>(a.L.nz);
+  k_ad_column<R, true><<<dim3((a.L.nx + kLcx<R> - 1) / kLcx<R>, a.L.ny), dim3(kLcx<R>, kLkl<R>), sm, st>>>(
+      a, d, scr.f[0], scr.f[1]);
+  k_ad_column_uv<R><<<grid_uv<R>(a.L), dim3(32, 4, 2), 0, st>>>(a, d, scr.f[0], scr.f[1]);
+  return 0;
+}
+
 #define WFE_INST(R)                                                              \
   template void ad_fill<R>(const FillArgs<R>&, cudaStream_t);                    \
   template void ad_flux<R>(const FluxArgs<R>&, cudaStream_t);                    \
@@ -1519,6 +1586,7 @@ int ad_column(const AcouArgs<R>& a, const AcouArgs<R>& d, const LinScratch<R>& s
   template void ad_uv<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
   template int tl_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, bool, cudaStream_t); \
   template int ad_column<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
+  template int ad_column_stored<R>(const AcouArgs<R>&, const AcouArgs<R>&, const LinScratch<R>&, cudaStream_t); \
   template void zero_ring<R>(R*, const Layout&, cudaStream_t);                        \
   template int copy_fields<R>(const CopyJob<R>&, size_t, cudaStream_t);               \
   template int lin_prepare<R>(int);

@@ -324,6 +324,19 @@ class LinT final : public Lin {
     return 0;
   }
 
+  // The adjoint of a column launch while its outputs (w_out, pi_next,
+  // th_out: undo-log slots base, base + 1, base + 2) still hold the forward
+  // values: w and theta' it updated in place are read from their undo-log
+  // copies, the forward solution from w_out and pi_next (no recomputation).
+  int ad_column_from_outputs(const Rec& r, size_t base) {
+    const auto& a = as<AcouArgs<R>>(r);
+    AcouArgs<R> in = a;
+    if (a.w_in == a.w_out) in.w_in = log_ + base * n3_;
+    if (a.th_in == a.th_out) in.th_in = log_ + (base + 2) * n3_;
+    if (ad_column_stored<R>(in, tr(a), scr_, st_)) return fail("column deeper than the linearised kernels hold");
+    return 0;
+  }
+
   // forward buffers a launch overwrites (saved before it runs)
   static void outputs(const Rec& r, std::vector<R*>* o) {
     o->clear();
@@ -522,7 +535,12 @@ class LinT final : public Lin {
           std::vector<R*> oo;
           for (size_t s = recs.size(); s-- > 0;)
             for (size_t q = recs[s].size(); q-- > 0;) {
-              outputs(recs[s][q], &oo);
+              const Rec& r = recs[s][q];
+              outputs(r, &oo);
+              // a column launch's adjoint runs before its outputs are
+              // restored: it reads the forward solution from them
+              const bool col = r.kind == K_COL;
+              if (col && ad_column_from_outputs(r, slot - oo.size())) return 1;
               CopyJob<R> job{};
               for (size_t z = oo.size(); z-- > 0;) {
                 --slot;
@@ -530,7 +548,7 @@ class LinT final : public Lin {
                 job.dst[job.count++] = oo[z];
               }
               if (copy_fields<R>(job, n3_, st_)) return fail("undo-log copy");
-              if (ad(recs[s][q])) return 1;
+              if (!col && ad(r)) return 1;
             }
           return 0;
         }))
