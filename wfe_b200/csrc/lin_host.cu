@@ -10,16 +10,20 @@
 // TL:  per launch, the TL kernel (forward values still in place) and then the
 //      forward launch; the column's TL launch writes the forward column's
 //      outputs itself, bit for bit.
-// AD:  the forward pass stores the time-n state every `every` steps.  The
-//      reverse sweep takes the segments last to first: it recomputes the
-//      segment storing every step's time-n state, then for each step (last
-//      first) restores its state, replays the step forward while saving the
-//      buffers each launch overwrites (an undo log), and walks the launches
-//      backwards: restore the launch's outputs, run its AD kernel.  A step is
-//      a function of its time-n state alone (every other buffer is written
-//      before it is read), so restoring that state reproduces the step.
-// Cost per step: three forward steps (run, segment recompute, replay), the
-// undo-log copies and the AD kernels.
+// AD:  the forward pass (the model's own graphs) stores the time-n state at
+//      the start of every segment of `every` steps (the last segment is not
+//      run there: its replay below is its forward run).  The reverse sweep
+//      takes the segments last to first: it restores the segment's start
+//      state, replays the segment forward with one graph that saves every
+//      buffer each launch overwrites (an undo log), and walks the launches
+//      backwards with a second graph: restore the launch's outputs from the
+//      log, run its AD kernel -- except the acoustic column, whose adjoint
+//      runs first and reads the forward solution from the outputs still in
+//      place (its inputs updated in place from the log).  A step is a
+//      function of its time-n state alone (every other buffer is written
+//      before it is read), so restoring that state reproduces the segment.
+// Cost per step: the forward pass (all segments but the last), the replay,
+// the undo-log copies and the AD kernels.
 #include <cuda_runtime.h>
 
 #include <cstring>
