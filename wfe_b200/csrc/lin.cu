@@ -17,7 +17,8 @@
 // sweep with the same matrix, right-hand side dD - dM w; the launch also
 // writes the forward column's outputs) and AD (the transposed tridiagonal
 // solve M^T lambda = wbar, then dDbar = lambda, dMbar = -lambda w^T on the
-// three diagonals; its u, v adjoints are gathered per face).
+// three diagonals, with the forward solution taken from the launch's outputs
+// in the adjoint sweep; its u, v adjoints are gathered per face).
 //
 // Output adjoints are cleared only after their values have been used: a
 // store issued while the load of the same address is in flight stalls the
