@@ -269,3 +269,59 @@ def test_gradient_with_interpolated_observations():
         assert abs(fd - an) <= 1e-7 * max(1.0, abs(an)), (fd, an)
     with pytest.raises(ValueError):
         AN.Obs(1, "a", idx, [1.0, 2.0], 1.0, w)  # one row per observation
+
+
+def test_gaussian_correlation_is_symmetric_with_unit_variance():
+    S = AN.GaussianCorrelation(3000.0, 1000.0, 2000.0)
+    rng = np.random.default_rng(17)
+    a, b = rng.standard_normal((2, 4, 30, 40))
+    assert abs(float(np.sum(S.apply("u", a) * b)) - float(np.sum(a * S.apply("u", b)))) <= 1e-10 * a.size
+    w = rng.standard_normal((2, 400, 400))
+    inner = S.apply("u", w)[:, 50:-50, 50:-50]
+    assert abs(inner.var() - 1.0) < 0.05
+    with pytest.raises(ValueError):
+        AN.GaussianCorrelation(0.0, 1.0)
+
+
+def test_correlated_linear_minimiser_is_the_closed_form():
+    """B^1/2 = sigma S: one outer loop with CG to convergence gives
+    x = xb + U (I + U^T G^T R^-1 G U)^-1 U^T G^T R^-1 d"""
+    m, xt, xb, obs = _problem(c=0.0)
+    S = AN.GaussianCorrelation(2.0, 1.0)
+    v = AN.FourDVar(m, xb, {"a": 0.3, "b": 0.2}, obs, corr=S)
+    nctl = v.pack(xb).size
+    r = v.minimise(outer=1, inner=3 * nctl, rtol=1e-13)
+    U = np.array([v._U(e) for e in np.eye(nctl)]).T
+    assert np.allclose(U, U.T, atol=1e-14)
+    G, y, w = [], [], []
+    for o in obs:
+        rows = [o.sample(m.forecast(v.unpack(e), o.step)) for e in np.eye(nctl)]
+        G.append(np.array(rows).T)
+        y.append(o.value - o.sample(m.forecast(xb, o.step)))
+        w.append(1.0 / o.sigma ** 2)
+    G, y, w = np.vstack(G), np.concatenate(y), np.concatenate(w)
+    GU = G @ U
+    chi = np.linalg.solve(np.eye(nctl) + GU.T @ (w[:, None] * GU), GU.T @ (w * y))
+    assert np.allclose(v.pack(r.x), v.pack(xb) + U @ chi, rtol=1e-9, atol=1e-11)
+    assert r.cost[-1] < r.cost[0]
+    # correlated increments are smooth: neighbouring points move together
+    inc = v.pack(r.x) - v.pack(xb)
+    assert np.corrcoef(inc[:-1], inc[1:])[0, 1] > 0.5
+    with pytest.raises(ValueError):
+        v.gradient(xb)
+    with pytest.raises(ValueError):
+        v.minimise(x0=xb)
+
+
+def test_gradient_in_the_control_variable():
+    m, xt, xb, obs = _problem(c=0.15)
+    v = AN.FourDVar(m, xb, 0.3, obs, corr=AN.GaussianCorrelation(1.5, 1.0))
+    rng = np.random.default_rng(23)
+    chi = 0.3 * rng.standard_normal(v.pack(xb).size)
+    j, g = v.gradient_chi(chi)
+    assert j == pytest.approx(v.cost_chi(chi), rel=1e-14)
+    for _ in range(4):
+        d = rng.standard_normal(chi.size)
+        eps = 1e-6
+        fd = (v.cost_chi(chi + eps * d) - v.cost_chi(chi - eps * d)) / (2 * eps)
+        assert abs(fd - float(g @ d)) <= 1e-7 * max(1.0, abs(fd)), (fd, float(g @ d))

@@ -201,6 +201,38 @@ class Obs:
                       (self.weight * np.asarray(r)[:, None]).ravel())
 
 
+class GaussianCorrelation:
+    """Horizontal background-error correlations for ``FourDVar(corr=...)``:
+    S, a separable Gaussian filter of length scale `length` along x (the last
+    axis, spacing dx) and y (the axis before it, spacing dy) on every level,
+    truncated at three length scales and normalised so that S applied to
+    white noise has unit variance.  B^1/2 = sigma S, so B = sigma^2 S S^T
+    correlates like a Gaussian of length sqrt(2) * length.  The filter is
+    zero outside the field, which keeps S symmetric, as the conjugate-
+    gradient inner loop requires."""
+
+    def __init__(self, length: float, dx: float, dy: float | None = None):
+        if not length > 0:
+            raise ValueError("the correlation length must be positive")
+
+        def kernel(d):
+            n = int(np.ceil(3.0 * length / d))
+            t = np.arange(-n, n + 1) * d
+            g = np.exp(-0.5 * (t / length) ** 2)
+            return g / np.sqrt(np.sum(g * g))
+
+        self.gx = kernel(dx)
+        self.gy = kernel(dy if dy is not None else dx)
+
+    def apply(self, name: str, f: np.ndarray) -> np.ndarray:
+        from scipy.ndimage import convolve1d
+
+        out = convolve1d(np.asarray(f, dtype=np.float64), self.gx, axis=-1, mode="constant")
+        if out.ndim >= 2:
+            out = convolve1d(out, self.gy, axis=-2, mode="constant")
+        return out
+
+
 @dataclass
 class Result:
     x: dict
@@ -210,8 +242,15 @@ class Result:
 
 # ---------------------------------------------------------------- 4D-Var
 class FourDVar:
-    def __init__(self, model, xb: dict, sigma_b: dict | float, obs: list):
+    """corr: background-error correlations (an object with a symmetric
+    ``apply(name, field)``, e.g. GaussianCorrelation); None for a diagonal B.
+    With correlations the control variable is chi, x = xb + B^1/2 chi, and
+    J_b = |chi|^2 / 2: the minimisation starts from the background and
+    ``gradient_chi`` gives the gradient in chi."""
+
+    def __init__(self, model, xb: dict, sigma_b: dict | float, obs: list, corr=None):
         self.m = model
+        self.corr = corr
         self.names = tuple(model.names)
         self.xb = {k: np.asarray(xb[k], dtype=np.float64) for k in self.names}
         sb = sigma_b if isinstance(sigma_b, dict) else {k: float(sigma_b) for k in self.names}
@@ -247,6 +286,13 @@ class FourDVar:
             o += n
         return out
 
+    def _U(self, v: np.ndarray) -> np.ndarray:
+        """B^1/2 on a packed control vector (symmetric: also its transpose)"""
+        if self.corr is None:
+            return self._sb_vec() * v
+        f = self.unpack(v)
+        return self.pack({k: self.sb[k] * self.corr.apply(k, f[k]) for k in self.names})
+
     def _sb_vec(self) -> np.ndarray:
         return np.concatenate([np.full(int(self._mask[k].sum()), self.sb[k]) for k in self.names])
 
@@ -266,12 +312,34 @@ class FourDVar:
     def _obs_at(self, t: int) -> list:
         return [o for o in self.obs if o.step == t]
 
+    def _jo(self, traj: dict) -> float:
+        return 0.5 * sum(float(np.sum(((o.sample(traj[o.step]) - o.value) / o.sigma) ** 2))
+                         for o in self.obs)
+
     def cost(self, x0: dict, traj: dict | None = None) -> float:
+        """J(x0) with the diagonal B (no correlations)"""
+        if self.corr is not None:
+            raise ValueError("with correlations J is a function of chi: use cost_chi")
         traj = traj or self.trajectory(x0)
         jb = sum(float(np.sum(((np.asarray(x0[k]) - self.xb[k])[self._mask[k]] / self.sb[k]) ** 2))
                  for k in self.names)
-        jo = sum(float(np.sum(((o.sample(traj[o.step]) - o.value) / o.sigma) ** 2)) for o in self.obs)
-        return 0.5 * (jb + jo)
+        return 0.5 * jb + self._jo(traj)
+
+    def state_of(self, chi: np.ndarray) -> dict:
+        """x = xb + B^1/2 chi"""
+        dx = self.unpack(self._U(chi))
+        return {k: self.xb[k] + dx[k] for k in self.names}
+
+    def cost_chi(self, chi: np.ndarray, traj: dict | None = None) -> float:
+        traj = traj or self.trajectory(self.state_of(chi))
+        return 0.5 * float(chi @ chi) + self._jo(traj)
+
+    def gradient_chi(self, chi: np.ndarray) -> tuple:
+        """(J, dJ/dchi) = (J, chi + B^1/2 M^T H^T R^-1 (H x - y))"""
+        x = self.state_of(chi)
+        traj = self.trajectory(x)
+        lam = self._adjoint_sweep(traj, lambda o: (o.sample(traj[o.step]) - o.value) / o.sigma ** 2)
+        return self.cost_chi(chi, traj), chi + self._U(self.pack(lam))
 
     def _adjoint_sweep(self, traj: dict, forcing) -> dict:
         """sum_k M_k^T H_k^T forcing(o) over the observations: forcing(o) is the
@@ -287,7 +355,9 @@ class FourDVar:
         return lam
 
     def gradient(self, x0: dict) -> tuple:
-        """(J, dJ/dx0) with dJ/dx0 zero off the control points"""
+        """(J, dJ/dx0) with dJ/dx0 zero off the control points (diagonal B)"""
+        if self.corr is not None:
+            raise ValueError("with correlations use gradient_chi")
         traj = self.trajectory(x0)
         lam = self._adjoint_sweep(traj, lambda o: (o.sample(traj[o.step]) - o.value) / o.sigma ** 2)
         g = {k: np.where(self._mask[k], lam[k] + (np.asarray(x0[k]) - self.xb[k]) / self.sb[k] ** 2,
@@ -311,24 +381,29 @@ class FourDVar:
         """Incremental 4D-Var from x0 (default: the background).  Each inner
         loop stops after `inner` CG iterations or when the residual falls
         below rtol times its initial norm."""
+        if self.corr is not None and x0 is not None:
+            raise ValueError("with correlations the minimisation starts from the background")
         x = {k: np.asarray((x0 or self.xb)[k], dtype=np.float64).copy() for k in self.names}
         res = Result(x=x)
         sbv = self._sb_vec()
+        chi_tot = np.zeros_like(sbv)  # with correlations: x = xb + B^1/2 chi_tot
         for _ in range(outer):
             traj = self.trajectory(x)
-            res.cost.append(self.cost(x, traj))
-            # innovations d_k = y_k - H_k x(t_k); background departure b = x - xb
+            res.cost.append(self.cost_chi(chi_tot, traj) if self.corr is not None
+                            else self.cost(x, traj))
+            # innovations d_k = y_k - H_k x(t_k); background departure in chi
             d = {id(o): o.value - o.sample(traj[o.step]) for o in self.obs}
-            bvec = self.pack({k: x[k] - self.xb[k] for k in self.names}) / sbv
+            bvec = (chi_tot if self.corr is not None
+                    else self.pack({k: x[k] - self.xb[k] for k in self.names}) / sbv)
 
             def hess(v):
-                hm = self._tangent_sweep(traj, self.unpack(sbv * v))
+                hm = self._tangent_sweep(traj, self.unpack(self._U(v)))
                 lam = self._adjoint_sweep(traj, lambda o: hm[id(o)] / o.sigma ** 2)
-                return v + sbv * self.pack(lam)
+                return v + self._U(self.pack(lam))
 
             # A chi = -b + B^1/2 M^T H^T R^-1 d
             lam = self._adjoint_sweep(traj, lambda o: d[id(o)] / o.sigma ** 2)
-            rhs = -bvec + sbv * self.pack(lam)
+            rhs = -bvec + self._U(self.pack(lam))
             chi = np.zeros_like(rhs)
             r = rhs.copy()
             p = r.copy()
@@ -347,10 +422,11 @@ class FourDVar:
                 p = r + (rr_new / rr) * p
                 rr = rr_new
             res.inner_residual.append(norms)
-            dx = self.unpack(sbv * chi)
+            chi_tot = chi_tot + chi
+            dx = self.unpack(self._U(chi))
             x = {k: x[k] + dx[k] for k in self.names}
         res.x = x
-        res.cost.append(self.cost(x))
+        res.cost.append(self.cost_chi(chi_tot) if self.corr is not None else self.cost(x))
         return res
 
 
