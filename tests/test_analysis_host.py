@@ -281,6 +281,12 @@ def test_gaussian_correlation_is_symmetric_with_unit_variance():
     assert abs(inner.var() - 1.0) < 0.05
     with pytest.raises(ValueError):
         AN.GaussianCorrelation(0.0, 1.0)
+    # with vertical correlations (level axis) it stays symmetric
+    Sz = AN.GaussianCorrelation(3000.0, 1000.0, 2000.0, levels=2.0)
+    a, b = rng.standard_normal((2, 12, 30, 40))
+    assert abs(float(np.sum(Sz.apply("u", a) * b)) - float(np.sum(a * Sz.apply("u", b)))) <= 1e-10 * a.size
+    wz = rng.standard_normal((60, 60, 60))
+    assert abs(Sz.apply("u", wz)[15:-15, 15:-15, 15:-15].var() - 1.0) < 0.1
 
 
 def test_correlated_linear_minimiser_is_the_closed_form():

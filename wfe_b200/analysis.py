@@ -207,22 +207,24 @@ class GaussianCorrelation:
     axis, spacing dx) and y (the axis before it, spacing dy) on every level,
     truncated at three length scales and normalised so that S applied to
     white noise has unit variance.  B^1/2 = sigma S, so B = sigma^2 S S^T
-    correlates like a Gaussian of length sqrt(2) * length.  The filter is
-    zero outside the field, which keeps S symmetric, as the conjugate-
-    gradient inner loop requires."""
+    correlates like a Gaussian of length sqrt(2) * length.  `levels` > 0
+    adds a Gaussian of that many levels along the level axis (the axis
+    before y, in level indices).  The filter is zero outside the field, which
+    keeps S symmetric, as the conjugate-gradient inner loop requires."""
 
-    def __init__(self, length: float, dx: float, dy: float | None = None):
-        if not length > 0:
-            raise ValueError("the correlation length must be positive")
+    def __init__(self, length: float, dx: float, dy: float | None = None, levels: float = 0.0):
+        if not length > 0 or levels < 0:
+            raise ValueError("correlation lengths must be positive")
 
-        def kernel(d):
-            n = int(np.ceil(3.0 * length / d))
+        def kernel(scale, d):
+            n = int(np.ceil(3.0 * scale / d))
             t = np.arange(-n, n + 1) * d
-            g = np.exp(-0.5 * (t / length) ** 2)
+            g = np.exp(-0.5 * (t / scale) ** 2)
             return g / np.sqrt(np.sum(g * g))
 
-        self.gx = kernel(dx)
-        self.gy = kernel(dy if dy is not None else dx)
+        self.gx = kernel(length, dx)
+        self.gy = kernel(length, dy if dy is not None else dx)
+        self.gz = kernel(levels, 1.0) if levels > 0 else None
 
     def apply(self, name: str, f: np.ndarray) -> np.ndarray:
         from scipy.ndimage import convolve1d
@@ -230,6 +232,8 @@ class GaussianCorrelation:
         out = convolve1d(np.asarray(f, dtype=np.float64), self.gx, axis=-1, mode="constant")
         if out.ndim >= 2:
             out = convolve1d(out, self.gy, axis=-2, mode="constant")
+        if self.gz is not None and out.ndim >= 3:
+            out = convolve1d(out, self.gz, axis=-3, mode="constant")
         return out
 
 
