@@ -9,6 +9,13 @@ is one large RK3 step (3 stages, 1 + 3 + 6 acoustic substeps, Kessler).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+--gpus N > 1 needs N ranks: started under torch.distributed.run (RANK,
+WORLD_SIZE, LOCAL_RANK in the environment) it checks that WORLD_SIZE is N;
+started without a launcher it runs itself again under
+`torch.distributed.run --nproc-per-node N --master-addr 127.0.0.1` and exits
+with that run's status.  It never runs fewer ranks than asked.  --dry-run
+joins the ranks and reports them without touching a GPU (--backend gloo).
+
 ours       K steps replayed from captured CUDA graphs, timed with CUDA events on
            the library's stream, max over ranks; N > 1 runs one independent
            member per GPU (weak scaling, no collective on the data path).
@@ -139,18 +146,43 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n):
+def _free_port() -> int:
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_ranks(n: int) -> int:
+    """--gpus N > 1 started without a launcher: run this command again as N
+    ranks under torch.distributed.run on 127.0.0.1 and return its exit code."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd, timeout=3600).returncode
+
+
+def dist_setup(n, backend="nccl"):
+    """Rank, world size and local rank; the process group for N > 1 ranks.
+    The world size must be the --gpus count: a mismatch is an error, never a
+    silent run on fewer GPUs."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != n:
+        raise SystemExit(f"bench.py: --gpus {n} but the launcher started {world} rank(s)")
     if world > 1:
         import torch
         import torch.distributed as dist
         from datetime import timedelta
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return rank, world, local
 
 
@@ -483,6 +515,8 @@ def adjoint_bench(args, device: int) -> dict:
     x0 = A.get_fields(c)
     A.set_fields(c, x0)
     c.sync()
+    sampler = ClockSampler(device)
+    time.sleep(0.3)
     fwd_ms = c.time_run(K)
     rng = np.random.default_rng(2)
     sc = {"qv": 1e-3, "qc": 1e-3, "qr": 1e-3}
@@ -506,6 +540,7 @@ def adjoint_bench(args, device: int) -> dict:
                 c.tl_run(K)
             t.append(time.perf_counter() - t0)
         times[name] = sorted(t[1:])[1] * 1e3  # median of the three later runs
+    clocks = sampler.stop()
     m = min(K, 10)
     mdx = A.tangent(c, x0, dx, m)
     mty = A.adjoint(c, x0, y, m, every=5)
@@ -525,6 +560,7 @@ def adjoint_bench(args, device: int) -> dict:
         "ad_auto_checkpoint_cost_over_forward": times["ad_auto"] / fwd_ms,
         "dot_test": {"steps": m, "lhs": lhs, "rhs": rhs,
                      "rel_gap": abs(lhs - rhs) / max(abs(lhs), abs(rhs))},
+        "clocks": clocks,
     }
 
 
@@ -538,9 +574,33 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=["wk82", "ensemble24", "adjoint"], default="wk82")
     ap.add_argument("--fp64", action="store_true", help="adjoint workload: FP64 state")
+    ap.add_argument("--backend", default="nccl", help="process-group backend for N > 1 ranks")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="start the ranks, join the process group and report them; no GPU work")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    rank, world, local = dist_setup(args.gpus)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args.gpus))
+    rank, world, local = dist_setup(args.gpus, args.backend)
+
+    if args.dry_run:
+        barrier(world)
+        if world > 1:
+            import torch.distributed as dist
+
+            t = [None] * world
+            dist.all_gather_object(t, rank)
+            ranks = sorted(t)
+        else:
+            ranks = [0]
+        if rank == 0:
+            print(json.dumps({"dry_run": True, "n_gpus": world, "ranks": ranks,
+                              "backend": args.backend if world > 1 else None}), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         if rank == 0:

@@ -262,9 +262,10 @@ int wfe_ensemble_variants(const wfe_ens* ens, int out[3]);
  * qr may be NULL for a dry state; out is a device double.  The call is
  * asynchronous on `stream` (a cudaStream_t, NULL for the legacy stream).
  * nz > WFE_NOALLOC_MAX_LEVELS is rejected with WFE_ERR_ARG and a message in
- * wfe_last_error(NULL).  The first call on a device looks up the array's
- * device address (with that device current); make it before any stream
- * capture.  All calls on a device share the array: calls that overlap on the
+ * wfe_last_error(NULL).  The first call in a CUDA context (normally the
+ * device's primary context) looks up the array's device address in that
+ * context, with the caller's device current; make it before any stream
+ * capture.  All calls in a context share the array: calls that overlap on the
  * GPU (different streams, or other host threads) race and must be serialised
  * by the caller. */
 #define WFE_NOALLOC_MAX_LEVELS 1024

@@ -156,7 +156,7 @@ def pack(raw: Path) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["run", "pack"])
-    ap.add_argument("--raw", default="gpurun_out/golden_raw")
+    ap.add_argument("--raw", required=True, help="directory of the raw reference outputs")
     ap.add_argument("--only-file", action="store_true", help="the file-mode cases only")
     a = ap.parse_args()
     os.chdir(ROOT)

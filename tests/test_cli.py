@@ -85,3 +85,55 @@ def test_cli_file_mode_matches_unmodified_reference_executable(tmp_path):
             ref = W[key].astype(np.float64)
             assert scaled_err(got, ref, floor=1e-12) <= 2.5e-7, (var, step)
     assert f"bitti: {FILE_SMALL_STEPS} adim" in log
+
+
+REF_EXE = ROOT / "oracle" / "_ref" / "wfe_f64"
+
+
+def _run_rc(exe, ini, out, extra, fp64=True):
+    cmd = [str(exe), str(ini), f"out_dir={out}", *extra] + (["--fp64"] if fp64 else [])
+    return subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+
+
+@pytest.mark.gpu
+def test_cli_watchdog_exit_3_with_emergency_snapshot(tmp_path):
+    """|w| above w_abort at the every-10-steps watchdog: the reference prints
+    its HATA line, writes the state at that step and exits 3
+    (src/main.cpp:429-438)."""
+    ini = CASES / "bubble_open.ini"
+    dt = float(re.search(r"^dt\s*=\s*([\d.]+)", ini.read_text(), re.M).group(1))
+    extra = ["w_abort=0.0001", f"t_end={40 * dt}", f"out_interval={100 * dt}",
+             f"diag_interval={100 * dt}"]
+    r = _run_rc(EXE, ini, tmp_path / "out", extra)
+    assert r.returncode == 3, r.stdout + r.stderr
+    assert "esigi asti (adim 10," in r.stderr
+    for var in ("u", "v", "w", "thp", "pip"):
+        assert (tmp_path / "out" / f"{var}_000010.bin").exists(), var
+    assert not (tmp_path / "out" / "w_000020.bin").exists()
+    assert "bitti:" not in r.stdout
+    w = _snap(tmp_path / "out", "w", 10)
+    assert np.isfinite(w).all() and np.abs(w).max() > 1e-4
+    if REF_EXE.exists():  # the unmodified reference executable, same case and threshold
+        rr = _run_rc(REF_EXE, ini, tmp_path / "ref", extra, fp64=False)
+        assert rr.returncode == 3 and "esigi asti (adim 10," in rr.stderr
+        wr = _snap(tmp_path / "ref", "w", 10).astype(np.float64)
+        assert scaled_err(w.astype(np.float64), wr, floor=1e-12) <= 2.5e-7
+
+
+@pytest.mark.gpu
+def test_cli_nan_exit_2(tmp_path):
+    """A non-finite state found by the diagnostics stops the run with exit 2
+    and the reference's HATA line (src/main.cpp:440-455).  The NaN is
+    injected on the host: bubble_dtheta = nan makes theta' NaN inside the
+    bubble of the initial state."""
+    ini = CASES / "bubble_open.ini"
+    dt = float(re.search(r"^dt\s*=\s*([\d.]+)", ini.read_text(), re.M).group(1))
+    extra = ["bubble_dtheta=nan", f"t_end={20 * dt}", f"out_interval={100 * dt}",
+             f"diag_interval={dt}"]
+    r = _run_rc(EXE, ini, tmp_path / "out", extra)
+    assert r.returncode == 2, r.stdout + r.stderr
+    assert "NaN/Inf tespit edildi" in r.stderr
+    assert [ln for ln in r.stdout.splitlines() if ln.startswith("adim")][-1].split()[1] == "1"
+    if REF_EXE.exists():
+        rr = _run_rc(REF_EXE, ini, tmp_path / "ref", extra, fp64=False)
+        assert rr.returncode == 2 and "NaN/Inf tespit edildi" in rr.stderr

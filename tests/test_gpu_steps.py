@@ -198,11 +198,13 @@ def test_acoustic_variants_are_bit_identical(name, prec, monkeypatch):
     """The TMA-staged acoustic column kernel (variant 6) and the fused substep
     kernel that computes its tile's u, v faces itself (variants 7-9: three tile
     shapes, ragged tiles where nx is no multiple of the tile width) and the
-    column kernel with contiguous level chunks per lane (variants 10-12) give
-    the same values, bit for bit, as the u, v kernel + shared-memory column
-    tile kernel (variant 0)."""
+    column kernel with contiguous level chunks per lane (variants 10-12) and
+    the persistent column kernel fed by a pipeline of bulk tensor loads
+    (variants 13-15: 32- and 16-column tiles, two and three stages; ragged
+    tiles, FP64 tiles in shared memory) give the same values, bit for bit, as
+    the u, v kernel + shared-memory column tile kernel (variant 0)."""
     out = {}
-    for v in ("0", "6", "7", "8", "9", "10", "11", "12"):
+    for v in ("0", "6", "7", "8", "9", "10", "11", "12", "13", "14", "15"):
         monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
         c = W.Case(CASES / f"{name}.ini", precision=prec)
         for s in range(4):
@@ -212,7 +214,7 @@ def test_acoustic_variants_are_bit_identical(name, prec, monkeypatch):
         kt = c.kernel_times()  # one more step, timed per kernel: which kernels ran
         assert ("acoustic_fused" in kt) == (v in ("7", "8", "9")), (v, sorted(kt))
         c.close()
-    for v in ("6", "7", "8", "9", "10", "11", "12"):
+    for v in ("6", "7", "8", "9", "10", "11", "12", "13", "14", "15"):
         for k in W.FIELDS:
             assert np.array_equal(out["0"][k], out[v][k]), (v, k)
 

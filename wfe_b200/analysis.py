@@ -226,14 +226,29 @@ class GaussianCorrelation:
         self.gy = kernel(length, dy if dy is not None else dx)
         self.gz = kernel(levels, 1.0) if levels > 0 else None
 
-    def apply(self, name: str, f: np.ndarray) -> np.ndarray:
-        from scipy.ndimage import convolve1d
+    @staticmethod
+    def _filter(a: np.ndarray, g: np.ndarray, axis: int) -> np.ndarray:
+        """sum over s of g[s] a[i + s] along `axis`, zero outside the field
+        (g is symmetric, so this is also the convolution)"""
+        a = np.moveaxis(a, axis, -1)
+        out = np.zeros_like(a)
+        n, m = len(g) // 2, a.shape[-1]
+        for s in range(-n, n + 1):
+            if abs(s) >= m:
+                continue
+            w = g[s + n]
+            if s >= 0:
+                out[..., :m - s] += w * a[..., s:]
+            else:
+                out[..., -s:] += w * a[..., :m + s]
+        return np.moveaxis(out, -1, axis)
 
-        out = convolve1d(np.asarray(f, dtype=np.float64), self.gx, axis=-1, mode="constant")
+    def apply(self, name: str, f: np.ndarray) -> np.ndarray:
+        out = self._filter(np.asarray(f, dtype=np.float64), self.gx, -1)
         if out.ndim >= 2:
-            out = convolve1d(out, self.gy, axis=-2, mode="constant")
+            out = self._filter(out, self.gy, -2)
         if self.gz is not None and out.ndim >= 3:
-            out = convolve1d(out, self.gz, axis=-3, mode="constant")
+            out = self._filter(out, self.gz, -3)
         return out
 
 

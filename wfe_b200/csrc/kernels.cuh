@@ -342,6 +342,31 @@ struct TmaColParams {
   int has_tpi;     // TC_TPI map valid
   CUtensorMap map[TC_N];
 };
+// Persistent, pipelined column kernel (dyn_acou_pipe.cu): one producer warp
+// streams each tile's input boxes (the TC_* fields above, levels 0..nz-1 and
+// w 0..nz) into a ring of shared-memory stages by bulk tensor loads while the
+// consumer warps run the column phases of the tile before; the same
+// expressions as the chunked kernel, bit for bit.  Maps are encoded with the
+// boxes of acoustic_pipe_box for the chosen shape.
+template <typename R>
+struct PipeColParams {
+  AcouArgs<R> a;
+  unsigned* err;   // set to 1 when a stage wait gave up
+  int has_tpi;     // TC_TPI map valid
+  CUtensorMap map[TC_N];
+};
+int acoustic_pipe_shapes();
+// box extents of field f (TC_*) for pipe shape `shape` and nz levels
+void acoustic_pipe_box(int shape, int f, int nz, int* bx, int* by, int* bz);
+// 0 when the shape's stages do not fit in shared memory
+template <typename R>
+size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi);
+// raises every shape's shared-memory limit to the largest layout it may use
+template <typename R>
+int prepare_acoustic_pipe(int nz);
+// Returns 0 ok, 2 does not fit
+template <typename R>
+int launch_acoustic_column_pipe(const PipeColParams<R>& p, int shape, cudaStream_t st);
 // shared memory of the TMA column kernel for nz levels (0: does not fit)
 template <typename R>
 size_t acoustic_column_tma_smem(int nz);

@@ -126,6 +126,7 @@ class ModelT final : public Model {
       return fail("nz too large for the column kernels' shared memory");
     tma_ok_ = tensor_map_encoder() && prepare_acoustic_column_tma<R>(g_.nz) == 0;
     fused_ok_ = prepare_acoustic_fused<R>(g_.nz) == 0;
+    pipe_ok_ = tensor_map_encoder() && prepare_acoustic_pipe<R>(g_.nz) == 0;
     tend_tma_ok_ = tensor_map_encoder() && tend_scal_tma_smem<R>() <= 227 * 1024 &&
                    prepare_tend_scal_tma<R>() == 0;
     CK(cudaMalloc(&tma_err_, sizeof(unsigned)));
@@ -728,7 +729,7 @@ class ModelT final : public Model {
   // the plain column tile shape of the variant in use (the linearised runs
   // launch the unfused kernels)
   int column_shape() const override {
-    if (chunked_index(tune_.column_cx) >= 0) return 0;
+    if (chunked_index(tune_.column_cx) >= 0 || pipe_index(tune_.column_cx) >= 0) return 0;
     const int f = tune_.column_cx - acoustic_column_shapes() - 1;
     return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
   }
@@ -740,6 +741,16 @@ class ModelT final : public Model {
   bool chunked_usable(int v) const {
     const int f = chunked_index(v);
     return f >= 0 && acoustic_chunked_fits<R>(g_.nz, f);
+  }
+  // pipelined column variants follow the chunked ones; -1 for other variants
+  int pipe_index(int v) const {
+    const int f = v - acoustic_column_shapes() - 1 - acoustic_fused_shapes() - acoustic_chunked_shapes();
+    return (f >= 0 && f < acoustic_pipe_shapes()) ? f : -1;
+  }
+  bool pipe_usable(int v) const {
+    const int f = pipe_index(v);
+    return pipe_ok_ && f >= 0 &&
+           acoustic_pipe_smem<R>(f, g_.nz, dp_.moisture != 0, bdy_on_) > 0;
   }
   bool fused_usable(int v) const {
     const int f = v - acoustic_column_shapes() - 1;
@@ -782,7 +793,7 @@ class ModelT final : public Model {
     std::string name = prop.name;
     for (char& ch : name)
       if (ch == ' ') ch = '_';
-    k << "v5|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
+    k << "v6|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
       << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0);
     return k.str();
   }
@@ -816,7 +827,8 @@ class ModelT final : public Model {
 
   // WFE_COLUMN_VARIANT=<n> forces the acoustic variant (0..5 column tile
   // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
-  // tile shapes, 10..12 the chunked column kernel) and WFE_TEND_VARIANT=<n>
+  // tile shapes, 10..12 the chunked column kernel, 13..15 the persistent
+  // pipelined column kernel) and WFE_TEND_VARIANT=<n>
   // the tendency
   // variant (0 fused, 1 split, 2 momentum + TMA-staged scalars) after tuning,
   // for tests and experiments
@@ -827,7 +839,7 @@ class ModelT final : public Model {
     if (first && cv && *cv) {
       const int v = std::atoi(cv);
       if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_) ||
-                     fused_usable(v) || chunked_usable(v)))
+                     fused_usable(v) || chunked_usable(v) || pipe_usable(v)))
         tune_.column_cx = v;
     }
     const char* tv = std::getenv("WFE_TEND_VARIANT");
@@ -868,10 +880,13 @@ class ModelT final : public Model {
     best = 1e30f;
     const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
     // tile shapes, the TMA-staged column, the fused substep kernels
-    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() + acoustic_chunked_shapes();
+    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() +
+                     acoustic_chunked_shapes() + acoustic_pipe_shapes();
     for (int cx = 0; cx < nvar; ++cx) {
       if (cx == acoustic_column_shapes() && !tma_ok_) continue;
-      if (cx > acoustic_column_shapes() && !fused_usable(cx) && !chunked_usable(cx)) continue;
+      if (cx > acoustic_column_shapes() && !fused_usable(cx) && !chunked_usable(cx) &&
+          !pipe_usable(cx))
+        continue;
       float ms;
       tune_.column_cx = cx;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -1080,6 +1095,15 @@ class ModelT final : public Model {
         if (chunked_usable(tune_.column_cx)) {
           const int f = chunked_index(tune_.column_cx);
           launch("acoustic_column", [&] { rc = launch_acoustic_column_chunked<R>(a, f, st_); });
+        } else if (pipe_usable(tune_.column_cx) &&
+                   acoustic_pipe_smem<R>(pipe_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
+                                         a.tpi != nullptr) > 0) {
+          // (operator-level calls add the slow pi' tendency box: when that no
+          // longer fits, the plain column kernel below takes the launch)
+          const int f = pipe_index(tune_.column_cx);
+          PipeColParams<R> pp;
+          if (pipe_params(a, f, &pp)) return 1;
+          launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe<R>(pp, f, st_); });
         } else if (tma_ok_ && tune_.column_cx == acoustic_column_shapes()) {
           TmaColParams<R> tp;
           if (tma_params(a, &tp)) return 1;
@@ -1181,6 +1205,26 @@ class ModelT final : public Model {
       const CUtensorMap* m = tmap(src[f], f);
       if (!m) return 1;
       tp->map[f] = *m;
+    }
+    return 0;
+  }
+
+  int pipe_params(const AcouArgs<R>& a, int shape, PipeColParams<R>* pp) {
+    std::memset(static_cast<void*>(pp), 0, sizeof(*pp));
+    pp->a = a;
+    pp->err = tma_err_;
+    pp->has_tpi = a.tpi != nullptr;
+    const R* src[TC_N] = {a.u_out,  a.co.rtjx, a.v_out, a.co.rtjy, a.w_in,   a.pi_cur,
+                          a.th_in,  a.tw,      a.tth,   a.tpi,     a.co.aw,  a.co.kt3,
+                          a.b.thbw, a.b.dthbdz, a.qv,   a.qc,      a.qr,     a.b.qvb};
+    for (int f = 0; f < TC_N; ++f) {
+      if (f == TC_TPI && !a.tpi) continue;
+      if (f >= TC_QV && !a.p.moisture) continue;
+      int bx, by, bz;
+      acoustic_pipe_box(shape, f, g_.nz, &bx, &by, &bz);
+      const CUtensorMap* m = tmap3(src[f], bx, by, bz);
+      if (!m) return 1;
+      pp->map[f] = *m;
     }
     return 0;
   }
@@ -1429,6 +1473,7 @@ class ModelT final : public Model {
   std::vector<Rec>* rec_ = nullptr;  // record mode when set
   bool tma_ok_ = false;              // TMA column variant usable
   bool fused_ok_ = false;            // fused substep kernels prepared
+  bool pipe_ok_ = false;             // pipelined column kernels prepared
   bool tend_tma_ok_ = false;         // TMA-staged scalar tendencies usable
   unsigned* tma_err_ = nullptr;      // set by a TMA tile load that timed out
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps_;

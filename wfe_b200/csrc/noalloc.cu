@@ -7,7 +7,9 @@
 // wfe_dry_mass_noalloc computes what wfe_dry_mass computes, but its per-level
 // partial sums live in a file-scope __device__ array of at most
 // WFE_NOALLOC_MAX_LEVELS doubles instead of a buffer the library allocates.
-// Every GPU that loads this library holds the array (8 KB) until exit.
+// Every GPU that loads this library holds the array (8 KB) until exit; each
+// CUDA context on a device has its own copy (the address is looked up once
+// per context, on the first call made in it).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -26,9 +28,42 @@ namespace {
 // overwrites the first nz entries before reading them.
 static __device__ __align__(256) double g_noalloc_planes[WFE_NOALLOC_MAX_LEVELS];
 
-constexpr int kMaxDevices = 64;
+// The array's device address belongs to the CUDA context the module was
+// loaded into, so it is cached per context, not per device ordinal: a
+// context created later on the same device (after cudaDeviceReset, or a
+// caller-made driver context) gets its own lookup.
+constexpr int kMaxContexts = 64;
 std::mutex g_mu;
-double* g_planes_addr[kMaxDevices] = {};  // device address of the array, per device
+void* g_ctx[kMaxContexts] = {};
+double* g_planes_addr[kMaxContexts] = {};
+int g_nctx = 0;
+
+using CtxGetCurrent = int (*)(void**);  // cuCtxGetCurrent(CUcontext*), CUresult as int
+
+// The context current on this thread, through the driver entry point the
+// runtime hands out (no link against libcuda needed).
+int current_context(void** ctx) {
+  static CtxGetCurrent fn = nullptr;
+  static std::once_flag once;
+  static cudaError_t init = cudaSuccess;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    init = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+    if (init == cudaSuccess && q != cudaDriverEntryPointSuccess) init = cudaErrorSymbolNotFound;
+    fn = reinterpret_cast<CtxGetCurrent>(f);
+  });
+  if (init != cudaSuccess || !fn) {
+    wfe::set_thread_error(std::string("cuCtxGetCurrent entry point: ") + cudaGetErrorString(init));
+    return WFE_ERR_CUDA;
+  }
+  *ctx = nullptr;
+  if (fn(ctx) != 0) {
+    wfe::set_thread_error("cuCtxGetCurrent failed");
+    return WFE_ERR_CUDA;
+  }
+  return WFE_OK;
+}
 
 // Same arithmetic and reduction order as the library's dry-mass diagnostic,
 // on the reference padded layout (NX = nx + 6, NY = ny + 6, ng = 3).
@@ -66,8 +101,9 @@ __global__ void k_dry_mass_total_ref(const double* planes, int nz, double area, 
   *out = t * area;
 }
 
-// Resolves the array's device address once per device, with that device
-// current (the first call on a device does this).
+// Resolves the array's device address once per context, with the caller's
+// device current (the first call in a context does this; with no context
+// current yet, the device's primary context is made current first).
 int planes_address(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -75,21 +111,37 @@ int planes_address(double** out) {
     wfe::set_thread_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     return WFE_ERR_CUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    wfe::set_thread_error("device index out of range");
-    return WFE_ERR_CUDA;
-  }
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_planes_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_planes);
+  void* ctx = nullptr;
+  int rc = current_context(&ctx);
+  if (rc) return rc;
+  if (!ctx) {
+    e = cudaSetDevice(dev);
     if (e != cudaSuccess) {
-      wfe::set_thread_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      wfe::set_thread_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
       return WFE_ERR_CUDA;
     }
-    g_planes_addr[dev] = static_cast<double*>(p);
+    if ((rc = current_context(&ctx))) return rc;
   }
-  *out = g_planes_addr[dev];
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (int q = 0; q < g_nctx; ++q)
+    if (g_ctx[q] == ctx) {
+      *out = g_planes_addr[q];
+      return WFE_OK;
+    }
+  if (g_nctx == kMaxContexts) {
+    wfe::set_thread_error("wfe_dry_mass_noalloc: more than 64 CUDA contexts");
+    return WFE_ERR_CUDA;
+  }
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_planes);
+  if (e != cudaSuccess) {
+    wfe::set_thread_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return WFE_ERR_CUDA;
+  }
+  g_ctx[g_nctx] = ctx;
+  g_planes_addr[g_nctx] = static_cast<double*>(p);
+  ++g_nctx;
+  *out = static_cast<double*>(p);
   return WFE_OK;
 }
 
