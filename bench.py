@@ -70,6 +70,20 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 CASE = ROOT / "cases" / "wk82_160.ini"
+# The single-case workloads: the headline WK82 case (configs' moist
+# supercell) and the other plain-step configurations, measured the same way
+# (--workload).  (case, description, moist, traffic summary)
+WORKLOADS = {
+    "wk82": ("wk82_160.ini", "WK82 supercell 160x160x40, dx=1 km, 20 km stretched top, moist + "
+             "Kessler, dt=6 s, ns=6", True, "traffic_wk82_160.txt"),
+    "bubble80": ("warm_bubble_80.ini", "dry warm bubble 80x80x40, dx=dy=dz=250 m, open lateral "
+                 "boundaries, Rayleigh layer, dt=1.5 s, ns=6", False, None),
+    "straka512": ("straka_512.ini", "Straka density current 512x4x64, dx=dz=100 m, periodic, "
+                  "K=75 m2/s, dt=0.5 s, ns=6", False, None),
+    "schaer400": ("schaer_400.ini", "Schaer mountain waves 400x4x65, dx=500 m, 20 km top, "
+                  "U=10 m/s, N=0.01/s, dt=4 s, ns=6", False, None),
+}
+WORKLOAD = "wk82"
 METRIC = "RK3 cell-updates/s"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM = 6650.0  # GB/s, used only when MEASURED_PEAKS.json is absent
@@ -90,9 +104,24 @@ KERNEL_FIELDS = {
     "pd_ratio": 8,
     "fill_ghosts": 0,   # surface-area only
 }
+# Dry cases: the moisture fields drop out (column: qv qc qr qv_b; u, v: qv;
+# tendencies: 3 moisture species read twice and written once).
+DRY_KERNEL_FIELDS = dict(KERNEL_FIELDS, acoustic_column=16, acoustic_uv=10, tendencies=13)
 # Per cell and step, the reference-set algorithmic bytes (moist + Kessler, ns=6):
-# 3 x 19 slow-tendency fields + 10 x 26 acoustic fields + 12 Kessler fields.
+# 3 x 19 slow-tendency fields + 10 x 26 acoustic fields + 12 Kessler fields;
+# dry: 3 x 10 + 10 x 22.
 STEP_FIELDS = 3 * 19 + 10 * 26 + 12
+DRY_STEP_FIELDS = 3 * 10 + 10 * 22
+
+
+def use_workload(name: str) -> None:
+    global CASE, WORKLOAD
+    WORKLOAD = name
+    CASE = ROOT / "cases" / WORKLOADS[name][0]
+
+
+def workload_desc() -> str:
+    return WORKLOADS[WORKLOAD][1]
 
 
 def peaks():
@@ -232,7 +261,7 @@ def cpu_baseline(seconds: float = 10.0):
             break
     return {"value": cells * n / el, "unit": "cell-updates/s", "cores": O.threads(),
             "kind": "port",
-            "sample": f"{n} RK3 steps of the full 160x160x40 WK82 case from t=0, FP64 CPU oracle "
+            "sample": f"{n} RK3 steps of the full {o.nx}x{o.ny}x{o.nz} case {CASE.name} from t=0, FP64 CPU oracle "
                       f"(oracle/wfe_oracle.cpp, OpenMP), {el:.1f} s"}
 
 
@@ -252,10 +281,10 @@ def run_reference(args) -> dict:
         "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s",
         "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (analytic WK82 sounding, seeded nothing: deterministic bubble)",
-        "config": {"workload": "WK82 supercell 160x160x40, dx=1 km, 20 km stretched top, "
-                               "moist + Kessler, dt=6 s, ns=6",
-                   "case": "cases/wk82_160.ini", "l2": "per-step working set > L2 (126 MB)"},
+        "data": "synthetic (analytic sounding and initial perturbation of the case, deterministic)",
+        "config": {"workload": workload_desc(), "case": f"cases/{CASE.name}",
+                   "l2": "per-step working set > L2 (126 MB)" if WORKLOAD == "wk82" else
+                         "per-step working set fits in L2 (126 MB)"},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                          "sample": f"{steps} steps of the same case through the reference's own "
                                    "Integrator::step, its CUDA build compiled from its sources "
@@ -572,7 +601,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["wk82", "ensemble24", "adjoint"], default="wk82")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["ensemble24", "adjoint"], default="wk82")
     ap.add_argument("--fp64", action="store_true", help="adjoint workload: FP64 state")
     ap.add_argument("--backend", default="nccl", help="process-group backend for N > 1 ranks")
     ap.add_argument("--dry-run", action="store_true",
@@ -582,6 +611,8 @@ def main():
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(launch_ranks(args.gpus))
     rank, world, local = dist_setup(args.gpus, args.backend)
+    if args.workload in WORKLOADS:
+        use_workload(args.workload)
 
     if args.dry_run:
         barrier(world)
@@ -653,12 +684,16 @@ def main():
     dom = max(kt.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     avg_ms = dom_ms / dom_n
-    alg_bytes = KERNEL_FIELDS.get(dom_name, 0) * 4 * cells
+    moist = WORKLOADS[WORKLOAD][2]
+    kf = KERNEL_FIELDS if moist else DRY_KERNEL_FIELDS
+    step_fields = STEP_FIELDS if moist else DRY_STEP_FIELDS
+    alg_bytes = kf.get(dom_name, 0) * 4 * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "traffic_wk82_160.txt"
-    if tf.exists():
+    tname = WORKLOADS[WORKLOAD][3]
+    tf = ROOT / "profiles" / tname if tname else None
+    if tf is not None and tf.exists():
         for ln in tf.read_text().splitlines():
             parts = ln.split()
             if len(parts) == 2 and not ln.startswith("#") and parts[0] == dom_name:
@@ -686,21 +721,22 @@ def main():
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (analytic WK82 sounding and bubble, deterministic)",
-            "config": {"workload": "WK82 supercell 160x160x40, dx=1 km, 20 km stretched top, "
-                                   "moist + Kessler, dt=6 s, ns=6",
-                       "case": "cases/wk82_160.ini", "precision": "f32",
+            "data": "synthetic (analytic sounding and initial perturbation of the case, deterministic)",
+            "config": {"workload": workload_desc(), "case": f"cases/{CASE.name}", "precision": "f32",
                        "parallelism": f"replicas x{world} (one member per GPU)",
-                       "l2": "no flush: per-step working set ~270 MB > L2 (126 MB)",
+                       "l2": "no flush: per-step working set ~270 MB > L2 (126 MB)"
+                             if WORKLOAD == "wk82" else
+                             "no flush: the per-step working set fits in L2 (126 MB); an "
+                             "L2/launch-bound measurement, not an HBM one",
                        "timing": "CUDA events on the library stream around graph replays"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                          "launches_per_step": dom_n},
-            "step_roofline": {"alg_bytes_per_cell": STEP_FIELDS * 4,
-                              "achieved_gbs": STEP_FIELDS * 4 * cells / (ms_max / args.steps / 1e3) / 1e9,
-                              "frac": STEP_FIELDS * 4 * cells / (ms_max / args.steps / 1e3) / 1e9 / hbm},
+            "step_roofline": {"alg_bytes_per_cell": step_fields * 4,
+                              "achieved_gbs": step_fields * 4 * cells / (ms_max / args.steps / 1e3) / 1e9,
+                              "frac": step_fields * 4 * cells / (ms_max / args.steps / 1e3) / 1e9 / hbm},
             "kernel_ms_per_step": {k: round(v[0], 4) for k, v in kt.items()},
             "kernel_sum_ms": step_kernel_ms,
             "gpu_launches": launches * args.steps,

@@ -56,9 +56,10 @@ def build(verbose: bool = False) -> Path:
     hdr = _headers()
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, hdr, verbose), _sources()))
-    newest = max(o.stat().st_mtime for o in objs)
+    newest = max([o.stat().st_mtime for o in objs] + [(CSRC / "exports.map").stat().st_mtime])
     if not LIB.exists() or LIB.stat().st_mtime < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs),
+               "-Xlinker", f"--version-script={CSRC / 'exports.map'}"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

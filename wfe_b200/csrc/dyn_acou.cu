@@ -162,8 +162,8 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
 // u (v) at an interior face from the cell values beside it: theta_v and pi*
 // at the face's two cells (kernels.cu:499-526)
 template <typename R>
-__device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
-                                            R ps0, R psx) {
+__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
+                                             R ps0, R psx, R uin, R tin) {
   const size_t pl = a.L.plane();
   R thb_f = (R)0.5 * (tvx + tv0);
   R mf = (R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]);
@@ -177,12 +177,18 @@ __device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, size_t c, size
              a.co.inv_dzc2[kk];
     grad -= slope / jf * dpdz;
   }
-  return a.u_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tu[c]);
+  return uin + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin);
 }
 
 template <typename R>
-__device__ __forceinline__ R v_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
-                                            R ps0, R psy) {
+__device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
+                                            R ps0, R psx) {
+  return u_interior_from(a, c, c2, kk, tv0, tvx, ps0, psx, a.u_in[c], a.tu[c]);
+}
+
+template <typename R>
+__device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
+                                             R ps0, R psy, R vin, R tin) {
   const size_t sy = a.L.px, pl = a.L.plane();
   R thb_f = (R)0.5 * (tvy + tv0);
   R mf = (R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]);
@@ -196,7 +202,13 @@ __device__ __forceinline__ R v_interior_val(const AcouArgs<R>& a, size_t c, size
              a.co.inv_dzc2[kk];
     grad -= slope / jf * dpdz;
   }
-  return a.v_in[c] + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + a.tv[c]);
+  return vin + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin);
+}
+
+template <typename R>
+__device__ __forceinline__ R v_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
+                                            R ps0, R psy) {
+  return v_interior_from(a, c, c2, kk, tv0, tvy, ps0, psy, a.v_in[c], a.tv[c]);
 }
 
 // Both faces of an interior point: the cell values at (i,j), (i-1,j) and
@@ -277,26 +289,48 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   const int k = bz * kUvBz + tz;
   const bool has_cell = i < L.nx && j < L.ny && k < L.nz;
   const size_t c = has_cell ? L.at(i, j, k) : 0;
-  R tv0 = 0, ps0 = 0;
+  const size_t sy = L.px;
+  // an interior point's own inputs, and its x (y) neighbour's values when the
+  // neighbour is not in the block, are loaded before the barrier so that
+  // their latency overlaps the shared values' (the same values either way)
+  const bool inner = uv_interior<R>(L, i, j, k);
+  R tv0 = 0, ps0 = 0, uin = 0, tun = 0, vin = 0, tvn = 0, tvx = 0, psx = 0, tvy = 0, psy = 0;
   if (has_cell) {
     tv0 = theta_v_at(a, c);
     ps0 = pistar_at(a, c);
+  }
+  if (inner) {
+    uin = a.u_in[c];
+    tun = a.tu[c];
+    vin = a.v_in[c];
+    tvn = a.tv[c];
+    if (tx == 0) {
+      tvx = theta_v_at(a, c - 1);
+      psx = pistar_at(a, c - 1);
+    }
+    if (ty == 0) {
+      tvy = theta_v_at(a, c - sy);
+      psy = pistar_at(a, c - sy);
+    }
   }
   s_tv[tz][ty][tx] = tv0;
   s_ps[tz][ty][tx] = ps0;
   __syncthreads();
   if (i > L.nx || j > L.ny || k >= L.nz) return;
-  if (uv_interior<R>(L, i, j, k)) {
+  if (inner) {
     // the same values uv_pair_interior loads (kernels.cu:499-526)
-    const size_t sy = L.px;
-    const R tvx = tx > 0 ? s_tv[tz][ty][tx - 1] : theta_v_at(a, c - 1);
-    const R psx = tx > 0 ? s_ps[tz][ty][tx - 1] : pistar_at(a, c - 1);
-    const R tvy = ty > 0 ? s_tv[tz][ty - 1][tx] : theta_v_at(a, c - sy);
-    const R psy = ty > 0 ? s_ps[tz][ty - 1][tx] : pistar_at(a, c - sy);
+    if (tx > 0) {
+      tvx = s_tv[tz][ty][tx - 1];
+      psx = s_ps[tz][ty][tx - 1];
+    }
+    if (ty > 0) {
+      tvy = s_tv[tz][ty - 1][tx];
+      psy = s_ps[tz][ty - 1][tx];
+    }
     const int kk = L.at1(k);
     const size_t c2 = L.at2(i, j);
-    a.u_out[c] = u_interior_val(a, c, c2, kk, tv0, tvx, ps0, psx);
-    a.v_out[c] = v_interior_val(a, c, c2, kk, tv0, tvy, ps0, psy);
+    a.u_out[c] = u_interior_from(a, c, c2, kk, tv0, tvx, ps0, psx, uin, tun);
+    a.v_out[c] = v_interior_from(a, c, c2, kk, tv0, tvy, ps0, psy, vin, tvn);
     return;
   }
   if (j < L.ny) a.u_out[L.at(i, j, k)] = u_face_edge(a, i, j, k);
