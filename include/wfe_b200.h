@@ -133,9 +133,10 @@ long wfe_launches_per_step(const wfe_ctx* ctx);
  * the reference times sections with host clocks under WFE_PROF,
  * src/dynamics/integrator.cpp:18-40). */
 int wfe_time_run(wfe_ctx* ctx, int nsteps, double dt, double t0, double* ms);
-/* One direct step with CUDA events around every kernel launch; per kernel
- * name (comma-separated in names_csv) the summed device time and launch
- * count.  Advances the state like wfe_step. */
+/* One step captured as a CUDA graph with an event node before and after
+ * every kernel launch, replayed once; per kernel name (comma-separated in
+ * names_csv) the summed device time and launch count.  Advances the state
+ * like wfe_step. */
 int wfe_kernel_times(wfe_ctx* ctx, double dt, double t, int cap, double* total_ms, int* counts,
                      char* names_csv, int names_len, int* n_out);
 
@@ -243,9 +244,12 @@ int wfe_ensemble_time_run(wfe_ens* ens, int nsteps, double dt, double t0, double
 /* launches per step; tuned variants: tendencies split, acoustic column tile
  * shape, and the mode (0 batched launches, one block per work item; 1
  * batched on a persistent grid; 2 every member's own graph on its own
- * stream, the members running concurrently).  The first run of 8 or more
- * steps times one step of each mode (after three warm-up steps of each) and
- * keeps the faster: both give the same values, bit for bit. */
+ * stream, the members running concurrently; 3 every member's own graphs,
+ * one member after another).  The first run of 15 or more steps times two
+ * steps of each of the batched, concurrent and one-after-another modes
+ * (after three warm-up steps of each) and keeps the fastest: all give the
+ * same values, bit for bit.  WFE_ENSEMBLE_MODE = batched | members |
+ * sequential forces one. */
 long wfe_ensemble_launches_per_step(const wfe_ens* ens);
 int wfe_ensemble_variants(const wfe_ens* ens, int out[3]);
 

@@ -65,10 +65,11 @@ def _alone(path, prec, n):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-@pytest.mark.parametrize("mode", ["batched", "members", ""])
+@pytest.mark.parametrize("mode", ["batched", "members", "sequential", ""])
 def test_ensemble_equals_members_alone(member_cases, prec, mode, monkeypatch):
-    """batched launches, the members' own graphs on concurrent streams, and
-    the mode the first run picks by timing one step of each ("")"""
+    """batched launches, the members' own graphs on concurrent streams, the
+    members' own graphs one after another, and the mode the first run picks
+    by timing two steps of each ("")"""
     monkeypatch.setenv("WFE_ENSEMBLE_MODE", mode)
     n = 65  # crosses the boundary-file switch at 3600 s
     mem = [W.Case(p, precision=prec) for p in member_cases]

@@ -489,4 +489,4 @@ class Ensemble:
         out = (C.c_int * 3)()
         self._check(self._lib.wfe_ensemble_variants(self._h, out))
         return {"tendencies": out[0], "column_shape": out[1], "persistent": out[2] == 1,
-                "mode": "members" if out[2] == 2 else "batched"}
+                "mode": {2: "members", 3: "sequential"}.get(out[2], "batched")}

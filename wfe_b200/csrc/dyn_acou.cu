@@ -160,24 +160,54 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
 }
 
 // u (v) at an interior face from the cell values beside it: theta_v and pi*
-// at the face's two cells (kernels.cu:499-526)
-template <typename R>
-__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
-                                             R ps0, R psx, R uin, R tin) {
-  const size_t pl = a.L.plane();
+// at the face's two cells (kernels.cu:499-526).  pz(p) gives the pi* values
+// the terrain term needs, p = {pi*(west/south, k+1), pi*(west/south, k-1),
+// pi*(k+1), pi*(k-1)}, from global or from shared memory.
+template <typename R, typename PZ>
+__device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, size_t c2, int kk, R tv0, R tvx, R ps0,
+                                             R psx, R uin, R tin, PZ pz) {
   R thb_f = (R)0.5 * (tvx + tv0);
   R mf = (R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]);
   R grad = (ps0 - psx) * a.co.inv_dx;
   R slope = a.m.hx_u[c2] * a.co.fac_c[kk];
   if (slope != (R)0) {
     R jf = (R)0.5 * (a.m.jac[c2 - 1] + a.m.jac[c2]);
-    R dpdz = (R)0.5 *
-             ((pistar_at(a, c - 1 + pl) - pistar_at(a, c - 1 - pl)) +
-              (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
-             a.co.inv_dzc2[kk];
+    R q[4];
+    pz(q);
+    R dpdz = (R)0.5 * ((q[0] - q[1]) + (q[2] - q[3])) * a.co.inv_dzc2[kk];
     grad -= slope / jf * dpdz;
   }
   return uin + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin);
+}
+
+template <typename R, typename PZ>
+__device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, size_t c2, int kk, R tv0, R tvy, R ps0,
+                                             R psy, R vin, R tin, PZ pz) {
+  const size_t sy = a.L.px;
+  R thb_f = (R)0.5 * (tvy + tv0);
+  R mf = (R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]);
+  R grad = (ps0 - psy) * a.co.inv_dy;
+  R slope = a.m.hy_v[c2] * a.co.fac_c[kk];
+  if (slope != (R)0) {
+    R jf = (R)0.5 * (a.m.jac[c2 - sy] + a.m.jac[c2]);
+    R q[4];
+    pz(q);
+    R dpdz = (R)0.5 * ((q[0] - q[1]) + (q[2] - q[3])) * a.co.inv_dzc2[kk];
+    grad -= slope / jf * dpdz;
+  }
+  return vin + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin);
+}
+
+template <typename R>
+__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
+                                             R ps0, R psx, R uin, R tin) {
+  const size_t pl = a.L.plane();
+  return u_interior_core(a, c2, kk, tv0, tvx, ps0, psx, uin, tin, [&](R* q) {
+    q[0] = pistar_at(a, c - 1 + pl);
+    q[1] = pistar_at(a, c - 1 - pl);
+    q[2] = pistar_at(a, c + pl);
+    q[3] = pistar_at(a, c - pl);
+  });
 }
 
 template <typename R>
@@ -190,19 +220,12 @@ template <typename R>
 __device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
                                              R ps0, R psy, R vin, R tin) {
   const size_t sy = a.L.px, pl = a.L.plane();
-  R thb_f = (R)0.5 * (tvy + tv0);
-  R mf = (R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]);
-  R grad = (ps0 - psy) * a.co.inv_dy;
-  R slope = a.m.hy_v[c2] * a.co.fac_c[kk];
-  if (slope != (R)0) {
-    R jf = (R)0.5 * (a.m.jac[c2 - sy] + a.m.jac[c2]);
-    R dpdz = (R)0.5 *
-             ((pistar_at(a, c - sy + pl) - pistar_at(a, c - sy - pl)) +
-              (pistar_at(a, c + pl) - pistar_at(a, c - pl))) *
-             a.co.inv_dzc2[kk];
-    grad -= slope / jf * dpdz;
-  }
-  return vin + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin);
+  return v_interior_core(a, c2, kk, tv0, tvy, ps0, psy, vin, tin, [&](R* q) {
+    q[0] = pistar_at(a, c - sy + pl);
+    q[1] = pistar_at(a, c - sy - pl);
+    q[2] = pistar_at(a, c + pl);
+    q[3] = pistar_at(a, c - pl);
+  });
 }
 
 template <typename R>
@@ -373,6 +396,186 @@ __global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv(AcouArgs<R
 template <typename R>
 __global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv_batch(Batch<AcouArgs<R>> b) {
   for_each_work(b, [](const AcouArgs<R>& a, int x, int y, int z) { uv_body(a, x, y, z); });
+}
+
+// ------------------------------------------ pipelined forward u, v
+// Persistent CTAs over tiles of kUvpX x kUvpY x kUvpZ faces.  One producer
+// warp streams each tile's boxes into a ring of kUvpStages shared-memory
+// stages (cp.async.bulk.tensor, no multicast, this GPU's own fields): pi',
+// pi'_prev, theta', theta_b and qv with one cell toward -x and -y and one
+// level below and above, and u, tu, v, tv of the tile.  Consumer thread
+// (tx, ty, tz) owns the u and v faces of cell (i0+tx, j0+ty, k0+tz):
+//   * interior faces from shared memory with uv_body's expressions;
+//   * the faces uv_body computes with the generic expressions (levels 0 and
+//     nz-1, u at j = 0, v at i = 0) from shared memory when the column has no
+//     terrain slope there (those expressions, with the same values);
+//   * every other face -- lateral edges with the radiation or periodic
+//     condition, sloped non-interior faces -- and u(nx), v(ny) by the
+//     thread of the cell beside them, with uv_body's global-memory path.
+// Every stage wait is bounded in wall time; on a timeout *err is set.
+constexpr int kUvpStages = 3;
+constexpr int kUvpThreads = kUvpX * kUvpY * kUvpZ;
+constexpr uint64_t kUvpWaitNs = 4000000000ull;
+
+template <typename R>
+struct UvpLayout {
+  size_t field[UV_N];
+  size_t stage0, stage_bytes, total;
+  uint32_t tx_bytes;
+  __host__ __device__ UvpLayout(bool moist) {
+    size_t o = 0;
+    tx_bytes = 0;
+    for (int f = 0; f < UV_N; ++f) {
+      field[f] = 0;
+      if (f == UV_QV && !moist) continue;
+      int bx, by, bz;
+      uv_pipe_box(f, &bx, &by, &bz);
+      const size_t b = (size_t)bx * by * bz * sizeof(R);
+      field[f] = o;
+      o += (b + 127) / 128 * 128;
+      tx_bytes += (uint32_t)b;
+    }
+    stage_bytes = o;
+    stage0 = 128;
+    total = stage0 + (size_t)kUvpStages * stage_bytes;
+  }
+};
+
+template <typename R>
+__global__ void __launch_bounds__(kUvpThreads + 32, 1)
+    k_acoustic_uv_pipe(const __grid_constant__ PipeUvParams<R> p) {
+  extern __shared__ __align__(128) unsigned char smem_uvp[];
+  const AcouArgs<R>& a = p.a;
+  const Layout& L = a.L;
+  const bool moist = a.p.moisture != 0;
+  const UvpLayout<R> lay(moist);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_uvp);
+  uint64_t* empty = full + kUvpStages;
+  const int tid = threadIdx.x;
+  const int ntx = (L.nx + kUvpX - 1) / kUvpX, nty = (L.ny + kUvpY - 1) / kUvpY;
+  const int ntz = (L.nz + kUvpZ - 1) / kUvpZ;
+  const int ntiles = ntx * nty * ntz;
+  if (tid == 0) {
+    for (int s = 0; s < kUvpStages; ++s) {
+      tma::mbar_init(&full[s], 1);
+      tma::mbar_init(&empty[s], 1);
+    }
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid >= kUvpThreads) {
+    // ------------------------------------------------------------ producer
+    if (tid != kUvpThreads) return;
+    int n = 0, armed[kUvpStages];
+    for (int s = 0; s < kUvpStages; ++s) armed[s] = -1;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
+      const int s = n % kUvpStages, use = n / kUvpStages;
+      if (use > 0 && !tma::mbar_wait_for(&empty[s], (use - 1) & 1, kUvpWaitNs)) {
+        atomicExch(p.err, 1u);
+        break;
+      }
+      tma::mbar_arrive_expect_tx(&full[s], lay.tx_bytes);
+      armed[s] = use;
+      unsigned char* stg = smem_uvp + lay.stage0 + (size_t)s * lay.stage_bytes;
+      const int i0 = (t % ntx) * kUvpX, j0 = (t / ntx % nty) * kUvpY, k0 = t / (ntx * nty) * kUvpZ;
+      for (int f = 0; f < UV_N; ++f) {
+        if (f == UV_QV && !moist) continue;
+        const bool halo = f <= UV_QV;
+        tma::load_3d(stg + lay.field[f], &p.map[f], i0 + kOX - (halo ? 4 : 0),
+                     j0 + kOY - (halo ? 1 : 0), k0 + kOZ - (halo ? 1 : 0), &full[s]);
+      }
+    }
+    for (int s = 0; s < kUvpStages; ++s)
+      if (armed[s] >= 0) tma::mbar_wait_for(&full[s], armed[s] & 1, kUvpWaitNs);
+    return;
+  }
+  // -------------------------------------------------------------- consumers
+  const int tx = tid % kUvpX, ty = tid / kUvpX % kUvpY, tz = tid / (kUvpX * kUvpY);
+  constexpr int HX = kUvpX + 4, HY = kUvpY + 1;
+  int n = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
+    const int s = n % kUvpStages, use = n / kUvpStages;
+    const bool ok = tma::mbar_wait_for(&full[s], use & 1, kUvpWaitNs);
+    if (tma::named_or(1, kUvpThreads, !ok)) {
+      if (tid == 0) atomicExch(p.err, 1u);
+      break;
+    }
+    const unsigned char* stg = smem_uvp + lay.stage0 + (size_t)s * lay.stage_bytes;
+    auto fld = [&](int f) { return reinterpret_cast<const R*>(stg + lay.field[f]); };
+    const R* sPI = fld(UV_PI);
+    const R* sPP = fld(UV_PIP);
+    const R* sTH = fld(UV_TH);
+    const R* sTB = fld(UV_THB);
+    const R* sQV = fld(UV_QV);
+    const int i0 = (t % ntx) * kUvpX, j0 = (t / ntx % nty) * kUvpY, k0 = t / (ntx * nty) * kUvpZ;
+    const int i = i0 + tx, j = j0 + ty, k = k0 + tz;
+    // halo-box index of cell (i + dx, j + dy, k + dz)
+    auto hix = [&](int dx, int dy, int dz) { return ((tz + 1 + dz) * HY + (ty + 1 + dy)) * HX + tx + 4 + dx; };
+    auto thv = [&](int h) {  // theta_v_at from shared memory
+      R tv = sTB[h] + sTH[h];
+      if (moist) tv *= (R)1 + Phys<R>::eps61 * sQV[h];
+      return tv;
+    };
+    auto pst = [&](int h) {  // pistar_at from shared memory
+      R cur = sPI[h];
+      return cur + a.p.acoustic_smdiv * (cur - sPP[h]);
+    };
+    R uo = 0, vo = 0;
+    bool u_done = false, v_done = false;
+    const bool cell = i < L.nx && j < L.ny && k < L.nz;
+    if (cell) {
+      const int kk = L.at1(k);
+      const size_t c2 = L.at2(i, j);
+      const int t0 = (tz * kUvpY + ty) * kUvpX + tx;  // tile-box index
+      const int h0 = hix(0, 0, 0);
+      const R tv0 = thv(h0), ps0 = pst(h0);
+      if (uv_interior<R>(L, i, j, k)) {
+        const R tvx = thv(h0 - 1), psx = pst(h0 - 1);
+        const R tvy = thv(h0 - HX), psy = pst(h0 - HX);
+        uo = u_interior_core(a, c2, kk, tv0, tvx, ps0, psx, fld(UV_U)[t0], fld(UV_TU)[t0], [&](R* q) {
+          q[0] = pst(hix(-1, 0, 1));
+          q[1] = pst(hix(-1, 0, -1));
+          q[2] = pst(hix(0, 0, 1));
+          q[3] = pst(hix(0, 0, -1));
+        });
+        vo = v_interior_core(a, c2, kk, tv0, tvy, ps0, psy, fld(UV_V)[t0], fld(UV_TV)[t0], [&](R* q) {
+          q[0] = pst(hix(0, -1, 1));
+          q[1] = pst(hix(0, -1, -1));
+          q[2] = pst(hix(0, 0, 1));
+          q[3] = pst(hix(0, 0, -1));
+        });
+        u_done = v_done = true;
+      } else {
+        // uv_body's generic expressions (u_forward / v_forward) where they
+        // read only this tile's cells and no terrain term
+        if (i >= 1 && a.m.hx_u[c2] * ((R)1 - a.m.zeta_c[kk] / a.m.zt) == (R)0) {
+          R thbu = (R)0.5 * (thv(h0 - 1) + tv0);
+          R mu = (R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]);
+          R grad = (ps0 - pst(h0 - 1)) / a.dx;
+          uo = fld(UV_U)[t0] + a.dtau * (-Phys<R>::cp * thbu * mu * grad + fld(UV_TU)[t0]);
+          u_done = true;
+        }
+        if (j >= 1 && a.m.hy_v[c2] * ((R)1 - a.m.zeta_c[kk] / a.m.zt) == (R)0) {
+          R thbv = (R)0.5 * (thv(h0 - HX) + tv0);
+          R mv = (R)0.5 * (a.m.mapf[c2 - L.px] + a.m.mapf[c2]);
+          R grad = (ps0 - pst(h0 - HX)) / a.dy;
+          vo = fld(UV_V)[t0] + a.dtau * (-Phys<R>::cp * thbv * mv * grad + fld(UV_TV)[t0]);
+          v_done = true;
+        }
+      }
+    }
+    // every input of the tile has been read from shared memory: the producer
+    // may refill the stage
+    tma::named_sync(1, kUvpThreads);
+    if (tid == 0) tma::mbar_arrive(&empty[s]);
+    if (cell) {
+      const size_t c = L.at(i, j, k);
+      a.u_out[c] = u_done ? uo : u_face_edge(a, i, j, k);
+      a.v_out[c] = v_done ? vo : v_face_edge(a, i, j, k);
+      if (i == L.nx - 1) a.u_out[L.at(L.nx, j, k)] = u_face_edge(a, L.nx, j, k);
+      if (j == L.ny - 1) a.v_out[L.at(i, L.ny, k)] = v_face_edge(a, i, L.ny, k);
+    }
+  }
 }
 
 // ------------------------------------------------- implicit w - pi' columns
@@ -1282,7 +1485,46 @@ int occupancy_column(int shape, int nz_max) {
   return e == cudaSuccess && n > 0 ? n : 1;
 }
 
+template <typename R>
+int prepare_acoustic_uv_pipe() {
+  const size_t sm = UvpLayout<R>(true).total;
+  if (sm > 227 * 1024) return 2;
+  return raise_smem_limit(k_acoustic_uv_pipe<R>, sm) == cudaSuccess ? 0 : 1;
+}
+
+template <typename R>
+int launch_acoustic_uv_pipe(const PipeUvParams<R>& p, cudaStream_t st) {
+  const size_t sm = UvpLayout<R>(p.a.p.moisture != 0).total;
+  if (sm > 227 * 1024) return 2;
+  static std::mutex mu;
+  static std::map<std::pair<int, size_t>, int> limit;  // (device, smem) -> resident CTAs
+  int dev = 0, lim = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 2;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = limit.find(std::make_pair(dev, sm));
+    if (it != limit.end()) {
+      lim = it->second;
+    } else {
+      int sms = 0, occ = 0;
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_acoustic_uv_pipe<R>, kUvpThreads + 32,
+                                                        sm) != cudaSuccess)
+        return 2;
+      lim = limit[std::make_pair(dev, sm)] = sms * occ;
+    }
+  }
+  if (lim <= 0) return 2;
+  const Layout& L = p.a.L;
+  const int ntiles = ((L.nx + kUvpX - 1) / kUvpX) * ((L.ny + kUvpY - 1) / kUvpY) *
+                     ((L.nz + kUvpZ - 1) / kUvpZ);
+  k_acoustic_uv_pipe<R><<<ntiles < lim ? ntiles : lim, kUvpThreads + 32, sm, st>>>(p);
+  return 0;
+}
+
 #define WFE_INST(R)                                                                            \
+  template int prepare_acoustic_uv_pipe<R>();                                                  \
+  template int launch_acoustic_uv_pipe<R>(const PipeUvParams<R>&, cudaStream_t);               \
   template size_t acoustic_column_tma_smem<R>(int);                                            \
   template int prepare_acoustic_column_tma<R>(int);                                            \
   template int launch_acoustic_column_tma<R>(const TmaColParams<R>&, cudaStream_t);            \

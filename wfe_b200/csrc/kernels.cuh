@@ -367,6 +367,32 @@ int prepare_acoustic_pipe(int nz);
 // Returns 0 ok, 2 does not fit
 template <typename R>
 int launch_acoustic_column_pipe(const PipeColParams<R>& p, int shape, cudaStream_t st);
+// Persistent, pipelined forward u, v kernel (dyn_acou_pipe.cu): tiles of
+// kUvpX x kUvpY x kUvpZ faces; a producer warp streams each tile's boxes (the
+// cell fields with a one-cell halo toward -x, -y and +-z, the face fields
+// without) into a ring of shared-memory stages; interior faces are computed
+// from shared memory with the u, v kernel's expressions (bit-identical),
+// the lateral edge faces (radiation or periodic) by its global-memory path.
+enum { UV_PI = 0, UV_PIP, UV_TH, UV_THB, UV_QV, UV_U, UV_TU, UV_V, UV_TV, UV_N };
+constexpr int kUvpX = 32, kUvpY = 4, kUvpZ = 4;
+// box extents of map f
+WFE_HD void uv_pipe_box(int f, int* bx, int* by, int* bz) {
+  const bool halo = f <= UV_QV;
+  *bx = halo ? kUvpX + 4 : kUvpX;
+  *by = halo ? kUvpY + 1 : kUvpY;
+  *bz = halo ? kUvpZ + 2 : kUvpZ;
+}
+template <typename R>
+struct PipeUvParams {
+  AcouArgs<R> a;
+  unsigned* err;
+  CUtensorMap map[UV_N];
+};
+template <typename R>
+int prepare_acoustic_uv_pipe();
+// Returns 0 ok, 2 not usable
+template <typename R>
+int launch_acoustic_uv_pipe(const PipeUvParams<R>& p, cudaStream_t st);
 // shared memory of the TMA column kernel for nz levels (0: does not fit)
 template <typename R>
 size_t acoustic_column_tma_smem(int nz);

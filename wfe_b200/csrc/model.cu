@@ -38,7 +38,9 @@ namespace wfe {
 struct Tune {
   int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches, 2 with TMA-staged scalars
   int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
-  int persist = 0;       // ensembles: 0 one block per work item, 1 persistent grid, 2 members' own graphs
+  int persist = 0;       // ensembles: 0 one block per work item, 1 persistent grid, 2 members' own
+                         // graphs on concurrent streams, 3 members' own graphs one after another
+  int uv_variant = 0;    // forward u, v: 0 thread per face, 1 persistent pipelined tiles
   bool done = false;
 };
 
@@ -69,6 +71,7 @@ bool tune_lookup(const std::string& key, Tune* t) {
     Tune v;
     if (ss >> k >> v.tend_variant >> v.column_cx && k == key) {
       if (!(ss >> v.persist)) v.persist = 0;
+      if (!(ss >> v.uv_variant)) v.uv_variant = 0;
       v.done = true;
       g_tune_cache[key] = v;
       *t = v;
@@ -83,7 +86,8 @@ void tune_store(const std::string& key, const Tune& t) {
   g_tune_cache[key] = t;
   // best effort: the cache file is an optimisation only (its directory must exist)
   std::ofstream f(tune_cache_path(), std::ios::app);
-  if (f) f << key << " " << t.tend_variant << " " << t.column_cx << " " << t.persist << "\n";
+  if (f) f << key << " " << t.tend_variant << " " << t.column_cx << " " << t.persist << " "
+           << t.uv_variant << "\n";
 }
 }  // namespace
 
@@ -127,6 +131,7 @@ class ModelT final : public Model {
     tma_ok_ = tensor_map_encoder() && prepare_acoustic_column_tma<R>(g_.nz) == 0;
     fused_ok_ = prepare_acoustic_fused<R>(g_.nz) == 0;
     pipe_ok_ = tensor_map_encoder() && prepare_acoustic_pipe<R>(g_.nz) == 0;
+    uvp_ok_ = tensor_map_encoder() && prepare_acoustic_uv_pipe<R>() == 0;
     tend_tma_ok_ = tensor_map_encoder() && tend_scal_tma_smem<R>() <= 227 * 1024 &&
                    prepare_tend_scal_tma<R>() == 0;
     CK(cudaMalloc(&tma_err_, sizeof(unsigned)));
@@ -489,13 +494,37 @@ class ModelT final : public Model {
     return rc;
   }
 
+  // One step captured into a CUDA graph with an event-record node before and
+  // after every kernel, replayed once: the per-kernel times of a replayed
+  // step (the timed runs replay graphs too), not of direct launches.
   int kernel_times(double dt, double t, std::vector<std::string>* names, std::vector<double>* ms,
                    std::vector<int>* counts) override {
+    if (autotune(dt)) return 1;
+    launch_clock(clock_, t, t_lo_, t_hi_, dt, 0, st_);
     prof_.clear();
     profiling_ = true;
-    int rc = step(dt, t);
+    const int ph = phase_;
+    const int saved[3] = {perm_[0], perm_[1], perm_[2]};
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    launches_ = 1;
+    int rc = enqueue_step((R)dt);
+    cudaError_t ce = cudaStreamEndCapture(st_, &gr);
     profiling_ = false;
     if (rc) return rc;
+    if (ce != cudaSuccess) return fail(std::string("graph capture: ") + cudaGetErrorString(ce));
+    perm_[0] = saved[0];
+    perm_[1] = saved[1];
+    perm_[2] = saved[2];
+    phase_ = ph;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaGraphInstantiate(&ge, gr, 0));
+    cudaGraphDestroy(gr);
+    CK(cudaGraphLaunch(ge, st_));
+    advance_rotation();
+    CK(cudaStreamSynchronize(st_));
+    cudaGraphExecDestroy(ge);
+    if (check_tma()) return 1;
     names->clear();
     ms->clear();
     counts->clear();
@@ -828,10 +857,10 @@ class ModelT final : public Model {
   // WFE_COLUMN_VARIANT=<n> forces the acoustic variant (0..5 column tile
   // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
   // tile shapes, 10..12 the chunked column kernel, 13..15 the persistent
-  // pipelined column kernel) and WFE_TEND_VARIANT=<n>
-  // the tendency
-  // variant (0 fused, 1 split, 2 momentum + TMA-staged scalars) after tuning,
-  // for tests and experiments
+  // pipelined column kernel), WFE_UV_VARIANT=<n> the forward u, v kernel (0
+  // thread per face, 1 persistent pipelined tiles) and WFE_TEND_VARIANT=<n>
+  // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars)
+  // after tuning, for tests and experiments
   int autotune(double dt) {
     const bool first = !tune_.done;
     int rc = autotune_variants(dt);
@@ -841,6 +870,11 @@ class ModelT final : public Model {
       if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_) ||
                      fused_usable(v) || chunked_usable(v) || pipe_usable(v)))
         tune_.column_cx = v;
+    }
+    const char* uvv = std::getenv("WFE_UV_VARIANT");
+    if (first && uvv && *uvv) {
+      const int v = std::atoi(uvv);
+      if (v == 0 || (v == 1 && uvp_ok_)) tune_.uv_variant = v;
     }
     const char* tv = std::getenv("WFE_TEND_VARIANT");
     if (first && tv && *tv) {
@@ -879,6 +913,17 @@ class ModelT final : public Model {
     }
     best = 1e30f;
     const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
+    for (int v = 0; v < (uvp_ok_ ? 2 : 1); ++v) {
+      float ms;
+      tune_.uv_variant = v;
+      if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
+      if (ms < best) {
+        best = ms;
+        cached.uv_variant = v;
+      }
+    }
+    tune_.uv_variant = cached.uv_variant;
+    best = 1e30f;
     // tile shapes, the TMA-staged column, the fused substep kernels
     const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() +
                      acoustic_chunked_shapes() + acoustic_pipe_shapes();
@@ -927,15 +972,15 @@ class ModelT final : public Model {
   template <class F>
   void launch(const char* name, F&& f) {
     ProfRec r{name, nullptr, nullptr};
-    if (profiling_) {
+    if (profiling_) {  // inside a capture: recorded as event nodes of the graph
       cudaEventCreate(&r.e0);
       cudaEventCreate(&r.e1);
-      cudaEventRecord(r.e0, st_);
+      cudaEventRecordWithFlags(r.e0, st_, cudaEventRecordExternal);
     }
     f();
     ++launches_;
     if (profiling_) {
-      cudaEventRecord(r.e1, st_);
+      cudaEventRecordWithFlags(r.e1, st_, cudaEventRecordExternal);
       prof_.push_back(r);
     }
   }
@@ -1089,7 +1134,14 @@ class ModelT final : public Model {
         const int f = tune_.column_cx - acoustic_column_shapes() - 1;
         launch("acoustic_fused", [&] { rc = launch_acoustic_fused<R>(a, f, st_); });
       } else if (!record(K_UV, a)) {
-        launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
+        if (uvp_ok_ && tune_.uv_variant == 1) {
+          PipeUvParams<R> up;
+          if (uv_pipe_params(a, &up)) return 1;
+          launch("acoustic_uv", [&] { rc = launch_acoustic_uv_pipe<R>(up, st_); });
+          if (rc) return fail("pipelined u, v launch");
+        } else {
+          launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
+        }
       }
       if (!fuse && !record(K_COL, a)) {
         if (chunked_usable(tune_.column_cx)) {
@@ -1205,6 +1257,22 @@ class ModelT final : public Model {
       const CUtensorMap* m = tmap(src[f], f);
       if (!m) return 1;
       tp->map[f] = *m;
+    }
+    return 0;
+  }
+
+  int uv_pipe_params(const AcouArgs<R>& a, PipeUvParams<R>* up) {
+    std::memset(static_cast<void*>(up), 0, sizeof(*up));
+    up->a = a;
+    up->err = tma_err_;
+    const R* src[UV_N] = {a.pi_cur, a.pi_prev, a.th_in, a.b.thb, a.qv, a.u_in, a.tu, a.v_in, a.tv};
+    for (int f = 0; f < UV_N; ++f) {
+      if (f == UV_QV && !a.p.moisture) continue;
+      int bx, by, bz;
+      uv_pipe_box(f, &bx, &by, &bz);
+      const CUtensorMap* m = tmap3(src[f], bx, by, bz);
+      if (!m) return 1;
+      up->map[f] = *m;
     }
     return 0;
   }
@@ -1474,6 +1542,7 @@ class ModelT final : public Model {
   bool tma_ok_ = false;              // TMA column variant usable
   bool fused_ok_ = false;            // fused substep kernels prepared
   bool pipe_ok_ = false;             // pipelined column kernels prepared
+  bool uvp_ok_ = false;              // pipelined u, v kernel prepared
   bool tend_tma_ok_ = false;         // TMA-staged scalar tendencies usable
   unsigned* tma_err_ = nullptr;      // set by a TMA tile load that timed out
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps_;
@@ -1528,50 +1597,68 @@ class EnsembleT final : public Ensemble {
     if (begin(dt)) return 1;
     for (auto* x : mem_) launch_clock(x->clock_ptr(), t0, x->bdy_t_lo(), x->bdy_t_hi(), dt, 0, st_);
     int s = 0;
-    const char* em = std::getenv("WFE_ENSEMBLE_MODE");  // "members" | "batched": no timing
+    // "members" | "sequential" | "batched": no timing
+    const char* em = std::getenv("WFE_ENSEMBLE_MODE");
     if (em && *em) {
       mode_done_ = true;
-      tune_.persist = std::string(em) == "members" ? 2 : ((tune_.persist & 1) | 4);
+      const std::string m(em);
+      tune_.persist = m == "members" ? 2 : (m == "sequential" ? 3 : ((tune_.persist & 1) | 4));
     }
-    if (!mode_done_ && nsteps >= 8) {
-      // pick between the batched launches and the members' own graphs on
-      // their own streams on real steps (both give the same values, bit for
-      // bit): three warm-up steps of each mode capture every phase's graphs,
-      // then one timed step each
-      float tb = 0, tc = 0;
-      if (batched_steps(3, dt) || timed([&] { return batched_steps(1, dt); }, &tb)) return 1;
-      if (member_steps(3, dt) || timed([&] { return member_steps(1, dt); }, &tc)) return 1;
-      s = 8;
+    if (!mode_done_ && nsteps >= 15) {
+      // pick on real steps among the batched launches, the members' own
+      // graphs on concurrent streams and the members' own graphs one after
+      // another (all three give the same values, bit for bit): three warm-up
+      // steps of each mode capture every phase's graphs, then two timed
+      // steps each
+      float tb = 0, tc = 0, tq = 0;
+      if (batched_steps(3, dt) || timed([&] { return batched_steps(2, dt); }, &tb)) return 1;
+      if (member_steps(3, dt, false) || timed([&] { return member_steps(2, dt, false); }, &tc)) return 1;
+      if (member_steps(3, dt, true) || timed([&] { return member_steps(2, dt, true); }, &tq)) return 1;
+      s = 15;
       mode_done_ = true;
-      tune_.persist = tc < tb ? 2 : ((tune_.persist & 1) | 4);
+      if (tc <= tb && tc <= tq) tune_.persist = 2;
+      else if (tq <= tb) tune_.persist = 3;
+      else tune_.persist = (tune_.persist & 1) | 4;
       tune_store(tune_key(), tune_);
     }
-    if (tune_.persist == 2) {
-      if (member_steps(nsteps - s, dt)) return 1;
+    if (tune_.persist == 2 || tune_.persist == 3) {
+      if (member_steps(nsteps - s, dt, tune_.persist == 3)) return 1;
       return 0;
     }
     if (batched_steps(nsteps - s, dt)) return 1;
     return finish();
   }
 
-  // members' own graphs, each on its own stream, interleaved step by step;
-  // ordered after the ensemble stream's work, and the ensemble stream after them
-  int member_steps(int nsteps, double dt) {
+  // members' own graphs, each on its own stream, ordered after the ensemble
+  // stream's work, and the ensemble stream after them: interleaved step by
+  // step so that the members run concurrently, or (sequential) each member's
+  // steps after the previous member's, as a serial run of the members does
+  int member_steps(int nsteps, double dt, bool sequential) {
     CK(cudaEventRecord(ev_, st_));
     for (auto* x : mem_) {
       CK(cudaStreamWaitEvent(x->stream(), ev_, 0));
       if (x->tune_for(dt)) return fail(x->error());
     }
-    for (int s = 0; s < nsteps; ++s)
-      for (auto* x : mem_)
-        if (x->graph_steps(1, dt)) return fail(x->error());
+    if (sequential) {
+      for (size_t q = 0; q < mem_.size(); ++q) {
+        if (q > 0) {
+          CK(cudaEventRecord(ev_, mem_[q - 1]->stream()));
+          CK(cudaStreamWaitEvent(mem_[q]->stream(), ev_, 0));
+        }
+        if (mem_[q]->graph_steps(nsteps, dt)) return fail(mem_[q]->error());
+      }
+    } else {
+      for (int s = 0; s < nsteps; ++s)
+        for (auto* x : mem_)
+          if (x->graph_steps(1, dt)) return fail(x->error());
+    }
     long l = 0;
     for (auto* x : mem_) {
       CK(cudaEventRecord(ev_, x->stream()));
       CK(cudaStreamWaitEvent(st_, ev_, 0));
       l += x->launches_per_step();
     }
-    if (tune_.persist == 2) launches_ = l;
+    if (tune_.persist == 2 || tune_.persist == 3) launches_ = l;
     return 0;
   }
 
@@ -1649,7 +1736,7 @@ class EnsembleT final : public Ensemble {
   void variants(int* tend, int* column, int* persist) const override {
     *tend = tune_.tend_variant;
     *column = tune_.column_cx;
-    *persist = tune_.persist & 3;
+    *persist = (tune_.persist & 4) ? (tune_.persist & 1) : tune_.persist;
   }
 
  private:
@@ -1830,7 +1917,7 @@ class EnsembleT final : public Ensemble {
     std::string name = prop.name;
     for (char& ch : name)
       if (ch == ' ') ch = '_';
-    k << "ens1|" << name << "|" << (sizeof(R) * 8) << "|" << mem_[0]->batch_signature();
+    k << "ens2|" << name << "|" << (sizeof(R) * 8) << "|" << mem_[0]->batch_signature();
     for (auto* x : mem_) k << "|" << x->layout().nx << "x" << x->layout().ny << "x" << x->layout().nz;
     return k.str();
   }
@@ -1847,7 +1934,7 @@ class EnsembleT final : public Ensemble {
     Tune cached;
     if (tune_lookup(key, &cached)) {
       tune_ = cached;
-      mode_done_ = tune_.persist == 2 || (tune_.persist & 4);
+      mode_done_ = tune_.persist == 2 || tune_.persist == 3 || (tune_.persist & 4);
       return 0;
     }
     int upto = -1;
