@@ -300,3 +300,44 @@ def test_cases_of_different_depths_share_the_kernels(monkeypatch):
         assert np.array_equal(a.field(k), ref.field(k)), k
     for c in (a, ref, shallow):
         c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "bubble_open", "straka_periodic",
+                                  "ops_periodic", "moist_blob"])
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-11), ("f32", 1e-5)])
+def test_parallel_solve_column_agrees_to_rounding(name, prec, tol, monkeypatch):
+    """The column kernels with the parallel tridiagonal solve (variants 16-18:
+    each level lane eliminates its own rows, cyclic reduction over the lanes)
+    solve the same rows as the Thomas-sweep kernels: after seven steps the
+    fields agree to rounding -- relative L2 <= 1e-11 (FP64) / 1e-5 (FP32) of
+    the field (u, v against the wind-speed scale) -- and the FP64 steps stay
+    within 1e-10 of the FP64 oracle."""
+    out = {}
+    variants = ["0"] + [v for v in ("16", "17", "18")]
+    for v in variants:
+        monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
+        c = W.Case(CASES / f"{name}.ini", precision=prec)
+        c.run(7, c.dt, 0.0)
+        c.sync()
+        out[v] = {k: c.field(k) for k in W.FIELDS}
+        kt = c.kernel_times()
+        assert "acoustic_column" in kt
+        c.close()
+    ref = out["0"]
+    speed = max(np.abs(ref["u"]).max(), np.abs(ref["v"]).max(), 1e-30)
+    for v in variants[1:]:
+        for k in W.FIELDS:
+            a, b = out[v][k], ref[k]
+            if k in ("u", "v"):
+                err = np.sqrt(((a - b) ** 2).mean()) / speed
+            else:
+                err = rel_l2(a, b) if np.abs(b).max() > 0 else np.abs(a).max()
+            assert err <= tol, (v, k, err)
+    if prec == "f64":
+        o, it = _oracle_run(name, 7)
+        for k in W.FIELDS:
+            c = W.Case(CASES / f"{name}.ini", precision="f64", device=-1)
+            e = scaled_err(_interior(c, out["16"][k], k), _interior(o, it.field(k), k))
+            c.close()
+            assert e <= 1e-10, (k, e)

@@ -948,6 +948,248 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
 #undef SQ
 }
 
+// Column variant with a parallel tridiagonal solve.  Level lane p owns the
+// KCH levels klo = p KCH .. klo + KCH - 1 (in registers); the system is
+// padded with identity rows (x = 0) at level 0, the lid and above it, which
+// leaves the solution unchanged (the rows beside them couple to them with
+// zero coefficients: A at level 1 and C at level nz - 1 multiply aw = 0), so
+// every lane has exactly KCH rows.  Instead of one lane sweeping the whole
+// column while the others wait, every lane works:
+//   1. it eliminates its first KCH - 1 rows, with its last row's unknown
+//      y_p and the previous lane's y_{p-1} as parameters: x_k = G_k +
+//      A_k y_{p-1} + B_k y_p (one Thomas pass, three right-hand sides);
+//   2. its last row, with the first-row expression of the lane above,
+//      becomes one row L y_{p-1} + M y_p + U y_{p+1} = F of a tridiagonal
+//      system in the lanes' y_p;
+//   3. that system is solved by parallel cyclic reduction over the level
+//      lanes through shared memory (log2(KL) steps), and each lane recovers
+//      its rows from y_{p-1} and y_p.
+// Phases 1-3 and 5 are the chunked kernel's expressions; the solution differs
+// from the serial Thomas sweep by rounding only (a different elimination
+// order), so this variant is not bit-identical to the other column kernels.
+template <typename R, int CX, int KL, int KCH>
+__global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_column_pcr(AcouArgs<R> a) {
+  static_assert(KCH >= 2, "every lane needs an interior row");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Layout& L = a.L;
+  const int nz = L.nz;
+  // shared arrays, [lane][column]: the first-row expressions (G, A, B), the
+  // reduced rows (L, M, U, F, double-buffered) and the lanes' y
+  constexpr int NL = KL * CX;
+  R* fG = reinterpret_cast<R*>(smem_raw);
+  R* fA = fG + NL;
+  R* fB = fA + NL;
+  R* red = fB + NL;
+  R* yv = red + 8 * NL;
+  const int tx = threadIdx.x, lane = threadIdx.y;
+  const int me = lane * CX + tx;
+  const int i = blockIdx.x * CX + tx, j = blockIdx.y;
+  const bool active = i < L.nx;
+  const R dtau = a.dtau;
+  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
+  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
+  const size_t c2d = L.at2(active ? i : 0, j);
+  const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
+  const R invJ = (R)1 / J;
+  const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
+  const bool terrain = hxc != (R)0 || hyc != (R)0;
+  const size_t sx = 1, sy = L.px, pl = L.plane();
+  const size_t c0 = L.at(active ? i : 0, j, 0);
+  const R* __restrict__ u = a.u_out;
+  const R* __restrict__ v = a.v_out;
+  const int klo = lane * KCH;
+  R av[KCH + 2], sv[KCH + 2], P[KCH + 1], E[KCH + 1], th[KCH + 1], tt[KCH + 1], db[KCH + 1];
+  R Ar[KCH + 1], Br[KCH + 1], Cr[KCH + 1], Dr[KCH + 1];
+  R wsurf = 0;
+#pragma unroll
+  for (int q = 0; q < KCH + 1; ++q) Ar[q] = 0, Br[q] = 1, Cr[q] = 0, Dr[q] = 0;
+  if (active) {
+    // phase 1 on levels klo-1 .. klo+KCH
+#pragma unroll
+    for (int q = 0; q < KCH + 2; ++q) {
+      const int k = klo - 1 + q;
+      R avk = 0, svk = 0;
+      if (k >= 1 && k < nz) {
+        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        avk = a.co.aw[c];
+        if (terrain) {
+          R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
+          R vw = (R)0.25 * (v[cm] + v[cm + sy] + v[c] + v[c + sy]);
+          svk = avk * (uw * hxc + vw * hyc) * a.co.fac_w[L.at1(k)];
+        }
+      }
+      av[q] = avk;
+      sv[q] = svk;
+    }
+    // phase 2 on levels klo-1 .. klo+KCH-1
+#pragma unroll
+    for (int q = 0; q < KCH + 1; ++q) {
+      const int k = klo - 1 + q;
+      R pk = 0, ek = 0;
+      if (k >= 0 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = c0 + (size_t)k * pl;
+        R Kt = a.co.kt3[c];
+        R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * mcx +
+               (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * mcy;
+        R idz = a.co.inv_dzc[kk];
+        R wk = a.w_in[c], wkp = a.w_in[c + pl];
+        R tpi = a.tpi ? a.tpi[c] : (R)0;
+        pk = a.pi_cur[c] + dtau * tpi -
+             dtau * Kt * (Dh - (sv[q + 1] - sv[q]) * idz + c2 * (av[q + 1] * wkp - av[q] * wk) * idz);
+        ek = dtau * Kt * c1 * idz;
+      }
+      P[q] = pk;
+      E[q] = ek;
+    }
+    // phase 3: rows of the inner levels, and phase 5's inputs
+#pragma unroll
+    for (int q = 1; q < KCH + 1; ++q) {
+      const int k = klo - 1 + q;
+      th[q] = tt[q] = db[q] = 0;
+      if (k < nz) {
+        const size_t c = c0 + (size_t)k * pl;
+        th[q] = a.th_in[c];
+        tt[q] = a.tth[c];
+        db[q] = a.b.dthbdz[c];
+      }
+      if (k >= 1 && k < nz) {
+        const int kk = L.at1(k);
+        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const R iJdz = invJ * a.co.inv_dzw[kk];
+        R thc = th[q], thm = a.th_in[cm];
+        R thbw = a.b.thbw[c];
+        R thvw = thbw + (R)0.5 * (thm + thc);
+        if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
+        R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
+        R Em = E[q - 1], Ek = E[q];
+        Ar[q] = -G * Em * av[q - 1];
+        Br[q] = (R)1 + G * av[q] * (Ek + Em);
+        Cr[q] = -G * Ek * av[q + 1];
+        R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
+        if (a.p.moisture) {
+          R dqv = (R)0.5 * (a.qv[cm] + a.qv[c]) - (R)0.5 * (a.b.qvb[cm] + a.b.qvb[c]);
+          R qcr = (R)0.5 * (a.qc[cm] + a.qc[c]) + (R)0.5 * (a.qr[cm] + a.qr[c]);
+          buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
+        }
+        R RHS = a.w_in[c] + dtau * (buoy + a.tw[c]) -
+                dtau * Phys<R>::cp * thvw * c2 * (a.pi_cur[c] - a.pi_cur[cm]) * iJdz;
+        Dr[q] = RHS - G * (P[q] - P[q - 1]);
+      }
+    }
+    if (lane == 0) {  // diagnostic surface w from the new u, v
+      R us = (R)0.5 * (u[c0] + u[c0 + sx]);
+      R vs = (R)0.5 * (v[c0] + v[c0 + sy]);
+      wsurf = us * hxc + vs * hyc;
+    }
+  }
+  // ---- 1. rows 1 .. KCH-1 in terms of (y_{p-1}, y_p)
+  R Gx[KCH + 1], Ax[KCH + 1], Bx[KCH + 1];
+  {
+    R cp[KCH], gp[KCH], ap[KCH], bp[KCH];
+#pragma unroll
+    for (int q = 1; q < KCH; ++q) {
+      const R r = (R)1 / (Br[q] - Ar[q] * (q > 1 ? cp[q - 1] : (R)0));
+      cp[q] = q == KCH - 1 ? (R)0 : Cr[q] * r;
+      gp[q] = (Dr[q] - Ar[q] * (q > 1 ? gp[q - 1] : (R)0)) * r;
+      ap[q] = ((q == 1 ? -Ar[q] : (R)0) - Ar[q] * (q > 1 ? ap[q - 1] : (R)0)) * r;
+      bp[q] = ((q == KCH - 1 ? -Cr[q] : (R)0) - Ar[q] * (q > 1 ? bp[q - 1] : (R)0)) * r;
+    }
+#pragma unroll
+    for (int q = KCH - 1; q >= 1; --q) {
+      if (q == KCH - 1) {
+        Gx[q] = gp[q], Ax[q] = ap[q], Bx[q] = bp[q];
+      } else {
+        Gx[q] = gp[q] - cp[q] * Gx[q + 1];
+        Ax[q] = ap[q] - cp[q] * Ax[q + 1];
+        Bx[q] = bp[q] - cp[q] * Bx[q + 1];
+      }
+    }
+  }
+  fG[me] = Gx[1];
+  fA[me] = Ax[1];
+  fB[me] = Bx[1];
+  __syncthreads();
+  // ---- 2. the lane's row of the reduced system: its last row with x of the
+  // row below it (this lane's row KCH - 1) and of the row above it (the
+  // first row of the lane above; none above the top lane)
+  R gn = 0, an = 0, bn = 0;
+  if (lane + 1 < KL) {
+    gn = fG[me + CX];
+    an = fA[me + CX];
+    bn = fB[me + CX];
+  }
+  R Lr = Ar[KCH] * Ax[KCH - 1];
+  R Mr = Br[KCH] + Ar[KCH] * Bx[KCH - 1] + Cr[KCH] * an;
+  R Ur = Cr[KCH] * bn;
+  R Fr = Dr[KCH] - Ar[KCH] * Gx[KCH - 1] - Cr[KCH] * gn;
+  // ---- 3. parallel cyclic reduction over the lanes
+  R* buf = red;
+  buf[me] = Lr;
+  buf[NL + me] = Mr;
+  buf[2 * NL + me] = Ur;
+  buf[3 * NL + me] = Fr;
+  __syncthreads();
+#pragma unroll
+  for (int h = 1; h < KL; h *= 2) {
+    R* nb = buf == red ? red + 4 * NL : red;
+    R al = 0, ga = 0, Lm = 0, Um = 0, Fm = 0, Lp = 0, Up = 0, Fp = 0;
+    if (lane - h >= 0) {
+      const int o = me - h * CX;
+      al = -Lr / buf[NL + o];
+      Lm = buf[o];
+      Um = buf[2 * NL + o];
+      Fm = buf[3 * NL + o];
+    }
+    if (lane + h < KL) {
+      const int o = me + h * CX;
+      ga = -Ur / buf[NL + o];
+      Lp = buf[o];
+      Up = buf[2 * NL + o];
+      Fp = buf[3 * NL + o];
+    }
+    Mr = Mr + al * Um + ga * Lp;
+    Fr = Fr + al * Fm + ga * Fp;
+    Lr = al * Lm;
+    Ur = ga * Up;
+    nb[me] = Lr;
+    nb[NL + me] = Mr;
+    nb[2 * NL + me] = Ur;
+    nb[3 * NL + me] = Fr;
+    buf = nb;
+    __syncthreads();
+  }
+  const R y = Fr / Mr;
+  yv[me] = y;
+  __syncthreads();
+  const R yprev = lane > 0 ? yv[me - CX] : (R)0;
+  const R ynext = lane + 1 < KL ? yv[me + CX] : (R)0;
+  // ---- phase 5: pi', theta', w of the lane's levels
+  if (active) {
+    R wl[KCH + 2];  // w at the lane's levels and the level above them
+#pragma unroll
+    for (int q = 1; q < KCH; ++q) wl[q] = Gx[q] + Ax[q] * yprev + Bx[q] * y;
+    wl[KCH] = y;
+    wl[KCH + 1] = gn + an * y + bn * ynext;
+    if (lane == 0) wl[1] = wsurf;  // level 0: the diagnostic surface w
+#pragma unroll
+    for (int q = 1; q < KCH + 1; ++q) {
+      const int k = klo - 1 + q;
+      if (k > nz) continue;
+      const size_t c = c0 + (size_t)k * pl;
+      if (k == nz) {
+        a.w_out[c] = 0;
+        continue;
+      }
+      const R wn = wl[q], wn1 = k + 1 >= nz ? (R)0 : wl[q + 1];
+      a.pi_next[c] = P[q] - E[q] * (av[q + 1] * wn1 - av[q] * wn);
+      R wc = (R)0.5 * (wn + wn1);
+      a.th_out[c] = th[q] + dtau * (tt[q] - wc * db[q]);
+      a.w_out[c] = wn;
+    }
+  }
+}
+
 // The whole substep in one launch: a CTA first computes the u faces
 // i0..i0+CX of its row and the v faces of rows j and j+1 of its columns with
 // uv_body's arithmetic into shared tiles (storing the faces it owns: u faces
@@ -1462,6 +1704,38 @@ int launch_acoustic_column_chunked(const AcouArgs<R>& a, int f, cudaStream_t st)
   return 0;
 }
 
+// Shapes of the parallel-solve column kernel: columns, level lanes, largest chunk
+static const int kPcrShapes[][3] = {{32, 16, 3}, {16, 32, 3}, {32, 16, 4}};
+constexpr int kNumPcrShapes = 3;
+
+int acoustic_pcr_shapes() { return kNumPcrShapes; }
+
+template <typename R>
+size_t pcr_smem(int cx, int kl) {
+  return (size_t)12 * cx * kl * sizeof(R);
+}
+
+template <typename R>
+bool acoustic_pcr_fits(int nz, int f) {
+  return f >= 0 && f < kNumPcrShapes && nz + 1 <= kPcrShapes[f][1] * kPcrShapes[f][2] &&
+         pcr_smem<R>(kPcrShapes[f][0], kPcrShapes[f][1]) <= 48 * 1024;
+}
+
+// f: index into the parallel-solve shapes.  Returns 0 ok, 2 does not fit.
+template <typename R>
+int launch_acoustic_column_pcr(const AcouArgs<R>& a, int f, cudaStream_t st) {
+  if (!acoustic_pcr_fits<R>(a.L.nz, f)) return 2;
+  const int cx = kPcrShapes[f][0], kl = kPcrShapes[f][1];
+  const size_t sm = pcr_smem<R>(cx, kl);
+  const dim3 grd((a.L.nx + cx - 1) / cx, a.L.ny, 1), blk(cx, kl);
+  switch (f) {
+    case 0: k_acoustic_column_pcr<R, 32, 16, 3><<<grd, blk, sm, st>>>(a); break;
+    case 1: k_acoustic_column_pcr<R, 16, 32, 3><<<grd, blk, sm, st>>>(a); break;
+    default: k_acoustic_column_pcr<R, 32, 16, 4><<<grd, blk, sm, st>>>(a); break;
+  }
+  return 0;
+}
+
 // the plain column tile shape of fused shape f
 int acoustic_fused_column_shape(int f) {
   return (f >= 0 && f < kNumFusedShapes) ? kFusedShapes[f] : 0;
@@ -1543,6 +1817,8 @@ int launch_acoustic_uv_pipe(const PipeUvParams<R>& p, cudaStream_t st) {
   template int prepare_acoustic_fused<R>(int);                                                 \
   template int launch_acoustic_fused<R>(const AcouArgs<R>&, int, cudaStream_t);                \
   template bool acoustic_chunked_fits<R>(int, int);                                            \
+  template bool acoustic_pcr_fits<R>(int, int);                                                \
+  template int launch_acoustic_column_pcr<R>(const AcouArgs<R>&, int, cudaStream_t);           \
   template int launch_acoustic_column_chunked<R>(const AcouArgs<R>&, int, cudaStream_t);
 WFE_INST(float)
 WFE_INST(double)

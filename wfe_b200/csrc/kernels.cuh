@@ -433,6 +433,14 @@ int launch_acoustic_column_chunked(const AcouArgs<R>& a, int f, cudaStream_t st)
 int acoustic_chunked_shapes();
 template <typename R>
 bool acoustic_chunked_fits(int nz, int f);
+// The column kernel with a parallel (partitioned + cyclic-reduction)
+// tridiagonal solve, acoustic_pcr_shapes() shapes; the same rows as the
+// other column kernels, the solution equal to theirs up to rounding.
+template <typename R>
+int launch_acoustic_column_pcr(const AcouArgs<R>& a, int f, cudaStream_t st);
+int acoustic_pcr_shapes();
+template <typename R>
+bool acoustic_pcr_fits(int nz, int f);
 // whether tile shape `shape` holds a column of nz levels in shared memory
 template <typename R>
 bool acoustic_column_fits(int nz, int shape);

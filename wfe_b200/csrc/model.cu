@@ -758,7 +758,9 @@ class ModelT final : public Model {
   // the plain column tile shape of the variant in use (the linearised runs
   // launch the unfused kernels)
   int column_shape() const override {
-    if (chunked_index(tune_.column_cx) >= 0 || pipe_index(tune_.column_cx) >= 0) return 0;
+    if (chunked_index(tune_.column_cx) >= 0 || pipe_index(tune_.column_cx) >= 0 ||
+        pcr_index(tune_.column_cx) >= 0)
+      return 0;
     const int f = tune_.column_cx - acoustic_column_shapes() - 1;
     return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
   }
@@ -775,6 +777,16 @@ class ModelT final : public Model {
   int pipe_index(int v) const {
     const int f = v - acoustic_column_shapes() - 1 - acoustic_fused_shapes() - acoustic_chunked_shapes();
     return (f >= 0 && f < acoustic_pipe_shapes()) ? f : -1;
+  }
+  // parallel-solve column variants follow the pipelined ones; -1 otherwise
+  int pcr_index(int v) const {
+    const int f = v - acoustic_column_shapes() - 1 - acoustic_fused_shapes() - acoustic_chunked_shapes() -
+                  acoustic_pipe_shapes();
+    return (f >= 0 && f < acoustic_pcr_shapes()) ? f : -1;
+  }
+  bool pcr_usable(int v) const {
+    const int f = pcr_index(v);
+    return f >= 0 && acoustic_pcr_fits<R>(g_.nz, f);
   }
   bool pipe_usable(int v) const {
     const int f = pipe_index(v);
@@ -854,10 +866,18 @@ class ModelT final : public Model {
     return 0;
   }
 
+  // whether the tuner may pick a column variant that is not bit-identical
+  // to the others (the parallel-solve kernels): WFE_EXACT_COLUMN=0
+  static bool pcr_allowed() {
+    const char* e = std::getenv("WFE_EXACT_COLUMN");
+    return e && e[0] == '0';
+  }
+
   // WFE_COLUMN_VARIANT=<n> forces the acoustic variant (0..5 column tile
   // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
   // tile shapes, 10..12 the chunked column kernel, 13..15 the persistent
-  // pipelined column kernel), WFE_UV_VARIANT=<n> the forward u, v kernel (0
+  // pipelined column kernel, 16..18 the parallel-solve column kernel, equal
+  // to the others up to rounding), WFE_UV_VARIANT=<n> the forward u, v kernel (0
   // thread per face, 1 persistent pipelined tiles) and WFE_TEND_VARIANT=<n>
   // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars)
   // after tuning, for tests and experiments
@@ -868,7 +888,7 @@ class ModelT final : public Model {
     if (first && cv && *cv) {
       const int v = std::atoi(cv);
       if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_) ||
-                     fused_usable(v) || chunked_usable(v) || pipe_usable(v)))
+                     fused_usable(v) || chunked_usable(v) || pipe_usable(v) || pcr_usable(v)))
         tune_.column_cx = v;
     }
     const char* uvv = std::getenv("WFE_UV_VARIANT");
@@ -926,12 +946,15 @@ class ModelT final : public Model {
     best = 1e30f;
     // tile shapes, the TMA-staged column, the fused substep kernels
     const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() +
-                     acoustic_chunked_shapes() + acoustic_pipe_shapes();
+                     acoustic_chunked_shapes() + acoustic_pipe_shapes() + acoustic_pcr_shapes();
     for (int cx = 0; cx < nvar; ++cx) {
       if (cx == acoustic_column_shapes() && !tma_ok_) continue;
       if (cx > acoustic_column_shapes() && !fused_usable(cx) && !chunked_usable(cx) &&
-          !pipe_usable(cx))
+          !pipe_usable(cx) && !pcr_usable(cx))
         continue;
+      // the parallel-solve variants agree with the others to rounding only:
+      // the tuner picks them only where allowed (WFE_EXACT_COLUMN=0)
+      if (pcr_index(cx) >= 0 && !pcr_allowed()) continue;
       float ms;
       tune_.column_cx = cx;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -1147,6 +1170,9 @@ class ModelT final : public Model {
         if (chunked_usable(tune_.column_cx)) {
           const int f = chunked_index(tune_.column_cx);
           launch("acoustic_column", [&] { rc = launch_acoustic_column_chunked<R>(a, f, st_); });
+        } else if (pcr_usable(tune_.column_cx)) {
+          const int f = pcr_index(tune_.column_cx);
+          launch("acoustic_column", [&] { rc = launch_acoustic_column_pcr<R>(a, f, st_); });
         } else if (pipe_usable(tune_.column_cx) &&
                    acoustic_pipe_smem<R>(pipe_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
                                          a.tpi != nullptr) > 0) {
