@@ -41,7 +41,7 @@ dim3 kind_grid(int kind, int variant, int sub, const void* args, int nz_max) {
     case K_UV: return grid_uv<R>(static_cast<const AcouArgs<R>*>(args)->L);
     case K_COL: return grid_column<R>(static_cast<const AcouArgs<R>*>(args)->L, variant);
     case K_KES: return grid_kessler<R>(static_cast<const KesArgs<R>*>(args)->L, nz_max);
-    case K_SFC: return grid_sfc<R>(static_cast<const SfcArgs<R>*>(args)->L, sub);
+    case K_SFC: return grid_sfc<R>(static_cast<const SfcArgs<R>*>(args)->L, sub, nz_max);
     case K_CLOCK: return grid_clock();
     default: return dim3(0, 0, 0);
   }
@@ -53,7 +53,7 @@ int kind_occupancy(int kind, int variant, int sub, int nz_max) {
     case K_TEND: return occupancy_tend<R>(variant, sub);
     case K_COL: return occupancy_column<R>(variant, nz_max);
     case K_KES: return occupancy_kessler<R>(nz_max);
-    case K_SFC: return 8;     // 128-thread column kernels
+    case K_SFC: return 4;     // 128-thread column kernels with shared columns
     case K_CLOCK: return 16;  // one warp
     default: return 6;        // 256-thread stencil kernels without shared arrays
   }
@@ -95,7 +95,7 @@ int launch_kind_batch(int kind, int variant, int sub, const void* d_args, const 
           nblocks, st);
     case K_SFC:
       batch_sfc<R>(Batch<SfcArgs<R>>{static_cast<const SfcArgs<R>*>(d_args), d_work, nwork}, sub,
-                   nblocks, st);
+                   nblocks, nz_max, st);
       return 0;
     case K_CLOCK:
       batch_clock(Batch<ClockArgs>{static_cast<const ClockArgs*>(d_args), d_work, nwork}, nblocks,

@@ -208,9 +208,15 @@ int batch_kessler(const Batch<KesArgs<R>>& b, int nz_max, int nblocks, cudaStrea
 template <typename R>
 int occupancy_kessler(int nz_max);
 template <typename R>
-dim3 grid_sfc(const Layout& L, int sub);
+dim3 grid_sfc(const Layout& L, int sub, int nz_max);
 template <typename R>
-void batch_sfc(const Batch<SfcArgs<R>>& b, int sub, int nblocks, cudaStream_t st);
+void batch_sfc(const Batch<SfcArgs<R>>& b, int sub, int nblocks, int nz_max, cudaStream_t st);
+// sets the shared-memory limits of the level-parallel surface kernels
+template <typename R>
+int prepare_sfc(int nz);
+// whether a column of nz levels needs the scratch buffer (sfc_scratch_count)
+template <typename R>
+bool sfc_needs_scratch(int nz);
 
 // Tangent-linear (tl_) and adjoint (ad_) launches of the dynamics (lin.cu)
 // and of the Kessler column (lin_kessler.cu): a is the forward argument block

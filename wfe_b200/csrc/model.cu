@@ -126,7 +126,7 @@ class ModelT final : public Model {
     dev_ = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    if (prepare_acoustic_column<R>(g_.nz) || prepare_kessler<R>(g_.nz))
+    if (prepare_acoustic_column<R>(g_.nz) || prepare_kessler<R>(g_.nz) || prepare_sfc<R>(g_.nz))
       return fail("nz too large for the column kernels' shared memory");
     tma_ok_ = tensor_map_encoder() && prepare_acoustic_column_tma<R>(g_.nz) == 0;
     fused_ok_ = prepare_acoustic_fused<R>(g_.nz) == 0;
@@ -653,6 +653,14 @@ class ModelT final : public Model {
     return 0;
   }
 
+  // the scratch of the one-thread-per-column surface kernels, which a batched
+  // launch runs when the ensemble's deepest column does not fit in shared
+  // memory
+  int ensure_sfc_scratch() {
+    if (!sfc_on_ || sf_.scratch) return 0;
+    return (sf_.scratch = alloc(sfc_scratch_count<R>(L_))) ? 0 : 1;
+  }
+
   int enable_physics(const double* tsk, const double* land, const double* lat, const double* lon,
                      const double* soilw, double start_hour, int doy, bool nonlocal) override {
     // SfcPBL::init (src/physics/surface.cu:440-482); inputs interior ny*nx
@@ -662,7 +670,8 @@ class ModelT final : public Model {
       if (!*p && !(*p = alloc(n2))) return 1;
     if (!sf_.km && !(sf_.km = alloc(L_.n3()))) return 1;
     if (!sf_.soilt && !(sf_.soilt = alloc(4 * n2))) return 1;
-    if (!sf_.scratch && !(sf_.scratch = alloc(sfc_scratch_count<R>(L_)))) return 1;
+    if (sfc_needs_scratch<R>(g_.nz) && !sf_.scratch && !(sf_.scratch = alloc(sfc_scratch_count<R>(L_))))
+      return 1;
     auto pad = [&](const double* in) {
       std::vector<double> o(g_.n2(), 0.0);
       for (int j = 0; j < g_.ny; ++j)
@@ -1612,8 +1621,11 @@ class EnsembleT final : public Ensemble {
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_));
     sms_ = sms;
-    if (prepare_acoustic_column<R>(nz_max_) || prepare_kessler<R>(nz_max_))
+    if (prepare_acoustic_column<R>(nz_max_) || prepare_kessler<R>(nz_max_) || prepare_sfc<R>(nz_max_))
       return fail("nz too large for the column kernels' shared memory");
+    if (sfc_needs_scratch<R>(nz_max_))
+      for (auto* x : mem_)
+        if (x->ensure_sfc_scratch()) return fail(x->error());
     gens_.assign(mem_.size(), -1);
     return 0;
   }
