@@ -246,19 +246,19 @@ def test_uv_variants_are_bit_identical(name, prec, monkeypatch):
 @pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "straka_periodic", "bubble_open"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_tendency_variants_are_bit_identical(name, prec, monkeypatch):
-    """The fused (0) and split (1) tendency kernels and the variant with
-    TMA-staged scalar tiles (2: each face flux computed once) give the same
-    values, bit for bit."""
+    """The fused (0) and split (1) tendency kernels, the variant with
+    TMA-staged scalar tiles (2: each face flux computed once) and the fused
+    kernel with two cells per thread (3) give the same values, bit for bit."""
     ov = {"pd_moist": "off"} if name == "wk82_small" else None
     out = {}
-    for v in ("0", "1", "2"):
+    for v in ("0", "1", "2", "3"):
         monkeypatch.setenv("WFE_TEND_VARIANT", v)
         c = W.Case(CASES / f"{name}.ini", overrides=ov, precision=prec)
         for s in range(4):
             c.step(c.dt, s * c.dt)
         out[v] = {k: c.field(k) for k in W.FIELDS}
         c.close()
-    for v in ("1", "2"):
+    for v in ("1", "2", "3"):
         for k in W.FIELDS:
             assert np.array_equal(out["0"][k], out[v][k]), (v, k)
 

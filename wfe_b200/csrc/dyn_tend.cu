@@ -302,15 +302,21 @@ __device__ __forceinline__ R laplacian(const TendArgs<R>& a, const R* f, int i, 
 
 // One moisture species: tendency (op API) or stage value (integrator).
 template <typename R>
-__device__ __forceinline__ void moist_species(const TendArgs<R>& a, const R* q, const R* ratio,
-                                              R* tq, const R* qn, R* qo, bool davies_qv, int i,
-                                              int j, int k, size_t c, R div0) {
+__device__ __forceinline__ R moist_species(const TendArgs<R>& a, const R* q, const R* ratio,
+                                           const R* qn, const R* qo, bool davies_qv, int i, int j,
+                                           int k, size_t c, R div0) {
   R t = (a.p.pd_moist && ratio) ? pd_adv(a, q, ratio, i, j, k, div0)
                                 : scalar_adv(a, q, i, j, k, div0);
   if (davies_qv) t += davies(a, 4, q, i, j, k);
-  if (qo) qo[c] = qn[c] + a.dt_stage * t;
-  else tq[c] = t;
+  return qo ? qn[c] + a.dt_stage * t : t;
 }
+
+// The outputs of one cell, computed before any of them is stored (so that a
+// thread computing two cells reads all its inputs before its first store).
+template <typename R>
+struct TendOut {
+  R tu, tv, tw, tth, tpi, q[3];
+};
 
 // ------------------------------------------------------ fused tendencies
 // PART selects the prognostics a launch computes: 1 = momentum (u, v, w),
@@ -319,12 +325,8 @@ __device__ __forceinline__ void moist_species(const TendArgs<R>& a, const R* q, 
 enum { TEND_MOM = 1, TEND_SCAL = 2, TEND_ALL = 3 };
 
 template <typename R, int PART>
-__device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, int bz) {
+__device__ __forceinline__ void tend_cell(const TendArgs<R>& a, int i, int j, int k, TendOut<R>& o) {
   const Layout& L = a.L;
-  const int i = bx * blockDim.x + threadIdx.x;
-  const int j = by * blockDim.y + threadIdx.y;
-  const int k = bz * blockDim.z + threadIdx.z;
-  if (i >= L.nx || j >= L.ny || k >= L.nz) return;
   const int kk = L.at1(k);
   const size_t c = L.at(i, j, k);
   const long sx = 1, sy = L.px, sz = (long)L.plane();
@@ -356,7 +358,7 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     R t = (-fdiv + U[0] * dv) / ru + fc * vavg + relax;
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.u, i, j, k, false);
     if (bdy) t += davies(a, 0, a.u, i, j, k);
-    a.tu[c] = t;
+    o.tu = t;
   }
   // ---- v on the y face j (kernels.cu:348-385)
   if (PART & TEND_MOM) {
@@ -381,7 +383,7 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     R t = (-fdiv + V[0] * dv) / rv - fc * (uavg - uref) + relax;
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.v, i, j, k, false);
     if (bdy) t += davies(a, 1, a.v, i, j, k);
-    a.tv[c] = t;
+    o.tv = t;
   }
   // ---- w on the inner level k >= 1 (kernels.cu:387-425)
   if ((PART & TEND_MOM) && k >= 1) {
@@ -406,7 +408,7 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     }
     R t = (-fdiv + wk * dv) / rw + relax;
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.w, i, j, k, true);
-    a.tw[c] = t;
+    o.tw = t;
   }
   if (!(PART & TEND_SCAL)) return;
   // ---- theta' (kernels.cu:114-146)
@@ -414,21 +416,78 @@ __device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, 
     R t = scalar_adv(a, a.thp, i, j, k, div0) - a.co.spg_c[kk] * a.thp[c];
     if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.thp, i, j, k, false);
     if (bdy) t += davies(a, 2, a.thp, i, j, k);
-    a.tth[c] = t;
+    o.tth = t;
   }
   // ---- pi': no slow advection; Davies only (kernels.cu:900-901)
-  if (a.tpi) a.tpi[c] = bdy ? davies(a, 3, a.pip, i, j, k) : (R)0;
+  if (a.tpi) o.tpi = bdy ? davies(a, 3, a.pip, i, j, k) : (R)0;
   // ---- moisture (kernels.cu:886-899) and its stage update (kernels.cu:268-273)
   if (a.p.moisture) {
-    moist_species(a, a.qv, a.ratio_v, a.tqv, a.qn_v, a.qo_v, bdy, i, j, k, c, div0);
-    moist_species(a, a.qc, a.ratio_c, a.tqc, a.qn_c, a.qo_c, false, i, j, k, c, div0);
-    moist_species(a, a.qr, a.ratio_r, a.tqr, a.qn_r, a.qo_r, false, i, j, k, c, div0);
+    o.q[0] = moist_species(a, a.qv, a.ratio_v, a.qn_v, a.qo_v, bdy, i, j, k, c, div0);
+    o.q[1] = moist_species(a, a.qc, a.ratio_c, a.qn_c, a.qo_c, false, i, j, k, c, div0);
+    o.q[2] = moist_species(a, a.qr, a.ratio_r, a.qn_r, a.qo_r, false, i, j, k, c, div0);
+  }
+}
+
+template <typename R, int PART>
+__device__ __forceinline__ void tend_store(const TendArgs<R>& a, int i, int j, int k, const TendOut<R>& o) {
+  const size_t c = a.L.at(i, j, k);
+  if (PART & TEND_MOM) {
+    a.tu[c] = o.tu;
+    a.tv[c] = o.tv;
+    if (k >= 1) a.tw[c] = o.tw;
+  }
+  if (!(PART & TEND_SCAL)) return;
+  a.tth[c] = o.tth;
+  if (a.tpi) a.tpi[c] = o.tpi;
+  if (a.p.moisture) {
+    (a.qo_v ? a.qo_v : a.tqv)[c] = o.q[0];
+    (a.qo_c ? a.qo_c : a.tqc)[c] = o.q[1];
+    (a.qo_r ? a.qo_r : a.tqr)[c] = o.q[2];
+  }
+}
+
+template <typename R, int PART>
+__device__ __forceinline__ void tend_body(const TendArgs<R>& a, int bx, int by, int bz) {
+  const Layout& L = a.L;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
+  if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+  TendOut<R> o;
+  tend_cell<R, PART>(a, i, j, k, o);
+  tend_store<R, PART>(a, i, j, k, o);
+}
+
+// Two neighbouring cells along x per thread, both computed before either is
+// stored: the cells' stencils share most of their loads and all of their
+// row and level offsets (the same values as tend_body).
+template <typename R, int PART>
+__device__ __forceinline__ void tend_body2(const TendArgs<R>& a, int bx, int by, int bz) {
+  const Layout& L = a.L;
+  const int i = 2 * (bx * blockDim.x + threadIdx.x);
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
+  if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+  TendOut<R> o0;
+  if (i + 1 < L.nx) {
+    TendOut<R> o1;
+    tend_cell<R, PART>(a, i, j, k, o0);
+    tend_cell<R, PART>(a, i + 1, j, k, o1);
+    tend_store<R, PART>(a, i, j, k, o0);
+    tend_store<R, PART>(a, i + 1, j, k, o1);
+  } else {
+    tend_cell<R, PART>(a, i, j, k, o0);
+    tend_store<R, PART>(a, i, j, k, o0);
   }
 }
 
 template <typename R, int PART>
 __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
   tend_body<R, PART>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename R, int PART>
+__global__ void __launch_bounds__(128) k_tendencies2(TendArgs<R> a) {
+  tend_body2<R, PART>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R, int PART>
 __global__ void __launch_bounds__(256) k_tendencies_batch(Batch<TendArgs<R>> b) {
@@ -536,7 +595,11 @@ template <typename R>
 void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
   dim3 blk(32, 4, 2);
   dim3 grd = grid_cells<R>(a.L);
-  if (variant == 3) {  // momentum only (beside the TMA-staged scalar kernel)
+  if (variant == 4) {  // two cells per thread along x
+    dim3 b2(16, 4, 2);
+    dim3 g2((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
+    k_tendencies2<R, TEND_ALL><<<g2, b2, 0, st>>>(a);
+  } else if (variant == 3) {  // momentum only (beside the TMA-staged scalar kernel)
     k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);
   } else if (variant == 1) {
     k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);

@@ -36,7 +36,8 @@ namespace wfe {
 // Kernel variants picked by the autotuner.  Every variant computes the same
 // values with the same arithmetic; only launch shapes differ.
 struct Tune {
-  int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches, 2 with TMA-staged scalars
+  int tend_variant = 0;  // 0 fused tendencies, 1 momentum + scalar launches, 2 with TMA-staged
+                         // scalars, 3 fused with two cells per thread
   int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
   int persist = 0;       // ensembles: 0 one block per work item, 1 persistent grid, 2 members' own
                          // graphs on concurrent streams, 3 members' own graphs one after another
@@ -888,7 +889,8 @@ class ModelT final : public Model {
   // pipelined column kernel, 16..18 the parallel-solve column kernel, equal
   // to the others up to rounding), WFE_UV_VARIANT=<n> the forward u, v kernel (0
   // thread per face, 1 persistent pipelined tiles) and WFE_TEND_VARIANT=<n>
-  // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars)
+  // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars,
+  // 3 fused with two cells per thread)
   // after tuning, for tests and experiments
   int autotune(double dt) {
     const bool first = !tune_.done;
@@ -908,7 +910,7 @@ class ModelT final : public Model {
     const char* tv = std::getenv("WFE_TEND_VARIANT");
     if (first && tv && *tv) {
       const int v = std::atoi(tv);
-      if (v >= 0 && (v < 2 || (v == 2 && tend_tma_usable()))) tune_.tend_variant = v;
+      if (v >= 0 && (v < 2 || (v == 2 && tend_tma_usable()) || v == 3)) tune_.tend_variant = v;
     }
     return rc;
   }
@@ -930,8 +932,10 @@ class ModelT final : public Model {
     GhostJob<R> job = ghost_job(N, false);
     launch_fill_ghosts<R>(L_, job, dp_.bc_x_open, dp_.bc_y_open, st_);
     float best = 1e30f;
-    const int ntend = tend_tma_usable() ? 3 : 2;  // 2: momentum + TMA-staged scalars
-    for (int v = 0; v < ntend; ++v) {
+    // 0 fused, 1 split, 2 momentum + TMA-staged scalars, 3 fused with two
+    // cells per thread
+    for (int v = 0; v < 4; ++v) {
+      if (v == 2 && !tend_tma_usable()) continue;
       float ms;
       tune_.tend_variant = v;
       if (time_ms([&] { tendencies(N, N, X, (R)dt, (R)dt / 3, false); return 0; }, &ms)) return 1;
@@ -1107,7 +1111,8 @@ class ModelT final : public Model {
           launch_tend_scal_tma<R>(tp, st_);
         });
       } else {
-        launch("tendencies", [&] { launch_tendencies<R>(a, tune_.tend_variant == 1 ? 1 : 0, st_); });
+        const int v = tune_.tend_variant == 1 ? 1 : (tune_.tend_variant == 3 ? 4 : 0);
+        launch("tendencies", [&] { launch_tendencies<R>(a, v, st_); });
       }
     }
   }
