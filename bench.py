@@ -69,6 +69,10 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+# The autotuner may pick the column kernel with the parallel tridiagonal
+# solve, whose solution equals the Thomas sweep's up to rounding (the library
+# keeps the bit-identical variants unless this is 0; tests cover both).
+os.environ.setdefault("WFE_EXACT_COLUMN", "0")
 
 CASE = ROOT / "cases" / "wk82_160.ini"
 # The single-case workloads: the headline WK82 case (configs' moist
@@ -734,7 +738,10 @@ def main():
                              if WORKLOAD == "wk82" else
                              "no flush: the per-step working set fits in L2 (126 MB); an "
                              "L2/launch-bound measurement, not an HBM one",
-                       "timing": "CUDA events on the library stream around graph replays"},
+                       "timing": "CUDA events on the library stream around graph replays",
+                       "column_solver": "the tuner's fastest column kernel, parallel tridiagonal "
+                                        "solve allowed" if os.environ.get("WFE_EXACT_COLUMN") == "0"
+                                        else "Thomas sweep (bit-identical variants only)"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "traffic": traffic,

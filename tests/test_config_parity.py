@@ -126,7 +126,11 @@ def test_straka_512(tmp_path, prec):
         assert not bad, bad
 
 
-def test_wk82_160_ten_and_twenty_minutes(tmp_path):
+@pytest.mark.parametrize("exact", ["1", "0"])
+def test_wk82_160_ten_and_twenty_minutes(tmp_path, exact, monkeypatch):
+    """exact = 0: the tuner may pick the column kernel with the parallel
+    tridiagonal solve (the benchmark's setting)"""
+    monkeypatch.setenv("WFE_EXACT_COLUMN", exact)
     c, ours, r64, r32 = _runs(tmp_path, R.CFG / "wk82_160.ini", 200, [100, 200])
     stated = lambda s, k: ((1e-3, 1e-2) if s == 100 else (1e-2, 5e-2))
     worst, bad = _compare(c, ours["f32"], r64, r32, F8, stated)

@@ -845,7 +845,8 @@ class ModelT final : public Model {
     for (char& ch : name)
       if (ch == ' ') ch = '_';
     k << "v6|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
-      << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0);
+      << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0) << "x"
+      << (pcr_allowed() ? 0 : 1);
     return k.str();
   }
 
