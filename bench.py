@@ -437,7 +437,7 @@ def ensemble_bench(args, rank, world, local):
     dt = mem[0].dt
     cells = sum(sizes[q] for q in mine)
     ens = W.Ensemble(mem)
-    # the first run of 15 or more steps picks the ensemble's mode on real
+    # the first run of 19 or more steps picks the ensemble's mode on real
     # steps (wfe_ensemble_run): that happens in the warm-up, never in the
     # timed region
     warm = max(args.warmup, 20)

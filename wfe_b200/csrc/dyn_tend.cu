@@ -157,26 +157,38 @@ __device__ __forceinline__ R divergence(const TendArgs<R>& a, int i, int j, int 
          (a.mfz[c + L.plane()] - a.mfz[c]) * a.co.inv_dzc[L.at1(k)];
 }
 
-// Flux-form advection of a cell-centred scalar (kernels.cu:114-179).
+// ------------------------------------------------------------ face fluxes
+// Every advective face flux is one exactly rounded product (mul_rn) of its
+// mass flux and its face5 value, and every output combines the differences
+// of its opposite faces in one expression: a kernel that evaluates each face
+// once and shares it gets the bits of one that evaluates the faces per cell.
+
+// The lower face (west, south or bottom, by the stride s) of the momentum
+// point at offset o (its upper face: o = s): mass flux averaged over the two
+// faces M[o + m0], M[o] beside it, the point's field Q on o - 3s .. o + 2s
+// (kernels.cu:308-425).
 template <typename R>
-__device__ __forceinline__ R scalar_adv(const TendArgs<R>& a, const R* __restrict__ q, int i, int j,
-                                        int k, R div) {
-  const Layout& L = a.L;
-  const size_t c = L.at(i, j, k);
-  const size_t sx = 1, sy = L.px, sz = L.plane();
-  const R* Q = q + c;
-  R fxL = a.mfx[c], fxR = a.mfx[c + sx];
-  R fyL = a.mfy[c], fyR = a.mfy[c + sy];
-  R fzB = a.mfz[c], fzT = a.mfz[c + sz];
-  R FxL = mul_rn(fxL, face5(Q[-3 * (long)sx], Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], fxL));
-  R FxR = mul_rn(fxR, face5(Q[-2 * (long)sx], Q[-1 * (long)sx], Q[0], Q[sx], Q[2 * sx], Q[3 * sx], fxR));
-  R FyL = mul_rn(fyL, face5(Q[-3 * (long)sy], Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], fyL));
-  R FyR = mul_rn(fyR, face5(Q[-2 * (long)sy], Q[-1 * (long)sy], Q[0], Q[sy], Q[2 * sy], Q[3 * sy], fyR));
-  R FzB = mul_rn(fzB, face5(Q[-3 * (long)sz], Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], fzB));
-  R FzT = mul_rn(fzT, face5(Q[-2 * (long)sz], Q[-1 * (long)sz], Q[0], Q[sz], Q[2 * sz], Q[3 * sz], fzT));
-  R fdiv = (FxR - FxL) * a.co.inv_dx + (FyR - FyL) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[L.at1(k)];
-  R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
-  return (-fdiv + Q[0] * div) / rt;
+__device__ __forceinline__ R face_mom(const R* M, long m0, const R* Q, long s, long o = 0) {
+  const R f = (R)0.5 * (M[o + m0] + M[o]);
+  return mul_rn(f, face5(Q[o - 3 * s], Q[o - 2 * s], Q[o - s], Q[o], Q[o + s], Q[o + 2 * s], f));
+}
+
+// The lower face of a cell-centred scalar: the face's mass flux M[0]
+// (kernels.cu:114-179, 187-218).
+template <typename R>
+__device__ __forceinline__ R face_sc(const R* M, const R* Q, long s) {
+  const R f = M[0];
+  return mul_rn(f, face5(Q[-3 * s], Q[-2 * s], Q[-s], Q[0], Q[s], Q[2 * s], f));
+}
+
+// Flux-form tendency of a scalar cell (value q0, level index kk) from the
+// face-flux differences east - west, north - south, top - bottom.
+template <typename R>
+__device__ __forceinline__ R scalar_tend(const TendArgs<R>& a, R q0, size_t c, int i, int j, int kk, R dX,
+                                         R dY, R dZ, R div) {
+  R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzc[kk];
+  R rt = a.b.rhob[c] * a.m.jac[a.L.at2(i, j)];
+  return (-fdiv + q0 * div) / rt;
 }
 
 // Face fluxes of a scalar used by the positive-definite limiter
@@ -184,61 +196,55 @@ __device__ __forceinline__ R scalar_adv(const TendArgs<R>& a, const R* __restric
 template <typename R>
 __device__ __forceinline__ R qflux_x(const TendArgs<R>& a, const R* q, int i, int j, int k) {
   const size_t c = a.L.at(i, j, k);
-  R f = a.mfx[c];
-  const R* Q = q + c;
-  return f * face5(Q[-3], Q[-2], Q[-1], Q[0], Q[1], Q[2], f);
+  return face_sc(a.mfx + c, q + c, 1);
 }
 template <typename R>
 __device__ __forceinline__ R qflux_y(const TendArgs<R>& a, const R* q, int i, int j, int k) {
   const size_t c = a.L.at(i, j, k);
-  const long s = a.L.px;
-  R f = a.mfy[c];
-  const R* Q = q + c;
-  return f * face5(Q[-3 * s], Q[-2 * s], Q[-s], Q[0], Q[s], Q[2 * s], f);
+  return face_sc(a.mfy + c, q + c, (long)a.L.px);
 }
 template <typename R>
 __device__ __forceinline__ R qflux_z(const TendArgs<R>& a, const R* q, int i, int j, int k) {
   const size_t c = a.L.at(i, j, k);
-  const long s = (long)a.L.plane();
-  R f = a.mfz[c];
-  const R* Q = q + c;
-  return f * face5(Q[-3 * s], Q[-2 * s], Q[-s], Q[0], Q[s], Q[2 * s], f);
+  return face_sc(a.mfz + c, q + c, (long)a.L.plane());
 }
 
-// Outflow ratio min(1, available / outgoing) per species (kernels.cu:221-238).
+// Outflow ratio min(1, available / outgoing) per species (kernels.cu:221-238),
+// one thread per cell.  The outgoing flux sums each direction's two faces and
+// scales the sum by the precomputed reciprocal spacing (the reference divides
+// each face by the spacing: the same value to rounding), one division per
+// species instead of seven.
 template <typename R>
 __device__ __forceinline__ void pd_body(const PdArgs<R>& P, int bx, int by, int bz) {
   const TendArgs<R>& a = P.t;
-  R* __restrict__ rv = P.rv;
-  R* __restrict__ rc = P.rc;
-  R* __restrict__ rr = P.rr;
   const Layout& L = a.L;
   const int i = bx * blockDim.x + threadIdx.x;
   const int j = by * blockDim.y + threadIdx.y;
   const int k = bz * blockDim.z + threadIdx.z;
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
-  const R dzc = a.m.dzeta_c[L.at1(k)];
-  const R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
-  const R* qs[3] = {a.qv, a.qc, a.qr};
-  R* outs[3] = {rv, rc, rr};
+  const size_t c = L.at(i, j, k);
+  const R idz = a.co.inv_dzc[L.at1(k)];
+  const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
-    const R* q = qs[s];
-    R out = fmax((R)0, qflux_x(a, q, i + 1, j, k)) / a.dx + fmax((R)0, -qflux_x(a, q, i, j, k)) / a.dx +
-            fmax((R)0, qflux_y(a, q, i, j + 1, k)) / a.dy + fmax((R)0, -qflux_y(a, q, i, j, k)) / a.dy +
-            fmax((R)0, qflux_z(a, q, i, j, k + 1)) / dzc + fmax((R)0, -qflux_z(a, q, i, j, k)) / dzc;
-    R avail = rt * fmax((R)0, q[L.at(i, j, k)]);
-    R r = (a.dt * out > (R)1e-20) ? avail / (a.dt * out) : (R)1;
-    outs[s][L.at(i, j, k)] = fmin((R)1, r);
+    const R* q = s == 0 ? a.qv : (s == 1 ? a.qc : a.qr);
+    R* outp = s == 0 ? P.rv : (s == 1 ? P.rc : P.rr);
+    const R ox = fmax((R)0, qflux_x(a, q, i + 1, j, k)) + fmax((R)0, -qflux_x(a, q, i, j, k));
+    const R oy = fmax((R)0, qflux_y(a, q, i, j + 1, k)) + fmax((R)0, -qflux_y(a, q, i, j, k));
+    const R oz = fmax((R)0, qflux_z(a, q, i, j, k + 1)) + fmax((R)0, -qflux_z(a, q, i, j, k));
+    const R out = ox * a.co.inv_dx + oy * a.co.inv_dy + oz * idz;
+    const R avail = rt * fmax((R)0, q[c]);
+    const R r = (a.dt * out > (R)1e-20) ? avail / (a.dt * out) : (R)1;
+    outp[c] = fmin((R)1, r);
   }
 }
 
 template <typename R>
-__global__ void k_pd_ratio(PdArgs<R> a) {
+__global__ void __launch_bounds__(256) k_pd_ratio(PdArgs<R> a) {
   pd_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R>
-__global__ void k_pd_ratio_batch(Batch<PdArgs<R>> b) {
+__global__ void __launch_bounds__(256) k_pd_ratio_batch(Batch<PdArgs<R>> b) {
   for_each_work(b, [](const PdArgs<R>& a, int x, int y, int z) { pd_body(a, x, y, z); });
 }
 
@@ -253,36 +259,32 @@ __device__ __forceinline__ R ratio_at(const TendArgs<R>& a, const R* ratio, int 
   return ratio[L.at(si, sj, sk)];
 }
 
-// Renormalised positive-definite advection (kernels.cu:241-264).
+// Limited face fluxes of the renormalised positive-definite advection
+// (kernels.cu:241-264): the flux on the lower face of cell (i, j, k) times
+// the outflow ratio of its upwind cell (read at its own index when that cell
+// is interior, through ratio_at's ghost map otherwise).
 template <typename R>
-__device__ __forceinline__ R pd_adv(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j,
-                                    int k, R div) {
-  const Layout& L = a.L;
-  R fxl = qflux_x(a, q, i, j, k), fxr = qflux_x(a, q, i + 1, j, k);
-  R fyl = qflux_y(a, q, i, j, k), fyr = qflux_y(a, q, i, j + 1, k);
-  R fzl = qflux_z(a, q, i, j, k), fzr = qflux_z(a, q, i, j, k + 1);
-  R sxl, sxr, syl, syr, szl, szr;
-  if (i > 0 && i < L.nx - 1 && j > 0 && j < L.ny - 1 && k > 0 && k < L.nz - 1) {
-    // every upwind cell is interior: plain offsets from the cell
-    const R* r0 = ratio + L.at(i, j, k);
-    const int sy = L.px, sz = (int)L.plane();
-    sxl = fxl * r0[fxl >= (R)0 ? -1 : 0];
-    sxr = fxr * r0[fxr >= (R)0 ? 0 : 1];
-    syl = fyl * r0[fyl >= (R)0 ? -sy : 0];
-    syr = fyr * r0[fyr >= (R)0 ? 0 : sy];
-    szl = fzl * r0[fzl >= (R)0 ? -sz : 0];
-    szr = fzr * r0[fzr >= (R)0 ? 0 : sz];
-  } else {
-    sxl = fxl * ratio_at(a, ratio, fxl >= (R)0 ? i - 1 : i, j, k);
-    sxr = fxr * ratio_at(a, ratio, fxr >= (R)0 ? i : i + 1, j, k);
-    syl = fyl * ratio_at(a, ratio, i, fyl >= (R)0 ? j - 1 : j, k);
-    syr = fyr * ratio_at(a, ratio, i, fyr >= (R)0 ? j : j + 1, k);
-    szl = fzl * ratio_at(a, ratio, i, j, fzl >= (R)0 ? k - 1 : k);
-    szr = fzr * ratio_at(a, ratio, i, j, fzr >= (R)0 ? k : k + 1);
-  }
-  R fdiv = (sxr - sxl) * a.co.inv_dx + (syr - syl) * a.co.inv_dy + (szr - szl) * a.co.inv_dzc[L.at1(k)];
-  R rt = a.b.rhob[L.at(i, j, k)] * a.m.jac[L.at2(i, j)];
-  return (-fdiv + q[L.at(i, j, k)] * div) / rt;
+__device__ __forceinline__ R pd_face_x(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j, int k) {
+  const size_t c = a.L.at(i, j, k);
+  const R F = face_sc(a.mfx + c, q + c, 1);
+  const int u = F >= (R)0 ? i - 1 : i;
+  return mul_rn(F, (u >= 0 && u < a.L.nx) ? ratio[c + (u - i)] : ratio_at(a, ratio, u, j, k));
+}
+template <typename R>
+__device__ __forceinline__ R pd_face_y(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j, int k) {
+  const size_t c = a.L.at(i, j, k);
+  const long sy = a.L.px;
+  const R F = face_sc(a.mfy + c, q + c, sy);
+  const int u = F >= (R)0 ? j - 1 : j;
+  return mul_rn(F, (u >= 0 && u < a.L.ny) ? ratio[c + (u - j) * sy] : ratio_at(a, ratio, i, u, k));
+}
+template <typename R>
+__device__ __forceinline__ R pd_face_z(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j, int k) {
+  const size_t c = a.L.at(i, j, k);
+  const long sz = (long)a.L.plane();
+  const R F = face_sc(a.mfz + c, q + c, sz);
+  const int u = F >= (R)0 ? k - 1 : k;
+  return mul_rn(F, (u >= 0 && u < a.L.nz) ? ratio[c + (u - k) * sz] : ratio_at(a, ratio, i, j, u));
 }
 
 // Constant-K Laplacian (kernels.cu:430-443).
@@ -300,15 +302,119 @@ __device__ __forceinline__ R laplacian(const TendArgs<R>& a, const R* f, int i, 
 }
 
 
-// One moisture species: tendency (op API) or stage value (integrator).
+// One moisture species: tendency (op API) or stage value (integrator) from
+// its face-flux differences (limited fluxes under the positive-definite
+// option).
 template <typename R>
-__device__ __forceinline__ R moist_species(const TendArgs<R>& a, const R* q, const R* ratio,
-                                           const R* qn, const R* qo, bool davies_qv, int i, int j,
-                                           int k, size_t c, R div0) {
-  R t = (a.p.pd_moist && ratio) ? pd_adv(a, q, ratio, i, j, k, div0)
-                                : scalar_adv(a, q, i, j, k, div0);
+__device__ __forceinline__ R moist_out(const TendArgs<R>& a, const R* q, const R* qn, const R* qo, bool davies_qv,
+                                       int i, int j, int k, size_t c, R dX, R dY, R dZ, R div0) {
+  R t = scalar_tend(a, q[c], c, i, j, a.L.at1(k), dX, dY, dZ, div0);
   if (davies_qv) t += davies(a, 4, q, i, j, k);
   return qo ? qn[c] + a.dt_stage * t : t;
+}
+
+// A species' stage value or tendency at cell (i, j, k), its faces evaluated
+// per cell.
+template <typename R>
+__device__ __forceinline__ R species_cell(const TendArgs<R>& a, const R* q, const R* ratio, const R* qn,
+                                          const R* qo, bool davies_qv, int i, int j, int k, size_t c, R div0) {
+  if (a.p.pd_moist && ratio)
+    return moist_out(a, q, qn, qo, davies_qv, i, j, k, c,
+                     pd_face_x(a, q, ratio, i + 1, j, k) - pd_face_x(a, q, ratio, i, j, k),
+                     pd_face_y(a, q, ratio, i, j + 1, k) - pd_face_y(a, q, ratio, i, j, k),
+                     pd_face_z(a, q, ratio, i, j, k + 1) - pd_face_z(a, q, ratio, i, j, k), div0);
+  const long sx = 1, sy = a.L.px, sz = (long)a.L.plane();
+  const R* MX = a.mfx + c;
+  const R* MY = a.mfy + c;
+  const R* MZ = a.mfz + c;
+  const R* Q = q + c;
+  return moist_out(a, q, qn, qo, davies_qv, i, j, k, c, face_sc(MX + sx, Q + sx, sx) - face_sc(MX, Q, sx),
+                   face_sc(MY + sy, Q + sy, sy) - face_sc(MY, Q, sy),
+                   face_sc(MZ + sz, Q + sz, sz) - face_sc(MZ, Q, sz), div0);
+}
+
+// u tendency on the x face i from its face-flux differences and the
+// divergences of the cells west of and at it (kernels.cu:308-346); the
+// neighbours' divergence comes from a callable, evaluated where the sum needs
+// it (fewer registers live across the face evaluations).
+template <typename R, class Div>
+__device__ __forceinline__ R u_out(const TendArgs<R>& a, int i, int j, int k, R dX, R dY, R dZ, Div div_w,
+                                   R div0, bool bdy) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  const long sx = 1, sy = L.px;
+  const R* U = a.u + c;
+  const R* V = a.v + c;
+  R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzc[kk];
+  R dv = (R)0.5 * (div_w() + div0);
+  R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+  R vavg = (R)0.25 * (V[-sx] + V[sy - sx] + V[0] + V[sy]);
+  R fc = (R)0.5 * (a.m.fcor[L.at2(i - 1, j)] + a.m.fcor[L.at2(i, j)]);
+  R relax = -a.co.spg_c[kk] * (U[0] - a.b.ub[kk]);
+  R t = (-fdiv + U[0] * dv) / ru + fc * vavg + relax;
+  if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.u, i, j, k, false);
+  if (bdy) t += davies(a, 0, a.u, i, j, k);
+  return t;
+}
+
+// v tendency on the y face j (kernels.cu:348-385); div_s: the cell south of it.
+template <typename R, class Div>
+__device__ __forceinline__ R v_out(const TendArgs<R>& a, int i, int j, int k, R dX, R dY, R dZ, Div div_s,
+                                   R div0, bool bdy) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  const long sx = 1, sy = L.px;
+  const R* U = a.u + c;
+  const R* V = a.v + c;
+  R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzc[kk];
+  R dv = (R)0.5 * (div_s() + div0);
+  R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+  R uavg = (R)0.25 * (U[-sy] + U[sx - sy] + U[0] + U[sx]);
+  R fc = (R)0.5 * (a.m.fcor[L.at2(i, j - 1)] + a.m.fcor[L.at2(i, j)]);
+  R uref = a.p.coriolis_use_ub ? a.b.ub[kk] : (R)0;
+  R relax = -a.co.spg_c[kk] * V[0];
+  R t = (-fdiv + V[0] * dv) / rv - fc * (uavg - uref) + relax;
+  if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.v, i, j, k, false);
+  if (bdy) t += davies(a, 1, a.v, i, j, k);
+  return t;
+}
+
+// w tendency on the inner level k >= 1 (kernels.cu:387-425); div_b: the cell
+// below it.
+template <typename R, class Div>
+__device__ __forceinline__ R w_out(const TendArgs<R>& a, int i, int j, int k, R dX, R dY, R dZ, Div div_b,
+                                   R div0) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  const R* W = a.w + c;
+  R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzw[kk];
+  R dv = (R)0.5 * (div_b() + div0);
+  R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
+  R relax = -a.co.spg_w[kk] * W[0];
+  R wk = W[0];
+  if (a.p.w_damping) {
+    R cr = fabs(wk) * a.dt / (a.m.dzeta_w[kk] * a.m.jac[L.at2(i, j)]);
+    if (cr > (R)1) relax -= (R)0.3 * (cr - (R)1) * wk / a.dt;
+  }
+  R t = (-fdiv + wk * dv) / rw + relax;
+  if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.w, i, j, k, true);
+  return t;
+}
+
+// theta' tendency (kernels.cu:114-146).
+template <typename R>
+__device__ __forceinline__ R th_out(const TendArgs<R>& a, int i, int j, int k, R dX, R dY, R dZ, R div0,
+                                    bool bdy) {
+  const Layout& L = a.L;
+  const int kk = L.at1(k);
+  const size_t c = L.at(i, j, k);
+  R t = scalar_tend(a, a.thp[c], c, i, j, kk, dX, dY, dZ, div0) - a.co.spg_c[kk] * a.thp[c];
+  if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.thp, i, j, k, false);
+  if (bdy) t += davies(a, 2, a.thp, i, j, k);
+  return t;
 }
 
 // The outputs of one cell, computed before any of them is stored (so that a
@@ -327,7 +433,6 @@ enum { TEND_MOM = 1, TEND_SCAL = 2, TEND_ALL = 3 };
 template <typename R, int PART>
 __device__ __forceinline__ void tend_cell(const TendArgs<R>& a, int i, int j, int k, TendOut<R>& o) {
   const Layout& L = a.L;
-  const int kk = L.at1(k);
   const size_t c = L.at(i, j, k);
   const long sx = 1, sy = L.px, sz = (long)L.plane();
   const bool bdy = a.lo[0] != nullptr;
@@ -336,95 +441,42 @@ __device__ __forceinline__ void tend_cell(const TendArgs<R>& a, int i, int j, in
   const R* MZ = a.mfz + c;
   const R div0 = divergence(a, i, j, k);
 
-  // ---- u on the x face i (kernels.cu:308-346)
   if (PART & TEND_MOM) {
     const R* U = a.u + c;
-    R fcL = (R)0.5 * (MX[-sx] + MX[0]), fcR = (R)0.5 * (MX[0] + MX[sx]);
-    R FxL = fcL * face5(U[-3 * sx], U[-2 * sx], U[-sx], U[0], U[sx], U[2 * sx], fcL);
-    R FxR = fcR * face5(U[-2 * sx], U[-sx], U[0], U[sx], U[2 * sx], U[3 * sx], fcR);
-    R fyB = (R)0.5 * (MY[-sx] + MY[0]), fyT = (R)0.5 * (MY[sy - sx] + MY[sy]);
-    R FyB = fyB * face5(U[-3 * sy], U[-2 * sy], U[-sy], U[0], U[sy], U[2 * sy], fyB);
-    R FyT = fyT * face5(U[-2 * sy], U[-sy], U[0], U[sy], U[2 * sy], U[3 * sy], fyT);
-    R fzB = (R)0.5 * (MZ[-sx] + MZ[0]), fzT = (R)0.5 * (MZ[sz - sx] + MZ[sz]);
-    R FzB = fzB * face5(U[-3 * sz], U[-2 * sz], U[-sz], U[0], U[sz], U[2 * sz], fzB);
-    R FzT = fzT * face5(U[-2 * sz], U[-sz], U[0], U[sz], U[2 * sz], U[3 * sz], fzT);
-    R fdiv = (FxR - FxL) * a.co.inv_dx + (FyT - FyB) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[kk];
-    R dv = (R)0.5 * (divergence(a, i - 1, j, k) + div0);
-    R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
-    const R* V = a.v + c;
-    R vavg = (R)0.25 * (V[-sx] + V[sy - sx] + V[0] + V[sy]);
-    R fc = (R)0.5 * (a.m.fcor[L.at2(i - 1, j)] + a.m.fcor[L.at2(i, j)]);
-    R relax = -a.co.spg_c[kk] * (U[0] - a.b.ub[kk]);
-    R t = (-fdiv + U[0] * dv) / ru + fc * vavg + relax;
-    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.u, i, j, k, false);
-    if (bdy) t += davies(a, 0, a.u, i, j, k);
-    o.tu = t;
+    const R dX = face_mom(MX, -sx, U, sx, sx) - face_mom(MX, -sx, U, sx);
+    const R dY = face_mom(MY, -sx, U, sy, sy) - face_mom(MY, -sx, U, sy);
+    const R dZ = face_mom(MZ, -sx, U, sz, sz) - face_mom(MZ, -sx, U, sz);
+    o.tu = u_out(a, i, j, k, dX, dY, dZ, [&] { return divergence(a, i - 1, j, k); }, div0, bdy);
   }
-  // ---- v on the y face j (kernels.cu:348-385)
   if (PART & TEND_MOM) {
     const R* V = a.v + c;
-    R fcB = (R)0.5 * (MY[-sy] + MY[0]), fcT = (R)0.5 * (MY[0] + MY[sy]);
-    R FyB = fcB * face5(V[-3 * sy], V[-2 * sy], V[-sy], V[0], V[sy], V[2 * sy], fcB);
-    R FyT = fcT * face5(V[-2 * sy], V[-sy], V[0], V[sy], V[2 * sy], V[3 * sy], fcT);
-    R fxL = (R)0.5 * (MX[-sy] + MX[0]), fxR = (R)0.5 * (MX[sx - sy] + MX[sx]);
-    R FxL = fxL * face5(V[-3 * sx], V[-2 * sx], V[-sx], V[0], V[sx], V[2 * sx], fxL);
-    R FxR = fxR * face5(V[-2 * sx], V[-sx], V[0], V[sx], V[2 * sx], V[3 * sx], fxR);
-    R fzB = (R)0.5 * (MZ[-sy] + MZ[0]), fzT = (R)0.5 * (MZ[sz - sy] + MZ[sz]);
-    R FzB = fzB * face5(V[-3 * sz], V[-2 * sz], V[-sz], V[0], V[sz], V[2 * sz], fzB);
-    R FzT = fzT * face5(V[-2 * sz], V[-sz], V[0], V[sz], V[2 * sz], V[3 * sz], fzT);
-    R fdiv = (FxR - FxL) * a.co.inv_dx + (FyT - FyB) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzc[kk];
-    R dv = (R)0.5 * (divergence(a, i, j - 1, k) + div0);
-    R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
-    const R* U = a.u + c;
-    R uavg = (R)0.25 * (U[-sy] + U[sx - sy] + U[0] + U[sx]);
-    R fc = (R)0.5 * (a.m.fcor[L.at2(i, j - 1)] + a.m.fcor[L.at2(i, j)]);
-    R uref = a.p.coriolis_use_ub ? a.b.ub[kk] : (R)0;
-    R relax = -a.co.spg_c[kk] * V[0];
-    R t = (-fdiv + V[0] * dv) / rv - fc * (uavg - uref) + relax;
-    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.v, i, j, k, false);
-    if (bdy) t += davies(a, 1, a.v, i, j, k);
-    o.tv = t;
+    const R dX = face_mom(MX, -sy, V, sx, sx) - face_mom(MX, -sy, V, sx);
+    const R dY = face_mom(MY, -sy, V, sy, sy) - face_mom(MY, -sy, V, sy);
+    const R dZ = face_mom(MZ, -sy, V, sz, sz) - face_mom(MZ, -sy, V, sz);
+    o.tv = v_out(a, i, j, k, dX, dY, dZ, [&] { return divergence(a, i, j - 1, k); }, div0, bdy);
   }
-  // ---- w on the inner level k >= 1 (kernels.cu:387-425)
   if ((PART & TEND_MOM) && k >= 1) {
     const R* W = a.w + c;
-    R fxL = (R)0.5 * (MX[-sz] + MX[0]), fxR = (R)0.5 * (MX[sx - sz] + MX[sx]);
-    R FxL = fxL * face5(W[-3 * sx], W[-2 * sx], W[-sx], W[0], W[sx], W[2 * sx], fxL);
-    R FxR = fxR * face5(W[-2 * sx], W[-sx], W[0], W[sx], W[2 * sx], W[3 * sx], fxR);
-    R fyB = (R)0.5 * (MY[-sz] + MY[0]), fyT = (R)0.5 * (MY[sy - sz] + MY[sy]);
-    R FyB = fyB * face5(W[-3 * sy], W[-2 * sy], W[-sy], W[0], W[sy], W[2 * sy], fyB);
-    R FyT = fyT * face5(W[-2 * sy], W[-sy], W[0], W[sy], W[2 * sy], W[3 * sy], fyT);
-    R fzB = (R)0.5 * (MZ[-sz] + MZ[0]), fzT = (R)0.5 * (MZ[0] + MZ[sz]);
-    R FzB = fzB * face5(W[-3 * sz], W[-2 * sz], W[-sz], W[0], W[sz], W[2 * sz], fzB);
-    R FzT = fzT * face5(W[-2 * sz], W[-sz], W[0], W[sz], W[2 * sz], W[3 * sz], fzT);
-    R fdiv = (FxR - FxL) * a.co.inv_dx + (FyT - FyB) * a.co.inv_dy + (FzT - FzB) * a.co.inv_dzw[kk];
-    R dv = (R)0.5 * (divergence(a, i, j, k - 1) + div0);
-    R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
-    R relax = -a.co.spg_w[kk] * W[0];
-    R wk = W[0];
-    if (a.p.w_damping) {
-      R cr = fabs(wk) * a.dt / (a.m.dzeta_w[kk] * a.m.jac[L.at2(i, j)]);
-      if (cr > (R)1) relax -= (R)0.3 * (cr - (R)1) * wk / a.dt;
-    }
-    R t = (-fdiv + wk * dv) / rw + relax;
-    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.w, i, j, k, true);
-    o.tw = t;
+    const R dX = face_mom(MX, -sz, W, sx, sx) - face_mom(MX, -sz, W, sx);
+    const R dY = face_mom(MY, -sz, W, sy, sy) - face_mom(MY, -sz, W, sy);
+    const R dZ = face_mom(MZ, -sz, W, sz, sz) - face_mom(MZ, -sz, W, sz);
+    o.tw = w_out(a, i, j, k, dX, dY, dZ, [&] { return divergence(a, i, j, k - 1); }, div0);
   }
   if (!(PART & TEND_SCAL)) return;
-  // ---- theta' (kernels.cu:114-146)
   {
-    R t = scalar_adv(a, a.thp, i, j, k, div0) - a.co.spg_c[kk] * a.thp[c];
-    if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.thp, i, j, k, false);
-    if (bdy) t += davies(a, 2, a.thp, i, j, k);
-    o.tth = t;
+    const R* T = a.thp + c;
+    const R dX = face_sc(MX + sx, T + sx, sx) - face_sc(MX, T, sx);
+    const R dY = face_sc(MY + sy, T + sy, sy) - face_sc(MY, T, sy);
+    const R dZ = face_sc(MZ + sz, T + sz, sz) - face_sc(MZ, T, sz);
+    o.tth = th_out(a, i, j, k, dX, dY, dZ, div0, bdy);
   }
-  // ---- pi': no slow advection; Davies only (kernels.cu:900-901)
+  // pi': no slow advection; Davies only (kernels.cu:900-901)
   if (a.tpi) o.tpi = bdy ? davies(a, 3, a.pip, i, j, k) : (R)0;
-  // ---- moisture (kernels.cu:886-899) and its stage update (kernels.cu:268-273)
+  // moisture (kernels.cu:886-899) and its stage update (kernels.cu:268-273)
   if (a.p.moisture) {
-    o.q[0] = moist_species(a, a.qv, a.ratio_v, a.qn_v, a.qo_v, bdy, i, j, k, c, div0);
-    o.q[1] = moist_species(a, a.qc, a.ratio_c, a.qn_c, a.qo_c, false, i, j, k, c, div0);
-    o.q[2] = moist_species(a, a.qr, a.ratio_r, a.qn_r, a.qo_r, false, i, j, k, c, div0);
+    o.q[0] = species_cell(a, a.qv, a.ratio_v, a.qn_v, a.qo_v, bdy, i, j, k, c, div0);
+    o.q[1] = species_cell(a, a.qc, a.ratio_c, a.qn_c, a.qo_c, false, i, j, k, c, div0);
+    o.q[2] = species_cell(a, a.qr, a.ratio_r, a.qn_r, a.qo_r, false, i, j, k, c, div0);
   }
 }
 
@@ -582,8 +634,13 @@ dim3 grid_cells(const Layout& L) {
 }
 
 template <typename R>
+dim3 grid_pd(const Layout& L) {
+  return grid_cells<R>(L);
+}
+
+template <typename R>
 void launch_pd_ratio(const TendArgs<R>& a, R* rv, R* rc, R* rr, cudaStream_t st) {
-  k_pd_ratio<R><<<grid_cells<R>(a.L), dim3(32, 4, 2), 0, st>>>(PdArgs<R>{a, rv, rc, rr});
+  k_pd_ratio<R><<<grid_pd<R>(a.L), dim3(32, 4, 2), 0, st>>>(PdArgs<R>{a, rv, rc, rr});
 }
 
 template <typename R>
@@ -644,6 +701,7 @@ int occupancy_tend(int variant, int sub) {
   template dim3 grid_fill<R>(const FillArgs<R>&);                                              \
   template dim3 grid_flux<R>(const FluxArgs<R>&);                                              \
   template dim3 grid_cells<R>(const Layout&);                                                   \
+  template dim3 grid_pd<R>(const Layout&);                                                      \
   template void batch_fill<R>(const Batch<FillArgs<R>>&, int, cudaStream_t);                   \
   template void batch_flux<R>(const Batch<FluxArgs<R>>&, int, cudaStream_t);                   \
   template void batch_pd<R>(const Batch<PdArgs<R>>&, int, cudaStream_t);                       \

@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kTtX * kTtY * 2) k_tend_scal_tma(const __grid_
     }
     const R* Q = sq[b];
     auto QB = [&](int x, int y, int z) -> R { return Q[((size_t)z * kQbY + y) * kQbX + x]; };
-    // face fluxes of the tile, each once (scalar_adv's expressions)
+    // face fluxes of the tile, each once (face_sc's expression)
     for (int f = tid; f < (kTtX + 1) * kTtY * kTtZ; f += kThreads) {
       const int ii = f % (kTtX + 1), r = f / (kTtX + 1), jj = r % kTtY, kz = r / kTtY;
       const R fv = smx[((size_t)kz * kTtY + jj) * kMxX + ii];

@@ -178,7 +178,9 @@ dim3 grid_fill(const FillArgs<R>& a);
 template <typename R>
 dim3 grid_flux(const FluxArgs<R>& a);
 template <typename R>
-dim3 grid_cells(const Layout& L);  // pd ratio and tendencies
+dim3 grid_cells(const Layout& L);  // tendencies
+template <typename R>
+dim3 grid_pd(const Layout& L);  // positive-definite outflow ratios
 dim3 grid_clock();
 template <typename R>
 void batch_fill(const Batch<FillArgs<R>>& b, int nblocks, cudaStream_t st);

@@ -1636,6 +1636,9 @@ class EnsembleT final : public Ensemble {
     return 0;
   }
 
+  // steps the first run takes to pick the mode (it needs at least this many)
+  static constexpr int kModePickSteps = 19;
+
   int run(int nsteps, double dt, double t0) override {
     CK(cudaSetDevice(dev_));
     if (begin(dt)) return 1;
@@ -1648,17 +1651,22 @@ class EnsembleT final : public Ensemble {
       const std::string m(em);
       tune_.persist = m == "members" ? 2 : (m == "sequential" ? 3 : ((tune_.persist & 1) | 4));
     }
-    if (!mode_done_ && nsteps >= 15) {
+    if (!mode_done_ && nsteps >= kModePickSteps) {
       // pick on real steps among the batched launches, the members' own
       // graphs on concurrent streams and the members' own graphs one after
       // another (all three give the same values, bit for bit): three warm-up
       // steps of each mode capture every phase's graphs, then two timed
-      // steps each
-      float tb = 0, tc = 0, tq = 0;
+      // steps each, and the two close ones (concurrent, one after another)
+      // timed once more in turn, the faster of each pair kept
+      float tb = 0, tc = 0, tq = 0, t2 = 0;
       if (batched_steps(3, dt) || timed([&] { return batched_steps(2, dt); }, &tb)) return 1;
       if (member_steps(3, dt, false) || timed([&] { return member_steps(2, dt, false); }, &tc)) return 1;
       if (member_steps(3, dt, true) || timed([&] { return member_steps(2, dt, true); }, &tq)) return 1;
-      s = 15;
+      if (timed([&] { return member_steps(2, dt, false); }, &t2)) return 1;
+      tc = std::min(tc, t2);
+      if (timed([&] { return member_steps(2, dt, true); }, &t2)) return 1;
+      tq = std::min(tq, t2);
+      s = kModePickSteps;
       mode_done_ = true;
       if (tc <= tb && tc <= tq) tune_.persist = 2;
       else if (tq <= tb) tune_.persist = 3;
