@@ -245,12 +245,13 @@ int wfe_ensemble_time_run(wfe_ens* ens, int nsteps, double dt, double t0, double
  * shape, and the mode (0 batched launches, one block per work item; 1
  * batched on a persistent grid; 2 every member's own graph on its own
  * stream, the members running concurrently; 3 every member's own graphs,
- * one member after another).  The first run of 19 or more steps times two
- * steps of each of the batched, concurrent and one-after-another modes
- * (after three warm-up steps of each; the concurrent and one-after-another
- * modes twice, the faster time of each kept) and keeps the fastest: all
- * give the same values, bit for bit.  WFE_ENSEMBLE_MODE = batched | members
- * | sequential forces one. */
+ * one member after another).  The first run of 19 or more steps times the
+ * batched, concurrent and one-after-another modes on real steps (after three
+ * warm-up steps of each: two timed steps batched, then four concurrent and
+ * four one after another, in the order concurrent, sequential, sequential,
+ * concurrent so that a drift of the step cost weighs on both) and keeps the
+ * fastest: all give the same values, bit for bit.  WFE_ENSEMBLE_MODE =
+ * batched | members | sequential forces one. */
 long wfe_ensemble_launches_per_step(const wfe_ens* ens);
 int wfe_ensemble_variants(const wfe_ens* ens, int out[3]);
 

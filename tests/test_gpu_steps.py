@@ -325,19 +325,41 @@ def test_cases_of_different_depths_share_the_kernels(monkeypatch):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "moist_blob"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_pipelined_parallel_solve_equals_parallel_solve(name, prec, monkeypatch):
+    """The pipelined parallel-solve column kernels (variants 19-21: tiles
+    streamed into shared memory by a producer warp) evaluate the
+    parallel-solve kernel's expressions (variant 16) on the same values: the
+    same fields, bit for bit, after five steps."""
+    out = {}
+    for v in ("16", "19", "20", "21"):
+        monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
+        c = W.Case(CASES / f"{name}.ini", precision=prec)
+        c.run(5, c.dt, 0.0)
+        c.sync()
+        out[v] = {k: c.field(k) for k in W.FIELDS}
+        c.close()
+    for v in ("19", "20", "21"):
+        for k in W.FIELDS:
+            assert np.array_equal(out["16"][k], out[v][k]), (v, k)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "bubble_open", "straka_periodic",
                                   "ops_periodic", "moist_blob"])
 @pytest.mark.parametrize("prec,tol", [("f64", 1e-11), ("f32", 1e-4)])
 def test_parallel_solve_column_agrees_to_rounding(name, prec, tol, monkeypatch):
     """The column kernels with the parallel tridiagonal solve (variants 16-18:
-    each level lane eliminates its own rows, cyclic reduction over the lanes)
-    solve the same rows as the Thomas-sweep kernels: after seven steps the
+    each level lane eliminates its own rows, cyclic reduction over the lanes;
+    19-21: the same fed by the pipelined bulk-tensor-load ring) solve the
+    same rows as the Thomas-sweep kernels: after seven steps the
     fields agree to rounding -- relative L2 <= 1e-11 (FP64) / 1e-4 (FP32, the
     FP32 step-parity bound against the oracle; measured up to 1.2e-5 on the
     moist convective case) of the field (u, v against the wind-speed
     scale) -- and the FP64 steps stay within 1e-10 of the FP64 oracle."""
     out = {}
-    variants = ["0"] + [v for v in ("16", "17", "18")]
+    variants = ["0"] + [v for v in ("16", "17", "18", "19", "20", "21")]
     for v in variants:
         monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
         c = W.Case(CASES / f"{name}.ini", precision=prec)

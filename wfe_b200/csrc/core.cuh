@@ -122,4 +122,24 @@ WFE_HD int map_lat(int i, int n, int last, int open) {
 // Vertical zero-gradient map for cell-centred fields (kernels.cu:695-707).
 WFE_HD int map_zc(int k, int nz) { return k < 0 ? 0 : (k > nz - 1 ? nz - 1 : k); }
 
+// The lateral ghost columns around the interior, kRefNG wide: the kRefNG rows
+// below and above it over the padded width, then the kRefNG columns west and
+// east of each interior row.  ring_column maps r in [0, ring_columns) to (i, j).
+WFE_HD long ring_columns(const Layout& L) { return 2L * kRefNG * (L.nx + 2 * kRefNG) + 2L * kRefNG * L.ny; }
+WFE_HD void ring_column(const Layout& L, long r, int* i, int* j) {
+  const long w = L.nx + 2 * kRefNG, band = (long)kRefNG * w;
+  if (r < band) {
+    *j = (int)(r / w) - kRefNG;
+    *i = (int)(r % w) - kRefNG;
+  } else if (r < 2 * band) {
+    *j = L.ny + (int)((r - band) / w);
+    *i = (int)((r - band) % w) - kRefNG;
+  } else {
+    const long q = r - 2 * band;
+    const int m = (int)(q % (2 * kRefNG));
+    *j = (int)(q / (2 * kRefNG));
+    *i = m < kRefNG ? m - kRefNG : L.nx + (m - kRefNG);
+  }
+}
+
 }  // namespace wfe

@@ -28,6 +28,7 @@
 
 #include "core.cuh"
 #include "kernels.cuh"
+#include "acou_pcr.cuh"
 #include "dyn_common.cuh"
 #include "tma.cuh"
 
@@ -948,41 +949,24 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
 #undef SQ
 }
 
-// Column variant with a parallel tridiagonal solve.  Level lane p owns the
-// KCH levels klo = p KCH .. klo + KCH - 1 (in registers); the system is
-// padded with identity rows (x = 0) at level 0, the lid and above it, which
-// leaves the solution unchanged (the rows beside them couple to them with
-// zero coefficients: A at level 1 and C at level nz - 1 multiply aw = 0), so
-// every lane has exactly KCH rows.  Instead of one lane sweeping the whole
-// column while the others wait, every lane works:
-//   1. it eliminates its first KCH - 1 rows, with its last row's unknown
-//      y_p and the previous lane's y_{p-1} as parameters: x_k = G_k +
-//      A_k y_{p-1} + B_k y_p (one Thomas pass, three right-hand sides);
-//   2. its last row, with the first-row expression of the lane above,
-//      becomes one row L y_{p-1} + M y_p + U y_{p+1} = F of a tridiagonal
-//      system in the lanes' y_p;
-//   3. that system is solved by parallel cyclic reduction over the level
-//      lanes through shared memory (log2(KL) steps), and each lane recovers
-//      its rows from y_{p-1} and y_p.
-// Phases 1-3 and 5 are the chunked kernel's expressions; the solution differs
-// from the serial Thomas sweep by rounding only (a different elimination
-// order), so this variant is not bit-identical to the other column kernels.
+// Column variant with a parallel tridiagonal solve (pcr_solve,
+// acou_pcr.cuh).  Level lane p owns the KCH levels klo = p KCH .. klo + KCH
+// - 1 (in registers); the system is padded with identity rows (x = 0) at
+// level 0, the lid and above it, which leaves the solution unchanged (the
+// rows beside them couple to them with zero coefficients: A at level 1 and C
+// at level nz - 1 multiply aw = 0), so every lane has exactly KCH rows and
+// every lane works, instead of one lane sweeping the whole column while the
+// others wait.  Phases 1-3 and 5 are the chunked kernel's expressions; the
+// solution differs from the serial Thomas sweep by rounding only (another
+// elimination order), so this variant is not bit-identical to the other
+// column kernels.
 template <typename R, int CX, int KL, int KCH>
 __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_column_pcr(AcouArgs<R> a) {
   static_assert(KCH >= 2, "every lane needs an interior row");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // pcr_solve's work area
   const Layout& L = a.L;
   const int nz = L.nz;
-  // shared arrays, [lane][column]: the first-row expressions (G, A, B), the
-  // reduced rows (L, M, U, F, double-buffered) and the lanes' y
-  constexpr int NL = KL * CX;
-  R* fG = reinterpret_cast<R*>(smem_raw);
-  R* fA = fG + NL;
-  R* fB = fA + NL;
-  R* red = fB + NL;
-  R* yv = red + 8 * NL;
   const int tx = threadIdx.x, lane = threadIdx.y;
-  const int me = lane * CX + tx;
   const int i = blockIdx.x * CX + tx, j = blockIdx.y;
   const bool active = i < L.nx;
   const R dtau = a.dtau;
@@ -1083,87 +1067,13 @@ __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_co
       wsurf = us * hxc + vs * hyc;
     }
   }
-  // ---- 1. rows 1 .. KCH-1 in terms of (y_{p-1}, y_p)
-  R Gx[KCH + 1], Ax[KCH + 1], Bx[KCH + 1];
-  {
-    R cp[KCH], gp[KCH], ap[KCH], bp[KCH];
-#pragma unroll
-    for (int q = 1; q < KCH; ++q) {
-      const R r = (R)1 / (Br[q] - Ar[q] * (q > 1 ? cp[q - 1] : (R)0));
-      cp[q] = q == KCH - 1 ? (R)0 : Cr[q] * r;
-      gp[q] = (Dr[q] - Ar[q] * (q > 1 ? gp[q - 1] : (R)0)) * r;
-      ap[q] = ((q == 1 ? -Ar[q] : (R)0) - Ar[q] * (q > 1 ? ap[q - 1] : (R)0)) * r;
-      bp[q] = ((q == KCH - 1 ? -Cr[q] : (R)0) - Ar[q] * (q > 1 ? bp[q - 1] : (R)0)) * r;
-    }
-#pragma unroll
-    for (int q = KCH - 1; q >= 1; --q) {
-      if (q == KCH - 1) {
-        Gx[q] = gp[q], Ax[q] = ap[q], Bx[q] = bp[q];
-      } else {
-        Gx[q] = gp[q] - cp[q] * Gx[q + 1];
-        Ax[q] = ap[q] - cp[q] * Ax[q + 1];
-        Bx[q] = bp[q] - cp[q] * Bx[q + 1];
-      }
-    }
-  }
-  fG[me] = Gx[1];
-  fA[me] = Ax[1];
-  fB[me] = Bx[1];
-  __syncthreads();
-  // ---- 2. the lane's row of the reduced system: its last row with x of the
-  // row below it (this lane's row KCH - 1) and of the row above it (the
-  // first row of the lane above; none above the top lane)
-  R gn = 0, an = 0, bn = 0;
-  if (lane + 1 < KL) {
-    gn = fG[me + CX];
-    an = fA[me + CX];
-    bn = fB[me + CX];
-  }
-  R Lr = Ar[KCH] * Ax[KCH - 1];
-  R Mr = Br[KCH] + Ar[KCH] * Bx[KCH - 1] + Cr[KCH] * an;
-  R Ur = Cr[KCH] * bn;
-  R Fr = Dr[KCH] - Ar[KCH] * Gx[KCH - 1] - Cr[KCH] * gn;
-  // ---- 3. parallel cyclic reduction over the lanes
-  R* buf = red;
-  buf[me] = Lr;
-  buf[NL + me] = Mr;
-  buf[2 * NL + me] = Ur;
-  buf[3 * NL + me] = Fr;
-  __syncthreads();
-#pragma unroll
-  for (int h = 1; h < KL; h *= 2) {
-    R* nb = buf == red ? red + 4 * NL : red;
-    R al = 0, ga = 0, Lm = 0, Um = 0, Fm = 0, Lp = 0, Up = 0, Fp = 0;
-    if (lane - h >= 0) {
-      const int o = me - h * CX;
-      al = -Lr / buf[NL + o];
-      Lm = buf[o];
-      Um = buf[2 * NL + o];
-      Fm = buf[3 * NL + o];
-    }
-    if (lane + h < KL) {
-      const int o = me + h * CX;
-      ga = -Ur / buf[NL + o];
-      Lp = buf[o];
-      Up = buf[2 * NL + o];
-      Fp = buf[3 * NL + o];
-    }
-    Mr = Mr + al * Um + ga * Lp;
-    Fr = Fr + al * Fm + ga * Fp;
-    Lr = al * Lm;
-    Ur = ga * Up;
-    nb[me] = Lr;
-    nb[NL + me] = Mr;
-    nb[2 * NL + me] = Ur;
-    nb[3 * NL + me] = Fr;
-    buf = nb;
-    __syncthreads();
-  }
-  const R y = Fr / Mr;
-  yv[me] = y;
-  __syncthreads();
-  const R yprev = lane > 0 ? yv[me - CX] : (R)0;
-  const R ynext = lane + 1 < KL ? yv[me + CX] : (R)0;
+  PcrLane<R, KCH> sol;
+  pcr_solve<R, CX, KL, KCH>(Ar, Br, Cr, Dr, reinterpret_cast<R*>(smem_raw), tx, lane,
+                            [] { __syncthreads(); }, sol);
+  const R y = sol.y, yprev = sol.yprev, ynext = sol.ynext, gn = sol.gn, an = sol.an, bn = sol.bn;
+  const R(&Gx)[KCH + 1] = sol.Gx;
+  const R(&Ax)[KCH + 1] = sol.Ax;
+  const R(&Bx)[KCH + 1] = sol.Bx;
   // ---- phase 5: pi', theta', w of the lane's levels
   if (active) {
     R wl[KCH + 2];  // w at the lane's levels and the level above them
@@ -1712,7 +1622,7 @@ int acoustic_pcr_shapes() { return kNumPcrShapes; }
 
 template <typename R>
 size_t pcr_smem(int cx, int kl) {
-  return (size_t)12 * cx * kl * sizeof(R);
+  return (size_t)kPcrWork * cx * kl * sizeof(R);
 }
 
 template <typename R>

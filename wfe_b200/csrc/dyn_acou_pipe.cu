@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 
+#include "acou_pcr.cuh"
 #include "core.cuh"
 #include "kernels.cuh"
 #include "dyn_common.cuh"
@@ -80,6 +81,39 @@ struct PipeLayout {
   }
 };
 
+// The producer thread of a pipelined column CTA: for each of the CTA's tiles
+// in order, wait until the consumers released the stage's previous tile,
+// then stream the tile's boxes into the stage with bulk tensor loads (no
+// multicast: the maps cover this GPU's own fields only).  Every wait is
+// bounded; on a timeout it sets *err and stops issuing.
+template <typename R, int CX, int NST>
+__device__ __forceinline__ void pipe_produce(const PipeColParams<R>& p, const PipeLayout<R>& lay,
+                                             unsigned char* smem_pipe, uint64_t* full, uint64_t* empty,
+                                             int ntx, int ntiles) {
+  const bool moist = p.a.p.moisture != 0;
+  const bool has_tpi = p.has_tpi != 0;
+  int n = 0, armed[NST];
+  for (int s = 0; s < NST; ++s) armed[s] = -1;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
+    const int s = n % NST, use = n / NST;
+    // the consumers released this stage's previous tile
+    if (use > 0 && !tma::mbar_wait_for(&empty[s], (use - 1) & 1, kPipeWaitNs)) {
+      atomicExch(p.err, 1u);
+      break;
+    }
+    tma::mbar_arrive_expect_tx(&full[s], lay.tx_bytes);
+    armed[s] = use;
+    unsigned char* stg = smem_pipe + lay.stage0 + (size_t)s * lay.stage_bytes;
+    const int x = (t % ntx) * CX + kOX, y = t / ntx + kOY, z = kOZ;
+    for (int f = 0; f < TC_N; ++f)
+      if (pipe_loaded(f, moist, has_tpi)) tma::load_3d(stg + lay.field[f], &p.map[f], x, y, z, &full[s]);
+  }
+  // loads this CTA armed must land before it exits (they have, unless the
+  // consumers gave up early)
+  for (int s = 0; s < NST; ++s)
+    if (armed[s] >= 0) tma::mbar_wait_for(&full[s], armed[s] & 1, kPipeWaitNs);
+}
+
 template <typename R, int CX, int KL, int KCH, int NST>
 __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
     k_acoustic_column_pipe(const __grid_constant__ PipeColParams<R> p) {
@@ -106,28 +140,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
   __syncthreads();
 
   if (tid >= NC) {
-    // ------------------------------------------------------------ producer
-    if (tid != NC) return;
-    int n = 0, armed[NST];
-    for (int s = 0; s < NST; ++s) armed[s] = -1;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
-      const int s = n % NST, use = n / NST;
-      // the consumers released this stage's previous tile
-      if (use > 0 && !tma::mbar_wait_for(&empty[s], (use - 1) & 1, kPipeWaitNs)) {
-        atomicExch(p.err, 1u);
-        break;
-      }
-      tma::mbar_arrive_expect_tx(&full[s], lay.tx_bytes);
-      armed[s] = use;
-      unsigned char* stg = smem_pipe + lay.stage0 + (size_t)s * lay.stage_bytes;
-      const int x = (t % ntx) * CX + kOX, y = t / ntx + kOY, z = kOZ;
-      for (int f = 0; f < TC_N; ++f)
-        if (pipe_loaded(f, moist, has_tpi)) tma::load_3d(stg + lay.field[f], &p.map[f], x, y, z, &full[s]);
-    }
-    // loads this CTA armed must land before it exits (they have, unless the
-    // consumers gave up early)
-    for (int s = 0; s < NST; ++s)
-      if (armed[s] >= 0) tma::mbar_wait_for(&full[s], armed[s] & 1, kPipeWaitNs);
+    if (tid == NC) pipe_produce<R, CX, NST>(p, lay, smem_pipe, full, empty, ntx, ntiles);
     return;
   }
 
@@ -333,6 +346,241 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
   }
 }
 
+// The pipelined column with the parallel solve: the producer warp and the
+// stage ring of k_acoustic_column_pipe, the phases and the solve of the
+// parallel-solve column kernel (dyn_acou.cu: level lane p owns the levels
+// p KCH .. p KCH + KCH - 1 in registers, identity rows pad the column,
+// pcr_solve).  The consumers release a stage as soon as phases 1-3 have read
+// it, so the next tile's boxes land while this tile is solved, and no lane
+// waits for a serial sweep.  Every expression is the parallel-solve kernel's
+// on the same values (from shared memory instead of global memory).
+template <typename R, int CX, int KL, int KCH, int NST>
+__global__ void __launch_bounds__(CX * KL + 32)
+    k_acoustic_column_pipe_pcr(const __grid_constant__ PipeColParams<R> p) {
+  extern __shared__ __align__(128) unsigned char smem_pipe[];
+  constexpr int NC = CX * KL;  // consumer threads; the last warp produces
+  const AcouArgs<R>& a = p.a;
+  const Layout& L = a.L;
+  const int nz = L.nz;
+  const bool moist = a.p.moisture != 0;
+  const bool has_tpi = p.has_tpi != 0;
+  const PipeLayout<R> lay(CX, nz, NST, moist, has_tpi);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_pipe);
+  uint64_t* empty = full + NST;
+  const int tid = threadIdx.x;
+  const int ntx = (L.nx + CX - 1) / CX;
+  const int ntiles = ntx * L.ny;
+  if (tid == 0) {
+    for (int s = 0; s < NST; ++s) {
+      tma::mbar_init(&full[s], 1);
+      tma::mbar_init(&empty[s], 1);
+    }
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid >= NC) {
+    if (tid == NC) pipe_produce<R, CX, NST>(p, lay, smem_pipe, full, empty, ntx, ntiles);
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const int tx = tid % CX, lane = tid / CX;
+  R* work = reinterpret_cast<R*>(smem_pipe + lay.work);
+  // the per-level tables every tile reads, once per CTA: 1/dzc, 1/dzw and the
+  // terrain factor of the w levels, at level k
+  R* lvl_idzc = work + kPcrWork * NC;
+  R* lvl_idzw = lvl_idzc + (nz + 1);
+  R* lvl_facw = lvl_idzw + (nz + 1);
+  for (int k = tid; k <= nz; k += NC) {
+    lvl_idzc[k] = a.co.inv_dzc[L.at1(k)];
+    lvl_idzw[k] = a.co.inv_dzw[L.at1(k)];
+    lvl_facw[k] = a.co.fac_w[L.at1(k)];
+  }
+  const R dtau = a.dtau;
+  const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
+  const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
+  const size_t pl = L.plane();
+  const int klo = lane * KCH;
+  auto csync = [] { tma::named_sync(1, NC); };
+  csync();
+  int n = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
+    const int s = n % NST, use = n / NST;
+    // the column's metric, loaded while the tile's boxes may still be landing
+    const int i = (t % ntx) * CX + tx, j = t / ntx;
+    const bool active = i < L.nx;
+    const size_t c2d = L.at2(active ? i : 0, j);
+    const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
+    const bool ok = tma::mbar_wait_for(&full[s], use & 1, kPipeWaitNs);
+    if (tma::named_or(1, NC, !ok)) {
+      if (tid == 0) atomicExch(p.err, 1u);
+      break;
+    }
+    const unsigned char* stg = smem_pipe + lay.stage0 + (size_t)s * lay.stage_bytes;
+    auto fld = [&](int f) { return reinterpret_cast<const R*>(stg + lay.field[f]); };
+    const R* sU = fld(TC_U);
+    const R* sRX = fld(TC_RTJX);
+    const R* sV = fld(TC_V);
+    const R* sRY = fld(TC_RTJY);
+    const R* sW = fld(TC_W);
+    const R* sPI = fld(TC_PI);
+    const R* sTH = fld(TC_TH);
+    const R* sTW = fld(TC_TW);
+    const R* sTTH = fld(TC_TTH);
+    const R* sTPI = fld(TC_TPI);
+    const R* sAW = fld(TC_AW);
+    const R* sKT = fld(TC_KT3);
+    const R* sTHBW = fld(TC_THBW);
+    const R* sDTHB = fld(TC_DTHB);
+    const R* sQV = fld(TC_QV);
+    const R* sQC = fld(TC_QC);
+    const R* sQR = fld(TC_QR);
+    const R* sQVB = fld(TC_QVB);
+#define UF(k, d) sU[(k) * (CX + 4) + tx + (d)]
+#define RXF(k, d) sRX[(k) * (CX + 4) + tx + (d)]
+#define VF(k, r) sV[((k) * 2 + (r)) * CX + tx]
+#define RYF(k, r) sRY[((k) * 2 + (r)) * CX + tx]
+#define CF(X, k) X[(k) * CX + tx]
+    const R invJ = (R)1 / J;
+    const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
+    const bool terrain = hxc != (R)0 || hyc != (R)0;
+    R av[KCH + 2], sv[KCH + 2], P[KCH + 1], E[KCH + 1], th[KCH + 1], tt[KCH + 1], db[KCH + 1];
+    R Ar[KCH + 1], Br[KCH + 1], Cr[KCH + 1], Dr[KCH + 1];
+    R wsurf = 0;
+#pragma unroll
+    for (int q = 0; q < KCH + 1; ++q) Ar[q] = 0, Br[q] = 1, Cr[q] = 0, Dr[q] = 0;
+    if (active) {
+      // phase 1 on levels klo-1 .. klo+KCH
+#pragma unroll
+      for (int q = 0; q < KCH + 2; ++q) {
+        const int k = klo - 1 + q;
+        R avk = 0, svk = 0;
+        if (k >= 1 && k < nz) {
+          avk = CF(sAW, k);
+          if (terrain) {
+            R uw = (R)0.25 * (UF(k - 1, 0) + UF(k - 1, 1) + UF(k, 0) + UF(k, 1));
+            R vw = (R)0.25 * (VF(k - 1, 0) + VF(k - 1, 1) + VF(k, 0) + VF(k, 1));
+            svk = avk * (uw * hxc + vw * hyc) * lvl_facw[k];
+          }
+        }
+        av[q] = avk;
+        sv[q] = svk;
+      }
+      // phase 2 on levels klo-1 .. klo+KCH-1
+#pragma unroll
+      for (int q = 0; q < KCH + 1; ++q) {
+        const int k = klo - 1 + q;
+        R pk = 0, ek = 0;
+        if (k >= 0 && k < nz) {
+          R Kt = CF(sKT, k);
+          R Dh = (RXF(k, 1) * UF(k, 1) - RXF(k, 0) * UF(k, 0)) * mcx +
+                 (RYF(k, 1) * VF(k, 1) - RYF(k, 0) * VF(k, 0)) * mcy;
+          R idz = lvl_idzc[k];
+          R wk = CF(sW, k), wkp = CF(sW, k + 1);
+          R tpi = has_tpi ? CF(sTPI, k) : (R)0;
+          pk = CF(sPI, k) + dtau * tpi -
+               dtau * Kt * (Dh - (sv[q + 1] - sv[q]) * idz + c2 * (av[q + 1] * wkp - av[q] * wk) * idz);
+          ek = dtau * Kt * c1 * idz;
+        }
+        P[q] = pk;
+        E[q] = ek;
+      }
+      // phase 3: rows of the inner levels, and phase 5's inputs
+#pragma unroll
+      for (int q = 1; q < KCH + 1; ++q) {
+        const int k = klo - 1 + q;
+        th[q] = tt[q] = db[q] = 0;
+        if (k < nz) {
+          th[q] = CF(sTH, k);
+          tt[q] = CF(sTTH, k);
+          db[q] = CF(sDTHB, k);
+        }
+        if (k >= 1 && k < nz) {
+          const R iJdz = invJ * lvl_idzw[k];
+          R thc = th[q], thm = CF(sTH, k - 1);
+          R thbw = CF(sTHBW, k);
+          R thvw = thbw + (R)0.5 * (thm + thc);
+          if (moist) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k));
+          R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
+          R Em = E[q - 1], Ek = E[q];
+          Ar[q] = -G * Em * av[q - 1];
+          Br[q] = (R)1 + G * av[q] * (Ek + Em);
+          Cr[q] = -G * Ek * av[q + 1];
+          R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
+          if (moist) {
+            R dqv = (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k)) - (R)0.5 * (CF(sQVB, k - 1) + CF(sQVB, k));
+            R qcr = (R)0.5 * (CF(sQC, k - 1) + CF(sQC, k)) + (R)0.5 * (CF(sQR, k - 1) + CF(sQR, k));
+            buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
+          }
+          R RHS = CF(sW, k) + dtau * (buoy + CF(sTW, k)) -
+                  dtau * Phys<R>::cp * thvw * c2 * (CF(sPI, k) - CF(sPI, k - 1)) * iJdz;
+          Dr[q] = RHS - G * (P[q] - P[q - 1]);
+        }
+      }
+      if (lane == 0) {  // diagnostic surface w from the new u, v
+        R us = (R)0.5 * (UF(0, 0) + UF(0, 1));
+        R vs = (R)0.5 * (VF(0, 0) + VF(0, 1));
+        wsurf = us * hxc + vs * hyc;
+      }
+    }
+#undef UF
+#undef RXF
+#undef VF
+#undef RYF
+#undef CF
+    // every input of this tile is in registers: the producer may refill the
+    // stage (the barrier also ends the previous tile's use of the work area)
+    csync();
+    if (tid == 0) tma::mbar_arrive(&empty[s]);
+    PcrLane<R, KCH> sol;
+    pcr_solve<R, CX, KL, KCH>(Ar, Br, Cr, Dr, work, tx, lane, csync, sol);
+    // phase 5: pi', theta', w of the lane's levels
+    if (active) {
+      const size_t c0 = L.at(i, j, 0);
+      R wl[KCH + 2];  // w at the lane's levels and the level above them
+#pragma unroll
+      for (int q = 1; q < KCH; ++q) wl[q] = sol.Gx[q] + sol.Ax[q] * sol.yprev + sol.Bx[q] * sol.y;
+      wl[KCH] = sol.y;
+      wl[KCH + 1] = sol.gn + sol.an * sol.y + sol.bn * sol.ynext;
+      if (lane == 0) wl[1] = wsurf;  // level 0: the diagnostic surface w
+#pragma unroll
+      for (int q = 1; q < KCH + 1; ++q) {
+        const int k = klo - 1 + q;
+        if (k > nz) continue;
+        const size_t c = c0 + (size_t)k * pl;
+        if (k == nz) {
+          a.w_out[c] = 0;
+          continue;
+        }
+        const R wn = wl[q], wn1 = k + 1 >= nz ? (R)0 : wl[q + 1];
+        a.pi_next[c] = P[q] - E[q] * (av[q + 1] * wn1 - av[q] * wn);
+        R wc = (R)0.5 * (wn + wn1);
+        a.th_out[c] = th[q] + dtau * (tt[q] - wc * db[q]);
+        a.w_out[c] = wn;
+      }
+    }
+  }
+}
+
+// columns, level lanes, levels per lane, stages
+constexpr PipeShape kPipePcrShapes[] = {{16, 16, 3, 2}, {8, 16, 3, 2}, {8, 16, 3, 3}};
+constexpr int kNumPipePcrShapes = 3;
+
+template <typename R, int F>
+struct PipePcrKernel {
+  static constexpr PipeShape S = kPipePcrShapes[F];
+  static constexpr auto fn = k_acoustic_column_pipe_pcr<R, S.cx, S.kl, S.kch, S.nst>;
+};
+
+template <typename R>
+const void* pipe_pcr_fn(int f) {
+  switch (f) {
+    case 0: return reinterpret_cast<const void*>(PipePcrKernel<R, 0>::fn);
+    case 1: return reinterpret_cast<const void*>(PipePcrKernel<R, 1>::fn);
+    default: return reinterpret_cast<const void*>(PipePcrKernel<R, 2>::fn);
+  }
+}
+
 template <typename R, int F>
 struct PipeKernel {
   static constexpr PipeShape S = kPipeShapes[F];
@@ -348,22 +596,20 @@ const void* pipe_fn(int f) {
   }
 }
 
-// resident CTAs per SM of shape f at `smem` bytes, and the SM count (cached)
-template <typename R>
-int pipe_grid_limit(int f, size_t smem) {
+// resident CTAs of kernel fn (threads per CTA, `smem` bytes) on the whole
+// device: the persistent grid (cached)
+int pipe_grid_limit(const void* fn, int threads, size_t smem) {
   static std::mutex mu;
-  static std::map<std::pair<int, std::pair<int, size_t>>, int> cache;
+  static std::map<std::pair<std::pair<int, const void*>, size_t>, int> cache;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   std::lock_guard<std::mutex> lk(mu);
-  const auto key = std::make_pair(dev, std::make_pair(f, smem));
+  const auto key = std::make_pair(std::make_pair(dev, fn), smem);
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   int sms = 0, occ = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  const int threads = kPipeShapes[f].cx * kPipeShapes[f].kl + 32;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pipe_fn<R>(f), threads, smem) != cudaSuccess)
-    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) return 0;
   return cache[key] = sms * occ;
 }
 
@@ -385,20 +631,56 @@ size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi) {
 }
 
 template <typename R>
+size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi) {
+  if (shape < 0 || shape >= kNumPipePcrShapes) return 0;
+  const PipeShape& S = kPipePcrShapes[shape];
+  if (nz + 1 > S.kl * S.kch || nz + 1 > 256) return 0;  // rows; a box extent is <= 256
+  const size_t t = PipeLayout<R>(S.cx, nz, S.nst, moist, tpi).work +
+                   ((size_t)kPcrWork * S.kl * S.cx + 3 * (size_t)(nz + 1)) * sizeof(R);
+  return t <= 227 * 1024 ? t : 0;
+}
+
+template <typename R>
 int prepare_acoustic_pipe(int nz) {
   bool any = false;
-  for (int f = 0; f < kNumPipeShapes; ++f) {
-    size_t sm = 0;
-    for (int moist = 0; moist < 2; ++moist)
-      for (int tpi = 0; tpi < 2; ++tpi) {
-        const size_t t = acoustic_pipe_smem<R>(f, nz, moist != 0, tpi != 0);
-        if (t > sm) sm = t;
-      }
-    if (!sm) continue;
-    if (raise_smem_limit(pipe_fn<R>(f), sm) != cudaSuccess) return 1;
-    any = true;
-  }
+  for (int pcr = 0; pcr < 2; ++pcr)
+    for (int f = 0; f < (pcr ? kNumPipePcrShapes : kNumPipeShapes); ++f) {
+      size_t sm = 0;
+      for (int moist = 0; moist < 2; ++moist)
+        for (int tpi = 0; tpi < 2; ++tpi) {
+          const size_t t = pcr ? acoustic_pipe_pcr_smem<R>(f, nz, moist != 0, tpi != 0)
+                               : acoustic_pipe_smem<R>(f, nz, moist != 0, tpi != 0);
+          if (t > sm) sm = t;
+        }
+      if (!sm) continue;
+      if (raise_smem_limit(pcr ? pipe_pcr_fn<R>(f) : pipe_fn<R>(f), sm) != cudaSuccess) return 1;
+      any = true;
+    }
   return any ? 0 : 2;
+}
+
+int acoustic_pipe_pcr_shapes() { return kNumPipePcrShapes; }
+
+void acoustic_pipe_pcr_box(int shape, int f, int nz, int* bx, int* by, int* bz) {
+  pipe_box(kPipePcrShapes[shape].cx, f, nz, bx, by, bz);
+}
+
+template <typename R>
+int launch_acoustic_column_pipe_pcr(const PipeColParams<R>& p, int f, cudaStream_t st) {
+  const size_t sm = acoustic_pipe_pcr_smem<R>(f, p.a.L.nz, p.a.p.moisture != 0, p.has_tpi != 0);
+  if (!sm) return 2;
+  const PipeShape& S = kPipePcrShapes[f];
+  const int ntiles = (p.a.L.nx + S.cx - 1) / S.cx * p.a.L.ny;
+  const int threads = S.cx * S.kl + 32;
+  const int lim = pipe_grid_limit(pipe_pcr_fn<R>(f), threads, sm);
+  if (lim <= 0) return 2;
+  const int grid = ntiles < lim ? ntiles : lim;
+  switch (f) {
+    case 0: PipePcrKernel<R, 0>::fn<<<grid, threads, sm, st>>>(p); break;
+    case 1: PipePcrKernel<R, 1>::fn<<<grid, threads, sm, st>>>(p); break;
+    default: PipePcrKernel<R, 2>::fn<<<grid, threads, sm, st>>>(p); break;
+  }
+  return 0;
 }
 
 template <typename R>
@@ -407,10 +689,10 @@ int launch_acoustic_column_pipe(const PipeColParams<R>& p, int f, cudaStream_t s
   if (!sm) return 2;
   const PipeShape& S = kPipeShapes[f];
   const int ntiles = (p.a.L.nx + S.cx - 1) / S.cx * p.a.L.ny;
-  const int lim = pipe_grid_limit<R>(f, sm);
+  const int threads = S.cx * S.kl + 32;
+  const int lim = pipe_grid_limit(pipe_fn<R>(f), threads, sm);
   if (lim <= 0) return 2;
   const int grid = ntiles < lim ? ntiles : lim;
-  const int threads = S.cx * S.kl + 32;
   switch (f) {
     case 0: PipeKernel<R, 0>::fn<<<grid, threads, sm, st>>>(p); break;
     case 1: PipeKernel<R, 1>::fn<<<grid, threads, sm, st>>>(p); break;
@@ -421,8 +703,10 @@ int launch_acoustic_column_pipe(const PipeColParams<R>& p, int f, cudaStream_t s
 
 #define WFE_INST(R)                                                              \
   template size_t acoustic_pipe_smem<R>(int, int, bool, bool);                   \
+  template size_t acoustic_pipe_pcr_smem<R>(int, int, bool, bool);               \
   template int prepare_acoustic_pipe<R>(int);                                    \
-  template int launch_acoustic_column_pipe<R>(const PipeColParams<R>&, int, cudaStream_t);
+  template int launch_acoustic_column_pipe<R>(const PipeColParams<R>&, int, cudaStream_t); \
+  template int launch_acoustic_column_pipe_pcr<R>(const PipeColParams<R>&, int, cudaStream_t);
 WFE_INST(float)
 WFE_INST(double)
 #undef WFE_INST

@@ -44,29 +44,38 @@ __host__ __device__ inline int fill_chunks(int nz) {
 
 template <typename R>
 __device__ __forceinline__ void fill_body(const FillArgs<R>& A, int bx, int by, int bz) {
-  // one thread per padded column (i, j) of one field and part: part 0 fills
-  // the ghost levels of the interior columns, part p >= 1 the p-th chunk of
-  // kFillChunk levels of the lateral ghost columns (so that no thread walks a
-  // whole column)
+  // one thread per work item of field bz: items [0, nx ny) fill the ghost
+  // levels of one interior column; the rest fill one chunk of kFillChunk
+  // levels of one lateral ghost column (ring_column), chunk by chunk over the
+  // ring -- no thread walks a whole column and none idles on a point that is
+  // not a ghost
   const Layout& L = A.L;
   const int open_x = A.open_x, open_y = A.open_y;
-  const int nparts = 1 + fill_chunks(L.nz);
-  const int f = bz / nparts, part = bz % nparts;
+  const int f = bz;
   if (f >= A.job.n) return;
   R* a = A.job.f[f];
   const int kind = A.job.kind[f];
-  const int i = (int)(bx * blockDim.x + threadIdx.x) - kRefNG;
-  const int j = (int)(by * blockDim.y + threadIdx.y) - kRefNG;
-  if (i > L.nx + 2 || j > L.ny + 2) return;
+  const long item = (long)bx * blockDim.x + threadIdx.x;
+  const long ncol = (long)L.nx * L.ny, nring = ring_columns(L);
+  int i, j, part;  // part 0: ghost levels of an interior column; p >= 1: chunk p - 1
+  if (item < ncol) {
+    i = (int)(item % L.nx);
+    j = (int)(item / L.nx);
+    part = 0;
+  } else {
+    const long r = item - ncol;
+    if (r >= nring * fill_chunks(L.nz)) return;
+    ring_column(L, r % nring, &i, &j);
+    part = 1 + (int)(r / nring);
+  }
   const int ilast = (kind == 1 && open_x) ? L.nx : L.nx - 1;
   const int jlast = (kind == 2 && open_y) ? L.ny : L.ny - 1;
   const int si = map_lat(i, L.nx, ilast, open_x);
   const int sj = map_lat(j, L.ny, jlast, open_y);
   const int k0 = -kRefNG, k1 = L.nz + kRefNG;  // inclusive
   if ((si != i) || (sj != j)) {
-    // lateral ghost column, levels of this part; the sources are another
+    // lateral ghost column, levels of this chunk; the sources are another
     // column, so the loads are issued before the stores
-    if (part == 0) return;
     const int kb = k0 + (part - 1) * kFillChunk;
     R v[kFillChunk];
 #pragma unroll
@@ -77,8 +86,11 @@ __device__ __forceinline__ void fill_body(const FillArgs<R>& A, int bx, int by, 
       if (kb + u <= k1) a[L.at(i, j, kb + u)] = v[u];
     return;
   }
-  if (part != 0) return;
-  // interior column: the levels below 0 and from nz up (w(nz) is the rigid lid)
+  // a column that is its own source: an interior column, or a ring column
+  // that is not a ghost (the u faces nx of an open x boundary, the v faces ny
+  // of an open y boundary; its first chunk's item fills it)
+  if (part > 1) return;
+  // the levels below 0 and from nz up (w(nz) is the rigid lid)
   R lo[kRefNG], hi[kRefNG + 1];
 #pragma unroll
   for (int m = 1; m <= kRefNG; ++m) lo[m - 1] = ghost_value(L, a, kind, i, j, -m);
@@ -593,9 +605,12 @@ void launch_axpy(const R* x, const R* y, R a, R* out, size_t n, cudaStream_t st)
 }
 
 // ------------------------------------------------------------ host launch
+// 256-thread blocks over the interior columns and the ring's chunks, one z
+// slice per field
 template <typename R>
 dim3 grid_fill(const FillArgs<R>& a) {
-  return dim3((a.L.nx + 6 + 31) / 32, (a.L.ny + 6 + 3) / 4, a.job.n * (1 + fill_chunks(a.L.nz)));
+  const long items = (long)a.L.nx * a.L.ny + ring_columns(a.L) * fill_chunks(a.L.nz);
+  return dim3((unsigned)((items + 255) / 256), 1, a.job.n);
 }
 
 template <typename R>
@@ -603,12 +618,12 @@ void launch_fill_ghosts(const Layout& L, const GhostJob<R>& job, int open_x, int
                         cudaStream_t st) {
   if (job.n == 0) return;
   FillArgs<R> a{L, job, open_x, open_y};
-  k_fill_ghosts<R><<<grid_fill(a), dim3(32, 4), 0, st>>>(a);
+  k_fill_ghosts<R><<<grid_fill(a), 256, 0, st>>>(a);
 }
 
 template <typename R>
 void batch_fill(const Batch<FillArgs<R>>& b, int nblocks, cudaStream_t st) {
-  k_fill_ghosts_batch<R><<<nblocks, dim3(32, 4), 0, st>>>(b);
+  k_fill_ghosts_batch<R><<<nblocks, 256, 0, st>>>(b);
 }
 
 template <typename R>

@@ -375,6 +375,17 @@ int prepare_acoustic_pipe(int nz);
 // Returns 0 ok, 2 does not fit
 template <typename R>
 int launch_acoustic_column_pipe(const PipeColParams<R>& p, int shape, cudaStream_t st);
+// The same pipeline feeding the parallel-solve column (level lanes own
+// consecutive rows in registers, cyclic reduction across the lanes: equal to
+// the Thomas kernels to rounding); its own shapes, boxes and layouts, the
+// same params (maps encoded with acoustic_pipe_pcr_box).  prepare_acoustic_pipe
+// raises these kernels' limits too.
+int acoustic_pipe_pcr_shapes();
+void acoustic_pipe_pcr_box(int shape, int f, int nz, int* bx, int* by, int* bz);
+template <typename R>
+size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi);
+template <typename R>
+int launch_acoustic_column_pipe_pcr(const PipeColParams<R>& p, int shape, cudaStream_t st);
 // Persistent, pipelined forward u, v kernel (dyn_acou_pipe.cu): tiles of
 // kUvpX x kUvpY x kUvpZ faces; a producer warp streams each tile's boxes (the
 // cell fields with a one-cell halo toward -x, -y and +-z, the face fields

@@ -401,25 +401,23 @@ __global__ void __launch_bounds__(256) k_ad_tend(TendArgs<R> a, TendArgs<R> d) {
 
 // ================================================================ ghost fill
 // Adjoint of the ghost fill (forward: dyn_tend.cu fill_body): every written
-// ghost value moves its adjoint onto its interior sources and is zeroed.  One
-// thread per (padded column, level, field); interior points return at once.
+// ghost value moves its adjoint onto its sources and is zeroed.  The sources
+// are interior points, never other ghosts, so the points can go in any order.
+// Threads cover only ghost points: k_ad_fill_levels the ghost levels of the
+// interior columns, k_ad_fill_ring every level of the lateral ghost columns.
 template <typename R>
-__global__ void k_ad_fill(FillArgs<R> A, int nk) {
+__device__ __forceinline__ void ad_fill_point(const FillArgs<R>& A, int f, int i, int j, int k) {
   const Layout& L = A.L;
-  const int f = blockIdx.z / nk;
-  const int k = (int)(blockIdx.z % nk) - kRefNG;
-  if (f >= A.job.n) return;
   R* a = A.job.f[f];
   const int kind = A.job.kind[f];
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - kRefNG;
-  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - kRefNG;
-  if (i > L.nx + 2 || j > L.ny + 2) return;
   const int ilast = (kind == 1 && A.open_x) ? L.nx : L.nx - 1;
   const int jlast = (kind == 2 && A.open_y) ? L.ny : L.ny - 1;
   const int si = map_lat(i, L.nx, ilast, A.open_x);
   const int sj = map_lat(j, L.ny, jlast, A.open_y);
   const bool lateral = (si != i) || (sj != j);
-  if (!lateral && k >= 0 && k < L.nz) return;  // interior level of an interior column
+  // an interior level of a column that is not a ghost (the u face nx of an
+  // open x boundary, the v face ny of an open y boundary)
+  if (!lateral && k >= 0 && k < L.nz) return;
   const size_t q = L.at(i, j, k);
   // the ghost's adjoint moves to its sources; it is cleared only once read
   // (a store issued while the load of the same address is in flight stalls
@@ -439,6 +437,31 @@ __global__ void k_ad_fill(FillArgs<R> A, int nk) {
   } else {
     atomicAdd(a + L.at(si, sj, map_zc(k, L.nz)), g);
   }
+}
+
+// grid (nx ny / 256, 7 ghost levels: -3..-1 and nz..nz+3, fields)
+template <typename R>
+__global__ void __launch_bounds__(256) k_ad_fill_levels(FillArgs<R> A) {
+  const Layout& L = A.L;
+  const int f = blockIdx.z;
+  const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= A.job.n || col >= (long)L.nx * L.ny) return;
+  const int m = blockIdx.y;
+  const int k = m < kRefNG ? m - kRefNG : L.nz + (m - kRefNG);
+  ad_fill_point(A, f, (int)(col % L.nx), (int)(col / L.nx), k);
+}
+
+// grid (ring columns / 256, levels -3..nz+3, fields): the lateral ghost
+// columns (ring_column)
+template <typename R>
+__global__ void __launch_bounds__(256) k_ad_fill_ring(FillArgs<R> A) {
+  const Layout& L = A.L;
+  const int f = blockIdx.z;
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= A.job.n || r >= ring_columns(L)) return;
+  int i, j;
+  ring_column(L, r, &i, &j);
+  ad_fill_point(A, f, i, j, (int)blockIdx.y - kRefNG);
 }
 
 // =============================================================== mass fluxes
@@ -1494,9 +1517,9 @@ template <typename R>
 void ad_fill(const FillArgs<R>& d, cudaStream_t st) {
   if (d.job.n == 0) return;
   const int nk = d.L.nz + 1 + 2 * kRefNG;  // levels -3 .. nz+3
-  dim3 g = grid_fill(d);
-  g.z = (unsigned)(d.job.n * nk);
-  k_ad_fill<R><<<g, dim3(32, 4), 0, st>>>(d, nk);
+  const long cols = (long)d.L.nx * d.L.ny, ring = ring_columns(d.L);
+  k_ad_fill_levels<R><<<dim3((unsigned)((cols + 255) / 256), 2 * kRefNG + 1, d.job.n), 256, 0, st>>>(d);
+  k_ad_fill_ring<R><<<dim3((unsigned)((ring + 255) / 256), nk, d.job.n), 256, 0, st>>>(d);
 }
 
 template <typename R>

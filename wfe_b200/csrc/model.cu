@@ -769,7 +769,7 @@ class ModelT final : public Model {
   // launch the unfused kernels)
   int column_shape() const override {
     if (chunked_index(tune_.column_cx) >= 0 || pipe_index(tune_.column_cx) >= 0 ||
-        pcr_index(tune_.column_cx) >= 0)
+        pcr_index(tune_.column_cx) >= 0 || pipe_pcr_index(tune_.column_cx) >= 0)
       return 0;
     const int f = tune_.column_cx - acoustic_column_shapes() - 1;
     return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
@@ -797,6 +797,16 @@ class ModelT final : public Model {
   bool pcr_usable(int v) const {
     const int f = pcr_index(v);
     return f >= 0 && acoustic_pcr_fits<R>(g_.nz, f);
+  }
+  // pipelined parallel-solve column variants follow those; -1 otherwise
+  int pipe_pcr_index(int v) const {
+    const int f = v - acoustic_column_shapes() - 1 - acoustic_fused_shapes() - acoustic_chunked_shapes() -
+                  acoustic_pipe_shapes() - acoustic_pcr_shapes();
+    return (f >= 0 && f < acoustic_pipe_pcr_shapes()) ? f : -1;
+  }
+  bool pipe_pcr_usable(int v) const {
+    const int f = pipe_pcr_index(v);
+    return pipe_ok_ && f >= 0 && acoustic_pipe_pcr_smem<R>(f, g_.nz, dp_.moisture != 0, bdy_on_) > 0;
   }
   bool pipe_usable(int v) const {
     const int f = pipe_index(v);
@@ -887,8 +897,9 @@ class ModelT final : public Model {
   // WFE_COLUMN_VARIANT=<n> forces the acoustic variant (0..5 column tile
   // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
   // tile shapes, 10..12 the chunked column kernel, 13..15 the persistent
-  // pipelined column kernel, 16..18 the parallel-solve column kernel, equal
-  // to the others up to rounding), WFE_UV_VARIANT=<n> the forward u, v kernel (0
+  // pipelined column kernel, 16..18 the parallel-solve column kernel and
+  // 19..21 its pipelined form, both equal to the others up to rounding),
+  // WFE_UV_VARIANT=<n> the forward u, v kernel (0
   // thread per face, 1 persistent pipelined tiles) and WFE_TEND_VARIANT=<n>
   // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars,
   // 3 fused with two cells per thread)
@@ -900,7 +911,8 @@ class ModelT final : public Model {
     if (first && cv && *cv) {
       const int v = std::atoi(cv);
       if (v >= 0 && (v < acoustic_column_shapes() || (v == acoustic_column_shapes() && tma_ok_) ||
-                     fused_usable(v) || chunked_usable(v) || pipe_usable(v) || pcr_usable(v)))
+                     fused_usable(v) || chunked_usable(v) || pipe_usable(v) || pcr_usable(v) ||
+                     pipe_pcr_usable(v)))
         tune_.column_cx = v;
     }
     const char* uvv = std::getenv("WFE_UV_VARIANT");
@@ -959,16 +971,16 @@ class ModelT final : public Model {
     tune_.uv_variant = cached.uv_variant;
     best = 1e30f;
     // tile shapes, the TMA-staged column, the fused substep kernels
-    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() +
-                     acoustic_chunked_shapes() + acoustic_pipe_shapes() + acoustic_pcr_shapes();
+    const int nvar = acoustic_column_shapes() + 1 + acoustic_fused_shapes() + acoustic_chunked_shapes() +
+                     acoustic_pipe_shapes() + acoustic_pcr_shapes() + acoustic_pipe_pcr_shapes();
     for (int cx = 0; cx < nvar; ++cx) {
       if (cx == acoustic_column_shapes() && !tma_ok_) continue;
       if (cx > acoustic_column_shapes() && !fused_usable(cx) && !chunked_usable(cx) &&
-          !pipe_usable(cx) && !pcr_usable(cx))
+          !pipe_usable(cx) && !pcr_usable(cx) && !pipe_pcr_usable(cx))
         continue;
       // the parallel-solve variants agree with the others to rounding only:
       // the tuner picks them only where allowed (WFE_EXACT_COLUMN=0)
-      if (pcr_index(cx) >= 0 && !pcr_allowed()) continue;
+      if ((pcr_index(cx) >= 0 || pipe_pcr_index(cx) >= 0) && !pcr_allowed()) continue;
       float ms;
       tune_.column_cx = cx;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -1188,6 +1200,13 @@ class ModelT final : public Model {
         } else if (pcr_usable(tune_.column_cx)) {
           const int f = pcr_index(tune_.column_cx);
           launch("acoustic_column", [&] { rc = launch_acoustic_column_pcr<R>(a, f, st_); });
+        } else if (pipe_pcr_usable(tune_.column_cx) &&
+                   acoustic_pipe_pcr_smem<R>(pipe_pcr_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
+                                             a.tpi != nullptr) > 0) {
+          const int f = pipe_pcr_index(tune_.column_cx);
+          PipeColParams<R> pp;
+          if (pipe_params(a, f, &pp, true)) return 1;
+          launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe_pcr<R>(pp, f, st_); });
         } else if (pipe_usable(tune_.column_cx) &&
                    acoustic_pipe_smem<R>(pipe_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
                                          a.tpi != nullptr) > 0) {
@@ -1318,7 +1337,8 @@ class ModelT final : public Model {
     return 0;
   }
 
-  int pipe_params(const AcouArgs<R>& a, int shape, PipeColParams<R>* pp) {
+  // pcr: the boxes of the pipelined parallel-solve shapes
+  int pipe_params(const AcouArgs<R>& a, int shape, PipeColParams<R>* pp, bool pcr = false) {
     std::memset(static_cast<void*>(pp), 0, sizeof(*pp));
     pp->a = a;
     pp->err = tma_err_;
@@ -1330,7 +1350,10 @@ class ModelT final : public Model {
       if (f == TC_TPI && !a.tpi) continue;
       if (f >= TC_QV && !a.p.moisture) continue;
       int bx, by, bz;
-      acoustic_pipe_box(shape, f, g_.nz, &bx, &by, &bz);
+      if (pcr)
+        acoustic_pipe_pcr_box(shape, f, g_.nz, &bx, &by, &bz);
+      else
+        acoustic_pipe_box(shape, f, g_.nz, &bx, &by, &bz);
       const CUtensorMap* m = tmap3(src[f], bx, by, bz);
       if (!m) return 1;
       pp->map[f] = *m;
@@ -1655,17 +1678,21 @@ class EnsembleT final : public Ensemble {
       // pick on real steps among the batched launches, the members' own
       // graphs on concurrent streams and the members' own graphs one after
       // another (all three give the same values, bit for bit): three warm-up
-      // steps of each mode capture every phase's graphs, then two timed
-      // steps each, and the two close ones (concurrent, one after another)
-      // timed once more in turn, the faster of each pair kept
-      float tb = 0, tc = 0, tq = 0, t2 = 0;
+      // steps of each mode capture every phase's graphs; then the batched
+      // mode is timed over two steps and the two close modes over four, in
+      // the order concurrent, sequential, sequential, concurrent, so that a
+      // step cost that drifts as the flow develops weighs on both alike
+      float tb = 0, tc = 0, tq = 0, t1 = 0, t2 = 0;
       if (batched_steps(3, dt) || timed([&] { return batched_steps(2, dt); }, &tb)) return 1;
-      if (member_steps(3, dt, false) || timed([&] { return member_steps(2, dt, false); }, &tc)) return 1;
-      if (member_steps(3, dt, true) || timed([&] { return member_steps(2, dt, true); }, &tq)) return 1;
-      if (timed([&] { return member_steps(2, dt, false); }, &t2)) return 1;
-      tc = std::min(tc, t2);
+      if (member_steps(3, dt, false) || member_steps(3, dt, true)) return 1;
+      if (timed([&] { return member_steps(2, dt, false); }, &t1)) return 1;
       if (timed([&] { return member_steps(2, dt, true); }, &t2)) return 1;
-      tq = std::min(tq, t2);
+      tq = t2;
+      if (timed([&] { return member_steps(2, dt, true); }, &t2)) return 1;
+      tq += t2;
+      if (timed([&] { return member_steps(2, dt, false); }, &t2)) return 1;
+      tc = t1 + t2;
+      tb *= 2;  // per four steps, as tc and tq
       s = kModePickSteps;
       mode_done_ = true;
       if (tc <= tb && tc <= tq) tune_.persist = 2;
