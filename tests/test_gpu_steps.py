@@ -352,14 +352,14 @@ def test_pipelined_parallel_solve_equals_parallel_solve(name, prec, monkeypatch)
 def test_parallel_solve_column_agrees_to_rounding(name, prec, tol, monkeypatch):
     """The column kernels with the parallel tridiagonal solve (variants 16-18:
     each level lane eliminates its own rows, cyclic reduction over the lanes;
-    19-21: the same fed by the pipelined bulk-tensor-load ring) solve the
+    19-22: the same fed by the pipelined bulk-tensor-load ring) solve the
     same rows as the Thomas-sweep kernels: after seven steps the
     fields agree to rounding -- relative L2 <= 1e-11 (FP64) / 1e-4 (FP32, the
     FP32 step-parity bound against the oracle; measured up to 1.2e-5 on the
     moist convective case) of the field (u, v against the wind-speed
     scale) -- and the FP64 steps stay within 1e-10 of the FP64 oracle."""
     out = {}
-    variants = ["0"] + [v for v in ("16", "17", "18", "19", "20", "21")]
+    variants = ["0"] + [v for v in ("16", "17", "18", "19", "20", "21", "22")]
     for v in variants:
         monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
         c = W.Case(CASES / f"{name}.ini", precision=prec)

@@ -13,7 +13,7 @@
 //   2. its last row, with the first-row expression of the lane above, is one
 //      row L y_{p-1} + M y_p + U y_{p+1} = F of a system in the lanes' y;
 //   3. that system is solved by parallel cyclic reduction over the lanes
-//      through shared memory (log2(KL) steps).
+//      through shared memory (ceil(log2(KL)) steps).
 // The quotients are products with IEEE reciprocals; the solution equals the
 // Thomas sweep's to rounding.
 #pragma once

@@ -562,9 +562,10 @@ __global__ void __launch_bounds__(CX * KL + 32)
   }
 }
 
-// columns, level lanes, levels per lane, stages
-constexpr PipeShape kPipePcrShapes[] = {{16, 16, 3, 2}, {8, 16, 3, 2}, {8, 16, 3, 3}};
-constexpr int kNumPipePcrShapes = 3;
+// columns, level lanes, levels per lane, stages (14 lanes of 3 levels hold
+// the 41 rows of a 40-level column with one identity row instead of seven)
+constexpr PipeShape kPipePcrShapes[] = {{16, 16, 3, 2}, {8, 16, 3, 2}, {8, 16, 3, 3}, {16, 14, 3, 2}};
+constexpr int kNumPipePcrShapes = 4;
 
 template <typename R, int F>
 struct PipePcrKernel {
@@ -577,7 +578,8 @@ const void* pipe_pcr_fn(int f) {
   switch (f) {
     case 0: return reinterpret_cast<const void*>(PipePcrKernel<R, 0>::fn);
     case 1: return reinterpret_cast<const void*>(PipePcrKernel<R, 1>::fn);
-    default: return reinterpret_cast<const void*>(PipePcrKernel<R, 2>::fn);
+    case 2: return reinterpret_cast<const void*>(PipePcrKernel<R, 2>::fn);
+    default: return reinterpret_cast<const void*>(PipePcrKernel<R, 3>::fn);
   }
 }
 
@@ -678,7 +680,8 @@ int launch_acoustic_column_pipe_pcr(const PipeColParams<R>& p, int f, cudaStream
   switch (f) {
     case 0: PipePcrKernel<R, 0>::fn<<<grid, threads, sm, st>>>(p); break;
     case 1: PipePcrKernel<R, 1>::fn<<<grid, threads, sm, st>>>(p); break;
-    default: PipePcrKernel<R, 2>::fn<<<grid, threads, sm, st>>>(p); break;
+    case 2: PipePcrKernel<R, 2>::fn<<<grid, threads, sm, st>>>(p); break;
+    default: PipePcrKernel<R, 3>::fn<<<grid, threads, sm, st>>>(p); break;
   }
   return 0;
 }

@@ -1468,19 +1468,25 @@ __global__ void __launch_bounds__(256) k_ad_column_uv(AcouArgs<R> a, AcouArgs<R>
 }
 
 // Undo-log copies: up to kCopyMax whole fields (n elements each) in one
-// launch, 16-byte vectors, grid-stride over fields x chunks.
+// launch, 16-byte vectors; blockIdx.y picks the field, a grid-stride loop
+// over it with four loads in flight per thread before their stores.
 template <typename R>
 __global__ void __launch_bounds__(256) k_copy_fields(CopyJob<R> job, size_t n) {
   const size_t nv = n * sizeof(R) / 16;  // n * sizeof(R) is a multiple of 16 (copy_fields)
-  const size_t total = nv * (size_t)job.count;
-  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const int f = (int)(q / nv);
-    const size_t e = q - (size_t)f * nv;
-    reinterpret_cast<uint4*>(job.dst[f])[e] = reinterpret_cast<const uint4*>(job.src[f])[e];
+  const int f = blockIdx.y;
+  const uint4* __restrict__ src = reinterpret_cast<const uint4*>(job.src[f]);
+  uint4* __restrict__ dst = reinterpret_cast<uint4*>(job.dst[f]);
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; e + 3 * stride < nv; e += 4 * stride) {
+    const uint4 v0 = src[e], v1 = src[e + stride], v2 = src[e + 2 * stride], v3 = src[e + 3 * stride];
+    dst[e] = v0;
+    dst[e + stride] = v1;
+    dst[e + 2 * stride] = v2;
+    dst[e + 3 * stride] = v3;
   }
+  for (; e < nv; e += stride) dst[e] = src[e];
 }
-
 
 // zero every stored point of a cell field outside the interior cells
 template <typename R>
@@ -1504,7 +1510,7 @@ int copy_fields(const CopyJob<R>& job, size_t n, cudaStream_t st) {
   if (job.count > kCopyMax || (n * sizeof(R)) % 16) return 1;
   for (int f = 0; f < job.count; ++f)
     if ((reinterpret_cast<uintptr_t>(job.src[f]) | reinterpret_cast<uintptr_t>(job.dst[f])) % 16) return 1;
-  k_copy_fields<R><<<148 * 8, 256, 0, st>>>(job, n);
+  k_copy_fields<R><<<dim3((148 * 8 + job.count - 1) / job.count, job.count), 256, 0, st>>>(job, n);
   return 0;
 }
 

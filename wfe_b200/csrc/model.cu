@@ -898,7 +898,7 @@ class ModelT final : public Model {
   // shapes, 6 the TMA-staged column, 7..9 the fused substep kernel in three
   // tile shapes, 10..12 the chunked column kernel, 13..15 the persistent
   // pipelined column kernel, 16..18 the parallel-solve column kernel and
-  // 19..21 its pipelined form, both equal to the others up to rounding),
+  // 19..22 its pipelined form, both equal to the others up to rounding),
   // WFE_UV_VARIANT=<n> the forward u, v kernel (0
   // thread per face, 1 persistent pipelined tiles) and WFE_TEND_VARIANT=<n>
   // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars,
