@@ -328,10 +328,10 @@ def test_cases_of_different_depths_share_the_kernels(monkeypatch):
 @pytest.mark.parametrize("name", ["wk82_small", "schaer_open", "moist_blob"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_pipelined_parallel_solve_equals_parallel_solve(name, prec, monkeypatch):
-    """The pipelined parallel-solve column kernels (variants 19-21: tiles
-    streamed into shared memory by a producer warp) evaluate the
-    parallel-solve kernel's expressions (variant 16) on the same values: the
-    same fields, bit for bit, after five steps."""
+    """The pipelined parallel-solve column kernels with 16 level lanes
+    (variants 19-21: tiles streamed into shared memory by a producer warp)
+    evaluate the parallel-solve kernel's expressions (variant 16) on the same
+    values: the same fields, bit for bit, after five steps."""
     out = {}
     for v in ("16", "19", "20", "21"):
         monkeypatch.setenv("WFE_COLUMN_VARIANT", v)

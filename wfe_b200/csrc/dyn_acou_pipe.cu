@@ -119,6 +119,9 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
     k_acoustic_column_pipe(const __grid_constant__ PipeColParams<R> p) {
   extern __shared__ __align__(128) unsigned char smem_pipe[];
   constexpr int NC = CX * KL;  // consumer threads; the last warp produces
+  // the consumers' named barrier counts whole warps, and the producer warp
+  // holds no consumer
+  static_assert(NC % 32 == 0, "consumer threads must fill whole warps");
   const AcouArgs<R>& a = p.a;
   const Layout& L = a.L;
   const int nz = L.nz;
@@ -359,6 +362,9 @@ __global__ void __launch_bounds__(CX * KL + 32)
     k_acoustic_column_pipe_pcr(const __grid_constant__ PipeColParams<R> p) {
   extern __shared__ __align__(128) unsigned char smem_pipe[];
   constexpr int NC = CX * KL;  // consumer threads; the last warp produces
+  // the consumers' named barrier counts whole warps, and the producer warp
+  // holds no consumer
+  static_assert(NC % 32 == 0, "consumer threads must fill whole warps");
   const AcouArgs<R>& a = p.a;
   const Layout& L = a.L;
   const int nz = L.nz;

@@ -142,11 +142,17 @@ __device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, 
     mfz[c] = 0;
     return;
   }
-  const int kk = L.at1(k);
-  R fac = (R)1 - m.zeta_w[kk] / m.zt;
-  R uw = (R)0.25 * (u[L.at(i, j, k - 1)] + u[L.at(i + 1, j, k - 1)] + u[c] + u[L.at(i + 1, j, k)]);
-  R vw = (R)0.25 * (v[L.at(i, j, k - 1)] + v[L.at(i, j + 1, k - 1)] + v[c] + v[L.at(i, j + 1, k)]);
-  R cross = (uw * m.hx[L.at2(i, j)] + vw * m.hy[L.at2(i, j)]) * fac;
+  // the terrain cross flux, where the column has a slope (flat columns skip
+  // the eight velocity loads: the product with a zero slope is zero)
+  const R hx = m.hx[L.at2(i, j)], hy = m.hy[L.at2(i, j)];
+  R cross = 0;
+  if (hx != (R)0 || hy != (R)0) {
+    const int kk = L.at1(k);
+    R fac = (R)1 - m.zeta_w[kk] / m.zt;
+    R uw = (R)0.25 * (u[L.at(i, j, k - 1)] + u[L.at(i + 1, j, k - 1)] + u[c] + u[L.at(i + 1, j, k)]);
+    R vw = (R)0.25 * (v[L.at(i, j, k - 1)] + v[L.at(i, j + 1, k - 1)] + v[c] + v[L.at(i, j + 1, k)]);
+    cross = (uw * hx + vw * hy) * fac;
+  }
   mfz[c] = b.rhobw[c] * (w[c] - cross);
 }
 
