@@ -297,11 +297,11 @@ __device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int
   return v_forward(a, i, j == L.ny ? 0 : j, k);
 }
 
-// Launched as (32, 4, 2) blocks.  Each thread computes theta_v and pi* of
+// Launched as kUvBx x kUvBy x kUvBz blocks.  Each thread computes theta_v and pi* of
 // its own cell once and shares them through shared memory: an interior
 // point takes its x (y) neighbour's values from the thread beside it in the
 // block when there is one, instead of loading the neighbour's five fields.
-constexpr int kUvBx = 32, kUvBy = 4, kUvBz = 2;
+constexpr int kUvBx = 16, kUvBy = 8, kUvBz = 2;
 
 template <typename R>
 __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
@@ -1401,9 +1401,16 @@ dim3 grid_uv(const Layout& L) {
   return dim3((L.nx + 1 + 31) / 32, (L.ny + 1 + 3) / 4, (L.nz + 1) / 2);
 }
 
+// the forward u, v kernel's grid: faces 0..nx x 0..ny in kUvBx x kUvBy x
+// kUvBz blocks
+template <typename R>
+dim3 grid_uv_fwd(const Layout& L) {
+  return dim3((L.nx + 1 + kUvBx - 1) / kUvBx, (L.ny + 1 + kUvBy - 1) / kUvBy, (L.nz + kUvBz - 1) / kUvBz);
+}
+
 template <typename R>
 void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st) {
-  k_acoustic_uv<R><<<grid_uv<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
+  k_acoustic_uv<R><<<grid_uv_fwd<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
 }
 
 template <typename R>
@@ -1713,6 +1720,7 @@ int launch_acoustic_uv_pipe(const PipeUvParams<R>& p, cudaStream_t st) {
   template int prepare_acoustic_column_tma<R>(int);                                            \
   template int launch_acoustic_column_tma<R>(const TmaColParams<R>&, cudaStream_t);            \
   template dim3 grid_uv<R>(const Layout&);                                                     \
+  template dim3 grid_uv_fwd<R>(const Layout&);                                                 \
   template dim3 grid_column<R>(const Layout&, int);                                            \
   template void batch_uv<R>(const Batch<AcouArgs<R>>&, int, cudaStream_t);                     \
   template int batch_column<R>(const Batch<AcouArgs<R>>&, int, int, int, cudaStream_t);        \

@@ -194,7 +194,9 @@ void batch_clock(const Batch<ClockArgs>& b, int nblocks, cudaStream_t st);
 template <typename R>
 int occupancy_tend(int variant, int sub);
 template <typename R>
-dim3 grid_uv(const Layout& L);
+dim3 grid_uv(const Layout& L);  // faces 0..nx x 0..ny in 32 x 4 x 2 blocks (linearised u, v)
+template <typename R>
+dim3 grid_uv_fwd(const Layout& L);  // the forward u, v kernel's blocks
 template <typename R>
 dim3 grid_column(const Layout& L, int shape);
 template <typename R>
