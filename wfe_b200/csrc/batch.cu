@@ -37,7 +37,7 @@ dim3 kind_grid(int kind, int variant, int sub, const void* args, int nz_max) {
     case K_FILL: return grid_fill<R>(*static_cast<const FillArgs<R>*>(args));
     case K_FLUX: return grid_flux<R>(*static_cast<const FluxArgs<R>*>(args));
     case K_PD: return grid_pd<R>(static_cast<const PdArgs<R>*>(args)->t.L);
-    case K_TEND: return grid_cells<R>(static_cast<const TendArgs<R>*>(args)->L);
+    case K_TEND: return grid_tend<R>(static_cast<const TendArgs<R>*>(args)->L);
     case K_UV: return grid_uv_fwd<R>(static_cast<const AcouArgs<R>*>(args)->L);
     case K_COL: return grid_column<R>(static_cast<const AcouArgs<R>*>(args)->L, variant);
     case K_KES: return grid_kessler<R>(static_cast<const KesArgs<R>*>(args)->L, nz_max);

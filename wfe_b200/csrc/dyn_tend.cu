@@ -669,10 +669,18 @@ void batch_pd(const Batch<PdArgs<R>>& b, int nblocks, cudaStream_t st) {
   k_pd_ratio_batch<R><<<nblocks, dim3(32, 4, 2), 0, st>>>(b);
 }
 
+// the fused and split tendency kernels' blocks
+constexpr int kTdBx = 32, kTdBy = 4, kTdBz = 2;
+
+template <typename R>
+dim3 grid_tend(const Layout& L) {
+  return dim3((L.nx + kTdBx - 1) / kTdBx, (L.ny + kTdBy - 1) / kTdBy, (L.nz + kTdBz - 1) / kTdBz);
+}
+
 template <typename R>
 void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 grd = grid_cells<R>(a.L);
+  dim3 blk(kTdBx, kTdBy, kTdBz);
+  dim3 grd = grid_tend<R>(a.L);
   if (variant == 4) {  // two cells per thread along x
     dim3 b2(16, 4, 2);
     dim3 g2((a.L.nx + 31) / 32, (a.L.ny + 3) / 4, (a.L.nz + 1) / 2);
@@ -690,7 +698,7 @@ void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
 // variant 1 runs two subs (momentum, scalars); variant 0 one fused sub
 template <typename R>
 void batch_tend(const Batch<TendArgs<R>>& b, int variant, int sub, int nblocks, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
+  dim3 blk(kTdBx, kTdBy, kTdBz);
   if (variant == 1) {
     if (sub == 0) k_tendencies_batch<R, TEND_MOM><<<nblocks, blk, 0, st>>>(b);
     else k_tendencies_batch<R, TEND_SCAL><<<nblocks, blk, 0, st>>>(b);
@@ -722,6 +730,7 @@ int occupancy_tend(int variant, int sub) {
   template dim3 grid_fill<R>(const FillArgs<R>&);                                              \
   template dim3 grid_flux<R>(const FluxArgs<R>&);                                              \
   template dim3 grid_cells<R>(const Layout&);                                                   \
+  template dim3 grid_tend<R>(const Layout&);                                                    \
   template dim3 grid_pd<R>(const Layout&);                                                      \
   template void batch_fill<R>(const Batch<FillArgs<R>>&, int, cudaStream_t);                   \
   template void batch_flux<R>(const Batch<FluxArgs<R>>&, int, cudaStream_t);                   \

@@ -178,7 +178,9 @@ dim3 grid_fill(const FillArgs<R>& a);
 template <typename R>
 dim3 grid_flux(const FluxArgs<R>& a);
 template <typename R>
-dim3 grid_cells(const Layout& L);  // tendencies
+dim3 grid_cells(const Layout& L);  // cells in 32 x 4 x 2 blocks
+template <typename R>
+dim3 grid_tend(const Layout& L);  // the tendency kernels' blocks
 template <typename R>
 dim3 grid_pd(const Layout& L);  // positive-definite outflow ratios
 dim3 grid_clock();
