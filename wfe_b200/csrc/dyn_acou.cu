@@ -301,7 +301,7 @@ __device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int
 // its own cell once and shares them through shared memory: an interior
 // point takes its x (y) neighbour's values from the thread beside it in the
 // block when there is one, instead of loading the neighbour's five fields.
-constexpr int kUvBx = 16, kUvBy = 8, kUvBz = 2;
+constexpr int kUvBx = 16, kUvBy = 16, kUvBz = 1;
 
 template <typename R>
 __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
