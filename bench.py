@@ -46,12 +46,14 @@ loop wall times is the reference figure.
 against the forward run on the same WK82 case with the linearised Kessler
 column (positive-definite limiter and w damping off, neither linearised):
 after W spin-up steps, value = wall time of wfe_ad_run over K steps
-(checkpoints every 30 steps, the fields already on the device; the second of
-two runs, the first captures the sweep's graphs) / CUDA-event time of the same
-K forward steps.  The line also gives the tangent-linear ratio, the adjoint's
-with checkpoint_every = 0 (the longest interval the device memory holds: no
-recomputation when the whole undo log fits) and the dot-product gap
+(checkpoints every 30 steps, the fields already on the device; the median of
+three runs after one that captures the sweep's graphs) / CUDA-event time of
+the same K forward steps.  The line also gives the tangent-linear ratio, the
+adjoint's with checkpoint_every = 0 (the longest interval the device memory
+holds: no recomputation when the whole undo log fits) and the dot-product gap
 <M dx, y> - <dx, M^T y> over min(K, 10) steps.  --fp64 runs the FP64 state.
+--workload adjoint_schaer measures the same on the dry Schaer mountain-wave
+slab (400x4x65, dt = 4 s; K = 900 is its 1 h sensitivity run).
 """
 
 from __future__ import annotations
@@ -539,15 +541,28 @@ def ensemble_bench(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+# The adjoint workloads: (case, overrides, description).  WK82 runs the
+# linearised Kessler column with the two nonlinear switches off; the Schaer
+# slab is the dry mountain-wave sensitivity case (1 h = 900 steps of 4 s).
+ADJOINT_CASES = {
+    "adjoint": ("wk82_160.ini", {"pd_moist": "off", "w_damping": "off"},
+                "WK82 supercell 160x160x40, moist + linearised Kessler, dt=6 s, ns=6, "
+                "pd_moist=off, w_damping=off"),
+    "adjoint_schaer": ("schaer_400.ini", {},
+                       "Schaer mountain waves 400x4x65, dry, dx=500 m, 20 km top, dt=4 s, ns=6"),
+}
+
+
 def adjoint_bench(args, device: int) -> dict:
-    """Adjoint and tangent-linear cost over the forward on the WK82 case."""
+    """Adjoint and tangent-linear cost over the forward (WK82 or Schaer)."""
     import numpy as np
     import wfe_b200 as W
     from wfe_b200 import adjoint as A
 
     prec = "f64" if args.fp64 else "f32"
     K = args.steps
-    c = W.Case(CASE, overrides={"pd_moist": "off", "w_damping": "off"}, precision=prec, device=device)
+    ini, over, desc = ADJOINT_CASES[args.workload]
+    c = W.Case(ROOT / "cases" / ini, overrides=over, precision=prec, device=device)
     c.run(args.warmup)
     c.sync()
     x0 = A.get_fields(c)
@@ -558,8 +573,9 @@ def adjoint_bench(args, device: int) -> dict:
     fwd_ms = c.time_run(K)
     rng = np.random.default_rng(2)
     sc = {"qv": 1e-3, "qc": 1e-3, "qr": 1e-3}
-    dx = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in A.FIELDS8}
-    y = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in A.FIELDS8}
+    names = A.state_names(c)
+    dx = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in names}
+    y = {k: rng.standard_normal(c.shape) * sc.get(k, 1.0) for k in names}
     c.lin_enable()
     times = {}
     for name in ("ad", "tl", "ad_auto"):
@@ -582,16 +598,14 @@ def adjoint_bench(args, device: int) -> dict:
     m = min(K, 10)
     mdx = A.tangent(c, x0, dx, m)
     mty = A.adjoint(c, x0, y, m, every=5)
-    lhs = sum(float(np.sum(mdx[k] * y[k])) for k in A.FIELDS8)
-    rhs = sum(float(np.sum(dx[k] * mty[k])) for k in A.FIELDS8)
+    lhs = sum(float(np.sum(mdx[k] * y[k])) for k in names)
+    rhs = sum(float(np.sum(dx[k] * mty[k])) for k in names)
     c.close()
     return {
         "metric": "adjoint_cost_over_forward", "value": times["ad"] / fwd_ms, "unit": "x",
         "higher_is_better": False, "n_gpus": 1, "steps": K, "warmup": args.warmup, "dtype": prec,
-        "data": "synthetic (analytic WK82 sounding and bubble, deterministic)",
-        "config": {"workload": "WK82 supercell 160x160x40, moist + linearised Kessler, dt=6 s, ns=6, "
-                               "pd_moist=off, w_damping=off", "case": "cases/wk82_160.ini",
-                   "checkpoint_every": 30},
+        "data": "synthetic (analytic initial state, deterministic)",
+        "config": {"workload": desc, "case": f"cases/{ini}", "checkpoint_every": 30},
         "statistic": "median of three runs after one that captures the graphs",
         "fwd_ms_per_step": fwd_ms / K, "ad_ms_per_step": times["ad"] / K,
         "tl_ms_per_step": times["tl"] / K, "tl_cost_over_forward": times["tl"] / fwd_ms,
@@ -610,7 +624,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=list(WORKLOADS) + ["ensemble24", "adjoint"], default="wk82")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["ensemble24"] + list(ADJOINT_CASES), default="wk82")
     ap.add_argument("--fp64", action="store_true", help="adjoint workload: FP64 state")
     ap.add_argument("--backend", default="nccl", help="process-group backend for N > 1 ranks")
     ap.add_argument("--dry-run", action="store_true",
@@ -652,7 +666,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    if args.workload == "adjoint":
+    if args.workload in ADJOINT_CASES:
         if rank == 0:
             print(json.dumps(adjoint_bench(args, local)), flush=True)
         if world > 1:
