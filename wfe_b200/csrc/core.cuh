@@ -40,7 +40,16 @@ struct Layout {
   WFE_HD size_t n3() const { return (size_t)px * py * pz; }
   WFE_HD size_t n2() const { return (size_t)px * py; }
   WFE_HD size_t plane() const { return (size_t)px * py; }
+  // 32-bit forms: a padded field holds fewer than 2^31 points (checked when a
+  // model is created), and a pointer plus an int offset is one wide
+  // multiply-add where a 64-bit offset costs a pair of adds per address
+  WFE_HD int ati(int i, int j, int k) const { return ((k + kOZ) * py + (j + kOY)) * px + (i + kOX); }
+  WFE_HD int at2i(int i, int j) const { return (j + kOY) * px + (i + kOX); }
+  WFE_HD int planei() const { return px * py; }
 };
+
+// the largest padded field the 32-bit index forms address
+constexpr size_t kMaxIndexedPoints = (size_t)1 << 31;
 
 inline Layout make_layout(int nx, int ny, int nz) {
   Layout L;

@@ -71,13 +71,13 @@ __device__ __forceinline__ bool uv_interior(const Layout& L, int i, int j, int k
 }
 
 template <typename R>
-__device__ __forceinline__ R pistar_at(const AcouArgs<R>& a, size_t c) {
+__device__ __forceinline__ R pistar_at(const AcouArgs<R>& a, int c) {
   R cur = a.pi_cur[c];
   return cur + a.p.acoustic_smdiv * (cur - a.pi_prev[c]);
 }
 
 template <typename R>
-__device__ __forceinline__ R theta_v_at(const AcouArgs<R>& a, size_t c) {
+__device__ __forceinline__ R theta_v_at(const AcouArgs<R>& a, int c) {
   R t = a.b.thb[c] + a.th_in[c];
   if (a.p.moisture) t *= (R)1 + Phys<R>::eps61 * a.qv[c];
   return t;
@@ -89,10 +89,10 @@ template <typename R>
 __device__ __forceinline__ R uv_forward_interior(const AcouArgs<R>& a, int i, int j, int k, bool is_u) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const size_t c2 = L.at2(i, j);
+  const int c = L.ati(i, j, k);
+  const int c2 = L.at2i(i, j);
   const int d = is_u ? 1 : L.px;
-  const int pl = (int)L.plane();
+  const int pl = L.planei();
   R thb_f = (R)0.5 * (theta_v_at(a, c - d) + theta_v_at(a, c));
   R mf = (R)0.5 * (a.m.mapf[c2 - d] + a.m.mapf[c2]);
   R p0 = pistar_at(a, c), pm = pistar_at(a, c - d);
@@ -120,19 +120,19 @@ __device__ __forceinline__ R u_forward(const AcouArgs<R>& a, int i, int j, int k
   const int kk = L.at1(k);
   const R zt = a.m.zt;
   R thbu = (R)0.5 * (theta_v(a, i - 1, j, k) + theta_v(a, i, j, k));
-  R mu = (R)0.5 * (a.m.mapf[L.at2(i - 1, j)] + a.m.mapf[L.at2(i, j)]);
+  R mu = (R)0.5 * (a.m.mapf[L.at2i(i - 1, j)] + a.m.mapf[L.at2i(i, j)]);
   R grad = (pistar(a, i, j, k) - pistar(a, i - 1, j, k)) / a.dx;
-  R zxu = a.m.hx_u[L.at2(i, j)] * ((R)1 - a.m.zeta_c[kk] / zt);
+  R zxu = a.m.hx_u[L.at2i(i, j)] * ((R)1 - a.m.zeta_c[kk] / zt);
   if (zxu != (R)0) {
     R dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
-    R ju = (R)0.5 * (a.m.jac[L.at2(i - 1, j)] + a.m.jac[L.at2(i, j)]);
+    R ju = (R)0.5 * (a.m.jac[L.at2i(i - 1, j)] + a.m.jac[L.at2i(i, j)]);
     R dpdz = (R)0.5 *
              ((pistar(a, i - 1, j, k + 1) - pistar(a, i - 1, j, k - 1)) +
               (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
              dzc2;
     grad -= zxu / ju * dpdz;
   }
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   return a.u_in[c] + a.dtau * (-Phys<R>::cp * thbu * mu * grad + a.tu[c]);
 }
 
@@ -144,19 +144,19 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
   const int kk = L.at1(k);
   const R zt = a.m.zt;
   R thbv = (R)0.5 * (theta_v(a, i, j - 1, k) + theta_v(a, i, j, k));
-  R mv = (R)0.5 * (a.m.mapf[L.at2(i, j - 1)] + a.m.mapf[L.at2(i, j)]);
+  R mv = (R)0.5 * (a.m.mapf[L.at2i(i, j - 1)] + a.m.mapf[L.at2i(i, j)]);
   R grad = (pistar(a, i, j, k) - pistar(a, i, j - 1, k)) / a.dy;
-  R zyv = a.m.hy_v[L.at2(i, j)] * ((R)1 - a.m.zeta_c[kk] / zt);
+  R zyv = a.m.hy_v[L.at2i(i, j)] * ((R)1 - a.m.zeta_c[kk] / zt);
   if (zyv != (R)0) {
     R dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
-    R jv = (R)0.5 * (a.m.jac[L.at2(i, j - 1)] + a.m.jac[L.at2(i, j)]);
+    R jv = (R)0.5 * (a.m.jac[L.at2i(i, j - 1)] + a.m.jac[L.at2i(i, j)]);
     R dpdz = (R)0.5 *
              ((pistar(a, i, j - 1, k + 1) - pistar(a, i, j - 1, k - 1)) +
               (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
              dzc2;
     grad -= zyv / jv * dpdz;
   }
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   return a.v_in[c] + a.dtau * (-Phys<R>::cp * thbv * mv * grad + a.tv[c]);
 }
 
@@ -165,7 +165,7 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
 // the terrain term needs, p = {pi*(west/south, k+1), pi*(west/south, k-1),
 // pi*(k+1), pi*(k-1)}, from global or from shared memory.
 template <typename R, typename PZ>
-__device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, size_t c2, int kk, R tv0, R tvx, R ps0,
+__device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, int c2, int kk, R tv0, R tvx, R ps0,
                                              R psx, R uin, R tin, PZ pz) {
   R thb_f = (R)0.5 * (tvx + tv0);
   R mf = (R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]);
@@ -182,9 +182,9 @@ __device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, size_t c2, in
 }
 
 template <typename R, typename PZ>
-__device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, size_t c2, int kk, R tv0, R tvy, R ps0,
+__device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, int c2, int kk, R tv0, R tvy, R ps0,
                                              R psy, R vin, R tin, PZ pz) {
-  const size_t sy = a.L.px;
+  const int sy = a.L.px;
   R thb_f = (R)0.5 * (tvy + tv0);
   R mf = (R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]);
   R grad = (ps0 - psy) * a.co.inv_dy;
@@ -200,9 +200,9 @@ __device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, size_t c2, in
 }
 
 template <typename R>
-__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
+__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvx,
                                              R ps0, R psx, R uin, R tin) {
-  const size_t pl = a.L.plane();
+  const int pl = a.L.planei();
   return u_interior_core(a, c2, kk, tv0, tvx, ps0, psx, uin, tin, [&](R* q) {
     q[0] = pistar_at(a, c - 1 + pl);
     q[1] = pistar_at(a, c - 1 - pl);
@@ -212,15 +212,15 @@ __device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, size_t c, siz
 }
 
 template <typename R>
-__device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvx,
+__device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvx,
                                             R ps0, R psx) {
   return u_interior_from(a, c, c2, kk, tv0, tvx, ps0, psx, a.u_in[c], a.tu[c]);
 }
 
 template <typename R>
-__device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
+__device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvy,
                                              R ps0, R psy, R vin, R tin) {
-  const size_t sy = a.L.px, pl = a.L.plane();
+  const int sy = a.L.px, pl = a.L.planei();
   return v_interior_core(a, c2, kk, tv0, tvy, ps0, psy, vin, tin, [&](R* q) {
     q[0] = pistar_at(a, c - sy + pl);
     q[1] = pistar_at(a, c - sy - pl);
@@ -230,7 +230,7 @@ __device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, size_t c, siz
 }
 
 template <typename R>
-__device__ __forceinline__ R v_interior_val(const AcouArgs<R>& a, size_t c, size_t c2, int kk, R tv0, R tvy,
+__device__ __forceinline__ R v_interior_val(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvy,
                                             R ps0, R psy) {
   return v_interior_from(a, c, c2, kk, tv0, tvy, ps0, psy, a.v_in[c], a.tv[c]);
 }
@@ -241,8 +241,8 @@ template <typename R>
 __device__ __forceinline__ void uv_pair_interior(const AcouArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k), c2 = L.at2(i, j);
-  const size_t sy = L.px;
+  const int c = L.ati(i, j, k), c2 = L.at2i(i, j);
+  const int sy = L.px;
   const R tv0 = theta_v_at(a, c), tvx = theta_v_at(a, c - 1), tvy = theta_v_at(a, c - sy);
   const R ps0 = pistar_at(a, c), psx = pistar_at(a, c - 1), psy = pistar_at(a, c - sy);
   a.u_out[c] = u_interior_val(a, c, c2, kk, tv0, tvx, ps0, psx);
@@ -258,13 +258,13 @@ __device__ __forceinline__ R u_face_edge(const AcouArgs<R>& a, int i, int j, int
   const R cstar = a.p.cstar;
   if (a.p.bc_x_open) {
     if (i == 0) {  // kernels.cu:654-660
-      R u0 = a.u_in[L.at(0, j, k)];
+      R u0 = a.u_in[L.ati(0, j, k)];
       if (u0 >= (R)0) return a.b.ub[kk];
       R cb = u0 - cstar;
       return u0 - a.dtau * cb * (u_forward(a, 1, j, k) - u0) / a.dx;
     }
     if (i == L.nx) {  // kernels.cu:661-667
-      R un = a.u_in[L.at(L.nx, j, k)];
+      R un = a.u_in[L.ati(L.nx, j, k)];
       if (un <= (R)0) return a.b.ub[kk];
       R cb = un + cstar;
       return un - a.dtau * cb * (un - u_forward(a, L.nx - 1, j, k)) / a.dx;
@@ -281,13 +281,13 @@ __device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int
   const R cstar = a.p.cstar;
   if (a.p.bc_y_open) {
     if (j == 0) {  // kernels.cu:674-680
-      R v0 = a.v_in[L.at(i, 0, k)];
+      R v0 = a.v_in[L.ati(i, 0, k)];
       if (v0 >= (R)0) return 0;
       R cb = v0 - cstar;
       return v0 - a.dtau * cb * (v_forward(a, i, 1, k) - v0) / a.dy;
     }
     if (j == L.ny) {  // kernels.cu:681-687
-      R vn = a.v_in[L.at(i, L.ny, k)];
+      R vn = a.v_in[L.ati(i, L.ny, k)];
       if (vn <= (R)0) return 0;
       R cb = vn + cstar;
       return vn - a.dtau * cb * (vn - v_forward(a, i, L.ny - 1, k)) / a.dy;
@@ -312,8 +312,8 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   const int j = by * kUvBy + ty;
   const int k = bz * kUvBz + tz;
   const bool has_cell = i < L.nx && j < L.ny && k < L.nz;
-  const size_t c = has_cell ? L.at(i, j, k) : 0;
-  const size_t sy = L.px;
+  const int c = has_cell ? L.ati(i, j, k) : 0;
+  const int sy = L.px;
   // an interior point's own inputs, and its x (y) neighbour's values when the
   // neighbour is not in the block, are loaded before the barrier so that
   // their latency overlaps the shared values' (the same values either way)
@@ -352,13 +352,13 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
       psy = s_ps[tz][ty - 1][tx];
     }
     const int kk = L.at1(k);
-    const size_t c2 = L.at2(i, j);
+    const int c2 = L.at2i(i, j);
     a.u_out[c] = u_interior_from(a, c, c2, kk, tv0, tvx, ps0, psx, uin, tun);
     a.v_out[c] = v_interior_from(a, c, c2, kk, tv0, tvy, ps0, psy, vin, tvn);
     return;
   }
-  if (j < L.ny) a.u_out[L.at(i, j, k)] = u_face_edge(a, i, j, k);
-  if (i < L.nx) a.v_out[L.at(i, j, k)] = v_face_edge(a, i, j, k);
+  if (j < L.ny) a.u_out[L.ati(i, j, k)] = u_face_edge(a, i, j, k);
+  if (i < L.nx) a.v_out[L.ati(i, j, k)] = v_face_edge(a, i, j, k);
 }
 
 // One face with uv_body's arithmetic (the fused substep kernel computes a
@@ -367,8 +367,8 @@ template <typename R>
 __device__ __forceinline__ R u_face(const AcouArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   if (uv_interior<R>(L, i, j, k)) {
-    const size_t c = L.at(i, j, k);
-    return u_interior_val(a, c, L.at2(i, j), L.at1(k), theta_v_at(a, c), theta_v_at(a, c - 1),
+    const int c = L.ati(i, j, k);
+    return u_interior_val(a, c, L.at2i(i, j), L.at1(k), theta_v_at(a, c), theta_v_at(a, c - 1),
                           pistar_at(a, c), pistar_at(a, c - 1));
   }
   return u_face_edge(a, i, j, k);
@@ -378,8 +378,8 @@ template <typename R>
 __device__ __forceinline__ R v_face(const AcouArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   if (uv_interior<R>(L, i, j, k)) {
-    const size_t c = L.at(i, j, k), sy = L.px;
-    return v_interior_val(a, c, L.at2(i, j), L.at1(k), theta_v_at(a, c), theta_v_at(a, c - sy),
+    const int c = L.ati(i, j, k), sy = L.px;
+    return v_interior_val(a, c, L.at2i(i, j), L.at1(k), theta_v_at(a, c), theta_v_at(a, c - sy),
                           pistar_at(a, c), pistar_at(a, c - sy));
   }
   return v_face_edge(a, i, j, k);

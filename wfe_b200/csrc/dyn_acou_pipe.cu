@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t pl = L.plane();
+  const int pl = L.planei();
   const int ch = (nz + KL) / KL;
   const int klo = lane * ch;
   int n = 0;
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
 #define SQ(X, k) X[(size_t)(k) * CX + tx]
     const int i = (t % ntx) * CX + tx, j = t / ntx;
     const bool active = i < L.nx;
-    const size_t c2d = L.at2(active ? i : 0, j);
+    const int c2d = L.at2i(active ? i : 0, j);
     const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
     const R invJ = (R)1 / J;
     const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
@@ -321,12 +321,12 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
     tma::named_sync(1, NC);
     // phase 5 on the chunk's levels
     if (active) {
-      const size_t c0 = L.at(i, j, 0);
+      const int c0 = L.ati(i, j, 0);
 #pragma unroll
       for (int q = 1; q < KCH + 1; ++q) {
         const int k = klo - 1 + q;
         if (q > ch || k > nz) continue;
-        const size_t c = c0 + (size_t)k * pl;
+        const int c = c0 + k * pl;
         if (k < nz) {
           R wn = SQ(sD, k), wn1 = SQ(sD, k + 1);
           a.pi_next[c] = P[q] - E[q] * (av[q + 1] * wn1 - av[q] * wn);
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t pl = L.plane();
+  const int pl = L.planei();
   const int klo = lane * KCH;
   auto csync = [] { tma::named_sync(1, NC); };
   csync();
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
     // the column's metric, loaded while the tile's boxes may still be landing
     const int i = (t % ntx) * CX + tx, j = t / ntx;
     const bool active = i < L.nx;
-    const size_t c2d = L.at2(active ? i : 0, j);
+    const int c2d = L.at2i(active ? i : 0, j);
     const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
     const bool ok = tma::mbar_wait_for(&full[s], use & 1, kPipeWaitNs);
     if (tma::named_or(1, NC, !ok)) {
@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
     pcr_solve<R, CX, KL, KCH>(Ar, Br, Cr, Dr, work, tx, lane, csync, sol);
     // phase 5: pi', theta', w of the lane's levels
     if (active) {
-      const size_t c0 = L.at(i, j, 0);
+      const int c0 = L.ati(i, j, 0);
       R wl[KCH + 2];  // w at the lane's levels and the level above them
 #pragma unroll
       for (int q = 1; q < KCH; ++q) wl[q] = sol.Gx[q] + sol.Ax[q] * sol.yprev + sol.Bx[q] * sol.y;
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
       for (int q = 1; q < KCH + 1; ++q) {
         const int k = klo - 1 + q;
         if (k > nz) continue;
-        const size_t c = c0 + (size_t)k * pl;
+        const int c = c0 + k * pl;
         if (k == nz) {
           a.w_out[c] = 0;
           continue;

@@ -7,8 +7,9 @@
 // value q_n + dt_m * tq directly instead of storing tq.
 //
 // The arithmetic of every output value follows the reference expression by
-// expression (src/dynamics/kernels.cu:42-443, 292-304, 268-273) so that the
-// FP64 build agrees with the reference FP64 build to rounding.
+// expression (src/dynamics/kernels.cu:42-443, 292-304, 268-273), the face5
+// stencil in its expanded one-sided form (dyn_common.cuh), so that the FP64
+// build agrees with the reference FP64 build to rounding.
 #include <cuda_runtime.h>
 
 #include "core.cuh"
@@ -130,11 +131,11 @@ __device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, 
   const int j = (int)(by * blockDim.y + threadIdx.y) - 2;
   const int k = (int)(bz * blockDim.z + threadIdx.z);
   if (i > L.nx + 2 || j > L.ny + 2 || k > L.nz) return;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   if (k < L.nz) {
-    R rjx = (R)0.5 * (b.rhob[L.at(i - 1, j, k)] * m.jac[L.at2(i - 1, j)] + b.rhob[c] * m.jac[L.at2(i, j)]);
+    R rjx = (R)0.5 * (b.rhob[L.ati(i - 1, j, k)] * m.jac[L.at2i(i - 1, j)] + b.rhob[c] * m.jac[L.at2i(i, j)]);
     mfx[c] = rjx * u[c];
-    R rjy = (R)0.5 * (b.rhob[L.at(i, j - 1, k)] * m.jac[L.at2(i, j - 1)] + b.rhob[c] * m.jac[L.at2(i, j)]);
+    R rjy = (R)0.5 * (b.rhob[L.ati(i, j - 1, k)] * m.jac[L.at2i(i, j - 1)] + b.rhob[c] * m.jac[L.at2i(i, j)]);
     mfy[c] = rjy * v[c];
   }
   if (i > L.nx + 1 || j > L.ny + 1) return;
@@ -144,13 +145,13 @@ __device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, 
   }
   // the terrain cross flux, where the column has a slope (flat columns skip
   // the eight velocity loads: the product with a zero slope is zero)
-  const R hx = m.hx[L.at2(i, j)], hy = m.hy[L.at2(i, j)];
+  const R hx = m.hx[L.at2i(i, j)], hy = m.hy[L.at2i(i, j)];
   R cross = 0;
   if (hx != (R)0 || hy != (R)0) {
     const int kk = L.at1(k);
     R fac = (R)1 - m.zeta_w[kk] / m.zt;
-    R uw = (R)0.25 * (u[L.at(i, j, k - 1)] + u[L.at(i + 1, j, k - 1)] + u[c] + u[L.at(i + 1, j, k)]);
-    R vw = (R)0.25 * (v[L.at(i, j, k - 1)] + v[L.at(i, j + 1, k - 1)] + v[c] + v[L.at(i, j + 1, k)]);
+    R uw = (R)0.25 * (u[L.ati(i, j, k - 1)] + u[L.ati(i + 1, j, k - 1)] + u[c] + u[L.ati(i + 1, j, k)]);
+    R vw = (R)0.25 * (v[L.ati(i, j, k - 1)] + v[L.ati(i, j + 1, k - 1)] + v[c] + v[L.ati(i, j + 1, k)]);
     cross = (uw * hx + vw * hy) * fac;
   }
   mfz[c] = b.rhobw[c] * (w[c] - cross);
@@ -170,9 +171,9 @@ __global__ void k_mass_flux_batch(Batch<FluxArgs<R>> b) {
 template <typename R>
 __device__ __forceinline__ R divergence(const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   return (a.mfx[c + 1] - a.mfx[c]) * a.co.inv_dx + (a.mfy[c + L.px] - a.mfy[c]) * a.co.inv_dy +
-         (a.mfz[c + L.plane()] - a.mfz[c]) * a.co.inv_dzc[L.at1(k)];
+         (a.mfz[c + L.planei()] - a.mfz[c]) * a.co.inv_dzc[L.at1(k)];
 }
 
 // ------------------------------------------------------------ face fluxes
@@ -186,7 +187,7 @@ __device__ __forceinline__ R divergence(const TendArgs<R>& a, int i, int j, int 
 // faces M[o + m0], M[o] beside it, the point's field Q on o - 3s .. o + 2s
 // (kernels.cu:308-425).
 template <typename R>
-__device__ __forceinline__ R face_mom(const R* M, long m0, const R* Q, long s, long o = 0) {
+__device__ __forceinline__ R face_mom(const R* M, int m0, const R* Q, int s, int o = 0) {
   const R f = (R)0.5 * (M[o + m0] + M[o]);
   return mul_rn(f, face5(Q[o - 3 * s], Q[o - 2 * s], Q[o - s], Q[o], Q[o + s], Q[o + 2 * s], f));
 }
@@ -194,7 +195,7 @@ __device__ __forceinline__ R face_mom(const R* M, long m0, const R* Q, long s, l
 // The lower face of a cell-centred scalar: the face's mass flux M[0]
 // (kernels.cu:114-179, 187-218).
 template <typename R>
-__device__ __forceinline__ R face_sc(const R* M, const R* Q, long s) {
+__device__ __forceinline__ R face_sc(const R* M, const R* Q, int s) {
   const R f = M[0];
   return mul_rn(f, face5(Q[-3 * s], Q[-2 * s], Q[-s], Q[0], Q[s], Q[2 * s], f));
 }
@@ -202,10 +203,10 @@ __device__ __forceinline__ R face_sc(const R* M, const R* Q, long s) {
 // Flux-form tendency of a scalar cell (value q0, level index kk) from the
 // face-flux differences east - west, north - south, top - bottom.
 template <typename R>
-__device__ __forceinline__ R scalar_tend(const TendArgs<R>& a, R q0, size_t c, int i, int j, int kk, R dX,
+__device__ __forceinline__ R scalar_tend(const TendArgs<R>& a, R q0, int c, int i, int j, int kk, R dX,
                                          R dY, R dZ, R div) {
   R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzc[kk];
-  R rt = a.b.rhob[c] * a.m.jac[a.L.at2(i, j)];
+  R rt = a.b.rhob[c] * a.m.jac[a.L.at2i(i, j)];
   return (-fdiv + q0 * div) / rt;
 }
 
@@ -213,18 +214,18 @@ __device__ __forceinline__ R scalar_tend(const TendArgs<R>& a, R q0, size_t c, i
 // (kernels.cu:187-218): F on the left/lower face of cell (i,j,k).
 template <typename R>
 __device__ __forceinline__ R qflux_x(const TendArgs<R>& a, const R* q, int i, int j, int k) {
-  const size_t c = a.L.at(i, j, k);
+  const int c = a.L.ati(i, j, k);
   return face_sc(a.mfx + c, q + c, 1);
 }
 template <typename R>
 __device__ __forceinline__ R qflux_y(const TendArgs<R>& a, const R* q, int i, int j, int k) {
-  const size_t c = a.L.at(i, j, k);
-  return face_sc(a.mfy + c, q + c, (long)a.L.px);
+  const int c = a.L.ati(i, j, k);
+  return face_sc(a.mfy + c, q + c, a.L.px);
 }
 template <typename R>
 __device__ __forceinline__ R qflux_z(const TendArgs<R>& a, const R* q, int i, int j, int k) {
-  const size_t c = a.L.at(i, j, k);
-  return face_sc(a.mfz + c, q + c, (long)a.L.plane());
+  const int c = a.L.ati(i, j, k);
+  return face_sc(a.mfz + c, q + c, a.L.planei());
 }
 
 // Outflow ratio min(1, available / outgoing) per species (kernels.cu:221-238),
@@ -240,9 +241,9 @@ __device__ __forceinline__ void pd_body(const PdArgs<R>& P, int bx, int by, int 
   const int j = by * blockDim.y + threadIdx.y;
   const int k = bz * blockDim.z + threadIdx.z;
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const R idz = a.co.inv_dzc[L.at1(k)];
-  const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
+  const R rt = a.b.rhob[c] * a.m.jac[L.at2i(i, j)];
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
     const R* q = s == 0 ? a.qv : (s == 1 ? a.qc : a.qr);
@@ -274,7 +275,7 @@ __device__ __forceinline__ R ratio_at(const TendArgs<R>& a, const R* ratio, int 
   int si = map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open);
   int sj = map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open);
   int sk = map_zc(k, L.nz);
-  return ratio[L.at(si, sj, sk)];
+  return ratio[L.ati(si, sj, sk)];
 }
 
 // Limited face fluxes of the renormalised positive-definite advection
@@ -283,23 +284,23 @@ __device__ __forceinline__ R ratio_at(const TendArgs<R>& a, const R* ratio, int 
 // is interior, through ratio_at's ghost map otherwise).
 template <typename R>
 __device__ __forceinline__ R pd_face_x(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j, int k) {
-  const size_t c = a.L.at(i, j, k);
+  const int c = a.L.ati(i, j, k);
   const R F = face_sc(a.mfx + c, q + c, 1);
   const int u = F >= (R)0 ? i - 1 : i;
   return mul_rn(F, (u >= 0 && u < a.L.nx) ? ratio[c + (u - i)] : ratio_at(a, ratio, u, j, k));
 }
 template <typename R>
 __device__ __forceinline__ R pd_face_y(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j, int k) {
-  const size_t c = a.L.at(i, j, k);
-  const long sy = a.L.px;
+  const int c = a.L.ati(i, j, k);
+  const int sy = a.L.px;
   const R F = face_sc(a.mfy + c, q + c, sy);
   const int u = F >= (R)0 ? j - 1 : j;
   return mul_rn(F, (u >= 0 && u < a.L.ny) ? ratio[c + (u - j) * sy] : ratio_at(a, ratio, i, u, k));
 }
 template <typename R>
 __device__ __forceinline__ R pd_face_z(const TendArgs<R>& a, const R* q, const R* ratio, int i, int j, int k) {
-  const size_t c = a.L.at(i, j, k);
-  const long sz = (long)a.L.plane();
+  const int c = a.L.ati(i, j, k);
+  const int sz = a.L.planei();
   const R F = face_sc(a.mfz + c, q + c, sz);
   const int u = F >= (R)0 ? k - 1 : k;
   return mul_rn(F, (u >= 0 && u < a.L.nz) ? ratio[c + (u - k) * sz] : ratio_at(a, ratio, i, j, u));
@@ -311,12 +312,12 @@ __device__ __forceinline__ R laplacian(const TendArgs<R>& a, const R* f, int i, 
                                        bool on_w) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  R dzl = (on_w ? a.m.dzeta_w[kk] : a.m.dzeta_c[kk]) * a.m.jac[L.at2(i, j)];
-  const size_t c = L.at(i, j, k);
+  R dzl = (on_w ? a.m.dzeta_w[kk] : a.m.dzeta_c[kk]) * a.m.jac[L.at2i(i, j)];
+  const int c = L.ati(i, j, k);
   R cc = f[c];
   return (f[c + 1] - 2 * cc + f[c - 1]) / (a.dx * a.dx) +
          (f[c + L.px] - 2 * cc + f[c - L.px]) / (a.dy * a.dy) +
-         (f[c + L.plane()] - 2 * cc + f[c - L.plane()]) / (dzl * dzl);
+         (f[c + L.planei()] - 2 * cc + f[c - L.planei()]) / (dzl * dzl);
 }
 
 
@@ -325,7 +326,7 @@ __device__ __forceinline__ R laplacian(const TendArgs<R>& a, const R* f, int i, 
 // option).
 template <typename R>
 __device__ __forceinline__ R moist_out(const TendArgs<R>& a, const R* q, const R* qn, const R* qo, bool davies_qv,
-                                       int i, int j, int k, size_t c, R dX, R dY, R dZ, R div0) {
+                                       int i, int j, int k, int c, R dX, R dY, R dZ, R div0) {
   R t = scalar_tend(a, q[c], c, i, j, a.L.at1(k), dX, dY, dZ, div0);
   if (davies_qv) t += davies(a, 4, q, i, j, k);
   return qo ? qn[c] + a.dt_stage * t : t;
@@ -335,13 +336,13 @@ __device__ __forceinline__ R moist_out(const TendArgs<R>& a, const R* q, const R
 // per cell.
 template <typename R>
 __device__ __forceinline__ R species_cell(const TendArgs<R>& a, const R* q, const R* ratio, const R* qn,
-                                          const R* qo, bool davies_qv, int i, int j, int k, size_t c, R div0) {
+                                          const R* qo, bool davies_qv, int i, int j, int k, int c, R div0) {
   if (a.p.pd_moist && ratio)
     return moist_out(a, q, qn, qo, davies_qv, i, j, k, c,
                      pd_face_x(a, q, ratio, i + 1, j, k) - pd_face_x(a, q, ratio, i, j, k),
                      pd_face_y(a, q, ratio, i, j + 1, k) - pd_face_y(a, q, ratio, i, j, k),
                      pd_face_z(a, q, ratio, i, j, k + 1) - pd_face_z(a, q, ratio, i, j, k), div0);
-  const long sx = 1, sy = a.L.px, sz = (long)a.L.plane();
+  const int sx = 1, sy = a.L.px, sz = a.L.planei();
   const R* MX = a.mfx + c;
   const R* MY = a.mfy + c;
   const R* MZ = a.mfz + c;
@@ -360,15 +361,15 @@ __device__ __forceinline__ R u_out(const TendArgs<R>& a, int i, int j, int k, R 
                                    R div0, bool bdy) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px;
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px;
   const R* U = a.u + c;
   const R* V = a.v + c;
   R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzc[kk];
   R dv = (R)0.5 * (div_w() + div0);
-  R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+  R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2i(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2i(i, j)]);
   R vavg = (R)0.25 * (V[-sx] + V[sy - sx] + V[0] + V[sy]);
-  R fc = (R)0.5 * (a.m.fcor[L.at2(i - 1, j)] + a.m.fcor[L.at2(i, j)]);
+  R fc = (R)0.5 * (a.m.fcor[L.at2i(i - 1, j)] + a.m.fcor[L.at2i(i, j)]);
   R relax = -a.co.spg_c[kk] * (U[0] - a.b.ub[kk]);
   R t = (-fdiv + U[0] * dv) / ru + fc * vavg + relax;
   if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.u, i, j, k, false);
@@ -382,15 +383,15 @@ __device__ __forceinline__ R v_out(const TendArgs<R>& a, int i, int j, int k, R 
                                    R div0, bool bdy) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px;
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px;
   const R* U = a.u + c;
   const R* V = a.v + c;
   R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzc[kk];
   R dv = (R)0.5 * (div_s() + div0);
-  R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+  R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2i(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2i(i, j)]);
   R uavg = (R)0.25 * (U[-sy] + U[sx - sy] + U[0] + U[sx]);
-  R fc = (R)0.5 * (a.m.fcor[L.at2(i, j - 1)] + a.m.fcor[L.at2(i, j)]);
+  R fc = (R)0.5 * (a.m.fcor[L.at2i(i, j - 1)] + a.m.fcor[L.at2i(i, j)]);
   R uref = a.p.coriolis_use_ub ? a.b.ub[kk] : (R)0;
   R relax = -a.co.spg_c[kk] * V[0];
   R t = (-fdiv + V[0] * dv) / rv - fc * (uavg - uref) + relax;
@@ -406,15 +407,15 @@ __device__ __forceinline__ R w_out(const TendArgs<R>& a, int i, int j, int k, R 
                                    R div0) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const R* W = a.w + c;
   R fdiv = dX * a.co.inv_dx + dY * a.co.inv_dy + dZ * a.co.inv_dzw[kk];
   R dv = (R)0.5 * (div_b() + div0);
-  R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
+  R rw = a.b.rhobw[c] * a.m.jac[L.at2i(i, j)];
   R relax = -a.co.spg_w[kk] * W[0];
   R wk = W[0];
   if (a.p.w_damping) {
-    R cr = fabs(wk) * a.dt / (a.m.dzeta_w[kk] * a.m.jac[L.at2(i, j)]);
+    R cr = fabs(wk) * a.dt / (a.m.dzeta_w[kk] * a.m.jac[L.at2i(i, j)]);
     if (cr > (R)1) relax -= (R)0.3 * (cr - (R)1) * wk / a.dt;
   }
   R t = (-fdiv + wk * dv) / rw + relax;
@@ -428,7 +429,7 @@ __device__ __forceinline__ R th_out(const TendArgs<R>& a, int i, int j, int k, R
                                     bool bdy) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   R t = scalar_tend(a, a.thp[c], c, i, j, kk, dX, dY, dZ, div0) - a.co.spg_c[kk] * a.thp[c];
   if (a.p.diff_K > (R)0) t += a.p.diff_K * laplacian(a, a.thp, i, j, k, false);
   if (bdy) t += davies(a, 2, a.thp, i, j, k);
@@ -451,8 +452,8 @@ enum { TEND_MOM = 1, TEND_SCAL = 2, TEND_ALL = 3 };
 template <typename R, int PART>
 __device__ __forceinline__ void tend_cell(const TendArgs<R>& a, int i, int j, int k, TendOut<R>& o) {
   const Layout& L = a.L;
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px, sz = (long)L.plane();
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px, sz = L.planei();
   const bool bdy = a.lo[0] != nullptr;
   const R* MX = a.mfx + c;
   const R* MY = a.mfy + c;
@@ -500,7 +501,7 @@ __device__ __forceinline__ void tend_cell(const TendArgs<R>& a, int i, int j, in
 
 template <typename R, int PART>
 __device__ __forceinline__ void tend_store(const TendArgs<R>& a, int i, int j, int k, const TendOut<R>& o) {
-  const size_t c = a.L.at(i, j, k);
+  const int c = a.L.ati(i, j, k);
   if (PART & TEND_MOM) {
     a.tu[c] = o.tu;
     a.tv[c] = o.tv;
@@ -554,6 +555,12 @@ __device__ __forceinline__ void tend_body2(const TendArgs<R>& a, int bx, int by,
 template <typename R, int PART>
 __global__ void __launch_bounds__(256) k_tendencies(TendArgs<R> a) {
   tend_body<R, PART>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+// the fused FP32 kernel held to 64 registers (4 blocks per SM): its
+// unconstrained allocation takes 80 and runs 3
+template <typename R>
+__global__ void __launch_bounds__(256, 4) k_tendencies_occ4(TendArgs<R> a) {
+  tend_body<R, TEND_ALL>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R, int PART>
 __global__ void __launch_bounds__(128) k_tendencies2(TendArgs<R> a) {
@@ -690,6 +697,8 @@ void launch_tendencies(const TendArgs<R>& a, int variant, cudaStream_t st) {
   } else if (variant == 1) {
     k_tendencies<R, TEND_MOM><<<grd, blk, 0, st>>>(a);
     k_tendencies<R, TEND_SCAL><<<grd, blk, 0, st>>>(a);
+  } else if constexpr (sizeof(R) == 4) {
+    k_tendencies_occ4<R><<<grd, blk, 0, st>>>(a);
   } else {
     k_tendencies<R, TEND_ALL><<<grd, blk, 0, st>>>(a);
   }

@@ -51,14 +51,14 @@ template <typename R, int N>
 struct TLAcc {  // gathers the row against the tangent inputs
   const Ptrs<R, N>& d;
   R sum;
-  __device__ __forceinline__ void operator()(int id, size_t idx, R coef) { sum += coef * d.p[id][idx]; }
+  __device__ __forceinline__ void operator()(int id, int idx, R coef) { sum += coef * d.p[id][idx]; }
 };
 
 template <typename R, int N>
 struct ADAcc {  // scatters the row, times the output adjoint, into the input adjoints
   const Ptrs<R, N>& b;
   R ybar;
-  __device__ __forceinline__ void operator()(int id, size_t idx, R coef) {
+  __device__ __forceinline__ void operator()(int id, int idx, R coef) {
     atomicAdd(b.p[id] + idx, coef * ybar);
   }
 };
@@ -74,7 +74,7 @@ __device__ __forceinline__ void face5_weights(R vel, R w[6]) {
   }
 }
 
-__device__ __forceinline__ size_t off(size_t c, long d) { return (size_t)((long)c + d); }
+__device__ __forceinline__ int off(int c, int d) { return c + d; }
 
 // ================================================================ tendencies
 enum { T_U = 0, T_V, T_W, T_TH, T_MFX, T_MFY, T_MFZ, T_QV, T_QC, T_QR, T_N };
@@ -84,15 +84,15 @@ enum { T_U = 0, T_V, T_W, T_TH, T_MFX, T_MFY, T_MFZ, T_QV, T_QC, T_QR, T_N };
 // into one weight per point: seven q terms instead of up to twelve.  Left
 // face mass flux: 0.5 (MF[maL] + MF[mbL]) (avg) or MF[maL]; right likewise.
 template <typename R, class Acc>
-__device__ __forceinline__ void emit_face_pair(Acc& acc, R cL, R cR, const R* MF, int mfid, size_t maL,
-                                               size_t mbL, size_t maR, size_t mbR, bool avg, const R* Q,
-                                               int qid, size_t c, long s) {
+__device__ __forceinline__ void emit_face_pair(Acc& acc, R cL, R cR, const R* MF, int mfid, int maL,
+                                               int mbL, int maR, int mbR, bool avg, const R* Q,
+                                               int qid, int c, int s) {
   const R fvL = avg ? (R)0.5 * (MF[maL] + MF[mbL]) : MF[maL];
   const R fvR = avg ? (R)0.5 * (MF[maR] + MF[mbR]) : MF[maR];
   const R* Qc = Q + c;
   R q[7];
 #pragma unroll
-  for (int n = 0; n < 7; ++n) q[n] = Qc[(long)(n - 3) * s];
+  for (int n = 0; n < 7; ++n) q[n] = Qc[(int)(n - 3) * s];
   const R faceL = face5(q[0], q[1], q[2], q[3], q[4], q[5], fvL);
   const R faceR = face5(q[1], q[2], q[3], q[4], q[5], q[6], fvR);
   if (avg) {
@@ -113,7 +113,7 @@ __device__ __forceinline__ void emit_face_pair(Acc& acc, R cL, R cR, const R* MF
     R wgt = 0;
     if (n < 6) wgt += gL * wL[n];
     if (n >= 1) wgt += gR * wR[n - 1];
-    if (wgt != (R)0) acc(qid, off(c, (long)(n - 3) * s), wgt);
+    if (wgt != (R)0) acc(qid, off(c, (int)(n - 3) * s), wgt);
   }
 }
 
@@ -121,13 +121,13 @@ __device__ __forceinline__ void emit_face_pair(Acc& acc, R cL, R cR, const R* MF
 template <typename R, class Acc>
 __device__ __forceinline__ void emit_div(Acc& acc, const TendArgs<R>& a, int i, int j, int k, R coef) {
   const Layout& L = a.L;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const R dzc = a.m.dzeta_c[L.at1(k)];
   acc(T_MFX, c + 1, coef / a.dx);
   acc(T_MFX, c, -coef / a.dx);
   acc(T_MFY, c + L.px, coef / a.dy);
   acc(T_MFY, c, -coef / a.dy);
-  acc(T_MFZ, c + L.plane(), coef / dzc);
+  acc(T_MFZ, c + L.planei(), coef / dzc);
   acc(T_MFZ, c, -coef / dzc);
 }
 
@@ -137,24 +137,24 @@ __device__ __forceinline__ void emit_lap(Acc& acc, const TendArgs<R>& a, int id,
                                          bool on_w, R coef) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const R dzl = (on_w ? a.m.dzeta_w[kk] : a.m.dzeta_c[kk]) * a.m.jac[L.at2(i, j)];
-  const size_t c = L.at(i, j, k);
+  const R dzl = (on_w ? a.m.dzeta_w[kk] : a.m.dzeta_c[kk]) * a.m.jac[L.at2i(i, j)];
+  const int c = L.ati(i, j, k);
   const R ax = coef / (a.dx * a.dx), ay = coef / (a.dy * a.dy), az = coef / (dzl * dzl);
   acc(id, c + 1, ax);
   acc(id, c - 1, ax);
   acc(id, c + L.px, ay);
   acc(id, c - L.px, ay);
-  acc(id, c + L.plane(), az);
-  acc(id, c - L.plane(), az);
+  acc(id, c + L.planei(), az);
+  acc(id, c - L.planei(), az);
   acc(id, c, -2 * (ax + ay + az));
 }
 
 template <typename R>
 __device__ __forceinline__ R div_value(const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
-  return (a.mfx[L.at(i + 1, j, k)] - a.mfx[L.at(i, j, k)]) / a.dx +
-         (a.mfy[L.at(i, j + 1, k)] - a.mfy[L.at(i, j, k)]) / a.dy +
-         (a.mfz[L.at(i, j, k + 1)] - a.mfz[L.at(i, j, k)]) / a.m.dzeta_c[L.at1(k)];
+  return (a.mfx[L.ati(i + 1, j, k)] - a.mfx[L.ati(i, j, k)]) / a.dx +
+         (a.mfy[L.ati(i, j + 1, k)] - a.mfy[L.ati(i, j, k)]) / a.dy +
+         (a.mfz[L.ati(i, j, k + 1)] - a.mfz[L.ati(i, j, k)]) / a.m.dzeta_c[L.at1(k)];
 }
 
 // u tendency row (forward: kernels.cu:308-346)
@@ -162,9 +162,9 @@ template <typename R, class Acc>
 __device__ void row_tu(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px, sz = (long)L.plane();
-  const R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px, sz = (int)L.planei();
+  const R ru = (R)0.5 * (a.b.rhob[c - sx] * a.m.jac[L.at2i(i - 1, j)] + a.b.rhob[c] * a.m.jac[L.at2i(i, j)]);
   const R dzc = a.m.dzeta_c[kk];
   emit_face_pair(acc, (R)1 / (a.dx * ru), -(R)1 / (a.dx * ru), a.mfx, T_MFX, off(c, -sx), c,
                  c, off(c, sx), true, a.u, T_U, c, sx);
@@ -177,7 +177,7 @@ __device__ void row_tu(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   emit_div(acc, a, i - 1, j, k, u0 * (R)0.5 / ru);
   emit_div(acc, a, i, j, k, u0 * (R)0.5 / ru);
   acc(T_U, c, dv / ru - sponge(a.m.zeta_c[kk], a.m.zt, a.p));
-  const R fc = (R)0.5 * (a.m.fcor[L.at2(i - 1, j)] + a.m.fcor[L.at2(i, j)]);
+  const R fc = (R)0.5 * (a.m.fcor[L.at2i(i - 1, j)] + a.m.fcor[L.at2i(i, j)]);
   acc(T_V, off(c, -sx), (R)0.25 * fc);
   acc(T_V, off(c, sy - sx), (R)0.25 * fc);
   acc(T_V, c, (R)0.25 * fc);
@@ -190,9 +190,9 @@ template <typename R, class Acc>
 __device__ void row_tv(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px, sz = (long)L.plane();
-  const R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2(i, j)]);
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px, sz = (int)L.planei();
+  const R rv = (R)0.5 * (a.b.rhob[c - sy] * a.m.jac[L.at2i(i, j - 1)] + a.b.rhob[c] * a.m.jac[L.at2i(i, j)]);
   const R dzc = a.m.dzeta_c[kk];
   emit_face_pair(acc, (R)1 / (a.dy * rv), -(R)1 / (a.dy * rv), a.mfy, T_MFY, off(c, -sy), c,
                  c, off(c, sy), true, a.v, T_V, c, sy);
@@ -205,7 +205,7 @@ __device__ void row_tv(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   emit_div(acc, a, i, j - 1, k, v0 * (R)0.5 / rv);
   emit_div(acc, a, i, j, k, v0 * (R)0.5 / rv);
   acc(T_V, c, dv / rv - sponge(a.m.zeta_c[kk], a.m.zt, a.p));
-  const R fc = (R)0.5 * (a.m.fcor[L.at2(i, j - 1)] + a.m.fcor[L.at2(i, j)]);
+  const R fc = (R)0.5 * (a.m.fcor[L.at2i(i, j - 1)] + a.m.fcor[L.at2i(i, j)]);
   acc(T_U, off(c, -sy), -(R)0.25 * fc);
   acc(T_U, off(c, sx - sy), -(R)0.25 * fc);
   acc(T_U, c, -(R)0.25 * fc);
@@ -218,9 +218,9 @@ template <typename R, class Acc>
 __device__ void row_tw(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px, sz = (long)L.plane();
-  const R rw = a.b.rhobw[c] * a.m.jac[L.at2(i, j)];
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px, sz = (int)L.planei();
+  const R rw = a.b.rhobw[c] * a.m.jac[L.at2i(i, j)];
   const R dzw = a.m.dzeta_w[kk];
   emit_face_pair(acc, (R)1 / (a.dx * rw), -(R)1 / (a.dx * rw), a.mfx, T_MFX, off(c, -sz), c,
                  off(c, sx - sz), off(c, sx), true, a.w, T_W, c, sx);
@@ -241,9 +241,9 @@ template <typename R, class Acc>
 __device__ void row_tth(Acc& acc, const TendArgs<R>& a, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px, sz = (long)L.plane();
-  const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px, sz = (int)L.planei();
+  const R rt = a.b.rhob[c] * a.m.jac[L.at2i(i, j)];
   const R dzc = a.m.dzeta_c[kk];
   emit_face_pair(acc, (R)1 / (a.dx * rt), -(R)1 / (a.dx * rt), a.mfx, T_MFX, c, c,
                  off(c, sx), 0, false, a.thp, T_TH, c, sx);
@@ -262,9 +262,9 @@ template <typename R, class Acc>
 __device__ void row_tq(Acc& acc, const TendArgs<R>& a, const R* q, int qid, int i, int j, int k) {
   const Layout& L = a.L;
   const int kk = L.at1(k);
-  const size_t c = L.at(i, j, k);
-  const long sx = 1, sy = L.px, sz = (long)L.plane();
-  const R rt = a.b.rhob[c] * a.m.jac[L.at2(i, j)];
+  const int c = L.ati(i, j, k);
+  const int sx = 1, sy = L.px, sz = (int)L.planei();
+  const R rt = a.b.rhob[c] * a.m.jac[L.at2i(i, j)];
   const R dzc = a.m.dzeta_c[kk];
   emit_face_pair(acc, (R)1 / (a.dx * rt), -(R)1 / (a.dx * rt), a.mfx, T_MFX, c, c,
                  off(c, sx), 0, false, q, qid, c, sx);
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(256) k_tl_tend(TendArgs<R> a, TendArgs<R> d) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const Ptrs<R, T_N> P = tend_ptrs(d);
   {
     TLAcc<R, T_N> acc{P, 0};
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256) k_ad_tend(TendArgs<R> a, TendArgs<R> d) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= L.nx || j >= L.ny || k >= L.nz) return;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const Ptrs<R, T_N> P = tend_ptrs(d);
   // each output adjoint is cleared once it has been read and used (a store
   // issued while the load of the same address is in flight stalls the
@@ -418,7 +418,7 @@ __device__ __forceinline__ void ad_fill_point(const FillArgs<R>& A, int f, int i
   // an interior level of a column that is not a ghost (the u face nx of an
   // open x boundary, the v face ny of an open y boundary)
   if (!lateral && k >= 0 && k < L.nz) return;
-  const size_t q = L.at(i, j, k);
+  const int q = L.ati(i, j, k);
   // the ghost's adjoint moves to its sources; it is cleared only once read
   // (a store issued while the load of the same address is in flight stalls
   // the memory pipeline)
@@ -427,15 +427,15 @@ __device__ __forceinline__ void ad_fill_point(const FillArgs<R>& A, int f, int i
   a[q] = 0;
   if (kind == 3) {
     if (k == L.nz) return;
-    if (k >= 0 && k < L.nz) atomicAdd(a + L.at(si, sj, k), g);
+    if (k >= 0 && k < L.nz) atomicAdd(a + L.ati(si, sj, k), g);
     else if (k < 0) {
-      atomicAdd(a + L.at(si, sj, 0), (R)2 * g);
-      atomicAdd(a + L.at(si, sj, -k), -g);
+      atomicAdd(a + L.ati(si, sj, 0), (R)2 * g);
+      atomicAdd(a + L.ati(si, sj, -k), -g);
     } else {
-      atomicAdd(a + L.at(si, sj, 2 * L.nz - k), -g);
+      atomicAdd(a + L.ati(si, sj, 2 * L.nz - k), -g);
     }
   } else {
-    atomicAdd(a + L.at(si, sj, map_zc(k, L.nz)), g);
+    atomicAdd(a + L.ati(si, sj, map_zc(k, L.nz)), g);
   }
 }
 
@@ -444,8 +444,8 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_ad_fill_levels(FillArgs<R> A) {
   const Layout& L = A.L;
   const int f = blockIdx.z;
-  const long col = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= A.job.n || col >= (long)L.nx * L.ny) return;
+  const int col = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= A.job.n || col >= (int)L.nx * L.ny) return;
   const int m = blockIdx.y;
   const int k = m < kRefNG ? m - kRefNG : L.nz + (m - kRefNG);
   ad_fill_point(A, f, (int)(col % L.nx), (int)(col / L.nx), k);
@@ -457,7 +457,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_ad_fill_ring(FillArgs<R> A) {
   const Layout& L = A.L;
   const int f = blockIdx.z;
-  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= A.job.n || r >= ring_columns(L)) return;
   int i, j;
   ring_column(L, r, &i, &j);
@@ -473,16 +473,16 @@ __global__ void k_ad_flux(FluxArgs<R> A) {
   const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 2;
   const int k = (int)(blockIdx.z * blockDim.z + threadIdx.z);
   if (i > L.nx + 2 || j > L.ny + 2 || k > L.nz) return;
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   R* ub = const_cast<R*>(A.u);
   R* vb = const_cast<R*>(A.v);
   R* wb = const_cast<R*>(A.w);
   if (k < L.nz) {
     const R gx = A.mfx[c], gy = A.mfy[c];
-    R rjx = (R)0.5 * (A.b.rhob[L.at(i - 1, j, k)] * A.m.jac[L.at2(i - 1, j)] +
-                      A.b.rhob[c] * A.m.jac[L.at2(i, j)]);
-    R rjy = (R)0.5 * (A.b.rhob[L.at(i, j - 1, k)] * A.m.jac[L.at2(i, j - 1)] +
-                      A.b.rhob[c] * A.m.jac[L.at2(i, j)]);
+    R rjx = (R)0.5 * (A.b.rhob[L.ati(i - 1, j, k)] * A.m.jac[L.at2i(i - 1, j)] +
+                      A.b.rhob[c] * A.m.jac[L.at2i(i, j)]);
+    R rjy = (R)0.5 * (A.b.rhob[L.ati(i, j - 1, k)] * A.m.jac[L.at2i(i, j - 1)] +
+                      A.b.rhob[c] * A.m.jac[L.at2i(i, j)]);
     if (gx != (R)0) {
       atomicAdd(ub + c, rjx * gx);
       A.mfx[c] = 0;
@@ -501,19 +501,19 @@ __global__ void k_ad_flux(FluxArgs<R> A) {
   R fac = (R)1 - A.m.zeta_w[kk] / A.m.zt;
   R rw = A.b.rhobw[c];
   atomicAdd(wb + c, rw * gz);
-  R cu = -rw * gz * (R)0.25 * A.m.hx[L.at2(i, j)] * fac;
-  R cv = -rw * gz * (R)0.25 * A.m.hy[L.at2(i, j)] * fac;
+  R cu = -rw * gz * (R)0.25 * A.m.hx[L.at2i(i, j)] * fac;
+  R cv = -rw * gz * (R)0.25 * A.m.hy[L.at2i(i, j)] * fac;
   if (cu != (R)0) {
-    atomicAdd(ub + L.at(i, j, k - 1), cu);
-    atomicAdd(ub + L.at(i + 1, j, k - 1), cu);
+    atomicAdd(ub + L.ati(i, j, k - 1), cu);
+    atomicAdd(ub + L.ati(i + 1, j, k - 1), cu);
     atomicAdd(ub + c, cu);
-    atomicAdd(ub + L.at(i + 1, j, k), cu);
+    atomicAdd(ub + L.ati(i + 1, j, k), cu);
   }
   if (cv != (R)0) {
-    atomicAdd(vb + L.at(i, j, k - 1), cv);
-    atomicAdd(vb + L.at(i, j + 1, k - 1), cv);
+    atomicAdd(vb + L.ati(i, j, k - 1), cv);
+    atomicAdd(vb + L.ati(i, j + 1, k - 1), cv);
     atomicAdd(vb + c, cv);
-    atomicAdd(vb + L.at(i, j + 1, k), cv);
+    atomicAdd(vb + L.ati(i, j + 1, k), cv);
   }
 }
 
@@ -535,11 +535,11 @@ __device__ __forceinline__ void emit_pistar(Acc& acc, const AcouArgs<R>& a, int 
   const R sm = a.p.acoustic_smdiv;
   const bool ghost = i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz;
   if (!ghost) {
-    const size_t c = L.at(i, j, k);
+    const int c = L.ati(i, j, k);
     acc(A_PICUR, c, coef * ((R)1 + sm));
     acc(A_PIPREV, c, -coef * sm);
   } else {
-    const size_t c = L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open),
+    const int c = L.ati(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open),
                           map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), map_zc(k, L.nz));
     acc(A_PICUR, c, coef * ((R)1 + sm));
     acc(A_NPIP, c, -coef * sm);
@@ -551,9 +551,9 @@ template <typename R, class Acc>
 __device__ __forceinline__ void emit_thv(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R coef) {
   const Layout& L = a.L;
   const bool lat = i < 0 || i >= L.nx || j < 0 || j >= L.ny;
-  const size_t c = L.at(i, j, k);
-  const size_t s =
-      lat ? L.at(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open), map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), k)
+  const int c = L.ati(i, j, k);
+  const int s =
+      lat ? L.ati(map_lat(i, L.nx, L.nx - 1, a.p.bc_x_open), map_lat(j, L.ny, L.ny - 1, a.p.bc_y_open), k)
           : c;
   R f = coef;
   if (a.p.moisture) {
@@ -579,15 +579,15 @@ __device__ __forceinline__ UvFace<R> uv_face_terms(const AcouArgs<R>& a, int i, 
   const int di = is_u ? 1 : 0, dj = is_u ? 0 : 1;
   UvFace<R> f;
   f.thf = (R)0.5 * (theta_v(a, i - di, j - dj, k) + theta_v(a, i, j, k));
-  f.mf = (R)0.5 * (a.m.mapf[L.at2(i - di, j - dj)] + a.m.mapf[L.at2(i, j)]);
+  f.mf = (R)0.5 * (a.m.mapf[L.at2i(i - di, j - dj)] + a.m.mapf[L.at2i(i, j)]);
   f.h = is_u ? a.dx : a.dy;
   f.grad = (pistar(a, i, j, k) - pistar(a, i - di, j - dj, k)) / f.h;
-  f.slope = (is_u ? a.m.hx_u[L.at2(i, j)] : a.m.hy_v[L.at2(i, j)]) * ((R)1 - a.m.zeta_c[kk] / a.m.zt);
+  f.slope = (is_u ? a.m.hx_u[L.at2i(i, j)] : a.m.hy_v[L.at2i(i, j)]) * ((R)1 - a.m.zeta_c[kk] / a.m.zt);
   f.dzc2 = 1;
   f.jf = 1;
   if (f.slope != (R)0) {
     f.dzc2 = a.m.zeta_c[kk + 1] - a.m.zeta_c[kk - 1];
-    f.jf = (R)0.5 * (a.m.jac[L.at2(i - di, j - dj)] + a.m.jac[L.at2(i, j)]);
+    f.jf = (R)0.5 * (a.m.jac[L.at2i(i - di, j - dj)] + a.m.jac[L.at2i(i, j)]);
     R dpdz = (R)0.5 *
              ((pistar(a, i - di, j - dj, k + 1) - pistar(a, i - di, j - dj, k - 1)) +
               (pistar(a, i, j, k + 1) - pistar(a, i, j, k - 1))) /
@@ -604,7 +604,7 @@ __device__ R uv_face(Acc* acc, const AcouArgs<R>& a, int i, int j, int k, bool i
   const Layout& L = a.L;
   const int di = is_u ? 1 : 0, dj = is_u ? 0 : 1;
   const UvFace<R> f = uv_face_terms(a, i, j, k, is_u);
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const R* tin = is_u ? a.tu : a.tv;
   const R* vin = is_u ? a.u_in : a.v_in;
   const R out = vin[c] + a.dtau * (-Phys<R>::cp * f.thf * f.mf * f.grad + tin[c]);
@@ -636,7 +636,7 @@ __device__ void row_u_out(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R
   const R cstar = a.p.cstar;
   if (a.p.bc_x_open) {
     if (i == 0) {
-      const size_t c0 = L.at(0, j, k);
+      const int c0 = L.ati(0, j, k);
       const R u0 = a.u_in[c0];
       if (u0 >= (R)0) return;  // out = ub
       const R cb = u0 - cstar;
@@ -644,7 +644,7 @@ __device__ void row_u_out(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R
       acc(A_UIN, c0, coef * ((R)1 - a.dtau / a.dx * (uf1 - u0 - cb)));
       uv_face(&acc, a, 1, j, k, true, -coef * a.dtau * cb / a.dx);
     } else if (i == L.nx) {
-      const size_t cn = L.at(L.nx, j, k);
+      const int cn = L.ati(L.nx, j, k);
       const R un = a.u_in[cn];
       if (un <= (R)0) return;
       const R cb = un + cstar;
@@ -665,7 +665,7 @@ __device__ void row_v_out(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R
   const R cstar = a.p.cstar;
   if (a.p.bc_y_open) {
     if (j == 0) {
-      const size_t c0 = L.at(i, 0, k);
+      const int c0 = L.ati(i, 0, k);
       const R v0 = a.v_in[c0];
       if (v0 >= (R)0) return;  // out = 0
       const R cb = v0 - cstar;
@@ -673,7 +673,7 @@ __device__ void row_v_out(Acc& acc, const AcouArgs<R>& a, int i, int j, int k, R
       acc(A_VIN, c0, coef * ((R)1 - a.dtau / a.dy * (vf1 - v0 - cb)));
       uv_face(&acc, a, i, 1, k, false, -coef * a.dtau * cb / a.dy);
     } else if (j == L.ny) {
-      const size_t cn = L.at(i, L.ny, k);
+      const int cn = L.ati(i, L.ny, k);
       const R vn = a.v_in[cn];
       if (vn <= (R)0) return;
       const R cb = vn + cstar;
@@ -703,12 +703,12 @@ __global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_tl_uv(AcouArgs<R> a
   if (j < L.ny) {
     TLAcc<R, A_N> acc{P, 0};
     row_u_out(acc, a, i, j, k, (R)1);
-    d.u_out[L.at(i, j, k)] = acc.sum;
+    d.u_out[L.ati(i, j, k)] = acc.sum;
   }
   if (i < L.nx) {
     TLAcc<R, A_N> acc{P, 0};
     row_v_out(acc, a, i, j, k, (R)1);
-    d.v_out[L.at(i, j, k)] = acc.sum;
+    d.v_out[L.ati(i, j, k)] = acc.sum;
   }
 }
 
@@ -741,8 +741,8 @@ __device__ __forceinline__ void ad_uv_face(const AcouArgs<R>& a, const AcouArgs<
   const R* xin = is_u ? a.u_in : a.v_in;
   R* xb = const_cast<R*>(is_u ? d.u_in : d.v_in);
   R* tb = const_cast<R*>(is_u ? d.tu : d.tv);
-  auto at_f = [&](int q) { return is_u ? L.at(q, j, k) : L.at(i, q, k); };
-  const size_t c = L.at(i, j, k);
+  auto at_f = [&](int q) { return is_u ? L.ati(q, j, k) : L.ati(i, q, k); };
+  const int c = L.ati(i, j, k);
   R ce = 0;  // coefficient of the uv_face row at this face
   if (open) {
     if (f == 0 || f == n) {
@@ -758,12 +758,12 @@ __device__ __forceinline__ void ad_uv_face(const AcouArgs<R>& a, const AcouArgs<
     } else {
       ce = yb[c];
       if (f == 1) {
-        const size_t c0 = at_f(0);
+        const int c0 = at_f(0);
         const R x0 = xin[c0];
         if (x0 < (R)0) ce += -yb[c0] * a.dtau * (x0 - cstar) / h;
       }
       if (f == n - 1) {
-        const size_t cn = at_f(n);
+        const int cn = at_f(n);
         const R xn = xin[cn];
         if (xn > (R)0) ce += yb[cn] * a.dtau * (xn + cstar) / h;
       }
@@ -809,10 +809,10 @@ __global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_ad_uv_cells(AcouArg
   if (i >= nx || j >= ny || k >= nz) return;
   // face coefficients, zero outside the faces that exist
   auto U = [&](const R* g, int fi, int fj, int fk) -> R {
-    return (fi >= 0 && fi <= nx && fj >= 0 && fj < ny && fk >= 0 && fk < nz) ? g[L.at(fi, fj, fk)] : (R)0;
+    return (fi >= 0 && fi <= nx && fj >= 0 && fj < ny && fk >= 0 && fk < nz) ? g[L.ati(fi, fj, fk)] : (R)0;
   };
   auto V = [&](const R* g, int fi, int fj, int fk) -> R {
-    return (fi >= 0 && fi < nx && fj >= 0 && fj <= ny && fk >= 0 && fk < nz) ? g[L.at(fi, fj, fk)] : (R)0;
+    return (fi >= 0 && fi < nx && fj >= 0 && fj <= ny && fk >= 0 && fk < nz) ? g[L.ati(fi, fj, fk)] : (R)0;
   };
   // adjoint of pi* at cell (ci, cj, ck), interior or ghost (emit_pistar)
   auto pbar = [&](int ci, int cj, int ck) -> R {
@@ -821,7 +821,7 @@ __global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_ad_uv_cells(AcouArg
            U(w.gs_u, ci + 1, cj, ck - 1) - U(w.gs_u, ci + 1, cj, ck + 1) + V(w.gs_v, ci, cj, ck - 1) -
            V(w.gs_v, ci, cj, ck + 1) + V(w.gs_v, ci, cj + 1, ck - 1) - V(w.gs_v, ci, cj + 1, ck + 1);
   };
-  const size_t c = L.at(i, j, k);
+  const int c = L.ati(i, j, k);
   const R sm = a.p.acoustic_smdiv;
   R* piC = const_cast<R*>(d.pi_cur);
   R* piP = const_cast<R*>(d.pi_prev);
@@ -870,7 +870,7 @@ __global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_ad_uv_cells(AcouArg
       }
     }
     R Tg[2] = {gx ? U(w.gt_u, 0, j, k) : (R)0, gy ? V(w.gt_v, i, 0, k) : (R)0};
-    const size_t gc[2] = {L.at(-1, j, k), L.at(i, -1, k)};
+    const int gc[2] = {L.ati(-1, j, k), L.ati(i, -1, k)};
     for (int q = 0; q < 2; ++q) {
       if (Tg[q] == (R)0) continue;
       if (moist) {
@@ -884,8 +884,8 @@ __global__ void __launch_bounds__(256, kUvLinMinBlocks<R>) k_ad_uv_cells(AcouArg
   // the output adjoints are consumed
   d.u_out[c] = 0;
   d.v_out[c] = 0;
-  if (i == nx - 1) d.u_out[L.at(nx, j, k)] = 0;
-  if (j == ny - 1) d.v_out[L.at(i, ny, k)] = 0;
+  if (i == nx - 1) d.u_out[L.ati(nx, j, k)] = 0;
+  if (j == ny - 1) d.v_out[L.ati(i, ny, k)] = 0;
 }
 
 // ================================================================ w - pi' column
@@ -963,7 +963,7 @@ template <typename R>
 struct ColArr {
   R* base;
   int n1;  // nz + 1
-  __device__ R* operator[](int q) const { return base + (size_t)q * n1 * kLcx<R>; }
+  __device__ R* operator[](int q) const { return base + (int)q * n1 * kLcx<R>; }
 };
 
 // What the TL and AD kernels of one column share: the column's geometry and
@@ -973,14 +973,14 @@ struct ColGeom {
   int nz;
   R dtau, c1, c2, J, invJ, hxc, hyc, mc, mcx, mcy;
   bool terrain;
-  size_t c0, sx, sy, pl;
+  int c0, sx, sy, pl;
   __device__ ColGeom(const AcouArgs<R>& a, int i, int j, bool active) {
     const Layout& L = a.L;
     nz = L.nz;
     dtau = a.dtau;
     c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
     c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-    const size_t c2d = L.at2(active ? i : 0, j);
+    const int c2d = L.at2i(active ? i : 0, j);
     J = a.m.jac[c2d];
     hxc = a.m.hx[c2d];
     hyc = a.m.hy[c2d];
@@ -991,10 +991,10 @@ struct ColGeom {
     terrain = hxc != (R)0 || hyc != (R)0;
     sx = 1;
     sy = L.px;
-    pl = L.plane();
-    c0 = L.at(active ? i : 0, j, 0);
+    pl = L.planei();
+    c0 = L.ati(active ? i : 0, j, 0);
   }
-  __device__ size_t at(int k) const { return c0 + (size_t)k * pl; }
+  __device__ int at(int k) const { return c0 + (int)k * pl; }
 };
 
 // Forward values of one column (kernels.cu:552-634) with the forward column
@@ -1011,7 +1011,7 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
   const R dtau = g.dtau, c1 = g.c1, c2 = g.c2;
   const R* __restrict__ u = a.u_out;
   const R* __restrict__ v = a.v_out;
-  const size_t sx = g.sx, sy = g.sy, pl = g.pl;
+  const int sx = g.sx, sy = g.sy, pl = g.pl;
   R *Av = S[V_AV] + tx, *Sv = S[V_SV] + tx, *P = S[V_P] + tx, *E = S[V_E] + tx;
   R *G = S[V_G] + tx, *A = S[V_A] + tx, *B = S[V_B] + tx, *C = S[V_C] + tx, *D = S[V_D] + tx;
   if (active)
@@ -1019,7 +1019,7 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
     for (int k = lane; k <= nz; k += kLkl<R>) {
       R av = 0, sv = 0;
       if (k >= 1 && k < nz) {
-        const size_t c = g.at(k), cm = c - pl;
+        const int c = g.at(k), cm = c - pl;
         av = a.co.aw[c];
         if (g.terrain) {
           R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
@@ -1034,7 +1034,7 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
   if (active)
 #pragma unroll 4
     for (int k = lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       R Kt = a.co.kt3[c];
       R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * g.mcx +
              (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * g.mcy;
@@ -1050,7 +1050,7 @@ __device__ __forceinline__ void column_values_s(const AcouArgs<R>& a, const ColG
   if (active)
 #pragma unroll 4
     for (int k = 1 + lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k), cm = c - pl;
+      const int c = g.at(k), cm = c - pl;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       R thc = a.th_in[c], thm = a.th_in[cm];
       R thbw = a.b.thbw[c];
@@ -1102,7 +1102,7 @@ __device__ __forceinline__ void column_values_stored_s(const AcouArgs<R>& a, con
   if (active)
 #pragma unroll 4
     for (int k = lane; k <= nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       Av[k * kLcx<R>] = (k >= 1 && k < nz) ? a.co.aw[c] : (R)0;
       W[k * kLcx<R>] = k < nz ? a.w_out[c] : (R)0;
     }
@@ -1110,7 +1110,7 @@ __device__ __forceinline__ void column_values_stored_s(const AcouArgs<R>& a, con
   if (active)
 #pragma unroll 4
     for (int k = lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       const int q = k * kLcx<R>;
       const R e = dtau * a.co.kt3[c] * c1 * a.co.inv_dzc[L.at1(k)];
       E[q] = e;
@@ -1120,7 +1120,7 @@ __device__ __forceinline__ void column_values_stored_s(const AcouArgs<R>& a, con
   if (active)
 #pragma unroll 4
     for (int k = 1 + lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k), cm = c - g.pl;
+      const int c = g.at(k), cm = c - g.pl;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       R thvw = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
       if (a.p.moisture) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (a.qv[cm] + a.qv[c]);
@@ -1150,7 +1150,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_tl_column(AcouArgs<R> a, 
   const R dtau = g.dtau, c1 = g.c1, c2 = g.c2;
   const R* __restrict__ du = d.u_out;
   const R* __restrict__ dv = d.v_out;
-  const size_t sx = g.sx, sy = g.sy, pl = g.pl;
+  const int sx = g.sx, sy = g.sy, pl = g.pl;
   R *dSv = S[T_DSV] + tx, *dth = S[T_DTH] + tx, *dP = S[T_DP] + tx;
   R *rhs = S[T_RHS] + tx, *dw = S[T_DW] + tx;
   // the tangent theta' in, before any in-place write of this launch
@@ -1165,7 +1165,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_tl_column(AcouArgs<R> a, 
     for (int k = lane; k <= nz; k += kLkl<R>) {
       R sv = 0;
       if (g.terrain && k >= 1 && k < nz) {
-        const size_t c = g.at(k), cm = c - pl;
+        const int c = g.at(k), cm = c - pl;
         R uw = (R)0.25 * (du[cm] + du[cm + sx] + du[c] + du[c + sx]);
         R vw = (R)0.25 * (dv[cm] + dv[cm + sy] + dv[c] + dv[c + sy]);
         sv = Av[k * kLcx<R>] * (uw * g.hxc + vw * g.hyc) * a.co.fac_w[L.at1(k)];
@@ -1176,7 +1176,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_tl_column(AcouArgs<R> a, 
   if (active)
 #pragma unroll 4
     for (int k = lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       R Kt = a.co.kt3[c];
       R dDh = (a.co.rtjx[c + sx] * du[c + sx] - a.co.rtjx[c] * du[c]) * g.mcx +
               (a.co.rtjy[c + sy] * dv[c + sy] - a.co.rtjy[c] * dv[c]) * g.mcy;
@@ -1191,7 +1191,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_tl_column(AcouArgs<R> a, 
   if (active)
 #pragma unroll 4
     for (int k = 1 + lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k), cm = c - pl;
+      const int c = g.at(k), cm = c - pl;
       const int q = k * kLcx<R>;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       const R thd = a.b.thbw[c] + (R)0.5 * (a.th_in[cm] + a.th_in[c]);
@@ -1228,7 +1228,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_tl_column(AcouArgs<R> a, 
   if (active)
 #pragma unroll 4
     for (int k = lane; k <= nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       const int q = k * kLcx<R>;
       if (k < nz) {
         d.pi_next[c] = dP[q] - E[q] * (Av[q + kLcx<R>] * dw[q + kLcx<R>] - Av[q] * dw[q]);
@@ -1272,7 +1272,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
   const ColGeom<R> g(a, i, j, active);
   const int nz = g.nz;
   const R dtau = g.dtau, c1 = g.c1, c2 = g.c2;
-  const size_t pl = g.pl;
+  const int pl = g.pl;
   R* wI = const_cast<R*>(d.w_in);
   R* piC = const_cast<R*>(d.pi_cur);
   R* thI = const_cast<R*>(d.th_in);
@@ -1298,7 +1298,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
   if (active)
 #pragma unroll 4
     for (int k = lane; k <= nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       const int q = k * kLcx<R>;
       wb[q] = d.w_out[c];
       if (k < nz) {
@@ -1317,7 +1317,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
 #pragma unroll 4
     for (int k = lane; k <= nz; k += kLkl<R>) {
       const int q = k * kLcx<R>;
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       R s = 0;
       if (k < nz) s += wb[q] - (R)0.5 * dtau * a.b.dthbdz[c] * tb[q] + E[q] * Av[q] * pb[q];
       if (k >= 1) s += -(R)0.5 * dtau * a.b.dthbdz[c - pl] * tb[q - kLcx<R>] - E[q - kLcx<R>] * Av[q] * pb[q - kLcx<R>];
@@ -1340,7 +1340,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
         QCB[q] = 0;
         continue;
       }
-      const size_t c = g.at(k), cm = c - pl;
+      const int c = g.at(k), cm = c - pl;
       const R iJdz = g.invJ * a.co.inv_dzw[L.at1(k)];
       const R lm = lam[q];
       const R Ab = k > 1 ? -lm * W[q - kLcx<R>] : (R)0;
@@ -1366,7 +1366,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
   if (active)
 #pragma unroll 4
     for (int k = lane; k < nz; k += kLkl<R>) {
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       const int q = k * kLcx<R>;
       // the adjoints this level accumulates into, all read first
       const R pic0 = piC[c];
@@ -1411,7 +1411,7 @@ __global__ void __launch_bounds__(kLcx<R> * kLkl<R>) k_ad_column(AcouArgs<R> a, 
 #pragma unroll 4
     for (int k = lane; k <= nz; k += kLkl<R>) {
       const int q = k * kLcx<R>;
-      const size_t c = g.at(k);
+      const int c = g.at(k);
       const R w0 = w_alias ? (R)0 : wI[c];
       R wsum = 0;
       if (k >= 1 && k < nz) wsum += lam[q];
@@ -1442,27 +1442,27 @@ __global__ void __launch_bounds__(256) k_ad_column_uv(AcouArgs<R> a, AcouArgs<R>
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   if (i > nx || j > ny || k >= nz) return;
-  const size_t c = L.at(i, j, k), pl = L.plane();
+  const int c = L.ati(i, j, k), pl = L.planei();
   // a column's weight at level k for the faces of level k: its own level and the one above
-  auto wsv = [&](size_t cc) { return sv[cc] + (k + 1 < nz ? sv[cc + pl] : (R)0); };
+  auto wsv = [&](int cc) { return sv[cc] + (k + 1 < nz ? sv[cc + pl] : (R)0); };
   if (j < ny) {  // u face i: columns i - 1 and i
     R g = 0;
     const R rj = a.co.rtjx[c] * a.co.inv_dx;
     if (i >= 1) {
-      const size_t cl = c - 1;
-      g += rj * dh[cl] + a.m.hx[L.at2(i - 1, j)] * wsv(cl);
+      const int cl = c - 1;
+      g += rj * dh[cl] + a.m.hx[L.at2i(i - 1, j)] * wsv(cl);
     }
-    if (i < nx) g += -rj * dh[c] + a.m.hx[L.at2(i, j)] * wsv(c);
+    if (i < nx) g += -rj * dh[c] + a.m.hx[L.at2i(i, j)] * wsv(c);
     if (g != (R)0) d.u_out[c] += g;
   }
   if (i < nx) {  // v face j: rows j - 1 and j
     R g = 0;
     const R rj = a.co.rtjy[c] * a.co.inv_dy;
     if (j >= 1) {
-      const size_t cl = c - L.px;
-      g += rj * dh[cl] + a.m.hy[L.at2(i, j - 1)] * wsv(cl);
+      const int cl = c - L.px;
+      g += rj * dh[cl] + a.m.hy[L.at2i(i, j - 1)] * wsv(cl);
     }
-    if (j < ny) g += -rj * dh[c] + a.m.hy[L.at2(i, j)] * wsv(c);
+    if (j < ny) g += -rj * dh[c] + a.m.hy[L.at2i(i, j)] * wsv(c);
     if (g != (R)0) d.v_out[c] += g;
   }
 }

@@ -124,6 +124,8 @@ class ModelT final : public Model {
     g_ = cs.g;
     hp_ = cs.p;
     L_ = make_layout(g_.nx, g_.ny, g_.nz);
+    if (L_.n3() >= kMaxIndexedPoints)
+      return fail("grid too large: a padded field must hold fewer than 2^31 points");
     dev_ = device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
