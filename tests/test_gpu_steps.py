@@ -346,6 +346,30 @@ def test_pipelined_parallel_solve_equals_parallel_solve(name, prec, monkeypatch)
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["wk82_small", "moist_blob", "bubble_open", "schaer_open"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_pipelined_parallel_solve_level_tables_equal_boxes(name, prec, monkeypatch):
+    """On flat ground the column coefficients (rtjx, rtjy, aw, kt3, theta_b^w,
+    dtheta_b/dz, qv_b) hold one value per level, and the pipelined
+    parallel-solve kernels read them from per-level tables instead of
+    streaming a box of each per tile: the same fields, bit for bit, as with
+    the boxes (WFE_COLUMN_PROFILES=0) after five steps.  With terrain
+    (schaer_open) the tables are not built and both runs stream boxes."""
+    for v in ("19", "20", "21", "22"):
+        monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
+        out = {}
+        for prof in ("1", "0"):
+            monkeypatch.setenv("WFE_COLUMN_PROFILES", prof)
+            c = W.Case(CASES / f"{name}.ini", precision=prec)
+            c.run(5, c.dt, 0.0)
+            c.sync()
+            out[prof] = {k: c.field(k) for k in W.FIELDS}
+            c.close()
+        for k in W.FIELDS:
+            assert np.array_equal(out["1"][k], out["0"][k]), (v, k)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("prec,tol", [("f64", 1e-11), ("f32", 1e-4)])
 def test_parallel_solve_columns_with_relaxation_and_surface_physics(prec, tol, monkeypatch, tmp_path):
     """The file-mode case (Davies relaxation, whose slow pi' tendency is one

@@ -164,13 +164,29 @@ __device__ __forceinline__ R v_forward(const AcouArgs<R>& a, int i, int j, int k
 // at the face's two cells (kernels.cu:499-526).  pz(p) gives the pi* values
 // the terrain term needs, p = {pi*(west/south, k+1), pi*(west/south, k-1),
 // pi*(k+1), pi*(k-1)}, from global or from shared memory.
+// The face's metric factors: the map factor averaged over the face's two
+// cells and the terrain slope term (zero on flat ground).
+template <typename R>
+struct FaceMetric {
+  R mf, slope;
+};
+template <typename R>
+__device__ __forceinline__ FaceMetric<R> u_metric(const AcouArgs<R>& a, int c2, int kk) {
+  return {(R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]), a.m.hx_u[c2] * a.co.fac_c[kk]};
+}
+template <typename R>
+__device__ __forceinline__ FaceMetric<R> v_metric(const AcouArgs<R>& a, int c2, int kk) {
+  const int sy = a.L.px;
+  return {(R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]), a.m.hy_v[c2] * a.co.fac_c[kk]};
+}
+
 template <typename R, typename PZ>
-__device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, int c2, int kk, R tv0, R tvx, R ps0,
-                                             R psx, R uin, R tin, PZ pz) {
+__device__ __forceinline__ R u_interior_core_m(const AcouArgs<R>& a, int c2, int kk, FaceMetric<R> g, R tv0,
+                                               R tvx, R ps0, R psx, R uin, R tin, PZ pz) {
   R thb_f = (R)0.5 * (tvx + tv0);
-  R mf = (R)0.5 * (a.m.mapf[c2 - 1] + a.m.mapf[c2]);
+  R mf = g.mf;
   R grad = (ps0 - psx) * a.co.inv_dx;
-  R slope = a.m.hx_u[c2] * a.co.fac_c[kk];
+  R slope = g.slope;
   if (slope != (R)0) {
     R jf = (R)0.5 * (a.m.jac[c2 - 1] + a.m.jac[c2]);
     R q[4];
@@ -182,13 +198,13 @@ __device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, int c2, int k
 }
 
 template <typename R, typename PZ>
-__device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, int c2, int kk, R tv0, R tvy, R ps0,
-                                             R psy, R vin, R tin, PZ pz) {
+__device__ __forceinline__ R v_interior_core_m(const AcouArgs<R>& a, int c2, int kk, FaceMetric<R> g, R tv0,
+                                               R tvy, R ps0, R psy, R vin, R tin, PZ pz) {
   const int sy = a.L.px;
   R thb_f = (R)0.5 * (tvy + tv0);
-  R mf = (R)0.5 * (a.m.mapf[c2 - sy] + a.m.mapf[c2]);
+  R mf = g.mf;
   R grad = (ps0 - psy) * a.co.inv_dy;
-  R slope = a.m.hy_v[c2] * a.co.fac_c[kk];
+  R slope = g.slope;
   if (slope != (R)0) {
     R jf = (R)0.5 * (a.m.jac[c2 - sy] + a.m.jac[c2]);
     R q[4];
@@ -199,16 +215,34 @@ __device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, int c2, int k
   return vin + a.dtau * (-Phys<R>::cp * thb_f * mf * grad + tin);
 }
 
+template <typename R, typename PZ>
+__device__ __forceinline__ R u_interior_core(const AcouArgs<R>& a, int c2, int kk, R tv0, R tvx, R ps0,
+                                             R psx, R uin, R tin, PZ pz) {
+  return u_interior_core_m(a, c2, kk, u_metric(a, c2, kk), tv0, tvx, ps0, psx, uin, tin, pz);
+}
+
+template <typename R, typename PZ>
+__device__ __forceinline__ R v_interior_core(const AcouArgs<R>& a, int c2, int kk, R tv0, R tvy, R ps0,
+                                             R psy, R vin, R tin, PZ pz) {
+  return v_interior_core_m(a, c2, kk, v_metric(a, c2, kk), tv0, tvy, ps0, psy, vin, tin, pz);
+}
+
 template <typename R>
-__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvx,
-                                             R ps0, R psx, R uin, R tin) {
+__device__ __forceinline__ R u_interior_from_m(const AcouArgs<R>& a, int c, int c2, int kk, FaceMetric<R> g,
+                                               R tv0, R tvx, R ps0, R psx, R uin, R tin) {
   const int pl = a.L.planei();
-  return u_interior_core(a, c2, kk, tv0, tvx, ps0, psx, uin, tin, [&](R* q) {
+  return u_interior_core_m(a, c2, kk, g, tv0, tvx, ps0, psx, uin, tin, [&](R* q) {
     q[0] = pistar_at(a, c - 1 + pl);
     q[1] = pistar_at(a, c - 1 - pl);
     q[2] = pistar_at(a, c + pl);
     q[3] = pistar_at(a, c - pl);
   });
+}
+
+template <typename R>
+__device__ __forceinline__ R u_interior_from(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvx,
+                                             R ps0, R psx, R uin, R tin) {
+  return u_interior_from_m(a, c, c2, kk, u_metric(a, c2, kk), tv0, tvx, ps0, psx, uin, tin);
 }
 
 template <typename R>
@@ -218,15 +252,21 @@ __device__ __forceinline__ R u_interior_val(const AcouArgs<R>& a, int c, int c2,
 }
 
 template <typename R>
-__device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvy,
-                                             R ps0, R psy, R vin, R tin) {
+__device__ __forceinline__ R v_interior_from_m(const AcouArgs<R>& a, int c, int c2, int kk, FaceMetric<R> g,
+                                               R tv0, R tvy, R ps0, R psy, R vin, R tin) {
   const int sy = a.L.px, pl = a.L.planei();
-  return v_interior_core(a, c2, kk, tv0, tvy, ps0, psy, vin, tin, [&](R* q) {
+  return v_interior_core_m(a, c2, kk, g, tv0, tvy, ps0, psy, vin, tin, [&](R* q) {
     q[0] = pistar_at(a, c - sy + pl);
     q[1] = pistar_at(a, c - sy - pl);
     q[2] = pistar_at(a, c + pl);
     q[3] = pistar_at(a, c - pl);
   });
+}
+
+template <typename R>
+__device__ __forceinline__ R v_interior_from(const AcouArgs<R>& a, int c, int c2, int kk, R tv0, R tvy,
+                                             R ps0, R psy, R vin, R tin) {
+  return v_interior_from_m(a, c, c2, kk, v_metric(a, c2, kk), tv0, tvy, ps0, psy, vin, tin);
 }
 
 template <typename R>
@@ -314,11 +354,15 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   const bool has_cell = i < L.nx && j < L.ny && k < L.nz;
   const int c = has_cell ? L.ati(i, j, k) : 0;
   const int sy = L.px;
-  // an interior point's own inputs, and its x (y) neighbour's values when the
-  // neighbour is not in the block, are loaded before the barrier so that
-  // their latency overlaps the shared values' (the same values either way)
+  // an interior point's own inputs and face metric, and its x (y)
+  // neighbour's values when the neighbour is not in the block, are loaded
+  // before the barrier so that their latency overlaps the shared values'
+  // (the same values either way)
   const bool inner = uv_interior<R>(L, i, j, k);
   R tv0 = 0, ps0 = 0, uin = 0, tun = 0, vin = 0, tvn = 0, tvx = 0, psx = 0, tvy = 0, psy = 0;
+  FaceMetric<R> gu{}, gv{};
+  const int kk = L.at1(k);
+  const int c2 = L.at2i(i, j);
   if (has_cell) {
     tv0 = theta_v_at(a, c);
     ps0 = pistar_at(a, c);
@@ -328,6 +372,8 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
     tun = a.tu[c];
     vin = a.v_in[c];
     tvn = a.tv[c];
+    gu = u_metric(a, c2, kk);
+    gv = v_metric(a, c2, kk);
     if (tx == 0) {
       tvx = theta_v_at(a, c - 1);
       psx = pistar_at(a, c - 1);
@@ -351,10 +397,8 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
       tvy = s_tv[tz][ty - 1][tx];
       psy = s_ps[tz][ty - 1][tx];
     }
-    const int kk = L.at1(k);
-    const int c2 = L.at2i(i, j);
-    a.u_out[c] = u_interior_from(a, c, c2, kk, tv0, tvx, ps0, psx, uin, tun);
-    a.v_out[c] = v_interior_from(a, c, c2, kk, tv0, tvy, ps0, psy, vin, tvn);
+    a.u_out[c] = u_interior_from_m(a, c, c2, kk, gu, tv0, tvx, ps0, psx, uin, tun);
+    a.v_out[c] = v_interior_from_m(a, c, c2, kk, gv, tv0, tvy, ps0, psy, vin, tvn);
     return;
   }
   if (j < L.ny) a.u_out[L.ati(i, j, k)] = u_face_edge(a, i, j, k);
@@ -526,7 +570,7 @@ __global__ void __launch_bounds__(kUvpThreads + 32, 1)
     const bool cell = i < L.nx && j < L.ny && k < L.nz;
     if (cell) {
       const int kk = L.at1(k);
-      const size_t c2 = L.at2(i, j);
+      const int c2 = L.at2i(i, j);
       const int t0 = (tz * kUvpY + ty) * kUvpX + tx;  // tile-box index
       const int h0 = hix(0, 0, 0);
       const R tv0 = thv(h0), ps0 = pst(h0);
@@ -570,11 +614,11 @@ __global__ void __launch_bounds__(kUvpThreads + 32, 1)
     tma::named_sync(1, kUvpThreads);
     if (tid == 0) tma::mbar_arrive(&empty[s]);
     if (cell) {
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       a.u_out[c] = u_done ? uo : u_face_edge(a, i, j, k);
       a.v_out[c] = v_done ? vo : v_face_edge(a, i, j, k);
-      if (i == L.nx - 1) a.u_out[L.at(L.nx, j, k)] = u_face_edge(a, L.nx, j, k);
-      if (j == L.ny - 1) a.v_out[L.at(i, L.ny, k)] = v_face_edge(a, i, L.ny, k);
+      if (i == L.nx - 1) a.u_out[L.ati(L.nx, j, k)] = u_face_edge(a, L.nx, j, k);
+      if (j == L.ny - 1) a.v_out[L.ati(i, L.ny, k)] = v_face_edge(a, i, L.ny, k);
     }
   }
 }
@@ -599,9 +643,9 @@ template <typename R>
 struct UvGlobal {
   const R* __restrict__ u;
   const R* __restrict__ v;
-  size_t c0, pl, sy;
-  __device__ R u_at(int k, int dx) const { return u[c0 + (size_t)k * pl + dx]; }
-  __device__ R v_at(int k, int dy) const { return v[c0 + (size_t)k * pl + (size_t)dy * sy]; }
+  int c0, pl, sy;
+  __device__ R u_at(int k, int dx) const { return u[c0 + k * pl + dx]; }
+  __device__ R v_at(int k, int dy) const { return v[c0 + k * pl + dy * sy]; }
 };
 
 // tiles: us[k * (CX + 1) + face], vs[(k * 2 + row) * CX + column]
@@ -627,14 +671,14 @@ __device__ __forceinline__ void column_core(const AcouArgs<R>& a, int bx, int by
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
+  const int c2d = L.at2i(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   const R invJ = (R)1 / J;
   const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
   const bool terrain = hxc != (R)0 || hyc != (R)0;
-  const size_t sx = 1, sy = L.px, pl = L.plane();
-  const size_t c0 = L.at(active ? i : 0, j, 0);  // level k at c0 + k * pl
-#define SM(X, k) S.X[(size_t)(k) * CX + tx]
+  const int sx = 1, sy = L.px, pl = L.planei();
+  const int c0 = L.ati(active ? i : 0, j, 0);  // level k at c0 + k * pl
+#define SM(X, k) S.X[(k) * CX + tx]
 
   // phase 1: Av = rho^w theta_v^w (0 at the rigid levels) and the explicit
   // terrain cross flux Sv with the new u, v (kernels.cu:552-568)
@@ -643,7 +687,7 @@ __device__ __forceinline__ void column_core(const AcouArgs<R>& a, int bx, int by
     for (int k = lane_k; k <= nz; k += KL) {
       R av = 0, sv = 0;
       if (k >= 1 && k < nz) {
-        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const int c = c0 + k * pl, cm = c - pl;
         av = a.co.aw[c];
         if (terrain) {
           R uw = (R)0.25 * (uv.u_at(k - 1, 0) + uv.u_at(k - 1, 1) + uv.u_at(k, 0) + uv.u_at(k, 1));
@@ -660,7 +704,7 @@ __device__ __forceinline__ void column_core(const AcouArgs<R>& a, int bx, int by
 #pragma unroll 4
     for (int k = lane_k; k < nz; k += KL) {
       const int kk = L.at1(k);
-      const size_t c = c0 + (size_t)k * pl;
+      const int c = c0 + k * pl;
       R Kt = a.co.kt3[c];
       R Dh = (a.co.rtjx[c + sx] * uv.u_at(k, 1) - a.co.rtjx[c] * uv.u_at(k, 0)) * mcx +
              (a.co.rtjy[c + sy] * uv.v_at(k, 1) - a.co.rtjy[c] * uv.v_at(k, 0)) * mcy;
@@ -679,7 +723,7 @@ __device__ __forceinline__ void column_core(const AcouArgs<R>& a, int bx, int by
 #pragma unroll 4
     for (int k = 1 + lane_k; k < nz; k += KL) {
       const int kk = L.at1(k);
-      const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+      const int c = c0 + k * pl, cm = c - pl;
       const R iJdz = invJ * a.co.inv_dzw[kk];
       R thc = a.th_in[c], thm = a.th_in[cm];
       R thbw = a.b.thbw[c];
@@ -747,7 +791,7 @@ __device__ __forceinline__ void column_core(const AcouArgs<R>& a, int bx, int by
   if (active)
 #pragma unroll 4
     for (int k = lane_k; k <= nz; k += KL) {
-      const size_t c = c0 + (size_t)k * pl;
+      const int c = c0 + k * pl;
       if (k < nz) {
         R wn = SM(Wn, k), wn1 = SM(Wn, k + 1);
         a.pi_next[c] = SM(P, k) - SM(E, k) * (SM(Av, k + 1) * wn1 - SM(Av, k) * wn);
@@ -766,7 +810,7 @@ __device__ __forceinline__ void column_body(const AcouArgs<R>& a, int bx, int by
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Layout& L = a.L;
   const int i = bx * CX + (int)threadIdx.x;
-  const UvGlobal<R> uv{a.u_out, a.v_out, L.at(i < L.nx ? i : 0, by, 0), L.plane(), (size_t)L.px};
+  const UvGlobal<R> uv{a.u_out, a.v_out, L.ati(i < L.nx ? i : 0, by, 0), L.planei(), L.px};
   column_core<R, CX, KL>(a, bx, by, reinterpret_cast<R*>(smem_raw), uv);
 }
 
@@ -801,19 +845,19 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
+  const int c2d = L.at2i(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   const R invJ = (R)1 / J;
   const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
   const bool terrain = hxc != (R)0 || hyc != (R)0;
-  const size_t sx = 1, sy = L.px, pl = L.plane();
-  const size_t c0 = L.at(active ? i : 0, j, 0);
+  const int sx = 1, sy = L.px, pl = L.planei();
+  const int c0 = L.ati(active ? i : 0, j, 0);
   const R* __restrict__ u = a.u_out;
   const R* __restrict__ v = a.v_out;
   const int ch = (nz + KL) / KL;
   const int klo = lane * ch;  // first level of the chunk; s = k - klo + 1
   R av[KCH + 2], sv[KCH + 2], P[KCH + 1], E[KCH + 1], th[KCH + 1], tt[KCH + 1], db[KCH + 1];
-#define SQ(X, k) X[(size_t)(k) * CX + tx]
+#define SQ(X, k) X[(k) * CX + tx]
   if (active) {
     // phase 1 on levels klo-1 .. klo+ch
 #pragma unroll
@@ -821,7 +865,7 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
       const int k = klo - 1 + s;
       R avk = 0, svk = 0;
       if (s <= ch + 1 && k >= 1 && k < nz) {
-        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const int c = c0 + k * pl, cm = c - pl;
         avk = a.co.aw[c];
         if (terrain) {
           R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
@@ -839,7 +883,7 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
       R pk = 0, ek = 0;
       if (s <= ch && k >= 0 && k < nz) {
         const int kk = L.at1(k);
-        const size_t c = c0 + (size_t)k * pl;
+        const int c = c0 + k * pl;
         R Kt = a.co.kt3[c];
         R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * mcx +
                (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * mcy;
@@ -858,14 +902,14 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
     for (int s = 1; s < KCH + 1; ++s) {
       const int k = klo - 1 + s;
       if (s <= ch && k < nz) {
-        const size_t c = c0 + (size_t)k * pl;
+        const int c = c0 + k * pl;
         th[s] = a.th_in[c];
         tt[s] = a.tth[c];
         db[s] = a.b.dthbdz[c];
       }
       if (s <= ch && k >= 1 && k < nz) {
         const int kk = L.at1(k);
-        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const int c = c0 + k * pl, cm = c - pl;
         const R iJdz = invJ * a.co.inv_dzw[kk];
         R thc = th[s], thm = a.th_in[cm];
         R thbw = a.b.thbw[c];
@@ -935,7 +979,7 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_column_chunked(AcouArgs<R>
     for (int s = 1; s < KCH + 1; ++s) {
       const int k = klo - 1 + s;
       if (s > ch || k > nz) continue;
-      const size_t c = c0 + (size_t)k * pl;
+      const int c = c0 + k * pl;
       if (k < nz) {
         R wn = SQ(sW, k), wn1 = SQ(sW, k + 1);
         a.pi_next[c] = P[s] - E[s] * (av[s + 1] * wn1 - av[s] * wn);
@@ -972,13 +1016,13 @@ __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_co
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
+  const int c2d = L.at2i(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   const R invJ = (R)1 / J;
   const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
   const bool terrain = hxc != (R)0 || hyc != (R)0;
-  const size_t sx = 1, sy = L.px, pl = L.plane();
-  const size_t c0 = L.at(active ? i : 0, j, 0);
+  const int sx = 1, sy = L.px, pl = L.planei();
+  const int c0 = L.ati(active ? i : 0, j, 0);
   const R* __restrict__ u = a.u_out;
   const R* __restrict__ v = a.v_out;
   const int klo = lane * KCH;
@@ -994,7 +1038,7 @@ __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_co
       const int k = klo - 1 + q;
       R avk = 0, svk = 0;
       if (k >= 1 && k < nz) {
-        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const int c = c0 + k * pl, cm = c - pl;
         avk = a.co.aw[c];
         if (terrain) {
           R uw = (R)0.25 * (u[cm] + u[cm + sx] + u[c] + u[c + sx]);
@@ -1012,7 +1056,7 @@ __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_co
       R pk = 0, ek = 0;
       if (k >= 0 && k < nz) {
         const int kk = L.at1(k);
-        const size_t c = c0 + (size_t)k * pl;
+        const int c = c0 + k * pl;
         R Kt = a.co.kt3[c];
         R Dh = (a.co.rtjx[c + sx] * u[c + sx] - a.co.rtjx[c] * u[c]) * mcx +
                (a.co.rtjy[c + sy] * v[c + sy] - a.co.rtjy[c] * v[c]) * mcy;
@@ -1032,14 +1076,14 @@ __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_co
       const int k = klo - 1 + q;
       th[q] = tt[q] = db[q] = 0;
       if (k < nz) {
-        const size_t c = c0 + (size_t)k * pl;
+        const int c = c0 + k * pl;
         th[q] = a.th_in[c];
         tt[q] = a.tth[c];
         db[q] = a.b.dthbdz[c];
       }
       if (k >= 1 && k < nz) {
         const int kk = L.at1(k);
-        const size_t c = c0 + (size_t)k * pl, cm = c - pl;
+        const int c = c0 + k * pl, cm = c - pl;
         const R iJdz = invJ * a.co.inv_dzw[kk];
         R thc = th[q], thm = a.th_in[cm];
         R thbw = a.b.thbw[c];
@@ -1086,7 +1130,7 @@ __global__ void __launch_bounds__(CX * KL, sizeof(R) == 4 ? 2 : 1) k_acoustic_co
     for (int q = 1; q < KCH + 1; ++q) {
       const int k = klo - 1 + q;
       if (k > nz) continue;
-      const size_t c = c0 + (size_t)k * pl;
+      const int c = c0 + k * pl;
       if (k == nz) {
         a.w_out[c] = 0;
         continue;
@@ -1125,7 +1169,7 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_fused(AcouArgs<R> a) {
       if (i <= L.nx) {
         const R val = u_face(a, i, j, k);
         us[e] = val;
-        if (f < CX || i == L.nx) a.u_out[L.at(i, j, k)] = val;
+        if (f < CX || i == L.nx) a.u_out[L.ati(i, j, k)] = val;
       }
     } else {
       const int e2 = e - nu, col = e2 % CX, row = (e2 / CX) & 1, k = e2 / (2 * CX);
@@ -1133,7 +1177,7 @@ __global__ void __launch_bounds__(CX * KL) k_acoustic_fused(AcouArgs<R> a) {
       if (i < L.nx) {
         const R val = v_face(a, i, jj, k);
         vs[e2] = val;
-        if (row == 0 || jj == L.ny) a.v_out[L.at(i, jj, k)] = val;
+        if (row == 0 || jj == L.ny) a.v_out[L.ati(i, jj, k)] = val;
       }
     }
   }
@@ -1234,7 +1278,7 @@ __global__ void __launch_bounds__(kTmaCX * kTmaKL)
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
-  const size_t c2d = L.at2(active ? i : 0, j);
+  const int c2d = L.at2i(active ? i : 0, j);
   const R J = a.m.jac[c2d], hxc = a.m.hx[c2d], hyc = a.m.hy[c2d], mc = a.m.mapf[c2d];
   const R invJ = (R)1 / J;
   const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
@@ -1339,9 +1383,9 @@ __global__ void __launch_bounds__(kTmaCX * kTmaKL)
   __syncthreads();
   // phase 5: pi', theta', w (kernels.cu:636-644)
   if (active) {
-    const size_t c0 = L.at(i, j, 0), pl = L.plane();
+    const int c0 = L.ati(i, j, 0), pl = L.planei();
     for (int k = lane_k; k <= nz; k += kTmaKL) {
-      const size_t c = c0 + (size_t)k * pl;
+      const int c = c0 + k * pl;
       if (k < nz) {
         R wn = SM(Wn, k), wn1 = SM(Wn, k + 1);
         a.pi_next[c] = SM(P, k) - SM(E, k) * (SM(Av, k + 1) * wn1 - SM(Av, k) * wn);

@@ -47,7 +47,8 @@ __host__ __device__ inline void pipe_box(int cx, int f, int nz, int* bx, int* by
   *bz = f == TC_W ? nz + 1 : nz;
 }
 
-__host__ __device__ inline bool pipe_loaded(int f, bool moist, bool tpi) {
+__host__ __device__ inline bool pipe_loaded(int f, bool moist, bool tpi, bool prof = false) {
+  if (prof && pipe_prof_slot(f) >= 0) return false;
   if (f == TC_TPI) return tpi;
   if (f >= TC_QV) return moist;
   return true;
@@ -61,12 +62,12 @@ struct PipeLayout {
   size_t field[TC_N];
   size_t stage0, stage_bytes, work, total;
   uint32_t tx_bytes;
-  __host__ __device__ PipeLayout(int cx, int nz, int nst, bool moist, bool tpi) {
+  __host__ __device__ PipeLayout(int cx, int nz, int nst, bool moist, bool tpi, bool prof = false) {
     size_t o = 0;
     tx_bytes = 0;
     for (int f = 0; f < TC_N; ++f) {
       field[f] = 0;
-      if (!pipe_loaded(f, moist, tpi)) continue;
+      if (!pipe_loaded(f, moist, tpi, prof)) continue;
       int bx, by, bz;
       pipe_box(cx, f, nz, &bx, &by, &bz);
       const size_t b = (size_t)bx * by * bz * sizeof(R);
@@ -86,7 +87,7 @@ struct PipeLayout {
 // then stream the tile's boxes into the stage with bulk tensor loads (no
 // multicast: the maps cover this GPU's own fields only).  Every wait is
 // bounded; on a timeout it sets *err and stops issuing.
-template <typename R, int CX, int NST>
+template <typename R, int CX, int NST, bool PROF = false>
 __device__ __forceinline__ void pipe_produce(const PipeColParams<R>& p, const PipeLayout<R>& lay,
                                              unsigned char* smem_pipe, uint64_t* full, uint64_t* empty,
                                              int ntx, int ntiles) {
@@ -106,7 +107,8 @@ __device__ __forceinline__ void pipe_produce(const PipeColParams<R>& p, const Pi
     unsigned char* stg = smem_pipe + lay.stage0 + (size_t)s * lay.stage_bytes;
     const int x = (t % ntx) * CX + kOX, y = t / ntx + kOY, z = kOZ;
     for (int f = 0; f < TC_N; ++f)
-      if (pipe_loaded(f, moist, has_tpi)) tma::load_3d(stg + lay.field[f], &p.map[f], x, y, z, &full[s]);
+      if (pipe_loaded(f, moist, has_tpi, PROF))
+        tma::load_3d(stg + lay.field[f], &p.map[f], x, y, z, &full[s]);
   }
   // loads this CTA armed must land before it exits (they have, unless the
   // consumers gave up early)
@@ -357,7 +359,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
 // it, so the next tile's boxes land while this tile is solved, and no lane
 // waits for a serial sweep.  Every expression is the parallel-solve kernel's
 // on the same values (from shared memory instead of global memory).
-template <typename R, int CX, int KL, int KCH, int NST>
+template <typename R, int CX, int KL, int KCH, int NST, bool PROF>
 __global__ void __launch_bounds__(CX * KL + 32)
     k_acoustic_column_pipe_pcr(const __grid_constant__ PipeColParams<R> p) {
   extern __shared__ __align__(128) unsigned char smem_pipe[];
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
   const int nz = L.nz;
   const bool moist = a.p.moisture != 0;
   const bool has_tpi = p.has_tpi != 0;
-  const PipeLayout<R> lay(CX, nz, NST, moist, has_tpi);
+  const PipeLayout<R> lay(CX, nz, NST, moist, has_tpi, PROF);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_pipe);
   uint64_t* empty = full + NST;
   const int tid = threadIdx.x;
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
   }
   __syncthreads();
   if (tid >= NC) {
-    if (tid == NC) pipe_produce<R, CX, NST>(p, lay, smem_pipe, full, empty, ntx, ntiles);
+    if (tid == NC) pipe_produce<R, CX, NST, PROF>(p, lay, smem_pipe, full, empty, ntx, ntiles);
     return;
   }
 
@@ -393,15 +395,19 @@ __global__ void __launch_bounds__(CX * KL + 32)
   const int tx = tid % CX, lane = tid / CX;
   R* work = reinterpret_cast<R*>(smem_pipe + lay.work);
   // the per-level tables every tile reads, once per CTA: 1/dzc, 1/dzw and the
-  // terrain factor of the w levels, at level k
+  // terrain factor of the w levels, at level k, and (PROF) the coefficient
+  // fields' level values
   R* lvl_idzc = work + kPcrWork * NC;
   R* lvl_idzw = lvl_idzc + (nz + 1);
   R* lvl_facw = lvl_idzw + (nz + 1);
+  R* lvl_prof = lvl_facw + (nz + 1);
   for (int k = tid; k <= nz; k += NC) {
     lvl_idzc[k] = a.co.inv_dzc[L.at1(k)];
     lvl_idzw[k] = a.co.inv_dzw[L.at1(k)];
     lvl_facw[k] = a.co.fac_w[L.at1(k)];
   }
+  if (PROF)
+    for (int q = tid; q < PF_N * (nz + 1); q += NC) lvl_prof[q] = p.prof[q];
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
@@ -443,10 +449,11 @@ __global__ void __launch_bounds__(CX * KL + 32)
     const R* sQR = fld(TC_QR);
     const R* sQVB = fld(TC_QVB);
 #define UF(k, d) sU[(k) * (CX + 4) + tx + (d)]
-#define RXF(k, d) sRX[(k) * (CX + 4) + tx + (d)]
+#define RXF(k, d) (PROF ? lvl_prof[PF_RTJX * (nz + 1) + (k)] : sRX[(k) * (CX + 4) + tx + (d)])
 #define VF(k, r) sV[((k) * 2 + (r)) * CX + tx]
-#define RYF(k, r) sRY[((k) * 2 + (r)) * CX + tx]
+#define RYF(k, r) (PROF ? lvl_prof[PF_RTJY * (nz + 1) + (k)] : sRY[((k) * 2 + (r)) * CX + tx])
 #define CF(X, k) X[(k) * CX + tx]
+#define PF(X, q, k) (PROF ? lvl_prof[(q) * (nz + 1) + (k)] : CF(X, k))
     const R invJ = (R)1 / J;
     const R mcx = mc * a.co.inv_dx, mcy = mc * a.co.inv_dy;
     const bool terrain = hxc != (R)0 || hyc != (R)0;
@@ -462,7 +469,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
         const int k = klo - 1 + q;
         R avk = 0, svk = 0;
         if (k >= 1 && k < nz) {
-          avk = CF(sAW, k);
+          avk = PF(sAW, PF_AW, k);
           if (terrain) {
             R uw = (R)0.25 * (UF(k - 1, 0) + UF(k - 1, 1) + UF(k, 0) + UF(k, 1));
             R vw = (R)0.25 * (VF(k - 1, 0) + VF(k - 1, 1) + VF(k, 0) + VF(k, 1));
@@ -478,7 +485,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
         const int k = klo - 1 + q;
         R pk = 0, ek = 0;
         if (k >= 0 && k < nz) {
-          R Kt = CF(sKT, k);
+          R Kt = PF(sKT, PF_KT3, k);
           R Dh = (RXF(k, 1) * UF(k, 1) - RXF(k, 0) * UF(k, 0)) * mcx +
                  (RYF(k, 1) * VF(k, 1) - RYF(k, 0) * VF(k, 0)) * mcy;
           R idz = lvl_idzc[k];
@@ -499,12 +506,12 @@ __global__ void __launch_bounds__(CX * KL + 32)
         if (k < nz) {
           th[q] = CF(sTH, k);
           tt[q] = CF(sTTH, k);
-          db[q] = CF(sDTHB, k);
+          db[q] = PF(sDTHB, PF_DTHB, k);
         }
         if (k >= 1 && k < nz) {
           const R iJdz = invJ * lvl_idzw[k];
           R thc = th[q], thm = CF(sTH, k - 1);
-          R thbw = CF(sTHBW, k);
+          R thbw = PF(sTHBW, PF_THBW, k);
           R thvw = thbw + (R)0.5 * (thm + thc);
           if (moist) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k));
           R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
@@ -514,7 +521,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
           Cr[q] = -G * Ek * av[q + 1];
           R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
           if (moist) {
-            R dqv = (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k)) - (R)0.5 * (CF(sQVB, k - 1) + CF(sQVB, k));
+            R dqv = (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k)) - (R)0.5 * (PF(sQVB, PF_QVB, k - 1) + PF(sQVB, PF_QVB, k));
             R qcr = (R)0.5 * (CF(sQC, k - 1) + CF(sQC, k)) + (R)0.5 * (CF(sQR, k - 1) + CF(sQR, k));
             buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
           }
@@ -534,6 +541,7 @@ __global__ void __launch_bounds__(CX * KL + 32)
 #undef VF
 #undef RYF
 #undef CF
+#undef PF
     // every input of this tile is in registers: the producer may refill the
     // stage (the barrier also ends the previous tile's use of the work area)
     csync();
@@ -573,19 +581,34 @@ __global__ void __launch_bounds__(CX * KL + 32)
 constexpr PipeShape kPipePcrShapes[] = {{16, 16, 3, 2}, {8, 16, 3, 2}, {8, 16, 3, 3}, {16, 14, 3, 2}};
 constexpr int kNumPipePcrShapes = 4;
 
-template <typename R, int F>
+template <typename R, int F, bool PROF>
 struct PipePcrKernel {
   static constexpr PipeShape S = kPipePcrShapes[F];
-  static constexpr auto fn = k_acoustic_column_pipe_pcr<R, S.cx, S.kl, S.kch, S.nst>;
+  static constexpr auto fn = k_acoustic_column_pipe_pcr<R, S.cx, S.kl, S.kch, S.nst, PROF>;
 };
 
-template <typename R>
+template <typename R, bool PROF>
 const void* pipe_pcr_fn(int f) {
   switch (f) {
-    case 0: return reinterpret_cast<const void*>(PipePcrKernel<R, 0>::fn);
-    case 1: return reinterpret_cast<const void*>(PipePcrKernel<R, 1>::fn);
-    case 2: return reinterpret_cast<const void*>(PipePcrKernel<R, 2>::fn);
-    default: return reinterpret_cast<const void*>(PipePcrKernel<R, 3>::fn);
+    case 0: return reinterpret_cast<const void*>(PipePcrKernel<R, 0, PROF>::fn);
+    case 1: return reinterpret_cast<const void*>(PipePcrKernel<R, 1, PROF>::fn);
+    case 2: return reinterpret_cast<const void*>(PipePcrKernel<R, 2, PROF>::fn);
+    default: return reinterpret_cast<const void*>(PipePcrKernel<R, 3, PROF>::fn);
+  }
+}
+
+template <typename R>
+const void* pipe_pcr_fn(int f, bool prof) {
+  return prof ? pipe_pcr_fn<R, true>(f) : pipe_pcr_fn<R, false>(f);
+}
+
+template <typename R, bool PROF>
+void launch_pipe_pcr(int f, int grid, int threads, size_t sm, cudaStream_t st, const PipeColParams<R>& p) {
+  switch (f) {
+    case 0: PipePcrKernel<R, 0, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
+    case 1: PipePcrKernel<R, 1, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
+    case 2: PipePcrKernel<R, 2, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
+    default: PipePcrKernel<R, 3, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
   }
 }
 
@@ -639,29 +662,32 @@ size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi) {
 }
 
 template <typename R>
-size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi) {
+size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi, bool prof) {
   if (shape < 0 || shape >= kNumPipePcrShapes) return 0;
   const PipeShape& S = kPipePcrShapes[shape];
   if (nz + 1 > S.kl * S.kch || nz + 1 > 256) return 0;  // rows; a box extent is <= 256
-  const size_t t = PipeLayout<R>(S.cx, nz, S.nst, moist, tpi).work +
-                   ((size_t)kPcrWork * S.kl * S.cx + 3 * (size_t)(nz + 1)) * sizeof(R);
+  const size_t tables = (size_t)(3 + (prof ? PF_N : 0)) * (nz + 1);
+  const size_t t = PipeLayout<R>(S.cx, nz, S.nst, moist, tpi, prof).work +
+                   ((size_t)kPcrWork * S.kl * S.cx + tables) * sizeof(R);
   return t <= 227 * 1024 ? t : 0;
 }
 
 template <typename R>
 int prepare_acoustic_pipe(int nz) {
   bool any = false;
-  for (int pcr = 0; pcr < 2; ++pcr)
-    for (int f = 0; f < (pcr ? kNumPipePcrShapes : kNumPipeShapes); ++f) {
+  // kinds: the Thomas pipeline, the parallel-solve pipeline with boxes for
+  // every field, and with the level tables
+  for (int kind = 0; kind < 3; ++kind)
+    for (int f = 0; f < (kind ? kNumPipePcrShapes : kNumPipeShapes); ++f) {
       size_t sm = 0;
       for (int moist = 0; moist < 2; ++moist)
         for (int tpi = 0; tpi < 2; ++tpi) {
-          const size_t t = pcr ? acoustic_pipe_pcr_smem<R>(f, nz, moist != 0, tpi != 0)
-                               : acoustic_pipe_smem<R>(f, nz, moist != 0, tpi != 0);
+          const size_t t = kind ? acoustic_pipe_pcr_smem<R>(f, nz, moist != 0, tpi != 0, kind == 2)
+                                : acoustic_pipe_smem<R>(f, nz, moist != 0, tpi != 0);
           if (t > sm) sm = t;
         }
       if (!sm) continue;
-      if (raise_smem_limit(pcr ? pipe_pcr_fn<R>(f) : pipe_fn<R>(f), sm) != cudaSuccess) return 1;
+      if (raise_smem_limit(kind ? pipe_pcr_fn<R>(f, kind == 2) : pipe_fn<R>(f), sm) != cudaSuccess) return 1;
       any = true;
     }
   return any ? 0 : 2;
@@ -675,20 +701,17 @@ void acoustic_pipe_pcr_box(int shape, int f, int nz, int* bx, int* by, int* bz) 
 
 template <typename R>
 int launch_acoustic_column_pipe_pcr(const PipeColParams<R>& p, int f, cudaStream_t st) {
-  const size_t sm = acoustic_pipe_pcr_smem<R>(f, p.a.L.nz, p.a.p.moisture != 0, p.has_tpi != 0);
+  const bool prof = p.prof != nullptr;
+  const size_t sm = acoustic_pipe_pcr_smem<R>(f, p.a.L.nz, p.a.p.moisture != 0, p.has_tpi != 0, prof);
   if (!sm) return 2;
   const PipeShape& S = kPipePcrShapes[f];
   const int ntiles = (p.a.L.nx + S.cx - 1) / S.cx * p.a.L.ny;
   const int threads = S.cx * S.kl + 32;
-  const int lim = pipe_grid_limit(pipe_pcr_fn<R>(f), threads, sm);
+  const int lim = pipe_grid_limit(pipe_pcr_fn<R>(f, prof), threads, sm);
   if (lim <= 0) return 2;
   const int grid = ntiles < lim ? ntiles : lim;
-  switch (f) {
-    case 0: PipePcrKernel<R, 0>::fn<<<grid, threads, sm, st>>>(p); break;
-    case 1: PipePcrKernel<R, 1>::fn<<<grid, threads, sm, st>>>(p); break;
-    case 2: PipePcrKernel<R, 2>::fn<<<grid, threads, sm, st>>>(p); break;
-    default: PipePcrKernel<R, 3>::fn<<<grid, threads, sm, st>>>(p); break;
-  }
+  if (prof) launch_pipe_pcr<R, true>(f, grid, threads, sm, st, p);
+  else launch_pipe_pcr<R, false>(f, grid, threads, sm, st, p);
   return 0;
 }
 
@@ -712,7 +735,7 @@ int launch_acoustic_column_pipe(const PipeColParams<R>& p, int f, cudaStream_t s
 
 #define WFE_INST(R)                                                              \
   template size_t acoustic_pipe_smem<R>(int, int, bool, bool);                   \
-  template size_t acoustic_pipe_pcr_smem<R>(int, int, bool, bool);               \
+  template size_t acoustic_pipe_pcr_smem<R>(int, int, bool, bool, bool);         \
   template int prepare_acoustic_pipe<R>(int);                                    \
   template int launch_acoustic_column_pipe<R>(const PipeColParams<R>&, int, cudaStream_t); \
   template int launch_acoustic_column_pipe_pcr<R>(const PipeColParams<R>&, int, cudaStream_t);

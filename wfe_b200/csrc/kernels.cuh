@@ -360,11 +360,29 @@ struct TmaColParams {
 // consumer warps run the column phases of the tile before; the same
 // expressions as the chunked kernel, bit for bit.  Maps are encoded with the
 // boxes of acoustic_pipe_box for the chosen shape.
+// The column inputs that depend on the level alone when the base state and
+// the metric are horizontally uniform (flat ground, one map factor): the
+// parallel-solve pipeline then reads them from per-level tables, in this
+// order, instead of streaming a box of each per tile.
+enum { PF_RTJX = 0, PF_RTJY, PF_AW, PF_KT3, PF_THBW, PF_DTHB, PF_QVB, PF_N };
+WFE_HD int pipe_prof_slot(int f) {
+  switch (f) {
+    case TC_RTJX: return PF_RTJX;
+    case TC_RTJY: return PF_RTJY;
+    case TC_AW: return PF_AW;
+    case TC_KT3: return PF_KT3;
+    case TC_THBW: return PF_THBW;
+    case TC_DTHB: return PF_DTHB;
+    case TC_QVB: return PF_QVB;
+    default: return -1;
+  }
+}
 template <typename R>
 struct PipeColParams {
   AcouArgs<R> a;
   unsigned* err;   // set to 1 when a stage wait gave up
   int has_tpi;     // TC_TPI map valid
+  const R* prof;   // PF_N tables of nz + 1 levels, or null (boxes for all)
   CUtensorMap map[TC_N];
 };
 int acoustic_pipe_shapes();
@@ -387,7 +405,7 @@ int launch_acoustic_column_pipe(const PipeColParams<R>& p, int shape, cudaStream
 int acoustic_pipe_pcr_shapes();
 void acoustic_pipe_pcr_box(int shape, int f, int nz, int* bx, int* by, int* bz);
 template <typename R>
-size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi);
+size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi, bool prof = false);
 template <typename R>
 int launch_acoustic_column_pipe_pcr(const PipeColParams<R>& p, int shape, cudaStream_t st);
 // Persistent, pipelined forward u, v kernel (dyn_acou_pipe.cu): tiles of

@@ -236,6 +236,7 @@ class ModelT final : public Model {
                      lb + n1,    lb + 2 * n1, lb + 3 * n1, lb + 4 * n1, lb + 5 * n1,
                      lb + 6 * n1, (R)(1.0 / g_.dx), (R)(1.0 / g_.dy)};
     }
+    if (level_tables()) return 1;
     if (!(rain_ = alloc(n2))) return 1;
     CK(cudaMalloc(&clock_, CLK_N * sizeof(double)));
     CK(cudaMemset(clock_, 0, CLK_N * sizeof(double)));
@@ -808,7 +809,8 @@ class ModelT final : public Model {
   }
   bool pipe_pcr_usable(int v) const {
     const int f = pipe_pcr_index(v);
-    return pipe_ok_ && f >= 0 && acoustic_pipe_pcr_smem<R>(f, g_.nz, dp_.moisture != 0, bdy_on_) > 0;
+    return pipe_ok_ && f >= 0 &&
+           acoustic_pipe_pcr_smem<R>(f, g_.nz, dp_.moisture != 0, bdy_on_, lvl_tab_ != nullptr) > 0;
   }
   bool pipe_usable(int v) const {
     const int f = pipe_index(v);
@@ -1204,7 +1206,7 @@ class ModelT final : public Model {
           launch("acoustic_column", [&] { rc = launch_acoustic_column_pcr<R>(a, f, st_); });
         } else if (pipe_pcr_usable(tune_.column_cx) &&
                    acoustic_pipe_pcr_smem<R>(pipe_pcr_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
-                                             a.tpi != nullptr) > 0) {
+                                             a.tpi != nullptr, lvl_tab_ != nullptr) > 0) {
           const int f = pipe_pcr_index(tune_.column_cx);
           PipeColParams<R> pp;
           if (pipe_params(a, f, &pp, true)) return 1;
@@ -1345,12 +1347,14 @@ class ModelT final : public Model {
     pp->a = a;
     pp->err = tma_err_;
     pp->has_tpi = a.tpi != nullptr;
+    pp->prof = pcr ? lvl_tab_ : nullptr;
     const R* src[TC_N] = {a.u_out,  a.co.rtjx, a.v_out, a.co.rtjy, a.w_in,   a.pi_cur,
                           a.th_in,  a.tw,      a.tth,   a.tpi,     a.co.aw,  a.co.kt3,
                           a.b.thbw, a.b.dthbdz, a.qv,   a.qc,      a.qr,     a.b.qvb};
     for (int f = 0; f < TC_N; ++f) {
       if (f == TC_TPI && !a.tpi) continue;
       if (f >= TC_QV && !a.p.moisture) continue;
+      if (pp->prof && pipe_prof_slot(f) >= 0) continue;
       int bx, by, bz;
       if (pcr)
         acoustic_pipe_pcr_box(shape, f, g_.nz, &bx, &by, &bz);
@@ -1443,6 +1447,37 @@ class ModelT final : public Model {
   }
 
   // --------------------------------------------------------------- memory
+  // When every column of the run-constant column coefficients (the
+  // reference's rtjx, rtjy, aw, kt3, theta_b^w, dtheta_b/dz, qv_b) holds the
+  // same values level by level -- flat ground and a uniform map factor --
+  // the pipelined parallel-solve column reads them from per-level tables
+  // (the values of column (0, 0)) instead of streaming a box of each per
+  // tile: the same values, bit for bit.  Checked over the points the column
+  // kernel reads; WFE_COLUMN_PROFILES=0 keeps the boxes.
+  int level_tables() {
+    const char* e = std::getenv("WFE_COLUMN_PROFILES");
+    if (e && e[0] == '0') return 0;
+    const int nx = g_.nx, ny = g_.ny, nz = g_.nz, n1 = nz + 1;
+    const R* src[PF_N] = {rtjx_, rtjy_, aw_, kt3_, db_.thbw, db_.dthbdz, db_.qvb};
+    std::vector<R> host(L_.n3()), tab((size_t)PF_N * n1);
+    for (int q = 0; q < PF_N; ++q) {
+      if (q == PF_QVB && !dp_.moisture) continue;
+      CK(cudaMemcpy(host.data(), src[q], L_.n3() * sizeof(R), cudaMemcpyDeviceToHost));
+      const int ilast = q == PF_RTJX ? nx : nx - 1, jlast = q == PF_RTJY ? ny : ny - 1;
+      for (int k = 0; k < n1; ++k) {
+        const R v = host[L_.at(0, 0, k)];
+        tab[(size_t)q * n1 + k] = v;
+        if (k == nz) continue;  // the kernel reads levels 0 .. nz-1
+        for (int j = 0; j <= jlast; ++j)
+          for (int i = 0; i <= ilast; ++i)
+            if (std::memcmp(&host[L_.at(i, j, k)], &v, sizeof(R)) != 0) return 0;
+      }
+    }
+    if (!(lvl_tab_ = alloc(tab.size()))) return 1;
+    CK(cudaMemcpy(lvl_tab_, tab.data(), tab.size() * sizeof(R), cudaMemcpyHostToDevice));
+    return 0;
+  }
+
   R* alloc(size_t n) {
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, n * sizeof(R));
@@ -1610,6 +1645,7 @@ class ModelT final : public Model {
   bool pipe_ok_ = false;             // pipelined column kernels prepared
   bool uvp_ok_ = false;              // pipelined u, v kernel prepared
   bool tend_tma_ok_ = false;         // TMA-staged scalar tendencies usable
+  R* lvl_tab_ = nullptr;             // the column coefficients' level tables (PF_*), or null
   unsigned* tma_err_ = nullptr;      // set by a TMA tile load that timed out
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps_;
   cudaStream_t cs_st_ = nullptr;     // snapshot copy stream

@@ -394,13 +394,13 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
   const bool active = i < L.nx && j < L.ny;
   using P = Phys<R>;
   const R KAPPA = (R)0.4, SIGMA = (R)5.67e-8, S0 = (R)1361, KM_MAX = (R)1000, KM_MIN = (R)0.1;
-  const size_t n1 = (size_t)(nz + 1) * kSfcCX;
-  auto X = [&](int q, int k) -> R& { return sm[(size_t)q * n1 + (size_t)k * kSfcCX + tx]; };
-  R* scal = sm + (size_t)SS_N * n1;
+  const int n1 = (nz + 1) * kSfcCX;
+  auto X = [&](int q, int k) -> R& { return sm[q * n1 + k * kSfcCX + tx]; };
+  R* scal = sm + SS_N * n1;
   auto S = [&](int q) -> R& { return scal[q * kSfcCX + tx]; };
   enum { SC_SHF, SC_QFLX, SC_HPBL, SC_WS, SC_GTH, SC_GQV, SC_POS, SC_RHO0 };
-  const size_t c2 = L.at2(active ? i : 0, j);
-  const size_t n2 = L.n2();
+  const int c2 = L.at2i(active ? i : 0, j);
+  const int n2 = L.planei();
   const R J = a.m.jac[c2];
   double tend_s = a.clock[CLK_T] + a.clock[CLK_DT];  // end of the step
   R utc = (R)(a.start_hour + tend_s / 3600.0);
@@ -414,11 +414,11 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
   if (cosz < (R)0) cosz = 0;
   const R mu = fmax(cosz, (R)0.05);
   auto ucen = [&](int k) {
-    const size_t c = L.at(i, j, k);
+    const int c = L.ati(i, j, k);
     return (R)0.5 * (a.u[c] + a.u[c + 1]);
   };
   auto vcen = [&](int k) {
-    const size_t c = L.at(i, j, k);
+    const int c = L.ati(i, j, k);
     return (R)0.5 * (a.v[c] + a.v[c + L.px]);
   };
   // ---- per level: the column, lwp terms, emissivity, temperature, the
@@ -426,7 +426,7 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
   if (active)
     for (int k = lane; k < nz; k += kSfcKL) {
       const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       const R rho = a.b.rhob[c];
       const R dzc = a.m.dzeta_c[kk] * J;
       const R th = a.b.thb[c] + a.thp[c];
@@ -483,7 +483,7 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
     } else {
       beta = (R)1;
     }
-    const size_t c0 = L.at(i, j, 0);
+    const int c0 = L.ati(i, j, 0);
     const R rho0 = a.b.rhob[c0];
     const R dzc0 = a.m.dzeta_c[L.at1(0)] * J;
     R z1 = (R)0.5 * dzc0;
@@ -563,7 +563,7 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
       R Cso = (R)1.2e6 + (R)3.2e6 * fmin(fmax(w, (R)0), (R)0.4);
       R Kso = (R)0.25 + (R)3.0 * fmin(fmax(w, (R)0), (R)0.4);
       R Tso[4], A[4], B[4], C[4], D[4];
-      for (int l = 0; l < 4; ++l) Tso[l] = a.soilt[(size_t)l * n2 + c2];
+      for (int l = 0; l < 4; ++l) Tso[l] = a.soilt[l * n2 + c2];
       for (int l = 0; l < 4; ++l) {
         R cap = Cso * SOIL_DZ[l] / a.dt;
         R ku = (l > 0) ? Kso / ((R)0.5 * (SOIL_DZ[l - 1] + SOIL_DZ[l])) : (R)0;
@@ -585,7 +585,7 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
       for (int l = 0; l < 4; ++l) {
         if (Tso[l] < (R)200) Tso[l] = 200;
         if (Tso[l] > (R)350) Tso[l] = 350;
-        a.soilt[(size_t)l * n2 + c2] = Tso[l];
+        a.soilt[l * n2 + c2] = Tso[l];
       }
       a.tsk[c2] = Tso[0];
     }
@@ -643,7 +643,7 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
     const bool pos = S(SC_POS) > (R)0;
     for (int k = lane; k < nz; k += kSfcKL) {
       const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       const R rho = a.b.rhob[c];
       const R dzc = a.m.dzeta_c[kk] * J;
       R pik = a.b.pib[c] + a.pip[c];
@@ -686,9 +686,9 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
   if (active)
     for (int k = lane; k < nz; k += kSfcKL) {
       const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       R av = (k > 0) ? a.b.rhobw[c] * X(SS_KW, k) / (a.m.dzeta_w[kk] * J) : (R)0;
-      R cv = (k < nz - 1) ? a.b.rhobw[c + L.plane()] * X(SS_KW, k + 1) / (a.m.dzeta_w[kk + 1] * J)
+      R cv = (k < nz - 1) ? a.b.rhobw[c + L.planei()] * X(SS_KW, k + 1) / (a.m.dzeta_w[kk + 1] * J)
                           : (R)0;
       R m = a.b.rhob[c] * (a.m.dzeta_c[kk] * J) / a.dt;
       X(SA, k) = -av;
@@ -724,7 +724,7 @@ __device__ __forceinline__ void sfc_scalar_cols(const SfcArgs<R>& a, int bx, int
   __syncthreads();
   if (active)
     for (int k = lane; k < nz; k += kSfcKL) {
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       R dth = a.dt * X(SS_RAD, k);
       if (dth > (R)0.02) dth = (R)0.02;
       if (dth < (R)-0.02) dth = (R)-0.02;
@@ -747,23 +747,23 @@ __device__ __forceinline__ void sfc_momentum_cols(const SfcArgs<R>& a, int bx, i
   const bool active = i < L.nx && j < L.ny;
   const int di = on_v ? 0 : 1, dj = on_v ? 1 : 0;
   R* f = on_v ? a.v : a.u;
-  const size_t n1 = (size_t)(nz + 1) * kSfcCX;
-  auto X = [&](int q, int k) -> R& { return sm[(size_t)q * n1 + (size_t)k * kSfcCX + tx]; };
-  const R J = active ? (R)0.5 * (a.m.jac[L.at2(i - di, j - dj)] + a.m.jac[L.at2(i, j)]) : (R)1;
+  const int n1 = (nz + 1) * kSfcCX;
+  auto X = [&](int q, int k) -> R& { return sm[q * n1 + k * kSfcCX + tx]; };
+  const R J = active ? (R)0.5 * (a.m.jac[L.at2i(i - di, j - dj)] + a.m.jac[L.at2i(i, j)]) : (R)1;
   auto Kw = [&](int k) {
-    return (R)0.5 * (a.km[L.at(i - di, j - dj, k)] + a.km[L.at(i, j, k)]);
+    return (R)0.5 * (a.km[L.ati(i - di, j - dj, k)] + a.km[L.ati(i, j, k)]);
   };
   if (active)
     for (int k = lane; k < nz; k += kSfcKL) {
       const int kk = L.at1(k);
-      const size_t c = L.at(i, j, k), cb = L.at(i - di, j - dj, k);
+      const int c = L.ati(i, j, k), cb = L.ati(i - di, j - dj, k);
       R av = 0, cv = 0;
       if (k > 0) {
         R rhow = (R)0.5 * (a.b.rhobw[cb] + a.b.rhobw[c]);
         av = rhow * Kw(k) / (a.m.dzeta_w[kk] * J);
       }
       if (k < nz - 1) {
-        const size_t pl = L.plane();
+        const int pl = L.planei();
         R rhow = (R)0.5 * (a.b.rhobw[cb + pl] + a.b.rhobw[c + pl]);
         cv = rhow * Kw(k + 1) / (a.m.dzeta_w[kk + 1] * J);
       }
@@ -776,8 +776,8 @@ __device__ __forceinline__ void sfc_momentum_cols(const SfcArgs<R>& a, int bx, i
     }
   __syncthreads();
   if (active && lane == 0) {
-    const size_t c0 = L.at(i, j, 0), cb0 = L.at(i - di, j - dj, 0);
-    R cdva = (R)0.5 * (a.cdv[L.at2(i - di, j - dj)] + a.cdv[L.at2(i, j)]);
+    const int c0 = L.ati(i, j, 0), cb0 = L.ati(i - di, j - dj, 0);
+    R cdva = (R)0.5 * (a.cdv[L.at2i(i - di, j - dj)] + a.cdv[L.at2i(i, j)]);
     R rho0 = (R)0.5 * (a.b.rhob[cb0] + a.b.rhob[c0]);
     X(SSM_D, 0) += -rho0 * cdva * f[c0];
     for (int k = 1; k < nz; ++k) {
@@ -794,7 +794,7 @@ __device__ __forceinline__ void sfc_momentum_cols(const SfcArgs<R>& a, int bx, i
   }
   __syncthreads();
   if (active)
-    for (int k = lane; k < nz; k += kSfcKL) f[L.at(i, j, k)] = X(SSM_PHI, k);
+    for (int k = lane; k < nz; k += kSfcKL) f[L.ati(i, j, k)] = X(SSM_PHI, k);
 }
 
 template <typename R>
