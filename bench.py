@@ -119,6 +119,12 @@ DRY_KERNEL_FIELDS = dict(KERNEL_FIELDS, acoustic_column=16, acoustic_uv=10, tend
 # dry: 3 x 10 + 10 x 22.
 STEP_FIELDS = 3 * 19 + 10 * 26 + 12
 DRY_STEP_FIELDS = 3 * 10 + 10 * 22
+# With the column coefficients in per-level tables (a horizontally uniform
+# set-up and a pipelined column kernel, variants 13-15 and 19-22) a column
+# launch reads none of theta_b^w, dtheta_b/dz, rtjx, rtjy, kt3, aw, qv_b per
+# cell: 7 fields fewer (6 dry).
+TABLE_FIELDS, DRY_TABLE_FIELDS = 7, 6
+PIPE_VARIANTS = set(range(13, 16)) | set(range(19, 23))
 
 
 def use_workload(name: str) -> None:
@@ -711,16 +717,23 @@ def main():
     moist = WORKLOADS[WORKLOAD][2]
     kf = KERNEL_FIELDS if moist else DRY_KERNEL_FIELDS
     step_fields = STEP_FIELDS if moist else DRY_STEP_FIELDS
+    variants = c.variants()
+    tables = variants["level_tables"] and variants["column"] in PIPE_VARIANTS
+    if tables:
+        tab = TABLE_FIELDS if moist else DRY_TABLE_FIELDS
+        kf = dict(kf, acoustic_column=kf["acoustic_column"] - tab)
+        step_fields -= tab * kt.get("acoustic_column", (0.0, 0))[1]
     alg_bytes = kf.get(dom_name, 0) * 4 * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
     traffic = None
     tname = WORKLOADS[WORKLOAD][3]
     tf = ROOT / "profiles" / tname if tname else None
+    tkey = dom_name + ("_tables" if tables and dom_name == "acoustic_column" else "")
     if tf is not None and tf.exists():
         for ln in tf.read_text().splitlines():
             parts = ln.split()
-            if len(parts) == 2 and not ln.startswith("#") and parts[0] == dom_name:
+            if len(parts) == 2 and not ln.startswith("#") and parts[0] == tkey:
                 traffic = int(parts[1])
     c.close()
 
@@ -755,7 +768,8 @@ def main():
                        "timing": "CUDA events on the library stream around graph replays",
                        "column_solver": "the tuner's fastest column kernel, parallel tridiagonal "
                                         "solve allowed" if os.environ.get("WFE_EXACT_COLUMN") == "0"
-                                        else "Thomas sweep (bit-identical variants only)"},
+                                        else "Thomas sweep (bit-identical variants only)",
+                       "variants": variants},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "traffic": traffic,

@@ -53,7 +53,7 @@ SYMBOLS = [
     "wfe_case_create", "wfe_case_create_text", "wfe_ctx_destroy", "wfe_last_error",
     "wfe_get_dims", "wfe_get_spacing", "wfe_get_flags", "wfe_get_metric", "wfe_get_base",
     "wfe_field_upload", "wfe_field_download", "wfe_field2d_download", "wfe_step", "wfe_run",
-    "wfe_sync", "wfe_absmax", "wfe_absmax_begin", "wfe_absmax_end", "wfe_dry_mass", "wfe_launches_per_step", "wfe_op_apply_bcs",
+    "wfe_sync", "wfe_absmax", "wfe_absmax_begin", "wfe_absmax_end", "wfe_dry_mass", "wfe_launches_per_step", "wfe_case_variants", "wfe_op_apply_bcs",
     "wfe_op_tendencies", "wfe_op_acoustic", "wfe_op_moisture_stage", "wfe_op_kessler",
     "wfe_op_sfc", "wfe_set_boundary", "wfe_bdy_weights", "wfe_clear_boundary", "wfe_set_physics", "wfe_time_run", "wfe_kernel_times",
     "wfe_dry_mass_noalloc", "wfe_ensemble_create", "wfe_ensemble_destroy", "wfe_ensemble_run",
@@ -108,6 +108,7 @@ def load_library(path: str | Path | None = None):
     lib.wfe_dry_mass.argtypes = [vp, dp]
     lib.wfe_launches_per_step.argtypes = [vp]
     lib.wfe_launches_per_step.restype = C.c_long
+    lib.wfe_case_variants.argtypes = [vp, ip]
     lib.wfe_op_apply_bcs.argtypes = [vp]
     lib.wfe_op_tendencies.argtypes = [vp, C.c_double, C.c_double]
     lib.wfe_op_acoustic.argtypes = [vp, C.c_double, C.c_int]
@@ -327,6 +328,13 @@ class Case:
 
     def launches_per_step(self) -> int:
         return int(self._lib.wfe_launches_per_step(self._h))
+
+    def variants(self) -> dict:
+        """The tuned kernel variants (-1 before the first step) and whether the
+        column coefficients are read from per-level tables."""
+        out = (C.c_int * 4)()
+        self._check(self._lib.wfe_case_variants(self._h, out))
+        return {"tendencies": out[0], "column": out[1], "uv": out[2], "level_tables": out[3] == 1}
 
     # ------------------------------------------------------ operator API
     def apply_bcs(self) -> None:

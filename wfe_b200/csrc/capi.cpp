@@ -392,6 +392,12 @@ long wfe_launches_per_step(const wfe_ctx* c) {
   return c && c->model ? c->model->launches_per_step() : -1;
 }
 
+int wfe_case_variants(const wfe_ctx* c, int out[4]) {
+  if (!c || !c->model || !out) return WFE_ERR_ARG;
+  c->model->variants(out);
+  return WFE_OK;
+}
+
 int wfe_time_run(wfe_ctx* c, int nsteps, double dt, double t0, double* ms) {
   NEED_MODEL(c);
   if (!ms || nsteps < 0) return WFE_ERR_ARG;

@@ -116,7 +116,7 @@ __device__ __forceinline__ void pipe_produce(const PipeColParams<R>& p, const Pi
     if (armed[s] >= 0) tma::mbar_wait_for(&full[s], armed[s] & 1, kPipeWaitNs);
 }
 
-template <typename R, int CX, int KL, int KCH, int NST>
+template <typename R, int CX, int KL, int KCH, int NST, bool PROF>
 __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
     k_acoustic_column_pipe(const __grid_constant__ PipeColParams<R> p) {
   extern __shared__ __align__(128) unsigned char smem_pipe[];
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
   const int nz = L.nz;
   const bool moist = a.p.moisture != 0;
   const bool has_tpi = p.has_tpi != 0;
-  const PipeLayout<R> lay(CX, nz, NST, moist, has_tpi);
+  const PipeLayout<R> lay(CX, nz, NST, moist, has_tpi, PROF);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_pipe);
   uint64_t* empty = full + NST;
   const int tid = threadIdx.x;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
   __syncthreads();
 
   if (tid >= NC) {
-    if (tid == NC) pipe_produce<R, CX, NST>(p, lay, smem_pipe, full, empty, ntx, ntiles);
+    if (tid == NC) pipe_produce<R, CX, NST, PROF>(p, lay, smem_pipe, full, empty, ntx, ntiles);
     return;
   }
 
@@ -156,6 +156,12 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
   R* sB = sA + n1;
   R* sC = sB + n1;
   R* sD = sC + n1;
+  // (PROF) the coefficient fields' level values, once per CTA
+  R* lvl_prof = sD + n1;
+  if (PROF) {
+    for (int q = tid; q < PF_N * (nz + 1); q += NC) lvl_prof[q] = p.prof[q];
+    tma::named_sync(1, NC);
+  }
   const R dtau = a.dtau;
   const R c1 = ((R)1 + a.p.acoustic_beta) * (R)0.5;
   const R c2 = ((R)1 - a.p.acoustic_beta) * (R)0.5;
@@ -191,10 +197,11 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
     const R* sQR = fld(TC_QR);
     const R* sQVB = fld(TC_QVB);
 #define UF(k, d) sU[(k) * (CX + 4) + tx + (d)]
-#define RXF(k, d) sRX[(k) * (CX + 4) + tx + (d)]
+#define RXF(k, d) (PROF ? lvl_prof[PF_RTJX * (nz + 1) + (k)] : sRX[(k) * (CX + 4) + tx + (d)])
 #define VF(k, r) sV[((k) * 2 + (r)) * CX + tx]
-#define RYF(k, r) sRY[((k) * 2 + (r)) * CX + tx]
+#define RYF(k, r) (PROF ? lvl_prof[PF_RTJY * (nz + 1) + (k)] : sRY[((k) * 2 + (r)) * CX + tx])
 #define CF(X, k) X[(k) * CX + tx]
+#define PF(X, q, k) (PROF ? lvl_prof[(q) * (nz + 1) + (k)] : CF(X, k))
 #define SQ(X, k) X[(size_t)(k) * CX + tx]
     const int i = (t % ntx) * CX + tx, j = t / ntx;
     const bool active = i < L.nx;
@@ -211,7 +218,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
         const int k = klo - 1 + q;
         R avk = 0, svk = 0;
         if (q <= ch + 1 && k >= 1 && k < nz) {
-          avk = CF(sAW, k);
+          avk = PF(sAW, PF_AW, k);
           if (terrain) {
             R uw = (R)0.25 * (UF(k - 1, 0) + UF(k - 1, 1) + UF(k, 0) + UF(k, 1));
             R vw = (R)0.25 * (VF(k - 1, 0) + VF(k - 1, 1) + VF(k, 0) + VF(k, 1));
@@ -228,7 +235,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
         R pk = 0, ek = 0;
         if (q <= ch && k >= 0 && k < nz) {
           const int kk = L.at1(k);
-          R Kt = CF(sKT, k);
+          R Kt = PF(sKT, PF_KT3, k);
           R Dh = (RXF(k, 1) * UF(k, 1) - RXF(k, 0) * UF(k, 0)) * mcx +
                  (RYF(k, 1) * VF(k, 1) - RYF(k, 0) * VF(k, 0)) * mcy;
           R idz = a.co.inv_dzc[kk];
@@ -248,13 +255,13 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
         if (q <= ch && k < nz) {
           th[q] = CF(sTH, k);
           tt[q] = CF(sTTH, k);
-          db[q] = CF(sDTHB, k);
+          db[q] = PF(sDTHB, PF_DTHB, k);
         }
         if (q <= ch && k >= 1 && k < nz) {
           const int kk = L.at1(k);
           const R iJdz = invJ * a.co.inv_dzw[kk];
           R thc = th[q], thm = CF(sTH, k - 1);
-          R thbw = CF(sTHBW, k);
+          R thbw = PF(sTHBW, PF_THBW, k);
           R thvw = thbw + (R)0.5 * (thm + thc);
           if (moist) thvw *= (R)1 + Phys<R>::eps61 * (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k));
           R G = dtau * Phys<R>::cp * thvw * c1 * iJdz;
@@ -264,7 +271,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
           SQ(sC, k) = -G * Ek * av[q + 1];
           R buoy = Phys<R>::grav * (R)0.5 * (thm + thc) / thbw;
           if (moist) {
-            R dqv = (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k)) - (R)0.5 * (CF(sQVB, k - 1) + CF(sQVB, k));
+            R dqv = (R)0.5 * (CF(sQV, k - 1) + CF(sQV, k)) - (R)0.5 * (PF(sQVB, PF_QVB, k - 1) + PF(sQVB, PF_QVB, k));
             R qcr = (R)0.5 * (CF(sQC, k - 1) + CF(sQC, k)) + (R)0.5 * (CF(sQR, k - 1) + CF(sQR, k));
             buoy += Phys<R>::grav * (Phys<R>::eps61 * dqv - qcr);
           }
@@ -347,6 +354,7 @@ __global__ void __launch_bounds__(CX * KL + 32, CX == 32 ? 1 : 2)
 #undef VF
 #undef RYF
 #undef CF
+#undef PF
 #undef SQ
   }
 }
@@ -612,18 +620,32 @@ void launch_pipe_pcr(int f, int grid, int threads, size_t sm, cudaStream_t st, c
   }
 }
 
-template <typename R, int F>
+template <typename R, int F, bool PROF>
 struct PipeKernel {
   static constexpr PipeShape S = kPipeShapes[F];
-  static constexpr auto fn = k_acoustic_column_pipe<R, S.cx, S.kl, S.kch, S.nst>;
+  static constexpr auto fn = k_acoustic_column_pipe<R, S.cx, S.kl, S.kch, S.nst, PROF>;
 };
 
-template <typename R>
+template <typename R, bool PROF>
 const void* pipe_fn(int f) {
   switch (f) {
-    case 0: return reinterpret_cast<const void*>(PipeKernel<R, 0>::fn);
-    case 1: return reinterpret_cast<const void*>(PipeKernel<R, 1>::fn);
-    default: return reinterpret_cast<const void*>(PipeKernel<R, 2>::fn);
+    case 0: return reinterpret_cast<const void*>(PipeKernel<R, 0, PROF>::fn);
+    case 1: return reinterpret_cast<const void*>(PipeKernel<R, 1, PROF>::fn);
+    default: return reinterpret_cast<const void*>(PipeKernel<R, 2, PROF>::fn);
+  }
+}
+
+template <typename R>
+const void* pipe_fn(int f, bool prof) {
+  return prof ? pipe_fn<R, true>(f) : pipe_fn<R, false>(f);
+}
+
+template <typename R, bool PROF>
+void launch_pipe(int f, int grid, int threads, size_t sm, cudaStream_t st, const PipeColParams<R>& p) {
+  switch (f) {
+    case 0: PipeKernel<R, 0, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
+    case 1: PipeKernel<R, 1, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
+    default: PipeKernel<R, 2, PROF>::fn<<<grid, threads, sm, st>>>(p); break;
   }
 }
 
@@ -653,11 +675,12 @@ void acoustic_pipe_box(int shape, int f, int nz, int* bx, int* by, int* bz) {
 }
 
 template <typename R>
-size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi) {
+size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi, bool prof) {
   if (shape < 0 || shape >= kNumPipeShapes) return 0;
   const PipeShape& S = kPipeShapes[shape];
   if (nz + 1 > S.kl * S.kch || nz + 1 > 256) return 0;  // chunks; a box extent is <= 256
-  const size_t t = PipeLayout<R>(S.cx, nz, S.nst, moist, tpi).total;
+  const size_t t = PipeLayout<R>(S.cx, nz, S.nst, moist, tpi, prof).total +
+                   (prof ? (size_t)PF_N * (nz + 1) * sizeof(R) : 0);
   return t <= 227 * 1024 ? t : 0;
 }
 
@@ -675,21 +698,23 @@ size_t acoustic_pipe_pcr_smem(int shape, int nz, bool moist, bool tpi, bool prof
 template <typename R>
 int prepare_acoustic_pipe(int nz) {
   bool any = false;
-  // kinds: the Thomas pipeline, the parallel-solve pipeline with boxes for
-  // every field, and with the level tables
-  for (int kind = 0; kind < 3; ++kind)
-    for (int f = 0; f < (kind ? kNumPipePcrShapes : kNumPipeShapes); ++f) {
-      size_t sm = 0;
-      for (int moist = 0; moist < 2; ++moist)
-        for (int tpi = 0; tpi < 2; ++tpi) {
-          const size_t t = kind ? acoustic_pipe_pcr_smem<R>(f, nz, moist != 0, tpi != 0, kind == 2)
-                                : acoustic_pipe_smem<R>(f, nz, moist != 0, tpi != 0);
-          if (t > sm) sm = t;
-        }
-      if (!sm) continue;
-      if (raise_smem_limit(kind ? pipe_pcr_fn<R>(f, kind == 2) : pipe_fn<R>(f), sm) != cudaSuccess) return 1;
-      any = true;
-    }
+  // kinds: the Thomas pipeline and the parallel-solve pipeline, each with
+  // boxes for every field (prof 0) and with the level tables (prof 1)
+  for (int pcr = 0; pcr < 2; ++pcr)
+    for (int prof = 0; prof < 2; ++prof)
+      for (int f = 0; f < (pcr ? kNumPipePcrShapes : kNumPipeShapes); ++f) {
+        size_t sm = 0;
+        for (int moist = 0; moist < 2; ++moist)
+          for (int tpi = 0; tpi < 2; ++tpi) {
+            const size_t t = pcr ? acoustic_pipe_pcr_smem<R>(f, nz, moist != 0, tpi != 0, prof != 0)
+                                 : acoustic_pipe_smem<R>(f, nz, moist != 0, tpi != 0, prof != 0);
+            if (t > sm) sm = t;
+          }
+        if (!sm) continue;
+        if (raise_smem_limit(pcr ? pipe_pcr_fn<R>(f, prof != 0) : pipe_fn<R>(f, prof != 0), sm) != cudaSuccess)
+          return 1;
+        any = true;
+      }
   return any ? 0 : 2;
 }
 
@@ -717,24 +742,22 @@ int launch_acoustic_column_pipe_pcr(const PipeColParams<R>& p, int f, cudaStream
 
 template <typename R>
 int launch_acoustic_column_pipe(const PipeColParams<R>& p, int f, cudaStream_t st) {
-  const size_t sm = acoustic_pipe_smem<R>(f, p.a.L.nz, p.a.p.moisture != 0, p.has_tpi != 0);
+  const bool prof = p.prof != nullptr;
+  const size_t sm = acoustic_pipe_smem<R>(f, p.a.L.nz, p.a.p.moisture != 0, p.has_tpi != 0, prof);
   if (!sm) return 2;
   const PipeShape& S = kPipeShapes[f];
   const int ntiles = (p.a.L.nx + S.cx - 1) / S.cx * p.a.L.ny;
   const int threads = S.cx * S.kl + 32;
-  const int lim = pipe_grid_limit(pipe_fn<R>(f), threads, sm);
+  const int lim = pipe_grid_limit(pipe_fn<R>(f, prof), threads, sm);
   if (lim <= 0) return 2;
   const int grid = ntiles < lim ? ntiles : lim;
-  switch (f) {
-    case 0: PipeKernel<R, 0>::fn<<<grid, threads, sm, st>>>(p); break;
-    case 1: PipeKernel<R, 1>::fn<<<grid, threads, sm, st>>>(p); break;
-    default: PipeKernel<R, 2>::fn<<<grid, threads, sm, st>>>(p); break;
-  }
+  if (prof) launch_pipe<R, true>(f, grid, threads, sm, st, p);
+  else launch_pipe<R, false>(f, grid, threads, sm, st, p);
   return 0;
 }
 
 #define WFE_INST(R)                                                              \
-  template size_t acoustic_pipe_smem<R>(int, int, bool, bool);                   \
+  template size_t acoustic_pipe_smem<R>(int, int, bool, bool, bool);             \
   template size_t acoustic_pipe_pcr_smem<R>(int, int, bool, bool, bool);         \
   template int prepare_acoustic_pipe<R>(int);                                    \
   template int launch_acoustic_column_pipe<R>(const PipeColParams<R>&, int, cudaStream_t); \

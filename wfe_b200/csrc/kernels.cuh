@@ -362,7 +362,7 @@ struct TmaColParams {
 // boxes of acoustic_pipe_box for the chosen shape.
 // The column inputs that depend on the level alone when the base state and
 // the metric are horizontally uniform (flat ground, one map factor): the
-// parallel-solve pipeline then reads them from per-level tables, in this
+// pipelined column kernels then read them from per-level tables, in this
 // order, instead of streaming a box of each per tile.
 enum { PF_RTJX = 0, PF_RTJY, PF_AW, PF_KT3, PF_THBW, PF_DTHB, PF_QVB, PF_N };
 WFE_HD int pipe_prof_slot(int f) {
@@ -390,7 +390,7 @@ int acoustic_pipe_shapes();
 void acoustic_pipe_box(int shape, int f, int nz, int* bx, int* by, int* bz);
 // 0 when the shape's stages do not fit in shared memory
 template <typename R>
-size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi);
+size_t acoustic_pipe_smem(int shape, int nz, bool moist, bool tpi, bool prof = false);
 // raises every shape's shared-memory limit to the largest layout it may use
 template <typename R>
 int prepare_acoustic_pipe(int nz);

@@ -777,6 +777,12 @@ class ModelT final : public Model {
     const int f = tune_.column_cx - acoustic_column_shapes() - 1;
     return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
   }
+  void variants(int out[4]) const override {
+    out[0] = tune_.done ? tune_.tend_variant : -1;
+    out[1] = tune_.done ? tune_.column_cx : -1;
+    out[2] = tune_.done ? tune_.uv_variant : -1;
+    out[3] = lvl_tab_ != nullptr ? 1 : 0;
+  }
   // chunked column variants follow the fused ones; -1 for other variants
   int chunked_index(int v) const {
     const int f = v - acoustic_column_shapes() - 1 - acoustic_fused_shapes();
@@ -815,7 +821,7 @@ class ModelT final : public Model {
   bool pipe_usable(int v) const {
     const int f = pipe_index(v);
     return pipe_ok_ && f >= 0 &&
-           acoustic_pipe_smem<R>(f, g_.nz, dp_.moisture != 0, bdy_on_) > 0;
+           acoustic_pipe_smem<R>(f, g_.nz, dp_.moisture != 0, bdy_on_, lvl_tab_ != nullptr) > 0;
   }
   bool fused_usable(int v) const {
     const int f = v - acoustic_column_shapes() - 1;
@@ -1213,7 +1219,7 @@ class ModelT final : public Model {
           launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe_pcr<R>(pp, f, st_); });
         } else if (pipe_usable(tune_.column_cx) &&
                    acoustic_pipe_smem<R>(pipe_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
-                                         a.tpi != nullptr) > 0) {
+                                         a.tpi != nullptr, lvl_tab_ != nullptr) > 0) {
           // (operator-level calls add the slow pi' tendency box: when that no
           // longer fits, the plain column kernel below takes the launch)
           const int f = pipe_index(tune_.column_cx);
@@ -1347,7 +1353,7 @@ class ModelT final : public Model {
     pp->a = a;
     pp->err = tma_err_;
     pp->has_tpi = a.tpi != nullptr;
-    pp->prof = pcr ? lvl_tab_ : nullptr;
+    pp->prof = lvl_tab_;
     const R* src[TC_N] = {a.u_out,  a.co.rtjx, a.v_out, a.co.rtjy, a.w_in,   a.pi_cur,
                           a.th_in,  a.tw,      a.tth,   a.tpi,     a.co.aw,  a.co.kt3,
                           a.b.thbw, a.b.dthbdz, a.qv,   a.qc,      a.qr,     a.b.qvb};
@@ -1450,7 +1456,7 @@ class ModelT final : public Model {
   // When every column of the run-constant column coefficients (the
   // reference's rtjx, rtjy, aw, kt3, theta_b^w, dtheta_b/dz, qv_b) holds the
   // same values level by level -- flat ground and a uniform map factor --
-  // the pipelined parallel-solve column reads them from per-level tables
+  // the pipelined column kernels read them from per-level tables
   // (the values of column (0, 0)) instead of streaming a box of each per
   // tile: the same values, bit for bit.  Checked over the points the column
   // kernel reads; WFE_COLUMN_PROFILES=0 keeps the boxes.

@@ -104,6 +104,9 @@ class Model {
   virtual void* state_field(int field) = 0;  // time-n device buffer of a field
   virtual void* stream_handle() const = 0;
   virtual int column_shape() const = 0;      // acoustic column tile in use
+  // tendency, acoustic column and u, v variants (-1 before tuning), and
+  // whether the column coefficients have per-level tables
+  virtual void variants(int out[4]) const = 0;
   // buffer -> linearised buffer map behind ROLE_LIN (empty function: none)
   virtual void set_lin_map(std::function<void*(const void*)> map) = 0;
   // whether the step is one the linearised kernels cover (why not, if not)
