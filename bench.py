@@ -125,6 +125,10 @@ DRY_STEP_FIELDS = 3 * 10 + 10 * 22
 # cell: 7 fields fewer (6 dry).
 TABLE_FIELDS, DRY_TABLE_FIELDS = 7, 6
 PIPE_VARIANTS = set(range(13, 16)) | set(range(19, 23))
+# With the base state in per-level tables (a horizontally uniform base state)
+# the mass fluxes read neither rho_b nor rho_b^w per cell, Kessler neither
+# theta_b, pi_b nor rho_b, the u, v step not theta_b.
+BASE_TABLE_FIELDS = {"mass_flux": 2, "kessler": 3, "acoustic_uv": 1}
 
 
 def use_workload(name: str) -> None:
@@ -723,13 +727,19 @@ def main():
         tab = TABLE_FIELDS if moist else DRY_TABLE_FIELDS
         kf = dict(kf, acoustic_column=kf["acoustic_column"] - tab)
         step_fields -= tab * kt.get("acoustic_column", (0.0, 0))[1]
+    if variants["base_tables"]:
+        for kname, nf in BASE_TABLE_FIELDS.items():
+            if kname in kf and (kname != "kessler" or moist):
+                kf = dict(kf, **{kname: kf[kname] - nf})
+                step_fields -= nf * kt.get(kname, (0.0, 0))[1]
     alg_bytes = kf.get(dom_name, 0) * 4 * cells
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (avg_ms / 1000.0) / 1e9
     traffic = None
     tname = WORKLOADS[WORKLOAD][3]
     tf = ROOT / "profiles" / tname if tname else None
-    tkey = dom_name + ("_tables" if tables and dom_name == "acoustic_column" else "")
+    tkey = dom_name + ("_tables" if (tables and dom_name == "acoustic_column") or
+                       (variants["base_tables"] and dom_name in BASE_TABLE_FIELDS) else "")
     if tf is not None and tf.exists():
         for ln in tf.read_text().splitlines():
             parts = ln.split()

@@ -130,9 +130,10 @@ long wfe_launches_per_step(const wfe_ctx* ctx);
 /* The kernel variants the case runs (no reference counterpart): out[0] the
  * tendency variant, out[1] the acoustic column variant, out[2] the forward
  * u, v variant (all -1 before the first wfe_step / wfe_run tunes them), and
- * out[3] 1 when the coefficient fields are horizontally uniform and the
- * pipelined column kernels (variants 13-15 and 19-22) read them from
- * per-level tables. */
+ * out[3] a bit set of the per-level tables in use where the set-up is
+ * horizontally uniform: 1 the column coefficients (read by the pipelined
+ * column kernels, variants 13-15 and 19-22), 2 the base state (read by the
+ * mass-flux, Kessler and u, v kernels). */
 int wfe_case_variants(const wfe_ctx* ctx, int out[4]);
 
 /* nsteps graph-replayed steps timed with CUDA events recorded on the

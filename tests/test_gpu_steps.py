@@ -348,19 +348,20 @@ def test_pipelined_parallel_solve_equals_parallel_solve(name, prec, monkeypatch)
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["wk82_small", "moist_blob", "bubble_open", "schaer_open"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_pipelined_column_level_tables_equal_boxes(name, prec, monkeypatch):
+def test_level_tables_equal_fields(name, prec, monkeypatch):
     """On flat ground the column coefficients (rtjx, rtjy, aw, kt3, theta_b^w,
-    dtheta_b/dz, qv_b) hold one value per level, and the pipelined column
-    kernels (Thomas 13-15, parallel solve 19-22) read them from per-level
-    tables instead of streaming a box of each per tile: the same fields, bit
-    for bit, as with the boxes (WFE_COLUMN_PROFILES=0) after five steps.
-    With terrain (schaer_open) the tables are not built and both runs stream
-    boxes."""
-    for v in ("13", "14", "15", "19", "20", "21", "22"):
+    dtheta_b/dz, qv_b) and the base state hold one value per level: the
+    pipelined column kernels (Thomas 13-15, parallel solve 19-22) read the
+    coefficients from per-level tables instead of streaming a box of each per
+    tile, and the mass-flux, Kessler and u, v kernels the base state
+    (thb, pib, rhob, rhobw).  The same fields, bit for bit, as from the 3D
+    fields (WFE_LEVEL_TABLES=0) after five steps, for those variants and the
+    plain column tile (0).  With terrain (schaer_open) no table is built."""
+    for v in ("0", "13", "14", "15", "19", "20", "21", "22"):
         monkeypatch.setenv("WFE_COLUMN_VARIANT", v)
         out = {}
         for prof in ("1", "0"):
-            monkeypatch.setenv("WFE_COLUMN_PROFILES", prof)
+            monkeypatch.setenv("WFE_LEVEL_TABLES", prof)
             c = W.Case(CASES / f"{name}.ini", precision=prec)
             c.run(5, c.dt, 0.0)
             c.sync()
@@ -368,6 +369,7 @@ def test_pipelined_column_level_tables_equal_boxes(name, prec, monkeypatch):
             var = c.variants()
             assert var["column"] == int(v)
             assert var["level_tables"] == (prof == "1" and name != "schaer_open"), (v, var)
+            assert var["base_tables"] == (prof == "1" and name != "schaer_open"), (v, var)
             c.close()
         for k in W.FIELDS:
             assert np.array_equal(out["1"][k], out["0"][k]), (v, k)

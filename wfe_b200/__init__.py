@@ -331,10 +331,11 @@ class Case:
 
     def variants(self) -> dict:
         """The tuned kernel variants (-1 before the first step) and whether the
-        column coefficients are read from per-level tables."""
+        column coefficients and the base state are read from per-level tables."""
         out = (C.c_int * 4)()
         self._check(self._lib.wfe_case_variants(self._h, out))
-        return {"tendencies": out[0], "column": out[1], "uv": out[2], "level_tables": out[3] == 1}
+        return {"tendencies": out[0], "column": out[1], "uv": out[2], "level_tables": bool(out[3] & 1),
+                "base_tables": bool(out[3] & 2)}
 
     # ------------------------------------------------------ operator API
     def apply_bcs(self) -> None:

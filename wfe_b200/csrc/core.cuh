@@ -75,7 +75,13 @@ template <typename R>
 struct DBase {
   const R *thb, *pib, *rhob, *dthbdz, *thbw, *rhobw, *thvb, *thvbw, *qvb;  // 3D
   const R* ub;                                                             // [pz]
+  // When the base state is horizontally uniform (its every column holds the
+  // same values): thb, pib, rhob and rhobw by level, BL_N x pz values (level
+  // index at1(k)), which the mass-flux, Kessler and u, v kernels read instead
+  // of the 3D fields -- the same values.  Null otherwise.
+  const R* lvl;
 };
+enum { BL_THB = 0, BL_PIB, BL_RHOB, BL_RHOBW, BL_N };
 
 // Run-constant acoustic coefficients (src/dynamics/kernels.hpp:46-52).
 template <typename R>

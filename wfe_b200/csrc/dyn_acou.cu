@@ -76,11 +76,17 @@ __device__ __forceinline__ R pistar_at(const AcouArgs<R>& a, int c) {
   return cur + a.p.acoustic_smdiv * (cur - a.pi_prev[c]);
 }
 
+// theta_v from the cell's base theta thb
 template <typename R>
-__device__ __forceinline__ R theta_v_at(const AcouArgs<R>& a, int c) {
-  R t = a.b.thb[c] + a.th_in[c];
+__device__ __forceinline__ R theta_v_with(const AcouArgs<R>& a, int c, R thb) {
+  R t = thb + a.th_in[c];
   if (a.p.moisture) t *= (R)1 + Phys<R>::eps61 * a.qv[c];
   return t;
+}
+
+template <typename R>
+__device__ __forceinline__ R theta_v_at(const AcouArgs<R>& a, int c) {
+  return theta_v_with(a, c, a.b.thb[c]);
 }
 
 // u (d = 1) or v (d = L.px) forward step at an interior face, with the
@@ -343,7 +349,8 @@ __device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int
 // block when there is one, instead of loading the neighbour's five fields.
 constexpr int kUvBx = 16, kUvBy = 16, kUvBz = 1;
 
-template <typename R>
+// HB: the base theta of the block's level from its level table (DBase::lvl)
+template <typename R, bool HB = false>
 __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
   __shared__ R s_tv[kUvBz][kUvBy][kUvBx], s_ps[kUvBz][kUvBy][kUvBx];
   const Layout& L = a.L;
@@ -363,8 +370,10 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
   FaceMetric<R> gu{}, gv{};
   const int kk = L.at1(k);
   const int c2 = L.at2i(i, j);
+  // theta_v of a cell of this level (the base theta from the table when HB)
+  auto thv = [&](int cc) { return HB ? theta_v_with(a, cc, a.b.lvl[BL_THB * L.pz + kk]) : theta_v_at(a, cc); };
   if (has_cell) {
-    tv0 = theta_v_at(a, c);
+    tv0 = thv(c);
     ps0 = pistar_at(a, c);
   }
   if (inner) {
@@ -375,11 +384,11 @@ __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, in
     gu = u_metric(a, c2, kk);
     gv = v_metric(a, c2, kk);
     if (tx == 0) {
-      tvx = theta_v_at(a, c - 1);
+      tvx = thv(c - 1);
       psx = pistar_at(a, c - 1);
     }
     if (ty == 0) {
-      tvy = theta_v_at(a, c - sy);
+      tvy = thv(c - sy);
       psy = pistar_at(a, c - sy);
     }
   }
@@ -434,9 +443,9 @@ __device__ __forceinline__ R v_face(const AcouArgs<R>& a, int i, int j, int k) {
 template <typename R>
 constexpr int kUvMinBlocks = sizeof(R) == 4 ? 8 : 1;
 
-template <typename R>
+template <typename R, bool HB>
 __global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv(AcouArgs<R> a) {
-  uv_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  uv_body<R, HB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R>
 __global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv_batch(Batch<AcouArgs<R>> b) {
@@ -1454,7 +1463,8 @@ dim3 grid_uv_fwd(const Layout& L) {
 
 template <typename R>
 void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st) {
-  k_acoustic_uv<R><<<grid_uv_fwd<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
+  if (a.b.lvl) k_acoustic_uv<R, true><<<grid_uv_fwd<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
+  else k_acoustic_uv<R, false><<<grid_uv_fwd<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
 }
 
 template <typename R>

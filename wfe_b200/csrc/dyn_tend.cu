@@ -115,8 +115,8 @@ __global__ void k_fill_ghosts_batch(Batch<FillArgs<R>> b) {
 // ------------------------------------------------------------- mass fluxes
 // rho_b J weighted horizontal fluxes on the ring -2..n+2 and the
 // contravariant vertical flux on -2..n+1 (kernels.cu:68-97); w levels 0 and
-// nz carry Omega = 0.
-template <typename R>
+// nz carry Omega = 0.  HB: the base state from its level tables (DBase::lvl).
+template <typename R, bool HB = false>
 __device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, int bz) {
   const Layout& L = A.L;
   const DBase<R>& b = A.b;
@@ -132,10 +132,14 @@ __device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, 
   const int k = (int)(bz * blockDim.z + threadIdx.z);
   if (i > L.nx + 2 || j > L.ny + 2 || k > L.nz) return;
   const int c = L.ati(i, j, k);
+  const int kk = L.at1(k);
   if (k < L.nz) {
-    R rjx = (R)0.5 * (b.rhob[L.ati(i - 1, j, k)] * m.jac[L.at2i(i - 1, j)] + b.rhob[c] * m.jac[L.at2i(i, j)]);
+    const R rb = HB ? b.lvl[BL_RHOB * L.pz + kk] : b.rhob[c];
+    const R rbx = HB ? rb : b.rhob[L.ati(i - 1, j, k)];
+    const R rby = HB ? rb : b.rhob[L.ati(i, j - 1, k)];
+    R rjx = (R)0.5 * (rbx * m.jac[L.at2i(i - 1, j)] + rb * m.jac[L.at2i(i, j)]);
     mfx[c] = rjx * u[c];
-    R rjy = (R)0.5 * (b.rhob[L.ati(i, j - 1, k)] * m.jac[L.at2i(i, j - 1)] + b.rhob[c] * m.jac[L.at2i(i, j)]);
+    R rjy = (R)0.5 * (rby * m.jac[L.at2i(i, j - 1)] + rb * m.jac[L.at2i(i, j)]);
     mfy[c] = rjy * v[c];
   }
   if (i > L.nx + 1 || j > L.ny + 1) return;
@@ -148,18 +152,17 @@ __device__ __forceinline__ void flux_body(const FluxArgs<R>& A, int bx, int by, 
   const R hx = m.hx[L.at2i(i, j)], hy = m.hy[L.at2i(i, j)];
   R cross = 0;
   if (hx != (R)0 || hy != (R)0) {
-    const int kk = L.at1(k);
     R fac = (R)1 - m.zeta_w[kk] / m.zt;
     R uw = (R)0.25 * (u[L.ati(i, j, k - 1)] + u[L.ati(i + 1, j, k - 1)] + u[c] + u[L.ati(i + 1, j, k)]);
     R vw = (R)0.25 * (v[L.ati(i, j, k - 1)] + v[L.ati(i, j + 1, k - 1)] + v[c] + v[L.ati(i, j + 1, k)]);
     cross = (uw * hx + vw * hy) * fac;
   }
-  mfz[c] = b.rhobw[c] * (w[c] - cross);
+  mfz[c] = (HB ? b.lvl[BL_RHOBW * L.pz + kk] : b.rhobw[c]) * (w[c] - cross);
 }
 
-template <typename R>
+template <typename R, bool HB>
 __global__ void k_mass_flux(FluxArgs<R> a) {
-  flux_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  flux_body<R, HB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R>
 __global__ void k_mass_flux_batch(Batch<FluxArgs<R>> b) {
@@ -648,7 +651,8 @@ template <typename R>
 void launch_mass_flux(const Layout& L, const DBase<R>& b, const DMetric<R>& m, const R* u,
                       const R* v, const R* w, R* mfx, R* mfy, R* mfz, cudaStream_t st) {
   FluxArgs<R> a{L, b, m, u, v, w, mfx, mfy, mfz};
-  k_mass_flux<R><<<grid_flux(a), dim3(32, 4, 2), 0, st>>>(a);
+  if (b.lvl) k_mass_flux<R, true><<<grid_flux(a), dim3(32, 4, 2), 0, st>>>(a);
+  else k_mass_flux<R, false><<<grid_flux(a), dim3(32, 4, 2), 0, st>>>(a);
 }
 
 template <typename R>

@@ -781,7 +781,7 @@ class ModelT final : public Model {
     out[0] = tune_.done ? tune_.tend_variant : -1;
     out[1] = tune_.done ? tune_.column_cx : -1;
     out[2] = tune_.done ? tune_.uv_variant : -1;
-    out[3] = lvl_tab_ != nullptr ? 1 : 0;
+    out[3] = (lvl_tab_ != nullptr ? 1 : 0) | (db_.lvl != nullptr ? 2 : 0);
   }
   // chunked column variants follow the fused ones; -1 for other variants
   int chunked_index(int v) const {
@@ -1459,10 +1459,14 @@ class ModelT final : public Model {
   // the pipelined column kernels read them from per-level tables
   // (the values of column (0, 0)) instead of streaming a box of each per
   // tile: the same values, bit for bit.  Checked over the points the column
-  // kernel reads; WFE_COLUMN_PROFILES=0 keeps the boxes.
+  // kernel reads.  Likewise the base state's thb, pib, rhob and rhobw for
+  // the mass-flux, Kessler and u, v kernels (DBase::lvl), checked over every
+  // column they read (the interior and its three-wide ring) at levels
+  // 0 .. nz.  WFE_LEVEL_TABLES=0 keeps the 3D fields.
   int level_tables() {
-    const char* e = std::getenv("WFE_COLUMN_PROFILES");
+    const char* e = std::getenv("WFE_LEVEL_TABLES");
     if (e && e[0] == '0') return 0;
+    if (base_tables()) return 1;
     const int nx = g_.nx, ny = g_.ny, nz = g_.nz, n1 = nz + 1;
     const R* src[PF_N] = {rtjx_, rtjy_, aw_, kt3_, db_.thbw, db_.dthbdz, db_.qvb};
     std::vector<R> host(L_.n3()), tab((size_t)PF_N * n1);
@@ -1481,6 +1485,28 @@ class ModelT final : public Model {
     }
     if (!(lvl_tab_ = alloc(tab.size()))) return 1;
     CK(cudaMemcpy(lvl_tab_, tab.data(), tab.size() * sizeof(R), cudaMemcpyHostToDevice));
+    return 0;
+  }
+
+  int base_tables() {
+    const int nx = g_.nx, ny = g_.ny, nz = g_.nz, pz = L_.pz;
+    const R* src[BL_N] = {db_.thb, db_.pib, db_.rhob, db_.rhobw};
+    std::vector<R> host(L_.n3()), tab((size_t)BL_N * pz);
+    for (int q = 0; q < BL_N; ++q) {
+      CK(cudaMemcpy(host.data(), src[q], L_.n3() * sizeof(R), cudaMemcpyDeviceToHost));
+      for (int k = -kOZ; k < pz - kOZ; ++k) {
+        const R v = host[L_.at(0, 0, k)];
+        tab[(size_t)q * pz + L_.at1(k)] = v;
+        if (k < 0 || k > nz) continue;
+        for (int j = -kRefNG; j < ny + kRefNG; ++j)
+          for (int i = -kRefNG; i < nx + kRefNG; ++i)
+            if (std::memcmp(&host[L_.at(i, j, k)], &v, sizeof(R)) != 0) return 0;
+      }
+    }
+    R* d = alloc(tab.size());
+    if (!d) return 1;
+    CK(cudaMemcpy(d, tab.data(), tab.size() * sizeof(R), cudaMemcpyHostToDevice));
+    db_.lvl = d;
     return 0;
   }
 

@@ -17,7 +17,8 @@
 
 namespace wfe {
 
-template <typename R, int CX>
+// HB: the base state from its level tables (DBase::lvl)
+template <typename R, int CX, bool HB = false>
 __device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const Layout& L = a.L;
@@ -34,19 +35,23 @@ __device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by
   __shared__ int nsub_s[CX];
   __shared__ R dts_s[CX];
 #define S(X, k) X[(size_t)(k) * CX + tx]
-  const R J = active ? a.m.jac[L.at2(i, j)] : (R)1;
-  const R rho_sfc = active ? a.b.rhob[L.at(i, j, 0)] : (R)1;
+  // base state at level k of this column (c its cell index)
+  auto rhob = [&](int c, int k) { return HB ? a.b.lvl[BL_RHOB * L.pz + L.at1(k)] : a.b.rhob[c]; };
+  auto thb = [&](int c, int k) { return HB ? a.b.lvl[BL_THB * L.pz + L.at1(k)] : a.b.thb[c]; };
+  auto pib = [&](int c, int k) { return HB ? a.b.lvl[BL_PIB * L.pz + L.at1(k)] : a.b.pib[c]; };
+  const R J = active ? a.m.jac[L.at2i(i, j)] : (R)1;
+  const R rho_sfc = active ? rhob(L.ati(i, j, 0), 0) : (R)1;
 
   // 1) column set-up and the first fall speeds (kessler.cu:199-214)
   R vmax = 0, dmin = (R)1e30;
   if (active)
     for (int k = lane; k < nz; k += KL) {
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       R q = a.qr[c];
       R qk = q > (R)0 ? q : (R)0;
-      R rh = a.b.rhob[c];
+      R rh = rhob(c, k);
       R dz = a.m.dzeta_c[L.at1(k)] * J;
-      R T = (a.b.thb[c] + a.thp[c]) * (a.b.pib[c] + a.pip[c]);
+      R T = (thb(c, k) + a.thp[c]) * (pib(c, k) + a.pip[c]);
       R vk = fall_speed(rh * qk, rho_sfc, rh, T);
       S(qrl, k) = qk;
       S(rhol, k) = rh;
@@ -90,24 +95,24 @@ __device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by
     __syncthreads();
     if (on && s + 1 < nsub)
       for (int k = lane; k < nz; k += KL) {
-        const size_t c = L.at(i, j, k);
+        const int c = L.ati(i, j, k);
         R q = S(qrl, k);
         R rq = S(rhol, k) * (q > (R)0 ? q : (R)0);
-        R T = (a.b.thb[c] + a.thp[c]) * (a.b.pib[c] + a.pip[c]);
+        R T = (thb(c, k) + a.thp[c]) * (pib(c, k) + a.pip[c]);
         S(vr, k) = fall_speed(rq, rho_sfc, S(rhol, k), T);
       }
     __syncthreads();
   }
-  if (active && lane == 0) a.rain[L.at2(i, j)] += acc;
+  if (active && lane == 0) a.rain[L.at2i(i, j)] += acc;
 
   // 3) conversions, evaporation and mixed-phase saturation adjustment,
   //    independent per level (kessler.cu:239-297; phys_common.cuh)
   if (active)
     for (int k = lane; k < nz; k += KL) {
-      const size_t c = L.at(i, j, k);
+      const int c = L.ati(i, j, k);
       R thp = a.thp[c], qv = a.qv[c], qc = a.qc[c], qr = S(qrl, k);
       const R pip = a.pip[c];
-      kessler_convert<R, R>(thp, qv, qc, qr, pip, S(rhol, k), a.b.thb[c], a.b.pib[c], a.dt);
+      kessler_convert<R, R>(thp, qv, qc, qr, pip, S(rhol, k), thb(c, k), pib(c, k), a.dt);
       a.thp[c] = thp;
       a.qv[c] = qv;
       a.qc[c] = qc;
@@ -116,9 +121,9 @@ __device__ __forceinline__ void kessler_body(const KesArgs<R>& a, int bx, int by
 #undef S
 }
 
-template <typename R, int CX>
+template <typename R, int CX, bool HB>
 __global__ void k_kessler(KesArgs<R> a) {
-  kessler_body<R, CX>(a, blockIdx.x, blockIdx.y);
+  kessler_body<R, CX, HB>(a, blockIdx.x, blockIdx.y);
 }
 template <typename R, int CX>
 __global__ void k_kessler_batch(Batch<KesArgs<R>> b) {
@@ -145,11 +150,13 @@ int prepare_kessler(int nz) {
   cudaError_t e;
   if (cx == 32) {
     const size_t sm = kessler_smem<R>(nz, 32, 8);
-    e = raise_smem_limit(k_kessler<R, 32>, sm);
+    e = raise_smem_limit(k_kessler<R, 32, false>, sm);
+    if (e == cudaSuccess) e = raise_smem_limit(k_kessler<R, 32, true>, sm);
     if (e == cudaSuccess) e = raise_smem_limit(k_kessler_batch<R, 32>, sm);
   } else if (cx == 8) {
     const size_t sm = kessler_smem<R>(nz, 8, 32);
-    e = raise_smem_limit(k_kessler<R, 8>, sm);
+    e = raise_smem_limit(k_kessler<R, 8, false>, sm);
+    if (e == cudaSuccess) e = raise_smem_limit(k_kessler<R, 8, true>, sm);
     if (e == cudaSuccess) e = raise_smem_limit(k_kessler_batch<R, 8>, sm);
   } else {
     return 2;
@@ -195,12 +202,18 @@ template <typename R>
 int launch_kessler(const KesArgs<R>& a, cudaStream_t st) {
   const int nz = a.L.nz;
   const int cx = kessler_cx<R>(nz);
-  if (cx == 32)
-    k_kessler<R, 32><<<dim3((a.L.nx + 31) / 32, a.L.ny), dim3(32, 8), kessler_smem<R>(nz, 32, 8), st>>>(a);
-  else if (cx == 8)
-    k_kessler<R, 8><<<dim3((a.L.nx + 7) / 8, a.L.ny), dim3(8, 32), kessler_smem<R>(nz, 8, 32), st>>>(a);
-  else
+  const bool hb = a.b.lvl != nullptr;
+  if (cx == 32) {
+    const dim3 g((a.L.nx + 31) / 32, a.L.ny), t(32, 8);
+    if (hb) k_kessler<R, 32, true><<<g, t, kessler_smem<R>(nz, 32, 8), st>>>(a);
+    else k_kessler<R, 32, false><<<g, t, kessler_smem<R>(nz, 32, 8), st>>>(a);
+  } else if (cx == 8) {
+    const dim3 g((a.L.nx + 7) / 8, a.L.ny), t(8, 32);
+    if (hb) k_kessler<R, 8, true><<<g, t, kessler_smem<R>(nz, 8, 32), st>>>(a);
+    else k_kessler<R, 8, false><<<g, t, kessler_smem<R>(nz, 8, 32), st>>>(a);
+  } else {
     return 2;
+  }
   return 0;
 }
 
