@@ -228,9 +228,10 @@ def test_uv_variants_are_bit_identical(name, prec, monkeypatch):
     interior faces and the flat generic faces from shared memory, lateral
     edges -- radiation or periodic -- and sloped faces by the global-memory
     path; ragged tiles, terrain, moisture, open and periodic boundaries)
-    gives the same values, bit for bit, as the thread-per-face kernel (0)."""
+    gives the same values, bit for bit, as the thread-per-face kernel (0),
+    and so does that kernel in slab-shaped blocks (2: 32 x 2 x 4)."""
     out = {}
-    for v in ("0", "1"):
+    for v in ("0", "1", "2"):
         monkeypatch.setenv("WFE_UV_VARIANT", v)
         c = W.Case(CASES / f"{name}.ini", precision=prec)
         for s in range(3):
@@ -238,8 +239,9 @@ def test_uv_variants_are_bit_identical(name, prec, monkeypatch):
         c.run(3, t0=3 * c.dt)
         out[v] = {k: c.field(k) for k in W.FIELDS}
         c.close()
-    for k in W.FIELDS:
-        assert np.array_equal(out["0"][k], out["1"][k]), k
+    for v in ("1", "2"):
+        for k in W.FIELDS:
+            assert np.array_equal(out["0"][k], out[v][k]), (v, k)
 
 
 @pytest.mark.gpu

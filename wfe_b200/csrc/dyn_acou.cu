@@ -343,21 +343,26 @@ __device__ __forceinline__ R v_face_edge(const AcouArgs<R>& a, int i, int j, int
   return v_forward(a, i, j == L.ny ? 0 : j, k);
 }
 
-// Launched as kUvBx x kUvBy x kUvBz blocks.  Each thread computes theta_v and pi* of
+// Launched as BX x BY x BZ blocks (kUvBx x kUvBy x kUvBz, or kUvShapes[1]
+// where the grid has few rows).  Each thread computes theta_v and pi* of
 // its own cell once and shares them through shared memory: an interior
 // point takes its x (y) neighbour's values from the thread beside it in the
 // block when there is one, instead of loading the neighbour's five fields.
 constexpr int kUvBx = 16, kUvBy = 16, kUvBz = 1;
+// the block shapes of launch_acoustic_uv: square tiles of faces, and tiles
+// two rows high and four levels deep for slabs of a few rows (a 16-row block
+// over the 5 face rows of a 4-row slab idles two thirds of its threads)
+constexpr int kUvShapes[2][3] = {{kUvBx, kUvBy, kUvBz}, {32, 2, 4}};
 
 // HB: the base theta of the block's level from its level table (DBase::lvl)
-template <typename R, bool HB = false>
+template <typename R, bool HB = false, int BX = kUvBx, int BY = kUvBy, int BZ = kUvBz>
 __device__ __forceinline__ void uv_body(const AcouArgs<R>& a, int bx, int by, int bz) {
-  __shared__ R s_tv[kUvBz][kUvBy][kUvBx], s_ps[kUvBz][kUvBy][kUvBx];
+  __shared__ R s_tv[BZ][BY][BX], s_ps[BZ][BY][BX];
   const Layout& L = a.L;
   const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
-  const int i = bx * kUvBx + tx;
-  const int j = by * kUvBy + ty;
-  const int k = bz * kUvBz + tz;
+  const int i = bx * BX + tx;
+  const int j = by * BY + ty;
+  const int k = bz * BZ + tz;
   const bool has_cell = i < L.nx && j < L.ny && k < L.nz;
   const int c = has_cell ? L.ati(i, j, k) : 0;
   const int sy = L.px;
@@ -443,9 +448,9 @@ __device__ __forceinline__ R v_face(const AcouArgs<R>& a, int i, int j, int k) {
 template <typename R>
 constexpr int kUvMinBlocks = sizeof(R) == 4 ? 8 : 1;
 
-template <typename R, bool HB>
+template <typename R, bool HB, int S>
 __global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv(AcouArgs<R> a) {
-  uv_body<R, HB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  uv_body<R, HB, kUvShapes[S][0], kUvShapes[S][1], kUvShapes[S][2]>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <typename R>
 __global__ void __launch_bounds__(256, kUvMinBlocks<R>) k_acoustic_uv_batch(Batch<AcouArgs<R>> b) {
@@ -1461,10 +1466,19 @@ dim3 grid_uv_fwd(const Layout& L) {
   return dim3((L.nx + 1 + kUvBx - 1) / kUvBx, (L.ny + 1 + kUvBy - 1) / kUvBy, (L.nz + kUvBz - 1) / kUvBz);
 }
 
+template <typename R, int S>
+static void launch_uv_shape(const AcouArgs<R>& a, cudaStream_t st) {
+  constexpr int BX = kUvShapes[S][0], BY = kUvShapes[S][1], BZ = kUvShapes[S][2];
+  const Layout& L = a.L;
+  const dim3 g((L.nx + 1 + BX - 1) / BX, (L.ny + 1 + BY - 1) / BY, (L.nz + BZ - 1) / BZ), t(BX, BY, BZ);
+  if (a.b.lvl) k_acoustic_uv<R, true, S><<<g, t, 0, st>>>(a);
+  else k_acoustic_uv<R, false, S><<<g, t, 0, st>>>(a);
+}
+
 template <typename R>
-void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st) {
-  if (a.b.lvl) k_acoustic_uv<R, true><<<grid_uv_fwd<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
-  else k_acoustic_uv<R, false><<<grid_uv_fwd<R>(a.L), dim3(kUvBx, kUvBy, kUvBz), 0, st>>>(a);
+void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st, int shape) {
+  if (shape == 1) launch_uv_shape<R, 1>(a, st);
+  else launch_uv_shape<R, 0>(a, st);
 }
 
 template <typename R>
@@ -1782,7 +1796,7 @@ int launch_acoustic_uv_pipe(const PipeUvParams<R>& p, cudaStream_t st) {
   template bool acoustic_column_fits<R>(int, int);                                             \
   template void launch_acoustic_coef<R>(const Layout&, const DBase<R>&, const DMetric<R>&, R*, \
                                         R*, R*, R*, R*, cudaStream_t);                         \
-  template void launch_acoustic_uv<R>(const AcouArgs<R>&, cudaStream_t);                       \
+  template void launch_acoustic_uv<R>(const AcouArgs<R>&, cudaStream_t, int);                  \
   template int launch_acoustic_column<R>(const AcouArgs<R>&, int, cudaStream_t);               \
   template int prepare_acoustic_column<R>(int);                                                 \
   template bool acoustic_fused_fits<R>(int, int);                                              \

@@ -331,7 +331,9 @@ template <typename R>
 void launch_acoustic_coef(const Layout& L, const DBase<R>& b, const DMetric<R>& m, R* scratch,
                           R* rtjx, R* rtjy, R* kt3, R* aw, cudaStream_t st);
 template <typename R>
-void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st);
+// shape 0: 16 x 16 x 1 face tiles, 1: 32 x 2 x 4 (grids of few rows); the
+// same values either way
+void launch_acoustic_uv(const AcouArgs<R>& a, cudaStream_t st, int shape = 0);
 // TMA variant of the column kernel (dyn_acou.cu): a CTA owns kTmaCX columns of
 // one row; every input column block (levels -1..nz) arrives in shared memory
 // by one bulk tensor load per field, then the five phases run from shared

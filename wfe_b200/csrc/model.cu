@@ -41,7 +41,8 @@ struct Tune {
   int column_cx = 0;     // acoustic column tile shape index (launch_acoustic_column)
   int persist = 0;       // ensembles: 0 one block per work item, 1 persistent grid, 2 members' own
                          // graphs on concurrent streams, 3 members' own graphs one after another
-  int uv_variant = 0;    // forward u, v: 0 thread per face, 1 persistent pipelined tiles
+  int uv_variant = 0;    // forward u, v: 0 thread per face pair in 16 x 16 x 1 blocks, 1 persistent
+                         // pipelined tiles, 2 thread per face pair in 32 x 2 x 4 blocks
   bool done = false;
 };
 
@@ -864,7 +865,7 @@ class ModelT final : public Model {
     std::string name = prop.name;
     for (char& ch : name)
       if (ch == ' ') ch = '_';
-    k << "v6|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
+    k << "v7|" << name << "|" << g_.nx << "x" << g_.ny << "x" << g_.nz << "|" << (sizeof(R) * 8) << "|m"
       << dp_.moisture << "pd" << dp_.pd_moist << "b" << bdy_on_ << "d" << (dp_.diff_K > 0) << "x"
       << (pcr_allowed() ? 0 : 1);
     return k.str();
@@ -910,7 +911,8 @@ class ModelT final : public Model {
   // pipelined column kernel, 16..18 the parallel-solve column kernel and
   // 19..22 its pipelined form, both equal to the others up to rounding),
   // WFE_UV_VARIANT=<n> the forward u, v kernel (0
-  // thread per face, 1 persistent pipelined tiles) and WFE_TEND_VARIANT=<n>
+  // thread per face pair in 16 x 16 x 1 blocks, 1 persistent pipelined tiles,
+  // 2 thread per face pair in 32 x 2 x 4 blocks) and WFE_TEND_VARIANT=<n>
   // the tendency variant (0 fused, 1 split, 2 momentum + TMA-staged scalars,
   // 3 fused with two cells per thread)
   // after tuning, for tests and experiments
@@ -928,7 +930,7 @@ class ModelT final : public Model {
     const char* uvv = std::getenv("WFE_UV_VARIANT");
     if (first && uvv && *uvv) {
       const int v = std::atoi(uvv);
-      if (v == 0 || (v == 1 && uvp_ok_)) tune_.uv_variant = v;
+      if (v == 0 || (v == 1 && uvp_ok_) || v == 2) tune_.uv_variant = v;
     }
     const char* tv = std::getenv("WFE_TEND_VARIANT");
     if (first && tv && *tv) {
@@ -969,7 +971,10 @@ class ModelT final : public Model {
     }
     best = 1e30f;
     const int ns = hp_.acoustic_ns > 1 ? hp_.acoustic_ns : 1;
-    for (int v = 0; v < (uvp_ok_ ? 2 : 1); ++v) {
+    // 0 and 2: one thread per face pair in square and slab-shaped blocks;
+    // 1: the persistent pipelined tiles
+    for (int v = 0; v < 3; ++v) {
+      if (v == 1 && !uvp_ok_) continue;
       float ms;
       tune_.uv_variant = v;
       if (time_ms([&] { return acoustic(N, X, (R)dt / (R)ns, 1, false); }, &ms)) return 1;
@@ -1200,7 +1205,7 @@ class ModelT final : public Model {
           launch("acoustic_uv", [&] { rc = launch_acoustic_uv_pipe<R>(up, st_); });
           if (rc) return fail("pipelined u, v launch");
         } else {
-          launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_); });
+          launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_, tune_.uv_variant == 2 ? 1 : 0); });
         }
       }
       if (!fuse && !record(K_COL, a)) {
