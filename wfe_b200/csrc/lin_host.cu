@@ -244,10 +244,14 @@ class LinT final : public Lin {
         break;
       }
       case K_TEND: launch_tendencies<R>(as<TendArgs<R>>(r), 0, st_); break;
-      case K_UV: launch_acoustic_uv<R>(as<AcouArgs<R>>(r), st_); break;
+      // the forward u, v and column launches through the variants the model
+      // runs (the column adjoint reads the solution from the launch's
+      // outputs, whichever kernel wrote them)
+      case K_UV:
+        if (m_->replay_uv(&as<AcouArgs<R>>(r))) return fail("u, v launch: " + m_->error());
+        break;
       case K_COL:
-        if (launch_acoustic_column<R>(as<AcouArgs<R>>(r), m_->column_shape(), st_))
-          return fail("acoustic column launch");
+        if (m_->replay_column(&as<AcouArgs<R>>(r))) return fail("acoustic column launch: " + m_->error());
         break;
       case K_KES: {
         KesArgs<R> a = as<KesArgs<R>>(r);

@@ -1148,6 +1148,64 @@ class ModelT final : public Model {
     }
   }
 
+  // The tuned forward u, v launch of one substep.
+  int uv_launch(const AcouArgs<R>& a) {
+    int rc = 0;
+    if (uvp_ok_ && tune_.uv_variant == 1) {
+      PipeUvParams<R> up;
+      if (uv_pipe_params(a, &up)) return 1;
+      launch("acoustic_uv", [&] { rc = launch_acoustic_uv_pipe<R>(up, st_); });
+      if (rc) return fail("pipelined u, v launch");
+    } else {
+      launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_, tune_.uv_variant == 2 ? 1 : 0); });
+    }
+    return 0;
+  }
+
+  // The column launch of column variant v (a fused variant's own column
+  // tile when the substep is not fused).
+  int column_launch(const AcouArgs<R>& a, int v) {
+    if (fused_usable(v)) v = acoustic_fused_column_shape(v - acoustic_column_shapes() - 1);
+    int rc = 0;
+    if (chunked_usable(v)) {
+      const int f = chunked_index(v);
+      launch("acoustic_column", [&] { rc = launch_acoustic_column_chunked<R>(a, f, st_); });
+    } else if (pcr_usable(v)) {
+      const int f = pcr_index(v);
+      launch("acoustic_column", [&] { rc = launch_acoustic_column_pcr<R>(a, f, st_); });
+    } else if (pipe_pcr_usable(v) &&
+               acoustic_pipe_pcr_smem<R>(pipe_pcr_index(v), g_.nz, dp_.moisture != 0, a.tpi != nullptr,
+                                         lvl_tab_ != nullptr) > 0) {
+      const int f = pipe_pcr_index(v);
+      PipeColParams<R> pp;
+      if (pipe_params(a, f, &pp, true)) return 1;
+      launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe_pcr<R>(pp, f, st_); });
+    } else if (pipe_usable(v) &&
+               acoustic_pipe_smem<R>(pipe_index(v), g_.nz, dp_.moisture != 0, a.tpi != nullptr,
+                                     lvl_tab_ != nullptr) > 0) {
+      // (operator-level calls add the slow pi' tendency box: when that no
+      // longer fits, the plain column kernel below takes the launch)
+      const int f = pipe_index(v);
+      PipeColParams<R> pp;
+      if (pipe_params(a, f, &pp)) return 1;
+      launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe<R>(pp, f, st_); });
+    } else if (tma_ok_ && v == acoustic_column_shapes()) {
+      TmaColParams<R> tp;
+      if (tma_params(a, &tp)) return 1;
+      launch("acoustic_column", [&] { rc = launch_acoustic_column_tma<R>(tp, st_); });
+    } else {
+      launch("acoustic_column",
+             [&] { rc = launch_acoustic_column<R>(a, v < acoustic_column_shapes() ? v : 0, st_); });
+    }
+    if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
+    return 0;
+  }
+
+  int replay_uv(const void* args) override { return uv_launch(*static_cast<const AcouArgs<R>*>(args)); }
+  int replay_column(const void* args) override {
+    return column_launch(*static_cast<const AcouArgs<R>*>(args), tune_.column_cx);
+  }
+
   // ns acoustic substeps from time n (N) into the stage output X
   int acoustic(R** N, R** X, R dtau, int ns, bool op) {
     AcouArgs<R> a{};
@@ -1202,47 +1260,10 @@ class ModelT final : public Model {
         const int f = tune_.column_cx - acoustic_column_shapes() - 1;
         launch("acoustic_fused", [&] { rc = launch_acoustic_fused<R>(a, f, st_); });
       } else if (!record(K_UV, a)) {
-        if (uvp_ok_ && tune_.uv_variant == 1) {
-          PipeUvParams<R> up;
-          if (uv_pipe_params(a, &up)) return 1;
-          launch("acoustic_uv", [&] { rc = launch_acoustic_uv_pipe<R>(up, st_); });
-          if (rc) return fail("pipelined u, v launch");
-        } else {
-          launch("acoustic_uv", [&] { launch_acoustic_uv<R>(a, st_, tune_.uv_variant == 2 ? 1 : 0); });
-        }
+        if (uv_launch(a)) return 1;
       }
-      if (!fuse && !record(K_COL, a)) {
-        if (chunked_usable(tune_.column_cx)) {
-          const int f = chunked_index(tune_.column_cx);
-          launch("acoustic_column", [&] { rc = launch_acoustic_column_chunked<R>(a, f, st_); });
-        } else if (pcr_usable(tune_.column_cx)) {
-          const int f = pcr_index(tune_.column_cx);
-          launch("acoustic_column", [&] { rc = launch_acoustic_column_pcr<R>(a, f, st_); });
-        } else if (pipe_pcr_usable(tune_.column_cx) &&
-                   acoustic_pipe_pcr_smem<R>(pipe_pcr_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
-                                             a.tpi != nullptr, lvl_tab_ != nullptr) > 0) {
-          const int f = pipe_pcr_index(tune_.column_cx);
-          PipeColParams<R> pp;
-          if (pipe_params(a, f, &pp, true)) return 1;
-          launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe_pcr<R>(pp, f, st_); });
-        } else if (pipe_usable(tune_.column_cx) &&
-                   acoustic_pipe_smem<R>(pipe_index(tune_.column_cx), g_.nz, dp_.moisture != 0,
-                                         a.tpi != nullptr, lvl_tab_ != nullptr) > 0) {
-          // (operator-level calls add the slow pi' tendency box: when that no
-          // longer fits, the plain column kernel below takes the launch)
-          const int f = pipe_index(tune_.column_cx);
-          PipeColParams<R> pp;
-          if (pipe_params(a, f, &pp)) return 1;
-          launch("acoustic_column", [&] { rc = launch_acoustic_column_pipe<R>(pp, f, st_); });
-        } else if (tma_ok_ && tune_.column_cx == acoustic_column_shapes()) {
-          TmaColParams<R> tp;
-          if (tma_params(a, &tp)) return 1;
-          launch("acoustic_column", [&] { rc = launch_acoustic_column_tma<R>(tp, st_); });
-        } else {
-          launch("acoustic_column", [&] { rc = launch_acoustic_column<R>(a, tune_.column_cx, st_); });
-        }
-      }
-      if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "column kernel launch");
+      if (!fuse && !record(K_COL, a) && column_launch(a, tune_.column_cx)) return 1;
+      if (rc) return fail(rc == 2 ? "column too deep for the acoustic kernel" : "fused substep launch");
       uin = uout;
       vin = vout;
       thin = thout;

@@ -104,6 +104,10 @@ class Model {
   virtual void* state_field(int field) = 0;  // time-n device buffer of a field
   virtual void* stream_handle() const = 0;
   virtual int column_shape() const = 0;      // acoustic column tile in use
+  // a recorded forward u, v (column) launch through the tuned variant: the
+  // argument is the launch's AcouArgs
+  virtual int replay_uv(const void* args) = 0;
+  virtual int replay_column(const void* args) = 0;
   // tendency, acoustic column and u, v variants (-1 before tuning), and
   // whether the column coefficients have per-level tables
   virtual void variants(int out[4]) const = 0;
