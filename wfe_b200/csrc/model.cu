@@ -769,15 +769,6 @@ class ModelT final : public Model {
     return (field >= 0 && field < 8) ? S_[perm_[0]][field] : nullptr;
   }
   void* stream_handle() const override { return st_; }
-  // the plain column tile shape of the variant in use (the linearised runs
-  // launch the unfused kernels)
-  int column_shape() const override {
-    if (chunked_index(tune_.column_cx) >= 0 || pipe_index(tune_.column_cx) >= 0 ||
-        pcr_index(tune_.column_cx) >= 0 || pipe_pcr_index(tune_.column_cx) >= 0)
-      return 0;
-    const int f = tune_.column_cx - acoustic_column_shapes() - 1;
-    return f >= 0 ? acoustic_fused_column_shape(f) : tune_.column_cx;
-  }
   void variants(int out[4]) const override {
     out[0] = tune_.done ? tune_.tend_variant : -1;
     out[1] = tune_.done ? tune_.column_cx : -1;

@@ -103,7 +103,6 @@ class Model {
   virtual std::vector<std::pair<void*, size_t>> state_buffers() const = 0;
   virtual void* state_field(int field) = 0;  // time-n device buffer of a field
   virtual void* stream_handle() const = 0;
-  virtual int column_shape() const = 0;      // acoustic column tile in use
   // a recorded forward u, v (column) launch through the tuned variant: the
   // argument is the launch's AcouArgs
   virtual int replay_uv(const void* args) = 0;
